@@ -1,0 +1,327 @@
+"""Benchmark: field solves/s to 1e-8 relative residual on the refined channel tree.
+
+Workload (one "step"): one Poisson field solve L u + s b = 0 from a zero initial guess
+to resnorm(u)/leafnorm(b) <= 1e-8 on the refined channel tree of ~1.5M leaf cells
+(config 2: base uniform tree to level 5 plus 4 refined levels, cylindrical r-z,
+order-2 stencil, Neumann axis/outer radius, Dirichlet electrodes).  Synthetic, seeded
+data with the shapes of the reference's own setup (no published data exists).
+
+  value      mixed-precision solves/s (FP32 V-cycles + FP64 defect correction, FP64
+             direct coarsest-level solve) with fields resident in HBM
+  fp64       the plain FP64 GPU multigrid (the reference's V-cycle, repeated to the
+             same tolerance) on the same tree
+  roofline   the plain FP64 V-cycle: algorithmic bytes of the multigrid model
+             (srmg.model.vcycle_bytes) / measured V-cycle time, against the measured
+             HBM copy peak
+  e2e        the same solve through the C ABI with host arrays (H2D of u and b and
+             D2H of u inside the timed region)
+  cpu_baseline  the oracle (C restatement of the reference FP64 solve, OpenMP) on
+             the host cores, on a bounded sample of V-cycles
+
+`--impl reference` times the reference's CPU algorithm (the oracle, since Julia is not
+available) on the same workload.  Multi-GPU: replicas (independent solves per rank,
+no data-path collective), weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "steamroller.jl_b200"))
+
+import numpy as np  # noqa: E402
+
+TOL = 1e-8
+SEED = 2
+TARGET_LEAF = 1_500_000
+METRIC = "field solves/sec at 1e-8 rel residual (mixed-precision multigrid; plain FP64 GPU alongside)"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) > 8:
+                for k, n in enumerate(names):
+                    if r[5 + k].lower() == "active":
+                        reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=None)
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(x, pg, device):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, device):
+    import torch
+    if pg is not None:
+        pg.barrier(device_ids=[device.index])
+    torch.cuda.synchronize()
+
+
+def run_cpu_reference(problem, fp64_cycles, budget_s=12.0, threads=None, warm=1):
+    """Time reference-algorithm V-cycles (the oracle, OpenMP) on the host cores and
+    scale to solves/s with the FP64 cycle count of the same solve."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc_mod
+    orc_mod.build() if not os.path.exists(orc_mod._LIB_PATH) else None
+    threads = threads or os.cpu_count()
+    orc = orc_mod.Oracle(problem, threads=threads)
+    u = np.zeros_like(problem.b)
+    b = problem.b.copy()
+    r, u1 = np.zeros_like(u), np.zeros_like(u)
+    for _ in range(warm):
+        orc.vcycle(u, b, r, u1, ndown=2, ntop=4, nup=2)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        orc.vcycle(u, b, r, u1, ndown=2, ntop=4, nup=2)
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = (time.perf_counter() - t0) / n
+    # one resnorm per cycle, as the solve loop does
+    t1 = time.perf_counter()
+    orc.resnorm(r, b, u)
+    dt += time.perf_counter() - t1
+    solves_per_s = 1.0 / (fp64_cycles * dt)
+    return {"value": solves_per_s, "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{n} FP64 V-cycles (+resnorm) of the same tree timed ({n * dt:.1f} s), "
+                      f"scaled by the {fp64_cycles} cycles one solve takes",
+            "s_per_vcycle": dt}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="srmg", choices=["srmg", "reference"])
+    ap.add_argument("--target-leaf", type=int, default=TARGET_LEAF)
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    from srmg import gen, model
+    from srmg.tree import leaf_cells
+
+    world, rank, local, pg = dist_setup()
+    problem = gen.config2(seed=SEED, target_leaf=args.target_leaf)
+    nleaf = leaf_cells(problem.tree)
+    cfg = {"workload": "config2: refined channel tree, Poisson, cylindrical r-z, tol 1e-8",
+           "leaf_cells": nleaf, "blocks": problem.tree.nblocks(), "levels": problem.tree.finest_level(),
+           "block": "16x16 + 2 ghosts", "tol": TOL, "vcycle": "(ndown,nup,ntop)=(2,2,4)",
+           "parallelism": f"replicas x{world}", "l2": "flushed between timed steps (256 MB write)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        # FP64 cycle count of this solve: the reference algorithm converges identically on
+        # the GPU path; count cycles with the oracle on a bounded sample instead.
+        cyc = fp64_cycle_count_estimate(problem)
+        cpu = run_cpu_reference(problem, cyc["cycles"], budget_s=max(5.0, 2.0 * args.steps))
+        line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": "solves/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 / cpu["value"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+                "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": cpu["value"], "unit": "solves/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0},
+                "fp64_cycles_per_solve": cyc}
+        print(json.dumps(line))
+        return
+
+    import torch
+    from srmg import multigrid as mg
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = mg.Context(local).set_tree(problem.tree, problem.conn)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    nblk = problem.nblk
+    b = torch.from_numpy(problem.b).to(dev)
+    u = torch.zeros_like(b)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    s, geom, bc = problem.s, problem.geom, problem.bc
+
+    def one_solve(mode, max_cycles=5000):
+        u.zero_()
+        return mg.solve(ctx, u, b, s, geom, bc, tol=TOL, mode=mode, max_cycles=max_cycles)
+
+    def timed(mode, steps, warm):
+        for _ in range(warm):
+            with torch.cuda.stream(stream):
+                st = one_solve(mode)
+        barrier(pg, dev)
+        total_ms, stats = 0.0, None
+        l0 = ctx.launches()
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                u.zero_()
+            stream.synchronize()
+            st = mg.solve(ctx, u, b, s, geom, bc, tol=TOL, mode=mode, max_cycles=5000)
+            total_ms += st["device_ms"]
+            stats = st
+        barrier(pg, dev)
+        return total_ms, stats, ctx.launches() - l0
+
+    with ClockSampler(local) as clk:
+        mixed_ms, mixed_st, launches = timed(mg.MODE_MIXED, args.steps, args.warmup)
+    fp64_steps = max(1, args.fp64_steps)
+    fp64_ms, fp64_st, _ = timed(mg.MODE_FP64, fp64_steps, 1)
+    mixed_ms = max_over_ranks(mixed_ms, pg, dev)
+    fp64_ms = max_over_ranks(fp64_ms, pg, dev)
+    value = world * args.steps / (mixed_ms / 1e3)
+    fp64_value = world * fp64_steps / (fp64_ms / 1e3)
+
+    # roofline of the plain FP64 V-cycle (model bytes / event-timed V-cycle)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    r_, u1_ = torch.zeros_like(b), torch.zeros_like(b)
+    bw = b.clone()
+    nv = 20
+    with torch.cuda.stream(stream):
+        u.zero_()
+        mg.vcycle_(ctx, u, bw, r_, u1_, s, geom, bc, ndown=2, ntop=4, nup=2, ncycles=3)
+        flush.fill_(2.0)
+        ev0.record(stream)
+        mg.vcycle_(ctx, u, bw, r_, u1_, s, geom, bc, ndown=2, ntop=4, nup=2, ncycles=nv)
+        ev1.record(stream)
+    ev1.synchronize()
+    vc_ms = ev0.elapsed_time(ev1) / nv
+    bytes_vc = model.vcycle_bytes(problem.tree, 8, 2, 2, 4)
+    hbm, src = peaks()
+    achieved = bytes_vc / (vc_ms / 1e3) / 1e9
+
+    # e2e through the host-pointer C ABI
+    uh = np.zeros_like(problem.b)
+    bh = problem.b.copy()
+    e2e_t = []
+    for i in range(args.warmup + args.steps):
+        uh[:] = 0.0
+        t0 = time.perf_counter()
+        mg.solve(ctx, uh, bh, s, geom, bc, tol=TOL, mode=mg.MODE_MIXED)
+        if i >= args.warmup:
+            e2e_t.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(float(np.sum(e2e_t)), pg, dev)
+    e2e = {"value": world * args.steps / e2e_s, "unit": "solves/s",
+           "h2d_bytes_per_step": 2 * nblk * 400 * 8, "d2h_bytes_per_step": nblk * 400 * 8}
+
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mixed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": cfg,
+            "fp64": {"value": fp64_value, "unit": "solves/s", "cycles_per_solve": fp64_st["cycles"],
+                     "ms_per_solve": fp64_ms / fp64_steps, "rel_residual": fp64_st["rel_residual"]},
+            "mixed": {"cycles_per_solve": mixed_st["cycles"], "outer_steps": mixed_st["outer"],
+                      "rel_residual": mixed_st["rel_residual"]},
+            "speedup_vs_fp64": value / fp64_value,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None, "peak_source": src,
+                         "kernel": "plain FP64 V-cycle (whole cycle)", "bytes_per_launch": bytes_vc,
+                         "ms_per_vcycle": vc_ms},
+            "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = run_cpu_reference(problem, fp64_st["cycles"])
+        line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def fp64_cycle_count_estimate(problem):
+    """Cycle count of the reference FP64 solve: the oracle's V-cycle contraction over a
+    bounded number of cycles, extrapolated geometrically to the tolerance."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc_mod
+    orc = orc_mod.Oracle(problem, threads=os.cpu_count())
+    u = np.zeros_like(problem.b)
+    b = problem.b.copy()
+    r, u1 = np.zeros_like(u), np.zeros_like(u)
+    bn = orc.leafnorm(b)
+    hist = [orc.resnorm(r, b, u) / bn]
+    for _ in range(12):
+        orc.vcycle(u, b, r, u1, ndown=2, ntop=4, nup=2)
+        hist.append(orc.resnorm(r, b, u) / bn)
+        if hist[-1] <= TOL:
+            return {"cycles": len(hist) - 1, "extrapolated": False}
+    rho = (hist[-1] / hist[-5]) ** 0.25
+    extra = int(np.ceil(np.log(TOL / hist[-1]) / np.log(rho)))
+    return {"cycles": len(hist) - 1 + extra, "extrapolated": True, "rho": rho}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,211 @@
+/*
+ * srmg.h -- C ABI of libsrmg, the B200-native (sm_100a) FAS multigrid field solve for
+ * Steamroller.jl block trees.
+ *
+ * The library replaces the bodies of the Julia entry points
+ *     vcycle!(u, b, r, u1, s, tree, conn, geometry, bc, lpldisc;
+ *             lmax=0, ndown=3, ntop=5, nup=3, omega=1.0)      src/multigrid.jl:60-106
+ *     fmg!(u, b, r, u1, s, tree, conn, geometry, bc, lpldisc;
+ *          lmax=0, ndown=3, ntop=5, nup=3, omega=1.25)        src/multigrid.jl:17-51
+ * and the helpers they call.  Julia keeps the tree and the fields; it passes them
+ * through ccall as plain pointers:
+ *   - fields: ScalarBlockField{2,M,G,Float64} contiguous storage
+ *     (src/blockfield.jl:33-40): nblk blocks of S x S doubles, S = M + 2G, dim 1 (r)
+ *     fastest; element (i, j, blk), 1-based, at (i-1) + S(j-1) + S*S(blk-1);
+ *   - the tree: BlockLayer.pairs per level (src/blocklayer.jl:23);
+ *   - connectivity: the four edge vectors per level (src/connectivity.jl:51-64).
+ * Edge structs below are the isbits layouts of the Julia structs, so Julia vectors
+ * are passed without conversion.  All block indices and coordinates are 1-based.
+ *
+ * Supported: D = 2, M = 16, G = 2, order-2 Laplacian / Helmholtz discretisations,
+ * Cartesian and cylindrical geometries, homogeneous boundary conditions
+ * (GeneralHomogeneousBoundaryConditions, src/boundary.jl:21-38) and a StarStencil
+ * connectivity.  Anything else returns SRMG_ERR_UNSUPPORTED and the Julia shim keeps
+ * the original Julia method.
+ *
+ * Every entry point returns SRMG_OK (0) or a negative SRMG_ERR_* code;
+ * srmg_last_error() gives the message.  A context is not thread-safe; distinct
+ * contexts may be used from distinct threads.
+ */
+#ifndef SRMG_H
+#define SRMG_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SRMG_OK               0
+#define SRMG_ERR_BADARG      -1
+#define SRMG_ERR_BADTREE     -2
+#define SRMG_ERR_CUDA        -3
+#define SRMG_ERR_TIMEOUT     -4
+#define SRMG_ERR_DIVERGED    -5
+#define SRMG_ERR_UNSUPPORTED -6
+#define SRMG_ERR_NOMEM       -7
+#define SRMG_ERR_NOTREE      -8
+
+/* lpldisc: LaplacianDiscretization{2,2} / HelmholtzDiscretization{2,2}(k2)
+ * (src/laplacian.jl:14, src/helmholtz.jl:9-11). */
+#define SRMG_OP_LAPLACIAN 0
+#define SRMG_OP_HELMHOLTZ 1
+/* geometry: CartesianGeometry, CylindricalGeometry{1}, CylindricalGeometry{2}
+ * (src/geometry.jl:14-20). */
+#define SRMG_GEOM_CARTESIAN 0
+#define SRMG_GEOM_CYL1      1
+#define SRMG_GEOM_CYL2      2
+
+/* Pair{CartesianIndex{2},Int}: coord => blk (src/blocklayer.jl:23). */
+typedef struct { int64_t coord[2]; int64_t blk; } srmg_pair;
+/* Neighbor{2} (src/connectivity.jl:14-20): ghost face -face of `to` <- `from`. */
+typedef struct { int64_t from, to; int64_t face[2]; } srmg_neighbor;
+/* Boundary{2} (src/connectivity.jl:6-11). */
+typedef struct { int64_t block; int64_t face[2]; int64_t bnd[2]; int64_t level; } srmg_boundary;
+/* RefBoundary{2} (src/connectivity.jl:23-32). */
+typedef struct { int64_t fine, coarse; int64_t face[2]; int64_t subblock[2]; } srmg_refbnd;
+/* Child{2} (src/connectivity.jl:36-42). */
+typedef struct { int64_t fine, coarse; int64_t subblock[2]; } srmg_child;
+
+typedef struct srmg_ctx srmg_ctx;
+
+/* Create a context on CUDA device `device` (D, M, G must be 2, 16, 2).  The context
+ * owns a CUDA stream, the device copy of the tree and the device mirrors of fields
+ * passed through the host-pointer entry points.  No counterpart in the reference
+ * (its state lives in Julia objects). */
+int srmg_create(srmg_ctx **ctx, int D, int M, int G, int device);
+void srmg_destroy(srmg_ctx *ctx);
+const char *srmg_last_error(const srmg_ctx *ctx);
+
+/* Replace the CUDA stream the context launches on (NULL = the context's own stream).
+ * The *_dev entry points are stream-ordered on it. */
+int srmg_set_stream(srmg_ctx *ctx, void *cuda_stream);
+int srmg_synchronize(srmg_ctx *ctx);
+
+/* Upload tree + connectivity (replaces reading `tree`/`conn` inside vcycle!).
+ * Arrays are indexed by level (level l at index l-1).  `generation` lets callers skip
+ * re-uploads: the Julia shim bumps it whenever connectivity!/refine! runs
+ * (src/streamer.jl:545-549).  Validates indices and nesting; a face written by two
+ * edges, an index out of range or a non-star face gives SRMG_ERR_BADTREE. */
+int srmg_set_tree(srmg_ctx *ctx, int nlev,
+                  const int64_t *npairs, const srmg_pair *const *pairs,
+                  const int64_t *nneighbor, const srmg_neighbor *const *neighbor,
+                  const int64_t *nboundary, const srmg_boundary *const *boundary,
+                  const int64_t *nrefbnd, const srmg_refbnd *const *refbnd,
+                  const int64_t *nchild, const srmg_child *const *child,
+                  uint64_t generation);
+uint64_t srmg_tree_generation(const srmg_ctx *ctx);
+
+/* ---- the ccall boundary: HOST pointers (Julia-owned arrays) --------------------- */
+
+/* `ncycles` x vcycle! (src/multigrid.jl:60-106) on host arrays of nblk_alloc blocks.
+ * u and b are in/out exactly as in the reference (b's non-leaf blocks receive the FAS
+ * right-hand side); r and u1 are scratch and are not written back.  Blocks until u
+ * and b are back in host memory.  bc is the 3x3 Int8 table of
+ * GeneralHomogeneousBoundaryConditions, column-major (src/boundary.jl:28-38). */
+int srmg_vcycle(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, int64_t nblk_alloc,
+                double s, int op, double k2, int geom, const int8_t bc[9],
+                int lmax, int ndown, int ntop, int nup, double omega, int ncycles);
+
+/* fmg! (src/multigrid.jl:17-51) on host arrays; u and b in/out, r and u1 scratch. */
+int srmg_fmg(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, int64_t nblk_alloc,
+             double s, int op, double k2, int geom, const int8_t bc[9],
+             int ndown, int ntop, int nup, double omega);
+
+/* resnorm! (src/multigrid.jl:391-417): *out = sqrt(sum over leaf cells of r^2 scaled
+ * by 4^-(l-1)), with r = -(b + L u / s_l) on every level.  r is scratch. */
+int srmg_resnorm(srmg_ctx *ctx, double *r, const double *b, const double *u, int64_t nblk_alloc,
+                 double s, int op, double k2, int geom, const int8_t bc[9], double *out);
+
+/* fill_ghost!(u, level, conn, bc) (src/connectivity.jl:155-159) on a host array. */
+int srmg_fill_ghost(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level, const int8_t bc[9]);
+
+/* Solve L u + s b = 0 to a relative residual: resnorm(u) / leafnorm(b) <= tol, where
+ * leafnorm is the resnorm! norm applied to b.  The reference has no tolerance loop
+ * (it runs poisson_iter fixed V-cycles, src/streamer.jl:322-334); this is the loop
+ * built on its vcycle!/resnorm! semantics.
+ *   mode SRMG_MODE_FP64 : repeated reference V-cycles in FP64 (bit-for-bit the
+ *                         vcycle! algorithm), residual checked after each cycle;
+ *   mode SRMG_MODE_MIXED: FP64 defect correction around FP32 V-cycles (smoothing,
+ *                         restriction, prolongation in FP32), FP64 residual, FP64
+ *                         coarsest-level direct solve and FP64 norms.
+ * u holds the initial guess on entry (ghosts filled) and the solution on exit
+ * (ghosts filled); b is read-only in both modes. */
+#define SRMG_MODE_FP64  0
+#define SRMG_MODE_MIXED 1
+typedef struct {
+    double tol;          /* relative residual target, e.g. 1e-8 */
+    int max_cycles;      /* cap on V-cycles (FP64) or outer steps (mixed) */
+    int mode;            /* SRMG_MODE_* */
+    int ndown, ntop, nup;
+    double omega;
+    int inner_cycles;    /* mixed: FP32 V-cycles per defect-correction step (>= 1) */
+    int warm_start;      /* 0: start from u; 1: learned initial guess (srmg_cnn_*) */
+} srmg_solve_opts;
+
+typedef struct {
+    int status;          /* SRMG_OK or an error code */
+    int cycles;          /* V-cycles run (FP64 or FP32) */
+    int outer;           /* defect-correction steps (mixed), 0 in FP64 mode */
+    double rel_residual; /* final resnorm(u)/leafnorm(b) */
+    double initial_rel;  /* before the first cycle */
+    double bnorm;        /* leafnorm(b) */
+    double device_ms;    /* device time of the solve (CUDA events) */
+} srmg_stats;
+
+void srmg_solve_opts_default(srmg_solve_opts *opts);
+int srmg_solve(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc,
+               double s, int op, double k2, int geom, const int8_t bc[9],
+               const srmg_solve_opts *opts, srmg_stats *stats);
+
+/* ---- DEVICE pointers (fields already resident in HBM) --------------------------- */
+/* Same semantics as the host entry points; pointers are device addresses of
+ * nblk_alloc-block fields; work is ordered on the context's stream and these calls
+ * return without synchronising (except solve/resnorm, which read a norm back). */
+int srmg_vcycle_dev(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
+                    int64_t nblk_alloc, double s, int op, double k2, int geom,
+                    const int8_t bc[9], int lmax, int ndown, int ntop, int nup,
+                    double omega, int ncycles);
+int srmg_fmg_dev(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, int64_t nblk_alloc,
+                 double s, int op, double k2, int geom, const int8_t bc[9],
+                 int ndown, int ntop, int nup, double omega);
+int srmg_resnorm_dev(srmg_ctx *ctx, double *r, const double *b, const double *u,
+                     int64_t nblk_alloc, double s, int op, double k2, int geom,
+                     const int8_t bc[9], double *out);
+int srmg_solve_dev(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc,
+                   double s, int op, double k2, int geom, const int8_t bc[9],
+                   const srmg_solve_opts *opts, srmg_stats *stats);
+
+/* Single reference routines on device fields (used for per-operation parity). */
+/* fill_ghost! parts (src/connectivity.jl:155-159): mask bit 0 = fill_ghost_copy!,
+ * bit 1 = fill_ghost_bnd!, bit 2 = fill_ghost_interp!; 7 = fill_ghost!. */
+int srmg_fill_ghost_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level,
+                        const int8_t bc[9], int mask);
+/* gauss_seidel_level!(..., RedBlack{parity}) (src/multigrid.jl:238-243). */
+int srmg_gs_level_dev(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, int level,
+                      double omega, double sl, int op, double k2, int geom, int parity);
+/* gauss_seidel_iter! (src/multigrid.jl:250-265). */
+int srmg_gs_iter_dev(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, int level,
+                     double omega, double sl, int n, int op, double k2, int geom,
+                     const int8_t bc[9]);
+/* residual_level! (src/multigrid.jl:349-354). */
+int srmg_residual_level_dev(srmg_ctx *ctx, double *r, const double *u, const double *b,
+                            int64_t nblk_alloc, int level, double sl, int op, double k2, int geom);
+/* restrict_level!(u, conn.child[level]) (src/restrict.jl:31-37). */
+int srmg_restrict_level_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level);
+/* interp_add_level!(u, u1, conn.child[level]) (src/interp.jl:107-115). */
+int srmg_interp_add_level_dev(srmg_ctx *ctx, double *u, const double *u1, int64_t nblk_alloc,
+                              int level);
+/* residual_postrestrict_level!(b, u, r, s, tree[level-1], conn.child[level], ...)
+ * (src/multigrid.jl:112-119); s is the coarse-level scale. */
+int srmg_residual_postrestrict_level_dev(srmg_ctx *ctx, double *b, const double *u,
+                                         const double *r, int64_t nblk_alloc, int level,
+                                         double s, int op, double k2, int geom);
+
+/* Number of CUDA kernel launches this context has issued (for launch accounting). */
+int64_t srmg_launch_count(const srmg_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

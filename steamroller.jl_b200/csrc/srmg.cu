@@ -1,0 +1,813 @@
+// srmg.cu -- C ABI of libsrmg: context, tree upload and validation, and the FP64
+// reference-semantics multigrid (vcycle!/fmg!/resnorm!) on device fields.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <unordered_map>
+#include <vector>
+
+#include "srmg_ctx.h"
+#include "srmg_internal.h"
+
+using namespace srmg;
+
+// ------------------------------------------------------------------ error plumbing
+
+int srmg::fail(srmg_ctx *c, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+int srmg::cuda_check(srmg_ctx *c, cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return SRMG_OK;
+  return fail(c, SRMG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call)                                              \
+  do {                                                        \
+    int _rc = cuda_check(ctx, (call), #call);                 \
+    if (_rc) return _rc;                                      \
+  } while (0)
+#define RC(call)               \
+  do {                         \
+    int _rc = (call);          \
+    if (_rc) return _rc;       \
+  } while (0)
+
+int srmg::ensure(srmg_ctx *ctx, DevBuf &b, size_t bytes) {
+  if (b.bytes >= bytes) return SRMG_OK;
+  if (b.p) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+  }
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) return fail(ctx, SRMG_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  b.bytes = bytes;
+  return SRMG_OK;
+}
+
+// ------------------------------------------------------------------ context
+
+extern "C" int srmg_create(srmg_ctx **out, int D, int M, int G, int device) {
+  if (!out) return SRMG_ERR_BADARG;
+  *out = nullptr;
+  if (D != 2 || M != kM || G != kG) return SRMG_ERR_UNSUPPORTED;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    return SRMG_ERR_CUDA;
+  srmg_ctx *ctx = new srmg_ctx();
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+      cudaMallocHost((void **)&ctx->h_small, 64 * sizeof(double)) != cudaSuccess) {
+    delete ctx;
+    return SRMG_ERR_CUDA;
+  }
+  ctx->stream = ctx->own_stream;
+  if (ensure(ctx, ctx->small, 64 * sizeof(double))) {
+    delete ctx;
+    return SRMG_ERR_NOMEM;
+  }
+  *out = ctx;
+  return SRMG_OK;
+}
+
+static void free_tree(srmg_ctx *ctx) {
+  if (ctx->d_tree) cudaFree(ctx->d_tree);
+  ctx->d_tree = nullptr;
+  ctx->lv.clear();
+  ctx->nblk_host.clear();
+  ctx->nch_host.clear();
+  ctx->has_tree = false;
+}
+
+extern "C" void srmg_destroy(srmg_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  free_tree(ctx);
+  for (auto &b : ctx->f64) if (b.p) cudaFree(b.p);
+  for (auto &b : ctx->f32) if (b.p) cudaFree(b.p);
+  if (ctx->part.p) cudaFree(ctx->part.p);
+  if (ctx->small.p) cudaFree(ctx->small.p);
+  if (ctx->coarse_inv.p) cudaFree(ctx->coarse_inv.p);
+  if (ctx->h_small) cudaFreeHost(ctx->h_small);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+}
+
+extern "C" const char *srmg_last_error(const srmg_ctx *ctx) {
+  return ctx ? ctx->err.c_str() : "null context";
+}
+
+extern "C" int srmg_set_stream(srmg_ctx *ctx, void *s) {
+  if (!ctx) return SRMG_ERR_BADARG;
+  ctx->stream = s ? (cudaStream_t)s : ctx->own_stream;
+  return SRMG_OK;
+}
+
+extern "C" int srmg_synchronize(srmg_ctx *ctx) {
+  if (!ctx) return SRMG_ERR_BADARG;
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SRMG_OK;
+}
+
+extern "C" int64_t srmg_launch_count(const srmg_ctx *ctx) { return ctx ? ctx->launches : -1; }
+extern "C" uint64_t srmg_tree_generation(const srmg_ctx *ctx) { return ctx ? ctx->generation : 0; }
+
+// ------------------------------------------------------------------ tree upload
+
+static int face_of(const int64_t f[2]) {
+  if (f[0] == -1 && f[1] == 0) return 0;
+  if (f[0] == 1 && f[1] == 0) return 1;
+  if (f[0] == 0 && f[1] == -1) return 2;
+  if (f[0] == 0 && f[1] == 1) return 3;
+  return -1;
+}
+
+extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
+                             const srmg_pair *const *pairs, const int64_t *nnb,
+                             const srmg_neighbor *const *nb, const int64_t *nbd,
+                             const srmg_boundary *const *bd, const int64_t *nrb,
+                             const srmg_refbnd *const *rb, const int64_t *nch,
+                             const srmg_child *const *ch, uint64_t generation) {
+  if (!ctx) return SRMG_ERR_BADARG;
+  if (nlev < 1 || nlev > 30 || !npairs || !pairs || !nnb || !nb || !nbd || !bd || !nrb || !rb ||
+      !nch || !ch)
+    return fail(ctx, SRMG_ERR_BADARG, "srmg_set_tree: bad level count or null arrays");
+  cudaSetDevice(ctx->device);
+
+  // blk (1-based) -> (level, index within level)
+  int64_t max_blk = 0, max_coord = 1;
+  for (int l = 0; l < nlev; l++) {
+    if (npairs[l] < 0 || (npairs[l] > 0 && !pairs[l]) || npairs[l] > (int64_t)INT32_MAX / 8)
+      return fail(ctx, SRMG_ERR_BADTREE, "level %d: bad block count", l + 1);
+    for (int64_t p = 0; p < npairs[l]; p++) {
+      const srmg_pair &pr = pairs[l][p];
+      if (pr.blk < 1 || pr.blk >= INT32_MAX)
+        return fail(ctx, SRMG_ERR_BADTREE, "level %d: block index %lld out of range", l + 1,
+                    (long long)pr.blk);
+      if (pr.coord[0] < 1 || pr.coord[1] < 1 || pr.coord[0] > (1 << 24) || pr.coord[1] > (1 << 24))
+        return fail(ctx, SRMG_ERR_BADTREE, "level %d: block coordinate out of range", l + 1);
+      max_blk = std::max(max_blk, pr.blk);
+      max_coord = std::max(max_coord, std::max(pr.coord[0], pr.coord[1]));
+    }
+  }
+  std::vector<int> lev_of(max_blk + 1, 0), idx_of(max_blk + 1, -1);
+  std::vector<int2> coord_of(max_blk + 1, make_int2(0, 0));
+  for (int l = 0; l < nlev; l++)
+    for (int64_t p = 0; p < npairs[l]; p++) {
+      const srmg_pair &pr = pairs[l][p];
+      if (lev_of[pr.blk] != 0)
+        return fail(ctx, SRMG_ERR_BADTREE, "block %lld appears twice in the tree", (long long)pr.blk);
+      lev_of[pr.blk] = l + 1;
+      idx_of[pr.blk] = (int)p;
+      coord_of[pr.blk] = make_int2((int)pr.coord[0], (int)pr.coord[1]);
+    }
+  auto at_level = [&](int64_t blk, int l) {
+    return blk >= 1 && blk <= max_blk && lev_of[blk] == l;
+  };
+
+  std::vector<std::vector<int4>> hb(nlev), hf(nlev), hc(nlev);
+  for (int l = 0; l < nlev; l++) {
+    const int lv = l + 1;
+    hb[l].resize(npairs[l]);
+    hf[l].assign(4 * npairs[l], make_int4(FACE_NONE, 0, 0, 0));
+    for (int64_t p = 0; p < npairs[l]; p++) {
+      const srmg_pair &pr = pairs[l][p];
+      hb[l][p] = make_int4((int)(pr.blk - 1), (int)pr.coord[0], (int)pr.coord[1], 0);
+    }
+    auto set_face = [&](int64_t blk, int face, int4 v) -> int {
+      int4 &slot = hf[l][4 * idx_of[blk] + face];
+      if (slot.x != FACE_NONE)
+        return fail(ctx, SRMG_ERR_BADTREE, "level %d: ghost face %d of block %lld written by two edges",
+                    lv, face, (long long)blk);
+      slot = v;
+      return SRMG_OK;
+    };
+    if (nnb[l] < 0 || (nnb[l] > 0 && !nb[l])) return fail(ctx, SRMG_ERR_BADTREE, "level %d: neighbours", lv);
+    for (int64_t k = 0; k < nnb[l]; k++) {
+      const srmg_neighbor &e = nb[l][k];
+      const int64_t mf[2] = {-e.face[0], -e.face[1]};
+      const int f = face_of(mf);
+      if (f < 0) return fail(ctx, SRMG_ERR_UNSUPPORTED, "level %d: neighbour face is not a star direction", lv);
+      if (!at_level(e.from, lv) || !at_level(e.to, lv))
+        return fail(ctx, SRMG_ERR_BADTREE, "level %d: neighbour edge %lld->%lld not on this level", lv,
+                    (long long)e.from, (long long)e.to);
+      RC(set_face(e.to, f, make_int4(FACE_NEIGHBOR, (int)(e.from - 1), 0, 0)));
+    }
+    if (nbd[l] < 0 || (nbd[l] > 0 && !bd[l])) return fail(ctx, SRMG_ERR_BADTREE, "level %d: boundaries", lv);
+    for (int64_t k = 0; k < nbd[l]; k++) {
+      const srmg_boundary &e = bd[l][k];
+      const int f = face_of(e.face);
+      if (f < 0 || e.bnd[0] != e.face[0] || e.bnd[1] != e.face[1])
+        return fail(ctx, SRMG_ERR_UNSUPPORTED, "level %d: boundary edge is not a star face", lv);
+      if (!at_level(e.block, lv) || e.level != lv)
+        return fail(ctx, SRMG_ERR_BADTREE, "level %d: boundary edge of block %lld not on this level",
+                    lv, (long long)e.block);
+      RC(set_face(e.block, f, make_int4(FACE_BOUNDARY, 0, 0, 0)));
+    }
+    if (nrb[l] < 0 || (nrb[l] > 0 && !rb[l])) return fail(ctx, SRMG_ERR_BADTREE, "level %d: refboundaries", lv);
+    for (int64_t k = 0; k < nrb[l]; k++) {
+      const srmg_refbnd &e = rb[l][k];
+      const int f = face_of(e.face);
+      if (f < 0) return fail(ctx, SRMG_ERR_UNSUPPORTED, "level %d: refinement face is not a star direction", lv);
+      if (lv < 2 || !at_level(e.fine, lv) || !at_level(e.coarse, lv - 1) || e.subblock[0] < 1 ||
+          e.subblock[0] > 2 || e.subblock[1] < 1 || e.subblock[1] > 2)
+        return fail(ctx, SRMG_ERR_BADTREE, "level %d: malformed refinement boundary %lld/%lld", lv,
+                    (long long)e.fine, (long long)e.coarse);
+      RC(set_face(e.fine, f, make_int4(FACE_REFBND, (int)(e.coarse - 1), (int)e.subblock[0],
+                                       (int)e.subblock[1])));
+    }
+    if (nch[l] < 0 || (nch[l] > 0 && !ch[l])) return fail(ctx, SRMG_ERR_BADTREE, "level %d: children", lv);
+    hc[l].resize(nch[l]);
+    for (int64_t k = 0; k < nch[l]; k++) {
+      const srmg_child &e = ch[l][k];
+      if (lv < 2 || !at_level(e.fine, lv) || !at_level(e.coarse, lv - 1) || e.subblock[0] < 1 ||
+          e.subblock[0] > 2 || e.subblock[1] < 1 || e.subblock[1] > 2)
+        return fail(ctx, SRMG_ERR_BADTREE, "level %d: malformed child edge %lld/%lld", lv,
+                    (long long)e.fine, (long long)e.coarse);
+      hc[l][k] = make_int4((int)(e.fine - 1), (int)(e.coarse - 1), (int)e.subblock[0], (int)e.subblock[1]);
+      int4 &cb = hb[l - 1][idx_of[e.coarse]];
+      const int bit = 1 << ((int)(e.subblock[0] - 1) + 2 * (int)(e.subblock[1] - 1));
+      if (cb.w & bit)
+        return fail(ctx, SRMG_ERR_BADTREE, "level %d: two children cover one subblock of block %lld",
+                    lv, (long long)e.coarse);
+      cb.w |= bit;
+    }
+  }
+
+  // radial weight tables, 1-based global index i in [1, 16*max_coord]
+  const int wn = (int)(kM * max_coord + 2);
+  std::vector<double> wm(wn, 0.0), wp(wn, 0.0);
+  std::vector<float> wm32(wn, 0.f), wp32(wn, 0.f);
+  for (int i = 1; i < wn; i++) {
+    wm[i] = (double)(2 * (int64_t)i - 2) / (double)(2 * (int64_t)i - 1);
+    wp[i] = (double)(2 * (int64_t)i) / (double)(2 * (int64_t)i - 1);
+    wm32[i] = (float)wm[i];
+    wp32[i] = (float)wp[i];
+  }
+
+  // layout: per level blocks/faces/child, then coord_of, then weight tables
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) & ~size_t(255);
+    return o;
+  };
+  std::vector<size_t> ob(nlev), of(nlev), oc(nlev);
+  for (int l = 0; l < nlev; l++) {
+    ob[l] = take(hb[l].size() * sizeof(int4));
+    of[l] = take(hf[l].size() * sizeof(int4));
+    oc[l] = take(hc[l].size() * sizeof(int4));
+  }
+  const size_t ocoord = take((max_blk + 1) * sizeof(int2));
+  const size_t owm = take(wn * sizeof(double)), owp = take(wn * sizeof(double));
+  const size_t owm32 = take(wn * sizeof(float)), owp32 = take(wn * sizeof(float));
+  std::vector<char> host(off, 0);
+  for (int l = 0; l < nlev; l++) {
+    memcpy(host.data() + ob[l], hb[l].data(), hb[l].size() * sizeof(int4));
+    memcpy(host.data() + of[l], hf[l].data(), hf[l].size() * sizeof(int4));
+    memcpy(host.data() + oc[l], hc[l].data(), hc[l].size() * sizeof(int4));
+  }
+  // coord_of indexed by 0-based block id
+  std::vector<int2> c0(max_blk + 1, make_int2(0, 0));
+  for (int64_t b = 1; b <= max_blk; b++) c0[b - 1] = coord_of[b];
+  memcpy(host.data() + ocoord, c0.data(), c0.size() * sizeof(int2));
+  memcpy(host.data() + owm, wm.data(), wn * sizeof(double));
+  memcpy(host.data() + owp, wp.data(), wn * sizeof(double));
+  memcpy(host.data() + owm32, wm32.data(), wn * sizeof(float));
+  memcpy(host.data() + owp32, wp32.data(), wn * sizeof(float));
+
+  CK(cudaStreamSynchronize(ctx->stream));
+  free_tree(ctx);
+  void *d = nullptr;
+  if (cudaMalloc(&d, off) != cudaSuccess) return fail(ctx, SRMG_ERR_NOMEM, "tree allocation of %zu bytes", off);
+  ctx->d_tree = d;
+  CK(cudaMemcpy(d, host.data(), off, cudaMemcpyHostToDevice));
+  char *base = (char *)d;
+  ctx->nlev = nlev;
+  ctx->lv.resize(nlev);
+  ctx->nblk_host.resize(nlev);
+  ctx->nch_host.resize(nlev);
+  for (int l = 0; l < nlev; l++) {
+    ctx->lv[l].nblk = (int)hb[l].size();
+    ctx->lv[l].nch = (int)hc[l].size();
+    ctx->lv[l].blocks = (int4 *)(base + ob[l]);
+    ctx->lv[l].faces = (int4 *)(base + of[l]);
+    ctx->lv[l].child = (int4 *)(base + oc[l]);
+    ctx->nblk_host[l] = ctx->lv[l].nblk;
+    ctx->nch_host[l] = ctx->lv[l].nch;
+  }
+  ctx->d_coord_of = (int2 *)(base + ocoord);
+  ctx->d_wm64 = (double *)(base + owm);
+  ctx->d_wp64 = (double *)(base + owp);
+  ctx->d_wm32 = (float *)(base + owm32);
+  ctx->d_wp32 = (float *)(base + owp32);
+  ctx->wtab_n = wn;
+  ctx->max_blk = max_blk;
+  ctx->generation = generation;
+  ctx->has_tree = true;
+  ctx->coarse_ok = false;
+  ctx->coarse_key.clear();
+  return SRMG_OK;
+}
+
+// ------------------------------------------------------------------ argument checks
+
+int srmg::check_call(srmg_ctx *ctx, int64_t nblk_alloc, int op, int geom, const int8_t *bc) {
+  if (!ctx) return SRMG_ERR_BADARG;
+  if (!ctx->has_tree) return fail(ctx, SRMG_ERR_NOTREE, "no tree: call srmg_set_tree first");
+  if (nblk_alloc < ctx->max_blk)
+    return fail(ctx, SRMG_ERR_BADARG, "field holds %lld blocks but the tree uses block %lld",
+                (long long)nblk_alloc, (long long)ctx->max_blk);
+  if (op != SRMG_OP_LAPLACIAN && op != SRMG_OP_HELMHOLTZ)
+    return fail(ctx, SRMG_ERR_UNSUPPORTED, "unsupported discretisation %d", op);
+  if (geom < 0 || geom > 2) return fail(ctx, SRMG_ERR_UNSUPPORTED, "unsupported geometry %d", geom);
+  if (bc) {
+    for (int i = 0; i < 9; i++)
+      if (bc[i] < -1 || bc[i] > 1) return fail(ctx, SRMG_ERR_BADARG, "boundary table entries must be -1, 0 or 1");
+  }
+  cudaSetDevice(ctx->device);
+  return SRMG_OK;
+}
+
+Signs srmg::make_signs(const int8_t *bc) {
+  Signs s;
+  for (int i = 0; i < 9; i++) s.v[i] = bc ? (double)bc[i] : 1.0;
+  return s;
+}
+
+// ------------------------------------------------------------------ launches
+
+static inline int grid_for(int64_t work, int threads, int cap) {
+  int64_t g = (work + threads - 1) / threads;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+constexpr int kGridCap = 148 * 16;
+
+template <typename T>
+WTab<T> wtab(srmg_ctx *ctx);
+template <>
+WTab<double> wtab<double>(srmg_ctx *ctx) { return WTab<double>{ctx->d_wm64, ctx->d_wp64}; }
+template <>
+WTab<float> wtab<float>(srmg_ctx *ctx) { return WTab<float>{ctx->d_wm32, ctx->d_wp32}; }
+
+template <typename T>
+OpParams<T> srmg::op_params(int op, int geom, double k2, double sl, double omega) {
+  OpParams<T> p;
+  p.op = op;
+  p.geom = geom;
+  p.s = (T)sl;
+  const double centre = (op == SRMG_OP_HELMHOLTZ) ? (-4.0 - sl * k2) : -4.0;
+  p.centre = (T)centre;
+  const double c = (op == SRMG_OP_HELMHOLTZ) ? (-4 - sl * k2) : -4.0;  // diagelm
+  p.nwc = (T)(-(omega / c));
+  return p;
+}
+template OpParams<double> srmg::op_params<double>(int, int, double, double, double);
+template OpParams<float> srmg::op_params<float>(int, int, double, double, double);
+
+double srmg::level_scale(double s, int l) {
+  const int64_t f = (int64_t)1 << (l - 1);
+  return s / (double)(f * f);
+}
+
+template <typename T>
+int srmg::L_fill_ghost(srmg_ctx *ctx, T *u, int l, const Signs &sg, int mask) {
+  const DevLevel &L = ctx->lv[l - 1];
+  if (L.nblk == 0) return SRMG_OK;
+  const int threads = 256;
+  k_fill_ghost<T><<<grid_for((int64_t)L.nblk * 4 * 32, threads, kGridCap), threads, 0, ctx->stream>>>(
+      u, L.view(l), sg, mask);
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+template <typename T>
+int srmg::L_gs_colour(srmg_ctx *ctx, T *u, const T *b, int l, const OpParams<T> &p, int parity) {
+  const DevLevel &L = ctx->lv[l - 1];
+  if (L.nblk == 0) return SRMG_OK;
+  const int threads = 128;
+  k_gs_colour<T><<<grid_for((int64_t)L.nblk * 128, threads, kGridCap), threads, 0, ctx->stream>>>(
+      u, b, L.view(l), p, wtab<T>(ctx), parity);
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+template <typename T>
+int srmg::L_gs_iter(srmg_ctx *ctx, T *u, const T *b, int l, const OpParams<T> &p, int n,
+                    const Signs &sg) {
+  for (int i = 0; i < n; i++) {
+    RC(L_gs_colour<T>(ctx, u, b, l, p, 0));
+    RC(L_fill_ghost<T>(ctx, u, l, sg, 3));
+    RC(L_gs_colour<T>(ctx, u, b, l, p, 1));
+    RC(L_fill_ghost<T>(ctx, u, l, sg, 3));
+  }
+  return SRMG_OK;
+}
+
+template <typename T>
+int srmg::L_residual(srmg_ctx *ctx, T *r, const T *u, const T *b, int l, const OpParams<T> &p) {
+  const DevLevel &L = ctx->lv[l - 1];
+  if (L.nblk == 0) return SRMG_OK;
+  k_residual<T><<<grid_for((int64_t)L.nblk * 256, 256, kGridCap), 256, 0, ctx->stream>>>(
+      r, u, b, L.view(l), p, wtab<T>(ctx));
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+template <typename T>
+int srmg::L_postrestrict(srmg_ctx *ctx, T *bf, const T *u, const T *r, int l, const OpParams<T> &pc) {
+  const DevLevel &L = ctx->lv[l - 1];
+  if (L.nch == 0) return SRMG_OK;
+  k_postrestrict<T><<<grid_for((int64_t)L.nch * 64, 256, kGridCap), 256, 0, ctx->stream>>>(
+      bf, u, r, L.view(l), ctx->d_coord_of, pc, wtab<T>(ctx));
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+template <typename T>
+int srmg::L_restrict(srmg_ctx *ctx, T *u, int l) {
+  const DevLevel &L = ctx->lv[l - 1];
+  if (L.nch == 0) return SRMG_OK;
+  k_restrict<T><<<grid_for((int64_t)L.nch * 64, 256, kGridCap), 256, 0, ctx->stream>>>(u, L.view(l));
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+template <typename T>
+int srmg::L_interp_add(srmg_ctx *ctx, T *u, const T *u1, int l) {
+  const DevLevel &L = ctx->lv[l - 1];
+  if (L.nch == 0) return SRMG_OK;
+  k_interp_add<T><<<grid_for((int64_t)L.nch * 256, 256, kGridCap), 256, 0, ctx->stream>>>(
+      u, u1, L.view(l));
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+template <typename T>
+int srmg::L_copy(srmg_ctx *ctx, T *dst, const T *src, int l) {
+  const DevLevel &L = ctx->lv[l - 1];
+  if (L.nblk == 0) return SRMG_OK;
+  k_copy_level<T><<<grid_for((int64_t)L.nblk * kSS, 256, kGridCap), 256, 0, ctx->stream>>>(
+      dst, src, L.view(l));
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+template <typename T>
+int srmg::L_diff(srmg_ctx *ctx, T *dst, const T *a1, const T *a2, int l) {
+  const DevLevel &L = ctx->lv[l - 1];
+  if (L.nblk == 0) return SRMG_OK;
+  k_diff_level<T><<<grid_for((int64_t)L.nblk * kSS, 256, kGridCap), 256, 0, ctx->stream>>>(
+      dst, a1, a2, L.view(l));
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+// ------------------------------------------------------------------ V-cycle / FMG
+
+template <typename T>
+int srmg::vcycle_dev(srmg_ctx *ctx, T *u, T *b, T *r, T *u1, double s, int op, double k2, int geom,
+                     const Signs &sg, int lmax, int ndown, int ntop, int nup, double omega) {
+  if (lmax == 0) lmax = ctx->nlev;
+  if (lmax < 1 || lmax > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "lmax %d out of range", lmax);
+  for (int l = lmax; l >= 2; l--) {
+    const double sl = level_scale(s, l);
+    const OpParams<T> p = op_params<T>(op, geom, k2, sl, omega);
+    const OpParams<T> pc = op_params<T>(op, geom, k2, 4 * sl, omega);
+    RC(L_gs_iter<T>(ctx, u, b, l, p, ndown, sg));
+    RC(L_restrict<T>(ctx, u, l));
+    RC(L_fill_ghost<T>(ctx, u, l - 1, sg, 7));
+    RC(L_copy<T>(ctx, u1, u, l - 1));
+    RC(L_residual<T>(ctx, r, u, b, l, p));
+    // fill_ghost!(r, l) and fill_ghost!(r, l-1) (src/multigrid.jl:80,83) are skipped:
+    // r is scratch and no later operation reads r's ghost cells.
+    RC(L_restrict<T>(ctx, r, l));
+    RC(L_postrestrict<T>(ctx, b, u, r, l, pc));
+  }
+  {
+    const OpParams<T> p = op_params<T>(op, geom, k2, s, omega);
+    RC(L_gs_iter<T>(ctx, u, b, 1, p, ntop, sg));
+  }
+  for (int l = 2; l <= lmax; l++) {
+    const double sl = level_scale(s, l);
+    const OpParams<T> p = op_params<T>(op, geom, k2, sl, omega);
+    RC(L_diff<T>(ctx, u1, u, u1, l - 1));
+    RC(L_fill_ghost<T>(ctx, u1, l - 1, sg, 7));
+    RC(L_interp_add<T>(ctx, u, u1, l));
+    RC(L_fill_ghost<T>(ctx, u, l, sg, 7));
+    RC(L_gs_iter<T>(ctx, u, b, l, p, nup, sg));
+    RC(L_fill_ghost<T>(ctx, u, l, sg, 7));
+  }
+  return SRMG_OK;
+}
+template int srmg::vcycle_dev<double>(srmg_ctx *, double *, double *, double *, double *, double, int,
+                                      double, int, const Signs &, int, int, int, int, double);
+template int srmg::vcycle_dev<float>(srmg_ctx *, float *, float *, float *, float *, double, int,
+                                     double, int, const Signs &, int, int, int, int, double);
+
+static int finest_level(srmg_ctx *ctx) {
+  int lmax = 0;
+  for (int l = 1; l <= ctx->nlev; l++)
+    if (ctx->nblk_host[l - 1] > 0) lmax = l;
+  return lmax;
+}
+
+template <typename T>
+static int fmg_dev_t(srmg_ctx *ctx, T *u, T *b, T *r, T *u1, double s, int op, double k2, int geom,
+                     const Signs &sg, int ndown, int ntop, int nup, double omega) {
+  const int lmax = finest_level(ctx);
+  for (int l = lmax; l >= 2; l--) {
+    const double sl = level_scale(s, l);
+    const OpParams<T> p = op_params<T>(op, geom, k2, sl, omega);
+    const OpParams<T> pc = op_params<T>(op, geom, k2, 4 * sl, omega);
+    RC(L_restrict<T>(ctx, u, l));
+    RC(L_fill_ghost<T>(ctx, u, l - 1, sg, 7));
+    RC(L_residual<T>(ctx, r, u, b, l, p));
+    RC(L_restrict<T>(ctx, r, l));
+    RC(L_postrestrict<T>(ctx, b, u, r, l, pc));
+  }
+  for (int l = 1; l <= lmax; l++) {
+    RC(L_copy<T>(ctx, u1, u, l));
+    if (l > 1) {
+      RC(L_diff<T>(ctx, u1, u, u1, l - 1));
+      RC(L_fill_ghost<T>(ctx, u1, l - 1, sg, 7));
+      RC(L_interp_add<T>(ctx, u, u1, l));
+    }
+    RC(L_fill_ghost<T>(ctx, u, l, sg, 7));
+    RC(vcycle_dev<T>(ctx, u, b, r, u1, s, op, k2, geom, sg, l, ndown, ntop, nup, omega));
+  }
+  return SRMG_OK;
+}
+
+// ------------------------------------------------------------------ norms
+
+// Leaf-weighted sum of squares of the residual (mode 0) or of b (mode 1) over all
+// levels, reduced in a fixed order into ctx->small[slot] (sqrt applied).
+template <typename T>
+int srmg::leafnorm_dev(srmg_ctx *ctx, const T *u, const T *b, double s, int op, double k2, int geom,
+                       int mode, int slot) {
+  constexpr int NT = 256;
+  int total_parts = 0;
+  std::vector<int> grids(ctx->nlev);
+  for (int l = 1; l <= ctx->nlev; l++) {
+    const int n = ctx->nblk_host[l - 1];
+    grids[l - 1] = n ? grid_for((int64_t)n * 256, NT, 148 * 4) : 0;
+    total_parts += grids[l - 1];
+  }
+  RC(ensure(ctx, ctx->part, sizeof(double) * std::max(total_parts, 1)));
+  double *part = (double *)ctx->part.p;
+  int off = 0;
+  for (int l = 1; l <= ctx->nlev; l++) {
+    if (!grids[l - 1]) continue;
+    const double sl = level_scale(s, l);
+    const OpParams<T> p = op_params<T>(op, geom, k2, sl, 1.0);
+    const double wl = 1.0 / (double)((int64_t)1 << (2 * (l - 1)));
+    k_leafsq<T, NT><<<grids[l - 1], NT, 0, ctx->stream>>>(part + off, u, b, ctx->lv[l - 1].view(l), p,
+                                                        wtab<T>(ctx), wl, mode);
+    ctx->launches++;
+    off += grids[l - 1];
+  }
+  double *out = (double *)ctx->small.p + slot;
+  if (total_parts == 0) {
+    CK(cudaMemsetAsync(out, 0, sizeof(double), ctx->stream));
+    return SRMG_OK;
+  }
+  k_reduce_sqrt<1024><<<1, 1024, 0, ctx->stream>>>(out, part, total_parts);
+  ctx->launches++;
+  return SRMG_OK;
+}
+template int srmg::leafnorm_dev<double>(srmg_ctx *, const double *, const double *, double, int, double,
+                                        int, int, int);
+template int srmg::leafnorm_dev<float>(srmg_ctx *, const float *, const float *, double, int, double,
+                                       int, int, int);
+
+int srmg::read_small(srmg_ctx *ctx, int n) {
+  CK(cudaMemcpyAsync(ctx->h_small, ctx->small.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SRMG_OK;
+}
+
+// ------------------------------------------------------------------ device entry points
+
+extern "C" int srmg_vcycle_dev(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
+                               int64_t nblk_alloc, double s, int op, double k2, int geom,
+                               const int8_t bc[9], int lmax, int ndown, int ntop, int nup,
+                               double omega, int ncycles) {
+  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  if (!u || !b || !r || !u1 || ndown < 0 || ntop < 0 || nup < 0 || ncycles < 0)
+    return fail(ctx, SRMG_ERR_BADARG, "srmg_vcycle: bad arguments");
+  const Signs sg = make_signs(bc);
+  for (int c = 0; c < ncycles; c++)
+    RC(vcycle_dev<double>(ctx, u, b, r, u1, s, op, k2, geom, sg, lmax, ndown, ntop, nup, omega));
+  CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+extern "C" int srmg_fmg_dev(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
+                            int64_t nblk_alloc, double s, int op, double k2, int geom,
+                            const int8_t bc[9], int ndown, int ntop, int nup, double omega) {
+  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  if (!u || !b || !r || !u1) return fail(ctx, SRMG_ERR_BADARG, "srmg_fmg: null field");
+  RC(fmg_dev_t<double>(ctx, u, b, r, u1, s, op, k2, geom, make_signs(bc), ndown, ntop, nup, omega));
+  CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+extern "C" int srmg_resnorm_dev(srmg_ctx *ctx, double *r, const double *b, const double *u,
+                                int64_t nblk_alloc, double s, int op, double k2, int geom,
+                                const int8_t bc[9], double *out) {
+  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  (void)r;
+  if (!b || !u || !out) return fail(ctx, SRMG_ERR_BADARG, "srmg_resnorm: null argument");
+  RC(leafnorm_dev<double>(ctx, u, b, s, op, k2, geom, 0, 0));
+  RC(read_small(ctx, 1));
+  *out = ctx->h_small[0];
+  return SRMG_OK;
+}
+
+extern "C" int srmg_fill_ghost_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level,
+                                   const int8_t bc[9], int mask) {
+  RC(check_call(ctx, nblk_alloc, 0, 0, bc));
+  if (!u || level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "fill_ghost: bad level");
+  RC(L_fill_ghost<double>(ctx, u, level, make_signs(bc), mask));
+  CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+extern "C" int srmg_gs_level_dev(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc,
+                                 int level, double omega, double sl, int op, double k2, int geom,
+                                 int parity) {
+  RC(check_call(ctx, nblk_alloc, op, geom, nullptr));
+  if (!u || !b || level < 1 || level > ctx->nlev || (parity != 0 && parity != 1))
+    return fail(ctx, SRMG_ERR_BADARG, "gs_level: bad arguments");
+  RC(L_gs_colour<double>(ctx, u, b, level, op_params<double>(op, geom, k2, sl, omega), parity));
+  CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+extern "C" int srmg_gs_iter_dev(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc,
+                                int level, double omega, double sl, int n, int op, double k2,
+                                int geom, const int8_t bc[9]) {
+  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  if (!u || !b || level < 1 || level > ctx->nlev || n < 0)
+    return fail(ctx, SRMG_ERR_BADARG, "gs_iter: bad arguments");
+  RC(L_gs_iter<double>(ctx, u, b, level, op_params<double>(op, geom, k2, sl, omega), n, make_signs(bc)));
+  CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+extern "C" int srmg_residual_level_dev(srmg_ctx *ctx, double *r, const double *u, const double *b,
+                                       int64_t nblk_alloc, int level, double sl, int op, double k2,
+                                       int geom) {
+  RC(check_call(ctx, nblk_alloc, op, geom, nullptr));
+  if (!r || !u || !b || level < 1 || level > ctx->nlev)
+    return fail(ctx, SRMG_ERR_BADARG, "residual_level: bad arguments");
+  RC(L_residual<double>(ctx, r, u, b, level, op_params<double>(op, geom, k2, sl, 1.0)));
+  CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+extern "C" int srmg_restrict_level_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level) {
+  RC(check_call(ctx, nblk_alloc, 0, 0, nullptr));
+  if (!u || level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "restrict_level: bad level");
+  RC(L_restrict<double>(ctx, u, level));
+  CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+extern "C" int srmg_interp_add_level_dev(srmg_ctx *ctx, double *u, const double *u1,
+                                         int64_t nblk_alloc, int level) {
+  RC(check_call(ctx, nblk_alloc, 0, 0, nullptr));
+  if (!u || !u1 || level < 1 || level > ctx->nlev)
+    return fail(ctx, SRMG_ERR_BADARG, "interp_add_level: bad level");
+  RC(L_interp_add<double>(ctx, u, u1, level));
+  CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+extern "C" int srmg_residual_postrestrict_level_dev(srmg_ctx *ctx, double *b, const double *u,
+                                                    const double *r, int64_t nblk_alloc, int level,
+                                                    double s, int op, double k2, int geom) {
+  RC(check_call(ctx, nblk_alloc, op, geom, nullptr));
+  if (!b || !u || !r || level < 1 || level > ctx->nlev)
+    return fail(ctx, SRMG_ERR_BADARG, "postrestrict: bad arguments");
+  RC(L_postrestrict<double>(ctx, b, u, r, level, op_params<double>(op, geom, k2, s, 1.0)));
+  CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+// ------------------------------------------------------------------ host entry points
+
+// Copy host fields into the context's device mirrors (slot i of f64).
+int srmg::stage_in(srmg_ctx *ctx, int slot, const double *h, int64_t nblk_alloc, double **d) {
+  const size_t bytes = (size_t)nblk_alloc * kSS * sizeof(double);
+  RC(ensure(ctx, ctx->f64[slot], bytes));
+  *d = (double *)ctx->f64[slot].p;
+  if (h) CK(cudaMemcpyAsync(*d, h, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  return SRMG_OK;
+}
+
+int srmg::stage_out(srmg_ctx *ctx, double *h, const double *d, int64_t nblk_alloc) {
+  const size_t bytes = (size_t)nblk_alloc * kSS * sizeof(double);
+  CK(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  return SRMG_OK;
+}
+
+extern "C" int srmg_vcycle(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
+                           int64_t nblk_alloc, double s, int op, double k2, int geom,
+                           const int8_t bc[9], int lmax, int ndown, int ntop, int nup, double omega,
+                           int ncycles) {
+  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  if (!u || !b) return fail(ctx, SRMG_ERR_BADARG, "srmg_vcycle: null field");
+  (void)r;
+  (void)u1;
+  double *du, *db, *dr, *du1;
+  RC(stage_in(ctx, 0, u, nblk_alloc, &du));
+  RC(stage_in(ctx, 1, b, nblk_alloc, &db));
+  RC(stage_in(ctx, 2, nullptr, nblk_alloc, &dr));
+  RC(stage_in(ctx, 3, nullptr, nblk_alloc, &du1));
+  RC(srmg_vcycle_dev(ctx, du, db, dr, du1, nblk_alloc, s, op, k2, geom, bc, lmax, ndown, ntop, nup,
+                     omega, ncycles));
+  RC(stage_out(ctx, u, du, nblk_alloc));
+  RC(stage_out(ctx, b, db, nblk_alloc));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SRMG_OK;
+}
+
+extern "C" int srmg_fmg(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
+                        int64_t nblk_alloc, double s, int op, double k2, int geom,
+                        const int8_t bc[9], int ndown, int ntop, int nup, double omega) {
+  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  if (!u || !b) return fail(ctx, SRMG_ERR_BADARG, "srmg_fmg: null field");
+  (void)r;
+  (void)u1;
+  double *du, *db, *dr, *du1;
+  RC(stage_in(ctx, 0, u, nblk_alloc, &du));
+  RC(stage_in(ctx, 1, b, nblk_alloc, &db));
+  RC(stage_in(ctx, 2, nullptr, nblk_alloc, &dr));
+  RC(stage_in(ctx, 3, nullptr, nblk_alloc, &du1));
+  RC(srmg_fmg_dev(ctx, du, db, dr, du1, nblk_alloc, s, op, k2, geom, bc, ndown, ntop, nup, omega));
+  RC(stage_out(ctx, u, du, nblk_alloc));
+  RC(stage_out(ctx, b, db, nblk_alloc));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SRMG_OK;
+}
+
+extern "C" int srmg_resnorm(srmg_ctx *ctx, double *r, const double *b, const double *u,
+                            int64_t nblk_alloc, double s, int op, double k2, int geom,
+                            const int8_t bc[9], double *out) {
+  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  if (!b || !u || !out) return fail(ctx, SRMG_ERR_BADARG, "srmg_resnorm: null argument");
+  double *du, *db;
+  RC(stage_in(ctx, 0, u, nblk_alloc, &du));
+  RC(stage_in(ctx, 1, b, nblk_alloc, &db));
+  RC(srmg_resnorm_dev(ctx, r, db, du, nblk_alloc, s, op, k2, geom, bc, out));
+  return SRMG_OK;
+}
+
+extern "C" int srmg_fill_ghost(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level,
+                               const int8_t bc[9]) {
+  RC(check_call(ctx, nblk_alloc, 0, 0, bc));
+  if (!u) return fail(ctx, SRMG_ERR_BADARG, "srmg_fill_ghost: null field");
+  double *du;
+  RC(stage_in(ctx, 0, u, nblk_alloc, &du));
+  RC(srmg_fill_ghost_dev(ctx, du, nblk_alloc, level, bc, 7));
+  RC(stage_out(ctx, u, du, nblk_alloc));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SRMG_OK;
+}
+
+// ------------------------------------------------------------------ explicit instantiations
+#define SRMG_INST(T)                                                                         \
+  template int srmg::L_fill_ghost<T>(srmg_ctx *, T *, int, const Signs &, int);              \
+  template int srmg::L_gs_colour<T>(srmg_ctx *, T *, const T *, int, const OpParams<T> &, int); \
+  template int srmg::L_gs_iter<T>(srmg_ctx *, T *, const T *, int, const OpParams<T> &, int,   \
+                                  const Signs &);                                            \
+  template int srmg::L_residual<T>(srmg_ctx *, T *, const T *, const T *, int, const OpParams<T> &); \
+  template int srmg::L_postrestrict<T>(srmg_ctx *, T *, const T *, const T *, int,           \
+                                       const OpParams<T> &);                                 \
+  template int srmg::L_restrict<T>(srmg_ctx *, T *, int);                                    \
+  template int srmg::L_interp_add<T>(srmg_ctx *, T *, const T *, int);                       \
+  template int srmg::L_copy<T>(srmg_ctx *, T *, const T *, int);                             \
+  template int srmg::L_diff<T>(srmg_ctx *, T *, const T *, const T *, int);
+SRMG_INST(double)
+SRMG_INST(float)

@@ -1,0 +1,346 @@
+// srmg_kernels.cuh -- per-operation CUDA kernels for the FAS multigrid on a block tree.
+//
+// Block geometry is fixed at compile time: M = 16 valid cells per side, G = 2 ghost
+// layers, S = 20, one block = S*S elements, dim 1 (r, "x") fastest.  All local indices
+// here are 0-based: valid cells are x, y in [2, 17]; element (x, y) of block blk is at
+// blk*400 + x + 20*y.  Block ids are 0-based on the device.
+//
+// Each kernel restates one reference routine and keeps its floating-point operation
+// order where the result must be bit-exact (ghost copies, mirrors, linear
+// interpolation, restriction); __dadd_rn/__dmul_rn stop the compiler from contracting
+// those into FMAs.  Stencil arithmetic only has to agree to rounding.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace srmg {
+
+constexpr int kM = 16;
+constexpr int kG = 2;
+constexpr int kS = kM + 2 * kG;
+constexpr int kSS = kS * kS;
+
+// Face numbering (the four StarStencil directions): 0 = -r, 1 = +r, 2 = -z, 3 = +z.
+enum FaceType : int { FACE_NONE = 0, FACE_NEIGHBOR = 1, FACE_BOUNDARY = 2, FACE_REFBND = 3 };
+
+// Per-level device view of the tree.
+struct LevelView {
+  const int4 *blocks;   // [nblk] {blk, coord_r, coord_z, child_mask}; coords 1-based
+  const int4 *faces;    // [nblk*4] {type, src_blk, sb_r, sb_z}
+  const int4 *child;    // [nch] {fine_blk, coarse_blk, sb_r, sb_z} (fine at this level)
+  int nblk;
+  int nch;
+  int level;
+};
+
+// Operator parameters for one level.
+template <typename T>
+struct OpParams {
+  int op;        // 0 Laplacian, 1 Helmholtz
+  int geom;      // 0 Cartesian, 1 cylindrical r = dim 1, 2 cylindrical r = dim 2
+  T s;           // level scale s_l
+  T centre;      // -4 or -4 - s_l*k2 (stencil centre, src/helmholtz.jl:43-45)
+  T nwc;         // -(omega / diagelm)  (src/multigrid.jl:177)
+};
+
+struct Signs { double v[9]; };  // boundary-condition table as doubles, column-major
+
+// Radial weights (2i-2)/(2i-1), 2i/(2i-1) tabulated by 1-based global index
+// (src/laplacian.jl:104-106).
+template <typename T>
+struct WTab { const T *wm; const T *wp; };
+
+__device__ __forceinline__ int face_sign_index(int f) {
+  // bnd == face for a star stencil; index (1 + bnd1) + 3 (1 + bnd2)
+  return f == 0 ? 3 : f == 1 ? 5 : f == 2 ? 1 : 7;
+}
+
+template <typename T> __device__ __forceinline__ T dadd(T a, T b);
+template <> __device__ __forceinline__ double dadd<double>(double a, double b) { return __dadd_rn(a, b); }
+template <> __device__ __forceinline__ float dadd<float>(float a, float b) { return __fadd_rn(a, b); }
+template <typename T> __device__ __forceinline__ T dmul(T a, T b);
+template <> __device__ __forceinline__ double dmul<double>(double a, double b) { return __dmul_rn(a, b); }
+template <> __device__ __forceinline__ float dmul<float>(float a, float b) { return __fmul_rn(a, b); }
+
+// Stencil weights of cell (x, y) of a block at 1-based coords (cr, cz).
+template <typename T>
+struct W5 { T zm, rm, rp, zp; };
+
+template <typename T>
+__device__ __forceinline__ W5<T> weights(const WTab<T> &wt, int geom, int cr, int cz, int x, int y) {
+  W5<T> w{T(1), T(1), T(1), T(1)};
+  if (geom == 1) {
+    const int i = x - 1 + kM * (cr - 1);
+    w.rm = wt.wm[i];
+    w.rp = wt.wp[i];
+  } else if (geom == 2) {
+    const int j = y - 1 + kM * (cz - 1);
+    w.zm = wt.wm[j];
+    w.zp = wt.wp[j];
+  }
+  return w;
+}
+
+// applystencil, order 2 (src/laplacian.jl:25-49,78-118; src/helmholtz.jl:17-57):
+// v = 0; v += c * u[I+S] over S = (0,-1), (-1,0), (0,0), (1,0), (0,1).
+template <typename T>
+__device__ __forceinline__ T apply5(const T *ub, int x, int y, const W5<T> &w, T centre) {
+  const int o = x + kS * y;
+  T v = w.zm * ub[o - kS];
+  v = v + w.rm * ub[o - 1];
+  v = v + centre * ub[o];
+  v = v + w.rp * ub[o + 1];
+  v = v + w.zp * ub[o + kS];
+  return v;
+}
+
+// ---- ghost fill (src/connectivity.jl:155-258) --------------------------------------
+// One warp per (block, face): lane -> (layer g = lane/16, position k = lane%16).
+template <typename T>
+__global__ void k_fill_ghost(T *__restrict__ u, LevelView lv, Signs sg, int mask) {
+  const int lane = threadIdx.x & 31;
+  const int warps_per_cta = blockDim.x >> 5;
+  const int g = lane >> 4, k = lane & 15;
+  const int total = lv.nblk * 4;
+  for (int w = blockIdx.x * warps_per_cta + (threadIdx.x >> 5); w < total;
+       w += gridDim.x * warps_per_cta) {
+    const int bi = w >> 2, f = w & 3;
+    const int4 fi = lv.faces[w];
+    if (fi.x == FACE_NONE) continue;
+    const int blk = lv.blocks[bi].x;
+    T *ub = u + (int64_t)blk * kSS;
+    int x, y;
+    if (f == 0) { x = g; y = 2 + k; }
+    else if (f == 1) { x = 18 + g; y = 2 + k; }
+    else if (f == 2) { x = 2 + k; y = g; }
+    else { x = 2 + k; y = 18 + g; }
+    if (fi.x == FACE_NEIGHBOR) {
+      if (!(mask & 1)) continue;
+      // _fill_ghost_copy! (src/connectivity.jl:184-198): ghost <- neighbour's valid
+      // cell M positions away along the face normal.
+      const T *src = u + (int64_t)fi.y * kSS;
+      int sx = x, sy = y;
+      if (f == 0) sx = x + kM; else if (f == 1) sx = x - kM;
+      else if (f == 2) sy = y + kM; else sy = y - kM;
+      ub[x + kS * y] = src[sx + kS * sy];
+    } else if (fi.x == FACE_BOUNDARY) {
+      if (!(mask & 2)) continue;
+      // fill_ghost_bnd! (src/connectivity.jl:217-231), mirrorghost (src/blockfield.jl:513-521)
+      int mx = x, my = y;
+      if (f == 0) mx = 2 * kG - 1 - x; else if (f == 1) mx = 2 * (kG + kM) - 1 - x;
+      else if (f == 2) my = 2 * kG - 1 - y; else my = 2 * (kG + kM) - 1 - y;
+      const T a = T(sg.v[face_sign_index(f)]);
+      ub[x + kS * y] = dmul<T>(a, ub[mx + kS * my]);
+    } else {
+      if (!(mask & 4)) continue;
+      // fill_ghost_interp! (src/connectivity.jl:251-258) + interp! (src/interp.jl:24-63)
+      // from the coarse block's subblockbnd(subblock, -face) (src/blockfield.jl:416-434).
+      const T *cb = u + (int64_t)fi.y * kSS;
+      const int sbr = fi.z, sbz = fi.w;
+      int jr, jz, ir, iz;  // coarse source cell and the 0/1 child offsets per dim
+      if (f <= 1) {
+        jr = (f == 0) ? (1 + 8 * sbr) : (2 + 8 * (sbr - 1));
+        ir = g;
+        jz = 2 + 8 * (sbz - 1) + (k >> 1);
+        iz = k & 1;
+      } else {
+        jz = (f == 2) ? (1 + 8 * sbz) : (2 + 8 * (sbz - 1));
+        iz = g;
+        jr = 2 + 8 * (sbr - 1) + (k >> 1);
+        ir = k & 1;
+      }
+      const int o = jr + kS * jz;
+      T v = dmul<T>(T(0.5), cb[o]);
+      v = dadd<T>(v, dmul<T>(T(0.25), cb[o + (2 * ir - 1)]));
+      v = dadd<T>(v, dmul<T>(T(0.25), cb[o + kS * (2 * iz - 1)]));
+      ub[x + kS * y] = v;
+    }
+  }
+}
+
+// ---- red-black Gauss-Seidel colour sweep (src/multigrid.jl:153-180, 238-243) ------
+// Colour P updates valid cells with (x + y + 1) & 1 == P (0-based local indices).
+template <typename T>
+__global__ void k_gs_colour(T *__restrict__ u, const T *__restrict__ b, LevelView lv,
+                            OpParams<T> p, WTab<T> wt, int parity) {
+  const int64_t total = (int64_t)lv.nblk * 128;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t >> 7), c = (int)(t & 127);
+    const int y = 2 + (c >> 3);
+    const int x = 2 + 2 * (c & 7) + ((parity ^ (y + 1)) & 1);
+    const int4 bk = lv.blocks[bi];
+    T *ub = u + (int64_t)bk.x * kSS;
+    const W5<T> w = weights<T>(wt, p.geom, bk.y, bk.z, x, y);
+    const T Lu = apply5<T>(ub, x, y, w, p.centre);
+    const int o = x + kS * y;
+    const T v = fma(p.s, b[(int64_t)bk.x * kSS + o], Lu);
+    ub[o] = fma(p.nwc, v, ub[o]);
+  }
+}
+
+// ---- residual (src/multigrid.jl:309-323, 349-354): r = -(b + Lu/s) ---------------
+template <typename T>
+__global__ void k_residual(T *__restrict__ r, const T *__restrict__ u, const T *__restrict__ b,
+                           LevelView lv, OpParams<T> p, WTab<T> wt) {
+  const int64_t total = (int64_t)lv.nblk * 256;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t >> 8), c = (int)(t & 255);
+    const int x = 2 + (c & 15), y = 2 + (c >> 4);
+    const int4 bk = lv.blocks[bi];
+    const int64_t base = (int64_t)bk.x * kSS;
+    const W5<T> w = weights<T>(wt, p.geom, bk.y, bk.z, x, y);
+    const T Lu = apply5<T>(u + base, x, y, w, p.centre);
+    const int64_t o = base + x + kS * y;
+    r[o] = -(b[o] + Lu / p.s);
+  }
+}
+
+// ---- FAS coarse RHS (src/multigrid.jl:112-119, 331-344) ----------------------------
+// For each Child edge of this level, on the coarse subblock: bf = -(r + L(u)/s_c).
+template <typename T>
+__global__ void k_postrestrict(T *__restrict__ bf, const T *__restrict__ u, const T *__restrict__ r,
+                               LevelView lv, const int2 *__restrict__ coord_of, OpParams<T> p,
+                               WTab<T> wt) {
+  const int64_t total = (int64_t)lv.nch * 64;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(t >> 6), c = (int)(t & 63);
+    const int4 ch = lv.child[e];
+    const int cblk = ch.y;
+    const int x = 2 + 8 * (ch.z - 1) + (c & 7), y = 2 + 8 * (ch.w - 1) + (c >> 3);
+    const int2 cc = coord_of[cblk];
+    const int64_t base = (int64_t)cblk * kSS;
+    const W5<T> w = weights<T>(wt, p.geom, cc.x, cc.y, x, y);
+    const T Lu = apply5<T>(u + base, x, y, w, p.centre);
+    const int64_t o = base + x + kS * y;
+    bf[o] = -(r[o] + Lu / p.s);
+  }
+}
+
+// ---- restriction (src/restrict.jl:5-37) --------------------------------------------
+// coarse = ((((0 + f00) + f10) + f01) + f11) / 4 for each Child edge of this level.
+template <typename T>
+__global__ void k_restrict(T *__restrict__ u, LevelView lv) {
+  const int64_t total = (int64_t)lv.nch * 64;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(t >> 6), c = (int)(t & 63);
+    const int4 ch = lv.child[e];
+    const int kx = c & 7, ky = c >> 3;
+    const T *fb = u + (int64_t)ch.x * kSS + (2 + 2 * kx) + kS * (2 + 2 * ky);
+    T f = dadd<T>(T(0), fb[0]);
+    f = dadd<T>(f, fb[1]);
+    f = dadd<T>(f, fb[kS]);
+    f = dadd<T>(f, fb[kS + 1]);
+    u[(int64_t)ch.y * kSS + (2 + 8 * (ch.z - 1) + kx) + kS * (2 + 8 * (ch.w - 1) + ky)] =
+        dmul<T>(f, T(0.25));
+  }
+}
+
+// ---- prolongation-add (src/interp.jl:24-63, 107-115): u_f += P(u1_c) -------------
+template <typename T>
+__global__ void k_interp_add(T *__restrict__ u, const T *__restrict__ u1, LevelView lv) {
+  const int64_t total = (int64_t)lv.nch * 256;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(t >> 8), c = (int)(t & 255);
+    const int4 ch = lv.child[e];
+    const int dx = c & 15, dy = c >> 4;
+    const int ir = dx & 1, iz = dy & 1;
+    const int jr = 2 + 8 * (ch.z - 1) + (dx >> 1), jz = 2 + 8 * (ch.w - 1) + (dy >> 1);
+    const T *cb = u1 + (int64_t)ch.y * kSS;
+    const int o = jr + kS * jz;
+    T v = dmul<T>(T(0.5), cb[o]);
+    v = dadd<T>(v, dmul<T>(T(0.25), cb[o + (2 * ir - 1)]));
+    v = dadd<T>(v, dmul<T>(T(0.25), cb[o + kS * (2 * iz - 1)]));
+    T *d = u + (int64_t)ch.x * kSS + (2 + dx) + kS * (2 + dy);
+    *d = dadd<T>(v, *d);
+  }
+}
+
+// ---- whole-block copy / difference over a level (src/blockfield.jl:557-576) ------
+template <typename T>
+__global__ void k_copy_level(T *__restrict__ dst, const T *__restrict__ src, LevelView lv) {
+  const int64_t total = (int64_t)lv.nblk * kSS;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t / kSS), c = (int)(t % kSS);
+    const int64_t o = (int64_t)lv.blocks[bi].x * kSS + c;
+    dst[o] = src[o];
+  }
+}
+
+template <typename T>
+__global__ void k_diff_level(T *__restrict__ dst, const T *__restrict__ a1, const T *a2,
+                             LevelView lv) {
+  const int64_t total = (int64_t)lv.nblk * kSS;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t / kSS), c = (int)(t % kSS);
+    const int64_t o = (int64_t)lv.blocks[bi].x * kSS + c;
+    dst[o] = a1[o] - a2[o];
+  }
+}
+
+// ---- residual norm pieces -----------------------------------------------------------
+// Sum over the level's LEAF cells (cells of subblocks without a child) of
+// w_l * f(x)^2, with f = residual (mode 0) or the field itself (mode 1).  One partial
+// per CTA, written to part[blockIdx.x]: deterministic for a fixed grid.
+// This is the value resnorm! (src/multigrid.jl:391-417) obtains by squaring every
+// cell and restricting the squares down to level 1: a leaf cell of level l ends up
+// weighted by 4^-(l-1).
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_leafsq(double *__restrict__ part, const T *__restrict__ u,
+                                               const T *__restrict__ b, LevelView lv,
+                                               OpParams<T> p, WTab<T> wt, double wl, int mode) {
+  double acc = 0.0;
+  const int64_t total = (int64_t)lv.nblk * 256;
+  for (int64_t t = blockIdx.x * (int64_t)NT + threadIdx.x; t < total; t += (int64_t)gridDim.x * NT) {
+    const int bi = (int)(t >> 8), c = (int)(t & 255);
+    const int x = 2 + (c & 15), y = 2 + (c >> 4);
+    const int4 bk = lv.blocks[bi];
+    const int sub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
+    if ((bk.w >> sub) & 1) continue;  // covered by a child: not a leaf cell
+    const int64_t base = (int64_t)bk.x * kSS;
+    const int64_t o = base + x + kS * y;
+    double v;
+    if (mode == 0) {
+      const W5<T> w = weights<T>(wt, p.geom, bk.y, bk.z, x, y);
+      const T Lu = apply5<T>(u + base, x, y, w, p.centre);
+      v = (double)(-(b[o] + Lu / p.s));
+    } else {
+      v = (double)b[o];
+    }
+    acc = fma(v, v, acc);
+  }
+  __shared__ double sh[NT / 32];
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = (threadIdx.x < NT / 32) ? sh[threadIdx.x] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if (threadIdx.x == 0) part[blockIdx.x] = v * wl;
+  }
+}
+
+// Final fixed-order reduction of n partials into out[0] (sqrt applied).
+template <int NT>
+__global__ void __launch_bounds__(NT) k_reduce_sqrt(double *__restrict__ out,
+                                                    const double *__restrict__ part, int n) {
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += NT) acc += part[i];
+  __shared__ double sh[NT / 32];
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = (threadIdx.x < NT / 32) ? sh[threadIdx.x] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if (threadIdx.x == 0) out[0] = sqrt(v);
+  }
+}
+
+}  // namespace srmg

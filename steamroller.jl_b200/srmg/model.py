@@ -1,0 +1,29 @@
+"""Algorithmic-bytes model of one FAS V-cycle, used for roofline fractions.
+
+With n_l the valid cells of level l (all blocks of the level, leaves and parents),
+w the bytes per value and (nd, nu, ntop) the sweep counts:
+
+  B = sum_{l=2..L} [ w n_l (3(nd+nu) + 8.5) + 5 w n_{l-1} ] + 3 w ntop n_1
+
+Terms: each Gauss-Seidel iteration reads u and b and writes u (3w per cell); the
+residual reads u, b and writes r (3w); restricting u and r reads 2w per fine cell and
+writes 2 w/4; the FAS right-hand side writes 3w/4; prolongation-add reads the fine u
+and writes it (2w) and reads w/4 of the coarse correction; the coarse copy u1 = u costs
+2w and the difference u1 = u - u1 costs 3w per coarse cell.  Ghost fills are not
+counted.  For (2,2,4) in FP64: 164 B per level-l cell + 40 B per level-(l-1) cell.
+"""
+from __future__ import annotations
+
+
+def level_cells(tree, M=16):
+    return [len(layer.index) * M * M for layer in tree]
+
+
+def vcycle_bytes(tree, w=8, ndown=2, nup=2, ntop=4, M=16):
+    n = level_cells(tree, M)
+    L = max((i + 1 for i, x in enumerate(n) if x), default=0)
+    total = 0.0
+    for l in range(2, L + 1):
+        total += w * n[l - 1] * (3 * (ndown + nup) + 8.5) + 5 * w * n[l - 2]
+    total += 3 * w * ntop * (n[0] if n else 0)
+    return total

@@ -1,0 +1,252 @@
+"""ctypes binding of libsrmg with the reference's entry-point names.
+
+``vcycle_`` / ``fmg_`` / ``resnorm`` / ``fill_ghost_`` take the same arguments, in the
+same order and with the same meaning, as the Julia functions they replace
+(src/multigrid.jl:17-106, 391-417; src/connectivity.jl:155-159); fields are numpy
+arrays of shape (nblk, 20, 20) in C order, i.e. Julia's column-major (i, j, blk)
+layout.  Errors raise ``SrmgError`` the way the reference raises Julia exceptions.
+
+There is no CPU fallback: if ``libsrmg.so`` is missing this module raises on import
+of the library (``lib()``), and every call runs on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .tree import Tree, Connectivity
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsrmg.so")
+
+SRMG_OK = 0
+ERRORS = {-1: "BADARG", -2: "BADTREE", -3: "CUDA", -4: "TIMEOUT", -5: "DIVERGED",
+          -6: "UNSUPPORTED", -7: "NOMEM", -8: "NOTREE"}
+MODE_FP64, MODE_MIXED = 0, 1
+
+
+class SrmgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"srmg error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class SolveOpts(ctypes.Structure):
+    _fields_ = [("tol", ctypes.c_double), ("max_cycles", ctypes.c_int), ("mode", ctypes.c_int),
+                ("ndown", ctypes.c_int), ("ntop", ctypes.c_int), ("nup", ctypes.c_int),
+                ("omega", ctypes.c_double), ("inner_cycles", ctypes.c_int),
+                ("warm_start", ctypes.c_int)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("cycles", ctypes.c_int), ("outer", ctypes.c_int),
+                ("rel_residual", ctypes.c_double), ("initial_rel", ctypes.c_double),
+                ("bnorm", ctypes.c_double), ("device_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+
+# name -> (restype, argtypes); the complete exported surface of include/srmg.h
+SIGNATURES = {
+    "srmg_create": (_I, [ctypes.POINTER(_P), _I, _I, _I, _I]),
+    "srmg_destroy": (None, [_P]),
+    "srmg_last_error": (ctypes.c_char_p, [_P]),
+    "srmg_set_stream": (_I, [_P, _P]),
+    "srmg_synchronize": (_I, [_P]),
+    "srmg_set_tree": (_I, [_P, _I] + [_P] * 10 + [ctypes.c_uint64]),
+    "srmg_tree_generation": (ctypes.c_uint64, [_P]),
+    "srmg_vcycle": (_I, [_P, _P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, _I, _I, _I, _I, _D, _I]),
+    "srmg_fmg": (_I, [_P, _P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, _I, _I, _I, _D]),
+    "srmg_resnorm": (_I, [_P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, ctypes.POINTER(_D)]),
+    "srmg_fill_ghost": (_I, [_P, _P, _I64, _I, _P]),
+    "srmg_solve_opts_default": (None, [ctypes.POINTER(SolveOpts)]),
+    "srmg_solve": (_I, [_P, _P, _P, _I64, _D, _I, _D, _I, _P, ctypes.POINTER(SolveOpts),
+                        ctypes.POINTER(Stats)]),
+    "srmg_vcycle_dev": (_I, [_P, _P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, _I, _I, _I, _I, _D, _I]),
+    "srmg_fmg_dev": (_I, [_P, _P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, _I, _I, _I, _D]),
+    "srmg_resnorm_dev": (_I, [_P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, ctypes.POINTER(_D)]),
+    "srmg_solve_dev": (_I, [_P, _P, _P, _I64, _D, _I, _D, _I, _P, ctypes.POINTER(SolveOpts),
+                            ctypes.POINTER(Stats)]),
+    "srmg_fill_ghost_dev": (_I, [_P, _P, _I64, _I, _P, _I]),
+    "srmg_gs_level_dev": (_I, [_P, _P, _P, _I64, _I, _D, _D, _I, _D, _I, _I]),
+    "srmg_gs_iter_dev": (_I, [_P, _P, _P, _I64, _I, _D, _D, _I, _I, _D, _I, _P]),
+    "srmg_residual_level_dev": (_I, [_P, _P, _P, _P, _I64, _I, _D, _I, _D, _I]),
+    "srmg_restrict_level_dev": (_I, [_P, _P, _I64, _I]),
+    "srmg_interp_add_level_dev": (_I, [_P, _P, _P, _I64, _I]),
+    "srmg_residual_postrestrict_level_dev": (_I, [_P, _P, _P, _P, _I64, _I, _D, _I, _D, _I]),
+    "srmg_launch_count": (_I64, [_P]),
+}
+
+
+def lib():
+    """Load libsrmg.so; raises if it has not been built (no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libsrmg.so not built at {LIB_PATH}; run __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    """Address of a numpy array (host) or a torch tensor (device)."""
+    if isinstance(a, np.ndarray):
+        assert a.flags.c_contiguous
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+class Context:
+    """An srmg context bound to one device with a tree uploaded."""
+
+    def __init__(self, device: int = 0):
+        self._h = _P()
+        rc = lib().srmg_create(ctypes.byref(self._h), 2, 16, 2, device)
+        if rc != SRMG_OK:
+            raise SrmgError(rc, "srmg_create failed")
+        self._tree_keep = None
+        self.generation = 0
+
+    def close(self):
+        if self._h:
+            lib().srmg_destroy(self._h)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def check(self, rc):
+        if rc != SRMG_OK:
+            msg = lib().srmg_last_error(self._h)
+            raise SrmgError(rc, msg.decode() if msg else "")
+
+    def set_tree(self, tree: Tree, conn: Connectivity, generation: int | None = None):
+        nlev = len(tree)
+        keep = []
+
+        def arrs(lists):
+            lists = [np.ascontiguousarray(x) for x in lists]
+            keep.extend(lists)
+            n = (ctypes.c_int64 * nlev)(*[len(x) for x in lists])
+            p = (_P * nlev)(*[x.ctypes.data if len(x) else 0 for x in lists])
+            keep.extend([n, p])
+            return ctypes.cast(n, _P), ctypes.cast(p, _P)
+
+        pairs = arrs([layer.pairs_array() for layer in tree])
+        nb = arrs(conn.neighbor)
+        bd = arrs(conn.boundary)
+        rb = arrs(conn.refboundary)
+        ch = arrs(conn.child)
+        self.generation = (self.generation + 1) if generation is None else generation
+        self.check(lib().srmg_set_tree(self._h, nlev, *pairs, *nb, *bd, *rb, *ch, self.generation))
+        self._tree_keep = keep
+        return self
+
+    def launches(self) -> int:
+        return lib().srmg_launch_count(self._h)
+
+    def synchronize(self):
+        self.check(lib().srmg_synchronize(self._h))
+
+    def set_stream(self, stream_ptr: int | None):
+        self.check(lib().srmg_set_stream(self._h, stream_ptr or None))
+
+
+def _bc(bc):
+    a = np.ascontiguousarray(np.asarray(bc, dtype=np.int8).reshape(9))
+    return a
+
+
+def _disc(lpldisc):
+    """(op, k2) from a discretisation descriptor: None/'laplacian' or ('helmholtz', k2)."""
+    if lpldisc is None or lpldisc == "laplacian" or lpldisc == 0:
+        return 0, 0.0
+    if isinstance(lpldisc, tuple) and lpldisc[0] in ("helmholtz", 1):
+        return 1, float(lpldisc[1])
+    raise ValueError(f"unsupported discretisation {lpldisc!r}")
+
+
+def vcycle_(ctx: Context, u, b, r, u1, s, geometry, bc, lpldisc=None, lmax=0, ndown=3, ntop=5,
+            nup=3, omega=1.0, ncycles=1):
+    """vcycle!(u, b, r, u1, s, tree, conn, geometry, bc, lpldisc; ...) (src/multigrid.jl:60)."""
+    op, k2 = _disc(lpldisc)
+    bca = _bc(bc)
+    dev = not isinstance(u, np.ndarray)
+    f = lib().srmg_vcycle_dev if dev else lib().srmg_vcycle
+    ctx.check(f(ctx.handle, _ptr(u), _ptr(b), _ptr(r), _ptr(u1), u.shape[0], s, op, k2, geometry,
+                bca.ctypes.data, lmax, ndown, ntop, nup, omega, ncycles))
+
+
+def fmg_(ctx: Context, u, b, r, u1, s, geometry, bc, lpldisc=None, ndown=3, ntop=5, nup=3,
+         omega=1.25):
+    """fmg!(u, b, r, u1, s, tree, conn, geometry, bc, lpldisc; ...) (src/multigrid.jl:17)."""
+    op, k2 = _disc(lpldisc)
+    bca = _bc(bc)
+    dev = not isinstance(u, np.ndarray)
+    f = lib().srmg_fmg_dev if dev else lib().srmg_fmg
+    ctx.check(f(ctx.handle, _ptr(u), _ptr(b), _ptr(r), _ptr(u1), u.shape[0], s, op, k2, geometry,
+                bca.ctypes.data, ndown, ntop, nup, omega))
+
+
+def resnorm(ctx: Context, r, b, u, s, geometry, bc, lpldisc=None) -> float:
+    """resnorm!(r, b, u, s, tree, conn, geometry, bc, lpldisc) (src/multigrid.jl:391)."""
+    op, k2 = _disc(lpldisc)
+    bca = _bc(bc)
+    out = ctypes.c_double()
+    dev = not isinstance(u, np.ndarray)
+    f = lib().srmg_resnorm_dev if dev else lib().srmg_resnorm
+    ctx.check(f(ctx.handle, _ptr(r) if r is not None else None, _ptr(b), _ptr(u), u.shape[0], s,
+                op, k2, geometry, bca.ctypes.data, ctypes.byref(out)))
+    return out.value
+
+
+def fill_ghost_(ctx: Context, u, l, bc, mask=7):
+    """fill_ghost!(u, l, conn, bc) (src/connectivity.jl:155-159)."""
+    bca = _bc(bc)
+    if isinstance(u, np.ndarray):
+        ctx.check(lib().srmg_fill_ghost(ctx.handle, _ptr(u), u.shape[0], l, bca.ctypes.data))
+    else:
+        ctx.check(lib().srmg_fill_ghost_dev(ctx.handle, _ptr(u), u.shape[0], l, bca.ctypes.data, mask))
+
+
+def solve(ctx: Context, u, b, s, geometry, bc, lpldisc=None, tol=1e-8, mode=MODE_FP64,
+          max_cycles=1000, ndown=2, ntop=4, nup=2, omega=1.0, inner_cycles=1, warm_start=0):
+    """Solve L u + s b = 0 to resnorm(u)/leafnorm(b) <= tol; returns the stats dict."""
+    op, k2 = _disc(lpldisc)
+    bca = _bc(bc)
+    o = SolveOpts(tol, max_cycles, mode, ndown, ntop, nup, omega, inner_cycles, warm_start)
+    st = Stats()
+    dev = not isinstance(u, np.ndarray)
+    f = lib().srmg_solve_dev if dev else lib().srmg_solve
+    rc = f(ctx.handle, _ptr(u), _ptr(b), u.shape[0], s, op, k2, geometry, bca.ctypes.data,
+           ctypes.byref(o), ctypes.byref(st))
+    ctx.check(rc)
+    return st.as_dict()
+
+
+def exported_symbols_from_header(header_path: str) -> list[str]:
+    """Names of the functions declared in include/srmg.h."""
+    import re
+    text = open(header_path).read()
+    return sorted(set(re.findall(r"\b(srmg_[a-z0-9_]+)\s*\(", text)))

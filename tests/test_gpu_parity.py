@@ -1,0 +1,307 @@
+"""Parity of the CUDA path (called through the C ABI) with the oracle.
+
+Bars: ghost fills, restriction and prolongation are bit-exact (integer/indexing work
+plus the reference's fixed-order, non-fused arithmetic); stencil sweeps agree to
+rounding (the reference's stencils are @fastmath); a full V-cycle agrees to
+<= 1e-12 relative L2 in the potential.
+"""
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+from oracle import Oracle, lib as olib, _ptr
+from srmg import gen, multigrid as mg
+from srmg.tree import connectivity
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not gpu_available(), reason="needs a CUDA GPU")]
+
+REL_VCYCLE = 1e-12   # relative L2 bar for the potential after V-cycles
+REL_SWEEP = 1e-13    # one stencil sweep: rounding only
+
+
+def torch_cuda(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def to_np(t):
+    return t.cpu().numpy()
+
+
+def rel_l2(a, b, mask=None):
+    if mask is not None:
+        a, b = a[mask], b[mask]
+    d = np.linalg.norm((a - b).ravel())
+    n = np.linalg.norm(b.ravel())
+    return d / n if n > 0 else d
+
+
+def valid_mask(shape):
+    m = np.zeros(shape, dtype=bool)
+    m[:, 2:18, 2:18] = True
+    return m
+
+
+def permute_blocks(p, seed):
+    """Renumber blocks with a random permutation (leaving gaps: nblk_alloc grows),
+    shuffle every level's pairs order and every edge list: results must not depend on
+    block numbering or on the Dict order of BlockLayer.pairs (src/blocklayer.jl:48-53)."""
+    rng = np.random.default_rng(seed)
+    n = p.nblk
+    nalloc = n + 7
+    perm = rng.permutation(nalloc)[:n] + 1  # old id i -> perm[i-1]
+    tree = p.tree
+    for layer in tree:
+        new_index = {c: int(perm[b - 1]) for c, b in layer.index.items()}
+        layer.index = new_index
+        layer.coord = {b: c for c, b in new_index.items()}
+        layer.sync(rng)
+    conn = connectivity(tree)
+    for lists in (conn.neighbor, conn.boundary, conn.refboundary, conn.child):
+        for k, arr in enumerate(lists):
+            lists[k] = arr[rng.permutation(len(arr))]
+    b = np.zeros((nalloc, 20, 20))
+    b[perm - 1] = p.b
+    return gen.Problem(tree=tree, conn=conn, b=b, s=p.s, op=p.op, k2=p.k2, geom=p.geom,
+                       bc=p.bc, h1=p.h1, name=p.name + "-permuted")
+
+
+def problems():
+    out = {}
+    out["uniform4"] = gen.make_problem(gen._uniform(4), lambda r, z, l, gi, gj: np.sin(r * 900) * np.cos(z * 700) * 1e19,
+                                       gen.poisson_scale(), name="uniform4")
+    p = gen.config2(seed=5, target_leaf=40_000, extra=3)
+    out["refined"] = p
+    out["refined_perm"] = permute_blocks(gen.config2(seed=5, target_leaf=40_000, extra=3), 9)
+    return out
+
+
+PROBS = problems()
+
+
+class Pair:
+    """A problem with its GPU context and oracle."""
+
+    def __init__(self, p):
+        self.p = p
+        self.ctx = mg.Context(0).set_tree(p.tree, p.conn)
+        self.orc = Oracle(p)
+
+
+@pytest.fixture(scope="module", params=list(PROBS))
+def pair(request):
+    return Pair(PROBS[request.param])
+
+
+def random_field(p, seed):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal((p.nblk, 20, 20))
+
+
+@pytest.mark.parametrize("mask", [1, 2, 4, 7])
+def test_fill_ghost_bitexact(pair, mask):
+    p = pair.p
+    u0 = random_field(p, 1)
+    for l in range(1, len(p.tree) + 1):
+        ug = torch_cuda(u0)
+        mg.fill_ghost_(pair.ctx, ug, l, p.bc, mask=mask)
+        pair.ctx.synchronize()
+        uo = u0.copy()
+        bcp = np.ascontiguousarray(p.bc, dtype=np.int8)
+        if mask & 1:
+            olib().orc_fill_ghost_copy(_ptr(uo), pair.orc.ot.ref, l)
+        if mask & 2:
+            olib().orc_fill_ghost_bnd(_ptr(uo), pair.orc.ot.ref, l, _ptr(bcp))
+        if mask & 4:
+            olib().orc_fill_ghost_interp(_ptr(uo), pair.orc.ot.ref, l)
+        np.testing.assert_array_equal(to_np(ug).view(np.uint64), uo.view(np.uint64),
+                                      err_msg=f"level {l} mask {mask}")
+
+
+def test_restrict_and_interp_bitexact(pair):
+    p = pair.p
+    u0, u1 = random_field(p, 2), random_field(p, 3)
+    for l in range(2, len(p.tree) + 1):
+        ug = torch_cuda(u0)
+        mg.lib().srmg_restrict_level_dev(pair.ctx.handle, ug.data_ptr(), p.nblk, l)
+        pair.ctx.synchronize()
+        uo = u0.copy()
+        olib().orc_restrict_level(_ptr(uo), pair.orc.ot.ref, l)
+        assert np.array_equal(to_np(ug).view(np.uint64), uo.view(np.uint64)), f"restrict l{l}"
+        ug = torch_cuda(u0)
+        vg = torch_cuda(u1)
+        pair.ctx.check(mg.lib().srmg_interp_add_level_dev(pair.ctx.handle, ug.data_ptr(), vg.data_ptr(), p.nblk, l))
+        pair.ctx.synchronize()
+        uo = u0.copy()
+        olib().orc_interp_add_level(_ptr(uo), _ptr(u1), pair.orc.ot.ref, l)
+        assert np.array_equal(to_np(ug).view(np.uint64), uo.view(np.uint64)), f"interp_add l{l}"
+
+
+@pytest.mark.parametrize("parity", [0, 1])
+def test_gs_colour_sweep(pair, parity):
+    import ctypes
+    p = pair.p
+    u0, b0 = random_field(p, 4), random_field(p, 5)
+    l = len(p.tree)
+    sl = 0.3
+    ug, bg = torch_cuda(u0), torch_cuda(b0)
+    pair.ctx.check(mg.lib().srmg_gs_level_dev(pair.ctx.handle, ug.data_ptr(), bg.data_ptr(), p.nblk, l,
+                                              1.0, sl, p.op, p.k2, p.geom, parity))
+    pair.ctx.synchronize()
+    uo = u0.copy()
+    olib().orc_gs_level(_ptr(uo), _ptr(b0), 1.0, sl, pair.orc.ot.ref, l, ctypes.byref(pair.orc.op), parity)
+    got = to_np(ug)
+    assert np.array_equal(got[:, :2], uo[:, :2])  # ghosts untouched
+    assert rel_l2(got, uo) < REL_SWEEP
+
+
+def test_residual_level(pair):
+    import ctypes
+    p = pair.p
+    u0, b0 = random_field(p, 6), random_field(p, 7)
+    for l in range(1, len(p.tree) + 1):
+        sl = gen.poisson_scale() / 4 ** (l - 1)
+        ug, bg, rg = torch_cuda(u0), torch_cuda(b0), torch_cuda(np.zeros_like(u0))
+        pair.ctx.check(mg.lib().srmg_residual_level_dev(pair.ctx.handle, rg.data_ptr(), ug.data_ptr(),
+                                                        bg.data_ptr(), p.nblk, l, sl, p.op, p.k2, p.geom))
+        pair.ctx.synchronize()
+        ro = np.zeros_like(u0)
+        olib().orc_residual_level(_ptr(ro), _ptr(u0), _ptr(b0), sl, pair.orc.ot.ref, l, ctypes.byref(pair.orc.op))
+        assert rel_l2(to_np(rg), ro) < REL_SWEEP
+
+
+def _prepared(pair):
+    p = pair.p
+    u = np.zeros_like(p.b)
+    pair.orc.fill_ghost_all(u)
+    return u, p.b.copy()
+
+
+@pytest.mark.parametrize("ncycles", [1, 3])
+def test_vcycle_matches_oracle(pair, ncycles):
+    p = pair.p
+    u, b = _prepared(pair)
+    ug, bg = torch_cuda(u), torch_cuda(b)
+    rg, u1g = torch_cuda(np.zeros_like(u)), torch_cuda(np.zeros_like(u))
+    mg.vcycle_(pair.ctx, ug, bg, rg, u1g, p.s, p.geom, p.bc, ndown=2, ntop=4, nup=2, ncycles=ncycles)
+    pair.ctx.synchronize()
+    uo, bo = u.copy(), b.copy()
+    r, u1 = np.zeros_like(u), np.zeros_like(u)
+    for _ in range(ncycles):
+        pair.orc.vcycle(uo, bo, r, u1, ndown=2, ntop=4, nup=2)
+    gu = to_np(ug)
+    vm = valid_mask(u.shape)
+    assert rel_l2(gu, uo, vm) <= REL_VCYCLE
+    assert rel_l2(gu, uo) <= REL_VCYCLE          # ghosts included
+    assert rel_l2(to_np(bg), bo, vm) <= 1e-10     # FAS right-hand sides
+
+
+def test_vcycle_host_pointer_entry_point(pair):
+    """srmg_vcycle (host arrays, the ccall boundary) == the device entry point."""
+    p = pair.p
+    u, b = _prepared(pair)
+    uh, bh = u.copy(), b.copy()
+    mg.vcycle_(pair.ctx, uh, bh, np.zeros_like(u), np.zeros_like(u), p.s, p.geom, p.bc,
+               ndown=2, ntop=4, nup=2, ncycles=2)
+    ug, bg = torch_cuda(u), torch_cuda(b)
+    mg.vcycle_(pair.ctx, ug, bg, torch_cuda(np.zeros_like(u)), torch_cuda(np.zeros_like(u)), p.s,
+               p.geom, p.bc, ndown=2, ntop=4, nup=2, ncycles=2)
+    pair.ctx.synchronize()
+    assert np.array_equal(uh.view(np.uint64), to_np(ug).view(np.uint64))
+    assert np.array_equal(bh.view(np.uint64), to_np(bg).view(np.uint64))
+
+
+@pytest.mark.parametrize("variant", ["helmholtz", "cartesian", "cyl2", "default_bc", "omega"])
+def test_vcycle_operator_variants(variant):
+    base = PROBS["refined"]
+    kw = dict(tree=base.tree, conn=base.conn, b=base.b.copy(), s=base.s, h1=base.h1, name=variant)
+    omega = 1.0
+    if variant == "helmholtz":
+        p = gen.Problem(**kw, op=gen.OP_HELMHOLTZ, k2=3.1e6, geom=gen.GEOM_CYL1, bc=gen.BC_PHOTO)
+        p.s = base.h1 ** 2
+    elif variant == "cartesian":
+        p = gen.Problem(**kw, geom=gen.GEOM_CART)
+    elif variant == "cyl2":
+        p = gen.Problem(**kw, geom=gen.GEOM_CYL2)
+    elif variant == "default_bc":
+        p = gen.Problem(**kw, bc=gen.BC_REFERENCE_DEFAULT)
+    else:
+        p = gen.Problem(**kw)
+        omega = 1.25
+    pr = Pair(p)
+    u, b = _prepared(pr)
+    ug, bg = torch_cuda(u), torch_cuda(b)
+    lpl = ("helmholtz", p.k2) if p.op == 1 else None
+    mg.vcycle_(pr.ctx, ug, bg, torch_cuda(np.zeros_like(u)), torch_cuda(np.zeros_like(u)), p.s, p.geom,
+               p.bc, lpldisc=lpl, ndown=2, ntop=4, nup=2, omega=omega, ncycles=2)
+    pr.ctx.synchronize()
+    uo, bo = u.copy(), b.copy()
+    r, u1 = np.zeros_like(u), np.zeros_like(u)
+    for _ in range(2):
+        pr.orc.vcycle(uo, bo, r, u1, ndown=2, ntop=4, nup=2, omega=omega)
+    assert rel_l2(to_np(ug), uo, valid_mask(u.shape)) <= REL_VCYCLE
+
+
+def test_fmg_matches_oracle(pair):
+    p = pair.p
+    u, b = _prepared(pair)
+    ug, bg = torch_cuda(u), torch_cuda(b)
+    mg.fmg_(pair.ctx, ug, bg, torch_cuda(np.zeros_like(u)), torch_cuda(np.zeros_like(u)), p.s, p.geom,
+            p.bc, ndown=2, ntop=4, nup=2)
+    pair.ctx.synchronize()
+    uo, bo = u.copy(), b.copy()
+    pair.orc.fmg(uo, bo, np.zeros_like(u), np.zeros_like(u), ndown=2, ntop=4, nup=2)
+    assert rel_l2(to_np(ug), uo, valid_mask(u.shape)) <= REL_VCYCLE
+
+
+def test_resnorm_matches_oracle(pair):
+    p = pair.p
+    u, b = _prepared(pair)
+    r, u1 = np.zeros_like(u), np.zeros_like(u)
+    pair.orc.vcycle(u, b.copy(), r, u1, ndown=2, ntop=4, nup=2)
+    pair.orc.fill_ghost_all(u)
+    got = mg.resnorm(pair.ctx, None, torch_cuda(b), torch_cuda(u), p.s, p.geom, p.bc)
+    want = pair.orc.resnorm(np.zeros_like(u), b, u)
+    assert abs(got - want) <= 1e-10 * abs(want)
+
+
+def test_fp64_solve_to_tolerance():
+    p = PROBS["refined"]
+    pr = Pair(p)
+    u, b = _prepared(pr)
+    ug = torch_cuda(u)
+    st = mg.solve(pr.ctx, ug, torch_cuda(b), p.s, p.geom, p.bc, tol=1e-8, mode=mg.MODE_FP64,
+                  max_cycles=2000)
+    uo = u.copy()
+    c, rel = pr.orc.solve(uo, b.copy(), 1e-8, max_cycles=2000)
+    assert st["rel_residual"] <= 1e-8 and rel <= 1e-8
+    assert abs(st["cycles"] - c) <= 1
+    if st["cycles"] == c:
+        assert rel_l2(to_np(ug), uo, valid_mask(u.shape)) <= REL_VCYCLE
+
+
+def test_mixed_solve_reaches_fp64_solution():
+    p = PROBS["refined"]
+    pr = Pair(p)
+    u, b = _prepared(pr)
+    ug = torch_cuda(u)
+    st = mg.solve(pr.ctx, ug, torch_cuda(b), p.s, p.geom, p.bc, tol=1e-8, mode=mg.MODE_MIXED,
+                  max_cycles=200)
+    assert st["rel_residual"] <= 1e-8
+    assert st["cycles"] < 40
+    # FP64 oracle solution at a tighter tolerance
+    uo = u.copy()
+    c, rel = pr.orc.solve(uo, b.copy(), 1e-11, max_cycles=5000)
+    leaf = leaf_mask(p)
+    err = rel_l2(to_np(ug), uo, leaf)
+    assert err < 1e-6, err
+
+
+def leaf_mask(p):
+    m = np.zeros(p.b.shape, dtype=bool)
+    for layer in p.tree:
+        for c, blk in layer.index.items():
+            if p.tree.isleaf(layer.level, c):
+                m[blk - 1, 2:18, 2:18] = True
+    return m
