@@ -102,6 +102,17 @@ def lib():
     return _lib
 
 
+def _order_after_torch(ctx, *arrays):
+    """Device arrays written by torch on another stream must be complete before the
+    context's stream reads them: synchronise torch's current stream unless the
+    context launches on it."""
+    if any(a is not None and not isinstance(a, np.ndarray) for a in arrays):
+        import torch
+        cur = torch.cuda.current_stream()
+        if cur.cuda_stream != ctx.stream_ptr:
+            cur.synchronize()
+
+
 def _ptr(a):
     """Address of a numpy array (host) or a torch tensor (device)."""
     if isinstance(a, np.ndarray):
@@ -120,6 +131,7 @@ class Context:
             raise SrmgError(rc, "srmg_create failed")
         self._tree_keep = None
         self.generation = 0
+        self.stream_ptr = -1  # the context's own stream
 
     def close(self):
         if self._h:
@@ -171,6 +183,7 @@ class Context:
 
     def set_stream(self, stream_ptr: int | None):
         self.check(lib().srmg_set_stream(self._h, stream_ptr or None))
+        self.stream_ptr = stream_ptr if stream_ptr else -1
 
 
 def _bc(bc):
@@ -193,6 +206,7 @@ def vcycle_(ctx: Context, u, b, r, u1, s, geometry, bc, lpldisc=None, lmax=0, nd
     op, k2 = _disc(lpldisc)
     bca = _bc(bc)
     dev = not isinstance(u, np.ndarray)
+    _order_after_torch(ctx, u, b, r, u1)
     f = lib().srmg_vcycle_dev if dev else lib().srmg_vcycle
     ctx.check(f(ctx.handle, _ptr(u), _ptr(b), _ptr(r), _ptr(u1), u.shape[0], s, op, k2, geometry,
                 bca.ctypes.data, lmax, ndown, ntop, nup, omega, ncycles))
@@ -204,6 +218,7 @@ def fmg_(ctx: Context, u, b, r, u1, s, geometry, bc, lpldisc=None, ndown=3, ntop
     op, k2 = _disc(lpldisc)
     bca = _bc(bc)
     dev = not isinstance(u, np.ndarray)
+    _order_after_torch(ctx, u, b, r, u1)
     f = lib().srmg_fmg_dev if dev else lib().srmg_fmg
     ctx.check(f(ctx.handle, _ptr(u), _ptr(b), _ptr(r), _ptr(u1), u.shape[0], s, op, k2, geometry,
                 bca.ctypes.data, ndown, ntop, nup, omega))
@@ -215,6 +230,7 @@ def resnorm(ctx: Context, r, b, u, s, geometry, bc, lpldisc=None) -> float:
     bca = _bc(bc)
     out = ctypes.c_double()
     dev = not isinstance(u, np.ndarray)
+    _order_after_torch(ctx, r, b, u)
     f = lib().srmg_resnorm_dev if dev else lib().srmg_resnorm
     ctx.check(f(ctx.handle, _ptr(r) if r is not None else None, _ptr(b), _ptr(u), u.shape[0], s,
                 op, k2, geometry, bca.ctypes.data, ctypes.byref(out)))
@@ -227,6 +243,7 @@ def fill_ghost_(ctx: Context, u, l, bc, mask=7):
     if isinstance(u, np.ndarray):
         ctx.check(lib().srmg_fill_ghost(ctx.handle, _ptr(u), u.shape[0], l, bca.ctypes.data))
     else:
+        _order_after_torch(ctx, u)
         ctx.check(lib().srmg_fill_ghost_dev(ctx.handle, _ptr(u), u.shape[0], l, bca.ctypes.data, mask))
 
 
@@ -238,6 +255,7 @@ def solve(ctx: Context, u, b, s, geometry, bc, lpldisc=None, tol=1e-8, mode=MODE
     o = SolveOpts(tol, max_cycles, mode, ndown, ntop, nup, omega, inner_cycles, warm_start)
     st = Stats()
     dev = not isinstance(u, np.ndarray)
+    _order_after_torch(ctx, u, b)
     f = lib().srmg_solve_dev if dev else lib().srmg_solve
     rc = f(ctx.handle, _ptr(u), _ptr(b), u.shape[0], s, op, k2, geometry, bca.ctypes.data,
            ctypes.byref(o), ctypes.byref(st))

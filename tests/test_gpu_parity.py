@@ -22,7 +22,9 @@ REL_SWEEP = 1e-13    # one stencil sweep: rounding only
 
 def torch_cuda(a):
     import torch
-    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    t = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    torch.cuda.synchronize()  # the context's stream does not order after torch's
+    return t
 
 
 def to_np(t):
