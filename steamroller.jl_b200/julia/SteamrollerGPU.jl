@@ -1,0 +1,194 @@
+"""
+    SteamrollerGPU
+
+Drop-in GPU field solve for Steamroller.jl.  `using SteamrollerGPU` after
+`using Steamroller` adds more specific methods of `Steamroller.vcycle!` and
+`Steamroller.fmg!` for the supported combination
+
+    ScalarBlockField{2,16,2,Float64} (contiguous storage),
+    LaplacianDiscretization{2,2} / HelmholtzDiscretization{2,2},
+    CartesianGeometry / CylindricalGeometry{1} / CylindricalGeometry{2},
+    GeneralHomogeneousBoundaryConditions{2},
+
+so `run_from_input(file)` runs unchanged and every Poisson and photoionization solve
+(src/streamer.jl:322-334, src/photo.jl:54-57, src/freebc.jl:67-79) goes through
+libsrmg.  Any other combination dispatches to the original Julia methods.
+
+Knobs (no input-file keys are needed): `SteamrollerGPU.configure!(; device=0,
+enabled=true)`, or the environment variables SRMG_DEVICE and SRMG_DISABLE=1.
+"""
+module SteamrollerGPU
+
+using Steamroller
+using Steamroller: ScalarBlockField, LaplacianDiscretization, HelmholtzDiscretization,
+    CartesianGeometry, CylindricalGeometry, GeneralHomogeneousBoundaryConditions,
+    Neighbor, Boundary, RefBoundary, Child
+
+const libsrmg = get(ENV, "SRMG_LIB", joinpath(@__DIR__, "..", "srmg", "libsrmg.so"))
+
+const SRMG_OK = Cint(0)
+
+mutable struct State
+    ctx::Ptr{Cvoid}
+    device::Int
+    enabled::Bool
+    fingerprint::UInt64
+    generation::UInt64
+end
+
+const STATE = State(C_NULL, parse(Int, get(ENV, "SRMG_DEVICE", "0")),
+                    get(ENV, "SRMG_DISABLE", "0") != "1", 0, 0)
+
+function configure!(; device=STATE.device, enabled=STATE.enabled)
+    if device != STATE.device && STATE.ctx != C_NULL
+        ccall((:srmg_destroy, libsrmg), Cvoid, (Ptr{Cvoid},), STATE.ctx)
+        STATE.ctx = C_NULL
+        STATE.fingerprint = 0
+    end
+    STATE.device = device
+    STATE.enabled = enabled
+    nothing
+end
+
+function check(rc)
+    rc == SRMG_OK && return nothing
+    msg = unsafe_string(ccall((:srmg_last_error, libsrmg), Cstring, (Ptr{Cvoid},), STATE.ctx))
+    error("libsrmg error $rc: $msg")
+end
+
+function context()
+    if STATE.ctx == C_NULL
+        r = Ref{Ptr{Cvoid}}(C_NULL)
+        rc = ccall((:srmg_create, libsrmg), Cint, (Ptr{Ptr{Cvoid}}, Cint, Cint, Cint, Cint),
+                   r, 2, 16, 2, STATE.device)
+        rc == SRMG_OK || error("srmg_create failed ($rc)")
+        STATE.ctx = r[]
+    end
+    STATE.ctx
+end
+
+# A cheap fingerprint of the tree: refine!/connectivity! (src/streamer.jl:545-549)
+# change at least one level's block set, so a checksum of every level's pairs decides
+# whether the device copy of the tree is stale.
+function fingerprint(tree)
+    h = UInt64(length(tree))
+    for layer in tree
+        h = h * 0x100000001b3 + UInt64(length(layer.pairs))
+        for (c, blk) in layer.pairs
+            h += UInt64(blk) * 0x9e3779b97f4a7c15 + UInt64(c[1]) * 1000003 + UInt64(c[2])
+        end
+    end
+    h
+end
+
+function upload!(tree, conn)
+    fp = fingerprint(tree)
+    fp == STATE.fingerprint && return nothing
+    nlev = length(tree)
+    npairs = Int64[length(l.pairs) for l in tree]
+    pairs = Ptr{Cvoid}[pointer(l.pairs) for l in tree]
+    lens(v) = Int64[length(x) for x in v]
+    ptrs(v) = Ptr{Cvoid}[pointer(x) for x in v]
+    STATE.generation += 1
+    GC.@preserve tree conn begin
+        check(ccall((:srmg_set_tree, libsrmg), Cint,
+                    (Ptr{Cvoid}, Cint, Ptr{Int64}, Ptr{Ptr{Cvoid}}, Ptr{Int64}, Ptr{Ptr{Cvoid}},
+                     Ptr{Int64}, Ptr{Ptr{Cvoid}}, Ptr{Int64}, Ptr{Ptr{Cvoid}}, Ptr{Int64},
+                     Ptr{Ptr{Cvoid}}, UInt64),
+                    context(), nlev, npairs, pairs,
+                    lens(conn.neighbor), ptrs(conn.neighbor),
+                    lens(conn.boundary), ptrs(conn.boundary),
+                    lens(conn.refboundary), ptrs(conn.refboundary),
+                    lens(conn.child), ptrs(conn.child), STATE.generation))
+    end
+    STATE.fingerprint = fp
+    nothing
+end
+
+geomcode(::CartesianGeometry) = Cint(0)
+geomcode(::CylindricalGeometry{1}) = Cint(1)
+geomcode(::CylindricalGeometry{2}) = Cint(2)
+opcode(::LaplacianDiscretization{2,2}) = (Cint(0), 0.0)
+opcode(h::HelmholtzDiscretization{2,2}) = (Cint(1), Float64(h.k2))
+
+const GPUField = ScalarBlockField{2,16,2,Float64}
+const GPUGeom = Union{CartesianGeometry, CylindricalGeometry{1}, CylindricalGeometry{2}}
+const GPUDisc = Union{LaplacianDiscretization{2,2}, HelmholtzDiscretization{2,2}}
+
+function Steamroller.vcycle!(u::GPUField, b::GPUField, r::GPUField, u1::GPUField, s,
+                             tree, conn, geometry::GPUGeom,
+                             bc::GeneralHomogeneousBoundaryConditions{2}, lpldisc::GPUDisc;
+                             lmax=0, ndown=3, ntop=5, nup=3, ω=1.0)
+    if !STATE.enabled
+        return invoke(Steamroller.vcycle!, Tuple{Any,Any,Any,Any,Any,Any,Any,Any,Any,Any},
+                      u, b, r, u1, s, tree, conn, geometry, bc, lpldisc;
+                      lmax, ndown, ntop, nup, ω)
+    end
+    upload!(tree, conn)
+    op, k2 = opcode(lpldisc)
+    a = Ref(bc.a)
+    GC.@preserve u b r u1 a begin
+        check(ccall((:srmg_vcycle, libsrmg), Cint,
+                    (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int64,
+                     Float64, Cint, Float64, Cint, Ptr{Int8}, Cint, Cint, Cint, Cint, Float64, Cint),
+                    context(), pointer(u.u), pointer(b.u), pointer(r.u), pointer(u1.u),
+                    size(u.u, 3), Float64(s), op, k2, geomcode(geometry),
+                    Base.unsafe_convert(Ptr{Int8}, a), lmax, ndown, ntop, nup, Float64(ω), 1))
+    end
+    nothing
+end
+
+function Steamroller.fmg!(u::GPUField, b::GPUField, r::GPUField, u1::GPUField, s,
+                          tree, conn, geometry::GPUGeom,
+                          bc::GeneralHomogeneousBoundaryConditions{2}, lpldisc::GPUDisc;
+                          lmax=0, ndown=3, ntop=5, nup=3, ω=1.25)
+    if !STATE.enabled
+        return invoke(Steamroller.fmg!, Tuple{Any,Any,Any,Any,Any,Any,Any,Any,Any,Any},
+                      u, b, r, u1, s, tree, conn, geometry, bc, lpldisc;
+                      lmax, ndown, ntop, nup, ω)
+    end
+    upload!(tree, conn)
+    op, k2 = opcode(lpldisc)
+    a = Ref(bc.a)
+    GC.@preserve u b r u1 a begin
+        check(ccall((:srmg_fmg, libsrmg), Cint,
+                    (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int64,
+                     Float64, Cint, Float64, Cint, Ptr{Int8}, Cint, Cint, Cint, Float64),
+                    context(), pointer(u.u), pointer(b.u), pointer(r.u), pointer(u1.u),
+                    size(u.u, 3), Float64(s), op, k2, geomcode(geometry),
+                    Base.unsafe_convert(Ptr{Int8}, a), ndown, ntop, nup, Float64(ω)))
+    end
+    nothing
+end
+
+"""
+    solve!(u, b, s, tree, conn, geometry, bc, lpldisc; tol=1e-8, mixed=true)
+
+Solve to `resnorm(u)/‖b‖ <= tol` (mixed: FP32 V-cycles inside FP64 defect
+correction).  Not used by `run_from_input`; for callers that want a tolerance.
+Returns (cycles, relative residual).
+"""
+function solve!(u::GPUField, b::GPUField, s, tree, conn, geometry::GPUGeom,
+                bc::GeneralHomogeneousBoundaryConditions{2}, lpldisc::GPUDisc;
+                tol=1e-8, mixed=true, max_cycles=1000, ndown=2, ntop=4, nup=2, ω=1.0)
+    upload!(tree, conn)
+    op, k2 = opcode(lpldisc)
+    a = Ref(bc.a)
+    # srmg_solve_opts / srmg_stats (include/srmg.h)
+    opts = (Float64(tol), Cint(max_cycles), Cint(mixed ? 1 : 0), Cint(ndown), Cint(ntop), Cint(nup),
+            Float64(ω), Cint(1), Cint(0))
+    optsref = Ref(opts)
+    stats = Ref((Cint(0), Cint(0), Cint(0), 0.0, 0.0, 0.0, 0.0))
+    GC.@preserve u b a optsref stats begin
+        check(ccall((:srmg_solve, libsrmg), Cint,
+                    (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int64, Float64, Cint, Float64, Cint,
+                     Ptr{Int8}, Ptr{Cvoid}, Ptr{Cvoid}),
+                    context(), pointer(u.u), pointer(b.u), size(u.u, 3), Float64(s), op, k2,
+                    geomcode(geometry), Base.unsafe_convert(Ptr{Int8}, a),
+                    Base.unsafe_convert(Ptr{Cvoid}, optsref), Base.unsafe_convert(Ptr{Cvoid}, stats)))
+    end
+    st = stats[]
+    (st[2], st[4])
+end
+
+end # module
