@@ -202,6 +202,23 @@ int srmg_residual_postrestrict_level_dev(srmg_ctx *ctx, double *b, const double 
                                          const double *r, int64_t nblk_alloc, int level,
                                          double s, int op, double k2, int geom);
 
+/* Allocation-free residual norm.  No counterpart in the reference: it exists for
+ * callers that cannot call cudaMalloc when they need the norm -- code inside CUDA
+ * stream capture, hosts whose device memory belongs to their own pool allocator, or
+ * loops that cannot take an allocation's implicit synchronisation.  Same value as
+ * srmg_resnorm_dev (resnorm!, src/multigrid.jl:391-417) up to summation order, but
+ * it calls no cudaMalloc/cudaFree or allocating library routine: its scratch (one
+ * partial sum per tree block) is a static device array of 65536 doubles (512 KiB),
+ * held by every GPU that loads the library until the process exits.  Trees of more
+ * than 65536 blocks are rejected with SRMG_ERR_BADARG.  `out` is a DEVICE address
+ * that receives the norm, stream-ordered on the context's stream; nothing is copied
+ * to the host.  The array is shared by all calls and keeps the last call's
+ * contents; calls that overlap on the GPU (several streams or contexts at once)
+ * race on it.  The first call on each device looks up the array's device address;
+ * make that first call before any stream capture begins. */
+int srmg_resnorm_noalloc(srmg_ctx *ctx, const double *b, const double *u, int64_t nblk_alloc,
+                         double s, int op, double k2, int geom, double *out);
+
 /* Number of CUDA kernel launches this context has issued (for launch accounting). */
 int64_t srmg_launch_count(const srmg_ctx *ctx);
 

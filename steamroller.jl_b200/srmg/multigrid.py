@@ -83,6 +83,7 @@ SIGNATURES = {
     "srmg_restrict_level_dev": (_I, [_P, _P, _I64, _I]),
     "srmg_interp_add_level_dev": (_I, [_P, _P, _P, _I64, _I]),
     "srmg_residual_postrestrict_level_dev": (_I, [_P, _P, _P, _P, _I64, _I, _D, _I, _D, _I]),
+    "srmg_resnorm_noalloc": (_I, [_P, _P, _P, _I64, _D, _I, _D, _I, _P]),
     "srmg_launch_count": (_I64, [_P]),
 }
 
