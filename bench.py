@@ -171,7 +171,12 @@ def main():
     ap.add_argument("--target-leaf", type=int, default=TARGET_LEAF)
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--only", default=None, choices=[None, "vcycle"],
+                    help="vcycle: time plain FP64 V-cycles only (profiling runs)")
+    ap.add_argument("--config", default="config2", choices=["config1", "config2", "config5"])
     args = ap.parse_args()
+    if args.only == "vcycle":
+        return vcycle_only(args)
 
     from srmg import gen, model
     from srmg.tree import leaf_cells
@@ -300,6 +305,35 @@ def main():
     ctx.close()
     if pg is not None:
         pg.destroy_process_group()
+
+
+def vcycle_only(args):
+    """Plain FP64 V-cycles (the persistent engine) on one config: W warm-up cycles, then
+    K timed cycles with CUDA events; prints one JSON line.  Used for ncu captures."""
+    import torch
+    from srmg import gen, model, multigrid as mg
+    problem = {"config1": gen.config1, "config2": lambda: gen.config2(seed=SEED, target_leaf=args.target_leaf),
+               "config5": gen.config5}[args.config]()
+    ctx = mg.Context(0).set_tree(problem.tree, problem.conn)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    b = torch.from_numpy(problem.b).cuda()
+    u, r, u1 = torch.zeros_like(b), torch.zeros_like(b), torch.zeros_like(b)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        mg.vcycle_(ctx, u, b, r, u1, problem.s, problem.geom, problem.bc, ndown=2, ntop=4, nup=2,
+                   ncycles=args.warmup)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        mg.vcycle_(ctx, u, b, r, u1, problem.s, problem.geom, problem.bc, ndown=2, ntop=4, nup=2,
+                   ncycles=args.steps)
+        e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / max(1, args.steps)
+    B = model.vcycle_bytes(problem.tree, 8, 2, 2, 4)
+    print(json.dumps({"only": "vcycle", "config": args.config, "blocks": problem.tree.nblocks(),
+                      "ms_per_vcycle": ms, "model_bytes": B, "model_GBps": B / (ms / 1e3) / 1e9}))
+    ctx.close()
 
 
 def fp64_cycle_count_estimate(problem):

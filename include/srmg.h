@@ -219,6 +219,20 @@ int srmg_residual_postrestrict_level_dev(srmg_ctx *ctx, double *b, const double 
 int srmg_resnorm_noalloc(srmg_ctx *ctx, const double *b, const double *u, int64_t nblk_alloc,
                          double s, int op, double k2, int geom, double *out);
 
+/* Tuning knobs (no reference counterpart; the autotuner drives them):
+ *   "engine"           1 = persistent one-launch V-cycle (default), 0 = one kernel per
+ *                      reference operation;
+ *   "local_max_blocks" coarse levels whose every coarser level has at most this many
+ *                      blocks run inside one CTA of the persistent kernel (default 16);
+ *   "engine_ctas"      CTAs of the persistent kernel (0 = one per SM);
+ *   "trace"            1 = record a %globaltimer stamp (ns) after every phase of the
+ *                      persistent kernel, read back with srmg_get_trace. */
+int srmg_set_option(srmg_ctx *ctx, const char *key, int64_t value);
+
+/* Phase timestamps of the last persistent-kernel launch (with option "trace" on);
+ * returns the number of entries written to out (<= max_entries), or an error code. */
+int srmg_get_trace(srmg_ctx *ctx, int64_t *out, int max_entries);
+
 /* Number of CUDA kernel launches this context has issued (for launch accounting). */
 int64_t srmg_launch_count(const srmg_ctx *ctx);
 

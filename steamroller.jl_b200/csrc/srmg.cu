@@ -101,6 +101,8 @@ extern "C" void srmg_destroy(srmg_ctx *ctx) {
   if (ctx->part.p) cudaFree(ctx->part.p);
   if (ctx->small.p) cudaFree(ctx->small.p);
   if (ctx->coarse_inv.p) cudaFree(ctx->coarse_inv.p);
+  if (ctx->sync.p) cudaFree(ctx->sync.p);
+  if (ctx->trace.p) cudaFree(ctx->trace.p);
   if (ctx->h_small) cudaFreeHost(ctx->h_small);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -122,7 +124,7 @@ extern "C" int srmg_synchronize(srmg_ctx *ctx) {
   if (!ctx) return SRMG_ERR_BADARG;
   cudaSetDevice(ctx->device);
   CK(cudaStreamSynchronize(ctx->stream));
-  return SRMG_OK;
+  return engine_check(ctx);
 }
 
 extern "C" int64_t srmg_launch_count(const srmg_ctx *ctx) { return ctx ? ctx->launches : -1; }
@@ -181,6 +183,9 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
     return blk >= 1 && blk <= max_blk && lev_of[blk] == l;
   };
 
+  std::vector<int4> binfo(max_blk + 1, make_int4(0, 0, 0, 0));
+  std::vector<int4> bface(4 * (max_blk + 1), make_int4(FACE_NONE, 0, 0, -1));
+  std::vector<int4> bkids(max_blk + 1, make_int4(-1, -1, -1, -1));
   std::vector<std::vector<int4>> hb(nlev), hf(nlev), hc(nlev);
   for (int l = 0; l < nlev; l++) {
     const int lv = l + 1;
@@ -208,6 +213,16 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
         return fail(ctx, SRMG_ERR_BADTREE, "level %d: neighbour edge %lld->%lld not on this level", lv,
                     (long long)e.from, (long long)e.to);
       RC(set_face(e.to, f, make_int4(FACE_NEIGHBOR, (int)(e.from - 1), 0, 0)));
+      {
+        int4 &pf = bface[4 * (e.to - 1) + f];
+        pf.x = FACE_NEIGHBOR;
+        pf.y = (int)(e.from - 1);
+        const int fp = face_of(e.face);
+        if (bface[4 * (e.from - 1) + fp].w >= 0)
+          return fail(ctx, SRMG_ERR_BADTREE, "level %d: block %lld has two neighbours across one face", lv,
+                      (long long)e.from);
+        bface[4 * (e.from - 1) + fp].w = (int)(e.to - 1);
+      }
     }
     if (nbd[l] < 0 || (nbd[l] > 0 && !bd[l])) return fail(ctx, SRMG_ERR_BADTREE, "level %d: boundaries", lv);
     for (int64_t k = 0; k < nbd[l]; k++) {
@@ -219,6 +234,7 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
         return fail(ctx, SRMG_ERR_BADTREE, "level %d: boundary edge of block %lld not on this level",
                     lv, (long long)e.block);
       RC(set_face(e.block, f, make_int4(FACE_BOUNDARY, 0, 0, 0)));
+      bface[4 * (e.block - 1) + f].x = FACE_BOUNDARY;
     }
     if (nrb[l] < 0 || (nrb[l] > 0 && !rb[l])) return fail(ctx, SRMG_ERR_BADTREE, "level %d: refboundaries", lv);
     for (int64_t k = 0; k < nrb[l]; k++) {
@@ -231,6 +247,12 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
                     (long long)e.fine, (long long)e.coarse);
       RC(set_face(e.fine, f, make_int4(FACE_REFBND, (int)(e.coarse - 1), (int)e.subblock[0],
                                        (int)e.subblock[1])));
+      {
+        int4 &pf = bface[4 * (e.fine - 1) + f];
+        pf.x = FACE_REFBND;
+        pf.y = (int)(e.coarse - 1);
+        pf.z = (int)e.subblock[0] | ((int)e.subblock[1] << 8);
+      }
     }
     if (nch[l] < 0 || (nch[l] > 0 && !ch[l])) return fail(ctx, SRMG_ERR_BADTREE, "level %d: children", lv);
     hc[l].resize(nch[l]);
@@ -247,6 +269,25 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
         return fail(ctx, SRMG_ERR_BADTREE, "level %d: two children cover one subblock of block %lld",
                     lv, (long long)e.coarse);
       cb.w |= bit;
+      const int sub = (int)(e.subblock[0] - 1) + 2 * (int)(e.subblock[1] - 1);
+      int4 &kd = bkids[e.coarse - 1];
+      (sub == 0 ? kd.x : sub == 1 ? kd.y : sub == 2 ? kd.z : kd.w) = (int)(e.fine - 1);
+    }
+  }
+
+  for (int l = 0; l < nlev; l++)
+    for (const int4 &b4 : hb[l]) binfo[b4.x] = make_int4(b4.y, b4.z, b4.w, l + 1);
+  for (int64_t b = 0; b < max_blk; b++)
+    for (int f = 0; f < 4; f++) {
+      int4 &fc = bface[4 * b + f];
+      if (fc.x == FACE_NEIGHBOR) fc.z = binfo[fc.y].z;  // the neighbour's child mask
+    }
+  std::vector<std::vector<int4>> hr(nlev);
+  for (int l = 0; l < nlev; l++) {
+    hr[l].resize(5 * hb[l].size());
+    for (size_t i = 0; i < hb[l].size(); i++) {
+      hr[l][5 * i] = hb[l][i];
+      for (int f = 0; f < 4; f++) hr[l][5 * i + 1 + f] = bface[4 * hb[l][i].x + f];
     }
   }
 
@@ -268,8 +309,9 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
     off += (bytes + 255) & ~size_t(255);
     return o;
   };
-  std::vector<size_t> ob(nlev), of(nlev), oc(nlev);
+  std::vector<size_t> ob(nlev), of(nlev), oc(nlev), orr(nlev);
   for (int l = 0; l < nlev; l++) {
+    orr[l] = take(hr[l].size() * sizeof(int4));
     ob[l] = take(hb[l].size() * sizeof(int4));
     of[l] = take(hf[l].size() * sizeof(int4));
     oc[l] = take(hc[l].size() * sizeof(int4));
@@ -277,8 +319,12 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
   const size_t ocoord = take((max_blk + 1) * sizeof(int2));
   const size_t owm = take(wn * sizeof(double)), owp = take(wn * sizeof(double));
   const size_t owm32 = take(wn * sizeof(float)), owp32 = take(wn * sizeof(float));
+  const size_t oinfo = take((max_blk + 1) * sizeof(int4));
+  const size_t ofaceb = take(4 * (max_blk + 1) * sizeof(int4));
+  const size_t okids = take((max_blk + 1) * sizeof(int4));
   std::vector<char> host(off, 0);
   for (int l = 0; l < nlev; l++) {
+    memcpy(host.data() + orr[l], hr[l].data(), hr[l].size() * sizeof(int4));
     memcpy(host.data() + ob[l], hb[l].data(), hb[l].size() * sizeof(int4));
     memcpy(host.data() + of[l], hf[l].data(), hf[l].size() * sizeof(int4));
     memcpy(host.data() + oc[l], hc[l].data(), hc[l].size() * sizeof(int4));
@@ -291,6 +337,9 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
   memcpy(host.data() + owp, wp.data(), wn * sizeof(double));
   memcpy(host.data() + owm32, wm32.data(), wn * sizeof(float));
   memcpy(host.data() + owp32, wp32.data(), wn * sizeof(float));
+  memcpy(host.data() + oinfo, binfo.data(), binfo.size() * sizeof(int4));
+  memcpy(host.data() + ofaceb, bface.data(), bface.size() * sizeof(int4));
+  memcpy(host.data() + okids, bkids.data(), bkids.size() * sizeof(int4));
 
   CK(cudaStreamSynchronize(ctx->stream));
   free_tree(ctx);
@@ -307,6 +356,7 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
     ctx->lv[l].nblk = (int)hb[l].size();
     ctx->lv[l].nch = (int)hc[l].size();
     ctx->lv[l].blocks = (int4 *)(base + ob[l]);
+    ctx->lv[l].rec = (int4 *)(base + orr[l]);
     ctx->lv[l].faces = (int4 *)(base + of[l]);
     ctx->lv[l].child = (int4 *)(base + oc[l]);
     ctx->nblk_host[l] = ctx->lv[l].nblk;
@@ -317,6 +367,9 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
   ctx->d_wp64 = (double *)(base + owp);
   ctx->d_wm32 = (float *)(base + owm32);
   ctx->d_wp32 = (float *)(base + owp32);
+  ctx->d_info = (int4 *)(base + oinfo);
+  ctx->d_faceb = (int4 *)(base + ofaceb);
+  ctx->d_kids = (int4 *)(base + okids);
   ctx->wtab_n = wn;
   ctx->max_blk = max_blk;
   ctx->generation = generation;
@@ -489,6 +542,13 @@ int srmg::vcycle_dev(srmg_ctx *ctx, T *u, T *b, T *r, T *u1, double s, int op, d
                      const Signs &sg, int lmax, int ndown, int ntop, int nup, double omega) {
   if (lmax == 0) lmax = ctx->nlev;
   if (lmax < 1 || lmax > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "lmax %d out of range", lmax);
+  // The persistent engine runs the whole cycle in one launch; r carries the coarse
+  // corrections there.  Sweep counts of zero keep the per-operation kernels.
+  // Bulk copies need 16-byte aligned block tiles.
+  const bool aligned = ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(b) |
+                         reinterpret_cast<uintptr_t>(r) | reinterpret_cast<uintptr_t>(u1)) & 15) == 0;
+  if (ctx->use_engine && aligned && ndown >= 1 && ntop >= 1 && nup >= 1 && ctx->nlev <= 30)
+    return engine_vcycle<T>(ctx, u, b, u1, r, s, op, k2, geom, sg, lmax, ndown, ntop, nup, omega);
   for (int l = lmax; l >= 2; l--) {
     const double sl = level_scale(s, l);
     const OpParams<T> p = op_params<T>(op, geom, k2, sl, omega);
@@ -603,6 +663,25 @@ template int srmg::leafnorm_dev<float>(srmg_ctx *, const float *, const float *,
 int srmg::read_small(srmg_ctx *ctx, int n) {
   CK(cudaMemcpyAsync(ctx->h_small, ctx->small.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  return engine_check(ctx);
+}
+
+extern "C" int srmg_set_option(srmg_ctx *ctx, const char *key, int64_t value) {
+  if (!ctx || !key) return SRMG_ERR_BADARG;
+  if (!strcmp(key, "engine")) ctx->use_engine = value != 0;
+  else if (!strcmp(key, "trace")) ctx->trace_on = value != 0;
+  else if (!strcmp(key, "local_max_blocks")) {
+    if (value < 0 || value > 1024) return fail(ctx, SRMG_ERR_BADARG, "local_max_blocks out of range");
+    ctx->local_max_blocks = (int)value;
+  } else if (!strcmp(key, "engine_ctas")) {
+    if (value < 0) return fail(ctx, SRMG_ERR_BADARG, "engine_ctas must be >= 0");
+    if (value > 0) {
+      int nsm = 0;
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+      if (value > nsm) return fail(ctx, SRMG_ERR_BADARG, "engine_ctas above the SM count (%d)", nsm);
+    }
+    ctx->engine_ctas = (int)value;
+  } else return fail(ctx, SRMG_ERR_BADARG, "unknown option '%s'", key);
   return SRMG_OK;
 }
 
@@ -750,7 +829,7 @@ extern "C" int srmg_vcycle(srmg_ctx *ctx, double *u, double *b, double *r, doubl
   RC(stage_out(ctx, u, du, nblk_alloc));
   RC(stage_out(ctx, b, db, nblk_alloc));
   CK(cudaStreamSynchronize(ctx->stream));
-  return SRMG_OK;
+  return engine_check(ctx);
 }
 
 extern "C" int srmg_fmg(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
@@ -769,7 +848,7 @@ extern "C" int srmg_fmg(srmg_ctx *ctx, double *u, double *b, double *r, double *
   RC(stage_out(ctx, u, du, nblk_alloc));
   RC(stage_out(ctx, b, db, nblk_alloc));
   CK(cudaStreamSynchronize(ctx->stream));
-  return SRMG_OK;
+  return engine_check(ctx);
 }
 
 extern "C" int srmg_resnorm(srmg_ctx *ctx, double *r, const double *b, const double *u,

@@ -18,6 +18,7 @@ struct DevLevel {
   int4 *blocks = nullptr;
   int4 *faces = nullptr;
   int4 *child = nullptr;
+  int4 *rec = nullptr;   // engine records: 5 int4 per block ({blk, cr, cz, child_mask}, face 0..3)
   LevelView view(int level) const { return LevelView{blocks, faces, child, nblk, nch, level}; }
 };
 
@@ -49,6 +50,19 @@ struct srmg_ctx {
   int2 *d_coord_of = nullptr;          // [max_blk] coords by 0-based block id
   double *d_wm64 = nullptr, *d_wp64 = nullptr;
   float *d_wm32 = nullptr, *d_wp32 = nullptr;
+  // block-id-indexed tables for the persistent engine
+  int4 *d_info = nullptr;    // {coord_r, coord_z, child_mask, level}
+  int4 *d_faceb = nullptr;   // [blk*4+f] {type, src, sb_r | sb_z << 8, push_to}
+  int4 *d_kids = nullptr;    // child block per subblock, -1 if none
+
+  // persistent engine
+  srmg::DevBuf sync;         // {barrier counter, error word}
+  int num_sms = 0;
+  int engine_ctas = 0;       // cooperative grid size (0 = not yet known)
+  int local_max_blocks = 16; // levels whose every coarser level has <= this many blocks run in CTA 0
+  bool use_engine = true;
+  bool trace_on = false;
+  srmg::DevBuf trace;        // %globaltimer stamps after every engine phase (CTA 0)
 
   // device mirrors of host fields (host-pointer entry points) and solver work buffers
   srmg::DevBuf f64[6];   // u, b, r, u1, bwork, spare

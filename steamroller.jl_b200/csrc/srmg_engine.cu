@@ -1,0 +1,141 @@
+// srmg_engine.cu -- host side of the persistent V-cycle engine (srmg_engine.cuh).
+#include <cstring>
+
+#include "srmg_ctx.h"
+#include "srmg_engine.cuh"
+#include "srmg_internal.h"
+
+using namespace srmg;
+
+#define CK(call)                                              \
+  do {                                                        \
+    int _rc = cuda_check(ctx, (call), #call);                 \
+    if (_rc) return _rc;                                      \
+  } while (0)
+#define RC(call)               \
+  do {                         \
+    int _rc = (call);          \
+    if (_rc) return _rc;       \
+  } while (0)
+
+namespace {
+
+template <typename T>
+WTab<T> wtab_of(srmg_ctx *ctx);
+template <>
+WTab<double> wtab_of<double>(srmg_ctx *ctx) { return WTab<double>{ctx->d_wm64, ctx->d_wp64}; }
+template <>
+WTab<float> wtab_of<float>(srmg_ctx *ctx) { return WTab<float>{ctx->d_wm32, ctx->d_wp32}; }
+
+template <typename T>
+int engine_grid(srmg_ctx *ctx, int *grid) {
+  if (ctx->num_sms == 0) CK(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_engine_vcycle<T>, 1024, 0));
+  if (per_sm < 1) return fail(ctx, SRMG_ERR_CUDA, "engine kernel cannot be resident (occupancy 0)");
+  *grid = ctx->num_sms * std::min(per_sm, 1);
+  return SRMG_OK;
+}
+
+}  // namespace
+
+// Levels 1..K run in CTA 0: the largest K such that every level 1..K holds at most
+// ctx->local_max_blocks blocks.
+int srmg::engine_local_top(srmg_ctx *ctx, int lmax) {
+  int K = 0;
+  for (int l = 1; l <= lmax; l++) {
+    if (ctx->nblk_host[l - 1] > ctx->local_max_blocks) break;
+    K = l;
+  }
+  return K;
+}
+
+template <typename T>
+int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, double s, int op, double k2, int geom,
+                        const Signs &sg, int lmax, int ndown, int ntop, int nup, double omega) {
+  if (ctx->nlev > kMaxLev) return fail(ctx, SRMG_ERR_UNSUPPORTED, "engine supports at most %d levels", kMaxLev);
+  if (lmax == 0) lmax = ctx->nlev;
+  int L = 0;
+  for (int l = 1; l <= lmax; l++)
+    if (ctx->nblk_host[l - 1] > 0) L = l;
+  if (L == 0) return SRMG_OK;
+  EngArgs<T> A;
+  memset(&A, 0, sizeof A);
+  A.u = u;
+  {
+    DevBuf &alt = (sizeof(T) == 8) ? ctx->f64[5] : ctx->f32[5];
+    RC(ensure(ctx, alt, (size_t)ctx->max_blk * kSS * sizeof(T)));
+    A.ualt = (T *)alt.p;
+  }
+  A.b = b;
+  A.u1 = u1;
+  A.e = e;
+  for (int l = 0; l < ctx->nlev; l++) {
+    A.tr.lvl_rec[l] = ctx->lv[l].rec;
+    A.tr.lvl_blocks[l] = ctx->lv[l].blocks;
+    A.tr.lvl_child[l] = ctx->lv[l].child;
+    A.tr.nblk[l] = ctx->nblk_host[l];
+    A.tr.nch[l] = ctx->nch_host[l];
+  }
+  A.tr.info = ctx->d_info;
+  A.tr.faces = ctx->d_faceb;
+  A.tr.kids = ctx->d_kids;
+  A.wt = wtab_of<T>(ctx);
+  A.sg = sg;
+  A.op = op;
+  A.geom = geom;
+  A.lmax = L;
+  A.ndown = ndown;
+  A.ntop = ntop;
+  A.nup = nup;
+  A.local_top = engine_local_top(ctx, L);
+  for (int l = 1; l <= L; l++) {
+    const OpParams<T> p = op_params<T>(op, geom, k2, level_scale(s, l), omega);
+    A.lev_s[l] = p.s;
+    A.lev_centre[l] = p.centre;
+    A.lev_nwc[l] = p.nwc;
+  }
+  RC(ensure(ctx, ctx->sync, 256));
+  A.bar = (unsigned *)ctx->sync.p;
+  A.err = (int *)((char *)ctx->sync.p + 128);
+  A.timeout_ns = 2000000000LL;  // 2 s per barrier wait
+  if (ctx->trace_on) {
+    RC(ensure(ctx, ctx->trace, kTraceMax * sizeof(long long)));
+    A.trace = (long long *)ctx->trace.p;
+  }
+  int grid = ctx->engine_ctas;
+  if (grid == 0) {
+    RC(engine_grid<T>(ctx, &grid));
+    ctx->engine_ctas = grid;
+  }
+  CK(cudaMemsetAsync(ctx->sync.p, 0, 256, ctx->stream));
+  void *args[] = {&A};
+  CK(cudaLaunchCooperativeKernel((const void *)k_engine_vcycle<T>, dim3(grid), dim3(1024), args, 0, ctx->stream));
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+template int srmg::engine_vcycle<double>(srmg_ctx *, double *, double *, double *, double *, double, int,
+                                         double, int, const Signs &, int, int, int, int, double);
+template int srmg::engine_vcycle<float>(srmg_ctx *, float *, float *, float *, float *, double, int,
+                                        double, int, const Signs &, int, int, int, int, double);
+
+extern "C" int srmg_get_trace(srmg_ctx *ctx, int64_t *out, int max_entries) {
+  if (!ctx || !out || max_entries < 0) return SRMG_ERR_BADARG;
+  if (!ctx->trace.p) return 0;
+  const int n = std::min(max_entries, kTraceMax);
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMemcpy(out, ctx->trace.p, n * sizeof(long long), cudaMemcpyDeviceToHost));
+  int k = 0;
+  while (k < n && out[k] != 0) k++;
+  return k;
+}
+
+// Reads the engine's error word (after the stream has been synchronised by the caller).
+int srmg::engine_check(srmg_ctx *ctx) {
+  if (!ctx->sync.p) return SRMG_OK;
+  int err = 0;
+  CK(cudaMemcpy(&err, (char *)ctx->sync.p + 128, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) return fail(ctx, SRMG_ERR_TIMEOUT, "engine barrier timed out (error word %d)", err);
+  return SRMG_OK;
+}

@@ -1,0 +1,592 @@
+// srmg_engine.cuh -- the persistent V-cycle engine: one cooperative launch runs a whole
+// FAS V-cycle (src/multigrid.jl:60-106) with grid barriers between dependent phases.
+//
+// Phases (per level l, fine to coarse and back):
+//   GS iteration     : one full red-black Gauss-Seidel iteration (red sweep, copy and
+//                      mirror ghost fills, black sweep, fills; src/multigrid.jl:250-265)
+//                      in ONE phase.  The iteration reads the level's current buffer and
+//                      writes the other one (ping-pong per level).  Each CTA stages its
+//                      block with ghosts in shared memory, updates the red cells, then
+//                      recomputes the red update of every neighbour edge cell its black
+//                      cells will read (their stencils touch only black cells and stored
+//                      ghosts of the old buffer, so the values are bit-identical to the
+//                      neighbour's own), updates the black cells, and writes the block
+//                      plus the ghost values it feeds: the facing ghosts of its
+//                      neighbours (fill_ghost_copy!), its mirror ghosts (fill_ghost_bnd!)
+//                      and its frozen refinement ghosts.  No two CTAs write one address.
+//   restrict         : per fine block: residual (src/multigrid.jl:309-323) and the
+//                      restriction of r and u to the parent's subblock
+//                      (src/restrict.jl:5-25, same summation order), with pushes of the
+//                      restricted u into the coarse ghosts.  The FAS right-hand side
+//                      (src/multigrid.jl:331-344) is formed at the start of the coarse
+//                      level's first GS iteration, whose old buffer is exactly the
+//                      post-restriction state; a neighbour's covered edge cells get the
+//                      same FAS value recomputed from the same tile values.
+//   prolongate       : per fine block: u += P(e) (src/interp.jl:24-63), pushes of the
+//                      new edge values, and the block's refinement-boundary ghosts
+//                      interpolated from the (final) coarser level.
+// The coarse correction e = u - u1 of a level (diffto!, src/blockfield.jl:569-576) and
+// its ghosts are produced in that level's last GS iteration.  Levels 1..local_top are
+// processed by CTA 0 alone with CTA barriers.  Block tiles reach shared memory through
+// bulk asynchronous copies (cp.async.bulk, no multicast) into a double-buffered
+// per-slot pipeline; every wait on an mbarrier or a barrier is bounded in time.
+#pragma once
+#include "srmg_kernels.cuh"
+
+namespace srmg {
+
+constexpr int kMaxLev = 30;
+constexpr int kTraceMax = 1024;
+
+struct EngTree {
+  const int4 *lvl_rec[kMaxLev];     // per level: 5 int4 per block ({blk, cr, cz, child_mask}, faces)
+  const int4 *lvl_blocks[kMaxLev];  // per level: {blk, coord_r, coord_z, child_mask}
+  const int4 *lvl_child[kMaxLev];   // per level: {fine, coarse, sb_r, sb_z}
+  int nblk[kMaxLev];
+  int nch[kMaxLev];
+  const int4 *info;    // by block id: {coord_r, coord_z, child_mask, level}
+  const int4 *faces;   // by block id * 4 + face: {type, src, sb_r | sb_z << 8 (refinement) or
+                       //  the neighbour's child mask (neighbour), push_to}
+  const int4 *kids;    // by block id: child block id per subblock, -1 if none
+};
+
+template <typename T>
+struct EngArgs {
+  T *u, *ualt, *b, *u1, *e;   // ualt: the second buffer of the per-level ping-pong
+  EngTree tr;
+  WTab<T> wt;
+  Signs sg;
+  int op, geom;
+  int lmax;          // finest non-empty level taking part
+  int ndown, ntop, nup;
+  int local_top;     // levels 1..local_top run inside CTA 0
+  T lev_s[kMaxLev + 1];       // s_l by level (index l)
+  T lev_centre[kMaxLev + 1];  // stencil centre by level
+  T lev_nwc[kMaxLev + 1];     // -(omega / diagelm) by level
+  unsigned *bar;     // barrier counter, zero at launch
+  int *err;          // error word (0 = ok)
+  long long timeout_ns;
+  long long *trace;  // optional: CTA 0 stamps %globaltimer after every phase
+};
+
+// ------------------------------------------------------------------ barriers
+
+__device__ __forceinline__ long long gtimer() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Grid-wide barrier on a monotonic counter.  A wait longer than timeout_ns sets the
+// error word and returns false; every CTA then leaves the kernel at its next check.
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err, unsigned &epoch,
+                                             long long timeout_ns) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    epoch++;
+    const unsigned target = epoch * gridDim.x;
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
+    int ok = 1;
+    const long long t0 = gtimer();
+    while (true) {
+      unsigned v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+      if (v >= target) break;
+      if (*(volatile int *)err) { ok = 0; break; }
+      if (gtimer() - t0 > timeout_ns) {
+        atomicCAS(err, 0, 1);
+        ok = 0;
+        break;
+      }
+      __nanosleep(20);
+    }
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+__device__ __forceinline__ void slot_sync(int slot) {
+  asm volatile("bar.sync %0, 256;" ::"r"(slot + 1) : "memory");
+}
+
+// ------------------------------------------------------------------ helpers
+
+template <typename T>
+__device__ __forceinline__ T restrict4(const T *f, int fx, int fy) {
+  const int o = fx + kS * fy;
+  T v = dadd<T>(T(0), f[o]);
+  v = dadd<T>(v, f[o + 1]);
+  v = dadd<T>(v, f[o + kS]);
+  v = dadd<T>(v, f[o + kS + 1]);
+  return dmul<T>(v, T(0.25));
+}
+
+// Bulk (TMA, non-multicast) copies global -> shared with an mbarrier, per slot.
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up (and raises the error word) after timeout_ns.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, long long timeout_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = gtimer();
+  while (!mbar_try_wait(bar, parity)) {
+    if (gtimer() - t0 > timeout_ns) {
+      atomicCAS(err, 0, 2);
+      return false;
+    }
+  }
+  return true;
+}
+
+// Per-slot staging: a double-buffered block tile and the records of up to 32 blocks.
+template <typename T>
+struct SlotSmem {
+  T tile[2][kSS];
+  int4 recs[32][5];
+  uint64_t bar[2];
+};
+
+// Write the value v of valid cell (x, y) of block X into the ghosts that copy or mirror
+// it, in `field`: the facing ghost of each neighbour (fill_ghost_copy!) and the block's
+// own mirror ghost (fill_ghost_bnd!).  fc: the block's four face records.
+template <typename T>
+__device__ __forceinline__ void push(const EngArgs<T> &A, T *field, int X, const int4 *fc, int x, int y, T v) {
+  T *xb = field + (int64_t)X * kSS;
+  if (x <= 3) {
+    const int4 fi = fc[0];
+    if (fi.w >= 0) field[(int64_t)fi.w * kSS + (x + kM) + kS * y] = v;
+    else if (fi.x == FACE_BOUNDARY) xb[(2 * kG - 1 - x) + kS * y] = dmul<T>(T(A.sg.v[3]), v);
+  }
+  if (x >= 16) {
+    const int4 fi = fc[1];
+    if (fi.w >= 0) field[(int64_t)fi.w * kSS + (x - kM) + kS * y] = v;
+    else if (fi.x == FACE_BOUNDARY) xb[(2 * (kG + kM) - 1 - x) + kS * y] = dmul<T>(T(A.sg.v[5]), v);
+  }
+  if (y <= 3) {
+    const int4 fi = fc[2];
+    if (fi.w >= 0) field[(int64_t)fi.w * kSS + x + kS * (y + kM)] = v;
+    else if (fi.x == FACE_BOUNDARY) xb[x + kS * (2 * kG - 1 - y)] = dmul<T>(T(A.sg.v[1]), v);
+  }
+  if (y >= 16) {
+    const int4 fi = fc[3];
+    if (fi.w >= 0) field[(int64_t)fi.w * kSS + x + kS * (y - kM)] = v;
+    else if (fi.x == FACE_BOUNDARY) xb[x + kS * (2 * (kG + kM) - 1 - y)] = dmul<T>(T(A.sg.v[7]), v);
+  }
+}
+
+// Ghost cell `lane` (0..31) of face f: layer lane/16, position lane%16.
+__device__ __forceinline__ void ghost_xy(int f, int lane, int &x, int &y) {
+  const int g = lane >> 4, k = lane & 15;
+  if (f == 0) { x = g; y = 2 + k; }
+  else if (f == 1) { x = 18 + g; y = 2 + k; }
+  else if (f == 2) { x = 2 + k; y = g; }
+  else { x = 2 + k; y = 18 + g; }
+}
+
+// Refinement-boundary ghost q (0..127) of block X in `dst`, interpolated from `src` on
+// the coarser level (fill_ghost_interp!, src/connectivity.jl:251-258).
+template <typename T>
+__device__ __forceinline__ void refbnd_ghost(T *dst, const T *src, int X, const int4 *fc, int q) {
+  const int f = q >> 5, lane = q & 31;
+  const int4 fi = fc[f];
+  if (fi.x != FACE_REFBND) return;
+  const int g = lane >> 4, k = lane & 15;
+  int x, y;
+  ghost_xy(f, lane, x, y);
+  const T *cb = src + (int64_t)fi.y * kSS;
+  const int sbr = fi.z & 0xff, sbz = fi.z >> 8;
+  int jr, jz, ir, iz;
+  if (f <= 1) {
+    jr = (f == 0) ? (1 + 8 * sbr) : (2 + 8 * (sbr - 1));
+    ir = g;
+    jz = 2 + 8 * (sbz - 1) + (k >> 1);
+    iz = k & 1;
+  } else {
+    jz = (f == 2) ? (1 + 8 * sbz) : (2 + 8 * (sbz - 1));
+    iz = g;
+    jr = 2 + 8 * (sbr - 1) + (k >> 1);
+    ir = k & 1;
+  }
+  const int o = jr + kS * jz;
+  T v = dmul<T>(T(0.5), cb[o]);
+  v = dadd<T>(v, dmul<T>(T(0.25), cb[o + (2 * ir - 1)]));
+  v = dadd<T>(v, dmul<T>(T(0.25), cb[o + kS * (2 * iz - 1)]));
+  dst[(int64_t)X * kSS + x + kS * y] = v;
+}
+
+// ------------------------------------------------------------------ phases
+
+// Issue the bulk copy of one block tile into buffer `buf` of a slot.
+template <typename T>
+__device__ __forceinline__ void issue_tile(SlotSmem<T> &S, int buf, const T *src, int X) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  mbar_expect_tx(&S.bar[buf], (uint32_t)(kSS * sizeof(T)));
+  bulk_g2s(S.tile[buf], src + (int64_t)X * kSS, (uint32_t)(kSS * sizeof(T)), &S.bar[buf]);
+}
+
+// Halo cell of thread t < 64: face t/16, position t%16 along the face, in the
+// block's frame; (nx, ny) is the same cell in the neighbour's frame.
+struct HaloCell {
+  int f, jj, hx, hy, nx, ny, nsub;
+  bool red;
+  int cx, cy;   // the one stencil neighbour that is a ghost corner of this block, or cx < 0
+  int cnx, cny; // that corner in the neighbour's frame
+};
+
+__device__ __forceinline__ HaloCell halo_cell(int t) {
+  HaloCell h;
+  h.f = t >> 4;
+  h.jj = t & 15;
+  if (h.f == 0) { h.hx = 1; h.hy = 2 + h.jj; }
+  else if (h.f == 1) { h.hx = 18; h.hy = 2 + h.jj; }
+  else if (h.f == 2) { h.hx = 2 + h.jj; h.hy = 1; }
+  else { h.hx = 2 + h.jj; h.hy = 18; }
+  const int dx = h.f == 0 ? kM : h.f == 1 ? -kM : 0, dy = h.f == 2 ? kM : h.f == 3 ? -kM : 0;
+  h.nx = h.hx + dx;
+  h.ny = h.hy + dy;
+  h.nsub = ((h.nx - 2) >> 3) + 2 * ((h.ny - 2) >> 3);
+  h.red = ((h.hx + h.hy) & 1) == 1;
+  h.cx = -1;
+  h.cy = -1;
+  if (h.jj == 0 || h.jj == 15) {
+    const int d = h.jj == 0 ? -1 : 1;
+    if (h.f <= 1) { h.cx = h.hx; h.cy = h.hy + d; }
+    else { h.cx = h.hx + d; h.cy = h.hy; }
+  }
+  h.cnx = h.cx + dx;
+  h.cny = h.cy + dy;
+  return h;
+}
+
+// One fused red-black GS iteration over level l: src -> dst.  256 threads per block,
+// thread t owns valid cell (2 + t%16, 2 + t/16).  Blocks stream through a
+// double-buffered shared-memory pipeline fed by bulk copies, and each block's scattered
+// inputs (its b, the neighbours' edge b and ghost corners) are loaded into registers
+// while the previous block computes.  With `fas`, the FAS right-hand side of the
+// covered cells (src/multigrid.jl:112-119) is formed first from the post-restriction
+// tile and the restricted residual held in e.
+template <typename T>
+__device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T *esrc, bool copy_u1,
+                       bool make_e, bool fas, int first, int step, int t, int slot, SlotSmem<T> &S,
+                       unsigned &pk) {
+  const int n = A.tr.nblk[l - 1];
+  const int4 *recs = A.tr.lvl_rec[l - 1];
+  const int nmine = (first < n) ? (n - 1 - first) / step + 1 : 0;
+  if (nmine == 0) return true;
+  const int x = 2 + (t & 15), y = 2 + (t >> 4);
+  const int o = x + kS * y;
+  const bool red = ((x + y) & 1) == 1;  // colour 0 of RedBlack{0}: updated first
+  const int mysub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
+  const T s = A.lev_s[l], centre = A.lev_centre[l], nwc = A.lev_nwc[l];
+  const HaloCell h = halo_cell(t < 64 ? t : 0);
+  // registers prefetched one block ahead
+  T b_nx = T(0), e_nx = T(0), hv_nx = T(0), hc_nx = T(0);
+  auto prefetch = [&](int j) {
+    const int4 bk = S.recs[j][0];
+    const int X = bk.x;
+    b_nx = A.b[(int64_t)X * kSS + o];
+    if (fas && ((bk.w >> mysub) & 1)) e_nx = A.e[(int64_t)X * kSS + o];
+    if (t < 64 && h.red) {
+      const int4 fi = S.recs[j][1 + h.f];
+      if (fi.x == FACE_NEIGHBOR) {
+        const int64_t nb = (int64_t)fi.y * kSS;
+        hv_nx = (fas && ((fi.z >> h.nsub) & 1)) ? A.e[nb + h.nx + kS * h.ny] : A.b[nb + h.nx + kS * h.ny];
+        if (h.cx >= 0) hc_nx = src[nb + h.cnx + kS * h.cny];
+      }
+    }
+  };
+  for (int c0 = 0; c0 < nmine; c0 += 32) {
+    const int cn = min(32, nmine - c0);
+    if (t < 5 * cn) {
+      const int q = t / 5, k = t - 5 * q;
+      S.recs[q][k] = recs[5 * (first + (c0 + q) * step) + k];
+    }
+    slot_sync(slot);
+    if (t == 0) issue_tile<T>(S, pk & 1, src, S.recs[0][0].x);
+    prefetch(0);
+    for (int j = 0; j < cn; ++j) {
+      const unsigned kb = pk + j;
+      const int buf = kb & 1;
+      const int4 bk = S.recs[j][0];
+      const int4 *fc = &S.recs[j][1];
+      const int X = bk.x;
+      if (t == 0 && j + 1 < cn) issue_tile<T>(S, (kb + 1) & 1, src, S.recs[j + 1][0].x);
+      T bx = b_nx;
+      const T ex = e_nx, hv = hv_nx, hc = hc_nx;
+      if (j + 1 < cn) prefetch(j + 1);
+      if (!mbar_wait(&S.bar[buf], (kb >> 1) & 1, A.err, A.timeout_ns)) {
+        // leave no copy in flight: wait (bounded) for the one issued for item j + 1
+        if (j + 1 < cn) mbar_wait(&S.bar[(kb + 1) & 1], ((kb + 1) >> 1) & 1, A.err, A.timeout_ns);
+        return false;
+      }
+      T *tile = S.tile[buf];
+      const W5<T> w = weights<T>(A.wt, A.geom, bk.y, bk.z, x, y);
+      if (copy_u1) A.u1[(int64_t)X * kSS + o] = tile[o];
+      if (fas) {
+        if ((bk.w >> mysub) & 1) {
+          const T Lu = apply5<T>(tile, x, y, w, centre);
+          bx = -(ex + Lu / s);
+          A.b[(int64_t)X * kSS + o] = bx;
+        }
+        slot_sync(slot);
+      }
+      if (red) {
+        const T Lu = apply5<T>(tile, x, y, w, centre);
+        tile[o] = fma(nwc, fma(s, bx, Lu), tile[o]);
+      }
+      if (t < 64 && h.red && fc[h.f].x == FACE_NEIGHBOR) {
+        // red update of the neighbour's edge cell that sits in this block's ghost layer
+        const int4 fi = fc[h.f];
+        auto at = [&](int a, int c) -> T { return (a == h.cx && c == h.cy) ? hc : tile[a + kS * c]; };
+        const W5<T> wh = weights<T>(A.wt, A.geom, bk.y, bk.z, h.hx, h.hy);
+        T v = wh.zm * at(h.hx, h.hy - 1);
+        v = v + wh.rm * at(h.hx - 1, h.hy);
+        v = v + centre * tile[h.hx + kS * h.hy];
+        v = v + wh.rp * at(h.hx + 1, h.hy);
+        v = v + wh.zp * at(h.hx, h.hy + 1);
+        const T bn = (fas && ((fi.z >> h.nsub) & 1)) ? -(hv + v / s) : hv;
+        tile[h.hx + kS * h.hy] = fma(nwc, fma(s, bn, v), tile[h.hx + kS * h.hy]);
+      }
+      slot_sync(slot);
+      if (!red) {
+        const T Lu = apply5<T>(tile, x, y, w, centre);
+        tile[o] = fma(nwc, fma(s, bx, Lu), tile[o]);
+      }
+      slot_sync(slot);
+      const T nu = tile[o];
+      dst[(int64_t)X * kSS + o] = nu;
+      push<T>(A, dst, X, fc, x, y, nu);
+      if (t < 128) {
+        const int f = t >> 5, lane = t & 31;
+        if (fc[f].x == FACE_REFBND) {
+          int gx, gy;
+          ghost_xy(f, lane, gx, gy);
+          dst[(int64_t)X * kSS + gx + kS * gy] = tile[gx + kS * gy];  // frozen during smoothing
+        }
+      }
+      if (make_e) {
+        const T ev = nu - A.u1[(int64_t)X * kSS + o];
+        A.e[(int64_t)X * kSS + o] = ev;
+        push<T>(A, A.e, X, fc, x, y, ev);
+        if (t < 128) refbnd_ghost<T>(A.e, esrc, X, fc, t);
+      }
+      slot_sync(slot);  // the buffer is refilled two items later
+    }
+    pk += cn;
+  }
+  return true;
+}
+
+// Residual and restriction of r and u, one fine block (Child edge of level l) per
+// 256-thread slot: the restricted u goes to the coarse block (and into the coarse
+// ghosts that copy it), the restricted r to e, where the coarse level's first GS
+// iteration reads it to form the FAS right-hand side.  uf: level l, uc: level l-1.
+template <typename T>
+__device__ void ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int first, int step, int t,
+                            int slot, T *buf) {
+  T *sr = buf, *su = buf + 256;
+  const int n = A.tr.nch[l - 1];
+  const int4 *ch = A.tr.lvl_child[l - 1];
+  const int x = 2 + (t & 15), y = 2 + (t >> 4);
+  const T s = A.lev_s[l], centre = A.lev_centre[l];
+  for (int i = first; i < n; i += step) {
+    const int4 e = ch[i];
+    const int F = e.x, C = e.y;
+    const int4 fi = A.tr.info[F];
+    const T *ufb = uf + (int64_t)F * kSS;
+    const int o = x + kS * y;
+    const W5<T> w = weights<T>(A.wt, A.geom, fi.x, fi.y, x, y);
+    const T Lu = apply5<T>(ufb, x, y, w, centre);
+    sr[t] = -(A.b[(int64_t)F * kSS + o] + Lu / s);
+    su[t] = ufb[o];
+    slot_sync(slot);
+    if (t < 64) {
+      const int kx = t & 7, ky = t >> 3;
+      const int cx = 2 + 8 * (e.z - 1) + kx, cy = 2 + 8 * (e.w - 1) + ky;
+      const int i00 = 2 * kx + 16 * 2 * ky;
+      T cu = dadd<T>(T(0), su[i00]);
+      cu = dadd<T>(cu, su[i00 + 1]);
+      cu = dadd<T>(cu, su[i00 + 16]);
+      cu = dadd<T>(cu, su[i00 + 17]);
+      cu = dmul<T>(cu, T(0.25));
+      T cr = dadd<T>(T(0), sr[i00]);
+      cr = dadd<T>(cr, sr[i00 + 1]);
+      cr = dadd<T>(cr, sr[i00 + 16]);
+      cr = dadd<T>(cr, sr[i00 + 17]);
+      cr = dmul<T>(cr, T(0.25));
+      uc[(int64_t)C * kSS + cx + kS * cy] = cu;
+      push<T>(A, uc, C, A.tr.faces + 4 * C, cx, cy, cu);
+      A.e[(int64_t)C * kSS + cx + kS * cy] = cr;
+    }
+    slot_sync(slot);
+  }
+}
+
+// u_fine += P(e_coarse) on every valid cell (in place in uf), pushes of the new edge
+// values, and the fine block's refinement-boundary ghosts from uc (final coarse level).
+template <typename T>
+__device__ void ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int first, int step, int t) {
+  const int n = A.tr.nch[l - 1];
+  const int4 *ch = A.tr.lvl_child[l - 1];
+  const int dx = t & 15, dy = t >> 4;
+  const int x = 2 + dx, y = 2 + dy;
+  for (int i = first; i < n; i += step) {
+    const int4 e = ch[i];
+    const int F = e.x, C = e.y;
+    const int ir = dx & 1, iz = dy & 1;
+    const int jr = 2 + 8 * (e.z - 1) + (dx >> 1), jz = 2 + 8 * (e.w - 1) + (dy >> 1);
+    const T *cb = A.e + (int64_t)C * kSS;
+    const int oc = jr + kS * jz;
+    T v = dmul<T>(T(0.5), cb[oc]);
+    v = dadd<T>(v, dmul<T>(T(0.25), cb[oc + (2 * ir - 1)]));
+    v = dadd<T>(v, dmul<T>(T(0.25), cb[oc + kS * (2 * iz - 1)]));
+    T *d = uf + (int64_t)F * kSS + x + kS * y;
+    const T nu = dadd<T>(v, *d);
+    *d = nu;
+    const int4 *fc = A.tr.faces + 4 * F;
+    push<T>(A, uf, F, fc, x, y, nu);
+    if (t < 128) refbnd_ghost<T>(uf, uc, F, fc, t);
+  }
+}
+
+// Copy level l's blocks (valid cells and face ghosts) from src to dst.
+template <typename T>
+__device__ void ph_copy_back(const EngArgs<T> &A, int l, const T *src, T *dst, int first, int step, int t) {
+  const int n = A.tr.nblk[l - 1];
+  const int4 *blocks = A.tr.lvl_blocks[l - 1];
+  for (int i = first; i < n; i += step) {
+    const int X = blocks[i].x;
+    for (int k = t; k < kSS; k += 256) {
+      const int x = k % kS, y = k / kS;
+      const bool corner = (x < 2 || x > 17) && (y < 2 || y > 17);
+      if (!corner) dst[(int64_t)X * kSS + k] = src[(int64_t)X * kSS + k];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ the kernel
+
+template <typename T>
+__global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant__ EngArgs<T> A) {
+  __shared__ __align__(128) SlotSmem<T> smem[4];
+  const int nslots = blockDim.x >> 8;
+  const int slot = threadIdx.x >> 8, t = threadIdx.x & 255;
+  const bool cta0 = blockIdx.x == 0;
+  SlotSmem<T> &S = smem[slot];
+  if (t == 0) {
+    mbar_init(&S.bar[0]);
+    mbar_init(&S.bar[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  unsigned pk = 0;  // items streamed through this slot's buffers so far
+  unsigned epoch = 0;
+  int ntrace = 0;
+  const int L = A.lmax, K = A.local_top;
+  unsigned cur = 0;  // bit l: level l currently lives in ualt
+  auto fld = [&](int l) -> T * { return ((cur >> l) & 1) ? A.ualt : A.u; };
+  auto oth = [&](int l) -> T * { return ((cur >> l) & 1) ? A.u : A.ualt; };
+  T *scratch = &S.tile[0][0];  // restriction phase staging (no bulk copies in flight then)
+
+  auto first_of = [&](bool loc) { return loc ? slot : blockIdx.x * nslots + slot; };
+  auto step_of = [&](bool loc) { return loc ? nslots : gridDim.x * nslots; };
+  auto stamp = [&]() {
+    if (A.trace && cta0 && threadIdx.x == 0 && ntrace < kTraceMax) A.trace[ntrace++] = gtimer();
+  };
+  // Barrier after a phase: CTA-local when this and the next phase are both local.
+  auto sync = [&](bool ok_in, bool cur_loc, bool next_loc) -> bool {
+    bool ok = ok_in;
+    if (cur_loc && next_loc) {
+      if (cta0) __syncthreads();
+      if (!ok_in) atomicCAS(A.err, 0, 3);
+    } else {
+      if (!ok_in) atomicCAS(A.err, 0, 3);
+      ok = grid_barrier(A.bar, A.err, epoch, A.timeout_ns) && ok_in;
+    }
+    stamp();
+    if (cta0 && cur_loc && next_loc) ok = ok && *(volatile int *)A.err == 0;
+    return ok;
+  };
+  auto runs = [&](bool loc) { return !loc || cta0; };
+  stamp();
+
+  // descending leg
+  for (int l = L; l >= 2; --l) {
+    const bool loc = l <= K;
+    for (int it = 0; it < A.ndown; ++it) {
+      bool ok = true;
+      if (runs(loc))
+        ok = ph_gsi<T>(A, l, fld(l), oth(l), nullptr, it == 0 && l < L, false, it == 0 && l < L, first_of(loc),
+                       step_of(loc), t, slot, S, pk);
+      cur ^= 1u << l;
+      if (!sync(ok, loc, loc)) return;
+    }
+    if (runs(loc)) ph_restrict<T>(A, l, fld(l), fld(l - 1), first_of(loc), step_of(loc), t, slot, scratch);
+    if (!sync(true, loc, (l - 1) <= K)) return;
+  }
+  // coarsest level
+  {
+    const bool loc = 1 <= K;
+    for (int it = 0; it < A.ntop; ++it) {
+      const bool last = it == A.ntop - 1;
+      bool ok = true;
+      if (runs(loc))
+        ok = ph_gsi<T>(A, 1, fld(1), oth(1), nullptr, it == 0 && L > 1, last && L > 1, it == 0 && L > 1,
+                       first_of(loc), step_of(loc), t, slot, S, pk);
+      cur ^= 1u << 1;
+      if (!sync(ok, loc, last ? (2 <= K || L < 2) : loc)) return;
+    }
+  }
+  // ascending leg
+  for (int l = 2; l <= L; ++l) {
+    const bool loc = l <= K;
+    if (runs(loc)) ph_prolong<T>(A, l, fld(l), fld(l - 1), first_of(loc), step_of(loc), t);
+    if (!sync(true, loc, loc)) return;
+    for (int it = 0; it < A.nup; ++it) {
+      const bool last = it == A.nup - 1;
+      bool ok = true;
+      if (runs(loc))
+        ok = ph_gsi<T>(A, l, fld(l), oth(l), A.e, false, last && l < L, false, first_of(loc), step_of(loc), t,
+                       slot, S, pk);
+      cur ^= 1u << l;
+      const bool next_loc = last ? ((l + 1) <= K) : loc;
+      if (!sync(ok, loc, l == L && last ? false : next_loc)) return;
+    }
+  }
+  // levels left in the second buffer go back to u
+  bool any = false;
+  for (int l = 1; l <= L; ++l)
+    if ((cur >> l) & 1) {
+      ph_copy_back<T>(A, l, A.ualt, A.u, blockIdx.x * nslots + slot, gridDim.x * nslots, t);
+      any = true;
+    }
+  if (any) grid_barrier(A.bar, A.err, epoch, A.timeout_ns);
+  if (A.trace && cta0 && threadIdx.x == 0 && ntrace < kTraceMax) A.trace[ntrace] = 0;
+}
+
+}  // namespace srmg

@@ -31,6 +31,12 @@ template <typename T>
 int leafnorm_dev(srmg_ctx *ctx, const T *u, const T *b, double s, int op, double k2, int geom,
                  int mode, int slot);
 int read_small(srmg_ctx *ctx, int n);
+
+int engine_local_top(srmg_ctx *ctx, int lmax);
+template <typename T>
+int engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, double s, int op, double k2, int geom,
+                  const Signs &sg, int lmax, int ndown, int ntop, int nup, double omega);
+int engine_check(srmg_ctx *ctx);
 int stage_in(srmg_ctx *ctx, int slot, const double *h, int64_t nblk_alloc, double **d);
 int stage_out(srmg_ctx *ctx, double *h, const double *d, int64_t nblk_alloc);
 

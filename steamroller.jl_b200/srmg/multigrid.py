@@ -84,6 +84,8 @@ SIGNATURES = {
     "srmg_interp_add_level_dev": (_I, [_P, _P, _P, _I64, _I]),
     "srmg_residual_postrestrict_level_dev": (_I, [_P, _P, _P, _P, _I64, _I, _D, _I, _D, _I]),
     "srmg_resnorm_noalloc": (_I, [_P, _P, _P, _I64, _D, _I, _D, _I, _P]),
+    "srmg_set_option": (_I, [_P, ctypes.c_char_p, _I64]),
+    "srmg_get_trace": (_I, [_P, _P, _I]),
     "srmg_launch_count": (_I64, [_P]),
 }
 
@@ -175,6 +177,18 @@ class Context:
         self.check(lib().srmg_set_tree(self._h, nlev, *pairs, *nb, *bd, *rb, *ch, self.generation))
         self._tree_keep = keep
         return self
+
+    def set_option(self, key: str, value: int):
+        self.check(lib().srmg_set_option(self._h, key.encode(), int(value)))
+        return self
+
+    def trace(self):
+        """Phase timestamps (ns) of the last persistent-kernel launch."""
+        out = np.zeros(1024, dtype=np.int64)
+        n = lib().srmg_get_trace(self._h, out.ctypes.data, len(out))
+        if n < 0:
+            self.check(n)
+        return out[:n].copy()
 
     def launches(self) -> int:
         return lib().srmg_launch_count(self._h)

@@ -199,6 +199,42 @@ def test_vcycle_matches_oracle(pair, ncycles):
     assert rel_l2(to_np(bg), bo, vm) <= 1e-10     # FAS right-hand sides
 
 
+def test_engine_matches_per_operation_kernels(pair):
+    """The persistent one-launch V-cycle reproduces the per-operation kernel sequence."""
+    p = pair.p
+    u, b = _prepared(pair)
+    out = {}
+    for engine in (0, 1):
+        pair.ctx.set_option("engine", engine)
+        ug, bg = torch_cuda(u), torch_cuda(b)
+        mg.vcycle_(pair.ctx, ug, bg, torch_cuda(np.zeros_like(u)), torch_cuda(np.zeros_like(u)), p.s,
+                   p.geom, p.bc, ndown=2, ntop=4, nup=2, ncycles=2)
+        pair.ctx.synchronize()
+        out[engine] = (to_np(ug), to_np(bg))
+    pair.ctx.set_option("engine", 1)
+    vm = valid_mask(u.shape)
+    assert rel_l2(out[1][0], out[0][0]) <= 1e-14
+    assert rel_l2(out[1][1], out[0][1], vm) <= 1e-13
+
+
+@pytest.mark.parametrize("local_max", [0, 4, 64])
+def test_engine_local_levels(local_max):
+    """Coarse levels run inside one CTA or across the grid: same iterates."""
+    p = PROBS["refined"]
+    pr = Pair(p)
+    u, b = _prepared(pr)
+    pr.ctx.set_option("local_max_blocks", local_max)
+    ug, bg = torch_cuda(u), torch_cuda(b)
+    mg.vcycle_(pr.ctx, ug, bg, torch_cuda(np.zeros_like(u)), torch_cuda(np.zeros_like(u)), p.s, p.geom,
+               p.bc, ndown=2, ntop=4, nup=2, ncycles=2)
+    pr.ctx.synchronize()
+    uo, bo = u.copy(), b.copy()
+    r, u1 = np.zeros_like(u), np.zeros_like(u)
+    for _ in range(2):
+        pr.orc.vcycle(uo, bo, r, u1, ndown=2, ntop=4, nup=2)
+    assert rel_l2(to_np(ug), uo) <= REL_VCYCLE
+
+
 def test_vcycle_host_pointer_entry_point(pair):
     """srmg_vcycle (host arrays, the ccall boundary) == the device entry point."""
     p = pair.p
