@@ -171,11 +171,12 @@ def main():
     ap.add_argument("--target-leaf", type=int, default=TARGET_LEAF)
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--only", default=None, choices=[None, "vcycle"],
-                    help="vcycle: time plain FP64 V-cycles only (profiling runs)")
+    ap.add_argument("--only", default=None, choices=[None, "vcycle", "smooth"],
+                    help="vcycle: time plain FP64 V-cycles only; smooth: GS iterations on the finest "
+                         "level only (profiling runs)")
     ap.add_argument("--config", default="config2", choices=["config1", "config2", "config5"])
     args = ap.parse_args()
-    if args.only == "vcycle":
+    if args.only in ("vcycle", "smooth"):
         return vcycle_only(args)
 
     from srmg import gen, model
@@ -320,6 +321,28 @@ def vcycle_only(args):
     b = torch.from_numpy(problem.b).cuda()
     u, r, u1 = torch.zeros_like(b), torch.zeros_like(b), torch.zeros_like(b)
     torch.cuda.synchronize()
+    if args.only == "smooth":
+        import ctypes
+        L = problem.tree.finest_level()
+        sl = problem.s / 4 ** (L - 1)
+        bca = np.ascontiguousarray(problem.bc, dtype=np.int8)
+        run = lambda n: ctx.check(mg.lib().srmg_gs_iter_dev(ctx.handle, u.data_ptr(), b.data_ptr(), problem.nblk, L,
+                                                            1.0, sl, n, problem.op, problem.k2, problem.geom,
+                                                            bca.ctypes.data))
+        with torch.cuda.stream(stream):
+            run(args.warmup)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run(args.steps)
+            e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / max(1, args.steps)
+        nb = len(problem.tree[L - 1])
+        byts = nb * 256 * 24  # model: read u, b; write u per iteration
+        print(json.dumps({"only": "smooth", "config": args.config, "level": L, "blocks": nb,
+                          "us_per_iteration": ms * 1e3, "model_GBps": byts / (ms / 1e3) / 1e9}))
+        ctx.close()
+        return
     with torch.cuda.stream(stream):
         mg.vcycle_(ctx, u, b, r, u1, problem.s, problem.geom, problem.bc, ndown=2, ntop=4, nup=2,
                    ncycles=args.warmup)

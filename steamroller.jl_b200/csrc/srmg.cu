@@ -367,6 +367,9 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
   ctx->d_wp64 = (double *)(base + owp);
   ctx->d_wm32 = (float *)(base + owm32);
   ctx->d_wp32 = (float *)(base + owp32);
+  ctx->refbnd_levels = 0;
+  for (int l = 0; l < nlev; l++)
+    if (nrb[l] > 0 && l + 1 < 32) ctx->refbnd_levels |= 1u << (l + 1);
   ctx->d_info = (int4 *)(base + oinfo);
   ctx->d_faceb = (int4 *)(base + ofaceb);
   ctx->d_kids = (int4 *)(base + okids);
@@ -749,7 +752,11 @@ extern "C" int srmg_gs_iter_dev(srmg_ctx *ctx, double *u, const double *b, int64
   RC(check_call(ctx, nblk_alloc, op, geom, bc));
   if (!u || !b || level < 1 || level > ctx->nlev || n < 0)
     return fail(ctx, SRMG_ERR_BADARG, "gs_iter: bad arguments");
-  RC(L_gs_iter<double>(ctx, u, b, level, op_params<double>(op, geom, k2, sl, omega), n, make_signs(bc)));
+  const bool aligned = ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(b)) & 15) == 0;
+  if (ctx->use_engine && aligned)
+    RC(engine_smooth<double>(ctx, u, b, level, omega, sl, n, op, k2, geom, make_signs(bc)));
+  else
+    RC(L_gs_iter<double>(ctx, u, b, level, op_params<double>(op, geom, k2, sl, omega), n, make_signs(bc)));
   CK(cudaGetLastError());
   return SRMG_OK;
 }

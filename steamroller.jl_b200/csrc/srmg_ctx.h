@@ -61,6 +61,7 @@ struct srmg_ctx {
   int engine_ctas = 0;       // cooperative grid size (0 = not yet known)
   int local_max_blocks = 16; // levels whose every coarser level has <= this many blocks run in CTA 0
   bool use_engine = true;
+  unsigned refbnd_levels = 0;  // bit l: level l has refinement-boundary faces
   bool trace_on = false;
   srmg::DevBuf trace;        // %globaltimer stamps after every engine phase (CTA 0)
 

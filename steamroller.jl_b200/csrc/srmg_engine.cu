@@ -30,8 +30,10 @@ WTab<float> wtab_of<float>(srmg_ctx *ctx) { return WTab<float>{ctx->d_wm32, ctx-
 template <typename T>
 int engine_grid(srmg_ctx *ctx, int *grid) {
   if (ctx->num_sms == 0) CK(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  const size_t smem = engine_smem_bytes<T>();
+  CK(cudaFuncSetAttribute(k_engine_vcycle<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_engine_vcycle<T>, 1024, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_engine_vcycle<T>, 1024, smem));
   if (per_sm < 1) return fail(ctx, SRMG_ERR_CUDA, "engine kernel cannot be resident (occupancy 0)");
   *grid = ctx->num_sms * std::min(per_sm, 1);
   return SRMG_OK;
@@ -52,7 +54,8 @@ int srmg::engine_local_top(srmg_ctx *ctx, int lmax) {
 
 template <typename T>
 int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, double s, int op, double k2, int geom,
-                        const Signs &sg, int lmax, int ndown, int ntop, int nup, double omega) {
+                        const Signs &sg, int lmax, int ndown, int ntop, int nup, double omega,
+                        const double *coarse_P, int coarse_n, const MixedStep *mixed) {
   if (ctx->nlev > kMaxLev) return fail(ctx, SRMG_ERR_UNSUPPORTED, "engine supports at most %d levels", kMaxLev);
   if (lmax == 0) lmax = ctx->nlev;
   int L = 0;
@@ -89,6 +92,10 @@ int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, double s, int op
   A.ntop = ntop;
   A.nup = nup;
   A.local_top = engine_local_top(ctx, L);
+  if (coarse_P && coarse_n == 256 * ctx->nblk_host[0] && ctx->nblk_host[0] <= 4) {
+    A.coarse_P = coarse_P;
+    A.coarse_n = coarse_n;
+  }
   for (int l = 1; l <= L; l++) {
     const OpParams<T> p = op_params<T>(op, geom, k2, level_scale(s, l), omega);
     A.lev_s[l] = p.s;
@@ -99,26 +106,99 @@ int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, double s, int op
   A.bar = (unsigned *)ctx->sync.p;
   A.err = (int *)((char *)ctx->sync.p + 128);
   A.timeout_ns = 2000000000LL;  // 2 s per barrier wait
+  if (mixed) {
+    A.mx.u64 = mixed->u64;
+    A.mx.b64 = mixed->b64;
+    A.mx.wt64 = WTab<double>{ctx->d_wm64, ctx->d_wp64};
+    for (int l = 1; l <= L; l++) {
+      const OpParams<double> p = op_params<double>(op, geom, k2, level_scale(s, l), omega);
+      A.mx.lev_s64[l] = p.s;
+      A.mx.lev_centre64[l] = p.centre;
+    }
+    A.mx.refbnd_levels = ctx->refbnd_levels;
+    A.mx.tol_abs = mixed->tol_abs;
+    A.mx.apply_update = mixed->apply_update;
+    RC(ensure(ctx, ctx->part, sizeof(double) * 4096));
+    A.mx.part = (double *)ctx->part.p;
+    A.mx.out = (double *)ctx->small.p + 4;
+  }
   if (ctx->trace_on) {
     RC(ensure(ctx, ctx->trace, kTraceMax * sizeof(long long)));
     A.trace = (long long *)ctx->trace.p;
   }
-  int grid = ctx->engine_ctas;
-  if (grid == 0) {
-    RC(engine_grid<T>(ctx, &grid));
-    ctx->engine_ctas = grid;
-  }
+  int grid = 0;
+  RC(engine_grid<T>(ctx, &grid));  // also raises the dynamic shared-memory limit
+  if (ctx->engine_ctas > 0 && ctx->engine_ctas < grid) grid = ctx->engine_ctas;
   CK(cudaMemsetAsync(ctx->sync.p, 0, 256, ctx->stream));
   void *args[] = {&A};
-  CK(cudaLaunchCooperativeKernel((const void *)k_engine_vcycle<T>, dim3(grid), dim3(1024), args, 0, ctx->stream));
+  CK(cudaLaunchCooperativeKernel((const void *)k_engine_vcycle<T>, dim3(grid), dim3(1024), args,
+                                 engine_smem_bytes<T>(), ctx->stream));
   ctx->launches++;
   return SRMG_OK;
 }
 
+// gauss_seidel_iter! on one level through the persistent kernel.
+template <typename T>
+int srmg::engine_smooth(srmg_ctx *ctx, T *u, const T *b, int level, double omega, double sl, int n, int op,
+                        double k2, int geom, const Signs &sg) {
+  if (n <= 0 || ctx->nblk_host[level - 1] == 0) return SRMG_OK;
+  EngArgs<T> A;
+  memset(&A, 0, sizeof A);
+  A.u = u;
+  {
+    DevBuf &alt = (sizeof(T) == 8) ? ctx->f64[5] : ctx->f32[5];
+    RC(ensure(ctx, alt, (size_t)ctx->max_blk * kSS * sizeof(T)));
+    A.ualt = (T *)alt.p;
+  }
+  A.b = const_cast<T *>(b);
+  for (int l = 0; l < ctx->nlev; l++) {
+    A.tr.lvl_rec[l] = ctx->lv[l].rec;
+    A.tr.lvl_blocks[l] = ctx->lv[l].blocks;
+    A.tr.lvl_child[l] = ctx->lv[l].child;
+    A.tr.nblk[l] = ctx->nblk_host[l];
+    A.tr.nch[l] = ctx->nch_host[l];
+  }
+  A.tr.info = ctx->d_info;
+  A.tr.faces = ctx->d_faceb;
+  A.tr.kids = ctx->d_kids;
+  A.wt = wtab_of<T>(ctx);
+  A.sg = sg;
+  A.op = op;
+  A.geom = geom;
+  A.lmax = level;
+  A.smooth_level = level;
+  A.smooth_n = n;
+  const OpParams<T> p = op_params<T>(op, geom, k2, sl, omega);
+  A.lev_s[level] = p.s;
+  A.lev_centre[level] = p.centre;
+  A.lev_nwc[level] = p.nwc;
+  RC(ensure(ctx, ctx->sync, 256));
+  A.bar = (unsigned *)ctx->sync.p;
+  A.err = (int *)((char *)ctx->sync.p + 128);
+  A.timeout_ns = 2000000000LL;
+  if (ctx->trace_on) {
+    RC(ensure(ctx, ctx->trace, kTraceMax * sizeof(long long)));
+    A.trace = (long long *)ctx->trace.p;
+  }
+  int grid = 0;
+  RC(engine_grid<T>(ctx, &grid));
+  if (ctx->engine_ctas > 0 && ctx->engine_ctas < grid) grid = ctx->engine_ctas;
+  CK(cudaMemsetAsync(ctx->sync.p, 0, 256, ctx->stream));
+  void *args[] = {&A};
+  CK(cudaLaunchCooperativeKernel((const void *)k_engine_vcycle<T>, dim3(grid), dim3(1024), args,
+                                 engine_smem_bytes<T>(), ctx->stream));
+  ctx->launches++;
+  return SRMG_OK;
+}
+template int srmg::engine_smooth<double>(srmg_ctx *, double *, const double *, int, double, double, int, int,
+                                         double, int, const Signs &);
+
 template int srmg::engine_vcycle<double>(srmg_ctx *, double *, double *, double *, double *, double, int,
-                                         double, int, const Signs &, int, int, int, int, double);
+                                         double, int, const Signs &, int, int, int, int, double,
+                                         const double *, int, const MixedStep *);
 template int srmg::engine_vcycle<float>(srmg_ctx *, float *, float *, float *, float *, double, int,
-                                        double, int, const Signs &, int, int, int, int, double);
+                                        double, int, const Signs &, int, int, int, int, double,
+                                        const double *, int, const MixedStep *);
 
 extern "C" int srmg_get_trace(srmg_ctx *ctx, int64_t *out, int max_entries) {
   if (!ctx || !out || max_entries < 0) return SRMG_ERR_BADARG;

@@ -50,6 +50,24 @@ struct EngTree {
   const int4 *kids;    // by block id: child block id per subblock, -1 if none
 };
 
+// FP64 side of one defect-correction step of the mixed-precision solve.  The launch
+// first applies the previous correction (u64 += u), makes u64 a composite-grid function
+// of its leaves (restriction chain, ghost refresh), forms the FP64 defect as the FP32
+// right-hand side with its leaf norm, and runs the FP32 V-cycle only if the norm is
+// still above tol_abs.
+struct MixedArgs {
+  double *u64;
+  const double *b64;
+  WTab<double> wt64;
+  double lev_s64[kMaxLev + 1];
+  double lev_centre64[kMaxLev + 1];
+  unsigned refbnd_levels;  // bit l: level l has refinement-boundary faces
+  double tol_abs;
+  int apply_update;
+  double *part;            // one partial per CTA
+  double *out;             // out[0] = defect leaf norm, out[1] = 1 if converged
+};
+
 template <typename T>
 struct EngArgs {
   T *u, *ualt, *b, *u1, *e;   // ualt: the second buffer of the per-level ping-pong
@@ -60,6 +78,8 @@ struct EngArgs {
   int lmax;          // finest non-empty level taking part
   int ndown, ntop, nup;
   int local_top;     // levels 1..local_top run inside CTA 0
+  int smooth_level;  // > 0: run smooth_n GS iterations on this level only (gauss_seidel_iter!)
+  int smooth_n;
   T lev_s[kMaxLev + 1];       // s_l by level (index l)
   T lev_centre[kMaxLev + 1];  // stencil centre by level
   T lev_nwc[kMaxLev + 1];     // -(omega / diagelm) by level
@@ -67,6 +87,9 @@ struct EngArgs {
   int *err;          // error word (0 = ok)
   long long timeout_ns;
   long long *trace;  // optional: CTA 0 stamps %globaltimer after every phase
+  const double *coarse_P;  // optional: the coarsest level is solved directly, u1 = P b1
+  int coarse_n;            // unknowns of the coarsest level (256 per block, <= 1024)
+  MixedArgs mx;            // mixed-precision outer step (mx.u64 != nullptr)
 };
 
 // ------------------------------------------------------------------ barriers
@@ -163,40 +186,46 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
   return true;
 }
 
-// Per-slot staging: a double-buffered block tile and the records of up to 32 blocks.
+// Per-slot staging: triple-buffered block tiles and the records of up to 32 blocks.
+constexpr int kBuf = 3;
 template <typename T>
 struct SlotSmem {
-  T tile[2][kSS];
+  T tile[kBuf][kSS];
   int4 recs[32][5];
-  uint64_t bar[2];
+  uint64_t bar[kBuf];
 };
 
 // Write the value v of valid cell (x, y) of block X into the ghosts that copy or mirror
 // it, in `field`: the facing ghost of each neighbour (fill_ghost_copy!) and the block's
 // own mirror ghost (fill_ghost_bnd!).  fc: the block's four face records.
-template <typename T>
-__device__ __forceinline__ void push(const EngArgs<T> &A, T *field, int X, const int4 *fc, int x, int y, T v) {
-  T *xb = field + (int64_t)X * kSS;
+template <typename F>
+__device__ __forceinline__ void push_f(const Signs &sg, F *field, int X, const int4 *fc, int x, int y, F v) {
+  F *xb = field + (int64_t)X * kSS;
   if (x <= 3) {
     const int4 fi = fc[0];
     if (fi.w >= 0) field[(int64_t)fi.w * kSS + (x + kM) + kS * y] = v;
-    else if (fi.x == FACE_BOUNDARY) xb[(2 * kG - 1 - x) + kS * y] = dmul<T>(T(A.sg.v[3]), v);
+    else if (fi.x == FACE_BOUNDARY) xb[(2 * kG - 1 - x) + kS * y] = dmul<F>(F(sg.v[3]), v);
   }
   if (x >= 16) {
     const int4 fi = fc[1];
     if (fi.w >= 0) field[(int64_t)fi.w * kSS + (x - kM) + kS * y] = v;
-    else if (fi.x == FACE_BOUNDARY) xb[(2 * (kG + kM) - 1 - x) + kS * y] = dmul<T>(T(A.sg.v[5]), v);
+    else if (fi.x == FACE_BOUNDARY) xb[(2 * (kG + kM) - 1 - x) + kS * y] = dmul<F>(F(sg.v[5]), v);
   }
   if (y <= 3) {
     const int4 fi = fc[2];
     if (fi.w >= 0) field[(int64_t)fi.w * kSS + x + kS * (y + kM)] = v;
-    else if (fi.x == FACE_BOUNDARY) xb[x + kS * (2 * kG - 1 - y)] = dmul<T>(T(A.sg.v[1]), v);
+    else if (fi.x == FACE_BOUNDARY) xb[x + kS * (2 * kG - 1 - y)] = dmul<F>(F(sg.v[1]), v);
   }
   if (y >= 16) {
     const int4 fi = fc[3];
     if (fi.w >= 0) field[(int64_t)fi.w * kSS + x + kS * (y - kM)] = v;
-    else if (fi.x == FACE_BOUNDARY) xb[x + kS * (2 * (kG + kM) - 1 - y)] = dmul<T>(T(A.sg.v[7]), v);
+    else if (fi.x == FACE_BOUNDARY) xb[x + kS * (2 * (kG + kM) - 1 - y)] = dmul<F>(F(sg.v[7]), v);
   }
+}
+
+template <typename T>
+__device__ __forceinline__ void push(const EngArgs<T> &A, T *field, int X, const int4 *fc, int x, int y, T v) {
+  push_f<T>(A.sg, field, X, fc, x, y, v);
 }
 
 // Ghost cell `lane` (0..31) of face f: layer lane/16, position lane%16.
@@ -327,21 +356,26 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
       S.recs[q][k] = recs[5 * (first + (c0 + q) * step) + k];
     }
     slot_sync(slot);
-    if (t == 0) issue_tile<T>(S, pk & 1, src, S.recs[0][0].x);
+    if (t == 0) {
+      issue_tile<T>(S, pk % kBuf, src, S.recs[0][0].x);
+      if (cn > 1) issue_tile<T>(S, (pk + 1) % kBuf, src, S.recs[1][0].x);
+    }
     prefetch(0);
     for (int j = 0; j < cn; ++j) {
       const unsigned kb = pk + j;
-      const int buf = kb & 1;
+      const int buf = kb % kBuf;
       const int4 bk = S.recs[j][0];
       const int4 *fc = &S.recs[j][1];
       const int X = bk.x;
-      if (t == 0 && j + 1 < cn) issue_tile<T>(S, (kb + 1) & 1, src, S.recs[j + 1][0].x);
+      // two blocks ahead: the buffer of block j - 1, free since the end of its item
+      if (t == 0 && j + 2 < cn) issue_tile<T>(S, (kb + 2) % kBuf, src, S.recs[j + 2][0].x);
       T bx = b_nx;
       const T ex = e_nx, hv = hv_nx, hc = hc_nx;
       if (j + 1 < cn) prefetch(j + 1);
-      if (!mbar_wait(&S.bar[buf], (kb >> 1) & 1, A.err, A.timeout_ns)) {
-        // leave no copy in flight: wait (bounded) for the one issued for item j + 1
-        if (j + 1 < cn) mbar_wait(&S.bar[(kb + 1) & 1], ((kb + 1) >> 1) & 1, A.err, A.timeout_ns);
+      if (!mbar_wait(&S.bar[buf], (kb / kBuf) & 1, A.err, A.timeout_ns)) {
+        // leave no copy in flight: wait (bounded) for those issued for the next items
+        for (int q = 1; q <= 2 && j + q < cn; ++q)
+          mbar_wait(&S.bar[(kb + q) % kBuf], ((kb + q) / kBuf) & 1, A.err, A.timeout_ns);
         return false;
       }
       T *tile = S.tile[buf];
@@ -395,7 +429,7 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
         push<T>(A, A.e, X, fc, x, y, ev);
         if (t < 128) refbnd_ghost<T>(A.e, esrc, X, fc, t);
       }
-      slot_sync(slot);  // the buffer is refilled two items later
+      slot_sync(slot);  // the buffer is refilled three items later
     }
     pk += cn;
   }
@@ -474,6 +508,142 @@ __device__ void ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int f
   }
 }
 
+// ---- mixed-precision outer step (FP64) ---------------------------------------------
+
+// u64 += u (FP32 correction) on every valid cell of every level, with pushes of the new
+// values into the copy and mirror ghosts of u64.
+template <typename T>
+__device__ void ph_update64(const EngArgs<T> &A, int t, int gslot, int gstep) {
+  const int x = 2 + (t & 15), y = 2 + (t >> 4), o = x + kS * y;
+  int base = 0;
+  for (int l = 1; l <= A.lmax; ++l) {
+    const int n = A.tr.nblk[l - 1];
+    const int4 *blocks = A.tr.lvl_blocks[l - 1];
+    // items are numbered across levels so that the work spreads over every slot
+    for (int i = (gslot - base % gstep + gstep) % gstep; i < n; i += gstep) {
+      const int X = blocks[i].x;
+      double *d = A.mx.u64 + (int64_t)X * kSS + o;
+      const double nv = *d + (double)A.u[(int64_t)X * kSS + o];
+      *d = nv;
+      push_f<double>(A.sg, A.mx.u64, X, A.tr.faces + 4 * X, x, y, nv);
+    }
+    base += n;
+  }
+}
+
+// Restriction of u64 from level l onto the covered subblocks of level l - 1, with pushes.
+template <typename T>
+__device__ void ph_restrict64(const EngArgs<T> &A, int l, int t, int gslot, int gstep) {
+  const int n = A.tr.nch[l - 1];
+  const int4 *ch = A.tr.lvl_child[l - 1];
+  if (t >= 64) return;
+  const int kx = t & 7, ky = t >> 3;
+  for (int i = gslot; i < n; i += gstep) {
+    const int4 e = ch[i];
+    const double v = restrict4<double>(A.mx.u64 + (int64_t)e.x * kSS, 2 + 2 * kx, 2 + 2 * ky);
+    const int cx = 2 + 8 * (e.z - 1) + kx, cy = 2 + 8 * (e.w - 1) + ky;
+    A.mx.u64[(int64_t)e.y * kSS + cx + kS * cy] = v;
+    push_f<double>(A.sg, A.mx.u64, e.y, A.tr.faces + 4 * e.y, cx, cy, v);
+  }
+}
+
+// Refinement-boundary ghosts of u64 on level l from level l - 1.
+template <typename T>
+__device__ void ph_refbnd64(const EngArgs<T> &A, int l, int t, int gslot, int gstep) {
+  const int n = A.tr.nblk[l - 1];
+  const int4 *blocks = A.tr.lvl_blocks[l - 1];
+  if (t >= 128) return;
+  for (int i = gslot; i < n; i += gstep) {
+    const int X = blocks[i].x;
+    refbnd_ghost<double>(A.mx.u64, A.mx.u64, X, A.tr.faces + 4 * X, t);
+  }
+}
+
+// FP64 defect r = -(b + L u64 / s_l) on every valid cell of every level, written as the
+// FP32 right-hand side -r; the FP32 correction is zeroed (ghosts included) and the leaf
+// cells' weighted squares r^2 4^-(l-1) are summed per CTA (fixed order).
+template <typename T>
+__device__ double ph_defect(const EngArgs<T> &A, int t, int gslot, int gstep) {
+  const int x = 2 + (t & 15), y = 2 + (t >> 4), o = x + kS * y;
+  const int mysub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
+  double acc = 0.0;
+  int base = 0;
+  for (int l = 1; l <= A.lmax; ++l) {
+    const int n = A.tr.nblk[l - 1];
+    const int4 *blocks = A.tr.lvl_blocks[l - 1];
+    const double s = A.mx.lev_s64[l], centre = A.mx.lev_centre64[l];
+    const double wl = 1.0 / (double)((int64_t)1 << (2 * (l - 1)));
+    double accl = 0.0;
+    for (int i = (gslot - base % gstep + gstep) % gstep; i < n; i += gstep) {
+      const int4 bk = blocks[i];
+      const int X = bk.x;
+      const W5<double> w = weights<double>(A.mx.wt64, A.geom, bk.y, bk.z, x, y);
+      const double Lu = apply5<double>(A.mx.u64 + (int64_t)X * kSS, x, y, w, centre);
+      const double r = -(A.mx.b64[(int64_t)X * kSS + o] + Lu / s);
+      A.b[(int64_t)X * kSS + o] = (T)(-r);
+      T *eb = A.u + (int64_t)X * kSS;
+      eb[t] = T(0);
+      if (t < kSS - 256) eb[t + 256] = T(0);
+      if (!((bk.w >> mysub) & 1)) accl = fma(r, r, accl);
+    }
+    acc = fma(accl, wl, acc);
+    base += n;
+  }
+  return acc;
+}
+
+// Coarsest level solved directly (mixed-precision solve): FAS right-hand side of the
+// covered cells, then u_1 = P b_1 with P = -s A_1^{-1} applied in FP64, ghosts pushed,
+// and the correction e = u_1 - u1 of the level.  CTA 0 only; level 1 has <= 4 blocks.
+template <typename T>
+__device__ void ph_direct_top(const EngArgs<T> &A, T *u, bool make_e, int t, int slot, double *sol) {
+  const int n1 = A.tr.nblk[0];
+  const int4 *blocks = A.tr.lvl_blocks[0];
+  const int x = 2 + (t & 15), y = 2 + (t >> 4);
+  const int o = x + kS * y;
+  const int mysub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
+  const T s = A.lev_s[1], centre = A.lev_centre[1];
+  if (slot < n1) {
+    const int4 bk = blocks[slot];
+    const int X = bk.x;
+    const T uo = u[(int64_t)X * kSS + o];
+    A.u1[(int64_t)X * kSS + o] = uo;
+    if ((bk.w >> mysub) & 1) {
+      const W5<T> w = weights<T>(A.wt, A.geom, bk.y, bk.z, x, y);
+      const T Lu = apply5<T>(u + (int64_t)X * kSS, x, y, w, centre);
+      A.b[(int64_t)X * kSS + o] = -(A.e[(int64_t)X * kSS + o] + Lu / s);
+    }
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int n = A.coarse_n;
+  for (int q = warp; q < n; q += nw) {
+    const double *pr = A.coarse_P + (int64_t)q * n;
+    double acc = 0.0;
+    for (int j = lane; j < n; j += 32) {
+      const int c = j & 255;
+      const int X = blocks[j >> 8].x;
+      acc = fma(pr[j], (double)A.b[(int64_t)X * kSS + (2 + (c & 15)) + kS * (2 + (c >> 4))], acc);
+    }
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (lane == 0) sol[q] = acc;
+  }
+  __syncthreads();
+  if (slot < n1) {
+    const int4 bk = blocks[slot];
+    const int X = bk.x;
+    const int4 *fc = A.tr.faces + 4 * X;
+    const T nu = (T)sol[slot * 256 + (t & 255)];
+    u[(int64_t)X * kSS + o] = nu;
+    push<T>(A, u, X, fc, x, y, nu);
+    if (make_e) {
+      const T ev = nu - A.u1[(int64_t)X * kSS + o];
+      A.e[(int64_t)X * kSS + o] = ev;
+      push<T>(A, A.e, X, fc, x, y, ev);
+    }
+  }
+}
+
 // Copy level l's blocks (valid cells and face ghosts) from src to dst.
 template <typename T>
 __device__ void ph_copy_back(const EngArgs<T> &A, int l, const T *src, T *dst, int first, int step, int t) {
@@ -492,15 +662,20 @@ __device__ void ph_copy_back(const EngArgs<T> &A, int l, const T *src, T *dst, i
 // ------------------------------------------------------------------ the kernel
 
 template <typename T>
+constexpr size_t engine_smem_bytes() {
+  return 4 * sizeof(SlotSmem<T>);
+}
+
+template <typename T>
 __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant__ EngArgs<T> A) {
-  __shared__ __align__(128) SlotSmem<T> smem[4];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  SlotSmem<T> *smem = reinterpret_cast<SlotSmem<T> *>(smem_raw);
   const int nslots = blockDim.x >> 8;
   const int slot = threadIdx.x >> 8, t = threadIdx.x & 255;
   const bool cta0 = blockIdx.x == 0;
   SlotSmem<T> &S = smem[slot];
   if (t == 0) {
-    mbar_init(&S.bar[0]);
-    mbar_init(&S.bar[1]);
+    for (int q = 0; q < kBuf; ++q) mbar_init(&S.bar[q]);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
@@ -512,6 +687,7 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
   auto fld = [&](int l) -> T * { return ((cur >> l) & 1) ? A.ualt : A.u; };
   auto oth = [&](int l) -> T * { return ((cur >> l) & 1) ? A.u : A.ualt; };
   T *scratch = &S.tile[0][0];  // restriction phase staging (no bulk copies in flight then)
+  __shared__ double s_direct[1024];  // coarsest-level direct solution (CTA 0)
 
   auto first_of = [&](bool loc) { return loc ? slot : blockIdx.x * nslots + slot; };
   auto step_of = [&](bool loc) { return loc ? nslots : gridDim.x * nslots; };
@@ -535,6 +711,67 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
   auto runs = [&](bool loc) { return !loc || cta0; };
   stamp();
 
+  if (A.mx.u64) {
+    const int gslot = blockIdx.x * nslots + slot, gstep = gridDim.x * nslots;
+    if (A.mx.apply_update) {
+      ph_update64<T>(A, t, gslot, gstep);
+      if (!sync(true, false, false)) return;
+    }
+    for (int l = L; l >= 2; --l) {
+      ph_restrict64<T>(A, l, t, gslot, gstep);
+      if (!sync(true, false, false)) return;
+    }
+    for (int l = 2; l <= L; ++l)
+      if ((A.mx.refbnd_levels >> l) & 1) {
+        ph_refbnd64<T>(A, l, t, gslot, gstep);
+        if (!sync(true, false, false)) return;
+      }
+    const double part = ph_defect<T>(A, t, gslot, gstep);
+    // fixed-order reduction: warps, then slots, then CTAs (every CTA sums all partials)
+    {
+      double v = part;
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      if ((threadIdx.x & 31) == 0) s_direct[threadIdx.x >> 5] = v;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double c = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) c += s_direct[w];
+        A.mx.part[blockIdx.x] = c;
+      }
+    }
+    if (!sync(true, false, false)) return;
+    __shared__ int s_conv;
+    if (threadIdx.x == 0) {
+      double tot = 0.0;
+      for (int c = 0; c < (int)gridDim.x; ++c) tot += *((volatile double *)A.mx.part + c);
+      const double nrm = sqrt(tot);
+      s_conv = !(nrm > A.mx.tol_abs);
+      if (cta0) {
+        A.mx.out[0] = nrm;
+        A.mx.out[1] = s_conv ? 1.0 : 0.0;
+      }
+    }
+    __syncthreads();
+    if (s_conv) return;
+  }
+
+  if (A.smooth_level > 0) {
+    // gauss_seidel_iter! (src/multigrid.jl:250-265) on one level
+    const int l = A.smooth_level;
+    for (int it = 0; it < A.smooth_n; ++it) {
+      const bool ok = ph_gsi<T>(A, l, fld(l), oth(l), nullptr, false, false, false, first_of(false),
+                                step_of(false), t, slot, S, pk);
+      cur ^= 1u << l;
+      if (!sync(ok, false, false)) return;
+    }
+    if ((cur >> l) & 1) {
+      ph_copy_back<T>(A, l, A.ualt, A.u, first_of(false), step_of(false), t);
+      grid_barrier(A.bar, A.err, epoch, A.timeout_ns);
+    }
+    if (A.trace && cta0 && threadIdx.x == 0 && ntrace < kTraceMax) A.trace[ntrace] = 0;
+    return;
+  }
+
   // descending leg
   for (int l = L; l >= 2; --l) {
     const bool loc = l <= K;
@@ -550,7 +787,10 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
     if (!sync(true, loc, (l - 1) <= K)) return;
   }
   // coarsest level
-  {
+  if (A.coarse_P) {
+    if (cta0) ph_direct_top<T>(A, fld(1), L > 1, t, slot, s_direct);
+    if (!sync(true, 1 <= K, 2 <= K || L < 2)) return;
+  } else {
     const bool loc = 1 <= K;
     for (int it = 0; it < A.ntop; ++it) {
       const bool last = it == A.ntop - 1;

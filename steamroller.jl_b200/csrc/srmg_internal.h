@@ -33,10 +33,21 @@ int leafnorm_dev(srmg_ctx *ctx, const T *u, const T *b, double s, int op, double
 int read_small(srmg_ctx *ctx, int n);
 
 int engine_local_top(srmg_ctx *ctx, int lmax);
+// FP64 side of one mixed-precision defect-correction step run by the engine launch.
+struct MixedStep {
+  double *u64;
+  const double *b64;
+  double tol_abs;
+  int apply_update;
+};
 template <typename T>
 int engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, double s, int op, double k2, int geom,
-                  const Signs &sg, int lmax, int ndown, int ntop, int nup, double omega);
+                  const Signs &sg, int lmax, int ndown, int ntop, int nup, double omega,
+                  const double *coarse_P = nullptr, int coarse_n = 0, const MixedStep *mixed = nullptr);
 int engine_check(srmg_ctx *ctx);
+template <typename T>
+int engine_smooth(srmg_ctx *ctx, T *u, const T *b, int level, double omega, double sl, int n, int op,
+                  double k2, int geom, const Signs &sg);
 int stage_in(srmg_ctx *ctx, int slot, const double *h, int64_t nblk_alloc, double **d);
 int stage_out(srmg_ctx *ctx, double *h, const double *d, int64_t nblk_alloc);
 

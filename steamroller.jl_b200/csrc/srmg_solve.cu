@@ -212,7 +212,8 @@ int prepare_coarse(srmg_ctx *ctx, double s, int op, double k2, int geom, const i
   return SRMG_OK;
 }
 
-// FP32 V-cycle with the FP64 direct coarsest-level solve (when available).  Same
+// FP32 V-cycle with the FP64 direct coarsest-level solve (when available), on the
+// per-operation kernels (used when the persistent engine is switched off).  Same
 // structure as the reference V-cycle; only the top changes.
 int vcycle_mixed(srmg_ctx *ctx, float *e, float *b, float *r, float *u1, double s, int op, double k2,
                  int geom, const Signs &sg, int ndown, int ntop, int nup, double omega) {
@@ -343,6 +344,46 @@ static int solve_fp64(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_al
   return SRMG_OK;
 }
 
+// One persistent launch per defect-correction step: the FP64 update, composite
+// consistency, defect and norm, then (if the norm is above tol) the FP32 V-cycle with
+// its FP64 direct coarsest-level solve.
+static int solve_mixed_engine(srmg_ctx *ctx, double *u, const double *b, double s, int op, double k2,
+                              int geom, const int8_t *bc, const srmg_solve_opts *o, srmg_stats *st,
+                              float *e, float *be, float *r, float *u1, double bn) {
+  const Signs sg = make_signs(bc);
+  MixedStep ms;
+  ms.u64 = u;
+  ms.b64 = b;
+  ms.tol_abs = o->tol * bn;
+  int outer = 0, cycles = 0;
+  double prev = 0;
+  for (int step = 0;; step++) {
+    ms.apply_update = step > 0;
+    RC(engine_vcycle<float>(ctx, e, be, u1, r, s, op, k2, geom, sg, 0, o->ndown, o->ntop, o->nup, o->omega,
+                            ctx->coarse_ok ? (const double *)ctx->coarse_inv.p : nullptr,
+                            ctx->coarse_ok ? ctx->coarse_n : 0, &ms));
+    RC(read_small(ctx, 6));
+    const double nrm = ctx->h_small[4];
+    const bool conv = ctx->h_small[5] != 0.0;
+    const double rel = nrm / bn;
+    if (step == 0) st->initial_rel = rel;
+    st->rel_residual = rel;
+    if (!std::isfinite(rel) || (step > 3 && rel > 10 * prev && rel > st->initial_rel)) {
+      st->cycles = cycles;
+      st->outer = outer;
+      return fail(ctx, SRMG_ERR_DIVERGED, "mixed solve diverged after %d steps", outer);
+    }
+    prev = rel;
+    if (conv) break;
+    cycles++;
+    outer++;
+    if (outer > o->max_cycles) break;
+  }
+  st->cycles = cycles;
+  st->outer = outer;
+  return SRMG_OK;
+}
+
 static int solve_mixed(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, double s, int op,
                        double k2, int geom, const int8_t *bc, const srmg_solve_opts *o,
                        srmg_stats *st) {
@@ -355,6 +396,14 @@ static int solve_mixed(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_a
   CK(cudaMemsetAsync(u1, 0, b32, ctx->stream));
   RC(prepare_coarse(ctx, s, op, k2, geom, bc));
   RC(leafnorm_dev<double>(ctx, u, b, s, op, k2, geom, 1, 1));
+  const bool aligned = ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(b)) & 15) == 0;
+  if (ctx->use_engine && aligned && o->ndown >= 1 && o->nup >= 1 && o->ntop >= 1 && ctx->nlev <= 30) {
+    RC(read_small(ctx, 2));
+    const double bn = ctx->h_small[1] > 0 ? ctx->h_small[1] : 1.0;
+    st->bnorm = ctx->h_small[1];
+    return solve_mixed_engine(ctx, u, b, s, op, k2, geom, bc, o, st, e, be, r, u1, bn);
+  }
+  // per-operation kernels
   RC(make_consistent(ctx, u, sg));
   RC(defect_all(ctx, be, e, u, b, s, op, k2, geom, 0));
   RC(read_small(ctx, 2));

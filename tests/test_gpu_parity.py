@@ -158,6 +158,30 @@ def test_gs_colour_sweep(pair, parity):
     assert rel_l2(got, uo) < REL_SWEEP
 
 
+@pytest.mark.parametrize("n", [1, 2, 3])
+def test_gs_iter_matches_oracle(pair, n):
+    """gauss_seidel_iter! (red, copy+mirror fills, black, fills) n times on one level."""
+    import ctypes
+    p = pair.p
+    u0, b0 = random_field(p, 14), random_field(p, 15)
+    l = len(p.tree)
+    while l > 1 and len(p.tree[l - 1]) == 0:
+        l -= 1
+    uo = u0.copy()
+    pair.orc.fill_ghost(uo, l)
+    ug, bg = torch_cuda(uo), torch_cuda(b0)
+    bca = np.ascontiguousarray(p.bc, dtype=np.int8)
+    pair.ctx.check(mg.lib().srmg_gs_iter_dev(pair.ctx.handle, ug.data_ptr(), bg.data_ptr(), p.nblk, l, 1.0,
+                                             0.3, n, p.op, p.k2, p.geom, bca.ctypes.data))
+    pair.ctx.synchronize()
+    olib().orc_gs_iter(_ptr(uo), _ptr(b0), 1.0, 0.3, n, l, pair.orc.ot.ref, ctypes.byref(pair.orc.op))
+    got = to_np(ug)
+    assert rel_l2(got, uo) < 1e-13
+    corner = np.zeros((20, 20), dtype=bool)
+    corner[:2, :2] = corner[:2, 18:] = corner[18:, :2] = corner[18:, 18:] = True
+    assert np.array_equal(got[:, corner], uo[:, corner])  # corner ghosts never written
+
+
 def test_residual_level(pair):
     import ctypes
     p = pair.p
@@ -319,9 +343,13 @@ def test_fp64_solve_to_tolerance():
         assert rel_l2(to_np(ug), uo, valid_mask(u.shape)) <= REL_VCYCLE
 
 
-def test_mixed_solve_reaches_fp64_solution():
+@pytest.mark.parametrize("engine", [1, 0])
+def test_mixed_solve_reaches_fp64_solution(engine):
+    """Mixed precision (FP32 V-cycles, FP64 defect correction, FP64 direct coarsest
+    level) reaches the FP64 solution: persistent launch per step, or per-operation kernels."""
     p = PROBS["refined"]
     pr = Pair(p)
+    pr.ctx.set_option("engine", engine)
     u, b = _prepared(pr)
     ug = torch_cuda(u)
     st = mg.solve(pr.ctx, ug, torch_cuda(b), p.s, p.geom, p.bc, tol=1e-8, mode=mg.MODE_MIXED,
