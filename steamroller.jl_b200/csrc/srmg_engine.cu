@@ -55,7 +55,9 @@ int srmg::engine_local_top(srmg_ctx *ctx, int lmax) {
 template <typename T>
 int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, double s, int op, double k2, int geom,
                         const Signs &sg, int lmax, int ndown, int ntop, int nup, double omega,
-                        const double *coarse_P, int coarse_n, const MixedStep *mixed) {
+                        const EngineRun *run) {
+  const EngineRun none;
+  if (!run) run = &none;
   if (ctx->nlev > kMaxLev) return fail(ctx, SRMG_ERR_UNSUPPORTED, "engine supports at most %d levels", kMaxLev);
   if (lmax == 0) lmax = ctx->nlev;
   int L = 0;
@@ -92,9 +94,9 @@ int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, double s, int op
   A.ntop = ntop;
   A.nup = nup;
   A.local_top = engine_local_top(ctx, L);
-  if (coarse_P && coarse_n == 256 * ctx->nblk_host[0] && ctx->nblk_host[0] <= 4) {
-    A.coarse_P = coarse_P;
-    A.coarse_n = coarse_n;
+  if (run->coarse_P && run->coarse_n == 256 * ctx->nblk_host[0] && ctx->nblk_host[0] <= 4) {
+    A.coarse_P = run->coarse_P;
+    A.coarse_n = run->coarse_n;
   }
   for (int l = 1; l <= L; l++) {
     const OpParams<T> p = op_params<T>(op, geom, k2, level_scale(s, l), omega);
@@ -106,9 +108,14 @@ int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, double s, int op
   A.bar = (unsigned *)ctx->sync.p;
   A.err = (int *)((char *)ctx->sync.p + 128);
   A.timeout_ns = 2000000000LL;  // 2 s per barrier wait
-  if (mixed) {
-    A.mx.u64 = mixed->u64;
-    A.mx.b64 = mixed->b64;
+  RC(ensure(ctx, ctx->part, sizeof(double) * 4096));
+  A.part = (double *)ctx->part.p;
+  A.out = (double *)ctx->small.p + 8;
+  A.max_cycles = run->max_cycles;
+  A.tol_abs = run->tol_abs;
+  if (run->u64) {
+    A.mx.u64 = run->u64;
+    A.mx.b64 = run->b64;
     A.mx.wt64 = WTab<double>{ctx->d_wm64, ctx->d_wp64};
     for (int l = 1; l <= L; l++) {
       const OpParams<double> p = op_params<double>(op, geom, k2, level_scale(s, l), omega);
@@ -116,11 +123,7 @@ int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, double s, int op
       A.mx.lev_centre64[l] = p.centre;
     }
     A.mx.refbnd_levels = ctx->refbnd_levels;
-    A.mx.tol_abs = mixed->tol_abs;
-    A.mx.apply_update = mixed->apply_update;
-    RC(ensure(ctx, ctx->part, sizeof(double) * 4096));
-    A.mx.part = (double *)ctx->part.p;
-    A.mx.out = (double *)ctx->small.p + 4;
+    A.mx.apply_update = run->apply_update;
   }
   if (ctx->trace_on) {
     RC(ensure(ctx, ctx->trace, kTraceMax * sizeof(long long)));
@@ -195,10 +198,10 @@ template int srmg::engine_smooth<double>(srmg_ctx *, double *, const double *, i
 
 template int srmg::engine_vcycle<double>(srmg_ctx *, double *, double *, double *, double *, double, int,
                                          double, int, const Signs &, int, int, int, int, double,
-                                         const double *, int, const MixedStep *);
+                                         const EngineRun *);
 template int srmg::engine_vcycle<float>(srmg_ctx *, float *, float *, float *, float *, double, int,
                                         double, int, const Signs &, int, int, int, int, double,
-                                        const double *, int, const MixedStep *);
+                                        const EngineRun *);
 
 extern "C" int srmg_get_trace(srmg_ctx *ctx, int64_t *out, int max_entries) {
   if (!ctx || !out || max_entries < 0) return SRMG_ERR_BADARG;

@@ -62,10 +62,7 @@ struct MixedArgs {
   double lev_s64[kMaxLev + 1];
   double lev_centre64[kMaxLev + 1];
   unsigned refbnd_levels;  // bit l: level l has refinement-boundary faces
-  double tol_abs;
-  int apply_update;
-  double *part;            // one partial per CTA
-  double *out;             // out[0] = defect leaf norm, out[1] = 1 if converged
+  int apply_update;        // apply the correction left by a previous launch first
 };
 
 template <typename T>
@@ -90,6 +87,13 @@ struct EngArgs {
   const double *coarse_P;  // optional: the coarsest level is solved directly, u1 = P b1
   int coarse_n;            // unknowns of the coarsest level (256 per block, <= 1024)
   MixedArgs mx;            // mixed-precision outer step (mx.u64 != nullptr)
+  // Device-side solve loop: with max_cycles > 0 the launch repeats V-cycles until the
+  // leaf norm of the residual (FP64 mode) or of the FP64 defect (mixed mode) is
+  // <= tol_abs or max_cycles V-cycles have run.
+  int max_cycles;
+  double tol_abs;
+  double *part;            // one partial sum per CTA
+  double *out;             // out[0] final norm, [1] converged, [2] V-cycles run, [3] initial norm
 };
 
 // ------------------------------------------------------------------ barriers
@@ -592,6 +596,35 @@ __device__ double ph_defect(const EngArgs<T> &A, int t, int gslot, int gstep) {
   return acc;
 }
 
+// Leaf-cell weighted sum of r^2, r = -(b + L u / s_l), over every level (the resnorm!
+// norm, src/multigrid.jl:391-417), per slot in a fixed order.
+template <typename T>
+__device__ double ph_resnorm(const EngArgs<T> &A, int t, int gslot, int gstep) {
+  const int x = 2 + (t & 15), y = 2 + (t >> 4), o = x + kS * y;
+  const int mysub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
+  double acc = 0.0;
+  int base = 0;
+  for (int l = 1; l <= A.lmax; ++l) {
+    const int n = A.tr.nblk[l - 1];
+    const int4 *blocks = A.tr.lvl_blocks[l - 1];
+    const T s = A.lev_s[l], centre = A.lev_centre[l];
+    const double wl = 1.0 / (double)((int64_t)1 << (2 * (l - 1)));
+    double accl = 0.0;
+    for (int i = (gslot - base % gstep + gstep) % gstep; i < n; i += gstep) {
+      const int4 bk = blocks[i];
+      if ((bk.w >> mysub) & 1) continue;
+      const int X = bk.x;
+      const W5<T> w = weights<T>(A.wt, A.geom, bk.y, bk.z, x, y);
+      const T Lu = apply5<T>(A.u + (int64_t)X * kSS, x, y, w, centre);
+      const double r = (double)(-(A.b[(int64_t)X * kSS + o] + Lu / s));
+      accl = fma(r, r, accl);
+    }
+    acc = fma(accl, wl, acc);
+    base += n;
+  }
+  return acc;
+}
+
 // Coarsest level solved directly (mixed-precision solve): FAS right-hand side of the
 // covered cells, then u_1 = P b_1 with P = -s A_1^{-1} applied in FP64, ghosts pushed,
 // and the correction e = u_1 - u1 of the level.  CTA 0 only; level 1 has <= 4 blocks.
@@ -711,50 +744,6 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
   auto runs = [&](bool loc) { return !loc || cta0; };
   stamp();
 
-  if (A.mx.u64) {
-    const int gslot = blockIdx.x * nslots + slot, gstep = gridDim.x * nslots;
-    if (A.mx.apply_update) {
-      ph_update64<T>(A, t, gslot, gstep);
-      if (!sync(true, false, false)) return;
-    }
-    for (int l = L; l >= 2; --l) {
-      ph_restrict64<T>(A, l, t, gslot, gstep);
-      if (!sync(true, false, false)) return;
-    }
-    for (int l = 2; l <= L; ++l)
-      if ((A.mx.refbnd_levels >> l) & 1) {
-        ph_refbnd64<T>(A, l, t, gslot, gstep);
-        if (!sync(true, false, false)) return;
-      }
-    const double part = ph_defect<T>(A, t, gslot, gstep);
-    // fixed-order reduction: warps, then slots, then CTAs (every CTA sums all partials)
-    {
-      double v = part;
-      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-      if ((threadIdx.x & 31) == 0) s_direct[threadIdx.x >> 5] = v;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double c = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) c += s_direct[w];
-        A.mx.part[blockIdx.x] = c;
-      }
-    }
-    if (!sync(true, false, false)) return;
-    __shared__ int s_conv;
-    if (threadIdx.x == 0) {
-      double tot = 0.0;
-      for (int c = 0; c < (int)gridDim.x; ++c) tot += *((volatile double *)A.mx.part + c);
-      const double nrm = sqrt(tot);
-      s_conv = !(nrm > A.mx.tol_abs);
-      if (cta0) {
-        A.mx.out[0] = nrm;
-        A.mx.out[1] = s_conv ? 1.0 : 0.0;
-      }
-    }
-    __syncthreads();
-    if (s_conv) return;
-  }
-
   if (A.smooth_level > 0) {
     // gauss_seidel_iter! (src/multigrid.jl:250-265) on one level
     const int l = A.smooth_level;
@@ -772,60 +761,142 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
     return;
   }
 
-  // descending leg
-  for (int l = L; l >= 2; --l) {
-    const bool loc = l <= K;
-    for (int it = 0; it < A.ndown; ++it) {
-      bool ok = true;
-      if (runs(loc))
-        ok = ph_gsi<T>(A, l, fld(l), oth(l), nullptr, it == 0 && l < L, false, it == 0 && l < L, first_of(loc),
-                       step_of(loc), t, slot, S, pk);
-      cur ^= 1u << l;
-      if (!sync(ok, loc, loc)) return;
+  const int gslot = blockIdx.x * nslots + slot, gstep = gridDim.x * nslots;
+  // Fixed-order grid reduction (warps, CTA, then every CTA sums all CTA partials in the
+  // same order), so every CTA takes the same decision from the same norm.
+  __shared__ double s_nrm;
+  auto grid_norm = [&](double part, bool &ok) -> double {
+    double v = part;
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0) s_direct[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double c = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) c += s_direct[w];
+      A.part[blockIdx.x] = c;
     }
-    if (runs(loc)) ph_restrict<T>(A, l, fld(l), fld(l - 1), first_of(loc), step_of(loc), t, slot, scratch);
-    if (!sync(true, loc, (l - 1) <= K)) return;
+    ok = sync(true, false, false);
+    if (threadIdx.x == 0) {
+      double tot = 0.0;
+      for (int c = 0; c < (int)gridDim.x; ++c) tot += *((volatile double *)A.part + c);
+      s_nrm = sqrt(tot);
+    }
+    __syncthreads();
+    return s_nrm;
+  };
+
+  // One FAS V-cycle (src/multigrid.jl:60-106) on the current fields.
+  auto vcycle_body = [&]() -> bool {
+    cur = 0;
+    // descending leg
+    for (int l = L; l >= 2; --l) {
+      const bool loc = l <= K;
+      for (int it = 0; it < A.ndown; ++it) {
+        bool ok = true;
+        if (runs(loc))
+          ok = ph_gsi<T>(A, l, fld(l), oth(l), nullptr, it == 0 && l < L, false, it == 0 && l < L, first_of(loc),
+                         step_of(loc), t, slot, S, pk);
+        cur ^= 1u << l;
+        if (!sync(ok, loc, loc)) return false;
+      }
+      if (runs(loc)) ph_restrict<T>(A, l, fld(l), fld(l - 1), first_of(loc), step_of(loc), t, slot, scratch);
+      if (!sync(true, loc, (l - 1) <= K)) return false;
+    }
+    // coarsest level
+    if (A.coarse_P) {
+      if (cta0) ph_direct_top<T>(A, fld(1), L > 1, t, slot, s_direct);
+      if (!sync(true, 1 <= K, 2 <= K || L < 2)) return false;
+    } else {
+      const bool loc = 1 <= K;
+      for (int it = 0; it < A.ntop; ++it) {
+        const bool last = it == A.ntop - 1;
+        bool ok = true;
+        if (runs(loc))
+          ok = ph_gsi<T>(A, 1, fld(1), oth(1), nullptr, it == 0 && L > 1, last && L > 1, it == 0 && L > 1,
+                         first_of(loc), step_of(loc), t, slot, S, pk);
+        cur ^= 1u << 1;
+        if (!sync(ok, loc, last ? (2 <= K || L < 2) : loc)) return false;
+      }
+    }
+    // ascending leg
+    for (int l = 2; l <= L; ++l) {
+      const bool loc = l <= K;
+      if (runs(loc)) ph_prolong<T>(A, l, fld(l), fld(l - 1), first_of(loc), step_of(loc), t);
+      if (!sync(true, loc, loc)) return false;
+      for (int it = 0; it < A.nup; ++it) {
+        const bool last = it == A.nup - 1;
+        bool ok = true;
+        if (runs(loc))
+          ok = ph_gsi<T>(A, l, fld(l), oth(l), A.e, false, last && l < L, false, first_of(loc), step_of(loc), t,
+                         slot, S, pk);
+        cur ^= 1u << l;
+        const bool next_loc = last ? ((l + 1) <= K) : loc;
+        if (!sync(ok, loc, l == L && last ? false : next_loc)) return false;
+      }
+    }
+
+    // levels left in the second buffer go back to u
+    bool any = false;
+    for (int l = 1; l <= L; ++l)
+      if ((cur >> l) & 1) {
+        ph_copy_back<T>(A, l, A.ualt, A.u, blockIdx.x * nslots + slot, gridDim.x * nslots, t);
+        any = true;
+      }
+    if (any && !grid_barrier(A.bar, A.err, epoch, A.timeout_ns)) return false;
+    return true;
+
+  };
+
+  const bool mixed = A.mx.u64 != nullptr;
+  const bool loop = A.max_cycles > 0;
+  int cycles = 0;
+  double nrm = -1.0, nrm0 = -1.0;
+  bool conv = false;
+  if (!mixed && loop) {
+    bool ok;
+    nrm = nrm0 = grid_norm(ph_resnorm<T>(A, t, gslot, gstep), ok);
+    if (!ok) return;
+    conv = !(nrm > A.tol_abs);
   }
-  // coarsest level
-  if (A.coarse_P) {
-    if (cta0) ph_direct_top<T>(A, fld(1), L > 1, t, slot, s_direct);
-    if (!sync(true, 1 <= K, 2 <= K || L < 2)) return;
-  } else {
-    const bool loc = 1 <= K;
-    for (int it = 0; it < A.ntop; ++it) {
-      const bool last = it == A.ntop - 1;
-      bool ok = true;
-      if (runs(loc))
-        ok = ph_gsi<T>(A, 1, fld(1), oth(1), nullptr, it == 0 && L > 1, last && L > 1, it == 0 && L > 1,
-                       first_of(loc), step_of(loc), t, slot, S, pk);
-      cur ^= 1u << 1;
-      if (!sync(ok, loc, last ? (2 <= K || L < 2) : loc)) return;
+  for (int iter = 0;; ++iter) {
+    if (mixed) {
+      // FP64 side of a defect-correction step
+      if (A.mx.apply_update || iter > 0) {
+        ph_update64<T>(A, t, gslot, gstep);
+        if (!sync(true, false, false)) return;
+      }
+      for (int l = L; l >= 2; --l) {
+        ph_restrict64<T>(A, l, t, gslot, gstep);
+        if (!sync(true, false, false)) return;
+      }
+      for (int l = 2; l <= L; ++l)
+        if ((A.mx.refbnd_levels >> l) & 1) {
+          ph_refbnd64<T>(A, l, t, gslot, gstep);
+          if (!sync(true, false, false)) return;
+        }
+      bool ok;
+      nrm = grid_norm(ph_defect<T>(A, t, gslot, gstep), ok);
+      if (!ok) return;
+      if (iter == 0) nrm0 = nrm;
+      conv = !(nrm > A.tol_abs);
     }
+    if (conv || (!isfinite(nrm) && nrm != -1.0) || (loop && cycles >= A.max_cycles)) break;
+    if (!vcycle_body()) return;
+    cycles++;
+    if (!mixed && loop) {
+      bool ok;
+      nrm = grid_norm(ph_resnorm<T>(A, t, gslot, gstep), ok);
+      if (!ok) return;
+      conv = !(nrm > A.tol_abs);
+    }
+    if (!loop) break;
   }
-  // ascending leg
-  for (int l = 2; l <= L; ++l) {
-    const bool loc = l <= K;
-    if (runs(loc)) ph_prolong<T>(A, l, fld(l), fld(l - 1), first_of(loc), step_of(loc), t);
-    if (!sync(true, loc, loc)) return;
-    for (int it = 0; it < A.nup; ++it) {
-      const bool last = it == A.nup - 1;
-      bool ok = true;
-      if (runs(loc))
-        ok = ph_gsi<T>(A, l, fld(l), oth(l), A.e, false, last && l < L, false, first_of(loc), step_of(loc), t,
-                       slot, S, pk);
-      cur ^= 1u << l;
-      const bool next_loc = last ? ((l + 1) <= K) : loc;
-      if (!sync(ok, loc, l == L && last ? false : next_loc)) return;
-    }
+  if (A.out && cta0 && threadIdx.x == 0) {
+    A.out[0] = nrm;
+    A.out[1] = conv ? 1.0 : 0.0;
+    A.out[2] = (double)cycles;
+    A.out[3] = nrm0;
   }
-  // levels left in the second buffer go back to u
-  bool any = false;
-  for (int l = 1; l <= L; ++l)
-    if ((cur >> l) & 1) {
-      ph_copy_back<T>(A, l, A.ualt, A.u, blockIdx.x * nslots + slot, gridDim.x * nslots, t);
-      any = true;
-    }
-  if (any) grid_barrier(A.bar, A.err, epoch, A.timeout_ns);
   if (A.trace && cta0 && threadIdx.x == 0 && ntrace < kTraceMax) A.trace[ntrace] = 0;
 }
 

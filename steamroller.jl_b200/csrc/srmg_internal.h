@@ -33,17 +33,20 @@ int leafnorm_dev(srmg_ctx *ctx, const T *u, const T *b, double s, int op, double
 int read_small(srmg_ctx *ctx, int n);
 
 int engine_local_top(srmg_ctx *ctx, int lmax);
-// FP64 side of one mixed-precision defect-correction step run by the engine launch.
-struct MixedStep {
-  double *u64;
-  const double *b64;
-  double tol_abs;
-  int apply_update;
+// Optional parts of a persistent-engine launch.
+struct EngineRun {
+  const double *coarse_P = nullptr;  // FP64 direct solve of the coarsest level
+  int coarse_n = 0;
+  double *u64 = nullptr;             // mixed precision: FP64 iterate and right-hand side
+  const double *b64 = nullptr;
+  int apply_update = 0;
+  int max_cycles = 0;                // > 0: device-side loop until the norm <= tol_abs
+  double tol_abs = 0.0;
 };
 template <typename T>
 int engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, double s, int op, double k2, int geom,
                   const Signs &sg, int lmax, int ndown, int ntop, int nup, double omega,
-                  const double *coarse_P = nullptr, int coarse_n = 0, const MixedStep *mixed = nullptr);
+                  const EngineRun *run = nullptr);
 int engine_check(srmg_ctx *ctx);
 template <typename T>
 int engine_smooth(srmg_ctx *ctx, T *u, const T *b, int level, double omega, double sl, int n, int op,

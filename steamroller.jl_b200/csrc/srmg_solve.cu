@@ -319,6 +319,27 @@ static int solve_fp64(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_al
   double *bw = (double *)ctx->f64[4].p, *r = (double *)ctx->f64[2].p, *u1 = (double *)ctx->f64[3].p;
   CK(cudaMemcpyAsync(bw, b, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
   RC(leafnorm_dev<double>(ctx, u, b, s, op, k2, geom, 1, 1));
+  const bool aligned = ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(bw) |
+                         reinterpret_cast<uintptr_t>(r) | reinterpret_cast<uintptr_t>(u1)) & 15) == 0;
+  if (ctx->use_engine && aligned && o->ndown >= 1 && o->ntop >= 1 && o->nup >= 1 && ctx->nlev <= 30) {
+    // the whole tolerance loop in one persistent launch
+    RC(read_small(ctx, 2));
+    const double bn = ctx->h_small[1] > 0 ? ctx->h_small[1] : 1.0;
+    st->bnorm = ctx->h_small[1];
+    EngineRun run;
+    run.max_cycles = std::max(1, o->max_cycles);
+    run.tol_abs = o->tol * bn;
+    RC(engine_vcycle<double>(ctx, u, bw, u1, r, s, op, k2, geom, sg, 0, o->ndown, o->ntop, o->nup, o->omega,
+                             &run));
+    RC(read_small(ctx, 12));
+    const double *out = ctx->h_small + 8;
+    st->rel_residual = out[0] / bn;
+    st->initial_rel = out[3] / bn;
+    st->cycles = (int)out[2];
+    if (!std::isfinite(st->rel_residual))
+      return fail(ctx, SRMG_ERR_DIVERGED, "residual is not finite after %d cycles", st->cycles);
+    return SRMG_OK;
+  }
   RC(leafnorm_dev<double>(ctx, u, bw, s, op, k2, geom, 0, 0));
   RC(read_small(ctx, 2));
   const double bn = ctx->h_small[1] > 0 ? ctx->h_small[1] : 1.0;
@@ -344,43 +365,32 @@ static int solve_fp64(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_al
   return SRMG_OK;
 }
 
-// One persistent launch per defect-correction step: the FP64 update, composite
-// consistency, defect and norm, then (if the norm is above tol) the FP32 V-cycle with
-// its FP64 direct coarsest-level solve.
+// The whole mixed-precision solve in one persistent launch: every defect-correction
+// step (FP64 update, composite consistency, FP64 defect and its leaf norm, FP32 V-cycle
+// with the FP64 direct coarsest-level solve) runs on the device until the defect norm
+// is <= tol * leafnorm(b).
 static int solve_mixed_engine(srmg_ctx *ctx, double *u, const double *b, double s, int op, double k2,
                               int geom, const int8_t *bc, const srmg_solve_opts *o, srmg_stats *st,
                               float *e, float *be, float *r, float *u1, double bn) {
   const Signs sg = make_signs(bc);
-  MixedStep ms;
-  ms.u64 = u;
-  ms.b64 = b;
-  ms.tol_abs = o->tol * bn;
-  int outer = 0, cycles = 0;
-  double prev = 0;
-  for (int step = 0;; step++) {
-    ms.apply_update = step > 0;
-    RC(engine_vcycle<float>(ctx, e, be, u1, r, s, op, k2, geom, sg, 0, o->ndown, o->ntop, o->nup, o->omega,
-                            ctx->coarse_ok ? (const double *)ctx->coarse_inv.p : nullptr,
-                            ctx->coarse_ok ? ctx->coarse_n : 0, &ms));
-    RC(read_small(ctx, 6));
-    const double nrm = ctx->h_small[4];
-    const bool conv = ctx->h_small[5] != 0.0;
-    const double rel = nrm / bn;
-    if (step == 0) st->initial_rel = rel;
-    st->rel_residual = rel;
-    if (!std::isfinite(rel) || (step > 3 && rel > 10 * prev && rel > st->initial_rel)) {
-      st->cycles = cycles;
-      st->outer = outer;
-      return fail(ctx, SRMG_ERR_DIVERGED, "mixed solve diverged after %d steps", outer);
-    }
-    prev = rel;
-    if (conv) break;
-    cycles++;
-    outer++;
-    if (outer > o->max_cycles) break;
-  }
-  st->cycles = cycles;
-  st->outer = outer;
+  EngineRun run;
+  run.coarse_P = ctx->coarse_ok ? (const double *)ctx->coarse_inv.p : nullptr;
+  run.coarse_n = ctx->coarse_ok ? ctx->coarse_n : 0;
+  run.u64 = u;
+  run.b64 = b;
+  run.apply_update = 0;
+  run.max_cycles = std::max(1, o->max_cycles);
+  run.tol_abs = o->tol * bn;
+  RC(engine_vcycle<float>(ctx, e, be, u1, r, s, op, k2, geom, sg, 0, o->ndown, o->ntop, o->nup, o->omega,
+                          &run));
+  RC(read_small(ctx, 12));
+  const double *out = ctx->h_small + 8;
+  st->rel_residual = out[0] / bn;
+  st->initial_rel = out[3] / bn;
+  st->cycles = (int)out[2];
+  st->outer = (int)out[2];
+  if (!std::isfinite(st->rel_residual))
+    return fail(ctx, SRMG_ERR_DIVERGED, "mixed solve: defect norm is not finite after %d steps", st->cycles);
   return SRMG_OK;
 }
 
