@@ -219,6 +219,49 @@ int srmg_residual_postrestrict_level_dev(srmg_ctx *ctx, double *b, const double 
 int srmg_resnorm_noalloc(srmg_ctx *ctx, const double *b, const double *u, int64_t nblk_alloc,
                          double s, int op, double k2, int geom, double *out);
 
+/* ---- batched solves: many independent problems in one persistent launch ----------
+ * No single counterpart in the reference: it solves the Poisson potential
+ * (src/streamer.jl:322-334) and each photoionization Helmholtz term (src/photo.jl,
+ * one HelmholtzDiscretization per screening constant) with separate vcycle!/fmg!
+ * calls, tree by tree.  A batch context holds a forest: one item per (tree,
+ * operator) pair, every item with its own copy of its tree's blocks.  An item's
+ * solve stops when its own relative residual reaches tol; the others continue, and
+ * each item's result is the one srmg_solve_dev gives for it alone.
+ * Limits: every item uses the persistent engine (option "engine" 1, sweep counts
+ * >= 1, 16-byte aligned fields); at most 4 blocks on an item's level 1 for the
+ * mixed mode's direct coarsest-level solve (more: smoothing at the top). */
+typedef struct {
+    const srmg_ctx *tree;  /* context whose uploaded tree the item solves on */
+    double s;              /* scale s of L u + s b = 0 */
+    int op;                /* SRMG_OP_LAPLACIAN or SRMG_OP_HELMHOLTZ */
+    double k2;             /* Helmholtz k^2 (screening constant squared) */
+    int8_t bc[9];          /* boundary table as in srmg_vcycle */
+} srmg_item;
+
+/* Build the forest of `batch` (a context created with srmg_create) from the items;
+ * every item's tree context must stay alive only for this call (the trees are
+ * copied).  All items share one geometry. */
+int srmg_batch_set(srmg_ctx *batch, int nitems, const srmg_item *items, int geom);
+int srmg_batch_items(const srmg_ctx *batch);
+/* First block (0-based) and block count of item `item` in the forest layout: item
+ * k's field occupies blocks [offset, offset + nblk) of a forest field, in its own
+ * tree's block order.  -1 on a bad argument. */
+int64_t srmg_batch_offset(const srmg_ctx *batch, int item);
+int64_t srmg_batch_nblk(const srmg_ctx *batch, int item);
+/* Solve every item.  u[k], b[k]: item k's DEVICE fields in its own tree's layout
+ * (at least srmg_batch_nblk(batch, k) blocks); u in/out, b read-only.  stats: one
+ * entry per item.  With option "graph" 1 the copies in and out and the solve are
+ * captured in a CUDA graph on the first call and replayed by later calls with the
+ * same pointers and options. */
+int srmg_batch_solve_dev(srmg_ctx *batch, double *const *u, const double *const *b,
+                         const srmg_solve_opts *opts, srmg_stats *stats);
+/* The same on HOST fields (copied in and out inside the call). */
+int srmg_batch_solve(srmg_ctx *batch, double *const *u, const double *const *b,
+                     const srmg_solve_opts *opts, srmg_stats *stats);
+/* The same on fields already in the forest layout (no copies). */
+int srmg_batch_solve_forest_dev(srmg_ctx *batch, double *u, const double *b,
+                                const srmg_solve_opts *opts, srmg_stats *stats);
+
 /* Tuning knobs (no reference counterpart; the autotuner drives them):
  *   "engine"           1 = persistent one-launch V-cycle (default), 0 = one kernel per
  *                      reference operation;
@@ -226,7 +269,8 @@ int srmg_resnorm_noalloc(srmg_ctx *ctx, const double *b, const double *u, int64_
  *                      blocks run inside one CTA of the persistent kernel (default 16);
  *   "engine_ctas"      CTAs of the persistent kernel (0 = one per SM);
  *   "trace"            1 = record a %globaltimer stamp (ns) after every phase of the
- *                      persistent kernel, read back with srmg_get_trace. */
+ *                      persistent kernel, read back with srmg_get_trace;
+ *   "graph"            1 = batched solves replay a captured CUDA graph. */
 int srmg_set_option(srmg_ctx *ctx, const char *key, int64_t value);
 
 /* Phase timestamps of the last persistent-kernel launch (with option "trace" on);

@@ -100,7 +100,12 @@ extern "C" void srmg_destroy(srmg_ctx *ctx) {
   for (auto &b : ctx->f32) if (b.p) cudaFree(b.p);
   if (ctx->part.p) cudaFree(ctx->part.p);
   if (ctx->small.p) cudaFree(ctx->small.p);
-  if (ctx->coarse_inv.p) cudaFree(ctx->coarse_inv.p);
+  for (auto &kv : ctx->coarse_cache) cudaFree(kv.second.p);
+  if (ctx->it_tab.p) cudaFree(ctx->it_tab.p);
+  if (ctx->istat.p) cudaFree(ctx->istat.p);
+  if (ctx->h_items) cudaFreeHost(ctx->h_items);
+  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+  for (auto &b : ctx->forest) if (b.p) cudaFree(b.p);
   if (ctx->sync.p) cudaFree(ctx->sync.p);
   if (ctx->trace.p) cudaFree(ctx->trace.p);
   if (ctx->h_small) cudaFreeHost(ctx->h_small);
@@ -140,12 +145,13 @@ static int face_of(const int64_t f[2]) {
   return -1;
 }
 
-extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
-                             const srmg_pair *const *pairs, const int64_t *nnb,
-                             const srmg_neighbor *const *nb, const int64_t *nbd,
-                             const srmg_boundary *const *bd, const int64_t *nrb,
-                             const srmg_refbnd *const *rb, const int64_t *nch,
-                             const srmg_child *const *ch, uint64_t generation) {
+// Validate and upload a tree (or a forest: item_of[blk] gives the item of every 1-based
+// block id, each item's blocks contiguous within every level's list).
+int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_pair *const *pairs,
+                     const int64_t *nnb, const srmg_neighbor *const *nb, const int64_t *nbd,
+                     const srmg_boundary *const *bd, const int64_t *nrb, const srmg_refbnd *const *rb,
+                     const int64_t *nch, const srmg_child *const *ch, uint64_t generation,
+                     const std::vector<int> *item_of, int nitems) {
   if (!ctx) return SRMG_ERR_BADARG;
   if (nlev < 1 || nlev > 30 || !npairs || !pairs || !nnb || !nb || !nbd || !bd || !nrb || !rb ||
       !nch || !ch)
@@ -275,12 +281,55 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
     }
   }
 
+  // items: per level, each item's blocks must form one contiguous run of the list
+  if (nitems < 1 || (item_of && (int64_t)item_of->size() < max_blk + 1))
+    return fail(ctx, SRMG_ERR_BADARG, "bad item table");
+  std::vector<int2> lrange((size_t)nitems * nlev, make_int2(0, 0));
+  for (int l = 0; l < nlev; l++) {
+    int prev = -1;
+    std::vector<char> seen(nitems, 0);
+    for (size_t i = 0; i < hb[l].size(); i++) {
+      int4 &b4 = hb[l][i];
+      const int it = item_of ? (*item_of)[b4.x + 1] : 0;
+      if (it < 0 || it >= nitems) return fail(ctx, SRMG_ERR_BADARG, "block %d: item out of range", b4.x + 1);
+      if (it != prev) {
+        if (seen[it]) return fail(ctx, SRMG_ERR_BADTREE, "level %d: blocks of item %d are not contiguous", l + 1, it);
+        seen[it] = 1;
+        lrange[(size_t)it * nlev + l] = make_int2((int)i, 0);
+        prev = it;
+      }
+      lrange[(size_t)it * nlev + l].y++;
+      b4.w |= it << 8;  // the item rides in bits 8.. of the child-mask word
+    }
+  }
+  if (item_of)
+    for (int l = 0; l < nlev; l++)
+      for (const int4 &e : hc[l])
+        if ((*item_of)[e.x + 1] != (*item_of)[e.y + 1])
+          return fail(ctx, SRMG_ERR_BADTREE, "level %d: child edge between two items", l + 1);
+  // norm chunks: up to kNormChunk consecutive blocks of one item on one level, ordered
+  // by item, then level, then position, so that every item's chunks are contiguous
+  std::vector<int4> chunks;
+  std::vector<int2> itch(nitems);
+  for (int it = 0; it < nitems; it++) {
+    itch[it].x = (int)chunks.size();
+    for (int l = 0; l < nlev; l++) {
+      const int2 rg = lrange[(size_t)it * nlev + l];
+      for (int q = 0; q < rg.y; q += kNormChunk)
+        chunks.push_back(make_int4(l + 1, rg.x + q, std::min(kNormChunk, rg.y - q), it));
+    }
+    itch[it].y = (int)chunks.size() - itch[it].x;
+  }
   for (int l = 0; l < nlev; l++)
     for (const int4 &b4 : hb[l]) binfo[b4.x] = make_int4(b4.y, b4.z, b4.w, l + 1);
   for (int64_t b = 0; b < max_blk; b++)
     for (int f = 0; f < 4; f++) {
       int4 &fc = bface[4 * b + f];
-      if (fc.x == FACE_NEIGHBOR) fc.z = binfo[fc.y].z;  // the neighbour's child mask
+      if (fc.x == FACE_NEIGHBOR) {
+        fc.z = binfo[fc.y].z & 15;  // the neighbour's child mask
+        if (binfo[fc.y].z >> 8 != binfo[b].z >> 8)
+          return fail(ctx, SRMG_ERR_BADTREE, "neighbour edge between two items");
+      }
     }
   std::vector<std::vector<int4>> hr(nlev);
   for (int l = 0; l < nlev; l++) {
@@ -322,6 +371,9 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
   const size_t oinfo = take((max_blk + 1) * sizeof(int4));
   const size_t ofaceb = take(4 * (max_blk + 1) * sizeof(int4));
   const size_t okids = take((max_blk + 1) * sizeof(int4));
+  const size_t olr = take(lrange.size() * sizeof(int2));
+  const size_t ochunk = take(std::max<size_t>(chunks.size(), 1) * sizeof(int4));
+  const size_t oitch = take(itch.size() * sizeof(int2));
   std::vector<char> host(off, 0);
   for (int l = 0; l < nlev; l++) {
     memcpy(host.data() + orr[l], hr[l].data(), hr[l].size() * sizeof(int4));
@@ -340,6 +392,9 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
   memcpy(host.data() + oinfo, binfo.data(), binfo.size() * sizeof(int4));
   memcpy(host.data() + ofaceb, bface.data(), bface.size() * sizeof(int4));
   memcpy(host.data() + okids, bkids.data(), bkids.size() * sizeof(int4));
+  memcpy(host.data() + olr, lrange.data(), lrange.size() * sizeof(int2));
+  memcpy(host.data() + ochunk, chunks.data(), chunks.size() * sizeof(int4));
+  memcpy(host.data() + oitch, itch.data(), itch.size() * sizeof(int2));
 
   CK(cudaStreamSynchronize(ctx->stream));
   free_tree(ctx);
@@ -373,12 +428,49 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
   ctx->d_info = (int4 *)(base + oinfo);
   ctx->d_faceb = (int4 *)(base + ofaceb);
   ctx->d_kids = (int4 *)(base + okids);
+  ctx->d_it_lrange = (int2 *)(base + olr);
+  ctx->d_chunks = (int4 *)(base + ochunk);
+  ctx->d_it_chunks = (int2 *)(base + oitch);
+  ctx->nchunk = (int)chunks.size();
+  ctx->it_lrange_host = lrange;
+  ctx->nitems = nitems;
+  ctx->l1_blocks = hb[0];
+  ctx->l1_faces = hf[0];
   ctx->wtab_n = wn;
   ctx->max_blk = max_blk;
   ctx->generation = generation;
   ctx->has_tree = true;
-  ctx->coarse_ok = false;
-  ctx->coarse_key.clear();
+  ctx->it_tab_host.clear();
+  return SRMG_OK;
+}
+
+extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
+                             const srmg_pair *const *pairs, const int64_t *nnb,
+                             const srmg_neighbor *const *nb, const int64_t *nbd,
+                             const srmg_boundary *const *bd, const int64_t *nrb,
+                             const srmg_refbnd *const *rb, const int64_t *nch,
+                             const srmg_child *const *ch, uint64_t generation) {
+  RC(build_tree(ctx, nlev, npairs, pairs, nnb, nb, nbd, bd, nrb, rb, nch, ch, generation, nullptr, 1));
+  // keep the arrays for forests built from this tree
+  HostTree &h = ctx->htree;
+  h.nlev = nlev;
+  h.max_blk = ctx->max_blk;
+  h.pairs.assign(nlev, {});
+  h.nb.assign(nlev, {});
+  h.bd.assign(nlev, {});
+  h.rb.assign(nlev, {});
+  h.ch.assign(nlev, {});
+  for (int l = 0; l < nlev; l++) {
+    h.pairs[l].assign(pairs[l], pairs[l] + npairs[l]);
+    h.nb[l].assign(nb[l], nb[l] + nnb[l]);
+    h.bd[l].assign(bd[l], bd[l] + nbd[l]);
+    h.rb[l].assign(rb[l], rb[l] + nrb[l]);
+    h.ch[l].assign(ch[l], ch[l] + nch[l]);
+  }
+  ctx->item_first.assign(1, 0);
+  ctx->item_nblk.assign(1, ctx->max_blk);
+  ctx->batch_items.clear();
+  ctx->geom_forest = -1;
   return SRMG_OK;
 }
 
@@ -405,6 +497,12 @@ Signs srmg::make_signs(const int8_t *bc) {
   Signs s;
   for (int i = 0; i < 9; i++) s.v[i] = bc ? (double)bc[i] : 1.0;
   return s;
+}
+
+std::vector<int8_t> srmg::bc_of(const Signs &sg) {
+  std::vector<int8_t> bc(9);
+  for (int i = 0; i < 9; i++) bc[i] = (int8_t)sg.v[i];
+  return bc;
 }
 
 // ------------------------------------------------------------------ launches
@@ -550,8 +648,12 @@ int srmg::vcycle_dev(srmg_ctx *ctx, T *u, T *b, T *r, T *u1, double s, int op, d
   // Bulk copies need 16-byte aligned block tiles.
   const bool aligned = ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(b) |
                          reinterpret_cast<uintptr_t>(r) | reinterpret_cast<uintptr_t>(u1)) & 15) == 0;
-  if (ctx->use_engine && aligned && ndown >= 1 && ntop >= 1 && nup >= 1 && ctx->nlev <= 30)
-    return engine_vcycle<T>(ctx, u, b, u1, r, s, op, k2, geom, sg, lmax, ndown, ntop, nup, omega);
+  if (ctx->use_engine && aligned && ndown >= 1 && ntop >= 1 && nup >= 1 && ctx->nlev <= 30) {
+    ItemTabs tabs;
+    const std::vector<ItemSpec> specs = uniform_items(ctx, s, op, k2, bc_of(sg).data());
+    RC(prepare_items(ctx, specs.data(), geom, omega, false, 0, 0.0, &tabs));
+    return engine_vcycle<T>(ctx, u, b, u1, r, tabs, geom, lmax, ndown, ntop, nup);
+  }
   for (int l = lmax; l >= 2; l--) {
     const double sl = level_scale(s, l);
     const OpParams<T> p = op_params<T>(op, geom, k2, sl, omega);
@@ -673,6 +775,7 @@ extern "C" int srmg_set_option(srmg_ctx *ctx, const char *key, int64_t value) {
   if (!ctx || !key) return SRMG_ERR_BADARG;
   if (!strcmp(key, "engine")) ctx->use_engine = value != 0;
   else if (!strcmp(key, "trace")) ctx->trace_on = value != 0;
+  else if (!strcmp(key, "graph")) ctx->use_graph = value != 0;
   else if (!strcmp(key, "local_max_blocks")) {
     if (value < 0 || value > 1024) return fail(ctx, SRMG_ERR_BADARG, "local_max_blocks out of range");
     ctx->local_max_blocks = (int)value;
@@ -753,9 +856,12 @@ extern "C" int srmg_gs_iter_dev(srmg_ctx *ctx, double *u, const double *b, int64
   if (!u || !b || level < 1 || level > ctx->nlev || n < 0)
     return fail(ctx, SRMG_ERR_BADARG, "gs_iter: bad arguments");
   const bool aligned = ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(b)) & 15) == 0;
-  if (ctx->use_engine && aligned)
-    RC(engine_smooth<double>(ctx, u, b, level, omega, sl, n, op, k2, geom, make_signs(bc)));
-  else
+  if (ctx->use_engine && aligned) {
+    ItemTabs tabs;
+    const std::vector<ItemSpec> specs = uniform_items(ctx, sl, op, k2, bc);
+    RC(prepare_items(ctx, specs.data(), geom, omega, false, level, sl, &tabs));
+    RC(engine_smooth<double>(ctx, u, b, tabs, geom, level, n));
+  } else
     RC(L_gs_iter<double>(ctx, u, b, level, op_params<double>(op, geom, k2, sl, omega), n, make_signs(bc)));
   CK(cudaGetLastError());
   return SRMG_OK;

@@ -28,6 +28,26 @@ struct DevBuf {
   size_t bytes = 0;
 };
 
+// Operator of one item (an independent problem of the context's forest).
+struct ItemSpec {
+  double s = 1.0;
+  int op = 0;
+  double k2 = 0.0;
+  int8_t bc[9] = {1, 1, 1, 1, 1, 1, 1, 1, 1};
+};
+
+// Host copy of an uploaded tree (the arrays srmg_set_tree received), kept so that
+// forests can be assembled from the trees of other contexts.
+struct HostTree {
+  int nlev = 0;
+  int64_t max_blk = 0;
+  std::vector<std::vector<srmg_pair>> pairs;
+  std::vector<std::vector<srmg_neighbor>> nb;
+  std::vector<std::vector<srmg_boundary>> bd;
+  std::vector<std::vector<srmg_refbnd>> rb;
+  std::vector<std::vector<srmg_child>> ch;
+};
+
 }  // namespace srmg
 
 struct srmg_ctx {
@@ -73,9 +93,34 @@ struct srmg_ctx {
   double *h_small = nullptr;  // pinned host mirror of `small`
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
-  // coarsest-level direct solver cache (mixed mode)
-  srmg::DevBuf coarse_inv;
-  std::vector<double> coarse_key;
-  int coarse_n = 0;
-  bool coarse_ok = false;
+  // items: independent problems of one forest (a plain tree is one item)
+  srmg::HostTree htree;
+  int nitems = 1;
+  int geom_forest = -1;                 // geometry fixed by srmg_batch_set (-1: any)
+  std::vector<int64_t> item_first;      // per item: first 0-based block id of its range
+  std::vector<int64_t> item_nblk;       // per item: blocks of its range
+  std::vector<int2> it_lrange_host;     // [item * nlev + l - 1] {first, count} in level l's list
+  int2 *d_it_lrange = nullptr;          // device copy (inside d_tree)
+  int4 *d_chunks = nullptr;             // norm chunks {level, first, count, item} (inside d_tree)
+  int2 *d_it_chunks = nullptr;          // per item: {first chunk, chunks}
+  int nchunk = 0;
+  std::vector<int4> l1_blocks, l1_faces;  // level 1 as uploaded (direct coarsest solve)
+  std::vector<srmg::ItemSpec> batch_items;       // operators given to srmg_batch_set
+
+  // per-item operator tables of the persistent engine
+  srmg::DevBuf it_tab;
+  std::vector<char> it_tab_host;        // what it_tab holds
+  // per-item results of the device loop, and their pinned host mirror
+  srmg::DevBuf istat;
+  double *h_items = nullptr;
+  size_t h_items_n = 0;
+
+  // batched solves: forest-layout fields (u, b) and the captured step sequence
+  srmg::DevBuf forest[2];
+  cudaGraphExec_t graph_exec = nullptr;
+  std::vector<const void *> graph_key;  // field pointers and options the graph was captured for
+  bool use_graph = false;
+
+  // coarsest-level direct inverses, by operator and level-1 structure
+  std::map<std::vector<double>, srmg::DevBuf> coarse_cache;
 };

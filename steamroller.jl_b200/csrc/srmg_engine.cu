@@ -52,10 +52,63 @@ int srmg::engine_local_top(srmg_ctx *ctx, int lmax) {
   return K;
 }
 
+// Launch state shared by every engine launch: tree tables, item tables, barrier and
+// error words, the frozen flags (zeroed) and norm scratch.
 template <typename T>
-int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, double s, int op, double k2, int geom,
-                        const Signs &sg, int lmax, int ndown, int ntop, int nup, double omega,
-                        const EngineRun *run) {
+static int engine_common(srmg_ctx *ctx, EngArgs<T> &A, T *u, const ItemTabs &tabs, int geom) {
+  memset(&A, 0, sizeof A);
+  A.u = u;
+  {
+    DevBuf &alt = (sizeof(T) == 8) ? ctx->f64[5] : ctx->f32[5];
+    RC(ensure(ctx, alt, (size_t)ctx->max_blk * kSS * sizeof(T)));
+    A.ualt = (T *)alt.p;
+  }
+  for (int l = 0; l < ctx->nlev; l++) {
+    A.tr.lvl_rec[l] = ctx->lv[l].rec;
+    A.tr.lvl_blocks[l] = ctx->lv[l].blocks;
+    A.tr.lvl_child[l] = ctx->lv[l].child;
+    A.tr.nblk[l] = ctx->nblk_host[l];
+    A.tr.nch[l] = ctx->nch_host[l];
+  }
+  A.tr.info = ctx->d_info;
+  A.tr.faces = ctx->d_faceb;
+  A.tr.kids = ctx->d_kids;
+  A.wt = wtab_of<T>(ctx);
+  A.geom = geom;
+  A.nitems = ctx->nitems;
+  A.nlev_tab = ctx->nlev;
+  A.it_par = (sizeof(T) == 8) ? (const T *)(const void *)tabs.par64 : (const T *)(const void *)tabs.par32;
+  A.it_sgbits = tabs.sgbits;
+  A.it_lrange = ctx->d_it_lrange;
+  const size_t sync_bytes = 256 + sizeof(int) * (size_t)ctx->nitems;
+  RC(ensure(ctx, ctx->sync, sync_bytes));
+  A.bar = (unsigned *)ctx->sync.p;
+  A.err = (int *)((char *)ctx->sync.p + 128);
+  A.frozen = (int *)((char *)ctx->sync.p + 256);
+  A.timeout_ns = 2000000000LL;  // 2 s per barrier wait
+  if (ctx->trace_on) {
+    RC(ensure(ctx, ctx->trace, kTraceMax * sizeof(long long)));
+    A.trace = (long long *)ctx->trace.p;
+  }
+  CK(cudaMemsetAsync(ctx->sync.p, 0, sync_bytes, ctx->stream));
+  return SRMG_OK;
+}
+
+template <typename T>
+static int engine_launch(srmg_ctx *ctx, EngArgs<T> &A) {
+  int grid = 0;
+  RC(engine_grid<T>(ctx, &grid));  // also raises the dynamic shared-memory limit
+  if (ctx->engine_ctas > 0 && ctx->engine_ctas < grid) grid = ctx->engine_ctas;
+  void *args[] = {&A};
+  CK(cudaLaunchCooperativeKernel((const void *)k_engine_vcycle<T>, dim3(grid), dim3(1024), args,
+                                 engine_smem_bytes<T>(), ctx->stream));
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+template <typename T>
+int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, const ItemTabs &tabs, int geom, int lmax,
+                        int ndown, int ntop, int nup, const EngineRun *run) {
   const EngineRun none;
   if (!run) run = &none;
   if (ctx->nlev > kMaxLev) return fail(ctx, SRMG_ERR_UNSUPPORTED, "engine supports at most %d levels", kMaxLev);
@@ -65,143 +118,61 @@ int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, double s, int op
     if (ctx->nblk_host[l - 1] > 0) L = l;
   if (L == 0) return SRMG_OK;
   EngArgs<T> A;
-  memset(&A, 0, sizeof A);
-  A.u = u;
-  {
-    DevBuf &alt = (sizeof(T) == 8) ? ctx->f64[5] : ctx->f32[5];
-    RC(ensure(ctx, alt, (size_t)ctx->max_blk * kSS * sizeof(T)));
-    A.ualt = (T *)alt.p;
-  }
+  RC(engine_common<T>(ctx, A, u, tabs, geom));
   A.b = b;
   A.u1 = u1;
   A.e = e;
-  for (int l = 0; l < ctx->nlev; l++) {
-    A.tr.lvl_rec[l] = ctx->lv[l].rec;
-    A.tr.lvl_blocks[l] = ctx->lv[l].blocks;
-    A.tr.lvl_child[l] = ctx->lv[l].child;
-    A.tr.nblk[l] = ctx->nblk_host[l];
-    A.tr.nch[l] = ctx->nch_host[l];
-  }
-  A.tr.info = ctx->d_info;
-  A.tr.faces = ctx->d_faceb;
-  A.tr.kids = ctx->d_kids;
-  A.wt = wtab_of<T>(ctx);
-  A.sg = sg;
-  A.op = op;
-  A.geom = geom;
   A.lmax = L;
   A.ndown = ndown;
   A.ntop = ntop;
   A.nup = nup;
   A.local_top = engine_local_top(ctx, L);
-  if (run->coarse_P && run->coarse_n == 256 * ctx->nblk_host[0] && ctx->nblk_host[0] <= 4) {
-    A.coarse_P = run->coarse_P;
-    A.coarse_n = run->coarse_n;
-  }
-  for (int l = 1; l <= L; l++) {
-    const OpParams<T> p = op_params<T>(op, geom, k2, level_scale(s, l), omega);
-    A.lev_s[l] = p.s;
-    A.lev_centre[l] = p.centre;
-    A.lev_nwc[l] = p.nwc;
-  }
-  RC(ensure(ctx, ctx->sync, 256));
-  A.bar = (unsigned *)ctx->sync.p;
-  A.err = (int *)((char *)ctx->sync.p + 128);
-  A.timeout_ns = 2000000000LL;  // 2 s per barrier wait
-  RC(ensure(ctx, ctx->part, sizeof(double) * 4096));
-  A.part = (double *)ctx->part.p;
-  A.out = (double *)ctx->small.p + 8;
+  if (run->direct && tabs.P) A.it_P = tabs.P;
   A.max_cycles = run->max_cycles;
-  A.tol_abs = run->tol_abs;
+  A.tol = run->tol;
+  if (run->max_cycles > 0) {
+    const int64_t total = std::max(ctx->nchunk, 1);
+    RC(ensure(ctx, ctx->part, sizeof(double) * 2 * (size_t)total));
+    A.bpart = (double *)ctx->part.p;
+    A.bpart_b = A.bpart + total;
+    A.chunks = ctx->d_chunks;
+    A.nchunk = ctx->nchunk;
+    A.it_chunks = ctx->d_it_chunks;
+    RC(ensure(ctx, ctx->istat, sizeof(double) * (4 * (size_t)ctx->nitems + 8)));
+    A.inorm = (double *)ctx->istat.p;
+    A.out = A.inorm + 4 * ctx->nitems;
+  }
   if (run->u64) {
+    if (run->max_cycles <= 0) return fail(ctx, SRMG_ERR_BADARG, "mixed engine step needs the device loop");
     A.mx.u64 = run->u64;
     A.mx.b64 = run->b64;
     A.mx.wt64 = WTab<double>{ctx->d_wm64, ctx->d_wp64};
-    for (int l = 1; l <= L; l++) {
-      const OpParams<double> p = op_params<double>(op, geom, k2, level_scale(s, l), omega);
-      A.mx.lev_s64[l] = p.s;
-      A.mx.lev_centre64[l] = p.centre;
-    }
+    A.mx.it_par64 = tabs.par64;
     A.mx.refbnd_levels = ctx->refbnd_levels;
     A.mx.apply_update = run->apply_update;
   }
-  if (ctx->trace_on) {
-    RC(ensure(ctx, ctx->trace, kTraceMax * sizeof(long long)));
-    A.trace = (long long *)ctx->trace.p;
-  }
-  int grid = 0;
-  RC(engine_grid<T>(ctx, &grid));  // also raises the dynamic shared-memory limit
-  if (ctx->engine_ctas > 0 && ctx->engine_ctas < grid) grid = ctx->engine_ctas;
-  CK(cudaMemsetAsync(ctx->sync.p, 0, 256, ctx->stream));
-  void *args[] = {&A};
-  CK(cudaLaunchCooperativeKernel((const void *)k_engine_vcycle<T>, dim3(grid), dim3(1024), args,
-                                 engine_smem_bytes<T>(), ctx->stream));
-  ctx->launches++;
-  return SRMG_OK;
+  return engine_launch<T>(ctx, A);
 }
 
-// gauss_seidel_iter! on one level through the persistent kernel.
+// gauss_seidel_iter! on one level through the persistent kernel (tabs built with the
+// level's scale).
 template <typename T>
-int srmg::engine_smooth(srmg_ctx *ctx, T *u, const T *b, int level, double omega, double sl, int n, int op,
-                        double k2, int geom, const Signs &sg) {
+int srmg::engine_smooth(srmg_ctx *ctx, T *u, const T *b, const ItemTabs &tabs, int geom, int level, int n) {
   if (n <= 0 || ctx->nblk_host[level - 1] == 0) return SRMG_OK;
   EngArgs<T> A;
-  memset(&A, 0, sizeof A);
-  A.u = u;
-  {
-    DevBuf &alt = (sizeof(T) == 8) ? ctx->f64[5] : ctx->f32[5];
-    RC(ensure(ctx, alt, (size_t)ctx->max_blk * kSS * sizeof(T)));
-    A.ualt = (T *)alt.p;
-  }
+  RC(engine_common<T>(ctx, A, u, tabs, geom));
   A.b = const_cast<T *>(b);
-  for (int l = 0; l < ctx->nlev; l++) {
-    A.tr.lvl_rec[l] = ctx->lv[l].rec;
-    A.tr.lvl_blocks[l] = ctx->lv[l].blocks;
-    A.tr.lvl_child[l] = ctx->lv[l].child;
-    A.tr.nblk[l] = ctx->nblk_host[l];
-    A.tr.nch[l] = ctx->nch_host[l];
-  }
-  A.tr.info = ctx->d_info;
-  A.tr.faces = ctx->d_faceb;
-  A.tr.kids = ctx->d_kids;
-  A.wt = wtab_of<T>(ctx);
-  A.sg = sg;
-  A.op = op;
-  A.geom = geom;
   A.lmax = level;
   A.smooth_level = level;
   A.smooth_n = n;
-  const OpParams<T> p = op_params<T>(op, geom, k2, sl, omega);
-  A.lev_s[level] = p.s;
-  A.lev_centre[level] = p.centre;
-  A.lev_nwc[level] = p.nwc;
-  RC(ensure(ctx, ctx->sync, 256));
-  A.bar = (unsigned *)ctx->sync.p;
-  A.err = (int *)((char *)ctx->sync.p + 128);
-  A.timeout_ns = 2000000000LL;
-  if (ctx->trace_on) {
-    RC(ensure(ctx, ctx->trace, kTraceMax * sizeof(long long)));
-    A.trace = (long long *)ctx->trace.p;
-  }
-  int grid = 0;
-  RC(engine_grid<T>(ctx, &grid));
-  if (ctx->engine_ctas > 0 && ctx->engine_ctas < grid) grid = ctx->engine_ctas;
-  CK(cudaMemsetAsync(ctx->sync.p, 0, 256, ctx->stream));
-  void *args[] = {&A};
-  CK(cudaLaunchCooperativeKernel((const void *)k_engine_vcycle<T>, dim3(grid), dim3(1024), args,
-                                 engine_smem_bytes<T>(), ctx->stream));
-  ctx->launches++;
-  return SRMG_OK;
+  return engine_launch<T>(ctx, A);
 }
-template int srmg::engine_smooth<double>(srmg_ctx *, double *, const double *, int, double, double, int, int,
-                                         double, int, const Signs &);
+template int srmg::engine_smooth<double>(srmg_ctx *, double *, const double *, const ItemTabs &, int, int, int);
 
-template int srmg::engine_vcycle<double>(srmg_ctx *, double *, double *, double *, double *, double, int,
-                                         double, int, const Signs &, int, int, int, int, double,
-                                         const EngineRun *);
-template int srmg::engine_vcycle<float>(srmg_ctx *, float *, float *, float *, float *, double, int,
-                                        double, int, const Signs &, int, int, int, int, double,
-                                        const EngineRun *);
+template int srmg::engine_vcycle<double>(srmg_ctx *, double *, double *, double *, double *, const ItemTabs &,
+                                         int, int, int, int, int, const EngineRun *);
+template int srmg::engine_vcycle<float>(srmg_ctx *, float *, float *, float *, float *, const ItemTabs &, int,
+                                        int, int, int, int, const EngineRun *);
 
 extern "C" int srmg_get_trace(srmg_ctx *ctx, int64_t *out, int max_entries) {
   if (!ctx || !out || max_entries < 0) return SRMG_ERR_BADARG;

@@ -28,8 +28,16 @@
 // The coarse correction e = u - u1 of a level (diffto!, src/blockfield.jl:569-576) and
 // its ghosts are produced in that level's last GS iteration.  Levels 1..local_top are
 // processed by CTA 0 alone with CTA barriers.  Block tiles reach shared memory through
-// bulk asynchronous copies (cp.async.bulk, no multicast) into a double-buffered
+// bulk asynchronous copies (cp.async.bulk, no multicast) into a triple-buffered
 // per-slot pipeline; every wait on an mbarrier or a barrier is bounded in time.
+//
+// One launch can carry several independent problems ("items"): the trees of a forest,
+// each with its own operator (Poisson or Helmholtz k^2, scale s, boundary table).  The
+// item of a block sits in bits 8.. of its child-mask word; operator parameters come from
+// per-item tables.  Norms are per item and formed in a fixed order (per-block warp
+// partials, then one CTA per item), so they do not depend on the grid size; an item
+// whose norm reaches its tolerance is frozen (no phase touches its blocks again) while
+// the others iterate, so every item ends exactly as if it had been solved alone.
 #pragma once
 #include "srmg_kernels.cuh"
 
@@ -54,13 +62,12 @@ struct EngTree {
 // first applies the previous correction (u64 += u), makes u64 a composite-grid function
 // of its leaves (restriction chain, ghost refresh), forms the FP64 defect as the FP32
 // right-hand side with its leaf norm, and runs the FP32 V-cycle only if the norm is
-// still above tol_abs.
+// still above its tolerance.
 struct MixedArgs {
   double *u64;
   const double *b64;
   WTab<double> wt64;
-  double lev_s64[kMaxLev + 1];
-  double lev_centre64[kMaxLev + 1];
+  const double *it_par64;  // per item: kParStride FP64 operator values
   unsigned refbnd_levels;  // bit l: level l has refinement-boundary faces
   int apply_update;        // apply the correction left by a previous launch first
 };
@@ -70,31 +77,44 @@ struct EngArgs {
   T *u, *ualt, *b, *u1, *e;   // ualt: the second buffer of the per-level ping-pong
   EngTree tr;
   WTab<T> wt;
-  Signs sg;
-  int op, geom;
+  int geom;
   int lmax;          // finest non-empty level taking part
   int ndown, ntop, nup;
   int local_top;     // levels 1..local_top run inside CTA 0
   int smooth_level;  // > 0: run smooth_n GS iterations on this level only (gauss_seidel_iter!)
   int smooth_n;
-  T lev_s[kMaxLev + 1];       // s_l by level (index l)
-  T lev_centre[kMaxLev + 1];  // stencil centre by level
-  T lev_nwc[kMaxLev + 1];     // -(omega / diagelm) by level
+  int nitems;
+  int nlev_tab;                // row length of it_lrange
+  const T *it_par;             // per item: kParStride operator values (s_l, centre_l, nwc_l)
+  const int *it_sgbits;        // per item: the 3x3 boundary table, entry k as (bc_k + 1) << 2k
+  const double *const *it_P;   // per item: P = -s A_1^{-1} of its level 1 (row-major), or null
+  const int2 *it_lrange;       // [item * nlev_tab + l - 1]: {first, count} in level l's block list
+  int *frozen;                 // per item: nonzero once it has stopped iterating (zero at launch)
   unsigned *bar;     // barrier counter, zero at launch
   int *err;          // error word (0 = ok)
   long long timeout_ns;
   long long *trace;  // optional: CTA 0 stamps %globaltimer after every phase
-  const double *coarse_P;  // optional: the coarsest level is solved directly, u1 = P b1
-  int coarse_n;            // unknowns of the coarsest level (256 per block, <= 1024)
   MixedArgs mx;            // mixed-precision outer step (mx.u64 != nullptr)
-  // Device-side solve loop: with max_cycles > 0 the launch repeats V-cycles until the
-  // leaf norm of the residual (FP64 mode) or of the FP64 defect (mixed mode) is
-  // <= tol_abs or max_cycles V-cycles have run.
+  // Device-side solve loop: with max_cycles > 0 the launch repeats V-cycles until every
+  // item's leaf norm of the residual (FP64 mode) or of the FP64 defect (mixed mode) is
+  // <= tol * (its leaf norm of b, or 1 if that is 0), or max_cycles V-cycles have run.
   int max_cycles;
-  double tol_abs;
-  double *part;            // one partial sum per CTA
-  double *out;             // out[0] final norm, [1] converged, [2] V-cycles run, [3] initial norm
+  double tol;
+  const int4 *chunks;      // norm chunks {level, first position, count, item}, by item
+  int nchunk;
+  const int2 *it_chunks;   // per item: {first chunk, chunks}
+  double *bpart;           // one partial sum per chunk: r^2
+  double *bpart_b;         // the same for b^2
+  double *inorm;           // per item: {norm, |b|, initial norm, V-cycles run}
+  double *out;             // out[0] V-cycles run by the launch
 };
+
+__device__ __forceinline__ int item_of(int4 bk) { return bk.w >> 8; }
+
+template <typename T>
+__device__ __forceinline__ bool is_frozen(const EngArgs<T> &A, int item) {
+  return A.nitems > 1 && A.frozen[item] != 0;
+}
 
 // ------------------------------------------------------------------ barriers
 
@@ -197,39 +217,49 @@ struct SlotSmem {
   T tile[kBuf][kSS];
   int4 recs[32][5];
   uint64_t bar[kBuf];
+  int sel[32];  // list positions of the chunk's blocks that take part
+  int cnt;
 };
+
+// Boundary sign k (-1, 0 or 1) of a packed boundary table.
+template <typename F>
+__device__ __forceinline__ F sign_at(unsigned sgb, int k) {
+  return F((int)((sgb >> (2 * k)) & 3u) - 1);
+}
 
 // Write the value v of valid cell (x, y) of block X into the ghosts that copy or mirror
 // it, in `field`: the facing ghost of each neighbour (fill_ghost_copy!) and the block's
-// own mirror ghost (fill_ghost_bnd!).  fc: the block's four face records.
+// own mirror ghost (fill_ghost_bnd!, src/connectivity.jl:191-213).  fc: the block's four
+// face records; sgb: the item's packed boundary table.
 template <typename F>
-__device__ __forceinline__ void push_f(const Signs &sg, F *field, int X, const int4 *fc, int x, int y, F v) {
+__device__ __forceinline__ void push_f(unsigned sgb, F *field, int X, const int4 *fc, int x, int y, F v) {
   F *xb = field + (int64_t)X * kSS;
   if (x <= 3) {
     const int4 fi = fc[0];
     if (fi.w >= 0) field[(int64_t)fi.w * kSS + (x + kM) + kS * y] = v;
-    else if (fi.x == FACE_BOUNDARY) xb[(2 * kG - 1 - x) + kS * y] = dmul<F>(F(sg.v[3]), v);
+    else if (fi.x == FACE_BOUNDARY) xb[(2 * kG - 1 - x) + kS * y] = dmul<F>(sign_at<F>(sgb, 3), v);
   }
   if (x >= 16) {
     const int4 fi = fc[1];
     if (fi.w >= 0) field[(int64_t)fi.w * kSS + (x - kM) + kS * y] = v;
-    else if (fi.x == FACE_BOUNDARY) xb[(2 * (kG + kM) - 1 - x) + kS * y] = dmul<F>(F(sg.v[5]), v);
+    else if (fi.x == FACE_BOUNDARY) xb[(2 * (kG + kM) - 1 - x) + kS * y] = dmul<F>(sign_at<F>(sgb, 5), v);
   }
   if (y <= 3) {
     const int4 fi = fc[2];
     if (fi.w >= 0) field[(int64_t)fi.w * kSS + x + kS * (y + kM)] = v;
-    else if (fi.x == FACE_BOUNDARY) xb[x + kS * (2 * kG - 1 - y)] = dmul<F>(F(sg.v[1]), v);
+    else if (fi.x == FACE_BOUNDARY) xb[x + kS * (2 * kG - 1 - y)] = dmul<F>(sign_at<F>(sgb, 1), v);
   }
   if (y >= 16) {
     const int4 fi = fc[3];
     if (fi.w >= 0) field[(int64_t)fi.w * kSS + x + kS * (y - kM)] = v;
-    else if (fi.x == FACE_BOUNDARY) xb[x + kS * (2 * (kG + kM) - 1 - y)] = dmul<F>(F(sg.v[7]), v);
+    else if (fi.x == FACE_BOUNDARY) xb[x + kS * (2 * (kG + kM) - 1 - y)] = dmul<F>(sign_at<F>(sgb, 7), v);
   }
 }
 
 template <typename T>
-__device__ __forceinline__ void push(const EngArgs<T> &A, T *field, int X, const int4 *fc, int x, int y, T v) {
-  push_f<T>(A.sg, field, X, fc, x, y, v);
+__device__ __forceinline__ void push(const EngArgs<T> &A, int item, T *field, int X, const int4 *fc, int x, int y,
+                                     T v) {
+  push_f<T>((unsigned)A.it_sgbits[item], field, X, fc, x, y, v);
 }
 
 // Ghost cell `lane` (0..31) of face f: layer lane/16, position lane%16.
@@ -335,7 +365,6 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
   const int o = x + kS * y;
   const bool red = ((x + y) & 1) == 1;  // colour 0 of RedBlack{0}: updated first
   const int mysub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
-  const T s = A.lev_s[l], centre = A.lev_centre[l], nwc = A.lev_nwc[l];
   const HaloCell h = halo_cell(t < 64 ? t : 0);
   // registers prefetched one block ahead
   T b_nx = T(0), e_nx = T(0), hv_nx = T(0), hc_nx = T(0);
@@ -353,13 +382,40 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
       }
     }
   };
+  // one item: the operator values stay in registers for the whole level
+  T s = A.it_par[l], centre = A.it_par[32 + l], nwc = A.it_par[64 + l];
   for (int c0 = 0; c0 < nmine; c0 += 32) {
-    const int cn = min(32, nmine - c0);
-    if (t < 5 * cn) {
-      const int q = t / 5, k = t - 5 * q;
-      S.recs[q][k] = recs[5 * (first + (c0 + q) * step) + k];
+    int cn;
+    if (A.nitems == 1) {
+      cn = min(32, nmine - c0);
+      if (t < 5 * cn) {
+        const int q = t / 5, k = t - 5 * q;
+        S.recs[q][k] = recs[5 * (first + (c0 + q) * step) + k];
+      }
+      slot_sync(slot);
+    } else {
+    // the chunk's next 32 list positions, without the blocks of frozen items
+    if (t < 32) {
+      const int idx = c0 + t;
+      int gi = 0;
+      bool take = false;
+      if (idx < nmine) {
+        gi = first + idx * step;
+        take = A.nitems == 1 || !A.frozen[item_of(recs[5 * gi])];
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, take);
+      if (take) S.sel[__popc(m & ((1u << t) - 1u))] = gi;
+      if (t == 0) S.cnt = __popc(m);
     }
     slot_sync(slot);
+    cn = S.cnt;
+    if (t < 5 * cn) {
+      const int q = t / 5, k = t - 5 * q;
+      S.recs[q][k] = recs[5 * S.sel[q] + k];
+    }
+    slot_sync(slot);
+    if (cn == 0) continue;
+    }
     if (t == 0) {
       issue_tile<T>(S, pk % kBuf, src, S.recs[0][0].x);
       if (cn > 1) issue_tile<T>(S, (pk + 1) % kBuf, src, S.recs[1][0].x);
@@ -383,6 +439,13 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
         return false;
       }
       T *tile = S.tile[buf];
+      const int item = item_of(bk);
+      if (A.nitems > 1) {
+        const T *par = A.it_par + item * kParStride;
+        s = par[l];
+        centre = par[32 + l];
+        nwc = par[64 + l];
+      }
       const W5<T> w = weights<T>(A.wt, A.geom, bk.y, bk.z, x, y);
       if (copy_u1) A.u1[(int64_t)X * kSS + o] = tile[o];
       if (fas) {
@@ -418,7 +481,7 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
       slot_sync(slot);
       const T nu = tile[o];
       dst[(int64_t)X * kSS + o] = nu;
-      push<T>(A, dst, X, fc, x, y, nu);
+      push<T>(A, item, dst, X, fc, x, y, nu);
       if (t < 128) {
         const int f = t >> 5, lane = t & 31;
         if (fc[f].x == FACE_REFBND) {
@@ -430,7 +493,7 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
       if (make_e) {
         const T ev = nu - A.u1[(int64_t)X * kSS + o];
         A.e[(int64_t)X * kSS + o] = ev;
-        push<T>(A, A.e, X, fc, x, y, ev);
+        push<T>(A, item, A.e, X, fc, x, y, ev);
         if (t < 128) refbnd_ghost<T>(A.e, esrc, X, fc, t);
       }
       slot_sync(slot);  // the buffer is refilled three items later
@@ -451,11 +514,14 @@ __device__ void ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
   const int n = A.tr.nch[l - 1];
   const int4 *ch = A.tr.lvl_child[l - 1];
   const int x = 2 + (t & 15), y = 2 + (t >> 4);
-  const T s = A.lev_s[l], centre = A.lev_centre[l];
   for (int i = first; i < n; i += step) {
     const int4 e = ch[i];
     const int F = e.x, C = e.y;
     const int4 fi = A.tr.info[F];
+    const int item = fi.z >> 8;
+    if (is_frozen(A, item)) continue;
+    const T *par = A.it_par + item * kParStride;
+    const T s = par[l], centre = par[32 + l];
     const T *ufb = uf + (int64_t)F * kSS;
     const int o = x + kS * y;
     const W5<T> w = weights<T>(A.wt, A.geom, fi.x, fi.y, x, y);
@@ -478,7 +544,7 @@ __device__ void ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
       cr = dadd<T>(cr, sr[i00 + 17]);
       cr = dmul<T>(cr, T(0.25));
       uc[(int64_t)C * kSS + cx + kS * cy] = cu;
-      push<T>(A, uc, C, A.tr.faces + 4 * C, cx, cy, cu);
+      push<T>(A, item, uc, C, A.tr.faces + 4 * C, cx, cy, cu);
       A.e[(int64_t)C * kSS + cx + kS * cy] = cr;
     }
     slot_sync(slot);
@@ -496,6 +562,8 @@ __device__ void ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int f
   for (int i = first; i < n; i += step) {
     const int4 e = ch[i];
     const int F = e.x, C = e.y;
+    const int item = A.tr.info[F].z >> 8;
+    if (is_frozen(A, item)) continue;
     const int ir = dx & 1, iz = dy & 1;
     const int jr = 2 + 8 * (e.z - 1) + (dx >> 1), jz = 2 + 8 * (e.w - 1) + (dy >> 1);
     const T *cb = A.e + (int64_t)C * kSS;
@@ -507,7 +575,7 @@ __device__ void ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int f
     const T nu = dadd<T>(v, *d);
     *d = nu;
     const int4 *fc = A.tr.faces + 4 * F;
-    push<T>(A, uf, F, fc, x, y, nu);
+    push<T>(A, item, uf, F, fc, x, y, nu);
     if (t < 128) refbnd_ghost<T>(uf, uc, F, fc, t);
   }
 }
@@ -525,11 +593,13 @@ __device__ void ph_update64(const EngArgs<T> &A, int t, int gslot, int gstep) {
     const int4 *blocks = A.tr.lvl_blocks[l - 1];
     // items are numbered across levels so that the work spreads over every slot
     for (int i = (gslot - base % gstep + gstep) % gstep; i < n; i += gstep) {
-      const int X = blocks[i].x;
+      const int4 bk = blocks[i];
+      if (is_frozen(A, item_of(bk))) continue;
+      const int X = bk.x;
       double *d = A.mx.u64 + (int64_t)X * kSS + o;
       const double nv = *d + (double)A.u[(int64_t)X * kSS + o];
       *d = nv;
-      push_f<double>(A.sg, A.mx.u64, X, A.tr.faces + 4 * X, x, y, nv);
+      push_f<double>((unsigned)A.it_sgbits[item_of(bk)], A.mx.u64, X, A.tr.faces + 4 * X, x, y, nv);
     }
     base += n;
   }
@@ -544,10 +614,12 @@ __device__ void ph_restrict64(const EngArgs<T> &A, int l, int t, int gslot, int 
   const int kx = t & 7, ky = t >> 3;
   for (int i = gslot; i < n; i += gstep) {
     const int4 e = ch[i];
+    const int item = A.tr.info[e.y].z >> 8;
+    if (is_frozen(A, item)) continue;
     const double v = restrict4<double>(A.mx.u64 + (int64_t)e.x * kSS, 2 + 2 * kx, 2 + 2 * ky);
     const int cx = 2 + 8 * (e.z - 1) + kx, cy = 2 + 8 * (e.w - 1) + ky;
     A.mx.u64[(int64_t)e.y * kSS + cx + kS * cy] = v;
-    push_f<double>(A.sg, A.mx.u64, e.y, A.tr.faces + 4 * e.y, cx, cy, v);
+    push_f<double>((unsigned)A.it_sgbits[item], A.mx.u64, e.y, A.tr.faces + 4 * e.y, cx, cy, v);
   }
 }
 
@@ -558,122 +630,193 @@ __device__ void ph_refbnd64(const EngArgs<T> &A, int l, int t, int gslot, int gs
   const int4 *blocks = A.tr.lvl_blocks[l - 1];
   if (t >= 128) return;
   for (int i = gslot; i < n; i += gstep) {
-    const int X = blocks[i].x;
-    refbnd_ghost<double>(A.mx.u64, A.mx.u64, X, A.tr.faces + 4 * X, t);
+    const int4 bk = blocks[i];
+    if (is_frozen(A, item_of(bk))) continue;
+    refbnd_ghost<double>(A.mx.u64, A.mx.u64, bk.x, A.tr.faces + 4 * bk.x, t);
   }
 }
 
-// FP64 defect r = -(b + L u64 / s_l) on every valid cell of every level, written as the
-// FP32 right-hand side -r; the FP32 correction is zeroed (ghosts included) and the leaf
-// cells' weighted squares r^2 4^-(l-1) are summed per CTA (fixed order).
+// Leaf sums of squares per norm chunk (up to kNormChunk consecutive blocks of one item
+// and level) at bpart[c]: per thread over the chunk's blocks in order, the warp sums,
+// then the 8 warp sums in order.  A leaf cell of level l is weighted by 4^-(l-1); cells
+// under a child are skipped (resnorm!, src/multigrid.jl:391-417).
+//   defect = false: r = -(b + L u / s_l) of the current iterate u;
+//   defect = true : the FP64 defect r = -(b64 + L u64 / s_l) of the mixed solve, also
+//                   written as the FP32 right-hand side -r, with the FP32 correction
+//                   zeroed (ghosts included).
+// with_b adds the same sums for b (b64 in mixed mode) in bpart_b.
 template <typename T>
-__device__ double ph_defect(const EngArgs<T> &A, int t, int gslot, int gstep) {
+__device__ void ph_blocknorm(const EngArgs<T> &A, bool defect, bool with_b, int t, int slot, int gslot, int gstep,
+                             double *red) {
   const int x = 2 + (t & 15), y = 2 + (t >> 4), o = x + kS * y;
   const int mysub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
-  double acc = 0.0;
-  int base = 0;
-  for (int l = 1; l <= A.lmax; ++l) {
-    const int n = A.tr.nblk[l - 1];
-    const int4 *blocks = A.tr.lvl_blocks[l - 1];
-    const double s = A.mx.lev_s64[l], centre = A.mx.lev_centre64[l];
+  const int lane = t & 31, w8 = t >> 5;
+  int nb = 0;
+  for (int c = gslot; c < A.nchunk; c += gstep) {
+    const int4 ck = A.chunks[c];  // {level, first, count, item}
+    const int item = ck.w;
+    if (is_frozen(A, item)) continue;
+    const int l = ck.x;
+    const int4 *blocks = A.tr.lvl_blocks[l - 1] + ck.y;
     const double wl = 1.0 / (double)((int64_t)1 << (2 * (l - 1)));
-    double accl = 0.0;
-    for (int i = (gslot - base % gstep + gstep) % gstep; i < n; i += gstep) {
-      const int4 bk = blocks[i];
+    double v = 0.0, vb = 0.0;
+    for (int j = 0; j < ck.z; ++j) {
+      const int4 bk = blocks[j];
       const int X = bk.x;
-      const W5<double> w = weights<double>(A.mx.wt64, A.geom, bk.y, bk.z, x, y);
-      const double Lu = apply5<double>(A.mx.u64 + (int64_t)X * kSS, x, y, w, centre);
-      const double r = -(A.mx.b64[(int64_t)X * kSS + o] + Lu / s);
-      A.b[(int64_t)X * kSS + o] = (T)(-r);
-      T *eb = A.u + (int64_t)X * kSS;
-      eb[t] = T(0);
-      if (t < kSS - 256) eb[t + 256] = T(0);
-      if (!((bk.w >> mysub) & 1)) accl = fma(r, r, accl);
+      const bool leaf = !((bk.w >> mysub) & 1);
+      double r, bv;
+      if (!defect) {
+        const T *par = A.it_par + item * kParStride;
+        const W5<T> w = weights<T>(A.wt, A.geom, bk.y, bk.z, x, y);
+        const T Lu = apply5<T>(A.u + (int64_t)X * kSS, x, y, w, par[32 + l]);
+        const T bb = A.b[(int64_t)X * kSS + o];
+        r = (double)(-(bb + Lu / par[l]));
+        bv = (double)bb;
+      } else {
+        const double *par = A.mx.it_par64 + item * kParStride;
+        const W5<double> w = weights<double>(A.mx.wt64, A.geom, bk.y, bk.z, x, y);
+        const double Lu = apply5<double>(A.mx.u64 + (int64_t)X * kSS, x, y, w, par[32 + l]);
+        bv = A.mx.b64[(int64_t)X * kSS + o];
+        r = -(bv + Lu / par[l]);
+        A.b[(int64_t)X * kSS + o] = (T)(-r);
+        T *eb = A.u + (int64_t)X * kSS;
+        eb[t] = T(0);
+        if (t < kSS - 256) eb[t + 256] = T(0);
+      }
+      if (leaf) {
+        v = fma(r, r, v);
+        vb = fma(bv, bv, vb);
+      }
     }
-    acc = fma(accl, wl, acc);
-    base += n;
+    for (int off = 16; off > 0; off >>= 1) {
+      v += __shfl_xor_sync(0xffffffffu, v, off);
+      vb += __shfl_xor_sync(0xffffffffu, vb, off);
+    }
+    // double-buffered per chunk: a buffer is rewritten two chunks later, after the next
+    // slot barrier, which thread 0 reaches only once it has read this one
+    double *rb = red + 16 * (nb & 1);
+    if (lane == 0) {
+      rb[w8] = v;
+      rb[8 + w8] = vb;
+    }
+    slot_sync(slot);
+    if (t == 0) {
+      double sv = 0.0, sb = 0.0;
+      for (int q = 0; q < 8; ++q) {
+        sv += rb[q];
+        sb += rb[8 + q];
+      }
+      A.bpart[c] = sv * wl;
+      if (with_b) A.bpart_b[c] = sb * wl;
+    }
+    ++nb;
   }
-  return acc;
 }
 
-// Leaf-cell weighted sum of r^2, r = -(b + L u / s_l), over every level (the resnorm!
-// norm, src/multigrid.jl:391-417), per slot in a fixed order.
+// Per-item norms from the chunk partials, one CTA (1024 threads) per item, in a fixed
+// order: thread-strided sums over the item's chunk partials, the warp sums, then the
+// 32 warp sums in order.  Writes inorm[4 k + 0] (and with `first` the |b| and
+// initial-norm entries), the item's V-cycle count, and freezes the item once its norm
+// is <= tol * |b| (|b| = 0 counts as 1) or not finite.  Items frozen before are skipped.
 template <typename T>
-__device__ double ph_resnorm(const EngArgs<T> &A, int t, int gslot, int gstep) {
-  const int x = 2 + (t & 15), y = 2 + (t >> 4), o = x + kS * y;
-  const int mysub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
-  double acc = 0.0;
-  int base = 0;
-  for (int l = 1; l <= A.lmax; ++l) {
-    const int n = A.tr.nblk[l - 1];
-    const int4 *blocks = A.tr.lvl_blocks[l - 1];
-    const T s = A.lev_s[l], centre = A.lev_centre[l];
-    const double wl = 1.0 / (double)((int64_t)1 << (2 * (l - 1)));
-    double accl = 0.0;
-    for (int i = (gslot - base % gstep + gstep) % gstep; i < n; i += gstep) {
-      const int4 bk = blocks[i];
-      if ((bk.w >> mysub) & 1) continue;
-      const int X = bk.x;
-      const W5<T> w = weights<T>(A.wt, A.geom, bk.y, bk.z, x, y);
-      const T Lu = apply5<T>(A.u + (int64_t)X * kSS, x, y, w, centre);
-      const double r = (double)(-(A.b[(int64_t)X * kSS + o] + Lu / s));
-      accl = fma(r, r, accl);
+__device__ void ph_itemnorm(const EngArgs<T> &A, bool first, int cycles, double *red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = blockIdx.x; k < A.nitems; k += gridDim.x) {
+    if (A.frozen[k]) continue;
+    double v = 0.0, vb = 0.0;
+    const int2 rg = A.it_chunks[k];
+    for (int j = threadIdx.x; j < rg.y; j += blockDim.x) {
+      v += A.bpart[rg.x + j];
+      if (first) vb += A.bpart_b[rg.x + j];
     }
-    acc = fma(accl, wl, acc);
-    base += n;
+    for (int off = 16; off > 0; off >>= 1) {
+      v += __shfl_xor_sync(0xffffffffu, v, off);
+      vb += __shfl_xor_sync(0xffffffffu, vb, off);
+    }
+    if (lane == 0) {
+      red[warp] = v;
+      red[32 + warp] = vb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double sv = 0.0, sb = 0.0;
+      for (int q = 0; q < 32; ++q) {
+        sv += red[q];
+        sb += red[32 + q];
+      }
+      const double nrm = sqrt(sv);
+      double *io = A.inorm + 4 * k;
+      if (first) {
+        io[1] = sqrt(sb);
+        io[2] = nrm;
+      }
+      io[0] = nrm;
+      io[3] = (double)cycles;
+      const double bn = io[1] > 0.0 ? io[1] : 1.0;
+      if (!(nrm > A.tol * bn) || !isfinite(nrm)) A.frozen[k] = 1;
+    }
+    __syncthreads();
   }
-  return acc;
 }
 
-// Coarsest level solved directly (mixed-precision solve): FAS right-hand side of the
-// covered cells, then u_1 = P b_1 with P = -s A_1^{-1} applied in FP64, ghosts pushed,
-// and the correction e = u_1 - u1 of the level.  CTA 0 only; level 1 has <= 4 blocks.
+// Coarsest level solved directly (mixed-precision solve), one item per CTA: FAS
+// right-hand side of the covered cells, then u_1 = P b_1 with the item's
+// P = -s A_1^{-1} applied in FP64 (one warp per row), ghosts pushed, and the
+// correction e = u_1 - u1 of the level.  An item's level 1 has <= 4 blocks.
 template <typename T>
-__device__ void ph_direct_top(const EngArgs<T> &A, T *u, bool make_e, int t, int slot, double *sol) {
-  const int n1 = A.tr.nblk[0];
-  const int4 *blocks = A.tr.lvl_blocks[0];
+__device__ void ph_direct_top(const EngArgs<T> &A, T *u, bool make_e, int first, int step, int t, int slot,
+                              double *sol) {
   const int x = 2 + (t & 15), y = 2 + (t >> 4);
   const int o = x + kS * y;
   const int mysub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
-  const T s = A.lev_s[1], centre = A.lev_centre[1];
-  if (slot < n1) {
-    const int4 bk = blocks[slot];
-    const int X = bk.x;
-    const T uo = u[(int64_t)X * kSS + o];
-    A.u1[(int64_t)X * kSS + o] = uo;
-    if ((bk.w >> mysub) & 1) {
-      const W5<T> w = weights<T>(A.wt, A.geom, bk.y, bk.z, x, y);
-      const T Lu = apply5<T>(u + (int64_t)X * kSS, x, y, w, centre);
-      A.b[(int64_t)X * kSS + o] = -(A.e[(int64_t)X * kSS + o] + Lu / s);
+  for (int k = first; k < A.nitems; k += step) {
+    if (is_frozen(A, k)) continue;
+    const int2 rg = A.it_lrange[k * A.nlev_tab];
+    const int n1 = rg.y;
+    const int4 *blocks = A.tr.lvl_blocks[0] + rg.x;
+    const T *par = A.it_par + k * kParStride;
+    const T s = par[1], centre = par[32 + 1];
+    if (slot < n1) {
+      const int4 bk = blocks[slot];
+      const int X = bk.x;
+      const T uo = u[(int64_t)X * kSS + o];
+      A.u1[(int64_t)X * kSS + o] = uo;
+      if ((bk.w >> mysub) & 1) {
+        const W5<T> w = weights<T>(A.wt, A.geom, bk.y, bk.z, x, y);
+        const T Lu = apply5<T>(u + (int64_t)X * kSS, x, y, w, centre);
+        A.b[(int64_t)X * kSS + o] = -(A.e[(int64_t)X * kSS + o] + Lu / s);
+      }
     }
-  }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const int n = A.coarse_n;
-  for (int q = warp; q < n; q += nw) {
-    const double *pr = A.coarse_P + (int64_t)q * n;
-    double acc = 0.0;
-    for (int j = lane; j < n; j += 32) {
-      const int c = j & 255;
-      const int X = blocks[j >> 8].x;
-      acc = fma(pr[j], (double)A.b[(int64_t)X * kSS + (2 + (c & 15)) + kS * (2 + (c >> 4))], acc);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int n = 256 * n1;
+    const double *P = A.it_P[k];
+    for (int q = warp; q < n; q += nw) {
+      const double *pr = P + (int64_t)q * n;
+      double acc = 0.0;
+      for (int j = lane; j < n; j += 32) {
+        const int c = j & 255;
+        const int X = blocks[j >> 8].x;
+        acc = fma(pr[j], (double)A.b[(int64_t)X * kSS + (2 + (c & 15)) + kS * (2 + (c >> 4))], acc);
+      }
+      for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+      if (lane == 0) sol[q] = acc;
     }
-    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-    if (lane == 0) sol[q] = acc;
-  }
-  __syncthreads();
-  if (slot < n1) {
-    const int4 bk = blocks[slot];
-    const int X = bk.x;
-    const int4 *fc = A.tr.faces + 4 * X;
-    const T nu = (T)sol[slot * 256 + (t & 255)];
-    u[(int64_t)X * kSS + o] = nu;
-    push<T>(A, u, X, fc, x, y, nu);
-    if (make_e) {
-      const T ev = nu - A.u1[(int64_t)X * kSS + o];
-      A.e[(int64_t)X * kSS + o] = ev;
-      push<T>(A, A.e, X, fc, x, y, ev);
+    __syncthreads();
+    if (slot < n1) {
+      const int4 bk = blocks[slot];
+      const int X = bk.x;
+      const int4 *fc = A.tr.faces + 4 * X;
+      const T nu = (T)sol[slot * 256 + (t & 255)];
+      u[(int64_t)X * kSS + o] = nu;
+      push<T>(A, k, u, X, fc, x, y, nu);
+      if (make_e) {
+        const T ev = nu - A.u1[(int64_t)X * kSS + o];
+        A.e[(int64_t)X * kSS + o] = ev;
+        push<T>(A, k, A.e, X, fc, x, y, ev);
+      }
     }
+    __syncthreads();
   }
 }
 
@@ -683,7 +826,9 @@ __device__ void ph_copy_back(const EngArgs<T> &A, int l, const T *src, T *dst, i
   const int n = A.tr.nblk[l - 1];
   const int4 *blocks = A.tr.lvl_blocks[l - 1];
   for (int i = first; i < n; i += step) {
-    const int X = blocks[i].x;
+    const int4 bk = blocks[i];
+    if (is_frozen(A, item_of(bk))) continue;
+    const int X = bk.x;
     for (int k = t; k < kSS; k += 256) {
       const int x = k % kS, y = k / kS;
       const bool corner = (x < 2 || x > 17) && (y < 2 || y > 17);
@@ -762,27 +907,22 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
   }
 
   const int gslot = blockIdx.x * nslots + slot, gstep = gridDim.x * nslots;
-  // Fixed-order grid reduction (warps, CTA, then every CTA sums all CTA partials in the
-  // same order), so every CTA takes the same decision from the same norm.
-  __shared__ double s_nrm;
-  auto grid_norm = [&](double part, bool &ok) -> double {
-    double v = part;
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-    if ((threadIdx.x & 31) == 0) s_direct[threadIdx.x >> 5] = v;
-    __syncthreads();
+  // Norm step: per-block partials, barrier, per-item sums and freezing, barrier.
+  auto norm_step = [&](bool defect, bool first, int ncyc) -> bool {
+    ph_blocknorm<T>(A, defect, first, t, slot, gslot, gstep, reinterpret_cast<double *>(&S.tile[0][0]));
+    if (!sync(true, false, false)) return false;
+    ph_itemnorm<T>(A, first, ncyc, s_direct);
+    return sync(true, false, false);
+  };
+  __shared__ int s_live;
+  auto any_live = [&]() -> bool {
     if (threadIdx.x == 0) {
-      double c = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) c += s_direct[w];
-      A.part[blockIdx.x] = c;
-    }
-    ok = sync(true, false, false);
-    if (threadIdx.x == 0) {
-      double tot = 0.0;
-      for (int c = 0; c < (int)gridDim.x; ++c) tot += *((volatile double *)A.part + c);
-      s_nrm = sqrt(tot);
+      int live = 0;
+      for (int k = 0; k < A.nitems && !live; ++k) live = *((volatile int *)A.frozen + k) == 0;
+      s_live = live;
     }
     __syncthreads();
-    return s_nrm;
+    return s_live != 0;
   };
 
   // One FAS V-cycle (src/multigrid.jl:60-106) on the current fields.
@@ -803,9 +943,10 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
       if (!sync(true, loc, (l - 1) <= K)) return false;
     }
     // coarsest level
-    if (A.coarse_P) {
-      if (cta0) ph_direct_top<T>(A, fld(1), L > 1, t, slot, s_direct);
-      if (!sync(true, 1 <= K, 2 <= K || L < 2)) return false;
+    if (A.it_P) {
+      const bool loc = 1 <= K;
+      if (runs(loc)) ph_direct_top<T>(A, fld(1), L > 1, loc ? 0 : blockIdx.x, loc ? 1 : gridDim.x, t, slot, s_direct);
+      if (!sync(true, loc, 2 <= K || L < 2)) return false;
     } else {
       const bool loc = 1 <= K;
       for (int it = 0; it < A.ntop; ++it) {
@@ -848,18 +989,11 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
   };
 
   const bool mixed = A.mx.u64 != nullptr;
-  const bool loop = A.max_cycles > 0;
+  const bool loop = A.max_cycles > 0;  // without it: one V-cycle (vcycle!), no norms
   int cycles = 0;
-  double nrm = -1.0, nrm0 = -1.0;
-  bool conv = false;
-  if (!mixed && loop) {
-    bool ok;
-    nrm = nrm0 = grid_norm(ph_resnorm<T>(A, t, gslot, gstep), ok);
-    if (!ok) return;
-    conv = !(nrm > A.tol_abs);
-  }
+  if (loop && !mixed && !norm_step(false, true, 0)) return;
   for (int iter = 0;; ++iter) {
-    if (mixed) {
+    if (loop && mixed) {
       // FP64 side of a defect-correction step
       if (A.mx.apply_update || iter > 0) {
         ph_update64<T>(A, t, gslot, gstep);
@@ -874,29 +1008,15 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
           ph_refbnd64<T>(A, l, t, gslot, gstep);
           if (!sync(true, false, false)) return;
         }
-      bool ok;
-      nrm = grid_norm(ph_defect<T>(A, t, gslot, gstep), ok);
-      if (!ok) return;
-      if (iter == 0) nrm0 = nrm;
-      conv = !(nrm > A.tol_abs);
+      if (!norm_step(true, iter == 0, cycles)) return;
     }
-    if (conv || (!isfinite(nrm) && nrm != -1.0) || (loop && cycles >= A.max_cycles)) break;
+    if (loop && (!any_live() || cycles >= A.max_cycles)) break;
     if (!vcycle_body()) return;
     cycles++;
-    if (!mixed && loop) {
-      bool ok;
-      nrm = grid_norm(ph_resnorm<T>(A, t, gslot, gstep), ok);
-      if (!ok) return;
-      conv = !(nrm > A.tol_abs);
-    }
     if (!loop) break;
+    if (!mixed && !norm_step(false, false, cycles)) return;
   }
-  if (A.out && cta0 && threadIdx.x == 0) {
-    A.out[0] = nrm;
-    A.out[1] = conv ? 1.0 : 0.0;
-    A.out[2] = (double)cycles;
-    A.out[3] = nrm0;
-  }
+  if (loop && A.out && cta0 && threadIdx.x == 0) A.out[0] = (double)cycles;
   if (A.trace && cta0 && threadIdx.x == 0 && ntrace < kTraceMax) A.trace[ntrace] = 0;
 }
 

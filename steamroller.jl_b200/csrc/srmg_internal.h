@@ -1,5 +1,8 @@
 // srmg_internal.h -- internal helpers shared by the library's translation units.
 #pragma once
+#include <initializer_list>
+#include <vector>
+
 #include "srmg_ctx.h"
 
 namespace srmg {
@@ -9,6 +12,12 @@ int cuda_check(srmg_ctx *c, cudaError_t e, const char *what);
 int ensure(srmg_ctx *ctx, DevBuf &b, size_t bytes);
 int check_call(srmg_ctx *ctx, int64_t nblk_alloc, int op, int geom, const int8_t *bc);
 Signs make_signs(const int8_t *bc);
+std::vector<int8_t> bc_of(const Signs &sg);
+int build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_pair *const *pairs,
+               const int64_t *nnb, const srmg_neighbor *const *nb, const int64_t *nbd,
+               const srmg_boundary *const *bd, const int64_t *nrb, const srmg_refbnd *const *rb,
+               const int64_t *nch, const srmg_child *const *ch, uint64_t generation,
+               const std::vector<int> *item_of, int nitems);
 double level_scale(double s, int l);
 
 template <typename T>
@@ -33,24 +42,53 @@ int leafnorm_dev(srmg_ctx *ctx, const T *u, const T *b, double s, int op, double
 int read_small(srmg_ctx *ctx, int n);
 
 int engine_local_top(srmg_ctx *ctx, int lmax);
+
+// Device tables of the items' operators, uploaded by prepare_items.
+struct ItemTabs {
+  const double *par64 = nullptr;     // per item kParStride FP64 values
+  const float *par32 = nullptr;      // per item kParStride FP32 values
+  const int *sgbits = nullptr;       // per item: boundary table, entry k as (bc_k + 1) << 2k
+  const double *const *P = nullptr;  // per item direct coarsest-level inverse, or null
+  const double *P0 = nullptr;        // item 0's inverse (per-operation kernels)
+  int n0 = 0;                        // its unknowns
+};
+// Upload the per-item tables for operators `specs` (ctx->nitems entries).  With
+// smooth_level > 0 the level's entries use the scale smooth_sl instead of s_l.  With
+// want_P the coarsest-level inverse of every item is prepared (cached); tabs->P stays
+// null when some item's level 1 has more than 4 blocks or its operator is singular.
+int prepare_items(srmg_ctx *ctx, const ItemSpec *specs, int geom, double omega, bool want_P,
+                  int smooth_level, double smooth_sl, ItemTabs *tabs);
+// The same operator for every item.
+std::vector<ItemSpec> uniform_items(srmg_ctx *ctx, double s, int op, double k2, const int8_t *bc);
+
 // Optional parts of a persistent-engine launch.
 struct EngineRun {
-  const double *coarse_P = nullptr;  // FP64 direct solve of the coarsest level
-  int coarse_n = 0;
+  bool direct = false;               // FP64 direct solve of the coarsest level (tabs.P)
   double *u64 = nullptr;             // mixed precision: FP64 iterate and right-hand side
   const double *b64 = nullptr;
   int apply_update = 0;
-  int max_cycles = 0;                // > 0: device-side loop until the norm <= tol_abs
-  double tol_abs = 0.0;
+  int max_cycles = 0;                // > 0: device-side loop until every item has converged
+  double tol = 0.0;                  // relative to each item's leaf norm of b
 };
 template <typename T>
-int engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, double s, int op, double k2, int geom,
-                  const Signs &sg, int lmax, int ndown, int ntop, int nup, double omega,
-                  const EngineRun *run = nullptr);
+int engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, const ItemTabs &tabs, int geom, int lmax,
+                  int ndown, int ntop, int nup, const EngineRun *run = nullptr);
 int engine_check(srmg_ctx *ctx);
 template <typename T>
-int engine_smooth(srmg_ctx *ctx, T *u, const T *b, int level, double omega, double sl, int n, int op,
-                  double k2, int geom, const Signs &sg);
+int engine_smooth(srmg_ctx *ctx, T *u, const T *b, const ItemTabs &tabs, int geom, int level, int n);
+// Copy the per-item results of the last device loop ({norm, |b|, initial, cycles} per
+// item, then the launch's V-cycle count) to ctx->h_items and check the error word.
+int read_items(srmg_ctx *ctx);
+int items_host_reserve(srmg_ctx *ctx);  // the pinned mirror (read_items calls it)
+int items_d2h(srmg_ctx *ctx);           // the copy alone, stream-ordered
+bool engine_ok(srmg_ctx *ctx, const srmg_solve_opts *o, std::initializer_list<const void *> ptrs);
+int solve_reserve(srmg_ctx *ctx, int64_t nblk_alloc, int mode);
+int solve_enqueue(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, const ItemTabs &tabs, int geom,
+                  const srmg_solve_opts *o);
+void items_stats(srmg_ctx *ctx, const srmg_solve_opts *o, srmg_stats *st);
+// Tolerance-driven solve of every item of the context (statistics per item in st).
+int solve_items(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, const ItemSpec *specs,
+                int geom, const srmg_solve_opts *opts, srmg_stats *st);
 int stage_in(srmg_ctx *ctx, int slot, const double *h, int64_t nblk_alloc, double **d);
 int stage_out(srmg_ctx *ctx, double *h, const double *d, int64_t nblk_alloc);
 

@@ -19,6 +19,12 @@ constexpr int kM = 16;
 constexpr int kG = 2;
 constexpr int kS = kM + 2 * kG;
 constexpr int kSS = kS * kS;
+// Per-item operator table of the persistent engine: s_l [32], stencil centre_l [32] and
+// -(omega / diagonal)_l [32], indexed by level l.
+constexpr int kParStride = 96;
+// Blocks per norm chunk: the leaf norms are summed per chunk of up to this many
+// consecutive blocks of one item and level, then per item over its chunks.
+constexpr int kNormChunk = 4;
 
 // Face numbering (the four StarStencil directions): 0 = -r, 1 = +r, 2 = -z, 3 = +z.
 enum FaceType : int { FACE_NONE = 0, FACE_NEIGHBOR = 1, FACE_BOUNDARY = 2, FACE_REFBND = 3 };

@@ -106,117 +106,11 @@ int grid_for(int64_t work, int threads, int cap) {
   return (int)g;
 }
 
-// Gauss-Jordan inverse with partial pivoting (n <= 1024).  Returns false if singular.
-bool invert(std::vector<double> &a, int n) {
-  std::vector<double> inv((size_t)n * n, 0.0);
-  for (int i = 0; i < n; i++) inv[(size_t)i * n + i] = 1.0;
-  for (int c = 0; c < n; c++) {
-    int piv = c;
-    double best = std::fabs(a[(size_t)c * n + c]);
-    for (int r = c + 1; r < n; r++) {
-      const double v = std::fabs(a[(size_t)r * n + c]);
-      if (v > best) { best = v; piv = r; }
-    }
-    if (best < 1e-300) return false;
-    if (piv != c)
-      for (int k = 0; k < n; k++) {
-        std::swap(a[(size_t)c * n + k], a[(size_t)piv * n + k]);
-        std::swap(inv[(size_t)c * n + k], inv[(size_t)piv * n + k]);
-      }
-    const double d = 1.0 / a[(size_t)c * n + c];
-    for (int k = 0; k < n; k++) {
-      a[(size_t)c * n + k] *= d;
-      inv[(size_t)c * n + k] *= d;
-    }
-    for (int r = 0; r < n; r++) {
-      if (r == c) continue;
-      const double f = a[(size_t)r * n + c];
-      if (f == 0.0) continue;
-      for (int k = 0; k < n; k++) {
-        a[(size_t)r * n + k] -= f * a[(size_t)c * n + k];
-        inv[(size_t)r * n + k] -= f * inv[(size_t)c * n + k];
-      }
-    }
-  }
-  a.swap(inv);
-  return true;
-}
-
-// Assemble the level-1 operator (ghosts resolved through copies and mirrors), invert
-// it and upload P = -s A^{-1}.  Cached by (s, op, k2, geom, bc, tree generation).
-int prepare_coarse(srmg_ctx *ctx, double s, int op, double k2, int geom, const int8_t *bc) {
-  std::vector<double> key = {s, (double)op, k2, (double)geom, (double)ctx->generation};
-  for (int i = 0; i < 9; i++) key.push_back(bc ? bc[i] : 1);
-  if (ctx->coarse_key == key) return SRMG_OK;
-  ctx->coarse_key = key;
-  ctx->coarse_ok = false;
-  const int nb = ctx->nblk_host[0];
-  const int n = nb * 256;
-  if (nb < 1 || n > 1024) return SRMG_OK;  // fall back to smoothing at the top
-  std::vector<int4> blocks(nb), faces(4 * nb);
-  CK(cudaMemcpy(blocks.data(), ctx->lv[0].blocks, nb * sizeof(int4), cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(faces.data(), ctx->lv[0].faces, 4 * nb * sizeof(int4), cudaMemcpyDeviceToHost));
-  std::vector<int> slot_of(ctx->max_blk + 1, -1);
-  for (int i = 0; i < nb; i++) slot_of[blocks[i].x] = i;
-  std::vector<double> A((size_t)n * n, 0.0);
-  const double centre = (op == SRMG_OP_HELMHOLTZ) ? (-4.0 - s * k2) : -4.0;
-  static const int sidx[4] = {3, 5, 1, 7};
-  for (int bi = 0; bi < nb; bi++) {
-    for (int y = 2; y < 18; y++)
-      for (int x = 2; x < 18; x++) {
-        const int row = bi * 256 + (y - 2) * 16 + (x - 2);
-        double wzm = 1, wrm = 1, wrp = 1, wzp = 1;
-        if (geom == 1) {
-          const int64_t i = x - 1 + 16 * (int64_t)(blocks[bi].y - 1);
-          wrm = (double)(2 * i - 2) / (double)(2 * i - 1);
-          wrp = (double)(2 * i) / (double)(2 * i - 1);
-        } else if (geom == 2) {
-          const int64_t j = y - 1 + 16 * (int64_t)(blocks[bi].z - 1);
-          wzm = (double)(2 * j - 2) / (double)(2 * j - 1);
-          wzp = (double)(2 * j) / (double)(2 * j - 1);
-        }
-        A[(size_t)row * n + row] += centre;
-        const int nx[4] = {x - 1, x + 1, x, x};
-        const int ny[4] = {y, y, y - 1, y + 1};
-        const double wv[4] = {wrm, wrp, wzm, wzp};
-        for (int q = 0; q < 4; q++) {
-          int cx = nx[q], cy = ny[q];
-          double coef = wv[q];
-          int cb = bi;
-          if (cx < 2 || cx > 17 || cy < 2 || cy > 17) {
-            const int f = q;  // the face crossed: 0 -r, 1 +r, 2 -z, 3 +z
-            const int4 fi = faces[4 * bi + f];
-            if (fi.x == FACE_NEIGHBOR) {
-              cb = slot_of[fi.y];
-              if (cb < 0) return SRMG_OK;
-              if (f == 0) cx += 16; else if (f == 1) cx -= 16; else if (f == 2) cy += 16; else cy -= 16;
-            } else if (fi.x == FACE_BOUNDARY) {
-              coef *= (bc ? (double)bc[sidx[f]] : 1.0);
-              if (f == 0) cx = 3 - cx; else if (f == 1) cx = 35 - cx;
-              else if (f == 2) cy = 3 - cy; else cy = 35 - cy;
-            } else {
-              return SRMG_OK;  // refinement boundary at level 1 cannot happen
-            }
-          }
-          const int col = cb * 256 + (cy - 2) * 16 + (cx - 2);
-          A[(size_t)row * n + col] += coef;
-        }
-      }
-  }
-  if (!invert(A, n)) return SRMG_OK;
-  for (auto &v : A) v *= -s;
-  RC(ensure(ctx, ctx->coarse_inv, A.size() * sizeof(double)));
-  CK(cudaMemcpy(ctx->coarse_inv.p, A.data(), A.size() * sizeof(double), cudaMemcpyHostToDevice));
-  ctx->coarse_n = n;
-  ctx->coarse_ok = true;
-  return SRMG_OK;
-}
-
 // FP32 V-cycle with the FP64 direct coarsest-level solve (when available), on the
 // per-operation kernels (used when the persistent engine is switched off).  Same
 // structure as the reference V-cycle; only the top changes.
 int vcycle_mixed(srmg_ctx *ctx, float *e, float *b, float *r, float *u1, double s, int op, double k2,
-                 int geom, const Signs &sg, int ndown, int ntop, int nup, double omega) {
+                 int geom, const Signs &sg, int ndown, int ntop, int nup, double omega, const ItemTabs &tabs) {
   const int lmax = ctx->nlev;
   for (int l = lmax; l >= 2; l--) {
     if (ctx->nblk_host[l - 1] == 0) continue;
@@ -231,10 +125,9 @@ int vcycle_mixed(srmg_ctx *ctx, float *e, float *b, float *r, float *u1, double 
     RC(L_restrict<float>(ctx, r, l));
     RC(L_postrestrict<float>(ctx, b, e, r, l, pc));
   }
-  if (ctx->coarse_ok) {
-    const int n = ctx->coarse_n;
-    k_coarse_direct<<<(n + 7) / 8, 256, 0, ctx->stream>>>(e, b, (const double *)ctx->coarse_inv.p,
-                                                          ctx->lv[0].view(1), n);
+  if (tabs.P0) {
+    const int n = tabs.n0;
+    k_coarse_direct<<<(n + 7) / 8, 256, 0, ctx->stream>>>(e, b, tabs.P0, ctx->lv[0].view(1), n);
     ctx->launches++;
     RC(L_fill_ghost<float>(ctx, e, 1, sg, 3));
   } else {
@@ -308,39 +201,88 @@ extern "C" void srmg_solve_opts_default(srmg_solve_opts *o) {
   o->warm_start = 0;
 }
 
-static int solve_fp64(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, double s, int op,
-                      double k2, int geom, const int8_t *bc, const srmg_solve_opts *o,
-                      srmg_stats *st) {
-  const Signs sg = make_signs(bc);
-  const size_t bytes = (size_t)nblk_alloc * kSS * sizeof(double);
-  RC(ensure(ctx, ctx->f64[4], bytes));
-  RC(ensure(ctx, ctx->f64[2], bytes));
-  RC(ensure(ctx, ctx->f64[3], bytes));
+// Per-item statistics from the device loop's results (read_items).
+static void item_stats(srmg_ctx *ctx, int k, srmg_stats *st) {
+  const double *io = ctx->h_items + 4 * k;
+  const double bn = io[1] > 0 ? io[1] : 1.0;
+  st->bnorm = io[1];
+  st->rel_residual = io[0] / bn;
+  st->initial_rel = io[2] / bn;
+  st->cycles = (int)io[3];
+  st->status = std::isfinite(st->rel_residual) ? SRMG_OK : SRMG_ERR_DIVERGED;
+}
+
+bool srmg::engine_ok(srmg_ctx *ctx, const srmg_solve_opts *o, std::initializer_list<const void *> ptrs) {
+  uintptr_t a = 0;
+  for (const void *p : ptrs) a |= reinterpret_cast<uintptr_t>(p);
+  return ctx->use_engine && (a & 15) == 0 && o->ndown >= 1 && o->ntop >= 1 && o->nup >= 1 && ctx->nlev <= 30;
+}
+
+// Work buffers of a solve (allocated before any capture: nothing allocates later).
+int srmg::solve_reserve(srmg_ctx *ctx, int64_t nblk_alloc, int mode) {
+  if (mode == SRMG_MODE_FP64) {
+    const size_t bytes = (size_t)nblk_alloc * kSS * sizeof(double);
+    for (int i : {2, 3, 4}) RC(ensure(ctx, ctx->f64[i], bytes));
+  } else {
+    const size_t b32 = (size_t)nblk_alloc * kSS * sizeof(float);
+    for (int i = 0; i < 4; i++) RC(ensure(ctx, ctx->f32[i], b32));
+  }
+  return SRMG_OK;
+}
+
+// The engine solve of every item, enqueued on the stream without any host
+// synchronisation (so that it can be captured); read_items / items_stats finish it.
+int srmg::solve_enqueue(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, const ItemTabs &tabs,
+                        int geom, const srmg_solve_opts *o) {
+  RC(solve_reserve(ctx, nblk_alloc, o->mode));
+  EngineRun run;
+  run.max_cycles = std::max(1, o->max_cycles);
+  run.tol = o->tol;
+  if (o->mode == SRMG_MODE_FP64) {
+    const size_t bytes = (size_t)nblk_alloc * kSS * sizeof(double);
+    double *bw = (double *)ctx->f64[4].p, *r = (double *)ctx->f64[2].p, *u1 = (double *)ctx->f64[3].p;
+    CK(cudaMemcpyAsync(bw, b, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    return engine_vcycle<double>(ctx, u, bw, u1, r, tabs, geom, 0, o->ndown, o->ntop, o->nup, &run);
+  }
+  const size_t b32 = (size_t)nblk_alloc * kSS * sizeof(float);
+  float *e = (float *)ctx->f32[0].p, *be = (float *)ctx->f32[1].p, *r = (float *)ctx->f32[2].p,
+        *u1 = (float *)ctx->f32[3].p;
+  CK(cudaMemsetAsync(r, 0, b32, ctx->stream));
+  CK(cudaMemsetAsync(u1, 0, b32, ctx->stream));
+  run.direct = true;
+  run.u64 = u;
+  run.b64 = b;
+  return engine_vcycle<float>(ctx, e, be, u1, r, tabs, geom, 0, o->ndown, o->ntop, o->nup, &run);
+}
+
+void srmg::items_stats(srmg_ctx *ctx, const srmg_solve_opts *o, srmg_stats *st) {
+  for (int k = 0; k < ctx->nitems; k++) {
+    item_stats(ctx, k, &st[k]);
+    if (o->mode == SRMG_MODE_MIXED) st[k].outer = st[k].cycles;
+  }
+}
+
+// FP64 solve of every item: the whole tolerance loop in one persistent launch.
+static int solve_fp64(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, const ItemSpec *specs,
+                      int geom, const srmg_solve_opts *o, srmg_stats *st) {
+  RC(solve_reserve(ctx, nblk_alloc, SRMG_MODE_FP64));
   double *bw = (double *)ctx->f64[4].p, *r = (double *)ctx->f64[2].p, *u1 = (double *)ctx->f64[3].p;
-  CK(cudaMemcpyAsync(bw, b, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
-  RC(leafnorm_dev<double>(ctx, u, b, s, op, k2, geom, 1, 1));
-  const bool aligned = ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(bw) |
-                         reinterpret_cast<uintptr_t>(r) | reinterpret_cast<uintptr_t>(u1)) & 15) == 0;
-  if (ctx->use_engine && aligned && o->ndown >= 1 && o->ntop >= 1 && o->nup >= 1 && ctx->nlev <= 30) {
-    // the whole tolerance loop in one persistent launch
-    RC(read_small(ctx, 2));
-    const double bn = ctx->h_small[1] > 0 ? ctx->h_small[1] : 1.0;
-    st->bnorm = ctx->h_small[1];
-    EngineRun run;
-    run.max_cycles = std::max(1, o->max_cycles);
-    run.tol_abs = o->tol * bn;
-    RC(engine_vcycle<double>(ctx, u, bw, u1, r, s, op, k2, geom, sg, 0, o->ndown, o->ntop, o->nup, o->omega,
-                             &run));
-    RC(read_small(ctx, 12));
-    const double *out = ctx->h_small + 8;
-    st->rel_residual = out[0] / bn;
-    st->initial_rel = out[3] / bn;
-    st->cycles = (int)out[2];
-    if (!std::isfinite(st->rel_residual))
-      return fail(ctx, SRMG_ERR_DIVERGED, "residual is not finite after %d cycles", st->cycles);
+  if (engine_ok(ctx, o, {u, b, bw, r, u1})) {
+    ItemTabs tabs;
+    RC(prepare_items(ctx, specs, geom, o->omega, false, 0, 0.0, &tabs));
+    RC(solve_enqueue(ctx, u, b, nblk_alloc, tabs, geom, o));
+    RC(read_items(ctx));
+    items_stats(ctx, o, st);
     return SRMG_OK;
   }
-  RC(leafnorm_dev<double>(ctx, u, bw, s, op, k2, geom, 0, 0));
+  const size_t bytes = (size_t)nblk_alloc * kSS * sizeof(double);
+  CK(cudaMemcpyAsync(bw, b, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  // per-operation kernels, host loop (one item)
+  if (ctx->nitems != 1) return fail(ctx, SRMG_ERR_UNSUPPORTED, "batched solves need the persistent engine");
+  const ItemSpec &sp = specs[0];
+  const Signs sg = make_signs(sp.bc);
+  RC(leafnorm_dev<double>(ctx, u, b, sp.s, sp.op, sp.k2, geom, 1, 1));
+  RC(leafnorm_dev<double>(ctx, u, bw, sp.s, sp.op, sp.k2, geom, 0, 0));
   RC(read_small(ctx, 2));
   const double bn = ctx->h_small[1] > 0 ? ctx->h_small[1] : 1.0;
   st->bnorm = ctx->h_small[1];
@@ -348,15 +290,17 @@ static int solve_fp64(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_al
   st->initial_rel = rel;
   int c = 0;
   while (rel > o->tol && c < o->max_cycles) {
-    RC(vcycle_dev<double>(ctx, u, bw, r, u1, s, op, k2, geom, sg, 0, o->ndown, o->ntop, o->nup, o->omega));
+    RC(vcycle_dev<double>(ctx, u, bw, r, u1, sp.s, sp.op, sp.k2, geom, sg, 0, o->ndown, o->ntop, o->nup,
+                          o->omega));
     c++;
-    RC(leafnorm_dev<double>(ctx, u, bw, s, op, k2, geom, 0, 0));
+    RC(leafnorm_dev<double>(ctx, u, bw, sp.s, sp.op, sp.k2, geom, 0, 0));
     RC(read_small(ctx, 1));
     const double nrel = ctx->h_small[0] / bn;
     if (!std::isfinite(nrel)) {
       st->cycles = c;
       st->rel_residual = nrel;
-      return fail(ctx, SRMG_ERR_DIVERGED, "residual is not finite after %d cycles", c);
+      st->status = SRMG_ERR_DIVERGED;
+      return SRMG_OK;
     }
     rel = nrel;
   }
@@ -365,55 +309,33 @@ static int solve_fp64(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_al
   return SRMG_OK;
 }
 
-// The whole mixed-precision solve in one persistent launch: every defect-correction
-// step (FP64 update, composite consistency, FP64 defect and its leaf norm, FP32 V-cycle
-// with the FP64 direct coarsest-level solve) runs on the device until the defect norm
-// is <= tol * leafnorm(b).
-static int solve_mixed_engine(srmg_ctx *ctx, double *u, const double *b, double s, int op, double k2,
-                              int geom, const int8_t *bc, const srmg_solve_opts *o, srmg_stats *st,
-                              float *e, float *be, float *r, float *u1, double bn) {
-  const Signs sg = make_signs(bc);
-  EngineRun run;
-  run.coarse_P = ctx->coarse_ok ? (const double *)ctx->coarse_inv.p : nullptr;
-  run.coarse_n = ctx->coarse_ok ? ctx->coarse_n : 0;
-  run.u64 = u;
-  run.b64 = b;
-  run.apply_update = 0;
-  run.max_cycles = std::max(1, o->max_cycles);
-  run.tol_abs = o->tol * bn;
-  RC(engine_vcycle<float>(ctx, e, be, u1, r, s, op, k2, geom, sg, 0, o->ndown, o->ntop, o->nup, o->omega,
-                          &run));
-  RC(read_small(ctx, 12));
-  const double *out = ctx->h_small + 8;
-  st->rel_residual = out[0] / bn;
-  st->initial_rel = out[3] / bn;
-  st->cycles = (int)out[2];
-  st->outer = (int)out[2];
-  if (!std::isfinite(st->rel_residual))
-    return fail(ctx, SRMG_ERR_DIVERGED, "mixed solve: defect norm is not finite after %d steps", st->cycles);
-  return SRMG_OK;
-}
-
-static int solve_mixed(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, double s, int op,
-                       double k2, int geom, const int8_t *bc, const srmg_solve_opts *o,
-                       srmg_stats *st) {
-  const Signs sg = make_signs(bc);
+// Mixed-precision solve of every item.  With the engine, every defect-correction step
+// (FP64 update, composite consistency, FP64 defect and its leaf norm, FP32 V-cycle
+// with the FP64 direct coarsest-level solve) runs in one persistent launch until each
+// item's defect norm is <= tol * leafnorm(b).
+static int solve_mixed(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, const ItemSpec *specs,
+                       int geom, const srmg_solve_opts *o, srmg_stats *st) {
+  ItemTabs tabs;
+  RC(prepare_items(ctx, specs, geom, o->omega, true, 0, 0.0, &tabs));
+  if (engine_ok(ctx, o, {u, b})) {
+    RC(solve_enqueue(ctx, u, b, nblk_alloc, tabs, geom, o));
+    RC(read_items(ctx));
+    items_stats(ctx, o, st);
+    return SRMG_OK;
+  }
+  RC(solve_reserve(ctx, nblk_alloc, SRMG_MODE_MIXED));
   const size_t b32 = (size_t)nblk_alloc * kSS * sizeof(float);
-  for (int i = 0; i < 4; i++) RC(ensure(ctx, ctx->f32[i], b32));
   float *e = (float *)ctx->f32[0].p, *be = (float *)ctx->f32[1].p, *r = (float *)ctx->f32[2].p,
         *u1 = (float *)ctx->f32[3].p;
   CK(cudaMemsetAsync(r, 0, b32, ctx->stream));
   CK(cudaMemsetAsync(u1, 0, b32, ctx->stream));
-  RC(prepare_coarse(ctx, s, op, k2, geom, bc));
+  // per-operation kernels, host loop (one item)
+  if (ctx->nitems != 1) return fail(ctx, SRMG_ERR_UNSUPPORTED, "batched solves need the persistent engine");
+  const ItemSpec &sp = specs[0];
+  const double s = sp.s, k2 = sp.k2;
+  const int op = sp.op;
+  const Signs sg = make_signs(sp.bc);
   RC(leafnorm_dev<double>(ctx, u, b, s, op, k2, geom, 1, 1));
-  const bool aligned = ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(b)) & 15) == 0;
-  if (ctx->use_engine && aligned && o->ndown >= 1 && o->nup >= 1 && o->ntop >= 1 && ctx->nlev <= 30) {
-    RC(read_small(ctx, 2));
-    const double bn = ctx->h_small[1] > 0 ? ctx->h_small[1] : 1.0;
-    st->bnorm = ctx->h_small[1];
-    return solve_mixed_engine(ctx, u, b, s, op, k2, geom, bc, o, st, e, be, r, u1, bn);
-  }
-  // per-operation kernels
   RC(make_consistent(ctx, u, sg));
   RC(defect_all(ctx, be, e, u, b, s, op, k2, geom, 0));
   RC(read_small(ctx, 2));
@@ -426,7 +348,7 @@ static int solve_mixed(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_a
   double prev = rel;
   while (rel > o->tol && outer < o->max_cycles) {
     for (int i = 0; i < inner; i++) {
-      RC(vcycle_mixed(ctx, e, be, r, u1, s, op, k2, geom, sg, o->ndown, o->ntop, o->nup, o->omega));
+      RC(vcycle_mixed(ctx, e, be, r, u1, s, op, k2, geom, sg, o->ndown, o->ntop, o->nup, o->omega, tabs));
       cycles++;
     }
     for (int l = 1; l <= ctx->nlev; l++) {
@@ -444,7 +366,8 @@ static int solve_mixed(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_a
       st->cycles = cycles;
       st->outer = outer;
       st->rel_residual = nrel;
-      return fail(ctx, SRMG_ERR_DIVERGED, "mixed solve diverged after %d steps", outer);
+      st->status = SRMG_ERR_DIVERGED;
+      return SRMG_OK;
     }
     prev = nrel;
     rel = nrel;
@@ -455,31 +378,50 @@ static int solve_mixed(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_a
   return SRMG_OK;
 }
 
-extern "C" int srmg_solve_dev(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, double s,
-                              int op, double k2, int geom, const int8_t bc[9],
-                              const srmg_solve_opts *opts, srmg_stats *stats) {
-  RC(check_call(ctx, nblk_alloc, op, geom, bc));
-  if (!u || !b) return fail(ctx, SRMG_ERR_BADARG, "srmg_solve: null field");
+int srmg::solve_items(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, const ItemSpec *specs,
+                      int geom, const srmg_solve_opts *opts, srmg_stats *st) {
   srmg_solve_opts o;
   if (opts) o = *opts; else srmg_solve_opts_default(&o);
   if (!(o.tol > 0) || o.max_cycles < 0 || o.ndown < 0 || o.nup < 0 || o.ntop < 0)
     return fail(ctx, SRMG_ERR_BADARG, "srmg_solve: bad options");
-  srmg_stats st;
-  memset(&st, 0, sizeof st);
+  for (int k = 0; k < ctx->nitems; k++) memset(&st[k], 0, sizeof(srmg_stats));
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   int rc;
-  if (o.mode == SRMG_MODE_FP64) rc = solve_fp64(ctx, u, b, nblk_alloc, s, op, k2, geom, bc, &o, &st);
-  else if (o.mode == SRMG_MODE_MIXED) rc = solve_mixed(ctx, u, b, nblk_alloc, s, op, k2, geom, bc, &o, &st);
+  if (o.mode == SRMG_MODE_FP64) rc = solve_fp64(ctx, u, b, nblk_alloc, specs, geom, &o, st);
+  else if (o.mode == SRMG_MODE_MIXED) rc = solve_mixed(ctx, u, b, nblk_alloc, specs, geom, &o, st);
   else rc = fail(ctx, SRMG_ERR_BADARG, "unknown solve mode %d", o.mode);
   cudaEventRecord(ctx->ev1, ctx->stream);
   cudaEventSynchronize(ctx->ev1);
   float ms = 0;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-  st.device_ms = ms;
-  st.status = rc;
-  if (stats) *stats = st;
+  for (int k = 0; k < ctx->nitems; k++) st[k].device_ms = ms;
   if (rc) return rc;
   CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+extern "C" int srmg_solve_dev(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, double s,
+                              int op, double k2, int geom, const int8_t bc[9],
+                              const srmg_solve_opts *opts, srmg_stats *stats) {
+  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  if (!u || !b) return fail(ctx, SRMG_ERR_BADARG, "srmg_solve: null field");
+  const std::vector<ItemSpec> specs = uniform_items(ctx, s, op, k2, bc);
+  std::vector<srmg_stats> st((size_t)ctx->nitems);
+  const int rc = solve_items(ctx, u, b, nblk_alloc, specs.data(), geom, opts, st.data());
+  // one set of statistics: the worst item
+  srmg_stats agg = st[0];
+  for (const srmg_stats &x : st) {
+    agg.cycles = std::max(agg.cycles, x.cycles);
+    agg.outer = std::max(agg.outer, x.outer);
+    if (!(x.rel_residual <= agg.rel_residual)) agg.rel_residual = x.rel_residual;
+    agg.initial_rel = std::max(agg.initial_rel, x.initial_rel);
+    if (x.status) agg.status = x.status;
+  }
+  if (rc) agg.status = rc;
+  if (stats) *stats = agg;
+  if (rc) return rc;
+  if (agg.status)
+    return fail(ctx, agg.status, "residual is not finite after %d cycles", agg.cycles);
   return SRMG_OK;
 }
 

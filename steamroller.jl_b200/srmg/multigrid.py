@@ -49,6 +49,12 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Item(ctypes.Structure):
+    """srmg_item: one problem of a batch (its tree's context and its operator)."""
+    _fields_ = [("tree", ctypes.c_void_p), ("s", ctypes.c_double), ("op", ctypes.c_int),
+                ("k2", ctypes.c_double), ("bc", ctypes.c_int8 * 9)]
+
+
 _lib = None
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -87,6 +93,13 @@ SIGNATURES = {
     "srmg_set_option": (_I, [_P, ctypes.c_char_p, _I64]),
     "srmg_get_trace": (_I, [_P, _P, _I]),
     "srmg_launch_count": (_I64, [_P]),
+    "srmg_batch_set": (_I, [_P, _I, ctypes.POINTER(Item), _I]),
+    "srmg_batch_items": (_I, [_P]),
+    "srmg_batch_offset": (_I64, [_P, _I]),
+    "srmg_batch_nblk": (_I64, [_P, _I]),
+    "srmg_batch_solve_dev": (_I, [_P, _P, _P, ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
+    "srmg_batch_solve": (_I, [_P, _P, _P, ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
+    "srmg_batch_solve_forest_dev": (_I, [_P, _P, _P, ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
 }
 
 
@@ -276,6 +289,55 @@ def solve(ctx: Context, u, b, s, geometry, bc, lpldisc=None, tol=1e-8, mode=MODE
            ctypes.byref(o), ctypes.byref(st))
     ctx.check(rc)
     return st.as_dict()
+
+
+class Batch(Context):
+    """A batch context: a forest of independent problems solved by one persistent launch.
+
+    ``problems`` is a list of ``(tree_context, s, lpldisc, bc)``; the same tree context
+    may appear several times (e.g. the Poisson potential and the three photoionization
+    Helmholtz terms of one tree).  No single counterpart in the reference, which calls
+    vcycle!/fmg! once per field (src/streamer.jl:322-334, src/photo.jl)."""
+
+    def __init__(self, problems, geometry, device: int = 0):
+        super().__init__(device)
+        items = (Item * len(problems))()
+        for i, (tctx, s, lpldisc, bc) in enumerate(problems):
+            op, k2 = _disc(lpldisc)
+            items[i].tree = tctx.handle.value
+            items[i].s = float(s)
+            items[i].op = op
+            items[i].k2 = k2
+            items[i].bc[:] = [int(v) for v in _bc(bc)]
+        self.check(lib().srmg_batch_set(self._h, len(problems), items, int(geometry)))
+        self.nitems = len(problems)
+        self.offsets = [lib().srmg_batch_offset(self._h, i) for i in range(self.nitems)]
+        self.nblks = [lib().srmg_batch_nblk(self._h, i) for i in range(self.nitems)]
+        self.total_blocks = sum(self.nblks)
+
+    def solve(self, us, bs, tol=1e-8, mode=MODE_FP64, max_cycles=1000, ndown=2, ntop=4, nup=2,
+              omega=1.0, inner_cycles=1, warm_start=0):
+        """Solve every item; ``us``/``bs`` are per-item fields (numpy arrays: host entry
+        point; torch tensors: device entry point).  Returns one stats dict per item."""
+        assert len(us) == self.nitems and len(bs) == self.nitems
+        o = SolveOpts(tol, max_cycles, mode, ndown, ntop, nup, omega, inner_cycles, warm_start)
+        st = (Stats * self.nitems)()
+        up = (_P * self.nitems)(*[_ptr(x) for x in us])
+        bp = (_P * self.nitems)(*[_ptr(x) for x in bs])
+        dev = not isinstance(us[0], np.ndarray)
+        _order_after_torch(self, *us, *bs)
+        f = lib().srmg_batch_solve_dev if dev else lib().srmg_batch_solve
+        self.check(f(self._h, ctypes.cast(up, _P), ctypes.cast(bp, _P), ctypes.byref(o), st))
+        return [x.as_dict() for x in st]
+
+    def solve_forest(self, u, b, tol=1e-8, mode=MODE_FP64, max_cycles=1000, ndown=2, ntop=4, nup=2,
+                     omega=1.0, inner_cycles=1, warm_start=0):
+        """Solve every item on device fields in the forest layout (no copies)."""
+        o = SolveOpts(tol, max_cycles, mode, ndown, ntop, nup, omega, inner_cycles, warm_start)
+        st = (Stats * self.nitems)()
+        _order_after_torch(self, u, b)
+        self.check(lib().srmg_batch_solve_forest_dev(self._h, _ptr(u), _ptr(b), ctypes.byref(o), st))
+        return [x.as_dict() for x in st]
 
 
 def exported_symbols_from_header(header_path: str) -> list[str]:
