@@ -171,6 +171,7 @@ def main():
     ap.add_argument("--target-leaf", type=int, default=TARGET_LEAF)
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched config-3 section")
     ap.add_argument("--only", default=None, choices=[None, "vcycle", "smooth"],
                     help="vcycle: time plain FP64 V-cycles only; smooth: GS iterations on the finest "
                          "level only (profiling runs)")
@@ -298,6 +299,12 @@ def main():
                          "kernel": "plain FP64 V-cycle (whole cycle)", "bytes_per_launch": bytes_vc,
                          "ms_per_vcycle": vc_ms},
             "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}
+    all_cells = sum(len(layer) for layer in problem.tree) * 256
+    line["cells_vcycles_per_s"] = {
+        "leaf": nleaf * mixed_st["cycles"] * value, "all_levels": all_cells * mixed_st["cycles"] * value,
+        "fp64_leaf": nleaf * fp64_st["cycles"] * fp64_value, "note": "cells x V-cycles per second"}
+    if not args.no_batch:
+        line["batch"] = run_batch(local, stream, min(args.steps, 3))
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = run_cpu_reference(problem, fp64_st["cycles"])
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -306,6 +313,73 @@ def main():
     ctx.close()
     if pg is not None:
         pg.destroy_process_group()
+
+
+def run_batch(local, stream, steps):
+    """Config 3: 16 independent trees with leaf counts log-uniform in [1e5, 3e6], each
+    with one Poisson and three photoionization Helmholtz right-hand sides: 64 solves to
+    1e-8 in ONE persistent launch (graph-captured batch), against the same 64 solves
+    run one by one in plain FP64 and in mixed precision."""
+    import torch
+    from srmg import gen, multigrid as mg
+    from srmg.tree import leaf_cells
+    trees = gen.config3_tree_problems()
+    ctxs, items = [], []
+    for pois, terms in trees:
+        c = mg.Context(local).set_tree(pois.tree, pois.conn)
+        c.set_stream(stream.cuda_stream)
+        ctxs.append(c)
+        for p in [pois] + terms:
+            items.append((c, p))
+    disc = lambda p: ("helmholtz", p.k2) if p.op else None
+    batch = mg.Batch([(c, p.s, disc(p), p.bc) for c, p in items], gen.GEOM_CYL1, device=local)
+    batch.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        us = [torch.zeros(p.b.shape, dtype=torch.float64, device="cuda") for _, p in items]
+        bs = [torch.from_numpy(p.b).cuda() for _, p in items]
+    stream.synchronize()
+    opts = dict(tol=TOL, ndown=2, ntop=4, nup=2, max_cycles=5000)
+
+    def zero():
+        with torch.cuda.stream(stream):
+            for u in us:
+                u.zero_()
+        stream.synchronize()
+
+    batch.set_option("graph", 1)
+    res = {}
+    for mode, name in ((mg.MODE_MIXED, "mixed"), (mg.MODE_FP64, "fp64")):
+        zero()
+        batch.solve(us, bs, mode=mode, **opts)  # warm-up (capture)
+        ms = []
+        n = steps if mode == mg.MODE_MIXED else 1
+        for _ in range(n):
+            zero()
+            st = batch.solve(us, bs, mode=mode, **opts)
+            ms.append(st[0]["device_ms"])
+        res[name + "_batched"] = {"value": len(items) / (np.mean(ms) / 1e3), "unit": "solves/s",
+                                  "ms_per_batch": float(np.mean(ms)),
+                                  "max_cycles": max(x["cycles"] for x in st),
+                                  "max_rel_residual": max(x["rel_residual"] for x in st)}
+    for mode, name in ((mg.MODE_MIXED, "mixed"), (mg.MODE_FP64, "fp64")):
+        tot = 0.0
+        for k, (c, p) in enumerate(items):
+            with torch.cuda.stream(stream):
+                us[k].zero_()
+            stream.synchronize()
+            st = mg.solve(c, us[k], bs[k], p.s, p.geom, p.bc, disc(p), mode=mode, **opts)
+            tot += st["device_ms"]
+        res[name + "_solo"] = {"value": len(items) / (tot / 1e3), "unit": "solves/s", "ms_total": tot}
+    out = {"workload": "config3: 16 trees (leaf cells log-uniform 1e5-3e6) x (Poisson + 3 Helmholtz "
+                       "photoionization terms), cylindrical r-z, tol 1e-8, one graph-captured persistent launch",
+           "items": len(items), "leaf_cells": int(sum(leaf_cells(p.tree) for p, _ in trees)),
+           "blocks": batch.total_blocks, **res,
+           "speedup_mixed_batched_vs_fp64_solo": res["mixed_batched"]["value"] / res["fp64_solo"]["value"],
+           "speedup_mixed_batched_vs_fp64_batched": res["mixed_batched"]["value"] / res["fp64_batched"]["value"]}
+    batch.close()
+    for c in ctxs:
+        c.close()
+    return out
 
 
 def vcycle_only(args):

@@ -262,6 +262,26 @@ int srmg_batch_solve(srmg_ctx *batch, double *const *u, const double *const *b,
 int srmg_batch_solve_forest_dev(srmg_ctx *batch, double *u, const double *b,
                                 const srmg_solve_opts *opts, srmg_stats *stats);
 
+/* ---- autotuner (no reference counterpart) ----------------------------------------
+ * Times complete solves to opts->tol from the caller's initial guess for a set of
+ * candidate launch shapes and sweep counts (30 candidates, each solved twice):
+ * engine_ctas (one CTA per SM or half as many: blocks per CTA), local_max_blocks
+ * (4, 16, 64: coarse levels kept inside one CTA) and (ndown, nup) in {(2,2), (1,1),
+ * (1,2), (2,1), (3,3)}.  The fastest candidate's options are set on the context and
+ * its sweep counts written to *opts; u is restored to its initial content.  Trials
+ * are reported in `trials` (up to max_trials).  Returns the number of trials run or
+ * an error code.  The tile shape is fixed: one 20 x 20 block per 256-thread slot. */
+typedef struct {
+    int engine_ctas, local_max_blocks, ndown, nup, ntop;
+    int cycles;          /* V-cycles (FP64) or defect-correction steps (mixed), worst item */
+    double ms;           /* best device time of the trial, -1 if it missed the tolerance */
+} srmg_tune_trial;
+int srmg_autotune(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc,
+                  double s, int op, double k2, int geom, const int8_t bc[9],
+                  srmg_solve_opts *opts, srmg_tune_trial *trials, int max_trials);
+int srmg_batch_autotune(srmg_ctx *batch, double *const *u, const double *const *b,
+                        srmg_solve_opts *opts, srmg_tune_trial *trials, int max_trials);
+
 /* Tuning knobs (no reference counterpart; the autotuner drives them):
  *   "engine"           1 = persistent one-launch V-cycle (default), 0 = one kernel per
  *                      reference operation;

@@ -145,7 +145,7 @@ int item_inverse(srmg_ctx *ctx, int item, const ItemSpec &sp, int geom, const do
   }
   if (!invert(A, n)) return SRMG_OK;
   for (auto &v : A) v *= -s;
-  if (ctx->coarse_cache.size() >= 64) {
+  if (ctx->coarse_cache.size() >= 256) {
     CK(cudaStreamSynchronize(ctx->stream));
     for (auto &kv : ctx->coarse_cache) cudaFree(kv.second.p);
     ctx->coarse_cache.clear();

@@ -1,0 +1,169 @@
+// srmg_tune.cu -- autotuner of the persistent engine's launch shape and of the
+// multigrid sweep counts (no reference counterpart: the reference's cycle parameters
+// are fixed inputs, src/simulate.jl:145).
+//
+// A trial is one complete tolerance-driven solve from the caller's initial guess on the
+// caller's own problem; its cost is the device time to reach the tolerance.  The
+// candidates are
+//   * grid size ("engine_ctas"): one CTA per SM, or fewer CTAs (more blocks per CTA,
+//     cheaper grid barriers);
+//   * CTA-local coarse levels ("local_max_blocks"): how many blocks a level may hold
+//     and still run inside CTA 0 with CTA barriers instead of grid barriers;
+//   * sweep counts (ndown, nup): smoothing per level on the way down and up; ntop
+//     only matters when the coarsest level is smoothed rather than solved directly.
+// The tile shape is fixed by the data layout (one 20 x 20 block per 256-thread slot,
+// four slots per CTA).  The fastest trial's settings are applied to the context and
+// written to *opts; the caller's fields are restored after every trial.
+#include <algorithm>
+#include <cstring>
+#include <functional>
+#include <vector>
+
+#include "srmg_ctx.h"
+#include "srmg_internal.h"
+
+using namespace srmg;
+
+#define CK(call)                                              \
+  do {                                                        \
+    int _rc = cuda_check(ctx, (call), #call);                 \
+    if (_rc) return _rc;                                      \
+  } while (0)
+#define RC(call)               \
+  do {                         \
+    int _rc = (call);          \
+    if (_rc) return _rc;       \
+  } while (0)
+
+namespace {
+
+struct Cand {
+  int ctas, local_max, ndown, nup;
+};
+
+// Run every candidate with `solve` (which restores its own inputs), keep the fastest.
+int tune(srmg_ctx *ctx, srmg_solve_opts *opts, srmg_tune_trial *trials, int max_trials,
+         const std::function<int(const srmg_solve_opts &, double *ms, int *cycles, bool *ok)> &solve) {
+  int nsm = 0;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device));
+  std::vector<Cand> cands;
+  const int sweeps[][2] = {{2, 2}, {1, 1}, {1, 2}, {2, 1}, {3, 3}};
+  for (int ctas : {0, nsm / 2})
+    for (int lm : {4, 16, 64})
+      for (const auto &sw : sweeps) cands.push_back({ctas, lm, sw[0], sw[1]});
+  const int save_ctas = ctx->engine_ctas, save_lm = ctx->local_max_blocks;
+  double best = 1e300;
+  Cand pick{save_ctas, save_lm, opts->ndown, opts->nup};
+  int n = 0;
+  for (const Cand &c : cands) {
+    ctx->engine_ctas = c.ctas;
+    ctx->local_max_blocks = c.local_max;
+    srmg_solve_opts o = *opts;
+    o.ndown = c.ndown;
+    o.nup = c.nup;
+    double ms = 0.0, ms2 = 0.0;
+    int cyc = 0;
+    bool ok = false;
+    int rc = solve(o, &ms, &cyc, &ok);   // first run also sizes buffers
+    if (!rc && ok) rc = solve(o, &ms2, &cyc, &ok);
+    if (rc) {
+      ctx->engine_ctas = save_ctas;
+      ctx->local_max_blocks = save_lm;
+      return rc;
+    }
+    const double t = std::min(ms, ms2);
+    if (trials && n < max_trials) {
+      srmg_tune_trial &tr = trials[n];
+      tr.engine_ctas = c.ctas;
+      tr.local_max_blocks = c.local_max;
+      tr.ndown = c.ndown;
+      tr.nup = c.nup;
+      tr.ntop = o.ntop;
+      tr.ms = ok ? t : -1.0;
+      tr.cycles = cyc;
+    }
+    n++;
+    if (ok && t < best) {
+      best = t;
+      pick = c;
+    }
+  }
+  ctx->engine_ctas = pick.ctas;
+  ctx->local_max_blocks = pick.local_max;
+  opts->ndown = pick.ndown;
+  opts->nup = pick.nup;
+  return n;
+}
+
+}  // namespace
+
+extern "C" int srmg_autotune(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, double s, int op,
+                             double k2, int geom, const int8_t bc[9], srmg_solve_opts *opts,
+                             srmg_tune_trial *trials, int max_trials) {
+  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  if (!u || !b || !opts || max_trials < 0) return fail(ctx, SRMG_ERR_BADARG, "srmg_autotune: bad arguments");
+  const size_t bytes = (size_t)nblk_alloc * kSS * sizeof(double);
+  DevBuf u0;
+  RC(ensure(ctx, u0, bytes));
+  CK(cudaMemcpyAsync(u0.p, u, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  const std::vector<ItemSpec> specs = uniform_items(ctx, s, op, k2, bc);
+  std::vector<srmg_stats> st((size_t)ctx->nitems);
+  auto solve = [&](const srmg_solve_opts &o, double *ms, int *cycles, bool *ok) -> int {
+    if (cudaMemcpyAsync(u, u0.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
+      return fail(ctx, SRMG_ERR_CUDA, "autotune: restore of u failed");
+    RC(solve_items(ctx, u, b, nblk_alloc, specs.data(), geom, &o, st.data()));
+    *ms = st[0].device_ms;
+    *cycles = 0;
+    *ok = true;
+    for (const srmg_stats &x : st) {
+      *cycles = std::max(*cycles, x.cycles);
+      if (x.status || !(x.rel_residual <= o.tol)) *ok = false;
+    }
+    return SRMG_OK;
+  };
+  const int n = tune(ctx, opts, trials, max_trials, solve);
+  cudaMemcpyAsync(u, u0.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(u0.p);
+  return n;
+}
+
+extern "C" int srmg_batch_autotune(srmg_ctx *ctx, double *const *u, const double *const *b, srmg_solve_opts *opts,
+                                   srmg_tune_trial *trials, int max_trials) {
+  if (!ctx) return SRMG_ERR_BADARG;
+  if (!ctx->has_tree || (int)ctx->batch_items.size() != ctx->nitems)
+    return fail(ctx, SRMG_ERR_NOTREE, "no batch: call srmg_batch_set first");
+  if (!u || !b || !opts || max_trials < 0) return fail(ctx, SRMG_ERR_BADARG, "srmg_batch_autotune: bad arguments");
+  cudaSetDevice(ctx->device);
+  const size_t bytes = (size_t)ctx->max_blk * kSS * sizeof(double);
+  DevBuf u0, fu, fb;
+  RC(ensure(ctx, u0, bytes));
+  RC(ensure(ctx, fu, bytes));
+  RC(ensure(ctx, fb, bytes));
+  for (int k = 0; k < ctx->nitems; k++) {
+    const size_t off = (size_t)ctx->item_first[k] * kSS, nb = (size_t)ctx->item_nblk[k] * kSS * sizeof(double);
+    CK(cudaMemcpyAsync((double *)u0.p + off, u[k], nb, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync((double *)fb.p + off, b[k], nb, cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  std::vector<srmg_stats> st((size_t)ctx->nitems);
+  auto solve = [&](const srmg_solve_opts &o, double *ms, int *cycles, bool *ok) -> int {
+    if (cudaMemcpyAsync(fu.p, u0.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
+      return fail(ctx, SRMG_ERR_CUDA, "autotune: restore of u failed");
+    RC(solve_items(ctx, (double *)fu.p, (const double *)fb.p, ctx->max_blk, ctx->batch_items.data(),
+                   ctx->geom_forest, &o, st.data()));
+    *ms = st[0].device_ms;
+    *cycles = 0;
+    *ok = true;
+    for (const srmg_stats &x : st) {
+      *cycles = std::max(*cycles, x.cycles);
+      if (x.status || !(x.rel_residual <= o.tol)) *ok = false;
+    }
+    return SRMG_OK;
+  };
+  const int n = tune(ctx, opts, trials, max_trials, solve);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(u0.p);
+  cudaFree(fu.p);
+  cudaFree(fb.p);
+  return n;
+}

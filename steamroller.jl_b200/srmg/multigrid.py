@@ -49,6 +49,14 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class TuneTrial(ctypes.Structure):
+    _fields_ = [("engine_ctas", ctypes.c_int), ("local_max_blocks", ctypes.c_int), ("ndown", ctypes.c_int),
+                ("nup", ctypes.c_int), ("ntop", ctypes.c_int), ("cycles", ctypes.c_int), ("ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Item(ctypes.Structure):
     """srmg_item: one problem of a batch (its tree's context and its operator)."""
     _fields_ = [("tree", ctypes.c_void_p), ("s", ctypes.c_double), ("op", ctypes.c_int),
@@ -100,6 +108,9 @@ SIGNATURES = {
     "srmg_batch_solve_dev": (_I, [_P, _P, _P, ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
     "srmg_batch_solve": (_I, [_P, _P, _P, ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
     "srmg_batch_solve_forest_dev": (_I, [_P, _P, _P, ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
+    "srmg_autotune": (_I, [_P, _P, _P, _I64, _D, _I, _D, _I, _P, ctypes.POINTER(SolveOpts),
+                           ctypes.POINTER(TuneTrial), _I]),
+    "srmg_batch_autotune": (_I, [_P, _P, _P, ctypes.POINTER(SolveOpts), ctypes.POINTER(TuneTrial), _I]),
 }
 
 
@@ -338,6 +349,39 @@ class Batch(Context):
         _order_after_torch(self, u, b)
         self.check(lib().srmg_batch_solve_forest_dev(self._h, _ptr(u), _ptr(b), ctypes.byref(o), st))
         return [x.as_dict() for x in st]
+
+
+def autotune(ctx: Context, u, b, s, geometry, bc, lpldisc=None, tol=1e-8, mode=MODE_MIXED,
+             max_cycles=1000, ndown=2, ntop=4, nup=2, omega=1.0):
+    """Autotune launch shape and sweep counts on this problem (device fields); returns
+    (chosen options dict, list of trial dicts).  The chosen launch options stay set on
+    the context."""
+    op, k2 = _disc(lpldisc)
+    bca = _bc(bc)
+    o = SolveOpts(tol, max_cycles, mode, ndown, ntop, nup, omega, 1, 0)
+    tr = (TuneTrial * 64)()
+    _order_after_torch(ctx, u, b)
+    n = lib().srmg_autotune(ctx.handle, _ptr(u), _ptr(b), u.shape[0], s, op, k2, geometry, bca.ctypes.data,
+                            ctypes.byref(o), tr, 64)
+    if n < 0:
+        ctx.check(n)
+    chosen = {k: getattr(o, k) for k, _ in SolveOpts._fields_}
+    return chosen, [tr[i].as_dict() for i in range(min(n, 64))]
+
+
+def batch_autotune(batch: "Batch", us, bs, tol=1e-8, mode=MODE_MIXED, max_cycles=1000, ndown=2, ntop=4,
+                   nup=2, omega=1.0):
+    """Autotune a batch on its items' device fields; returns (options, trials)."""
+    o = SolveOpts(tol, max_cycles, mode, ndown, ntop, nup, omega, 1, 0)
+    tr = (TuneTrial * 64)()
+    up = (_P * batch.nitems)(*[_ptr(x) for x in us])
+    bp = (_P * batch.nitems)(*[_ptr(x) for x in bs])
+    _order_after_torch(batch, *us, *bs)
+    n = lib().srmg_batch_autotune(batch.handle, ctypes.cast(up, _P), ctypes.cast(bp, _P), ctypes.byref(o), tr, 64)
+    if n < 0:
+        batch.check(n)
+    chosen = {k: getattr(o, k) for k, _ in SolveOpts._fields_}
+    return chosen, [tr[i].as_dict() for i in range(min(n, 64))]
 
 
 def exported_symbols_from_header(header_path: str) -> list[str]:

@@ -139,3 +139,30 @@ def test_batch_rejects_bad_items(setup):
     empty = mg.Context(0)
     with pytest.raises(mg.SrmgError):
         mg.Batch([(empty, p.s, None, p.bc)], gen.GEOM_CYL1)
+
+
+def test_autotune_single_and_batch(setup):
+    """The autotuner times every candidate to the tolerance, restores the caller's
+    initial guess, and leaves the fastest launch shape and sweep counts in force."""
+    ctxs, items, batch = setup
+    c, p = items[0]
+    u0 = np.zeros_like(p.b)
+    ug, bg = torch_cuda(u0), torch_cuda(p.b)
+    chosen, trials = mg.autotune(c, ug, bg, p.s, p.geom, p.bc, disc(p), tol=1e-8, mode=mg.MODE_MIXED)
+    assert len(trials) == 30
+    assert all(t["ms"] > 0 for t in trials)
+    best = min(trials, key=lambda t: t["ms"])
+    assert (chosen["ndown"], chosen["nup"]) == (best["ndown"], best["nup"])
+    np.testing.assert_array_equal(to_np(ug), u0)  # initial guess restored
+    st = mg.solve(c, ug, bg, p.s, p.geom, p.bc, disc(p), tol=1e-8, mode=mg.MODE_MIXED,
+                  ndown=chosen["ndown"], nup=chosen["nup"], ntop=chosen["ntop"])
+    assert st["rel_residual"] <= 1e-8
+    c.set_option("engine_ctas", 0).set_option("local_max_blocks", 16)
+    us = [torch_cuda(np.zeros_like(q.b)) for _, q in items]
+    bs = [torch_cuda(q.b) for _, q in items]
+    chosen, trials = mg.batch_autotune(batch, us, bs, tol=1e-8, mode=mg.MODE_MIXED)
+    assert len(trials) == 30 and all(t["ms"] > 0 for t in trials)
+    sts = batch.solve(us, bs, mode=mg.MODE_MIXED, tol=1e-8, ndown=chosen["ndown"], nup=chosen["nup"],
+                      ntop=chosen["ntop"], max_cycles=400)
+    assert all(s["rel_residual"] <= 1e-8 for s in sts)
+    batch.set_option("engine_ctas", 0).set_option("local_max_blocks", 16)
