@@ -101,7 +101,8 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def dist_setup():
+def dist_setup(backend=None):
+    """One process per GPU (torchrun env); NCCL on GPUs, gloo on the host (tests)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -109,8 +110,7 @@ def dist_setup():
     if world > 1:
         import torch.distributed as dist
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=None)
+        dist.init_process_group(backend or "nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
 
@@ -127,8 +127,17 @@ def max_over_ranks(x, pg, device):
 def barrier(pg, device):
     import torch
     if pg is not None:
-        pg.barrier(device_ids=[device.index])
-    torch.cuda.synchronize()
+        if device.type == "cuda":
+            pg.barrier(device_ids=[device.index])
+        else:
+            pg.barrier()
+    if device.type == "cuda":
+        torch.cuda.synchronize()
+
+
+def shard(n, rank, world):
+    """Independent work units (trees) of this rank: round-robin, no exchange needed."""
+    return list(range(rank, n, world))
 
 
 def run_cpu_reference(problem, fp64_cycles, budget_s=12.0, threads=None, warm=1):
@@ -304,7 +313,7 @@ def main():
         "leaf": nleaf * mixed_st["cycles"] * value, "all_levels": all_cells * mixed_st["cycles"] * value,
         "fp64_leaf": nleaf * fp64_st["cycles"] * fp64_value, "note": "cells x V-cycles per second"}
     if not args.no_batch:
-        line["batch"] = run_batch(local, stream, min(args.steps, 3))
+        line["batch"] = run_batch(local, stream, min(args.steps, 3), rank, world, pg, dev)
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = run_cpu_reference(problem, fp64_st["cycles"])
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -315,15 +324,19 @@ def main():
         pg.destroy_process_group()
 
 
-def run_batch(local, stream, steps):
+def run_batch(local, stream, steps, rank=0, world=1, pg=None, dev=None):
     """Config 3: 16 independent trees with leaf counts log-uniform in [1e5, 3e6], each
     with one Poisson and three photoionization Helmholtz right-hand sides: 64 solves to
     1e-8 in ONE persistent launch (graph-captured batch), against the same 64 solves
-    run one by one in plain FP64 and in mixed precision."""
+    run one by one in plain FP64 and in mixed precision.  With several ranks the trees
+    are shared out round-robin (no exchange); times are the max over ranks and the
+    solves/s count every rank's items (strong scaling: the 64 solves are fixed)."""
     import torch
     from srmg import gen, multigrid as mg
     from srmg.tree import leaf_cells
-    trees = gen.config3_tree_problems()
+    all_trees = gen.config3_tree_problems()
+    trees = [all_trees[i] for i in shard(len(all_trees), rank, world)]
+    n_total = 4 * len(all_trees)
     ctxs, items = [], []
     for pois, terms in trees:
         c = mg.Context(local).set_tree(pois.tree, pois.conn)
@@ -357,8 +370,9 @@ def run_batch(local, stream, steps):
             zero()
             st = batch.solve(us, bs, mode=mode, **opts)
             ms.append(st[0]["device_ms"])
-        res[name + "_batched"] = {"value": len(items) / (np.mean(ms) / 1e3), "unit": "solves/s",
-                                  "ms_per_batch": float(np.mean(ms)),
+        t = max_over_ranks(float(np.mean(ms)), pg, dev)
+        res[name + "_batched"] = {"value": n_total / (t / 1e3), "unit": "solves/s",
+                                  "ms_per_batch": t,
                                   "max_cycles": max(x["cycles"] for x in st),
                                   "max_rel_residual": max(x["rel_residual"] for x in st)}
     for mode, name in ((mg.MODE_MIXED, "mixed"), (mg.MODE_FP64, "fp64")):
@@ -369,10 +383,12 @@ def run_batch(local, stream, steps):
             stream.synchronize()
             st = mg.solve(c, us[k], bs[k], p.s, p.geom, p.bc, disc(p), mode=mode, **opts)
             tot += st["device_ms"]
-        res[name + "_solo"] = {"value": len(items) / (tot / 1e3), "unit": "solves/s", "ms_total": tot}
+        tot = max_over_ranks(tot, pg, dev)
+        res[name + "_solo"] = {"value": n_total / (tot / 1e3), "unit": "solves/s", "ms_total": tot}
     out = {"workload": "config3: 16 trees (leaf cells log-uniform 1e5-3e6) x (Poisson + 3 Helmholtz "
                        "photoionization terms), cylindrical r-z, tol 1e-8, one graph-captured persistent launch",
-           "items": len(items), "leaf_cells": int(sum(leaf_cells(p.tree) for p, _ in trees)),
+           "items": n_total, "leaf_cells": int(sum(leaf_cells(p.tree) for p, _ in all_trees)),
+           "scaling": "strong", "ranks": world,
            "blocks": batch.total_blocks, **res,
            "speedup_mixed_batched_vs_fp64_solo": res["mixed_batched"]["value"] / res["fp64_solo"]["value"],
            "speedup_mixed_batched_vs_fp64_batched": res["mixed_batched"]["value"] / res["fp64_batched"]["value"]}
