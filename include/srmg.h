@@ -282,6 +282,48 @@ int srmg_autotune(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc,
 int srmg_batch_autotune(srmg_ctx *batch, double *const *u, const double *const *b,
                         srmg_solve_opts *opts, srmg_tune_trial *trials, int max_trials);
 
+/* ---- learned warm start (no reference counterpart) --------------------------------
+ * A 6-layer BF16 convolutional network (3x3 convolutions, 32 channels, ReLU; zero
+ * padding at the tile edge) maps, per block, the 20 x 20 tile (16 x 16 cells plus the
+ * 2-cell ghost halo) of (phi_prev * a, (b - b_prev) * c) to (phi_new - phi_prev) /
+ * (s_l * |b - b_prev|) on the block's 16 x 16 cells, with a = 1/|phi_prev|,
+ * c = 1/|b - b_prev| (|.| = the resnorm! leaf norm, per tree).  Forward, backward
+ * and optimiser kernels run on the tensor cores; parameters are an FP32 master
+ * vector (per layer W [tap][co][ci], then b [co]). */
+typedef struct srmg_cnn srmg_cnn;
+int srmg_cnn_create(srmg_cnn **net, int device, uint64_t seed);  /* He-initialised */
+void srmg_cnn_destroy(srmg_cnn *net);
+const char *srmg_cnn_last_error(const srmg_cnn *net);
+int srmg_cnn_nparams(void);
+int srmg_cnn_get_params(srmg_cnn *net, float *host, int n);
+int srmg_cnn_set_params(srmg_cnn *net, const float *host, int n);  /* resets Adam state */
+int srmg_cnn_synchronize(srmg_cnn *net);
+/* Samples: x DEVICE bf16 [n][400][2] (tile pixel y*20+x, channels (phi, db));
+ * targets/outputs DEVICE float [n][16][16]. */
+int srmg_cnn_forward(srmg_cnn *net, const uint16_t *x, float *y, int n);
+/* Mean-squared-error loss over the n x 256 outputs and its gradient (host copy of the
+ * gradient in master layout if grad_host is not NULL; host loss). */
+int srmg_cnn_gradients(srmg_cnn *net, const uint16_t *x, const float *t, int n, float *grad_host,
+                       double *loss);
+/* One Adam step (beta 0.9/0.999, eps 1e-8) on the loss of the n samples. */
+int srmg_cnn_train_step(srmg_cnn *net, const uint16_t *x, const float *t, int n, float lr,
+                        double *loss);
+/* Tree fields -> samples, one per block holding a leaf cell (srmg_cnn_leaf_blocks of
+ * them): x as above, scale[k] = s_l * |b - b_prev| of the sample's block, blk[k] its
+ * 0-based block id.  DEVICE pointers; returns the sample count. */
+int srmg_cnn_leaf_blocks(const srmg_ctx *ctx);
+int srmg_cnn_pack_dev(srmg_ctx *ctx, const double *phi, const double *b, const double *b_prev,
+                      int64_t nblk_alloc, double s, int op, double k2, int geom, const int8_t bc[9],
+                      uint16_t *x, double *scale, int *blk, int max_samples);
+/* Warm start: u holds phi_prev (ghosts filled) on entry.  The network's guess of the
+ * new potential is formed on the leaf cells, made a composite-grid function (ghosts
+ * filled) and kept only if its residual norm is below that of phi_prev (*used = 1);
+ * otherwise u is left unchanged (*used = 0).  The solve then iterates to its
+ * tolerance from u as usual. */
+int srmg_cnn_predict_dev(srmg_ctx *ctx, srmg_cnn *net, double *u, const double *b,
+                         const double *b_prev, int64_t nblk_alloc, double s, int op, double k2,
+                         int geom, const int8_t bc[9], int *used);
+
 /* Tuning knobs (no reference counterpart; the autotuner drives them):
  *   "engine"           1 = persistent one-launch V-cycle (default), 0 = one kernel per
  *                      reference operation;

@@ -106,6 +106,7 @@ extern "C" void srmg_destroy(srmg_ctx *ctx) {
   if (ctx->h_items) cudaFreeHost(ctx->h_items);
   if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
   for (auto &b : ctx->forest) if (b.p) cudaFree(b.p);
+  for (auto &b : ctx->cnn_work) if (b.p) cudaFree(b.p);
   if (ctx->sync.p) cudaFree(ctx->sync.p);
   if (ctx->trace.p) cudaFree(ctx->trace.p);
   if (ctx->h_small) cudaFreeHost(ctx->h_small);
@@ -320,6 +321,11 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
     }
     itch[it].y = (int)chunks.size() - itch[it].x;
   }
+  // blocks holding at least one leaf cell, with their level (learned warm start)
+  std::vector<int2> leafblk;
+  for (int l = 0; l < nlev; l++)
+    for (const int4 &b4 : hb[l])
+      if ((b4.w & 15) != 15) leafblk.push_back(make_int2(b4.x, l + 1));
   for (int l = 0; l < nlev; l++)
     for (const int4 &b4 : hb[l]) binfo[b4.x] = make_int4(b4.y, b4.z, b4.w, l + 1);
   for (int64_t b = 0; b < max_blk; b++)
@@ -374,6 +380,7 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
   const size_t olr = take(lrange.size() * sizeof(int2));
   const size_t ochunk = take(std::max<size_t>(chunks.size(), 1) * sizeof(int4));
   const size_t oitch = take(itch.size() * sizeof(int2));
+  const size_t oleaf = take(std::max<size_t>(leafblk.size(), 1) * sizeof(int2));
   std::vector<char> host(off, 0);
   for (int l = 0; l < nlev; l++) {
     memcpy(host.data() + orr[l], hr[l].data(), hr[l].size() * sizeof(int4));
@@ -395,6 +402,7 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
   memcpy(host.data() + olr, lrange.data(), lrange.size() * sizeof(int2));
   memcpy(host.data() + ochunk, chunks.data(), chunks.size() * sizeof(int4));
   memcpy(host.data() + oitch, itch.data(), itch.size() * sizeof(int2));
+  memcpy(host.data() + oleaf, leafblk.data(), leafblk.size() * sizeof(int2));
 
   CK(cudaStreamSynchronize(ctx->stream));
   free_tree(ctx);
@@ -432,6 +440,8 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
   ctx->d_chunks = (int4 *)(base + ochunk);
   ctx->d_it_chunks = (int2 *)(base + oitch);
   ctx->nchunk = (int)chunks.size();
+  ctx->d_leaf = (int2 *)(base + oleaf);
+  ctx->nleaf = (int)leafblk.size();
   ctx->it_lrange_host = lrange;
   ctx->nitems = nitems;
   ctx->l1_blocks = hb[0];

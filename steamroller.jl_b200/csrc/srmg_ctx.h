@@ -104,6 +104,9 @@ struct srmg_ctx {
   int4 *d_chunks = nullptr;             // norm chunks {level, first, count, item} (inside d_tree)
   int2 *d_it_chunks = nullptr;          // per item: {first chunk, chunks}
   int nchunk = 0;
+  int2 *d_leaf = nullptr;               // blocks with a leaf cell: {0-based id, level}
+  int nleaf = 0;
+  srmg::DevBuf cnn_work[3];             // learned warm start: db, candidate guess, samples
   std::vector<int4> l1_blocks, l1_faces;  // level 1 as uploaded (direct coarsest solve)
   std::vector<srmg::ItemSpec> batch_items;       // operators given to srmg_batch_set
 

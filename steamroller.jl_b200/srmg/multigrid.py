@@ -111,6 +111,19 @@ SIGNATURES = {
     "srmg_autotune": (_I, [_P, _P, _P, _I64, _D, _I, _D, _I, _P, ctypes.POINTER(SolveOpts),
                            ctypes.POINTER(TuneTrial), _I]),
     "srmg_batch_autotune": (_I, [_P, _P, _P, ctypes.POINTER(SolveOpts), ctypes.POINTER(TuneTrial), _I]),
+    "srmg_cnn_create": (_I, [ctypes.POINTER(_P), _I, ctypes.c_uint64]),
+    "srmg_cnn_destroy": (None, [_P]),
+    "srmg_cnn_last_error": (ctypes.c_char_p, [_P]),
+    "srmg_cnn_nparams": (_I, []),
+    "srmg_cnn_get_params": (_I, [_P, _P, _I]),
+    "srmg_cnn_set_params": (_I, [_P, _P, _I]),
+    "srmg_cnn_synchronize": (_I, [_P]),
+    "srmg_cnn_forward": (_I, [_P, _P, _P, _I]),
+    "srmg_cnn_gradients": (_I, [_P, _P, _P, _I, _P, ctypes.POINTER(_D)]),
+    "srmg_cnn_train_step": (_I, [_P, _P, _P, _I, ctypes.c_float, ctypes.POINTER(_D)]),
+    "srmg_cnn_leaf_blocks": (_I, [_P]),
+    "srmg_cnn_pack_dev": (_I, [_P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, _P, _P, _P, _I]),
+    "srmg_cnn_predict_dev": (_I, [_P, _P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, ctypes.POINTER(_I)]),
 }
 
 
@@ -382,6 +395,107 @@ def batch_autotune(batch: "Batch", us, bs, tol=1e-8, mode=MODE_MIXED, max_cycles
         batch.check(n)
     chosen = {k: getattr(o, k) for k, _ in SolveOpts._fields_}
     return chosen, [tr[i].as_dict() for i in range(min(n, 64))]
+
+
+class Cnn:
+    """The learned warm-start network (BF16, tensor-core kernels of libsrmg)."""
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        self._h = _P()
+        rc = lib().srmg_cnn_create(ctypes.byref(self._h), device, seed)
+        if rc != SRMG_OK:
+            raise SrmgError(rc, "srmg_cnn_create failed")
+        self.device = device
+        self.nparams = lib().srmg_cnn_nparams()
+
+    def close(self):
+        if self._h:
+            lib().srmg_cnn_destroy(self._h)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def check(self, rc):
+        if rc != SRMG_OK:
+            msg = lib().srmg_cnn_last_error(self._h)
+            raise SrmgError(rc, msg.decode() if msg else "")
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(self.nparams, dtype=np.float32)
+        self.check(lib().srmg_cnn_get_params(self._h, out.ctypes.data, self.nparams))
+        return out
+
+    def set_params(self, theta):
+        a = np.ascontiguousarray(theta, dtype=np.float32)
+        assert a.size == self.nparams
+        self.check(lib().srmg_cnn_set_params(self._h, a.ctypes.data, self.nparams))
+
+    def synchronize(self):
+        self.check(lib().srmg_cnn_synchronize(self._h))
+
+    def forward(self, x):
+        """x: torch bf16 [n, 400, 2] on the device -> torch float32 [n, 256]."""
+        import torch
+        n = x.shape[0]
+        y = torch.empty((n, 256), dtype=torch.float32, device=x.device)
+        torch.cuda.synchronize()
+        self.check(lib().srmg_cnn_forward(self._h, x.data_ptr(), y.data_ptr(), n))
+        self.synchronize()
+        return y
+
+    def gradients(self, x, t):
+        g = np.zeros(self.nparams, dtype=np.float32)
+        loss = ctypes.c_double()
+        import torch
+        torch.cuda.synchronize()
+        self.check(lib().srmg_cnn_gradients(self._h, x.data_ptr(), t.data_ptr(), x.shape[0], g.ctypes.data,
+                                            ctypes.byref(loss)))
+        return loss.value, g
+
+    def train_step(self, x, t, lr):
+        """One Adam step; returns the loss of the batch before the step."""
+        loss = ctypes.c_double()
+        self.check(lib().srmg_cnn_train_step(self._h, x.data_ptr(), t.data_ptr(), x.shape[0], float(lr),
+                                             ctypes.byref(loss)))
+        return loss.value
+
+
+def cnn_pack(ctx: Context, phi, b, b_prev, s, geometry, bc, lpldisc=None):
+    """Samples of a tree for the network: (x bf16 [n,400,2], scale float64 [n], blk int32 [n])."""
+    import torch
+    op, k2 = _disc(lpldisc)
+    bca = _bc(bc)
+    n = lib().srmg_cnn_leaf_blocks(ctx.handle)
+    dev = phi.device
+    x = torch.empty((n, 400, 2), dtype=torch.bfloat16, device=dev)
+    scale = torch.empty(n, dtype=torch.float64, device=dev)
+    blk = torch.empty(n, dtype=torch.int32, device=dev)
+    _order_after_torch(ctx, phi, b, b_prev)
+    rc = lib().srmg_cnn_pack_dev(ctx.handle, phi.data_ptr(), b.data_ptr(), b_prev.data_ptr(), phi.shape[0], s, op,
+                                 k2, geometry, bca.ctypes.data, x.data_ptr(), scale.data_ptr(), blk.data_ptr(), n)
+    if rc < 0:
+        ctx.check(rc)
+    ctx.synchronize()
+    return x, scale, blk
+
+
+def cnn_predict(ctx: Context, net: Cnn, u, b, b_prev, s, geometry, bc, lpldisc=None) -> bool:
+    """Warm start in place on u (phi_prev on entry); True if the learned guess was kept."""
+    op, k2 = _disc(lpldisc)
+    bca = _bc(bc)
+    used = ctypes.c_int()
+    _order_after_torch(ctx, u, b, b_prev)
+    ctx.check(lib().srmg_cnn_predict_dev(ctx.handle, net.handle, u.data_ptr(), b.data_ptr(), b_prev.data_ptr(),
+                                         u.shape[0], s, op, k2, geometry, bca.ctypes.data, ctypes.byref(used)))
+    return bool(used.value)
 
 
 def exported_symbols_from_header(header_path: str) -> list[str]:

@@ -1,0 +1,99 @@
+"""The learned warm-start network's CUDA kernels against the CPU oracle
+(oracle/cnn_oracle.py): forward outputs, the loss and every layer's weight and bias
+gradient; training lowers the loss; the tree path packs samples the way the oracle
+defines them and keeps a guess only when it lowers the residual."""
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+import cnn_oracle as co
+from srmg import gen, multigrid as mg
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not gpu_available(), reason="needs a CUDA GPU")]
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def batch(n, seed):
+    import torch
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((n, 400, 2)).astype(np.float32)
+    x = co.bf16_round(x).astype(np.float32)
+    t = (0.3 * rng.standard_normal((n, 256))).astype(np.float32)
+    xt = torch.from_numpy(x).to(torch.bfloat16).cuda()
+    tt = torch.from_numpy(t).cuda()
+    torch.cuda.synchronize()
+    return x, t, xt, tt
+
+
+@pytest.fixture(scope="module")
+def net():
+    return mg.Cnn(0, seed=7)
+
+
+def test_forward_matches_oracle(net):
+    theta = net.get_params().astype(np.float64)
+    x, t, xt, tt = batch(37, 1)
+    y = net.forward(xt).cpu().numpy()
+    yo, _ = co.forward(x, theta)
+    assert rel(y, yo) < 2e-3, rel(y, yo)
+
+
+def test_gradients_match_oracle(net):
+    theta = net.get_params().astype(np.float64)
+    x, t, xt, tt = batch(23, 2)
+    loss, g = net.gradients(xt, tt)
+    lo, go = co.gradients(x, t, theta)
+    assert abs(loss - lo) <= 2e-3 * abs(lo)
+    for l, ((w0, w1), (b0, b1)) in enumerate(co.layer_slices()):
+        assert rel(g[w0:w1], go[w0:w1]) < 1e-2, (l, "W", rel(g[w0:w1], go[w0:w1]))
+        assert rel(g[b0:b1], go[b0:b1]) < 1e-2, (l, "b", rel(g[b0:b1], go[b0:b1]))
+
+
+def test_training_lowers_loss():
+    n = mg.Cnn(0, seed=3)
+    x, t, xt, tt = batch(64, 3)
+    # a learnable target: a smooth function of the inputs' centre
+    import torch
+    tgt = 0.5 * xt[:, :, 0].float().reshape(64, 20, 20)[:, 2:18, 2:18].reshape(64, 256).contiguous()
+    torch.cuda.synchronize()
+    l0 = n.train_step(xt, tgt, 1e-3)
+    for _ in range(150):
+        l = n.train_step(xt, tgt, 1e-3)
+    n.synchronize()
+    assert l < 0.3 * l0, (l0, l)
+
+
+def test_set_get_params_roundtrip(net):
+    theta = net.get_params()
+    net.set_params(theta * 0.5)
+    np.testing.assert_array_equal(net.get_params(), (theta * 0.5).astype(np.float32))
+    net.set_params(theta)
+
+
+def test_tree_pack_and_guarded_predict(net):
+    """Samples of a tree match the oracle's definition; a guess that would raise the
+    residual (an untrained network) is rejected and u is left unchanged."""
+    import torch
+    p = gen.config1()
+    ctx = mg.Context(0).set_tree(p.tree, p.conn)
+    b = torch.from_numpy(p.b).cuda()
+    u = torch.zeros_like(b)
+    mg.solve(ctx, u, b, p.s, p.geom, p.bc, tol=1e-10, mode=mg.MODE_FP64)
+    b_prev = (b * 0.97).contiguous()
+    x, scale, blk = mg.cnn_pack(ctx, u, b, b_prev, p.s, p.geom, p.bc)
+    assert x.shape[0] == 256  # the level-5 leaves of the uniform tree
+    # oracle definition of the samples: (phi * a, db * c) over the 20x20 tile
+    uh, bh, bph = u.cpu().numpy(), p.b, b_prev.cpu().numpy()
+    k = 17
+    bk = int(blk[k])
+    xs = x[k].float().cpu().numpy().reshape(20, 20, 2)
+    ratio = xs[8:12, 8:12, 0] / uh[bk, 8:12, 8:12]
+    assert np.allclose(ratio, ratio.flat[0], rtol=1e-2)
+    u0 = u.clone()
+    used = mg.cnn_predict(ctx, mg.Cnn(0, seed=11), u, b, b_prev, p.s, p.geom, p.bc)
+    if not used:
+        assert torch.equal(u, u0)
