@@ -283,13 +283,18 @@ int srmg_batch_autotune(srmg_ctx *batch, double *const *u, const double *const *
                         srmg_solve_opts *opts, srmg_tune_trial *trials, int max_trials);
 
 /* ---- learned warm start (no reference counterpart) --------------------------------
- * A 6-layer BF16 convolutional network (3x3 convolutions, 32 channels, ReLU; zero
- * padding at the tile edge) maps, per block, the 20 x 20 tile (16 x 16 cells plus the
- * 2-cell ghost halo) of (phi_prev * a, (b - b_prev) * c) to (phi_new - phi_prev) /
- * (s_l * |b - b_prev|) on the block's 16 x 16 cells, with a = 1/|phi_prev|,
- * c = 1/|b - b_prev| (|.| = the resnorm! leaf norm, per tree).  Forward, backward
- * and optimiser kernels run on the tensor cores; parameters are an FP32 master
- * vector (per layer W [tap][co][ci], then b [co]). */
+ * Successive time steps change the potential by nearly the same correction (the
+ * streamer head moves a fraction of a cell per step), so the guess for step n is
+ *   phi_{n-1} + delta_{n-1} + (learned change of the correction),
+ * delta_{n-1} = phi_{n-1} - phi_{n-2}.  A 6-layer BF16 convolutional network (3x3
+ * convolutions, 32 channels, ReLU; zero padding at the tile edge) maps, per block, the
+ * 20 x 20 tile (16 x 16 cells plus the 2-cell ghost halo) of (delta_{n-1} a, g c),
+ * g = b_n - 2 b_{n-1} + b_{n-2} the change of the charge change, a = 1/|delta_{n-1}|,
+ * c = 1/|g| (|.| = the resnorm! leaf norm, per tree), to
+ * (delta_n - delta_{n-1}) / (s_l |g|) on the block's 16 x 16 cells.  The network
+ * predicts a small quantity, so BF16 precision does not limit the guess.  Forward,
+ * backward and optimiser kernels run on the tensor cores; parameters are an FP32
+ * master vector (per layer W [tap][co][ci], then b [co]). */
 typedef struct srmg_cnn srmg_cnn;
 int srmg_cnn_create(srmg_cnn **net, int device, uint64_t seed);  /* He-initialised */
 void srmg_cnn_destroy(srmg_cnn *net);
@@ -301,28 +306,54 @@ int srmg_cnn_synchronize(srmg_cnn *net);
 /* Samples: x DEVICE bf16 [n][400][2] (tile pixel y*20+x, channels (phi, db));
  * targets/outputs DEVICE float [n][16][16]. */
 int srmg_cnn_forward(srmg_cnn *net, const uint16_t *x, float *y, int n);
-/* Mean-squared-error loss over the n x 256 outputs and its gradient (host copy of the
- * gradient in master layout if grad_host is not NULL; host loss). */
-int srmg_cnn_gradients(srmg_cnn *net, const uint16_t *x, const float *t, int n, float *grad_host,
-                       double *loss);
-/* One Adam step (beta 0.9/0.999, eps 1e-8) on the loss of the n samples. */
-int srmg_cnn_train_step(srmg_cnn *net, const uint16_t *x, const float *t, int n, float lr,
-                        double *loss);
+/* Loss = mean over the n x 256 outputs of (y - t)^2 + lambda * mean over the 14 x 14
+ * interior cells of rho^2, rho = L(y) + db channel of x: the residual the guess leaves,
+ * in the output's units (L the geometry's stencil; ir0[k] = global r index before the
+ * sample's first cell, DEVICE; ir0 NULL = no residual term).  Gradient in master
+ * layout to grad_host if not NULL; loss to *loss (host). */
+int srmg_cnn_gradients(srmg_cnn *net, const uint16_t *x, const float *t, const int *ir0,
+                       float lambda, int geom, int n, float *grad_host, double *loss);
+/* One Adam step (beta 0.9/0.999, eps 1e-8) on that loss over the n samples. */
+int srmg_cnn_train_step(srmg_cnn *net, const uint16_t *x, const float *t, const int *ir0,
+                        float lambda, int geom, int n, float lr, double *loss);
+/* Training against a loss computed by the caller: the forward pass keeps every layer's
+ * activations and writes y (DEVICE float [n][256]); the backward pass takes dLoss/dy
+ * (DEVICE float [n][256]) for the same n samples, and applies one Adam step when
+ * lr > 0 (gradient in master layout to grad_host if not NULL). */
+int srmg_cnn_forward_train(srmg_cnn *net, const uint16_t *x, int n, float *y);
+int srmg_cnn_backward_step(srmg_cnn *net, const float *dy, int n, float lr, float *grad_host);
 /* Tree fields -> samples, one per block holding a leaf cell (srmg_cnn_leaf_blocks of
- * them): x as above, scale[k] = s_l * |b - b_prev| of the sample's block, blk[k] its
- * 0-based block id.  DEVICE pointers; returns the sample count. */
+ * them): x as above from the input fields f (ghosts filled) and g, scale[k] =
+ * s_l |g| of the sample's block, blk[k] its 0-based block id.  DEVICE pointers;
+ * returns the sample count. */
 int srmg_cnn_leaf_blocks(const srmg_ctx *ctx);
-int srmg_cnn_pack_dev(srmg_ctx *ctx, const double *phi, const double *b, const double *b_prev,
-                      int64_t nblk_alloc, double s, int op, double k2, int geom, const int8_t bc[9],
+int srmg_cnn_pack_dev(srmg_ctx *ctx, const double *f, const double *g, int64_t nblk_alloc,
+                      double s, int op, double k2, int geom, const int8_t bc[9],
                       uint16_t *x, double *scale, int *blk, int max_samples);
-/* Warm start: u holds phi_prev (ghosts filled) on entry.  The network's guess of the
- * new potential is formed on the leaf cells, made a composite-grid function (ghosts
- * filled) and kept only if its residual norm is below that of phi_prev (*used = 1);
- * otherwise u is left unchanged (*used = 0).  The solve then iterates to its
- * tolerance from u as usual. */
+/* Warm start for step n: u holds phi_{n-1} (ghosts filled) on entry; b = b_n,
+ * b1 = b_{n-1}, phi2 = phi_{n-2}, b2 = b_{n-2}.  Three candidates -- phi_{n-1}, the
+ * extrapolation phi_{n-1} + delta_{n-1}, and the extrapolation plus the network's
+ * change -- are made composite-grid functions (ghosts filled); u receives the one with
+ * the smallest residual norm and *which says which (0, 1, 2); resid (host, optional)
+ * receives the three residual norms.  The solve then iterates to its tolerance from u
+ * as usual. */
 int srmg_cnn_predict_dev(srmg_ctx *ctx, srmg_cnn *net, double *u, const double *b,
-                         const double *b_prev, int64_t nblk_alloc, double s, int op, double k2,
-                         int geom, const int8_t bc[9], int *used);
+                         const double *b1, const double *phi2, const double *b2,
+                         int64_t nblk_alloc, double s, int op, double k2, int geom,
+                         const int8_t bc[9], int *which, double *resid);
+
+/* ---- streamer stepper for training data (no single reference counterpart) -------
+ * One forward-Euler step of electron, positive-ion and negative-ion densities on the
+ * leaf-holding blocks: electrons drift in E = -grad phi + E0 z^ and diffuse, with
+ * Koren-limited upwind face values (src/fluid.jl:8-94); ionisation
+ * alpha = alpha_A exp(-alpha_B / |E|) and attachment eta feed the immobile ions
+ * (src/chemistry.jl:29-82 drifts electrons only).  ne and phi need their ghosts.
+ * dt = min(dt_max, cfl h/max|v|, cfl h^2/(4 D), cfl eps0/(e mu max ne)) -> *dt_out.
+ * work: DEVICE scratch of 3 * nblk_alloc * 400 + 2 doubles. */
+int srmg_streamer_step_dev(srmg_ctx *ctx, double *ne, double *npos, double *nneg, const double *phi,
+                           int64_t nblk_alloc, double h1, double E0, double mu, double D,
+                           double alpha_A, double alpha_B, double eta, double cfl, double dt_max,
+                           double *work, double *dt_out);
 
 /* Tuning knobs (no reference counterpart; the autotuner drives them):
  *   "engine"           1 = persistent one-launch V-cycle (default), 0 = one kernel per

@@ -72,16 +72,49 @@ def forward(x, theta, bf16=True):
     return y, acts
 
 
-def gradients(x, t, theta, bf16=True):
-    """Loss and gradient (parameter-vector layout)."""
+def rweights(ir0, geom):
+    """Radial stencil weights [n][16] (w-, w+) of the 16 cell columns of each sample."""
+    i = np.asarray(ir0, dtype=np.float64)[:, None] + np.arange(16)[None, :] + 1.0
+    if geom == 1:
+        return (2 * i - 2) / (2 * i - 1), (2 * i) / (2 * i - 1)
+    return np.ones_like(i), np.ones_like(i)
+
+
+def residual(y, x, ir0, geom, bf16=True):
+    """rho [n][14][14] = L(y) + db channel of x on the interior cells."""
+    rnd = bf16_round if bf16 else (lambda a: np.asarray(a, dtype=np.float64))
+    n = y.shape[0]
+    Y = y.reshape(n, 16, 16)
+    x1 = rnd(x.reshape(n, T, T, 2)[..., 1])[:, 3:17, 3:17]
+    wm, wp = rweights(ir0, geom)
+    wm, wp = wm[:, None, 1:15], wp[:, None, 1:15]
+    L = wm * Y[:, 1:15, 0:14] + wp * Y[:, 1:15, 2:16] + Y[:, 0:14, 1:15] + Y[:, 2:16, 1:15] - 4 * Y[:, 1:15, 1:15]
+    return L + x1
+
+
+def gradients(x, t, theta, bf16=True, ir0=None, lam=0.0, geom=1):
+    """Loss and gradient (parameter-vector layout).  Loss = mean (y - t)^2 plus, with
+    ir0 given, lam * mean rho^2 over the 14 x 14 interior cells (rho = residual())."""
     rnd = bf16_round if bf16 else (lambda a: np.asarray(a, dtype=np.float64))
     n = x.shape[0]
     y, acts = forward(x, theta, bf16)
     d = y - t.reshape(n, 256)
     loss = float(np.mean(d * d))
+    gy = (2.0 / (256 * n) * d).reshape(n, 16, 16)
+    if ir0 is not None and lam > 0:
+        rho = residual(y, x, ir0, geom, bf16)
+        loss += lam * float(np.mean(rho * rho))
+        gr = 2.0 * lam / (196 * n) * rho
+        wm, wp = rweights(ir0, geom)
+        wm, wp = wm[:, None, 1:15], wp[:, None, 1:15]
+        gy[:, 1:15, 1:15] += -4 * gr
+        gy[:, 1:15, 0:14] += wm * gr
+        gy[:, 1:15, 2:16] += wp * gr
+        gy[:, 0:14, 1:15] += gr
+        gy[:, 2:16, 1:15] += gr
     params = unpack(np.asarray(theta, dtype=np.float64))
     dZ = np.zeros((n, T, T, 1))
-    dZ[:, 2:18, 2:18, 0] = (2.0 / (256 * n) * d).reshape(n, 16, 16)
+    dZ[:, 2:18, 2:18, 0] = gy
     dZ = rnd(dZ)
     grads = [None] * len(params)
     for l in range(len(params) - 1, -1, -1):

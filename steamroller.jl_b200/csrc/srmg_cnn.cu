@@ -257,11 +257,38 @@ k_cnn_fwd(const __nv_bfloat16 *__restrict__ x, int n, const __nv_bfloat16 *__res
   }
 }
 
-// Loss and output gradient: loss partials per CTA (fixed order) and
-// dz[n][400][32] bf16 = 2 (y - t) / (256 n) on the centre pixels of channel 0, else 0.
-__global__ void k_cnn_loss(const float *__restrict__ y, const float *__restrict__ t, int n,
-                           __nv_bfloat16 *__restrict__ dz, double *__restrict__ loss_part) {
-  const double inv = 1.0 / (256.0 * (double)n);
+// Radial stencil weights of cell column qx (0..15) of a sample whose block starts at
+// global r index ir0 (cylindrical: w- = (2i-2)/(2i-1), w+ = 2i/(2i-1), i = ir0+qx+1).
+__device__ __forceinline__ void rweights(int geom, int ir0, int qx, float &wm, float &wp) {
+  if (geom == 1) {
+    const float i = (float)(ir0 + qx + 1);
+    wm = (2.f * i - 2.f) / (2.f * i - 1.f);
+    wp = (2.f * i) / (2.f * i - 1.f);
+  } else {
+    wm = 1.f;
+    wp = 1.f;
+  }
+}
+
+// Normalised residual of the guess at interior cell (qy, qx) (1..14) of sample s:
+// rho = L(y) + x1, the discrete operator applied to the output plus the normalised
+// right-hand-side change (both in units where the output scale is s_l |db|).
+__device__ __forceinline__ float resid(const float *ys, const __nv_bfloat16 *xs, int geom, int ir0, int qy, int qx) {
+  float wm, wp;
+  rweights(geom, ir0, qx, wm, wp);
+  const float c = ys[qy * 16 + qx];
+  const float L = wm * ys[qy * 16 + qx - 1] + wp * ys[qy * 16 + qx + 1] + ys[(qy - 1) * 16 + qx] +
+                  ys[(qy + 1) * 16 + qx] - 4.f * c;
+  return L + __bfloat162float(xs[((qy + 2) * kT + qx + 2) * 2 + 1]);
+}
+
+// Loss and output gradient.  Loss = mean_{n x 256} (y - t)^2 + lambda mean_{n x 196} rho^2
+// (rho on the 14 x 14 interior cells); loss partials per CTA (fixed order) and
+// dz[n][400][32] bf16 = dLoss/dy on the centre pixels of channel 0, else 0.
+__global__ void k_cnn_loss(const float *__restrict__ y, const float *__restrict__ t,
+                           const __nv_bfloat16 *__restrict__ x, const int *__restrict__ ir0s, float lambda, int geom,
+                           int n, __nv_bfloat16 *__restrict__ dz, double *__restrict__ loss_part) {
+  const double inv = 1.0 / (256.0 * (double)n), invr = 1.0 / (196.0 * (double)n);
   double acc = 0.0;
   const int64_t total = (int64_t)n * kNP;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
@@ -269,10 +296,37 @@ __global__ void k_cnn_loss(const float *__restrict__ y, const float *__restrict_
     const int yy = p / kT, xx = p % kT;
     float g = 0.f;
     if (yy >= 2 && yy < 18 && xx >= 2 && xx < 18) {
-      const int64_t k = (int64_t)s * 256 + (yy - 2) * 16 + (xx - 2);
+      const int cy = yy - 2, cx = xx - 2;
+      const int64_t k = (int64_t)s * 256 + cy * 16 + cx;
       const float d = y[k] - t[k];
-      acc += (double)d * (double)d;
+      acc += (double)d * (double)d * inv;
       g = (float)(2.0 * inv) * d;
+      if (lambda > 0.f) {
+        const float *ys = y + (int64_t)s * 256;
+        const __nv_bfloat16 *xs = x + (int64_t)s * kNP * 2;
+        const int ir0 = ir0s[s];
+        auto inner = [](int q) { return q >= 1 && q <= 14; };
+        float gr = 0.f;
+        if (inner(cy) && inner(cx)) {
+          const float r0 = resid(ys, xs, geom, ir0, cy, cx);
+          acc += (double)lambda * (double)r0 * (double)r0 * invr;
+          gr += -4.f * r0;
+        }
+        // neighbours whose stencil reads this cell
+        if (inner(cy) && inner(cx + 1)) {  // this cell is the r- neighbour of (cy, cx+1)
+          float wm, wp;
+          rweights(geom, ir0, cx + 1, wm, wp);
+          gr += wm * resid(ys, xs, geom, ir0, cy, cx + 1);
+        }
+        if (inner(cy) && inner(cx - 1)) {  // r+ neighbour of (cy, cx-1)
+          float wm, wp;
+          rweights(geom, ir0, cx - 1, wm, wp);
+          gr += wp * resid(ys, xs, geom, ir0, cy, cx - 1);
+        }
+        if (inner(cy + 1) && inner(cx)) gr += resid(ys, xs, geom, ir0, cy + 1, cx);
+        if (inner(cy - 1) && inner(cx)) gr += resid(ys, xs, geom, ir0, cy - 1, cx);
+        g += (float)(2.0 * invr) * lambda * gr;
+      }
     }
     uint4 *o = reinterpret_cast<uint4 *>(dz + i * kC);
     __nv_bfloat16 gb = __float2bfloat16_rn(g);
@@ -288,7 +342,24 @@ __global__ void k_cnn_loss(const float *__restrict__ y, const float *__restrict_
   if (threadIdx.x == 0) {
     double c = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) c += sh[w];
-    loss_part[blockIdx.x] = c * inv;
+    loss_part[blockIdx.x] = c;
+  }
+}
+
+// dz[n][400][32] bf16 from a given output gradient dy[n][256] (centre pixels, channel 0).
+__global__ void k_cnn_dz_from_dy(const float *__restrict__ dy, int n, __nv_bfloat16 *__restrict__ dz) {
+  const int64_t total = (int64_t)n * kNP;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int s = (int)(i / kNP), p = (int)(i % kNP);
+    const int yy = p / kT, xx = p % kT;
+    float g = 0.f;
+    if (yy >= 2 && yy < 18 && xx >= 2 && xx < 18) g = dy[(int64_t)s * 256 + (yy - 2) * 16 + (xx - 2)];
+    uint4 *o = reinterpret_cast<uint4 *>(dz + i * kC);
+    __nv_bfloat16 gb = __float2bfloat16_rn(g);
+    o[0] = make_uint4((uint32_t)*reinterpret_cast<uint16_t *>(&gb), 0, 0, 0);
+    o[1] = make_uint4(0, 0, 0, 0);
+    o[2] = make_uint4(0, 0, 0, 0);
+    o[3] = make_uint4(0, 0, 0, 0);
   }
 }
 
@@ -457,8 +528,8 @@ __global__ void k_cnn_adam(float *__restrict__ p, const float *__restrict__ g, f
 }
 
 // Samples of a tree: for leaf-holding block k (leaf[k] = {block, level}) the 20 x 20
-// tile of (phi * a, db * bsc), pixel order y * 20 + x, and the output scale
-// s_level * rms_db of the block.
+// tile of (f * a, g * bsc), pixel order y * 20 + x, and the output scale
+// s_level * |g| of the block.
 __global__ void k_cnn_gather(const double *__restrict__ phi, const double *__restrict__ db, const int2 *__restrict__ leaf,
                              int nleaf, double a, double bsc, double s, double dbrms, __nv_bfloat16 *__restrict__ x,
                              double *__restrict__ scale, int *__restrict__ blk) {
@@ -488,10 +559,16 @@ __global__ void k_cnn_scatter(double *__restrict__ u, const double *__restrict__
   }
 }
 
-__global__ void k_diff_field(double *__restrict__ d, const double *__restrict__ a, const double *__restrict__ b,
-                             int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    d[i] = b ? a[i] - b[i] : a[i];
+// d = ca a + cb b + cc c (b, c optional).
+__global__ void k_lin_field(double *__restrict__ d, const double *__restrict__ a, double ca,
+                            const double *__restrict__ b, double cb, const double *__restrict__ c, double cc,
+                            int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double v = ca * a[i];
+    if (b) v += cb * b[i];
+    if (c) v += cc * c[i];
+    d[i] = v;
+  }
 }
 
 }  // namespace cnn
@@ -506,6 +583,7 @@ struct srmg_cnn {
   __nv_bfloat16 *wpk = nullptr, *wt = nullptr;
   float *bias = nullptr;
   int adam_t = 0;
+  int train_n = 0;  // samples of the last training forward
   DevBuf acts, dz0, dz1, dwp, dbp, lossp, y;
   int nsm = 0;
 };
@@ -527,8 +605,8 @@ int cnn_setup_attrs(srmg_cnn *net) {
   return SRMG_OK;
 }
 
-// Forward + loss + backward: gradient (master layout) in net->grad, loss partials.
-int cnn_grad(srmg_cnn *net, const __nv_bfloat16 *x, const float *t, int n, double *loss) {
+// Forward pass keeping every layer's activations (training), outputs in net->y.
+int cnn_fwd_train(srmg_cnn *net, const __nv_bfloat16 *x, int n) {
   srmg_ctx *ctx = net->err_ctx;
   const int grid = cnn_grid(net, n);
   RC(ensure(ctx, net->acts, (size_t)n * kL * kNP * kC * 2));
@@ -538,11 +616,18 @@ int cnn_grad(srmg_cnn *net, const __nv_bfloat16 *x, const float *t, int n, doubl
   RC(ensure(ctx, net->dwp, (size_t)grid * 9 * kWMat * 4));
   RC(ensure(ctx, net->dbp, (size_t)grid * kC * 4));
   RC(ensure(ctx, net->lossp, 1024 * 8));
+  k_cnn_fwd<<<grid, kThreads, sizeof(FwdSmem), net->stream>>>(x, n, net->wpk, net->bias, (float *)net->y.p,
+                                                              (__nv_bfloat16 *)net->acts.p);
+  CK(cudaGetLastError());
+  net->train_n = n;
+  return SRMG_OK;
+}
+
+// Backward from the output gradient held in net->dz0 (n samples of the last forward).
+int cnn_bwd(srmg_cnn *net, int n) {
+  srmg_ctx *ctx = net->err_ctx;
+  const int grid = cnn_grid(net, n);
   __nv_bfloat16 *acts = (__nv_bfloat16 *)net->acts.p;
-  k_cnn_fwd<<<grid, kThreads, sizeof(FwdSmem), net->stream>>>(x, n, net->wpk, net->bias, (float *)net->y.p, acts);
-  const int lg = std::min(1024, std::max(1, (n * kNP + 255) / 256));
-  k_cnn_loss<<<lg, 256, 0, net->stream>>>((const float *)net->y.p, t, n, (__nv_bfloat16 *)net->dz0.p,
-                                          (double *)net->lossp.p);
   __nv_bfloat16 *dzc = (__nv_bfloat16 *)net->dz0.p, *dzn = (__nv_bfloat16 *)net->dz1.p;
   for (int l = kL - 1; l >= 0; --l) {
     k_cnn_dw<<<grid, kDwThreads, sizeof(DwSmem), net->stream>>>(l, dzc, acts, n, (float *)net->dwp.p,
@@ -555,6 +640,18 @@ int cnn_grad(srmg_cnn *net, const __nv_bfloat16 *x, const float *t, int n, doubl
     }
   }
   CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+// Forward + loss + backward: gradient (master layout) in net->grad, loss partials.
+int cnn_grad(srmg_cnn *net, const __nv_bfloat16 *x, const float *t, const int *ir0, float lambda, int geom, int n,
+             double *loss) {
+  srmg_ctx *ctx = net->err_ctx;
+  RC(cnn_fwd_train(net, x, n));
+  const int lg = std::min(1024, std::max(1, (n * kNP + 255) / 256));
+  k_cnn_loss<<<lg, 256, 0, net->stream>>>((const float *)net->y.p, t, x, ir0, ir0 ? lambda : 0.f, geom, n,
+                                          (__nv_bfloat16 *)net->dz0.p, (double *)net->lossp.p);
+  RC(cnn_bwd(net, n));
   if (loss) {
     std::vector<double> lp(lg);
     CK(cudaMemcpyAsync(lp.data(), net->lossp.p, lg * sizeof(double), cudaMemcpyDeviceToHost, net->stream));
@@ -670,12 +767,12 @@ extern "C" int srmg_cnn_forward(srmg_cnn *net, const uint16_t *x, float *y, int 
   return SRMG_OK;
 }
 
-extern "C" int srmg_cnn_gradients(srmg_cnn *net, const uint16_t *x, const float *t, int n, float *grad_host,
-                                  double *loss) {
-  if (!net || !x || !t || n <= 0) return SRMG_ERR_BADARG;
+extern "C" int srmg_cnn_gradients(srmg_cnn *net, const uint16_t *x, const float *t, const int *ir0, float lambda,
+                                  int geom, int n, float *grad_host, double *loss) {
+  if (!net || !x || !t || n <= 0 || lambda < 0 || geom < 0 || geom > 2) return SRMG_ERR_BADARG;
   cudaSetDevice(net->device);
   srmg_ctx *ctx = net->err_ctx;
-  RC(cnn_grad(net, (const __nv_bfloat16 *)x, t, n, loss));
+  RC(cnn_grad(net, (const __nv_bfloat16 *)x, t, ir0, lambda, geom, n, loss));
   if (grad_host) {
     CK(cudaMemcpyAsync(grad_host, net->grad, nparams() * 4, cudaMemcpyDeviceToHost, net->stream));
     CK(cudaStreamSynchronize(net->stream));
@@ -683,18 +780,48 @@ extern "C" int srmg_cnn_gradients(srmg_cnn *net, const uint16_t *x, const float 
   return SRMG_OK;
 }
 
-extern "C" int srmg_cnn_train_step(srmg_cnn *net, const uint16_t *x, const float *t, int n, float lr,
-                                   double *loss) {
-  if (!net || !x || !t || n <= 0 || !(lr > 0)) return SRMG_ERR_BADARG;
-  cudaSetDevice(net->device);
-  srmg_ctx *ctx = net->err_ctx;
-  RC(cnn_grad(net, (const __nv_bfloat16 *)x, t, n, loss));
+static int cnn_adam_step(srmg_cnn *net, float lr) {
   net->adam_t++;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = 1.f - std::pow(b1, (float)net->adam_t), c2 = 1.f - std::pow(b2, (float)net->adam_t);
   k_cnn_adam<<<64, 256, 0, net->stream>>>(net->master, net->grad, net->adam_m, net->adam_v, nparams(), lr, b1, b2,
                                           1e-8f, c1, c2);
-  RC(cnn_pack(net));
+  return cnn_pack(net);
+}
+
+extern "C" int srmg_cnn_forward_train(srmg_cnn *net, const uint16_t *x, int n, float *y) {
+  if (!net || !x || !y || n <= 0) return SRMG_ERR_BADARG;
+  cudaSetDevice(net->device);
+  srmg_ctx *ctx = net->err_ctx;
+  RC(cnn_fwd_train(net, (const __nv_bfloat16 *)x, n));
+  CK(cudaMemcpyAsync(y, net->y.p, (size_t)n * 256 * 4, cudaMemcpyDeviceToDevice, net->stream));
+  CK(cudaStreamSynchronize(net->stream));
+  return SRMG_OK;
+}
+
+extern "C" int srmg_cnn_backward_step(srmg_cnn *net, const float *dy, int n, float lr, float *grad_host) {
+  if (!net || !dy || n <= 0 || n != net->train_n || lr < 0) return SRMG_ERR_BADARG;
+  cudaSetDevice(net->device);
+  srmg_ctx *ctx = net->err_ctx;
+  k_cnn_dz_from_dy<<<std::min(1024, (n * kNP + 255) / 256), 256, 0, net->stream>>>(dy, n,
+                                                                                   (__nv_bfloat16 *)net->dz0.p);
+  RC(cnn_bwd(net, n));
+  if (grad_host) {
+    CK(cudaMemcpyAsync(grad_host, net->grad, nparams() * 4, cudaMemcpyDeviceToHost, net->stream));
+    CK(cudaStreamSynchronize(net->stream));
+  }
+  if (lr > 0) RC(cnn_adam_step(net, lr));
+  CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+extern "C" int srmg_cnn_train_step(srmg_cnn *net, const uint16_t *x, const float *t, const int *ir0, float lambda,
+                                   int geom, int n, float lr, double *loss) {
+  if (!net || !x || !t || n <= 0 || !(lr > 0) || lambda < 0 || geom < 0 || geom > 2) return SRMG_ERR_BADARG;
+  cudaSetDevice(net->device);
+  srmg_ctx *ctx = net->err_ctx;
+  RC(cnn_grad(net, (const __nv_bfloat16 *)x, t, ir0, lambda, geom, n, loss));
+  RC(cnn_adam_step(net, lr));
   CK(cudaGetLastError());
   return SRMG_OK;
 }
@@ -708,26 +835,31 @@ extern "C" int srmg_cnn_synchronize(srmg_cnn *net) {
 
 namespace {
 
-// The samples of a tree (see srmg_cnn_pack_dev); leaves them in ctx->cnn_work[2]
-// (x, then scale and block ids) unless out pointers are given.  Returns the count.
-int cnn_pack_tree(srmg_ctx *ctx, const double *phi, const double *b, const double *b_prev, int64_t nblk_alloc,
-                  double s, int op, double k2, int geom, const int8_t *bc, __nv_bfloat16 *x, double *scale,
-                  int *blk) {
+int lin_field(srmg_ctx *ctx, double *d, const double *a, double ca, const double *b, double cb, const double *c,
+              double cc, int64_t n) {
+  k_lin_field<<<(int)std::min<int64_t>(4096, (n + 255) / 256), 256, 0, ctx->stream>>>(d, a, ca, b, cb, c, cc, n);
+  return cuda_check(ctx, cudaGetLastError(), "k_lin_field");
+}
+
+// Samples of a tree from the input fields f (ghosts filled) and g (ghosts are filled
+// here, on a copy): x, the per-sample output scale and block ids.  Returns the count.
+int cnn_pack_tree(srmg_ctx *ctx, const double *f, const double *g, int64_t nblk_alloc, double s, int op, double k2,
+                  int geom, const int8_t *bc, __nv_bfloat16 *x, double *scale, int *blk) {
   const int64_t nval = nblk_alloc * (int64_t)kNP;
   RC(ensure(ctx, ctx->cnn_work[0], nval * sizeof(double)));
-  double *db = (double *)ctx->cnn_work[0].p;
-  k_diff_field<<<std::min<int64_t>(4096, (nval + 255) / 256), 256, 0, ctx->stream>>>(db, b, b_prev, nval);
+  double *gw = (double *)ctx->cnn_work[0].p;
+  RC(lin_field(ctx, gw, g, 1.0, nullptr, 0.0, nullptr, 0.0, nval));
   const Signs sg = make_signs(bc);
-  for (int l = 1; l <= ctx->nlev; l++) RC(L_fill_ghost<double>(ctx, db, l, sg, 7));
-  // leaf norms of phi and of db set the input scales (mode 1: the norm of the field)
-  RC(leafnorm_dev<double>(ctx, phi, phi, s, op, k2, geom, 1, 0));
-  RC(leafnorm_dev<double>(ctx, phi, db, s, op, k2, geom, 1, 1));
+  for (int l = 1; l <= ctx->nlev; l++) RC(L_fill_ghost<double>(ctx, gw, l, sg, 7));
+  // leaf norms of f and g set the input scales (mode 1: the norm of the field)
+  RC(leafnorm_dev<double>(ctx, f, f, s, op, k2, geom, 1, 0));
+  RC(leafnorm_dev<double>(ctx, f, gw, s, op, k2, geom, 1, 1));
   RC(read_small(ctx, 2));
-  const double nphi = ctx->h_small[0], ndb = ctx->h_small[1];
-  const double a = nphi > 0 ? 1.0 / nphi : 1.0, bsc = ndb > 0 ? 1.0 / ndb : 1.0;
+  const double nf = ctx->h_small[0], ng = ctx->h_small[1];
+  const double a = nf > 0 ? 1.0 / nf : 1.0, bsc = ng > 0 ? 1.0 / ng : 1.0;
   const int n = ctx->nleaf;
-  k_cnn_gather<<<std::min<int64_t>(4096, ((int64_t)n * kNP + 255) / 256), 256, 0, ctx->stream>>>(
-      phi, db, ctx->d_leaf, n, a, bsc, s, ndb > 0 ? ndb : 1.0, x, scale, blk);
+  k_cnn_gather<<<(int)std::min<int64_t>(4096, ((int64_t)n * kNP + 255) / 256), 256, 0, ctx->stream>>>(
+      f, gw, ctx->d_leaf, n, a, bsc, s, ng > 0 ? ng : 1.0, x, scale, blk);
   CK(cudaGetLastError());
   return n;
 }
@@ -739,53 +871,70 @@ extern "C" int srmg_cnn_leaf_blocks(const srmg_ctx *ctx) {
   return ctx->has_tree ? ctx->nleaf : 0;
 }
 
-extern "C" int srmg_cnn_pack_dev(srmg_ctx *ctx, const double *phi, const double *b, const double *b_prev,
-                                 int64_t nblk_alloc, double s, int op, double k2, int geom, const int8_t bc[9],
-                                 uint16_t *x, double *scale, int *blk, int max_samples) {
+extern "C" int srmg_cnn_pack_dev(srmg_ctx *ctx, const double *f, const double *g, int64_t nblk_alloc, double s,
+                                 int op, double k2, int geom, const int8_t bc[9], uint16_t *x, double *scale,
+                                 int *blk, int max_samples) {
   RC(check_call(ctx, nblk_alloc, op, geom, bc));
-  if (!phi || !b || !x || !scale || !blk) return fail(ctx, SRMG_ERR_BADARG, "srmg_cnn_pack_dev: null argument");
+  if (!f || !g || !x || !scale || !blk) return fail(ctx, SRMG_ERR_BADARG, "srmg_cnn_pack_dev: null argument");
   if (max_samples < ctx->nleaf)
     return fail(ctx, SRMG_ERR_BADARG, "srmg_cnn_pack_dev: room for %d samples, the tree has %d", max_samples,
                 ctx->nleaf);
-  return cnn_pack_tree(ctx, phi, b, b_prev, nblk_alloc, s, op, k2, geom, bc, (__nv_bfloat16 *)x, scale, blk);
+  return cnn_pack_tree(ctx, f, g, nblk_alloc, s, op, k2, geom, bc, (__nv_bfloat16 *)x, scale, blk);
 }
 
-extern "C" int srmg_cnn_predict_dev(srmg_ctx *ctx, srmg_cnn *net, double *u, const double *b, const double *b_prev,
-                                    int64_t nblk_alloc, double s, int op, double k2, int geom, const int8_t bc[9],
-                                    int *used) {
+extern "C" int srmg_cnn_predict_dev(srmg_ctx *ctx, srmg_cnn *net, double *u, const double *b, const double *b1,
+                                    const double *phi2, const double *b2, int64_t nblk_alloc, double s, int op,
+                                    double k2, int geom, const int8_t bc[9], int *which, double *resid) {
   RC(check_call(ctx, nblk_alloc, op, geom, bc));
-  if (!net || !u || !b || !b_prev) return fail(ctx, SRMG_ERR_BADARG, "srmg_cnn_predict_dev: null argument");
+  if (!net || !u || !b || !b1 || !phi2 || !b2) return fail(ctx, SRMG_ERR_BADARG, "srmg_cnn_predict_dev: null argument");
   if (net->device != ctx->device) return fail(ctx, SRMG_ERR_BADARG, "network and context on different devices");
   const int n = ctx->nleaf;
-  const size_t xb = (size_t)n * kNP * 2, yb = (size_t)n * 256 * 4, sb = (size_t)n * 8, bb = (size_t)n * 4;
+  const int64_t nval = nblk_alloc * (int64_t)kNP;
+  // work: f = u - phi2 (previous correction), g = b - 2 b1 + b2, the extrapolated and the
+  // learned guesses
+  RC(ensure(ctx, ctx->cnn_work[1], 4 * nval * sizeof(double)));
+  double *f = (double *)ctx->cnn_work[1].p, *g = f + nval, *ext = g + nval, *lrn = ext + nval;
+  // x: [n][400][2] bf16; y: [n][256] float; scale: [n] double; blk: [n] int
+  const size_t xb = (size_t)n * kNP * 2 * sizeof(__nv_bfloat16), yb = (size_t)n * 256 * sizeof(float),
+               sb = (size_t)n * sizeof(double), bb = (size_t)n * sizeof(int);
   RC(ensure(ctx, ctx->cnn_work[2], xb + yb + sb + bb + 64));
   char *w = (char *)ctx->cnn_work[2].p;
   __nv_bfloat16 *x = (__nv_bfloat16 *)w;
   float *y = (float *)(w + ((xb + 15) & ~size_t(15)));
   double *scale = (double *)((char *)y + ((yb + 15) & ~size_t(15)));
   int *blk = (int *)((char *)scale + ((sb + 15) & ~size_t(15)));
-  const int got = cnn_pack_tree(ctx, u, b, b_prev, nblk_alloc, s, op, k2, geom, bc, x, scale, blk);
+  RC(lin_field(ctx, f, u, 1.0, phi2, -1.0, nullptr, 0.0, nval));
+  RC(lin_field(ctx, g, b, 1.0, b1, -2.0, b2, 1.0, nval));
+  RC(lin_field(ctx, ext, u, 1.0, f, 1.0, nullptr, 0.0, nval));
+  const int got = cnn_pack_tree(ctx, f, g, nblk_alloc, s, op, k2, geom, bc, x, scale, blk);
   if (got < 0) return got;
-  // the network runs on the context's stream
   k_cnn_fwd<<<cnn_grid(net, n), kThreads, sizeof(FwdSmem), ctx->stream>>>(x, n, net->wpk, net->bias, y, nullptr);
   CK(cudaGetLastError());
-  const int64_t nval = nblk_alloc * (int64_t)kNP;
-  RC(ensure(ctx, ctx->cnn_work[1], nval * sizeof(double)));
-  double *ug = (double *)ctx->cnn_work[1].p;
-  CK(cudaMemcpyAsync(ug, u, nval * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-  k_cnn_scatter<<<std::min<int64_t>(4096, ((int64_t)n * 256 + 255) / 256), 256, 0, ctx->stream>>>(
-      ug, u, y, scale, ctx->d_leaf, n);
-  // composite-grid function of the new leaves, ghosts filled
+  CK(cudaMemcpyAsync(lrn, ext, nval * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  k_cnn_scatter<<<(int)std::min<int64_t>(4096, ((int64_t)n * 256 + 255) / 256), 256, 0, ctx->stream>>>(
+      lrn, ext, y, scale, ctx->d_leaf, n);
+  // composite-grid functions of their leaves, ghosts filled
   const Signs sg = make_signs(bc);
-  for (int l = ctx->nlev; l >= 2; l--) RC(L_restrict<double>(ctx, ug, l));
-  for (int l = 1; l <= ctx->nlev; l++) RC(L_fill_ghost<double>(ctx, ug, l, sg, 7));
-  // keep the guess only if its residual is below that of the previous potential
+  for (double *v : {ext, lrn}) {
+    for (int l = ctx->nlev; l >= 2; l--) RC(L_restrict<double>(ctx, v, l));
+    for (int l = 1; l <= ctx->nlev; l++) RC(L_fill_ghost<double>(ctx, v, l, sg, 7));
+  }
+  // keep the guess with the smallest residual: previous potential, extrapolation, learned
   RC(leafnorm_dev<double>(ctx, u, b, s, op, k2, geom, 0, 0));
-  RC(leafnorm_dev<double>(ctx, ug, b, s, op, k2, geom, 0, 1));
-  RC(read_small(ctx, 2));
-  const bool better = ctx->h_small[1] < ctx->h_small[0];
-  if (better) CK(cudaMemcpyAsync(u, ug, nval * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-  if (used) *used = better ? 1 : 0;
+  RC(leafnorm_dev<double>(ctx, ext, b, s, op, k2, geom, 0, 1));
+  RC(leafnorm_dev<double>(ctx, lrn, b, s, op, k2, geom, 0, 2));
+  RC(read_small(ctx, 3));
+  const double r0 = ctx->h_small[0], r1 = ctx->h_small[1], r2 = ctx->h_small[2];
+  int pick = 0;
+  if (r1 < r0) pick = 1;
+  if (r2 < (pick ? r1 : r0)) pick = 2;
+  if (pick) CK(cudaMemcpyAsync(u, pick == 1 ? ext : lrn, nval * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  if (which) *which = pick;
+  if (resid) {
+    resid[0] = r0;
+    resid[1] = r1;
+    resid[2] = r2;
+  }
   CK(cudaGetLastError());
   return SRMG_OK;
 }

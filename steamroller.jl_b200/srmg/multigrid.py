@@ -119,11 +119,15 @@ SIGNATURES = {
     "srmg_cnn_set_params": (_I, [_P, _P, _I]),
     "srmg_cnn_synchronize": (_I, [_P]),
     "srmg_cnn_forward": (_I, [_P, _P, _P, _I]),
-    "srmg_cnn_gradients": (_I, [_P, _P, _P, _I, _P, ctypes.POINTER(_D)]),
-    "srmg_cnn_train_step": (_I, [_P, _P, _P, _I, ctypes.c_float, ctypes.POINTER(_D)]),
+    "srmg_cnn_gradients": (_I, [_P, _P, _P, _P, ctypes.c_float, _I, _I, _P, ctypes.POINTER(_D)]),
+    "srmg_cnn_train_step": (_I, [_P, _P, _P, _P, ctypes.c_float, _I, _I, ctypes.c_float, ctypes.POINTER(_D)]),
+    "srmg_cnn_forward_train": (_I, [_P, _P, _I, _P]),
+    "srmg_cnn_backward_step": (_I, [_P, _P, _I, ctypes.c_float, _P]),
     "srmg_cnn_leaf_blocks": (_I, [_P]),
-    "srmg_cnn_pack_dev": (_I, [_P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, _P, _P, _P, _I]),
-    "srmg_cnn_predict_dev": (_I, [_P, _P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, ctypes.POINTER(_I)]),
+    "srmg_cnn_pack_dev": (_I, [_P, _P, _P, _I64, _D, _I, _D, _I, _P, _P, _P, _P, _I]),
+    "srmg_cnn_predict_dev": (_I, [_P, _P, _P, _P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, ctypes.POINTER(_I),
+                                  ctypes.POINTER(_D)]),
+    "srmg_streamer_step_dev": (_I, [_P, _P, _P, _P, _P, _I64] + [_D] * 9 + [_P, ctypes.POINTER(_D)]),
 }
 
 
@@ -451,51 +455,82 @@ class Cnn:
         self.synchronize()
         return y
 
-    def gradients(self, x, t):
+    def gradients(self, x, t, ir0=None, lam=0.0, geom=1):
         g = np.zeros(self.nparams, dtype=np.float32)
         loss = ctypes.c_double()
         import torch
         torch.cuda.synchronize()
-        self.check(lib().srmg_cnn_gradients(self._h, x.data_ptr(), t.data_ptr(), x.shape[0], g.ctypes.data,
-                                            ctypes.byref(loss)))
+        self.check(lib().srmg_cnn_gradients(self._h, x.data_ptr(), t.data_ptr(),
+                                            ir0.data_ptr() if ir0 is not None else None, float(lam), int(geom),
+                                            x.shape[0], g.ctypes.data, ctypes.byref(loss)))
         return loss.value, g
 
-    def train_step(self, x, t, lr):
+    def train_step(self, x, t, lr, ir0=None, lam=0.0, geom=1):
         """One Adam step; returns the loss of the batch before the step."""
         loss = ctypes.c_double()
-        self.check(lib().srmg_cnn_train_step(self._h, x.data_ptr(), t.data_ptr(), x.shape[0], float(lr),
-                                             ctypes.byref(loss)))
+        self.check(lib().srmg_cnn_train_step(self._h, x.data_ptr(), t.data_ptr(),
+                                             ir0.data_ptr() if ir0 is not None else None, float(lam), int(geom),
+                                             x.shape[0], float(lr), ctypes.byref(loss)))
         return loss.value
 
 
-def cnn_pack(ctx: Context, phi, b, b_prev, s, geometry, bc, lpldisc=None):
-    """Samples of a tree for the network: (x bf16 [n,400,2], scale float64 [n], blk int32 [n])."""
+def _cnn_forward_train(self, x):
+    """Forward keeping activations; returns y (torch float32 [n, 256])."""
+    import torch
+    y = torch.empty((x.shape[0], 256), dtype=torch.float32, device=x.device)
+    torch.cuda.synchronize()
+    self.check(lib().srmg_cnn_forward_train(self._h, x.data_ptr(), x.shape[0], y.data_ptr()))
+    return y
+
+
+def _cnn_backward_step(self, dy, lr, want_grad=False):
+    """Backward from dLoss/dy of the last forward_train; Adam step when lr > 0."""
+    import torch
+    g = np.zeros(self.nparams, dtype=np.float32) if want_grad else None
+    dy = dy.contiguous()
+    torch.cuda.synchronize()
+    self.check(lib().srmg_cnn_backward_step(self._h, dy.data_ptr(), dy.shape[0], float(lr),
+                                            g.ctypes.data if want_grad else None))
+    return g
+
+
+Cnn.forward_train = _cnn_forward_train
+Cnn.backward_step = _cnn_backward_step
+
+
+def cnn_pack(ctx: Context, f, g, s, geometry, bc, lpldisc=None):
+    """Samples of a tree for the network from input fields f and g:
+    (x bf16 [n,400,2], scale float64 [n], blk int32 [n])."""
     import torch
     op, k2 = _disc(lpldisc)
     bca = _bc(bc)
     n = lib().srmg_cnn_leaf_blocks(ctx.handle)
-    dev = phi.device
+    dev = f.device
     x = torch.empty((n, 400, 2), dtype=torch.bfloat16, device=dev)
     scale = torch.empty(n, dtype=torch.float64, device=dev)
     blk = torch.empty(n, dtype=torch.int32, device=dev)
-    _order_after_torch(ctx, phi, b, b_prev)
-    rc = lib().srmg_cnn_pack_dev(ctx.handle, phi.data_ptr(), b.data_ptr(), b_prev.data_ptr(), phi.shape[0], s, op,
-                                 k2, geometry, bca.ctypes.data, x.data_ptr(), scale.data_ptr(), blk.data_ptr(), n)
+    _order_after_torch(ctx, f, g)
+    rc = lib().srmg_cnn_pack_dev(ctx.handle, f.data_ptr(), g.data_ptr(), f.shape[0], s, op, k2, geometry,
+                                 bca.ctypes.data, x.data_ptr(), scale.data_ptr(), blk.data_ptr(), n)
     if rc < 0:
         ctx.check(rc)
     ctx.synchronize()
     return x, scale, blk
 
 
-def cnn_predict(ctx: Context, net: Cnn, u, b, b_prev, s, geometry, bc, lpldisc=None) -> bool:
-    """Warm start in place on u (phi_prev on entry); True if the learned guess was kept."""
+def cnn_predict(ctx: Context, net: Cnn, u, b, b1, phi2, b2, s, geometry, bc, lpldisc=None, resid=False):
+    """Warm start in place on u (phi_{n-1} on entry); returns which guess was kept:
+    0 the previous potential, 1 the extrapolation, 2 the learned guess (and, with
+    resid=True, the three candidates' residual norms)."""
     op, k2 = _disc(lpldisc)
     bca = _bc(bc)
-    used = ctypes.c_int()
-    _order_after_torch(ctx, u, b, b_prev)
-    ctx.check(lib().srmg_cnn_predict_dev(ctx.handle, net.handle, u.data_ptr(), b.data_ptr(), b_prev.data_ptr(),
-                                         u.shape[0], s, op, k2, geometry, bca.ctypes.data, ctypes.byref(used)))
-    return bool(used.value)
+    which = ctypes.c_int()
+    r3 = (_D * 3)()
+    _order_after_torch(ctx, u, b, b1, phi2, b2)
+    ctx.check(lib().srmg_cnn_predict_dev(ctx.handle, net.handle, u.data_ptr(), b.data_ptr(), b1.data_ptr(),
+                                         phi2.data_ptr(), b2.data_ptr(), u.shape[0], s, op, k2, geometry,
+                                         bca.ctypes.data, ctypes.byref(which), r3))
+    return (which.value, list(r3)) if resid else which.value
 
 
 def exported_symbols_from_header(header_path: str) -> list[str]:

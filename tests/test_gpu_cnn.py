@@ -53,6 +53,19 @@ def test_gradients_match_oracle(net):
         assert rel(g[b0:b1], go[b0:b1]) < 1e-2, (l, "b", rel(g[b0:b1], go[b0:b1]))
 
 
+def test_residual_loss_gradients_match_oracle(net):
+    import torch
+    theta = net.get_params().astype(np.float64)
+    x, t, xt, tt = batch(19, 4)
+    ir0 = np.arange(19, dtype=np.int32) * 16
+    ir0t = torch.from_numpy(ir0).cuda()
+    torch.cuda.synchronize()
+    loss, g = net.gradients(xt, tt, ir0t, lam=0.5, geom=1)
+    lo, go = co.gradients(x, t, theta, ir0=ir0, lam=0.5, geom=1)
+    assert abs(loss - lo) <= 2e-3 * abs(lo)
+    assert rel(g, go) < 1e-2, rel(g, go)
+
+
 def test_training_lowers_loss():
     n = mg.Cnn(0, seed=3)
     x, t, xt, tt = batch(64, 3)
@@ -75,25 +88,65 @@ def test_set_get_params_roundtrip(net):
 
 
 def test_tree_pack_and_guarded_predict(net):
-    """Samples of a tree match the oracle's definition; a guess that would raise the
-    residual (an untrained network) is rejected and u is left unchanged."""
+    """Samples of a tree match their definition; the guarded prediction never keeps a
+    guess whose residual is above the previous potential's."""
     import torch
     p = gen.config1()
     ctx = mg.Context(0).set_tree(p.tree, p.conn)
-    b = torch.from_numpy(p.b).cuda()
-    u = torch.zeros_like(b)
-    mg.solve(ctx, u, b, p.s, p.geom, p.bc, tol=1e-10, mode=mg.MODE_FP64)
-    b_prev = (b * 0.97).contiguous()
-    x, scale, blk = mg.cnn_pack(ctx, u, b, b_prev, p.s, p.geom, p.bc)
+    b2 = torch.from_numpy(p.b).cuda()
+    b1 = (b2 * 1.01).contiguous()
+    b = (b2 * 1.02).contiguous()  # a linear change: g = 0
+    phi2 = torch.zeros_like(b2)
+    phi1 = torch.zeros_like(b2)
+    mg.solve(ctx, phi2, b2, p.s, p.geom, p.bc, tol=1e-10, mode=mg.MODE_FP64)
+    mg.solve(ctx, phi1, b1, p.s, p.geom, p.bc, tol=1e-10, mode=mg.MODE_FP64)
+    f = (phi1 - phi2).contiguous()
+    g = (b - 2 * b1 + b2).contiguous()
+    x, scale, blk = mg.cnn_pack(ctx, f, g, p.s, p.geom, p.bc)
     assert x.shape[0] == 256  # the level-5 leaves of the uniform tree
-    # oracle definition of the samples: (phi * a, db * c) over the 20x20 tile
-    uh, bh, bph = u.cpu().numpy(), p.b, b_prev.cpu().numpy()
+    fh = f.cpu().numpy()
     k = 17
     bk = int(blk[k])
     xs = x[k].float().cpu().numpy().reshape(20, 20, 2)
-    ratio = xs[8:12, 8:12, 0] / uh[bk, 8:12, 8:12]
+    ratio = xs[8:12, 8:12, 0] / fh[bk, 8:12, 8:12]
     assert np.allclose(ratio, ratio.flat[0], rtol=1e-2)
-    u0 = u.clone()
-    used = mg.cnn_predict(ctx, mg.Cnn(0, seed=11), u, b, b_prev, p.s, p.geom, p.bc)
-    if not used:
-        assert torch.equal(u, u0)
+    u = phi1.clone()
+    rn = lambda v: mg.resnorm(ctx, None, b, v, p.s, p.geom, p.bc)
+    r_prev = rn(phi1)
+    which = mg.cnn_predict(ctx, mg.Cnn(0, seed=11), u, b, b1, phi2, b2, p.s, p.geom, p.bc)
+    assert which in (0, 1, 2)
+    assert rn(u) <= r_prev
+    # a linear change of b: the extrapolation is exact up to the solve tolerance
+    assert which in (1, 2) and rn(u) < 1e-3 * r_prev
+
+
+def test_predict_matches_separate_path(net):
+    """The library's guarded prediction forms the learned candidate exactly as the
+    separate pack -> forward -> scatter path does (residual norms agree)."""
+    import torch
+    p = gen.config1()
+    ctx = mg.Context(0).set_tree(p.tree, p.conn)
+    b2 = torch.from_numpy(p.b).cuda()
+    b1 = (b2 * 1.01).contiguous()
+    b = (b2 * 1.025).contiguous()
+    phi2, phi1 = torch.zeros_like(b2), torch.zeros_like(b2)
+    mg.solve(ctx, phi2, b2, p.s, p.geom, p.bc, tol=1e-10, mode=mg.MODE_FP64)
+    mg.solve(ctx, phi1, b1, p.s, p.geom, p.bc, tol=1e-10, mode=mg.MODE_FP64)
+    u = phi1.clone()
+    which, r3 = mg.cnn_predict(ctx, net, u, b, b1, phi2, b2, p.s, p.geom, p.bc, resid=True)
+    assert all(np.isfinite(r3))
+    f = (phi1 - phi2).contiguous()
+    g = (b - 2 * b1 + b2).contiguous()
+    x, scale, blk = mg.cnn_pack(ctx, f, g, p.s, p.geom, p.bc)
+    y = net.forward(x)
+    lrn = (phi1 + f).contiguous()
+    lrn[blk.long(), 2:18, 2:18] += (y.double() * scale[:, None]).reshape(-1, 16, 16)
+    torch.cuda.synchronize()
+    for l in range(len(p.tree), 1, -1):
+        ctx.check(mg.lib().srmg_restrict_level_dev(ctx.handle, lrn.data_ptr(), p.nblk, l))
+    for l in range(1, len(p.tree) + 1):
+        mg.fill_ghost_(ctx, lrn, l, p.bc)
+    ctx.synchronize()
+    r_sep = mg.resnorm(ctx, None, b, lrn, p.s, p.geom, p.bc)
+    assert abs(r_sep - r3[2]) <= 1e-9 * r3[2]
+    assert mg.resnorm(ctx, None, b, u, p.s, p.geom, p.bc) == min(r3)
