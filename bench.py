@@ -181,6 +181,8 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched config-3 section")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start (config-4) section")
+    ap.add_argument("--learned-pairs", type=int, default=20000, help="solve pairs generated for training")
     ap.add_argument("--only", default=None, choices=[None, "vcycle", "smooth"],
                     help="vcycle: time plain FP64 V-cycles only; smooth: GS iterations on the finest "
                          "level only (profiling runs)")
@@ -314,6 +316,8 @@ def main():
         "fp64_leaf": nleaf * fp64_st["cycles"] * fp64_value, "note": "cells x V-cycles per second"}
     if not args.no_batch:
         line["batch"] = run_batch(local, stream, min(args.steps, 3), rank, world, pg, dev)
+    if not args.no_learned:
+        line["learned"] = run_learned(local, args.learned_pairs)
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = run_cpu_reference(problem, fp64_st["cycles"])
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -395,6 +399,44 @@ def run_batch(local, stream, steps, rank=0, world=1, pg=None, dev=None):
     batch.close()
     for c in ctxs:
         c.close()
+    return out
+
+
+def run_learned(local, npairs):
+    """Config 4: the learned warm start.  Solve pairs from seeded streamer runs on
+    config-1-sized trees (1.5 MV/m applied field), generated by the library's own solver;
+    the BF16 network trained by the library's kernels; then on held-out runs every 20th
+    step is solved to 1e-8 from a zero guess, the previous-step potential, the time
+    extrapolation, and the learned guess (mixed precision), plus the plain FP64 solve
+    from the previous-step potential.  Times include the prediction."""
+    import torch
+    from srmg import learn, multigrid as mg
+    runs = max(1, npairs // 2500)
+    t0 = time.time()
+    pairs = learn.generate(runs=runs, steps=(npairs + runs - 1) // runs + 2, seed=1, device=local)
+    t_gen = time.time() - t0
+    net = mg.Cnn(local, seed=5)
+    t0 = time.time()
+    losses = learn.train(net, pairs, steps=3000, batch=4, lr=1e-3, mu=0.001)
+    torch.cuda.synchronize()
+    t_train = time.time() - t0
+    ev = learn.evaluate(net, runs=2, steps=1500, every=20, seed=77, device=local)
+    ev_fp64 = learn.evaluate(net, runs=1, steps=600, every=20, seed=78, device=local, mode=mg.MODE_FP64)
+    out = {"workload": "config4: streamer runs on the uniform level-5 tree (256 x 256 cells), 1.5 MV/m, "
+                       "Poisson solves to 1e-8 along held-out runs",
+           "pairs": int(pairs.n), "generate_s": t_gen, "train_steps": 3000, "train_s": t_train,
+           "loss_first": losses[0], "loss_last": float(np.mean(losses[-100:])),
+           "mixed": ev, "fp64": {k: ev_fp64[k] for k in ("zero", "prev", "extrapolated", "learned")}}
+    fp64_prev_ms = ev_fp64["prev"]["mean_ms"]
+    out["solves_per_s"] = {"mixed_learned": 1e3 / ev["learned"]["mean_ms"],
+                           "mixed_prev": 1e3 / ev["prev"]["mean_ms"],
+                           "fp64_prev": 1e3 / fp64_prev_ms,
+                           "fp64_zero": 1e3 / ev_fp64["zero"]["mean_ms"]}
+    out["speedup_mixed_learned_vs_fp64_prev"] = fp64_prev_ms / ev["learned"]["mean_ms"]
+    out["speedup_mixed_learned_vs_fp64_zero"] = ev_fp64["zero"]["mean_ms"] / ev["learned"]["mean_ms"]
+    net.close()
+    del pairs
+    torch.cuda.empty_cache()
     return out
 
 
