@@ -41,6 +41,9 @@ TOL = 1e-8
 SEED = 2
 TARGET_LEAF = 1_500_000
 METRIC = "field solves/sec at 1e-8 rel residual (mixed-precision multigrid; plain FP64 GPU alongside)"
+# DRAM bytes of one plain FP64 V-cycle launch on the config-2 tree, from an ncu capture
+# (54.45 MB read + 48.00 MB written)
+TRAFFIC_VCYCLE_CONFIG2 = 102.45e6
 
 
 def peaks():
@@ -306,7 +309,10 @@ def main():
                       "rel_residual": mixed_st["rel_residual"]},
             "speedup_vs_fp64": value / fp64_value,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None, "peak_source": src,
+                         "frac": achieved / hbm, "traffic": TRAFFIC_VCYCLE_CONFIG2 if nleaf == 1503232 else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one V-cycle launch "
+                                           "on this tree (most of the working set stays in L2)",
+                         "peak_source": src,
                          "kernel": "plain FP64 V-cycle (whole cycle)", "bytes_per_launch": bytes_vc,
                          "ms_per_vcycle": vc_ms},
             "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}
