@@ -337,6 +337,8 @@ int srmg_cnn_pack_dev(srmg_ctx *ctx, const double *f, const double *g, int64_t n
  * the smallest residual norm and *which says which (0, 1, 2); resid (host, optional)
  * receives the three residual norms.  The solve then iterates to its tolerance from u
  * as usual. */
+/* Blocks the network ran on in the last prediction whose `which` was read back. */
+int srmg_cnn_last_active(const srmg_ctx *ctx);
 int srmg_cnn_predict_dev(srmg_ctx *ctx, srmg_cnn *net, double *u, const double *b,
                          const double *b1, const double *phi2, const double *b2,
                          int64_t nblk_alloc, double s, int op, double k2, int geom,
@@ -363,7 +365,11 @@ int srmg_streamer_step_dev(srmg_ctx *ctx, double *ne, double *npos, double *nneg
  *   "engine_ctas"      CTAs of the persistent kernel (0 = one per SM);
  *   "trace"            1 = record a %globaltimer stamp (ns) after every phase of the
  *                      persistent kernel, read back with srmg_get_trace;
- *   "graph"            1 = batched solves replay a captured CUDA graph. */
+ *   "graph"            1 = batched solves replay a captured CUDA graph;
+ *   "cnn_active_ppm"   the learned warm start runs the network only on blocks whose
+ *                      share of (b_n - 2 b_{n-1} + b_{n-2})^2 is at least this many
+ *                      millionths of the largest block's (default 0 = every
+ *                      leaf-holding block); the others keep the extrapolation. */
 int srmg_set_option(srmg_ctx *ctx, const char *key, int64_t value);
 
 /* Phase timestamps of the last persistent-kernel launch (with option "trace" on);

@@ -786,6 +786,10 @@ extern "C" int srmg_set_option(srmg_ctx *ctx, const char *key, int64_t value) {
   if (!strcmp(key, "engine")) ctx->use_engine = value != 0;
   else if (!strcmp(key, "trace")) ctx->trace_on = value != 0;
   else if (!strcmp(key, "graph")) ctx->use_graph = value != 0;
+  else if (!strcmp(key, "cnn_active_ppm")) {
+    if (value < 0 || value > 1000000) return fail(ctx, SRMG_ERR_BADARG, "cnn_active_ppm out of range");
+    ctx->cnn_active_ppm = (int)value;
+  }
   else if (!strcmp(key, "local_max_blocks")) {
     if (value < 0 || value > 1024) return fail(ctx, SRMG_ERR_BADARG, "local_max_blocks out of range");
     ctx->local_max_blocks = (int)value;

@@ -202,9 +202,11 @@ __device__ void load_tile(__nv_bfloat16 *t, const __nv_bfloat16 *g) {
 // bf16, the input of every layer.
 __global__ void __launch_bounds__(kThreads, 1)
 k_cnn_fwd(const __nv_bfloat16 *__restrict__ x, int n, const __nv_bfloat16 *__restrict__ wpk,
-          const float *__restrict__ bias, float *__restrict__ y, __nv_bfloat16 *__restrict__ acts) {
+          const float *__restrict__ bias, float *__restrict__ y, __nv_bfloat16 *__restrict__ acts,
+          const int *__restrict__ n_dev = nullptr) {
   extern __shared__ __align__(128) unsigned char smraw[];
   FwdSmem &S = *reinterpret_cast<FwdSmem *>(smraw);
+  if (n_dev) n = min(n, *n_dev);  // sample count decided on the device
   {
     const uint4 *src = reinterpret_cast<const uint4 *>(wpk);
     uint4 *dst = reinterpret_cast<uint4 *>(S.w);
@@ -531,12 +533,18 @@ __global__ void k_cnn_adam(float *__restrict__ p, const float *__restrict__ g, f
 // tile of (f * a, g * bsc), pixel order y * 20 + x, and the output scale
 // s_level * |g| of the block.
 __global__ void k_cnn_gather(const double *__restrict__ phi, const double *__restrict__ db, const int2 *__restrict__ leaf,
-                             int nleaf, double a, double bsc, double s, double dbrms, __nv_bfloat16 *__restrict__ x,
-                             double *__restrict__ scale, int *__restrict__ blk) {
-  const int64_t total = (int64_t)nleaf * kNP;
+                             int nleaf, const double *__restrict__ norms, double s, __nv_bfloat16 *__restrict__ x,
+                             double *__restrict__ scale, int *__restrict__ blk, const int *__restrict__ list = nullptr,
+                             const int *__restrict__ count = nullptr) {
+  // norms[0] = |phi|, norms[1] = |db| (leaf norms); 0 counts as 1.  With a list, sample
+  // k is leaf block list[k], k < *count.
+  const double a = norms[0] > 0 ? 1.0 / norms[0] : 1.0, bsc = norms[1] > 0 ? 1.0 / norms[1] : 1.0;
+  const double dbrms = norms[1] > 0 ? norms[1] : 1.0;
+  const int n = count ? min(nleaf, *count) : nleaf;
+  const int64_t total = (int64_t)n * kNP;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
     const int k = (int)(i / kNP), p = (int)(i % kNP);
-    const int2 lb = leaf[k];
+    const int2 lb = leaf[list ? list[k] : k];
     const int64_t o = (int64_t)lb.x * kNP + p;
     reinterpret_cast<__nv_bfloat162 *>(x)[i] =
         __floats2bfloat162_rn((float)(phi[o] * a), (float)(db[o] * bsc));
@@ -550,11 +558,13 @@ __global__ void k_cnn_gather(const double *__restrict__ phi, const double *__res
 
 // Guess on the valid cells of every leaf-holding block: u = phi + y * scale.
 __global__ void k_cnn_scatter(double *__restrict__ u, const double *__restrict__ phi, const float *__restrict__ y,
-                              const double *__restrict__ scale, const int2 *__restrict__ leaf, int nleaf) {
-  const int64_t total = (int64_t)nleaf * 256;
+                              const double *__restrict__ scale, const int2 *__restrict__ leaf, int nleaf,
+                              const int *__restrict__ list = nullptr, const int *__restrict__ count = nullptr) {
+  const int n = count ? min(nleaf, *count) : nleaf;
+  const int64_t total = (int64_t)n * 256;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
     const int k = (int)(i >> 8), c = (int)(i & 255);
-    const int64_t o = (int64_t)leaf[k].x * kNP + (2 + (c >> 4)) * kT + 2 + (c & 15);
+    const int64_t o = (int64_t)leaf[list ? list[k] : k].x * kNP + (2 + (c >> 4)) * kT + 2 + (c & 15);
     u[o] = phi[o] + (double)y[i] * scale[k];
   }
 }
@@ -569,6 +579,136 @@ __global__ void k_lin_field(double *__restrict__ d, const double *__restrict__ a
     if (c) v += cc * c[i];
     d[i] = v;
   }
+}
+
+// Leaf-cell sums of squares of up to three fields over the leaf-holding blocks, one
+// 256-thread block per tree block: part[k * 3 + j] = 4^-(l-1) sum over the block's leaf
+// cells of f_j^2.  With `resid`, f_j is the residual -(b + L v_j / s_l) of candidate
+// v_j instead of v_j itself.
+__global__ void __launch_bounds__(256) k_leaf_sq3(const double *__restrict__ v0, const double *__restrict__ v1,
+                                                  const double *__restrict__ v2, int nf, const double *__restrict__ b,
+                                                  bool resid, double s, int op, double k2, int geom,
+                                                  WTab<double> wt, const int2 *__restrict__ leaf,
+                                                  const int4 *__restrict__ info, int nleaf,
+                                                  double *__restrict__ part) {
+  __shared__ double red[3][8];
+  const int t = threadIdx.x;
+  const int x = 2 + (t & 15), y = 2 + (t >> 4), o = x + kS * y;
+  const int sub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
+  for (int k = blockIdx.x; k < nleaf; k += gridDim.x) {
+    const int2 lb = leaf[k];
+    const int4 bi = info[lb.x];
+    const bool is_leaf = !(((bi.z & 15) >> sub) & 1);
+    const double f = (double)((int64_t)1 << (lb.y - 1));
+    const double sl = s / (f * f), wl = 1.0 / (f * f);
+    const double centre = op == 1 ? -4.0 - sl * k2 : -4.0;
+    const int64_t base = (int64_t)lb.x * kSS;
+    const W5<double> w = weights<double>(wt, geom, bi.x, bi.y, x, y);
+    double sq[3] = {0.0, 0.0, 0.0};
+    const double *vs[3] = {v0, v1, v2};
+    for (int j = 0; j < nf; ++j) {
+      double val = vs[j][base + o];
+      if (resid) val = -(b[base + o] + apply5<double>(vs[j] + base, x, y, w, centre) / sl);
+      sq[j] = is_leaf ? val * val : 0.0;
+    }
+    for (int j = 0; j < 3; ++j) {
+      double v = sq[j];
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      if ((t & 31) == 0) red[j][t >> 5] = v;
+    }
+    __syncthreads();
+    if (t < 3) {
+      double c = 0.0;
+      for (int q = 0; q < 8; ++q) c += red[t][q];
+      part[(int64_t)k * 3 + t] = c * wl;
+    }
+    __syncthreads();
+  }
+}
+
+// Fixed-order sums of the per-block partials: out[j] = sqrt(sum_k part[k * 3 + j]).
+__global__ void __launch_bounds__(1024) k_leaf_sq3_reduce(const double *__restrict__ part, int nleaf, int nf,
+                                                         double *__restrict__ out) {
+  __shared__ double red[3][32];
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int k = threadIdx.x; k < nleaf; k += blockDim.x)
+    for (int j = 0; j < nf; ++j) v[j] += part[(int64_t)k * 3 + j];
+  for (int j = 0; j < 3; ++j) {
+    double a = v[j];
+    for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+    if ((threadIdx.x & 31) == 0) red[j][threadIdx.x >> 5] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x < (unsigned)nf) {
+    double c = 0.0;
+    for (int q = 0; q < 32; ++q) c += red[threadIdx.x][q];
+    out[threadIdx.x] = sqrt(c);
+  }
+}
+
+// Active blocks: the leaf-holding blocks whose g energy (part[k * 3 + 1]) is at least
+// theta times the largest, listed in leaf order (one CTA, fixed order).
+__global__ void __launch_bounds__(1024) k_select_active(const double *__restrict__ part, int nleaf, double theta,
+                                                       int *__restrict__ list, int *__restrict__ count) {
+  __shared__ double smax[32];
+  __shared__ int scnt[1024];
+  double m = 0.0;
+  for (int k = threadIdx.x; k < nleaf; k += blockDim.x) m = fmax(m, part[(int64_t)k * 3 + 1]);
+  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mm = 0.0;
+    for (int q = 0; q < 32; ++q) mm = fmax(mm, smax[q]);
+    smax[0] = mm;
+  }
+  __syncthreads();
+  const double thr = theta * smax[0];
+  const int chunk = (nleaf + blockDim.x - 1) / blockDim.x;
+  const int k0 = threadIdx.x * chunk, k1 = min(nleaf, k0 + chunk);
+  int c = 0;
+  for (int k = k0; k < k1; ++k) c += part[(int64_t)k * 3 + 1] >= thr && part[(int64_t)k * 3 + 1] > 0.0;
+  scnt[threadIdx.x] = c;
+  __syncthreads();
+  for (int off = 1; off < (int)blockDim.x; off <<= 1) {  // inclusive scan
+    const int v = threadIdx.x >= (unsigned)off ? scnt[threadIdx.x - off] : 0;
+    __syncthreads();
+    scnt[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int w = scnt[threadIdx.x] - c;
+  for (int k = k0; k < k1; ++k)
+    if (part[(int64_t)k * 3 + 1] >= thr && part[(int64_t)k * 3 + 1] > 0.0) list[w++] = k;
+  if (threadIdx.x == blockDim.x - 1) *count = scnt[threadIdx.x];
+}
+
+// f = u - phi2, g = b - 2 b1 + b2, ext = u + f, lrn = ext (every element).
+__global__ void k_predict_prep(const double *__restrict__ u, const double *__restrict__ phi2,
+                               const double *__restrict__ b, const double *__restrict__ b1,
+                               const double *__restrict__ b2, double *__restrict__ f, double *__restrict__ g,
+                               double *__restrict__ ext, double *__restrict__ lrn, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double ui = u[i], fi = ui - phi2[i];
+    f[i] = fi;
+    g[i] = b[i] - 2.0 * b1[i] + b2[i];
+    ext[i] = ui + fi;
+    lrn[i] = ui + fi;
+  }
+}
+
+// Keep the candidate with the smallest residual norm (ties: the earlier one):
+// r[0] previous potential (u itself), r[1] ext, r[2] lrn; copy it into u.
+__global__ void k_predict_select(double *__restrict__ u, const double *__restrict__ ext,
+                                 const double *__restrict__ lrn, const double *__restrict__ r, int *__restrict__ pick,
+                                 int64_t n) {
+  int p = 0;
+  if (r[1] < r[0]) p = 1;
+  if (r[2] < (p ? r[1] : r[0])) p = 2;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *pick = p;
+  if (p == 0) return;
+  const double *src = p == 1 ? ext : lrn;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    u[i] = src[i];
 }
 
 }  // namespace cnn
@@ -841,30 +981,41 @@ int lin_field(srmg_ctx *ctx, double *d, const double *a, double ca, const double
   return cuda_check(ctx, cudaGetLastError(), "k_lin_field");
 }
 
+// Leaf norms (sqrt of 4^-(l-1)-weighted sums over leaf cells) of up to three fields,
+// or of their residuals, into out[0..nf) on the device.
+int leaf_norms(srmg_ctx *ctx, const double *v0, const double *v1, const double *v2, int nf, const double *b,
+               bool resid, double s, int op, double k2, int geom, double *part, double *out) {
+  const int n = ctx->nleaf;
+  if (n == 0) return cuda_check(ctx, cudaMemsetAsync(out, 0, nf * sizeof(double), ctx->stream), "memset");
+  k_leaf_sq3<<<std::min(n, 148 * 8), 256, 0, ctx->stream>>>(v0, v1, v2, nf, b, resid, s, op, k2, geom,
+                                                           WTab<double>{ctx->d_wm64, ctx->d_wp64}, ctx->d_leaf,
+                                                           ctx->d_info, n, part);
+  k_leaf_sq3_reduce<<<1, 1024, 0, ctx->stream>>>(part, n, nf, out);
+  return cuda_check(ctx, cudaGetLastError(), "leaf norms");
+}
+
 // Samples of a tree from the input fields f (ghosts filled) and g (ghosts are filled
-// here, on a copy): x, the per-sample output scale and block ids.  Returns the count.
-int cnn_pack_tree(srmg_ctx *ctx, const double *f, const double *g, int64_t nblk_alloc, double s, int op, double k2,
-                  int geom, const int8_t *bc, __nv_bfloat16 *x, double *scale, int *blk) {
+// here, on the copy gw unless gw == g): x, the per-sample output scale and block ids,
+// with the input norms computed on the device (norms[0..1]).  No host synchronisation.
+int cnn_pack_tree(srmg_ctx *ctx, const double *f, const double *g, double *gw, int64_t nblk_alloc, double s,
+                  int op, double k2, int geom, const int8_t *bc, __nv_bfloat16 *x, double *scale, int *blk,
+                  double *part, double *norms, int *list = nullptr, int *count = nullptr, double theta = 0.0) {
   const int64_t nval = nblk_alloc * (int64_t)kNP;
-  RC(ensure(ctx, ctx->cnn_work[0], nval * sizeof(double)));
-  double *gw = (double *)ctx->cnn_work[0].p;
-  RC(lin_field(ctx, gw, g, 1.0, nullptr, 0.0, nullptr, 0.0, nval));
+  if (gw != g) RC(lin_field(ctx, gw, g, 1.0, nullptr, 0.0, nullptr, 0.0, nval));
   const Signs sg = make_signs(bc);
   for (int l = 1; l <= ctx->nlev; l++) RC(L_fill_ghost<double>(ctx, gw, l, sg, 7));
-  // leaf norms of f and g set the input scales (mode 1: the norm of the field)
-  RC(leafnorm_dev<double>(ctx, f, f, s, op, k2, geom, 1, 0));
-  RC(leafnorm_dev<double>(ctx, f, gw, s, op, k2, geom, 1, 1));
-  RC(read_small(ctx, 2));
-  const double nf = ctx->h_small[0], ng = ctx->h_small[1];
-  const double a = nf > 0 ? 1.0 / nf : 1.0, bsc = ng > 0 ? 1.0 / ng : 1.0;
+  RC(leaf_norms(ctx, f, gw, nullptr, 2, nullptr, false, s, op, k2, geom, part, norms));
   const int n = ctx->nleaf;
+  if (list) k_select_active<<<1, 1024, 0, ctx->stream>>>(part, n, theta, list, count);
   k_cnn_gather<<<(int)std::min<int64_t>(4096, ((int64_t)n * kNP + 255) / 256), 256, 0, ctx->stream>>>(
-      f, gw, ctx->d_leaf, n, a, bsc, s, ng > 0 ? ng : 1.0, x, scale, blk);
+      f, gw, ctx->d_leaf, n, norms, s, x, scale, blk, list, count);
   CK(cudaGetLastError());
   return n;
 }
 
 }  // namespace
+
+extern "C" int srmg_cnn_last_active(const srmg_ctx *ctx) { return ctx ? ctx->cnn_last_active : SRMG_ERR_BADARG; }
 
 extern "C" int srmg_cnn_leaf_blocks(const srmg_ctx *ctx) {
   if (!ctx) return SRMG_ERR_BADARG;
@@ -879,7 +1030,14 @@ extern "C" int srmg_cnn_pack_dev(srmg_ctx *ctx, const double *f, const double *g
   if (max_samples < ctx->nleaf)
     return fail(ctx, SRMG_ERR_BADARG, "srmg_cnn_pack_dev: room for %d samples, the tree has %d", max_samples,
                 ctx->nleaf);
-  return cnn_pack_tree(ctx, f, g, nblk_alloc, s, op, k2, geom, bc, (__nv_bfloat16 *)x, scale, blk);
+  const int64_t nval = nblk_alloc * (int64_t)kNP;
+  RC(ensure(ctx, ctx->cnn_work[0], nval * sizeof(double) + (3 * (size_t)ctx->nleaf + 8) * sizeof(double)));
+  double *gw = (double *)ctx->cnn_work[0].p, *part = gw + nval, *norms = part + 3 * (size_t)ctx->nleaf;
+  const int n = cnn_pack_tree(ctx, f, g, gw, nblk_alloc, s, op, k2, geom, bc, (__nv_bfloat16 *)x, scale, blk,
+                              part, norms);
+  if (n < 0) return n;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return n;
 }
 
 extern "C" int srmg_cnn_predict_dev(srmg_ctx *ctx, srmg_cnn *net, double *u, const double *b, const double *b1,
@@ -890,10 +1048,12 @@ extern "C" int srmg_cnn_predict_dev(srmg_ctx *ctx, srmg_cnn *net, double *u, con
   if (net->device != ctx->device) return fail(ctx, SRMG_ERR_BADARG, "network and context on different devices");
   const int n = ctx->nleaf;
   const int64_t nval = nblk_alloc * (int64_t)kNP;
-  // work: f = u - phi2 (previous correction), g = b - 2 b1 + b2, the extrapolated and the
-  // learned guesses
-  RC(ensure(ctx, ctx->cnn_work[1], 4 * nval * sizeof(double)));
+  // work: f = u - phi2 (previous correction), g = b - 2 b1 + b2 (ghosts filled in place),
+  // the extrapolated and the learned candidates, per-block partials and norms
+  RC(ensure(ctx, ctx->cnn_work[1], (4 * (size_t)nval + 3 * (size_t)n + 16) * sizeof(double) + (n + 8) * sizeof(int)));
   double *f = (double *)ctx->cnn_work[1].p, *g = f + nval, *ext = g + nval, *lrn = ext + nval;
+  double *part = lrn + nval, *norms = part + 3 * (size_t)n;  // norms[0..1] inputs, [2..4] residuals
+  int *pick = (int *)(norms + 8), *count = pick + 1, *list = pick + 2;
   // x: [n][400][2] bf16; y: [n][256] float; scale: [n] double; blk: [n] int
   const size_t xb = (size_t)n * kNP * 2 * sizeof(__nv_bfloat16), yb = (size_t)n * 256 * sizeof(float),
                sb = (size_t)n * sizeof(double), bb = (size_t)n * sizeof(int);
@@ -903,38 +1063,41 @@ extern "C" int srmg_cnn_predict_dev(srmg_ctx *ctx, srmg_cnn *net, double *u, con
   float *y = (float *)(w + ((xb + 15) & ~size_t(15)));
   double *scale = (double *)((char *)y + ((yb + 15) & ~size_t(15)));
   int *blk = (int *)((char *)scale + ((sb + 15) & ~size_t(15)));
-  RC(lin_field(ctx, f, u, 1.0, phi2, -1.0, nullptr, 0.0, nval));
-  RC(lin_field(ctx, g, b, 1.0, b1, -2.0, b2, 1.0, nval));
-  RC(lin_field(ctx, ext, u, 1.0, f, 1.0, nullptr, 0.0, nval));
-  const int got = cnn_pack_tree(ctx, f, g, nblk_alloc, s, op, k2, geom, bc, x, scale, blk);
-  if (got < 0) return got;
-  k_cnn_fwd<<<cnn_grid(net, n), kThreads, sizeof(FwdSmem), ctx->stream>>>(x, n, net->wpk, net->bias, y, nullptr);
+  const int grid = (int)std::min<int64_t>(4096, (nval + 255) / 256);
+  k_predict_prep<<<grid, 256, 0, ctx->stream>>>(u, phi2, b, b1, b2, f, g, ext, lrn, nval);
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(lrn, ext, nval * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  // the network runs on the active blocks (g energy >= theta * the largest); the others
+  // keep the extrapolation
+  const double theta = ctx->cnn_active_ppm * 1e-6;
+  const bool sel = ctx->cnn_active_ppm > 0;
+  const int got = cnn_pack_tree(ctx, f, g, g, nblk_alloc, s, op, k2, geom, bc, x, scale, blk, part, norms,
+                                sel ? list : nullptr, sel ? count : nullptr, theta);
+  if (got < 0) return got;
+  k_cnn_fwd<<<cnn_grid(net, n), kThreads, sizeof(FwdSmem), ctx->stream>>>(x, n, net->wpk, net->bias, y, nullptr,
+                                                                          sel ? count : nullptr);
+  CK(cudaGetLastError());
   k_cnn_scatter<<<(int)std::min<int64_t>(4096, ((int64_t)n * 256 + 255) / 256), 256, 0, ctx->stream>>>(
-      lrn, ext, y, scale, ctx->d_leaf, n);
+      lrn, ext, y, scale, ctx->d_leaf, n, sel ? list : nullptr, sel ? count : nullptr);
   // composite-grid functions of their leaves, ghosts filled
   const Signs sg = make_signs(bc);
   for (double *v : {ext, lrn}) {
     for (int l = ctx->nlev; l >= 2; l--) RC(L_restrict<double>(ctx, v, l));
     for (int l = 1; l <= ctx->nlev; l++) RC(L_fill_ghost<double>(ctx, v, l, sg, 7));
   }
-  // keep the guess with the smallest residual: previous potential, extrapolation, learned
-  RC(leafnorm_dev<double>(ctx, u, b, s, op, k2, geom, 0, 0));
-  RC(leafnorm_dev<double>(ctx, ext, b, s, op, k2, geom, 0, 1));
-  RC(leafnorm_dev<double>(ctx, lrn, b, s, op, k2, geom, 0, 2));
-  RC(read_small(ctx, 3));
-  const double r0 = ctx->h_small[0], r1 = ctx->h_small[1], r2 = ctx->h_small[2];
-  int pick = 0;
-  if (r1 < r0) pick = 1;
-  if (r2 < (pick ? r1 : r0)) pick = 2;
-  if (pick) CK(cudaMemcpyAsync(u, pick == 1 ? ext : lrn, nval * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-  if (which) *which = pick;
-  if (resid) {
-    resid[0] = r0;
-    resid[1] = r1;
-    resid[2] = r2;
-  }
+  // residual norms of the three candidates; keep the smallest (device-side)
+  RC(leaf_norms(ctx, u, ext, lrn, 3, b, true, s, op, k2, geom, part, norms + 2));
+  k_predict_select<<<grid, 256, 0, ctx->stream>>>(u, ext, lrn, norms + 2, pick, nval);
   CK(cudaGetLastError());
+  if (which || resid) {
+    double h[3];
+    int hp[2] = {0, n};
+    CK(cudaMemcpyAsync(h, norms + 2, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(hp, pick, (sel ? 2 : 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (which) *which = hp[0];
+    ctx->cnn_last_active = sel ? hp[1] : n;
+    if (resid)
+      for (int j = 0; j < 3; j++) resid[j] = h[j];
+  }
   return SRMG_OK;
 }

@@ -107,6 +107,8 @@ struct srmg_ctx {
   int2 *d_leaf = nullptr;               // blocks with a leaf cell: {0-based id, level}
   int nleaf = 0;
   srmg::DevBuf cnn_work[3];             // learned warm start: db, candidate guess, samples
+  int cnn_active_ppm = 0;               // > 0: network only on blocks with g energy >= ppm 1e-6 x max
+  int cnn_last_active = 0;              // active blocks of the last prediction (when read back)
   std::vector<int4> l1_blocks, l1_faces;  // level 1 as uploaded (direct coarsest solve)
   std::vector<srmg::ItemSpec> batch_items;       // operators given to srmg_batch_set
 

@@ -179,6 +179,7 @@ def evaluate(net: mg.Cnn, runs, steps, every=10, seed=99, device=0, mode=mg.MODE
             c, ms, ini = run(u)
             res["learned"] = (c, ms + t_pred, ini)
             res["which"] = which
+            res["active"] = mg.lib().srmg_cnn_last_active(s.ctx.handle) / mg.lib().srmg_cnn_leaf_blocks(s.ctx.handle)
             res["predict_ms"] = t_pred
             rows.append(res)
             s.phi.copy_(u)
@@ -197,6 +198,7 @@ def evaluate(net: mg.Cnn, runs, steps, every=10, seed=99, device=0, mode=mg.MODE
     out["kept"] = {"previous": float(np.mean(w == 0)), "extrapolated": float(np.mean(w == 1)),
                    "learned": float(np.mean(w == 2))}
     out["predict_ms"] = float(np.mean([r["predict_ms"] for r in rows]))
+    out["active_block_fraction"] = float(np.mean([r["active"] for r in rows]))
     out["solves"] = len(rows)
     out["cycles_saved_vs_prev"] = out["prev"]["mean_cycles"] - out["learned"]["mean_cycles"]
     out["cycles_saved_vs_zero"] = out["zero"]["mean_cycles"] - out["learned"]["mean_cycles"]

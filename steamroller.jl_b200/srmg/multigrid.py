@@ -124,6 +124,7 @@ SIGNATURES = {
     "srmg_cnn_forward_train": (_I, [_P, _P, _I, _P]),
     "srmg_cnn_backward_step": (_I, [_P, _P, _I, ctypes.c_float, _P]),
     "srmg_cnn_leaf_blocks": (_I, [_P]),
+    "srmg_cnn_last_active": (_I, [_P]),
     "srmg_cnn_pack_dev": (_I, [_P, _P, _P, _I64, _D, _I, _D, _I, _P, _P, _P, _P, _I]),
     "srmg_cnn_predict_dev": (_I, [_P, _P, _P, _P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, ctypes.POINTER(_I),
                                   ctypes.POINTER(_D)]),
