@@ -186,6 +186,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched config-3 section")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start (config-4) section")
     ap.add_argument("--learned-pairs", type=int, default=20000, help="solve pairs generated for training")
+    ap.add_argument("--no-config5", action="store_true", help="skip the full-size timestep (config-5) section")
+    ap.add_argument("--config5-steps", type=int, default=200)
     ap.add_argument("--only", default=None, choices=[None, "vcycle", "smooth"],
                     help="vcycle: time plain FP64 V-cycles only; smooth: GS iterations on the finest "
                          "level only (profiling runs)")
@@ -323,7 +325,10 @@ def main():
     if not args.no_batch:
         line["batch"] = run_batch(local, stream, min(args.steps, 3), rank, world, pg, dev)
     if not args.no_learned:
-        line["learned"] = run_learned(local, args.learned_pairs)
+        line["learned"], net = run_learned(local, args.learned_pairs)
+        if not args.no_config5:
+            line["config5"] = run_config5(local, net, args.config5_steps, cpu=(rank == 0 and not args.no_cpu))
+        net.close()
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = run_cpu_reference(problem, fp64_st["cycles"])
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -440,9 +445,35 @@ def run_learned(local, npairs):
                            "fp64_zero": 1e3 / ev_fp64["zero"]["mean_ms"]}
     out["speedup_mixed_learned_vs_fp64_prev"] = fp64_prev_ms / ev["learned"]["mean_ms"]
     out["speedup_mixed_learned_vs_fp64_zero"] = ev_fp64["zero"]["mean_ms"] / ev["learned"]["mean_ms"]
-    net.close()
     del pairs
     torch.cuda.empty_cache()
+    return out, net
+
+
+def run_config5(local, net, steps, cpu=True):
+    """Config 5: the full-size timestep field solve (Poisson + 3 Helmholtz per step,
+    learned warm start + mixed precision) on the 8-12M-leaf tree, beside the plain FP64
+    GPU solves of sampled steps and, on rank 0, the oracle's FP64 V-cycle time on the
+    host cores (a bounded sample of 2 V-cycles scaled by the FP64 cycle count)."""
+    from srmg import timestep
+    out, problem = timestep.run(net, steps=steps, device=local)
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc_mod
+        orc = orc_mod.Oracle(problem, threads=os.cpu_count())
+        u = np.zeros_like(problem.b)
+        b = problem.b.copy()
+        r, u1 = np.zeros_like(u), np.zeros_like(u)
+        orc.vcycle(u, b, r, u1, ndown=2, ntop=4, nup=2)
+        t0 = time.perf_counter()
+        for _ in range(2):
+            orc.vcycle(u, b, r, u1, ndown=2, ntop=4, nup=2)
+        spv = (time.perf_counter() - t0) / 2
+        cyc = out["fp64_gpu"]["poisson_cycles"]
+        out["cpu_baseline"] = {"value": 1.0 / (spv * cyc), "unit": "Poisson solves/s", "cores": os.cpu_count(),
+                               "kind": "port", "s_per_vcycle": spv,
+                               "sample": f"2 oracle FP64 V-cycles on this tree, scaled by the {cyc:.0f} cycles of "
+                                         "the FP64 Poisson solve from the previous potential"}
     return out
 
 

@@ -30,22 +30,47 @@ BC_DENSITY = np.ones(9, dtype=np.int8)  # zero-gradient ghosts for the densities
 
 class Streamer:
     def __init__(self, seed: int, device: int = 0, level: int = 5, E0: float = E_APPLIED,
-                 background: float = 1e13, cfl: float = 0.4):
+                 background: float = 1e13, cfl: float = 0.4, problem=None, stream=None):
+        """A seeded run on the uniform tree of `level`, or on `problem`'s tree: then the
+        densities start as a neutral conducting plasma where the problem's charge is
+        (n_e = background + 10 |b|, n+ = n_e + b, so the initial net charge is b)."""
         import torch
         self.rng = np.random.default_rng(seed)
-        self.tree = gen._uniform(level)
-        self.problem = gen.make_problem(self.tree, lambda r, z, l, gi, gj: np.zeros_like(r), gen.poisson_scale())
+        given = problem is not None
+        if not given:
+            self.tree = gen._uniform(level)
+            problem = gen.make_problem(self.tree, lambda r, z, l, gi, gj: np.zeros_like(r), gen.poisson_scale())
+        self.tree = problem.tree
+        self.problem = problem
         p = self.problem
         self.s, self.geom, self.bc = p.s, p.geom, p.bc
         self.h1 = p.h1
         self.E0 = E0
         self.cfl = cfl
         self.ctx = mg.Context(device).set_tree(p.tree, p.conn)
+        if stream is not None:
+            self.ctx.set_stream(stream.cuda_stream)
         self.nblk = p.nblk
         dev = torch.device("cuda", device)
         z = lambda: torch.zeros((self.nblk, 20, 20), dtype=torch.float64, device=dev)
         self.ne, self.npos, self.nneg, self.phi, self.b = z(), z(), z(), z(), z()
         self.work = torch.zeros(3 * self.nblk * 400 + 2, dtype=torch.float64, device=dev)
+        if given:
+            bh = p.b.copy()
+            leaf = np.zeros(bh.shape, dtype=bool)
+            for layer in self.tree:
+                for cc, blk in layer.index.items():
+                    if self.tree.isleaf(layer.level, cc):
+                        leaf[blk - 1, 2:18, 2:18] = True
+            ne = np.where(leaf, background + 10.0 * np.abs(bh), 0.0)
+            npos = np.where(leaf, ne + bh, 0.0)
+            self.ne.copy_(torch.from_numpy(ne))
+            self.npos.copy_(torch.from_numpy(npos))
+            self.t = 0.0
+            self._charge()
+            torch.cuda.synchronize()
+            mg.solve(self.ctx, self.phi, self.b, self.s, self.geom, self.bc, tol=1e-8, mode=mg.MODE_MIXED)
+            return
         # seed: an elongated neutral plasma column on the axis hanging from near the top
         # electrode (Gaussian radial profile and ends), length, radius, density and
         # position jittered
@@ -87,7 +112,8 @@ class Streamer:
         its previous value for the caller to solve.  Returns (phi_prev, b_prev)."""
         import torch
         torch.cuda.synchronize()
-        mg.fill_ghost_(self.ctx, self.ne, len(self.tree), BC_DENSITY)
+        for l in range(1, len(self.tree) + 1):
+            mg.fill_ghost_(self.ctx, self.ne, l, BC_DENSITY)
         dt = ctypes.c_double()
         self.ctx.check(mg.lib().srmg_streamer_step_dev(
             self.ctx.handle, self.ne.data_ptr(), self.npos.data_ptr(), self.nneg.data_ptr(), self.phi.data_ptr(),
