@@ -215,6 +215,7 @@ constexpr int kBuf = 3;
 template <typename T>
 struct SlotSmem {
   T tile[kBuf][kSS];
+  T red[256];   // restriction phase: the residual of the block being restricted
   int4 recs[32][5];
   uint64_t bar[kBuf];
   int sel[32];  // list positions of the chunk's blocks that take part
@@ -507,48 +508,91 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
 // 256-thread slot: the restricted u goes to the coarse block (and into the coarse
 // ghosts that copy it), the restricted r to e, where the coarse level's first GS
 // iteration reads it to form the FAS right-hand side.  uf: level l, uc: level l-1.
+// The fine blocks' tiles stream through the slot's triple-buffered bulk-copy pipeline
+// (as in the GS phase) and each block's b is loaded one block ahead, so the residual
+// reads shared memory.  Children of frozen items are skipped.
 template <typename T>
-__device__ void ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int first, int step, int t,
-                            int slot, T *buf) {
-  T *sr = buf, *su = buf + 256;
+__device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int first, int step, int t, int slot,
+                            SlotSmem<T> &S, unsigned &pk) {
   const int n = A.tr.nch[l - 1];
   const int4 *ch = A.tr.lvl_child[l - 1];
+  const int nmine = (first < n) ? (n - 1 - first) / step + 1 : 0;
+  if (nmine == 0) return true;
   const int x = 2 + (t & 15), y = 2 + (t >> 4);
-  for (int i = first; i < n; i += step) {
-    const int4 e = ch[i];
-    const int F = e.x, C = e.y;
-    const int4 fi = A.tr.info[F];
-    const int item = fi.z >> 8;
-    if (is_frozen(A, item)) continue;
-    const T *par = A.it_par + item * kParStride;
-    const T s = par[l], centre = par[32 + l];
-    const T *ufb = uf + (int64_t)F * kSS;
-    const int o = x + kS * y;
-    const W5<T> w = weights<T>(A.wt, A.geom, fi.x, fi.y, x, y);
-    const T Lu = apply5<T>(ufb, x, y, w, centre);
-    sr[t] = -(A.b[(int64_t)F * kSS + o] + Lu / s);
-    su[t] = ufb[o];
-    slot_sync(slot);
-    if (t < 64) {
-      const int kx = t & 7, ky = t >> 3;
-      const int cx = 2 + 8 * (e.z - 1) + kx, cy = 2 + 8 * (e.w - 1) + ky;
-      const int i00 = 2 * kx + 16 * 2 * ky;
-      T cu = dadd<T>(T(0), su[i00]);
-      cu = dadd<T>(cu, su[i00 + 1]);
-      cu = dadd<T>(cu, su[i00 + 16]);
-      cu = dadd<T>(cu, su[i00 + 17]);
-      cu = dmul<T>(cu, T(0.25));
-      T cr = dadd<T>(T(0), sr[i00]);
-      cr = dadd<T>(cr, sr[i00 + 1]);
-      cr = dadd<T>(cr, sr[i00 + 16]);
-      cr = dadd<T>(cr, sr[i00 + 17]);
-      cr = dmul<T>(cr, T(0.25));
-      uc[(int64_t)C * kSS + cx + kS * cy] = cu;
-      push<T>(A, item, uc, C, A.tr.faces + 4 * C, cx, cy, cu);
-      A.e[(int64_t)C * kSS + cx + kS * cy] = cr;
+  const int o = x + kS * y;
+  T *sr = S.red;
+  T b_nx = T(0);
+  auto prefetch = [&](int j) { b_nx = A.b[(int64_t)S.recs[j][0].x * kSS + o]; };
+  for (int c0 = 0; c0 < nmine; c0 += 32) {
+    // the chunk's next 32 child edges, without those of frozen items:
+    // recs[q][0] = {fine, coarse, sb_r, sb_z}, recs[q][1] = info of the fine block
+    if (t < 32) {
+      const int idx = c0 + t;
+      int gi = 0;
+      bool take = false;
+      if (idx < nmine) {
+        gi = first + idx * step;
+        take = A.nitems == 1 || !A.frozen[A.tr.info[ch[gi].x].z >> 8];
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, take);
+      if (take) S.sel[__popc(m & ((1u << t) - 1u))] = gi;
+      if (t == 0) S.cnt = __popc(m);
     }
     slot_sync(slot);
+    const int cn = S.cnt;
+    if (t < 2 * cn) {
+      const int q = t >> 1;
+      const int4 e = ch[S.sel[q]];
+      S.recs[q][t & 1] = (t & 1) ? A.tr.info[e.x] : e;
+    }
+    slot_sync(slot);
+    if (cn == 0) continue;
+    if (t == 0) {
+      issue_tile<T>(S, pk % kBuf, uf, S.recs[0][0].x);
+      if (cn > 1) issue_tile<T>(S, (pk + 1) % kBuf, uf, S.recs[1][0].x);
+    }
+    prefetch(0);
+    for (int j = 0; j < cn; ++j) {
+      const unsigned kb = pk + j;
+      const int buf = kb % kBuf;
+      const int4 e = S.recs[j][0], fi = S.recs[j][1];
+      const int C = e.y;
+      if (t == 0 && j + 2 < cn) issue_tile<T>(S, (kb + 2) % kBuf, uf, S.recs[j + 2][0].x);
+      const T bx = b_nx;
+      if (j + 1 < cn) prefetch(j + 1);
+      if (!mbar_wait(&S.bar[buf], (kb / kBuf) & 1, A.err, A.timeout_ns)) {
+        for (int q = 1; q <= 2 && j + q < cn; ++q)
+          mbar_wait(&S.bar[(kb + q) % kBuf], ((kb + q) / kBuf) & 1, A.err, A.timeout_ns);
+        return false;
+      }
+      const T *tile = S.tile[buf];
+      const int item = fi.z >> 8;
+      const T *par = A.it_par + item * kParStride;
+      const T s = par[l], centre = par[32 + l];
+      const W5<T> w = weights<T>(A.wt, A.geom, fi.x, fi.y, x, y);
+      const T Lu = apply5<T>(tile, x, y, w, centre);
+      sr[t] = -(bx + Lu / s);
+      slot_sync(slot);
+      if (t < 64) {
+        const int kx = t & 7, ky = t >> 3;
+        const int cx = 2 + 8 * (e.z - 1) + kx, cy = 2 + 8 * (e.w - 1) + ky;
+        // 2x2 sums in the reference's order: (i, j), (i+1, j), (i, j+1), (i+1, j+1)
+        const T cu = restrict4<T>(tile, 2 + 2 * kx, 2 + 2 * ky);
+        const int i00 = 2 * kx + 16 * 2 * ky;
+        T cr = dadd<T>(T(0), sr[i00]);
+        cr = dadd<T>(cr, sr[i00 + 1]);
+        cr = dadd<T>(cr, sr[i00 + 16]);
+        cr = dadd<T>(cr, sr[i00 + 17]);
+        cr = dmul<T>(cr, T(0.25));
+        uc[(int64_t)C * kSS + cx + kS * cy] = cu;
+        push<T>(A, item, uc, C, A.tr.faces + 4 * C, cx, cy, cu);
+        A.e[(int64_t)C * kSS + cx + kS * cy] = cr;
+      }
+      slot_sync(slot);  // sr and the tile buffer are reused
+    }
+    pk += cn;
   }
+  return true;
 }
 
 // u_fine += P(e_coarse) on every valid cell (in place in uf), pushes of the new edge
@@ -864,7 +908,6 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
   unsigned cur = 0;  // bit l: level l currently lives in ualt
   auto fld = [&](int l) -> T * { return ((cur >> l) & 1) ? A.ualt : A.u; };
   auto oth = [&](int l) -> T * { return ((cur >> l) & 1) ? A.u : A.ualt; };
-  T *scratch = &S.tile[0][0];  // restriction phase staging (no bulk copies in flight then)
   __shared__ double s_direct[1024];  // coarsest-level direct solution (CTA 0)
 
   auto first_of = [&](bool loc) { return loc ? slot : blockIdx.x * nslots + slot; };
@@ -939,8 +982,9 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
         cur ^= 1u << l;
         if (!sync(ok, loc, loc)) return false;
       }
-      if (runs(loc)) ph_restrict<T>(A, l, fld(l), fld(l - 1), first_of(loc), step_of(loc), t, slot, scratch);
-      if (!sync(true, loc, (l - 1) <= K)) return false;
+      bool okr = true;
+      if (runs(loc)) okr = ph_restrict<T>(A, l, fld(l), fld(l - 1), first_of(loc), step_of(loc), t, slot, S, pk);
+      if (!sync(okr, loc, (l - 1) <= K)) return false;
     }
     // coarsest level
     if (A.it_P) {
