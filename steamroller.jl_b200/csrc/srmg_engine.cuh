@@ -215,6 +215,7 @@ constexpr int kBuf = 3;
 template <typename T>
 struct SlotSmem {
   T tile[kBuf][kSS];
+  T tile2[kBuf][kSS];  // prolongation phase: the parent block's e tile
   T red[256];   // restriction phase: the residual of the block being restricted
   int4 recs[32][5];
   uint64_t bar[kBuf];
@@ -311,6 +312,15 @@ __device__ __forceinline__ void issue_tile(SlotSmem<T> &S, int buf, const T *src
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   mbar_expect_tx(&S.bar[buf], (uint32_t)(kSS * sizeof(T)));
   bulk_g2s(S.tile[buf], src + (int64_t)X * kSS, (uint32_t)(kSS * sizeof(T)), &S.bar[buf]);
+}
+
+// Two tiles on one mbarrier: block X of src into tile[buf], block Y of src2 into tile2[buf].
+template <typename T>
+__device__ __forceinline__ void issue_pair(SlotSmem<T> &S, int buf, const T *src, int X, const T *src2, int Y) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  mbar_expect_tx(&S.bar[buf], (uint32_t)(2 * kSS * sizeof(T)));
+  bulk_g2s(S.tile[buf], src + (int64_t)X * kSS, (uint32_t)(kSS * sizeof(T)), &S.bar[buf]);
+  bulk_g2s(S.tile2[buf], src2 + (int64_t)Y * kSS, (uint32_t)(kSS * sizeof(T)), &S.bar[buf]);
 }
 
 // Halo cell of thread t < 64: face t/16, position t%16 along the face, in the
@@ -597,31 +607,77 @@ __device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
 
 // u_fine += P(e_coarse) on every valid cell (in place in uf), pushes of the new edge
 // values, and the fine block's refinement-boundary ghosts from uc (final coarse level).
+// Per child edge the fine block's u tile and its parent's e tile arrive together by
+// two bulk copies on one mbarrier of the slot's triple-buffered pipeline, and the
+// child's face records are staged in shared memory.  Children of frozen items are
+// skipped.
 template <typename T>
-__device__ void ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int first, int step, int t) {
+__device__ bool ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int first, int step, int t, int slot,
+                           SlotSmem<T> &S, unsigned &pk) {
   const int n = A.tr.nch[l - 1];
   const int4 *ch = A.tr.lvl_child[l - 1];
+  const int nmine = (first < n) ? (n - 1 - first) / step + 1 : 0;
+  if (nmine == 0) return true;
   const int dx = t & 15, dy = t >> 4;
   const int x = 2 + dx, y = 2 + dy;
-  for (int i = first; i < n; i += step) {
-    const int4 e = ch[i];
-    const int F = e.x, C = e.y;
-    const int item = A.tr.info[F].z >> 8;
-    if (is_frozen(A, item)) continue;
-    const int ir = dx & 1, iz = dy & 1;
-    const int jr = 2 + 8 * (e.z - 1) + (dx >> 1), jz = 2 + 8 * (e.w - 1) + (dy >> 1);
-    const T *cb = A.e + (int64_t)C * kSS;
-    const int oc = jr + kS * jz;
-    T v = dmul<T>(T(0.5), cb[oc]);
-    v = dadd<T>(v, dmul<T>(T(0.25), cb[oc + (2 * ir - 1)]));
-    v = dadd<T>(v, dmul<T>(T(0.25), cb[oc + kS * (2 * iz - 1)]));
-    T *d = uf + (int64_t)F * kSS + x + kS * y;
-    const T nu = dadd<T>(v, *d);
-    *d = nu;
-    const int4 *fc = A.tr.faces + 4 * F;
-    push<T>(A, item, uf, F, fc, x, y, nu);
-    if (t < 128) refbnd_ghost<T>(uf, uc, F, fc, t);
+  const int ir = dx & 1, iz = dy & 1;
+  for (int c0 = 0; c0 < nmine; c0 += 32) {
+    // the chunk's next 32 child edges, without those of frozen items:
+    // recs[q][0] = {fine, coarse, sb_r, sb_z}, recs[q][1..4] = the fine block's faces
+    if (t < 32) {
+      const int idx = c0 + t;
+      int gi = 0;
+      bool take = false;
+      if (idx < nmine) {
+        gi = first + idx * step;
+        take = A.nitems == 1 || !A.frozen[A.tr.info[ch[gi].x].z >> 8];
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, take);
+      if (take) S.sel[__popc(m & ((1u << t) - 1u))] = gi;
+      if (t == 0) S.cnt = __popc(m);
+    }
+    slot_sync(slot);
+    const int cn = S.cnt;
+    if (t < 5 * cn) {
+      const int q = t / 5, k = t - 5 * q;
+      const int4 e = ch[S.sel[q]];
+      S.recs[q][k] = k == 0 ? e : A.tr.faces[4 * e.x + k - 1];
+    }
+    slot_sync(slot);
+    if (cn == 0) continue;
+    if (t == 0) {
+      issue_pair<T>(S, pk % kBuf, uf, S.recs[0][0].x, A.e, S.recs[0][0].y);
+      if (cn > 1) issue_pair<T>(S, (pk + 1) % kBuf, uf, S.recs[1][0].x, A.e, S.recs[1][0].y);
+    }
+    for (int j = 0; j < cn; ++j) {
+      const unsigned kb = pk + j;
+      const int buf = kb % kBuf;
+      const int4 e = S.recs[j][0];
+      const int4 *fc = &S.recs[j][1];
+      const int F = e.x;
+      if (t == 0 && j + 2 < cn)
+        issue_pair<T>(S, (kb + 2) % kBuf, uf, S.recs[j + 2][0].x, A.e, S.recs[j + 2][0].y);
+      if (!mbar_wait(&S.bar[buf], (kb / kBuf) & 1, A.err, A.timeout_ns)) {
+        for (int q = 1; q <= 2 && j + q < cn; ++q)
+          mbar_wait(&S.bar[(kb + q) % kBuf], ((kb + q) / kBuf) & 1, A.err, A.timeout_ns);
+        return false;
+      }
+      const T *ut = S.tile[buf], *cb = S.tile2[buf];
+      const int jr = 2 + 8 * (e.z - 1) + (dx >> 1), jz = 2 + 8 * (e.w - 1) + (dy >> 1);
+      const int oc = jr + kS * jz;
+      T v = dmul<T>(T(0.5), cb[oc]);
+      v = dadd<T>(v, dmul<T>(T(0.25), cb[oc + (2 * ir - 1)]));
+      v = dadd<T>(v, dmul<T>(T(0.25), cb[oc + kS * (2 * iz - 1)]));
+      const T nu = dadd<T>(v, ut[x + kS * y]);
+      uf[(int64_t)F * kSS + x + kS * y] = nu;
+      const int item = A.tr.info[F].z >> 8;
+      push<T>(A, item, uf, F, fc, x, y, nu);
+      if (t < 128) refbnd_ghost<T>(uf, uc, F, fc, t);
+      slot_sync(slot);  // the buffers are refilled three items later
+    }
+    pk += cn;
   }
+  return true;
 }
 
 // ---- mixed-precision outer step (FP64) ---------------------------------------------
@@ -1006,8 +1062,9 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
     // ascending leg
     for (int l = 2; l <= L; ++l) {
       const bool loc = l <= K;
-      if (runs(loc)) ph_prolong<T>(A, l, fld(l), fld(l - 1), first_of(loc), step_of(loc), t);
-      if (!sync(true, loc, loc)) return false;
+      bool okp = true;
+      if (runs(loc)) okp = ph_prolong<T>(A, l, fld(l), fld(l - 1), first_of(loc), step_of(loc), t, slot, S, pk);
+      if (!sync(okp, loc, loc)) return false;
       for (int it = 0; it < A.nup; ++it) {
         const bool last = it == A.nup - 1;
         bool ok = true;
