@@ -316,6 +316,12 @@ int srmg_cnn_gradients(srmg_cnn *net, const uint16_t *x, const float *t, const i
 /* One Adam step (beta 0.9/0.999, eps 1e-8) on that loss over the n samples. */
 int srmg_cnn_train_step(srmg_cnn *net, const uint16_t *x, const float *t, const int *ir0,
                         float lambda, int geom, int n, float lr, double *loss);
+/* The same inference forward on the 5th-generation tensor cores (tcgen05 MMAs with
+ * accumulators in tensor memory); srmg_cnn_tc_status synchronises and reports a timed-
+ * out MMA completion wait; srmg_cnn_use_tcgen05 makes srmg_cnn_predict_dev use it. */
+int srmg_cnn_forward_tc(srmg_cnn *net, const uint16_t *x, float *y, int n);
+int srmg_cnn_tc_status(srmg_cnn *net);
+int srmg_cnn_use_tcgen05(srmg_cnn *net, int enable);
 /* Training against a loss computed by the caller: the forward pass keeps every layer's
  * activations and writes y (DEVICE float [n][256]); the backward pass takes dLoss/dy
  * (DEVICE float [n][256]) for the same n samples, and applies one Adam step when

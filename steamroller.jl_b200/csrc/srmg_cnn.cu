@@ -492,11 +492,13 @@ __global__ void k_cnn_reduce(int l, const float *__restrict__ dw_part, const flo
   }
 }
 
+#include "srmg_cnn_tc.cuh"
+
 // Packed BF16 weights from the master vector: wpk (forward: rows co, columns ci) and
 // wt (input gradient: rows ci, columns co), both [layer][tap][32 x 32 swizzled], zero
 // where a layer has fewer channels; bias [layer][32].
 __global__ void k_cnn_pack(const float *__restrict__ master, __nv_bfloat16 *__restrict__ wpk,
-                           __nv_bfloat16 *__restrict__ wt, float *__restrict__ bias) {
+                           __nv_bfloat16 *__restrict__ wt, float *__restrict__ bias, unsigned char *__restrict__ wtc) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kL * 9 * kWMat; i += gridDim.x * blockDim.x) {
     const int l = i / (9 * kWMat), rem = i % (9 * kWMat), tap = rem / kWMat, r = (rem % kWMat) / kC,
               c = rem % kC;
@@ -508,6 +510,9 @@ __global__ void k_cnn_pack(const float *__restrict__ master, __nv_bfloat16 *__re
     const int base = (l * 9 + tap) * kWMat * 2;
     *reinterpret_cast<__nv_bfloat16 *>(reinterpret_cast<char *>(wpk) + base + swz(r, c)) = __float2bfloat16_rn(vf);
     *reinterpret_cast<__nv_bfloat16 *>(reinterpret_cast<char *>(wt) + base + swz(r, c)) = __float2bfloat16_rn(vt);
+    // tensor-core copy: canonical no-swizzle K-major, rows co, 16-byte chunks of ci
+    *reinterpret_cast<__nv_bfloat16 *>(wtc + (l * 9 + tap) * 2048 + cm_off(r, c >> 3) + (c & 7) * 2) =
+        __float2bfloat16_rn(vf);
   }
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kL * kC; i += gridDim.x * blockDim.x) {
     const int l = i / kC, co = i % kC;
@@ -722,6 +727,9 @@ struct srmg_cnn {
   float *master = nullptr, *grad = nullptr, *adam_m = nullptr, *adam_v = nullptr;
   __nv_bfloat16 *wpk = nullptr, *wt = nullptr;
   float *bias = nullptr;
+  unsigned char *wtc = nullptr;  // weights in the tcgen05 operand layout
+  int *tc_err = nullptr;         // error word of the tcgen05 forward
+  bool use_tc = false;           // the warm start's forward pass on tcgen05
   int adam_t = 0;
   int train_n = 0;  // samples of the last training forward
   DevBuf acts, dz0, dz1, dwp, dbp, lossp, y;
@@ -733,7 +741,7 @@ namespace {
 int cnn_grid(srmg_cnn *net, int n) { return std::max(1, std::min(n, net->nsm)); }
 
 int cnn_pack(srmg_cnn *net) {
-  k_cnn_pack<<<64, 256, 0, net->stream>>>(net->master, net->wpk, net->wt, net->bias);
+  k_cnn_pack<<<64, 256, 0, net->stream>>>(net->master, net->wpk, net->wt, net->bias, net->wtc);
   return cuda_check(net->err_ctx, cudaGetLastError(), "k_cnn_pack");
 }
 
@@ -742,6 +750,7 @@ int cnn_setup_attrs(srmg_cnn *net) {
   CK(cudaFuncSetAttribute(k_cnn_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FwdSmem)));
   CK(cudaFuncSetAttribute(k_cnn_dx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FwdSmem)));
   CK(cudaFuncSetAttribute(k_cnn_dw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DwSmem)));
+  CK(cudaFuncSetAttribute(k_cnn_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem)));
   return SRMG_OK;
 }
 
@@ -840,7 +849,8 @@ extern "C" int srmg_cnn_create(srmg_cnn **out, int device, uint64_t seed) {
   if (!dalloc((void **)&net->master, np * 4) || !dalloc((void **)&net->grad, np * 4) ||
       !dalloc((void **)&net->adam_m, np * 4) || !dalloc((void **)&net->adam_v, np * 4) ||
       !dalloc((void **)&net->wpk, kWElems * 2) || !dalloc((void **)&net->wt, kWElems * 2) ||
-      !dalloc((void **)&net->bias, kL * kC * 4)) {
+      !dalloc((void **)&net->bias, kL * kC * 4) || !dalloc((void **)&net->wtc, kTcWBytes) ||
+      !dalloc((void **)&net->tc_err, sizeof(int))) {
     srmg_cnn_destroy(net);
     return SRMG_ERR_NOMEM;
   }
@@ -848,6 +858,8 @@ extern "C" int srmg_cnn_create(srmg_cnn **out, int device, uint64_t seed) {
   cudaMemset(net->adam_m, 0, np * 4);
   cudaMemset(net->adam_v, 0, np * 4);
   cudaMemset(net->grad, 0, np * 4);
+  cudaMemset(net->wtc, 0, kTcWBytes);
+  cudaMemset(net->tc_err, 0, sizeof(int));
   if ((rc = cnn_setup_attrs(net)) || (rc = cnn_pack(net))) {
     srmg_cnn_destroy(net);
     return rc;
@@ -862,7 +874,7 @@ extern "C" void srmg_cnn_destroy(srmg_cnn *net) {
   cudaSetDevice(net->device);
   cudaStreamSynchronize(net->stream);
   for (void *p : {(void *)net->master, (void *)net->grad, (void *)net->adam_m, (void *)net->adam_v, (void *)net->wpk,
-                  (void *)net->wt, (void *)net->bias})
+                  (void *)net->wt, (void *)net->bias, (void *)net->wtc, (void *)net->tc_err})
     if (p) cudaFree(p);
   for (DevBuf *b : {&net->acts, &net->dz0, &net->dz1, &net->dwp, &net->dbp, &net->lossp, &net->y})
     if (b->p) cudaFree(b->p);
@@ -904,6 +916,33 @@ extern "C" int srmg_cnn_forward(srmg_cnn *net, const uint16_t *x, float *y, int 
   k_cnn_fwd<<<cnn_grid(net, n), kThreads, sizeof(FwdSmem), net->stream>>>((const __nv_bfloat16 *)x, n, net->wpk,
                                                                           net->bias, y, nullptr);
   CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+extern "C" int srmg_cnn_forward_tc(srmg_cnn *net, const uint16_t *x, float *y, int n) {
+  if (!net || !x || !y || n < 0) return SRMG_ERR_BADARG;
+  if (n == 0) return SRMG_OK;
+  cudaSetDevice(net->device);
+  srmg_ctx *ctx = net->err_ctx;
+  k_cnn_fwd_tc<<<cnn_grid(net, n), kTcThreads, sizeof(TcSmem), net->stream>>>((const __nv_bfloat16 *)x, n, net->wtc,
+                                                                            net->bias, y, net->tc_err, nullptr);
+  CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+extern "C" int srmg_cnn_tc_status(srmg_cnn *net) {
+  if (!net) return SRMG_ERR_BADARG;
+  cudaSetDevice(net->device);
+  srmg_ctx *ctx = net->err_ctx;
+  int e = 0;
+  CK(cudaStreamSynchronize(net->stream));
+  CK(cudaMemcpy(&e, net->tc_err, sizeof(int), cudaMemcpyDeviceToHost));
+  return e ? fail(ctx, SRMG_ERR_TIMEOUT, "tcgen05 forward: MMA completion wait timed out") : SRMG_OK;
+}
+
+extern "C" int srmg_cnn_use_tcgen05(srmg_cnn *net, int enable) {
+  if (!net) return SRMG_ERR_BADARG;
+  net->use_tc = enable != 0;
   return SRMG_OK;
 }
 
@@ -1073,8 +1112,12 @@ extern "C" int srmg_cnn_predict_dev(srmg_ctx *ctx, srmg_cnn *net, double *u, con
   const int got = cnn_pack_tree(ctx, f, g, g, nblk_alloc, s, op, k2, geom, bc, x, scale, blk, part, norms,
                                 sel ? list : nullptr, sel ? count : nullptr, theta);
   if (got < 0) return got;
-  k_cnn_fwd<<<cnn_grid(net, n), kThreads, sizeof(FwdSmem), ctx->stream>>>(x, n, net->wpk, net->bias, y, nullptr,
-                                                                          sel ? count : nullptr);
+  if (net->use_tc)
+    k_cnn_fwd_tc<<<cnn_grid(net, n), kTcThreads, sizeof(TcSmem), ctx->stream>>>(x, n, net->wtc, net->bias, y,
+                                                                                net->tc_err, sel ? count : nullptr);
+  else
+    k_cnn_fwd<<<cnn_grid(net, n), kThreads, sizeof(FwdSmem), ctx->stream>>>(x, n, net->wpk, net->bias, y, nullptr,
+                                                                            sel ? count : nullptr);
   CK(cudaGetLastError());
   k_cnn_scatter<<<(int)std::min<int64_t>(4096, ((int64_t)n * 256 + 255) / 256), 256, 0, ctx->stream>>>(
       lrn, ext, y, scale, ctx->d_leaf, n, sel ? list : nullptr, sel ? count : nullptr);

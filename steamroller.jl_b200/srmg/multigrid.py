@@ -122,6 +122,9 @@ SIGNATURES = {
     "srmg_cnn_gradients": (_I, [_P, _P, _P, _P, ctypes.c_float, _I, _I, _P, ctypes.POINTER(_D)]),
     "srmg_cnn_train_step": (_I, [_P, _P, _P, _P, ctypes.c_float, _I, _I, ctypes.c_float, ctypes.POINTER(_D)]),
     "srmg_cnn_forward_train": (_I, [_P, _P, _I, _P]),
+    "srmg_cnn_forward_tc": (_I, [_P, _P, _P, _I]),
+    "srmg_cnn_tc_status": (_I, [_P]),
+    "srmg_cnn_use_tcgen05": (_I, [_P, _I]),
     "srmg_cnn_backward_step": (_I, [_P, _P, _I, ctypes.c_float, _P]),
     "srmg_cnn_leaf_blocks": (_I, [_P]),
     "srmg_cnn_last_active": (_I, [_P]),
@@ -495,6 +498,24 @@ def _cnn_backward_step(self, dy, lr, want_grad=False):
     return g
 
 
+def _cnn_forward_tc(self, x):
+    """Inference forward on the tcgen05 tensor cores: x torch bf16 [n, 400, 2] -> float32 [n, 256]."""
+    import torch
+    n = x.shape[0]
+    y = torch.empty((n, 256), dtype=torch.float32, device=x.device)
+    torch.cuda.synchronize()
+    self.check(lib().srmg_cnn_forward_tc(self._h, x.data_ptr(), y.data_ptr(), n))
+    self.check(lib().srmg_cnn_tc_status(self._h))
+    return y
+
+
+def _cnn_use_tcgen05(self, enable=True):
+    self.check(lib().srmg_cnn_use_tcgen05(self._h, int(enable)))
+    return self
+
+
+Cnn.forward_tc = _cnn_forward_tc
+Cnn.use_tcgen05 = _cnn_use_tcgen05
 Cnn.forward_train = _cnn_forward_train
 Cnn.backward_step = _cnn_backward_step
 
