@@ -357,6 +357,23 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
     wp32[i] = (float)wp[i];
   }
 
+  // The same tables as rows per block coordinate c (geometry 1: the block's r
+  // coordinate, geometry 2: its z coordinate): row c holds wm, then wp, at the 20 tile
+  // positions k = 0..19 (global index i = k - 1 + 16 (c - 1)), zero where i falls
+  // outside the table.  The engine copies one row per block with the block's tiles.
+  const int nwrow = (int)max_coord + 1;
+  std::vector<double> wrow(2 * kS * (size_t)nwrow, 0.0);
+  std::vector<float> wrow32(2 * kS * (size_t)nwrow, 0.f);
+  for (int c = 1; c < nwrow; c++)
+    for (int k = 0; k < kS; k++) {
+      const int64_t i = k - 1 + (int64_t)kM * (c - 1);
+      if (i < 0 || i >= wn) continue;
+      wrow[2 * kS * (size_t)c + k] = wm[i];
+      wrow[2 * kS * (size_t)c + kS + k] = wp[i];
+      wrow32[2 * kS * (size_t)c + k] = wm32[i];
+      wrow32[2 * kS * (size_t)c + kS + k] = wp32[i];
+    }
+
   // layout: per level blocks/faces/child, then coord_of, then weight tables
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -374,6 +391,7 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
   const size_t ocoord = take((max_blk + 1) * sizeof(int2));
   const size_t owm = take(wn * sizeof(double)), owp = take(wn * sizeof(double));
   const size_t owm32 = take(wn * sizeof(float)), owp32 = take(wn * sizeof(float));
+  const size_t owr = take(wrow.size() * sizeof(double)), owr32 = take(wrow32.size() * sizeof(float));
   const size_t oinfo = take((max_blk + 1) * sizeof(int4));
   const size_t ofaceb = take(4 * (max_blk + 1) * sizeof(int4));
   const size_t okids = take((max_blk + 1) * sizeof(int4));
@@ -396,6 +414,8 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
   memcpy(host.data() + owp, wp.data(), wn * sizeof(double));
   memcpy(host.data() + owm32, wm32.data(), wn * sizeof(float));
   memcpy(host.data() + owp32, wp32.data(), wn * sizeof(float));
+  memcpy(host.data() + owr, wrow.data(), wrow.size() * sizeof(double));
+  memcpy(host.data() + owr32, wrow32.data(), wrow32.size() * sizeof(float));
   memcpy(host.data() + oinfo, binfo.data(), binfo.size() * sizeof(int4));
   memcpy(host.data() + ofaceb, bface.data(), bface.size() * sizeof(int4));
   memcpy(host.data() + okids, bkids.data(), bkids.size() * sizeof(int4));
@@ -409,7 +429,9 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
   void *d = nullptr;
   if (cudaMalloc(&d, off) != cudaSuccess) return fail(ctx, SRMG_ERR_NOMEM, "tree allocation of %zu bytes", off);
   ctx->d_tree = d;
-  CK(cudaMemcpy(d, host.data(), off, cudaMemcpyHostToDevice));
+  // on the context's (non-blocking) stream, so that its later work is ordered after it
+  CK(cudaMemcpyAsync(d, host.data(), off, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   char *base = (char *)d;
   ctx->nlev = nlev;
   ctx->lv.resize(nlev);
@@ -430,6 +452,8 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
   ctx->d_wp64 = (double *)(base + owp);
   ctx->d_wm32 = (float *)(base + owm32);
   ctx->d_wp32 = (float *)(base + owp32);
+  ctx->d_wrow64 = (double *)(base + owr);
+  ctx->d_wrow32 = (float *)(base + owr32);
   ctx->refbnd_levels = 0;
   for (int l = 0; l < nlev; l++)
     if (nrb[l] > 0 && l + 1 < 32) ctx->refbnd_levels |= 1u << (l + 1);

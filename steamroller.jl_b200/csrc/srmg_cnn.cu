@@ -854,12 +854,17 @@ extern "C" int srmg_cnn_create(srmg_cnn **out, int device, uint64_t seed) {
     srmg_cnn_destroy(net);
     return SRMG_ERR_NOMEM;
   }
-  cudaMemcpy(net->master, h.data(), np * 4, cudaMemcpyHostToDevice);
-  cudaMemset(net->adam_m, 0, np * 4);
-  cudaMemset(net->adam_v, 0, np * 4);
-  cudaMemset(net->grad, 0, np * 4);
-  cudaMemset(net->wtc, 0, kTcWBytes);
-  cudaMemset(net->tc_err, 0, sizeof(int));
+  // Everything on the network's stream, in order: the stream is non-blocking, so
+  // nothing orders it after work on the legacy default stream (a plain cudaMemset of
+  // wtc could otherwise land after the pack below and wipe it).
+  bool set = cudaMemcpyAsync(net->master, h.data(), np * 4, cudaMemcpyHostToDevice, net->stream) == cudaSuccess;
+  for (auto [p, b] : {std::pair<void *, size_t>{net->adam_m, np * 4}, {net->adam_v, np * 4}, {net->grad, np * 4},
+                      {net->wtc, (size_t)kTcWBytes}, {net->tc_err, sizeof(int)}})
+    set = set && cudaMemsetAsync(p, 0, b, net->stream) == cudaSuccess;
+  if (!set) {
+    srmg_cnn_destroy(net);
+    return SRMG_ERR_CUDA;
+  }
   if ((rc = cnn_setup_attrs(net)) || (rc = cnn_pack(net))) {
     srmg_cnn_destroy(net);
     return rc;

@@ -70,6 +70,8 @@ struct srmg_ctx {
   int2 *d_coord_of = nullptr;          // [max_blk] coords by 0-based block id
   double *d_wm64 = nullptr, *d_wp64 = nullptr;
   float *d_wm32 = nullptr, *d_wp32 = nullptr;
+  double *d_wrow64 = nullptr;  // the weight tables as rows per block coordinate (2 x 20 values)
+  float *d_wrow32 = nullptr;
   // block-id-indexed tables for the persistent engine
   int4 *d_info = nullptr;    // {coord_r, coord_z, child_mask, level}
   int4 *d_faceb = nullptr;   // [blk*4+f] {type, src, sb_r | sb_z << 8, push_to}

@@ -26,6 +26,12 @@ template <>
 WTab<double> wtab_of<double>(srmg_ctx *ctx) { return WTab<double>{ctx->d_wm64, ctx->d_wp64}; }
 template <>
 WTab<float> wtab_of<float>(srmg_ctx *ctx) { return WTab<float>{ctx->d_wm32, ctx->d_wp32}; }
+template <typename T>
+const T *wrow_of(srmg_ctx *ctx);
+template <>
+const double *wrow_of<double>(srmg_ctx *ctx) { return ctx->d_wrow64; }
+template <>
+const float *wrow_of<float>(srmg_ctx *ctx) { return ctx->d_wrow32; }
 
 template <typename T>
 int engine_grid(srmg_ctx *ctx, int *grid) {
@@ -74,6 +80,7 @@ static int engine_common(srmg_ctx *ctx, EngArgs<T> &A, T *u, const ItemTabs &tab
   A.tr.faces = ctx->d_faceb;
   A.tr.kids = ctx->d_kids;
   A.wt = wtab_of<T>(ctx);
+  A.wrow = (geom == 1 || geom == 2) ? wrow_of<T>(ctx) : nullptr;
   A.geom = geom;
   A.nitems = ctx->nitems;
   A.nlev_tab = ctx->nlev;
@@ -120,6 +127,11 @@ int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, const ItemTabs &
   EngArgs<T> A;
   RC(engine_common<T>(ctx, A, u, tabs, geom));
   A.b = b;
+  // Tolerance-driven solves run on the engine's own copy of b (FP64: a copy of the
+  // caller's b; mixed: the FP32 defect), whose ghost cells then carry the neighbours'
+  // edge values, filled once per launch (FP64) or with every defect (mixed).  One
+  // V-cycle per launch (vcycle!) leaves the caller's b ghosts alone.
+  A.bghost = run->max_cycles > 0 ? 1 : 0;
   A.u1 = u1;
   A.e = e;
   A.lmax = L;
@@ -161,7 +173,7 @@ int srmg::engine_smooth(srmg_ctx *ctx, T *u, const T *b, const ItemTabs &tabs, i
   if (n <= 0 || ctx->nblk_host[level - 1] == 0) return SRMG_OK;
   EngArgs<T> A;
   RC(engine_common<T>(ctx, A, u, tabs, geom));
-  A.b = const_cast<T *>(b);
+  A.b = const_cast<T *>(b);  // read only: bghost stays 0
   A.lmax = level;
   A.smooth_level = level;
   A.smooth_n = n;

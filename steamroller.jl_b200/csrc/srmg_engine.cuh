@@ -77,7 +77,9 @@ struct EngArgs {
   T *u, *ualt, *b, *u1, *e;   // ualt: the second buffer of the per-level ping-pong
   EngTree tr;
   WTab<T> wt;
+  const T *wrow;     // weight rows per block coordinate (2 x kS values each), or null (geometry 0)
   int geom;
+  int bghost;        // b's neighbour-copy ghosts are kept filled (the launch may write them)
   int lmax;          // finest non-empty level taking part
   int ndown, ntop, nup;
   int local_top;     // levels 1..local_top run inside CTA 0
@@ -129,6 +131,8 @@ __device__ __forceinline__ long long gtimer() {
 __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err, unsigned &epoch,
                                              long long timeout_ns) {
   __shared__ int ok_s;
+  // this phase's generic-proxy stores are ordered before the next phase's bulk copies
+  asm volatile("fence.proxy.async.global;" ::: "memory");
   __syncthreads();
   if (threadIdx.x == 0) {
     epoch++;
@@ -151,6 +155,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err, unsigned &
     ok_s = ok;
   }
   __syncthreads();
+  asm volatile("fence.proxy.async.global;" ::: "memory");
   return ok_s != 0;
 }
 
@@ -210,18 +215,61 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
   return true;
 }
 
-// Per-slot staging: triple-buffered block tiles and the records of up to 32 blocks.
-constexpr int kBuf = 3;
+// Per-slot staging: kBuf buffers of block tiles and the records of a chunk of up to
+// kChunk blocks.  The GS and restriction phases take two blocks per iteration (one per
+// half slot), so four buffers hold the current pair and the next; the prolongation
+// phase runs kBuf - 1 blocks ahead.  Shared memory is kept small on purpose: what the
+// CTA does not claim stays L1 cache for the scattered loads (face records, coarse
+// values of refinement ghosts, spills), and a larger staging area measured slower.
+constexpr int kBuf = 4;
+constexpr int kChunk = 32;
+constexpr int kWRow = 2 * kS;  // a weight row: wm, then wp, at the tile positions 0..19
 template <typename T>
 struct SlotSmem {
   T tile[kBuf][kSS];
-  T tile2[kBuf][kSS];  // prolongation phase: the parent block's e tile
-  T red[256];   // restriction phase: the residual of the block being restricted
-  int4 recs[32][5];
+  T tile2[kBuf][kSS];  // the second tile of a pair: b (GS, restriction) or the parent's e (prolongation)
+  T wst[kBuf][kWRow];  // the block's weight row (GS, restriction)
+  int4 recs[kChunk][6];
   uint64_t bar[kBuf];
-  int sel[32];  // list positions of the chunk's blocks that take part
+  int sel[kChunk];  // list positions of the chunk's blocks that take part
   int cnt;
 };
+// Bulk copies land on 16-byte boundaries: every tile buffer of every slot.
+static_assert(sizeof(SlotSmem<double>) % 16 == 0 && sizeof(SlotSmem<float>) % 16 == 0, "slot size");
+static_assert((kSS * sizeof(float)) % 16 == 0 && (kBuf * kSS * sizeof(float)) % 16 == 0, "tile offsets");
+static_assert((kWRow * sizeof(float)) % 16 == 0, "weight rows");
+
+// Warp 0 of a slot: the list positions first + idx * step, c0 <= idx < min(c0 + kChunk,
+// nmine), whose item is live (take(gi) true), compacted in order into S.sel; S.cnt
+// their number.  The caller synchronises the slot before reading them.
+template <typename T, typename Take>
+__device__ __forceinline__ void select_chunk(SlotSmem<T> &S, int t, int c0, int nmine, int first, int step,
+                                             Take take_of) {
+  if (t < 32) {
+    int base = 0;
+    for (int h = 0; h < kChunk / 32; ++h) {
+      const int idx = c0 + 32 * h + t;
+      int gi = 0;
+      bool take = false;
+      if (idx < nmine) {
+        gi = first + idx * step;
+        take = take_of(gi);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, take);
+      if (take) S.sel[base + __popc(m & ((1u << t) - 1u))] = gi;
+      base += __popc(m);
+    }
+    if (t == 0) S.cnt = base;
+  }
+}
+
+// After a failed wait on block j's buffer: wait (bounded) for the copies issued for
+// blocks j + 1 .. j + kBuf - 1 of the chunk, so that none is left in flight.
+template <typename T>
+__device__ __forceinline__ void drain_slot(const EngArgs<T> &A, SlotSmem<T> &S, unsigned kb, int j, int cn) {
+  for (int q = 1; q < kBuf && j + q < cn; ++q)
+    mbar_wait(&S.bar[(kb + q) % kBuf], ((kb + q) / kBuf) & 1, A.err, A.timeout_ns);
+}
 
 // Boundary sign k (-1, 0 or 1) of a packed boundary table.
 template <typename F>
@@ -255,6 +303,28 @@ __device__ __forceinline__ void push_f(unsigned sgb, F *field, int X, const int4
     const int4 fi = fc[3];
     if (fi.w >= 0) field[(int64_t)fi.w * kSS + x + kS * (y - kM)] = v;
     else if (fi.x == FACE_BOUNDARY) xb[x + kS * (2 * (kG + kM) - 1 - y)] = dmul<F>(sign_at<F>(sgb, 7), v);
+  }
+}
+
+// The neighbour copies of push_f only (no mirror ghosts).
+template <typename F>
+__device__ __forceinline__ void copy_ghost(F *field, int X, const int4 *fc, int x, int y, F v) {
+  (void)X;
+  if (x <= 3) {
+    const int4 fi = fc[0];
+    if (fi.w >= 0) field[(int64_t)fi.w * kSS + (x + kM) + kS * y] = v;
+  }
+  if (x >= 16) {
+    const int4 fi = fc[1];
+    if (fi.w >= 0) field[(int64_t)fi.w * kSS + (x - kM) + kS * y] = v;
+  }
+  if (y <= 3) {
+    const int4 fi = fc[2];
+    if (fi.w >= 0) field[(int64_t)fi.w * kSS + x + kS * (y + kM)] = v;
+  }
+  if (y >= 16) {
+    const int4 fi = fc[3];
+    if (fi.w >= 0) field[(int64_t)fi.w * kSS + x + kS * (y - kM)] = v;
   }
 }
 
@@ -306,14 +376,6 @@ __device__ __forceinline__ void refbnd_ghost(T *dst, const T *src, int X, const 
 
 // ------------------------------------------------------------------ phases
 
-// Issue the bulk copy of one block tile into buffer `buf` of a slot.
-template <typename T>
-__device__ __forceinline__ void issue_tile(SlotSmem<T> &S, int buf, const T *src, int X) {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  mbar_expect_tx(&S.bar[buf], (uint32_t)(kSS * sizeof(T)));
-  bulk_g2s(S.tile[buf], src + (int64_t)X * kSS, (uint32_t)(kSS * sizeof(T)), &S.bar[buf]);
-}
-
 // Two tiles on one mbarrier: block X of src into tile[buf], block Y of src2 into tile2[buf].
 template <typename T>
 __device__ __forceinline__ void issue_pair(SlotSmem<T> &S, int buf, const T *src, int X, const T *src2, int Y) {
@@ -321,6 +383,33 @@ __device__ __forceinline__ void issue_pair(SlotSmem<T> &S, int buf, const T *src
   mbar_expect_tx(&S.bar[buf], (uint32_t)(2 * kSS * sizeof(T)));
   bulk_g2s(S.tile[buf], src + (int64_t)X * kSS, (uint32_t)(kSS * sizeof(T)), &S.bar[buf]);
   bulk_g2s(S.tile2[buf], src2 + (int64_t)Y * kSS, (uint32_t)(kSS * sizeof(T)), &S.bar[buf]);
+}
+
+// The u and b tiles of block X and, with a weight table, the weight row of the block's
+// coordinate (cr for geometry 1, cz for geometry 2), on one mbarrier.
+template <typename T>
+__device__ __forceinline__ void issue_block(const EngArgs<T> &A, SlotSmem<T> &S, int buf, const T *src, int X,
+                                            int cr, int cz) {
+  const uint32_t wb = A.wrow ? (uint32_t)(kWRow * sizeof(T)) : 0u;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  mbar_expect_tx(&S.bar[buf], (uint32_t)(2 * kSS * sizeof(T)) + wb);
+  bulk_g2s(S.tile[buf], src + (int64_t)X * kSS, (uint32_t)(kSS * sizeof(T)), &S.bar[buf]);
+  bulk_g2s(S.tile2[buf], A.b + (int64_t)X * kSS, (uint32_t)(kSS * sizeof(T)), &S.bar[buf]);
+  if (wb) bulk_g2s(S.wst[buf], A.wrow + (int64_t)(A.geom == 1 ? cr : cz) * kWRow, wb, &S.bar[buf]);
+}
+
+// weights() from a staged weight row.
+template <typename T>
+__device__ __forceinline__ W5<T> wrow_w(int geom, const T *row, int x, int y) {
+  W5<T> w{T(1), T(1), T(1), T(1)};
+  if (geom == 1) {
+    w.rm = row[x];
+    w.rp = row[kS + x];
+  } else if (geom == 2) {
+    w.zm = row[y];
+    w.zp = row[kS + y];
+  }
+  return w;
 }
 
 // Halo cell of thread t < 64: face t/16, position t%16 along the face, in the
@@ -357,13 +446,103 @@ __device__ __forceinline__ HaloCell halo_cell(int t) {
   return h;
 }
 
-// One fused red-black GS iteration over level l: src -> dst.  256 threads per block,
-// thread t owns valid cell (2 + t%16, 2 + t/16).  Blocks stream through a
-// double-buffered shared-memory pipeline fed by bulk copies, and each block's scattered
-// inputs (its b, the neighbours' edge b and ghost corners) are loaded into registers
-// while the previous block computes.  With `fas`, the FAS right-hand side of the
-// covered cells (src/multigrid.jl:112-119) is formed first from the post-restriction
-// tile and the restricted residual held in e.
+// Vector access to the two cells (x, x+1), x even, of a tile row: 16 bytes (FP64) or 8
+// bytes (FP32), aligned because tiles and fields are 16-byte aligned and kS is even.
+template <typename T> struct Pair2;
+template <> struct Pair2<double> { using V = double2; };
+template <> struct Pair2<float> { using V = float2; };
+template <typename T>
+__device__ __forceinline__ void ld_pair(const T *p, T &a, T &b) {
+  const typename Pair2<T>::V v = *reinterpret_cast<const typename Pair2<T>::V *>(p);
+  a = v.x;
+  b = v.y;
+}
+template <typename T>
+__device__ __forceinline__ void st_pair(T *p, T a, T b) {
+  typename Pair2<T>::V v;
+  v.x = a;
+  v.y = b;
+  *reinterpret_cast<typename Pair2<T>::V *>(p) = v;
+}
+
+// The order-2 stencil of applystencil (src/laplacian.jl:25-49,78-118) on values already
+// loaded: the same products and sums, in the same order, as apply5.
+template <typename T>
+__device__ __forceinline__ T sten5(const W5<T> &w, T centre, T zm, T rm, T c, T rp, T zp) {
+  T v = w.zm * zm;
+  v = v + w.rm * rm;
+  v = v + centre * c;
+  v = v + w.rp * rp;
+  v = v + w.zp * zp;
+  return v;
+}
+
+// push_f for the two cells (x0, y), (x0 + 1, y) of one thread, x0 even: the copies into
+// the neighbours' facing ghosts and (kMirror) the block's own mirror ghosts, as pair
+// stores.
+template <typename F, bool kMirror = true>
+__device__ __forceinline__ void push_pair(unsigned sgb, F *field, int X, const int4 *fc, int x0, int y, F v0,
+                                          F v1) {
+  F *xb = field + (int64_t)X * kSS;
+  if (x0 == 2) {
+    const int4 fi = fc[0];
+    if (fi.w >= 0) st_pair<F>(field + (int64_t)fi.w * kSS + (x0 + kM) + kS * y, v0, v1);
+    else if (kMirror && fi.x == FACE_BOUNDARY) {
+      const F sg = sign_at<F>(sgb, 3);
+      st_pair<F>(xb + kS * y, dmul<F>(sg, v1), dmul<F>(sg, v0));  // x = 3 -> 0, x = 2 -> 1
+    }
+  }
+  if (x0 == 16) {
+    const int4 fi = fc[1];
+    if (fi.w >= 0) st_pair<F>(field + (int64_t)fi.w * kSS + (x0 - kM) + kS * y, v0, v1);
+    else if (kMirror && fi.x == FACE_BOUNDARY) {
+      const F sg = sign_at<F>(sgb, 5);
+      st_pair<F>(xb + 18 + kS * y, dmul<F>(sg, v1), dmul<F>(sg, v0));  // x = 17 -> 18, x = 16 -> 19
+    }
+  }
+  if (y <= 3) {
+    const int4 fi = fc[2];
+    if (fi.w >= 0) st_pair<F>(field + (int64_t)fi.w * kSS + x0 + kS * (y + kM), v0, v1);
+    else if (kMirror && fi.x == FACE_BOUNDARY) {
+      const F sg = sign_at<F>(sgb, 1);
+      st_pair<F>(xb + x0 + kS * (2 * kG - 1 - y), dmul<F>(sg, v0), dmul<F>(sg, v1));
+    }
+  }
+  if (y >= 16) {
+    const int4 fi = fc[3];
+    if (fi.w >= 0) st_pair<F>(field + (int64_t)fi.w * kSS + x0 + kS * (y - kM), v0, v1);
+    else if (kMirror && fi.x == FACE_BOUNDARY) {
+      const F sg = sign_at<F>(sgb, 7);
+      st_pair<F>(xb + x0 + kS * (2 * (kG + kM) - 1 - y), dmul<F>(sg, v0), dmul<F>(sg, v1));
+    }
+  }
+}
+
+// Named barrier of a slot that also ANDs a predicate over its 256 threads.
+__device__ __forceinline__ bool slot_and(int slot, bool ok) {
+  uint32_t r;
+  asm volatile(
+      "{ .reg .pred p, q; setp.ne.u32 q, %1, 0; bar.red.and.pred p, %2, 256, q; selp.u32 %0, 1, 0, p; }"
+      : "=r"(r)
+      : "r"((uint32_t)ok), "r"(slot + 1)
+      : "memory");
+  return r != 0;
+}
+
+// One fused red-black GS iteration over level l: src -> dst (gauss_seidel_iter!,
+// src/multigrid.jl:250-265).  A slot's 256 threads smooth two blocks at a time, one per
+// half; thread h of a half owns the cell pair (x0, y), (x0 + 1, y), x0 = 2 + 2 (h % 8),
+// y = 2 + h / 8, which holds one red and one black cell.  Each block's u tile (with
+// ghosts) and b tile stream through the slot's kBuf-deep shared-memory pipeline as two
+// bulk copies on one mbarrier; the few scattered inputs (the FAS restricted residual,
+// u1 for e, the neighbours' edge b and ghost corners) are loaded into registers one
+// iteration ahead.  Per iteration: the red cells of the pair and the neighbours' red
+// edge cells held in this block's ghost layer are updated in shared memory; one slot
+// barrier; the black cells are updated in registers and the pair is written out with
+// its ghost copies.  With `fas`, the FAS right-hand side of the covered cells
+// (src/multigrid.jl:112-119) is formed first from the post-restriction tile and the
+// restricted residual held in e, and a second barrier separates those reads from the
+// red writes.
 template <typename T>
 __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T *esrc, bool copy_u1,
                        bool make_e, bool fas, int first, int step, int t, int slot, SlotSmem<T> &S,
@@ -372,155 +551,196 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
   const int4 *recs = A.tr.lvl_rec[l - 1];
   const int nmine = (first < n) ? (n - 1 - first) / step + 1 : 0;
   if (nmine == 0) return true;
-  const int x = 2 + (t & 15), y = 2 + (t >> 4);
-  const int o = x + kS * y;
-  const bool red = ((x + y) & 1) == 1;  // colour 0 of RedBlack{0}: updated first
-  const int mysub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
-  const HaloCell h = halo_cell(t < 64 ? t : 0);
-  // registers prefetched one block ahead
-  T b_nx = T(0), e_nx = T(0), hv_nx = T(0), hc_nx = T(0);
+  const int half = t >> 7, h = t & 127;
+  // warp wv of a half holds rows of one parity (wv / 2: even, odd), so that the red and
+  // black roles of a thread's two cells are uniform across the warp
+  const int wv = h >> 5, lane = h & 31;
+  const int x0 = 2 + 2 * (lane & 7), y = 2 + (wv >> 1) + 2 * (4 * (wv & 1) + (lane >> 3));
+  const int o0 = x0 + kS * y;
+  const bool yodd = (y & 1) != 0;  // red (colour 0 of RedBlack{0}, updated first) is x0 if y is odd
+  const int xr = yodd ? x0 : x0 + 1, xbk = yodd ? x0 + 1 : x0;  // the pair's red and black cells
+  const int mysub = ((x0 - 2) >> 3) + 2 * ((y - 2) >> 3);
+  // lanes 0-7 of warp wv: the red cells 2 lane + (wv % 2) of ghost face wv
+  const bool hthr = lane < 8;
+  const int hidx = 16 * wv + 2 * (lane & 7) + (wv & 1);
+  // neighbour values of the halo cell, loaded one iteration ahead
+  // (b comes from b's ghost layer when A.bghost, except the FAS right-hand side of a
+  // covered neighbour cell, formed here from the neighbour's restricted residual in e)
+  T hvn = T(0), hcn = T(0);
   auto prefetch = [&](int j) {
-    const int4 bk = S.recs[j][0];
-    const int X = bk.x;
-    b_nx = A.b[(int64_t)X * kSS + o];
-    if (fas && ((bk.w >> mysub) & 1)) e_nx = A.e[(int64_t)X * kSS + o];
-    if (t < 64 && h.red) {
-      const int4 fi = S.recs[j][1 + h.f];
+    if (hthr) {
+      const HaloCell hc_ = halo_cell(hidx);
+      const int4 fi = S.recs[j][1 + hc_.f];
       if (fi.x == FACE_NEIGHBOR) {
         const int64_t nb = (int64_t)fi.y * kSS;
-        hv_nx = (fas && ((fi.z >> h.nsub) & 1)) ? A.e[nb + h.nx + kS * h.ny] : A.b[nb + h.nx + kS * h.ny];
-        if (h.cx >= 0) hc_nx = src[nb + h.cnx + kS * h.cny];
+        const bool covn = fas && ((fi.z >> hc_.nsub) & 1);
+        if (covn) hvn = A.e[nb + hc_.nx + kS * hc_.ny];
+        else if (!A.bghost) hvn = A.b[nb + hc_.nx + kS * hc_.ny];
+        if (hc_.cx >= 0) hcn = src[nb + hc_.cnx + kS * hc_.cny];
       }
     }
   };
+  auto issue = [&](int j) {
+    const int4 bk = S.recs[j][0];
+    issue_block<T>(A, S, (pk + j) % kBuf, src, bk.x, bk.y, bk.z);
+  };
   // one item: the operator values stay in registers for the whole level
   T s = A.it_par[l], centre = A.it_par[32 + l], nwc = A.it_par[64 + l];
-  for (int c0 = 0; c0 < nmine; c0 += 32) {
+  for (int c0 = 0; c0 < nmine; c0 += kChunk) {
     int cn;
     if (A.nitems == 1) {
-      cn = min(32, nmine - c0);
-      if (t < 5 * cn) {
-        const int q = t / 5, k = t - 5 * q;
+      cn = min(kChunk, nmine - c0);
+      for (int i = t; i < 5 * cn; i += 256) {
+        const int q = i / 5, k = i - 5 * q;
         S.recs[q][k] = recs[5 * (first + (c0 + q) * step) + k];
       }
       slot_sync(slot);
     } else {
-    // the chunk's next 32 list positions, without the blocks of frozen items
-    if (t < 32) {
-      const int idx = c0 + t;
-      int gi = 0;
-      bool take = false;
-      if (idx < nmine) {
-        gi = first + idx * step;
-        take = A.nitems == 1 || !A.frozen[item_of(recs[5 * gi])];
+      // the chunk's next list positions, without the blocks of frozen items
+      select_chunk<T>(S, t, c0, nmine, first, step, [&](int gi) { return !A.frozen[item_of(recs[5 * gi])]; });
+      slot_sync(slot);
+      cn = S.cnt;
+      for (int i = t; i < 5 * cn; i += 256) {
+        const int q = i / 5, k = i - 5 * q;
+        S.recs[q][k] = recs[5 * S.sel[q] + k];
       }
-      const unsigned m = __ballot_sync(0xffffffffu, take);
-      if (take) S.sel[__popc(m & ((1u << t) - 1u))] = gi;
-      if (t == 0) S.cnt = __popc(m);
+      slot_sync(slot);
+      if (cn == 0) continue;
     }
-    slot_sync(slot);
-    cn = S.cnt;
-    if (t < 5 * cn) {
-      const int q = t / 5, k = t - 5 * q;
-      S.recs[q][k] = recs[5 * S.sel[q] + k];
-    }
-    slot_sync(slot);
-    if (cn == 0) continue;
-    }
-    if (t == 0) {
-      issue_tile<T>(S, pk % kBuf, src, S.recs[0][0].x);
-      if (cn > 1) issue_tile<T>(S, (pk + 1) % kBuf, src, S.recs[1][0].x);
-    }
-    prefetch(0);
-    for (int j = 0; j < cn; ++j) {
+    if (t == 0)
+      for (int q = 0; q < kBuf && q < cn; ++q) issue(q);
+    if (half < cn) prefetch(half);
+    for (int i = 0; 2 * i < cn; ++i) {
+      const int j = 2 * i + half;
+      const bool act = j < cn;
       const unsigned kb = pk + j;
       const int buf = kb % kBuf;
-      const int4 bk = S.recs[j][0];
-      const int4 *fc = &S.recs[j][1];
-      const int X = bk.x;
-      // two blocks ahead: the buffer of block j - 1, free since the end of its item
-      if (t == 0 && j + 2 < cn) issue_tile<T>(S, (kb + 2) % kBuf, src, S.recs[j + 2][0].x);
-      T bx = b_nx;
-      const T ex = e_nx, hv = hv_nx, hc = hc_nx;
-      if (j + 1 < cn) prefetch(j + 1);
-      if (!mbar_wait(&S.bar[buf], (kb / kBuf) & 1, A.err, A.timeout_ns)) {
-        // leave no copy in flight: wait (bounded) for those issued for the next items
-        for (int q = 1; q <= 2 && j + q < cn; ++q)
-          mbar_wait(&S.bar[(kb + q) % kBuf], ((kb + q) / kBuf) & 1, A.err, A.timeout_ns);
+      const T hv = hvn, hc = hcn;
+      if (j + 2 < cn) prefetch(j + 2);
+      const int4 bk = S.recs[act ? j : 0][0];
+      const int4 *fc = &S.recs[act ? j : 0][1];
+      const int64_t xo = (int64_t)bk.x * kSS + o0;
+      const bool cov = fas && ((bk.w >> mysub) & 1);
+      // the covered cells' restricted residual (FAS), loaded while the tiles arrive
+      T ex0 = T(0), ex1 = T(0);
+      if (act && cov) ld_pair<T>(A.e + xo, ex0, ex1);
+      bool ok = true;
+      if (act) ok = mbar_wait(&S.bar[buf], (kb / kBuf) & 1, A.err, A.timeout_ns);
+      T *tile = S.tile[buf];
+      T cb = T(0), red_new = T(0), bb = T(0);  // the black cell's old value and b; the new red value
+      if (act && ok) {
+        if (A.nitems > 1) {
+          const T *par = A.it_par + item_of(bk) * kParStride;
+          s = par[l];
+          centre = par[32 + l];
+          nwc = par[64 + l];
+        }
+        T c0v, c1v, b0, b1, dn0, dn1, up0, up1;
+        ld_pair<T>(tile + o0, c0v, c1v);
+        ld_pair<T>(S.tile2[buf] + o0, b0, b1);
+        ld_pair<T>(tile + o0 - kS, dn0, dn1);
+        ld_pair<T>(tile + o0 + kS, up0, up1);
+        if (copy_u1) st_pair<T>(A.u1 + xo, c0v, c1v);
+        T Lr;  // the red cell's stencil
+        if (cov) {
+          const W5<T> w0 = wrow_w<T>(A.geom, S.wst[buf], x0, y);
+          const W5<T> w1 = wrow_w<T>(A.geom, S.wst[buf], x0 + 1, y);
+          const T Lu0 = sten5<T>(w0, centre, dn0, tile[o0 - 1], c0v, c1v, up0);
+          const T Lu1 = sten5<T>(w1, centre, dn1, c0v, c1v, tile[o0 + 2], up1);
+          b0 = -(ex0 + Lu0 / s);
+          b1 = -(ex1 + Lu1 / s);
+          st_pair<T>(A.b + xo, b0, b1);
+          if (A.bghost) push_pair<T, false>(0u, A.b, bk.x, fc, x0, y, b0, b1);
+          Lr = yodd ? Lu0 : Lu1;
+        } else {
+          const W5<T> wr = wrow_w<T>(A.geom, S.wst[buf], xr, y);
+          Lr = yodd ? sten5<T>(wr, centre, dn0, tile[o0 - 1], c0v, c1v, up0)
+                    : sten5<T>(wr, centre, dn1, c0v, c1v, tile[o0 + 2], up1);
+        }
+        red_new = yodd ? fma(nwc, fma(s, b0, Lr), c0v) : fma(nwc, fma(s, b1, Lr), c1v);
+        cb = yodd ? c1v : c0v;
+        bb = yodd ? b1 : b0;
+      }
+      // red update of the neighbour's edge cell that sits in this block's ghost layer
+      T halo_new = T(0);
+      int halo_o = -1;
+      if (act && ok && hthr) {
+        const HaloCell hc_ = halo_cell(hidx);
+        const int4 fi = fc[hc_.f];
+        if (fi.x == FACE_NEIGHBOR) {
+          auto at = [&](int a, int c) -> T { return (a == hc_.cx && c == hc_.cy) ? hc : tile[a + kS * c]; };
+          const W5<T> wh = wrow_w<T>(A.geom, S.wst[buf], hc_.hx, hc_.hy);
+          T v = wh.zm * at(hc_.hx, hc_.hy - 1);
+          v = v + wh.rm * at(hc_.hx - 1, hc_.hy);
+          v = v + centre * tile[hc_.hx + kS * hc_.hy];
+          v = v + wh.rp * at(hc_.hx + 1, hc_.hy);
+          v = v + wh.zp * at(hc_.hx, hc_.hy + 1);
+          const T bn = (fas && ((fi.z >> hc_.nsub) & 1)) ? -(hv + v / s)
+                       : A.bghost                          ? S.tile2[buf][hc_.hx + kS * hc_.hy]
+                                                           : hv;
+          halo_o = hc_.hx + kS * hc_.hy;
+          halo_new = fma(nwc, fma(s, bn, v), tile[halo_o]);
+        }
+      }
+      if (fas) ok = slot_and(slot, ok);  // every old value is read before the red writes
+      if (act && ok) {
+        tile[xr + kS * y] = red_new;
+        if (halo_o >= 0) tile[halo_o] = halo_new;
+      }
+      if (!slot_and(slot, ok)) {
+        // leave no copy in flight: wait (bounded) for every one issued and not consumed
+        const int issued = min(cn, kBuf + 2 * max(0, i - 1));
+        for (int q = 2 * i; q < issued; ++q)
+          mbar_wait(&S.bar[(pk + q) % kBuf], ((pk + q) / kBuf) & 1, A.err, A.timeout_ns);
         return false;
       }
-      T *tile = S.tile[buf];
-      const int item = item_of(bk);
-      if (A.nitems > 1) {
-        const T *par = A.it_par + item * kParStride;
-        s = par[l];
-        centre = par[32 + l];
-        nwc = par[64 + l];
-      }
-      const W5<T> w = weights<T>(A.wt, A.geom, bk.y, bk.z, x, y);
-      if (copy_u1) A.u1[(int64_t)X * kSS + o] = tile[o];
-      if (fas) {
-        if ((bk.w >> mysub) & 1) {
-          const T Lu = apply5<T>(tile, x, y, w, centre);
-          bx = -(ex + Lu / s);
-          A.b[(int64_t)X * kSS + o] = bx;
-        }
-        slot_sync(slot);
-      }
-      if (red) {
-        const T Lu = apply5<T>(tile, x, y, w, centre);
-        tile[o] = fma(nwc, fma(s, bx, Lu), tile[o]);
-      }
-      if (t < 64 && h.red && fc[h.f].x == FACE_NEIGHBOR) {
-        // red update of the neighbour's edge cell that sits in this block's ghost layer
-        const int4 fi = fc[h.f];
-        auto at = [&](int a, int c) -> T { return (a == h.cx && c == h.cy) ? hc : tile[a + kS * c]; };
-        const W5<T> wh = weights<T>(A.wt, A.geom, bk.y, bk.z, h.hx, h.hy);
-        T v = wh.zm * at(h.hx, h.hy - 1);
-        v = v + wh.rm * at(h.hx - 1, h.hy);
-        v = v + centre * tile[h.hx + kS * h.hy];
-        v = v + wh.rp * at(h.hx + 1, h.hy);
-        v = v + wh.zp * at(h.hx, h.hy + 1);
-        const T bn = (fas && ((fi.z >> h.nsub) & 1)) ? -(hv + v / s) : hv;
-        tile[h.hx + kS * h.hy] = fma(nwc, fma(s, bn, v), tile[h.hx + kS * h.hy]);
-      }
-      slot_sync(slot);
-      if (!red) {
-        const T Lu = apply5<T>(tile, x, y, w, centre);
-        tile[o] = fma(nwc, fma(s, bx, Lu), tile[o]);
-      }
-      slot_sync(slot);
-      const T nu = tile[o];
-      dst[(int64_t)X * kSS + o] = nu;
-      push<T>(A, item, dst, X, fc, x, y, nu);
-      if (t < 128) {
-        const int f = t >> 5, lane = t & 31;
-        if (fc[f].x == FACE_REFBND) {
+      // the buffers of the previous iteration are free: refill them kBuf blocks later
+      if (t == 0 && i >= 1)
+        for (int q = 2 * i - 2 + kBuf; q < 2 * i + kBuf && q < cn; ++q) issue(q);
+      if (act) {
+        T dn0, dn1, up0, up1;
+        ld_pair<T>(tile + o0 - kS, dn0, dn1);
+        ld_pair<T>(tile + o0 + kS, up0, up1);
+        const W5<T> wb = wrow_w<T>(A.geom, S.wst[buf], xbk, y);
+        const T Lb = yodd ? sten5<T>(wb, centre, dn1, red_new, cb, tile[o0 + 2], up1)
+                          : sten5<T>(wb, centre, dn0, tile[o0 - 1], cb, red_new, up0);
+        const T black_new = fma(nwc, fma(s, bb, Lb), cb);
+        const T nu0 = yodd ? red_new : black_new, nu1 = yodd ? black_new : red_new;
+        const int X = bk.x;
+        const unsigned sgb = (unsigned)A.it_sgbits[item_of(bk)];
+        st_pair<T>(dst + xo, nu0, nu1);
+        push_pair<T>(sgb, dst, X, fc, x0, y, nu0, nu1);
+        if (fc[wv].x == FACE_REFBND) {  // warp wv: the 32 ghost cells of face wv
           int gx, gy;
-          ghost_xy(f, lane, gx, gy);
+          ghost_xy(wv, lane, gx, gy);
           dst[(int64_t)X * kSS + gx + kS * gy] = tile[gx + kS * gy];  // frozen during smoothing
         }
+        if (make_e) {
+          T uo0, uo1;
+          ld_pair<T>(A.u1 + xo, uo0, uo1);
+          const T ev0 = nu0 - uo0, ev1 = nu1 - uo1;
+          st_pair<T>(A.e + xo, ev0, ev1);
+          push_pair<T>(sgb, A.e, X, fc, x0, y, ev0, ev1);
+          refbnd_ghost<T>(A.e, esrc, X, fc, h);
+        }
       }
-      if (make_e) {
-        const T ev = nu - A.u1[(int64_t)X * kSS + o];
-        A.e[(int64_t)X * kSS + o] = ev;
-        push<T>(A, item, A.e, X, fc, x, y, ev);
-        if (t < 128) refbnd_ghost<T>(A.e, esrc, X, fc, t);
-      }
-      slot_sync(slot);  // the buffer is refilled three items later
     }
     pk += cn;
+    slot_sync(slot);  // the chunk's records and buffers are no longer read
   }
   return true;
 }
 
-// Residual and restriction of r and u, one fine block (Child edge of level l) per
-// 256-thread slot: the restricted u goes to the coarse block (and into the coarse
+// Residual and restriction of r and u (src/multigrid.jl:60-106 with restrict!,
+// src/restrict.jl:5-25): the restricted u goes to the coarse block (and into the coarse
 // ghosts that copy it), the restricted r to e, where the coarse level's first GS
 // iteration reads it to form the FAS right-hand side.  uf: level l, uc: level l-1.
-// The fine blocks' tiles stream through the slot's triple-buffered bulk-copy pipeline
-// (as in the GS phase) and each block's b is loaded one block ahead, so the residual
-// reads shared memory.  Children of frozen items are skipped.
+// A slot's halves take one child edge each per iteration; each fine block's u and b
+// tiles stream through the slot's kBuf-deep bulk-copy pipeline, thread h of a half
+// forms the residual of its cell pair from shared memory, and after one slot barrier
+// 64 threads of the half restrict (the coarse block's face records are staged with the
+// chunk).  The residual is double-buffered by iteration, so that one barrier per
+// iteration suffices.  Children of frozen items are skipped.
 template <typename T>
 __device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int first, int step, int t, int slot,
                             SlotSmem<T> &S, unsigned &pk) {
@@ -528,79 +748,80 @@ __device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
   const int4 *ch = A.tr.lvl_child[l - 1];
   const int nmine = (first < n) ? (n - 1 - first) / step + 1 : 0;
   if (nmine == 0) return true;
-  const int x = 2 + (t & 15), y = 2 + (t >> 4);
-  const int o = x + kS * y;
-  T *sr = S.red;
-  T b_nx = T(0);
-  auto prefetch = [&](int j) { b_nx = A.b[(int64_t)S.recs[j][0].x * kSS + o]; };
-  for (int c0 = 0; c0 < nmine; c0 += 32) {
-    // the chunk's next 32 child edges, without those of frozen items:
-    // recs[q][0] = {fine, coarse, sb_r, sb_z}, recs[q][1] = info of the fine block
-    if (t < 32) {
-      const int idx = c0 + t;
-      int gi = 0;
-      bool take = false;
-      if (idx < nmine) {
-        gi = first + idx * step;
-        take = A.nitems == 1 || !A.frozen[A.tr.info[ch[gi].x].z >> 8];
-      }
-      const unsigned m = __ballot_sync(0xffffffffu, take);
-      if (take) S.sel[__popc(m & ((1u << t) - 1u))] = gi;
-      if (t == 0) S.cnt = __popc(m);
-    }
+  const int half = t >> 7, h = t & 127;
+  const int x0 = 2 + 2 * (h & 7), y = 2 + (h >> 3);
+  const int o0 = x0 + kS * y;
+  auto issue = [&](int j) {
+    const int4 fi = S.recs[j][1];
+    issue_block<T>(A, S, (pk + j) % kBuf, uf, S.recs[j][0].x, fi.x, fi.y);
+  };
+  for (int c0 = 0; c0 < nmine; c0 += kChunk) {
+    // the chunk's next child edges, without those of frozen items: recs[q][0] = {fine,
+    // coarse, sb_r, sb_z}, recs[q][1] = info of the fine block, recs[q][2..5] = the
+    // coarse block's faces
+    select_chunk<T>(S, t, c0, nmine, first, step,
+                    [&](int gi) { return A.nitems == 1 || !A.frozen[A.tr.info[ch[gi].x].z >> 8]; });
     slot_sync(slot);
     const int cn = S.cnt;
-    if (t < 2 * cn) {
-      const int q = t >> 1;
+    for (int i = t; i < 6 * cn; i += 256) {
+      const int q = i / 6, k = i - 6 * q;
       const int4 e = ch[S.sel[q]];
-      S.recs[q][t & 1] = (t & 1) ? A.tr.info[e.x] : e;
+      S.recs[q][k] = k == 0 ? e : k == 1 ? A.tr.info[e.x] : A.tr.faces[4 * e.y + k - 2];
     }
     slot_sync(slot);
     if (cn == 0) continue;
-    if (t == 0) {
-      issue_tile<T>(S, pk % kBuf, uf, S.recs[0][0].x);
-      if (cn > 1) issue_tile<T>(S, (pk + 1) % kBuf, uf, S.recs[1][0].x);
-    }
-    prefetch(0);
-    for (int j = 0; j < cn; ++j) {
+    if (t == 0)
+      for (int q = 0; q < kBuf && q < cn; ++q) issue(q);
+    for (int i = 0; 2 * i < cn; ++i) {
+      const int j = 2 * i + half;
+      const bool act = j < cn;
       const unsigned kb = pk + j;
       const int buf = kb % kBuf;
-      const int4 e = S.recs[j][0], fi = S.recs[j][1];
-      const int C = e.y;
-      if (t == 0 && j + 2 < cn) issue_tile<T>(S, (kb + 2) % kBuf, uf, S.recs[j + 2][0].x);
-      const T bx = b_nx;
-      if (j + 1 < cn) prefetch(j + 1);
-      if (!mbar_wait(&S.bar[buf], (kb / kBuf) & 1, A.err, A.timeout_ns)) {
-        for (int q = 1; q <= 2 && j + q < cn; ++q)
-          mbar_wait(&S.bar[(kb + q) % kBuf], ((kb + q) / kBuf) & 1, A.err, A.timeout_ns);
+      bool ok = true;
+      if (act) ok = mbar_wait(&S.bar[buf], (kb / kBuf) & 1, A.err, A.timeout_ns);
+      const T *tile = S.tile[buf];
+      const int jj = act ? j : 0;
+      const int4 e = S.recs[jj][0], fi = S.recs[jj][1];
+      const int item = fi.z >> 8;
+      if (act && ok) {
+        const T *par = A.it_par + item * kParStride;
+        const T s = par[l], centre = par[32 + l];
+        const W5<T> w0 = wrow_w<T>(A.geom, S.wst[buf], x0, y);
+        const W5<T> w1 = wrow_w<T>(A.geom, S.wst[buf], x0 + 1, y);
+        T c0v, c1v, b0, b1, dn0, dn1, up0, up1;
+        ld_pair<T>(tile + o0, c0v, c1v);
+        ld_pair<T>(S.tile2[buf] + o0, b0, b1);
+        ld_pair<T>(tile + o0 - kS, dn0, dn1);
+        ld_pair<T>(tile + o0 + kS, up0, up1);
+        const T Lu0 = sten5<T>(w0, centre, dn0, tile[o0 - 1], c0v, c1v, up0);
+        const T Lu1 = sten5<T>(w1, centre, dn1, c0v, c1v, tile[o0 + 2], up1);
+        // the residual replaces the pair's own b values in the b tile (read by no one else)
+        st_pair<T>(S.tile2[buf] + o0, -(b0 + Lu0 / s), -(b1 + Lu1 / s));
+      }
+      if (!slot_and(slot, ok)) {
+        // leave no copy in flight: wait (bounded) for every one issued and not consumed
+        const int issued = min(cn, kBuf + 2 * max(0, i - 1));
+        for (int q = 2 * i; q < issued; ++q)
+          mbar_wait(&S.bar[(pk + q) % kBuf], ((pk + q) / kBuf) & 1, A.err, A.timeout_ns);
         return false;
       }
-      const T *tile = S.tile[buf];
-      const int item = fi.z >> 8;
-      const T *par = A.it_par + item * kParStride;
-      const T s = par[l], centre = par[32 + l];
-      const W5<T> w = weights<T>(A.wt, A.geom, fi.x, fi.y, x, y);
-      const T Lu = apply5<T>(tile, x, y, w, centre);
-      sr[t] = -(bx + Lu / s);
-      slot_sync(slot);
-      if (t < 64) {
-        const int kx = t & 7, ky = t >> 3;
+      // the buffers of the previous iteration are free: refill them kBuf blocks later
+      if (t == 0 && i >= 1)
+        for (int q = 2 * i - 2 + kBuf; q < 2 * i + kBuf && q < cn; ++q) issue(q);
+      if (act && h < 64) {
+        const int kx = h & 7, ky = h >> 3;
+        const int C = e.y;
         const int cx = 2 + 8 * (e.z - 1) + kx, cy = 2 + 8 * (e.w - 1) + ky;
         // 2x2 sums in the reference's order: (i, j), (i+1, j), (i, j+1), (i+1, j+1)
         const T cu = restrict4<T>(tile, 2 + 2 * kx, 2 + 2 * ky);
-        const int i00 = 2 * kx + 16 * 2 * ky;
-        T cr = dadd<T>(T(0), sr[i00]);
-        cr = dadd<T>(cr, sr[i00 + 1]);
-        cr = dadd<T>(cr, sr[i00 + 16]);
-        cr = dadd<T>(cr, sr[i00 + 17]);
-        cr = dmul<T>(cr, T(0.25));
+        const T cr = restrict4<T>(S.tile2[buf], 2 + 2 * kx, 2 + 2 * ky);
         uc[(int64_t)C * kSS + cx + kS * cy] = cu;
-        push<T>(A, item, uc, C, A.tr.faces + 4 * C, cx, cy, cu);
+        push_f<T>((unsigned)A.it_sgbits[item], uc, C, &S.recs[j][2], cx, cy, cu);
         A.e[(int64_t)C * kSS + cx + kS * cy] = cr;
       }
-      slot_sync(slot);  // sr and the tile buffer are reused
     }
     pk += cn;
+    slot_sync(slot);  // the chunk's records and buffers are no longer read
   }
   return true;
 }
@@ -608,9 +829,8 @@ __device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
 // u_fine += P(e_coarse) on every valid cell (in place in uf), pushes of the new edge
 // values, and the fine block's refinement-boundary ghosts from uc (final coarse level).
 // Per child edge the fine block's u tile and its parent's e tile arrive together by
-// two bulk copies on one mbarrier of the slot's triple-buffered pipeline, and the
-// child's face records are staged in shared memory.  Children of frozen items are
-// skipped.
+// two bulk copies on one mbarrier of the slot's kBuf-deep pipeline, and the child's
+// face records are staged in shared memory.  Children of frozen items are skipped.
 template <typename T>
 __device__ bool ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int first, int step, int t, int slot,
                            SlotSmem<T> &S, unsigned &pk) {
@@ -621,45 +841,32 @@ __device__ bool ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int f
   const int dx = t & 15, dy = t >> 4;
   const int x = 2 + dx, y = 2 + dy;
   const int ir = dx & 1, iz = dy & 1;
-  for (int c0 = 0; c0 < nmine; c0 += 32) {
-    // the chunk's next 32 child edges, without those of frozen items:
+  auto issue = [&](unsigned kb, int j) { issue_pair<T>(S, kb % kBuf, uf, S.recs[j][0].x, A.e, S.recs[j][0].y); };
+  for (int c0 = 0; c0 < nmine; c0 += kChunk) {
+    // the chunk's next child edges, without those of frozen items:
     // recs[q][0] = {fine, coarse, sb_r, sb_z}, recs[q][1..4] = the fine block's faces
-    if (t < 32) {
-      const int idx = c0 + t;
-      int gi = 0;
-      bool take = false;
-      if (idx < nmine) {
-        gi = first + idx * step;
-        take = A.nitems == 1 || !A.frozen[A.tr.info[ch[gi].x].z >> 8];
-      }
-      const unsigned m = __ballot_sync(0xffffffffu, take);
-      if (take) S.sel[__popc(m & ((1u << t) - 1u))] = gi;
-      if (t == 0) S.cnt = __popc(m);
-    }
+    select_chunk<T>(S, t, c0, nmine, first, step,
+                    [&](int gi) { return A.nitems == 1 || !A.frozen[A.tr.info[ch[gi].x].z >> 8]; });
     slot_sync(slot);
     const int cn = S.cnt;
-    if (t < 5 * cn) {
-      const int q = t / 5, k = t - 5 * q;
+    for (int i = t; i < 5 * cn; i += 256) {
+      const int q = i / 5, k = i - 5 * q;
       const int4 e = ch[S.sel[q]];
       S.recs[q][k] = k == 0 ? e : A.tr.faces[4 * e.x + k - 1];
     }
     slot_sync(slot);
     if (cn == 0) continue;
-    if (t == 0) {
-      issue_pair<T>(S, pk % kBuf, uf, S.recs[0][0].x, A.e, S.recs[0][0].y);
-      if (cn > 1) issue_pair<T>(S, (pk + 1) % kBuf, uf, S.recs[1][0].x, A.e, S.recs[1][0].y);
-    }
+    if (t == 0)
+      for (int q = 0; q < kBuf - 1 && q < cn; ++q) issue(pk + q, q);
     for (int j = 0; j < cn; ++j) {
       const unsigned kb = pk + j;
       const int buf = kb % kBuf;
       const int4 e = S.recs[j][0];
       const int4 *fc = &S.recs[j][1];
       const int F = e.x;
-      if (t == 0 && j + 2 < cn)
-        issue_pair<T>(S, (kb + 2) % kBuf, uf, S.recs[j + 2][0].x, A.e, S.recs[j + 2][0].y);
+      if (t == 0 && j + kBuf - 1 < cn) issue(kb + kBuf - 1, j + kBuf - 1);
       if (!mbar_wait(&S.bar[buf], (kb / kBuf) & 1, A.err, A.timeout_ns)) {
-        for (int q = 1; q <= 2 && j + q < cn; ++q)
-          mbar_wait(&S.bar[(kb + q) % kBuf], ((kb + q) / kBuf) & 1, A.err, A.timeout_ns);
+        drain_slot<T>(A, S, kb, j, cn);
         return false;
       }
       const T *ut = S.tile[buf], *cb = S.tile2[buf];
@@ -673,11 +880,43 @@ __device__ bool ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int f
       const int item = A.tr.info[F].z >> 8;
       push<T>(A, item, uf, F, fc, x, y, nu);
       if (t < 128) refbnd_ghost<T>(uf, uc, F, fc, t);
-      slot_sync(slot);  // the buffers are refilled three items later
+      slot_sync(slot);  // the buffers are refilled kBuf - 1 items later
     }
     pk += cn;
   }
   return true;
+}
+
+// b's neighbour-copy ghosts: the valid cells next to each face of every block of levels
+// 1..lmax are copied into the facing ghost layer of its same-level neighbour
+// (fill_ghost_copy!, src/connectivity.jl:191-213, applied to b; the outer ghost layer
+// is not needed).  The reference never reads b's ghosts; the engine keeps them so that
+// the GS halo update finds a neighbour's b in the b tile.  One warp per block, lane q
+// moving cell q / 2 of faces 2 (q & 1) and 2 (q & 1) + 1; the warps of a CTA keep
+// their blocks' loads in flight together.
+template <typename T>
+__device__ void ph_bghost(const EngArgs<T> &A, int gwarp, int nwarps) {
+  const int lane = threadIdx.x & 31;
+  const int k = 2 + (lane >> 1);  // position along the face
+  for (int l = 1; l <= A.lmax; ++l) {
+    const int n = A.tr.nblk[l - 1];
+    const int4 *blocks = A.tr.lvl_blocks[l - 1];
+    for (int i = gwarp; i < n; i += nwarps) {
+      const int X = blocks[i].x;
+      const int4 *fc = A.tr.faces + 4 * X;
+      const T *xb = A.b + (int64_t)X * kSS;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int f = 2 * (lane & 1) + h;
+        const int4 fi = fc[f];
+        if (fi.w < 0) continue;
+        // the valid cell next to face f and its place in the neighbour's ghost layer
+        const int x = f == 0 ? 2 : f == 1 ? 17 : k, y = f <= 1 ? k : f == 2 ? 2 : 17;
+        const int gx = f == 0 ? 18 : f == 1 ? 1 : k, gy = f <= 1 ? k : f == 2 ? 18 : 1;
+        A.b[(int64_t)fi.w * kSS + gx + kS * gy] = xb[x + kS * y];
+      }
+    }
+  }
 }
 
 // ---- mixed-precision outer step (FP64) ---------------------------------------------
@@ -779,6 +1018,8 @@ __device__ void ph_blocknorm(const EngArgs<T> &A, bool defect, bool with_b, int 
         bv = A.mx.b64[(int64_t)X * kSS + o];
         r = -(bv + Lu / par[l]);
         A.b[(int64_t)X * kSS + o] = (T)(-r);
+        if (A.bghost && (x <= 3 || x >= 16 || y <= 3 || y >= 16))
+          copy_ghost<T>(A.b, X, A.tr.faces + 4 * X, x, y, (T)(-r));
         T *eb = A.u + (int64_t)X * kSS;
         eb[t] = T(0);
         if (t < kSS - 256) eb[t + 256] = T(0);
@@ -975,7 +1216,11 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
   auto sync = [&](bool ok_in, bool cur_loc, bool next_loc) -> bool {
     bool ok = ok_in;
     if (cur_loc && next_loc) {
-      if (cta0) __syncthreads();
+      if (cta0) {
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        __syncthreads();
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+      }
       if (!ok_in) atomicCAS(A.err, 0, 3);
     } else {
       if (!ok_in) atomicCAS(A.err, 0, 3);
@@ -1092,6 +1337,10 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
   const bool mixed = A.mx.u64 != nullptr;
   const bool loop = A.max_cycles > 0;  // without it: one V-cycle (vcycle!), no norms
   int cycles = 0;
+  if (A.bghost && !mixed) {
+    ph_bghost<T>(A, blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), gridDim.x * (blockDim.x >> 5));
+    if (!sync(true, false, false)) return;
+  }
   if (loop && !mixed && !norm_step(false, true, 0)) return;
   for (int iter = 0;; ++iter) {
     if (loop && mixed) {

@@ -152,7 +152,9 @@ int item_inverse(srmg_ctx *ctx, int item, const ItemSpec &sp, int geom, const do
   }
   DevBuf buf;
   RC(ensure(ctx, buf, A.size() * sizeof(double)));
-  CK(cudaMemcpy(buf.p, A.data(), A.size() * sizeof(double), cudaMemcpyHostToDevice));
+  // on the context's (non-blocking) stream, so that the solves that read it are ordered after it
+  CK(cudaMemcpyAsync(buf.p, A.data(), A.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   ctx->coarse_cache[key] = buf;
   *P = (const double *)buf.p;
   return SRMG_OK;
