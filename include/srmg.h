@@ -139,7 +139,9 @@ typedef struct {
     int mode;            /* SRMG_MODE_* */
     int ndown, ntop, nup;
     double omega;
-    int inner_cycles;    /* mixed: FP32 V-cycles per defect-correction step (>= 1) */
+    int inner_cycles;    /* mixed: at most this many FP32 V-cycles per defect-correction step
+                            (>= 1; default 2); the engine runs one per decade between the
+                            defect norm and the tolerance, up to this cap */
     int warm_start;      /* 0: start from u; 1: learned initial guess (srmg_cnn_*) */
 } srmg_solve_opts;
 

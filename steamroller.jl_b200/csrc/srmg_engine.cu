@@ -150,9 +150,9 @@ int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, const ItemTabs &
     A.chunks = ctx->d_chunks;
     A.nchunk = ctx->nchunk;
     A.it_chunks = ctx->d_it_chunks;
-    RC(ensure(ctx, ctx->istat, sizeof(double) * (4 * (size_t)ctx->nitems + 8)));
+    RC(ensure(ctx, ctx->istat, sizeof(double) * (kItemRec * (size_t)ctx->nitems + 8)));
     A.inorm = (double *)ctx->istat.p;
-    A.out = A.inorm + 4 * ctx->nitems;
+    A.out = A.inorm + kItemRec * ctx->nitems;
   }
   if (run->u64) {
     if (run->max_cycles <= 0) return fail(ctx, SRMG_ERR_BADARG, "mixed engine step needs the device loop");
@@ -162,6 +162,7 @@ int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, const ItemTabs &
     A.mx.it_par64 = tabs.par64;
     A.mx.refbnd_levels = ctx->refbnd_levels;
     A.mx.apply_update = run->apply_update;
+    A.inner = std::max(1, run->inner);
   }
   return engine_launch<T>(ctx, A);
 }

@@ -97,6 +97,7 @@ struct EngArgs {
   long long timeout_ns;
   long long *trace;  // optional: CTA 0 stamps %globaltimer after every phase
   MixedArgs mx;            // mixed-precision outer step (mx.u64 != nullptr)
+  int inner;               // mixed: FP32 V-cycles per defect-correction step (>= 1)
   // Device-side solve loop: with max_cycles > 0 the launch repeats V-cycles until every
   // item's leaf norm of the residual (FP64 mode) or of the FP64 defect (mixed mode) is
   // <= tol * (its leaf norm of b, or 1 if that is 0), or max_cycles V-cycles have run.
@@ -343,16 +344,15 @@ __device__ __forceinline__ void ghost_xy(int f, int lane, int &x, int &y) {
   else { x = 2 + k; y = 18 + g; }
 }
 
-// Refinement-boundary ghost q (0..127) of block X in `dst`, interpolated from `src` on
-// the coarser level (fill_ghost_interp!, src/connectivity.jl:251-258).
+// Refinement-boundary ghost q (0..127) of a block whose face record for face q / 32 is
+// fi: the ghost's position (gx, gy) and its value interpolated from `src` on the
+// coarser level (fill_ghost_interp!, src/connectivity.jl:251-258).  fi must be a
+// FACE_REFBND record.
 template <typename T>
-__device__ __forceinline__ void refbnd_ghost(T *dst, const T *src, int X, const int4 *fc, int q) {
+__device__ __forceinline__ T refbnd_val(const T *src, int4 fi, int q, int &gx, int &gy) {
   const int f = q >> 5, lane = q & 31;
-  const int4 fi = fc[f];
-  if (fi.x != FACE_REFBND) return;
   const int g = lane >> 4, k = lane & 15;
-  int x, y;
-  ghost_xy(f, lane, x, y);
+  ghost_xy(f, lane, gx, gy);
   const T *cb = src + (int64_t)fi.y * kSS;
   const int sbr = fi.z & 0xff, sbz = fi.z >> 8;
   int jr, jz, ir, iz;
@@ -371,7 +371,47 @@ __device__ __forceinline__ void refbnd_ghost(T *dst, const T *src, int X, const 
   T v = dmul<T>(T(0.5), cb[o]);
   v = dadd<T>(v, dmul<T>(T(0.25), cb[o + (2 * ir - 1)]));
   v = dadd<T>(v, dmul<T>(T(0.25), cb[o + kS * (2 * iz - 1)]));
+  return v;
+}
+
+// Refinement-boundary ghost q (0..127) of block X in `dst`, from `src` on the coarser level.
+template <typename T>
+__device__ __forceinline__ void refbnd_ghost(T *dst, const T *src, int X, const int4 *fc, int q) {
+  const int4 fi = fc[q >> 5];
+  if (fi.x != FACE_REFBND) return;
+  int x, y;
+  const T v = refbnd_val<T>(src, fi, q, x, y);
   dst[(int64_t)X * kSS + x + kS * y] = v;
+}
+
+// {type, push target} of face f of a block (a face record's x and w), for pushes from
+// records preloaded in registers.
+__device__ __forceinline__ int2 face_tw(const int4 *fc, int f) {
+  const int4 r = fc[f];
+  return make_int2(r.x, r.w);
+}
+
+// push_f with the records of the x-face (face 0 if x <= 3, 1 if x >= 16) and the y-face
+// (face 2 if y <= 3, 3 if y >= 16) of cell (x, y) given as {type, push target}.
+template <typename F>
+__device__ __forceinline__ void push_tw(unsigned sgb, F *field, int X, int2 fx, int2 fy, int x, int y, F v) {
+  F *xb = field + (int64_t)X * kSS;
+  if (x <= 3) {
+    if (fx.y >= 0) field[(int64_t)fx.y * kSS + (x + kM) + kS * y] = v;
+    else if (fx.x == FACE_BOUNDARY) xb[(2 * kG - 1 - x) + kS * y] = dmul<F>(sign_at<F>(sgb, 3), v);
+  }
+  if (x >= 16) {
+    if (fx.y >= 0) field[(int64_t)fx.y * kSS + (x - kM) + kS * y] = v;
+    else if (fx.x == FACE_BOUNDARY) xb[(2 * (kG + kM) - 1 - x) + kS * y] = dmul<F>(sign_at<F>(sgb, 5), v);
+  }
+  if (y <= 3) {
+    if (fy.y >= 0) field[(int64_t)fy.y * kSS + x + kS * (y + kM)] = v;
+    else if (fy.x == FACE_BOUNDARY) xb[x + kS * (2 * kG - 1 - y)] = dmul<F>(sign_at<F>(sgb, 1), v);
+  }
+  if (y >= 16) {
+    if (fy.y >= 0) field[(int64_t)fy.y * kSS + x + kS * (y - kM)] = v;
+    else if (fy.x == FACE_BOUNDARY) xb[x + kS * (2 * (kG + kM) - 1 - y)] = dmul<F>(sign_at<F>(sgb, 7), v);
+  }
 }
 
 // ------------------------------------------------------------------ phases
@@ -922,56 +962,140 @@ __device__ void ph_bghost(const EngArgs<T> &A, int gwarp, int nwarps) {
 // ---- mixed-precision outer step (FP64) ---------------------------------------------
 
 // u64 += u (FP32 correction) on every valid cell of every level, with pushes of the new
-// values into the copy and mirror ghosts of u64.
+// values into the copy and mirror ghosts of u64.  A slot takes kUpd blocks of a level
+// per pass, their records, values and face records loaded before any store, so that
+// the loads of several blocks are in flight together.
+constexpr int kUpd = 4;
 template <typename T>
 __device__ void ph_update64(const EngArgs<T> &A, int t, int gslot, int gstep) {
   const int x = 2 + (t & 15), y = 2 + (t >> 4), o = x + kS * y;
+  const bool ex = x <= 3 || x >= 16, ey = y <= 3 || y >= 16;
+  const int fxi = x <= 3 ? 0 : 1, fyi = y <= 3 ? 2 : 3;
   int base = 0;
   for (int l = 1; l <= A.lmax; ++l) {
     const int n = A.tr.nblk[l - 1];
     const int4 *blocks = A.tr.lvl_blocks[l - 1];
     // items are numbered across levels so that the work spreads over every slot
-    for (int i = (gslot - base % gstep + gstep) % gstep; i < n; i += gstep) {
-      const int4 bk = blocks[i];
-      if (is_frozen(A, item_of(bk))) continue;
-      const int X = bk.x;
-      double *d = A.mx.u64 + (int64_t)X * kSS + o;
-      const double nv = *d + (double)A.u[(int64_t)X * kSS + o];
-      *d = nv;
-      push_f<double>((unsigned)A.it_sgbits[item_of(bk)], A.mx.u64, X, A.tr.faces + 4 * X, x, y, nv);
+    for (int i = (gslot - base % gstep + gstep) % gstep; i < n; i += kUpd * gstep) {
+      int X[kUpd];
+      unsigned sg[kUpd];
+      bool on[kUpd];
+#pragma unroll
+      for (int k = 0; k < kUpd; ++k) {
+        const int ik = i + k * gstep;
+        on[k] = false;
+        X[k] = 0;
+        sg[k] = 0u;
+        if (ik < n) {
+          const int4 bk = blocks[ik];
+          on[k] = !is_frozen(A, item_of(bk));
+          X[k] = bk.x;
+          if (ex || ey) sg[k] = (unsigned)A.it_sgbits[item_of(bk)];
+        }
+      }
+      double nv[kUpd];
+      int2 fx[kUpd], fy[kUpd];
+#pragma unroll
+      for (int k = 0; k < kUpd; ++k) {
+        nv[k] = 0.0;
+        fx[k] = fy[k] = make_int2(FACE_NONE, -1);
+        if (on[k]) {
+          const int64_t a = (int64_t)X[k] * kSS + o;
+          nv[k] = A.mx.u64[a] + (double)A.u[a];
+          if (ex) fx[k] = face_tw(A.tr.faces + 4 * X[k], fxi);
+          if (ey) fy[k] = face_tw(A.tr.faces + 4 * X[k], fyi);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kUpd; ++k)
+        if (on[k]) {
+          A.mx.u64[(int64_t)X[k] * kSS + o] = nv[k];
+          push_tw<double>(sg[k], A.mx.u64, X[k], fx[k], fy[k], x, y, nv[k]);
+        }
     }
     base += n;
   }
 }
 
 // Restriction of u64 from level l onto the covered subblocks of level l - 1, with pushes.
+// The four 64-thread quarters of a slot take one child edge each, two rounds per pass
+// with every load issued before the stores.
 template <typename T>
 __device__ void ph_restrict64(const EngArgs<T> &A, int l, int t, int gslot, int gstep) {
+  constexpr int R = 2;
   const int n = A.tr.nch[l - 1];
   const int4 *ch = A.tr.lvl_child[l - 1];
-  if (t >= 64) return;
-  const int kx = t & 7, ky = t >> 3;
-  for (int i = gslot; i < n; i += gstep) {
-    const int4 e = ch[i];
-    const int item = A.tr.info[e.y].z >> 8;
-    if (is_frozen(A, item)) continue;
-    const double v = restrict4<double>(A.mx.u64 + (int64_t)e.x * kSS, 2 + 2 * kx, 2 + 2 * ky);
-    const int cx = 2 + 8 * (e.z - 1) + kx, cy = 2 + 8 * (e.w - 1) + ky;
-    A.mx.u64[(int64_t)e.y * kSS + cx + kS * cy] = v;
-    push_f<double>((unsigned)A.it_sgbits[item], A.mx.u64, e.y, A.tr.faces + 4 * e.y, cx, cy, v);
+  const int quarter = t >> 6, c = t & 63, kx = c & 7, ky = c >> 3;
+  for (int i = 4 * gslot + quarter; i < n; i += R * 4 * gstep) {
+    int4 e[R];
+    bool on[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int ik = i + k * 4 * gstep;
+      on[k] = ik < n;
+      e[k] = on[k] ? ch[ik] : make_int4(0, 0, 1, 1);
+    }
+    double v[R];
+    int item[R];
+    int2 fx[R], fy[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      v[k] = 0.0;
+      item[k] = 0;
+      fx[k] = fy[k] = make_int2(FACE_NONE, -1);
+      if (on[k]) {
+        item[k] = A.tr.info[e[k].y].z >> 8;
+        v[k] = restrict4<double>(A.mx.u64 + (int64_t)e[k].x * kSS, 2 + 2 * kx, 2 + 2 * ky);
+        const int cx = 2 + 8 * (e[k].z - 1) + kx, cy = 2 + 8 * (e[k].w - 1) + ky;
+        if (cx <= 3 || cx >= 16) fx[k] = face_tw(A.tr.faces + 4 * e[k].y, cx <= 3 ? 0 : 1);
+        if (cy <= 3 || cy >= 16) fy[k] = face_tw(A.tr.faces + 4 * e[k].y, cy <= 3 ? 2 : 3);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      if (!on[k] || is_frozen(A, item[k])) continue;
+      const int cx = 2 + 8 * (e[k].z - 1) + kx, cy = 2 + 8 * (e[k].w - 1) + ky;
+      A.mx.u64[(int64_t)e[k].y * kSS + cx + kS * cy] = v[k];
+      push_tw<double>((unsigned)A.it_sgbits[item[k]], A.mx.u64, e[k].y, fx[k], fy[k], cx, cy, v[k]);
+    }
   }
 }
 
-// Refinement-boundary ghosts of u64 on level l from level l - 1.
+// Refinement-boundary ghosts of u64 on level l from level l - 1: the two halves of a slot
+// take one block each, two rounds per pass, loads before stores.
 template <typename T>
 __device__ void ph_refbnd64(const EngArgs<T> &A, int l, int t, int gslot, int gstep) {
+  constexpr int R = 2;
   const int n = A.tr.nblk[l - 1];
   const int4 *blocks = A.tr.lvl_blocks[l - 1];
-  if (t >= 128) return;
-  for (int i = gslot; i < n; i += gstep) {
-    const int4 bk = blocks[i];
-    if (is_frozen(A, item_of(bk))) continue;
-    refbnd_ghost<double>(A.mx.u64, A.mx.u64, bk.x, A.tr.faces + 4 * bk.x, t);
+  const int half = t >> 7, q = t & 127;
+  for (int i = 2 * gslot + half; i < n; i += R * 2 * gstep) {
+    int X[R];
+    int4 fi[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int ik = i + k * 2 * gstep;
+      X[k] = -1;
+      fi[k] = make_int4(FACE_NONE, 0, 0, -1);
+      if (ik < n) {
+        const int4 bk = blocks[ik];
+        if (!is_frozen(A, item_of(bk))) {
+          X[k] = bk.x;
+          fi[k] = A.tr.faces[4 * bk.x + (q >> 5)];
+        }
+      }
+    }
+    double v[R];
+    int gx[R], gy[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      v[k] = 0.0;
+      gx[k] = gy[k] = 0;
+      if (X[k] >= 0 && fi[k].x == FACE_REFBND) v[k] = refbnd_val<double>(A.mx.u64, fi[k], q, gx[k], gy[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k)
+      if (X[k] >= 0 && fi[k].x == FACE_REFBND) A.mx.u64[(int64_t)X[k] * kSS + gx[k] + kS * gy[k]] = v[k];
   }
 }
 
@@ -998,25 +1122,42 @@ __device__ void ph_blocknorm(const EngArgs<T> &A, bool defect, bool with_b, int 
     const int l = ck.x;
     const int4 *blocks = A.tr.lvl_blocks[l - 1] + ck.y;
     const double wl = 1.0 / (double)((int64_t)1 << (2 * (l - 1)));
-    double v = 0.0, vb = 0.0;
-    for (int j = 0; j < ck.z; ++j) {
-      const int4 bk = blocks[j];
+    // the chunk's blocks: records first, then every block's residual (loads of all blocks
+    // in flight together: no store in between), then the stores and the sums in order
+    int4 bks[kNormChunk];
+#pragma unroll
+    for (int j = 0; j < kNormChunk; ++j) bks[j] = j < ck.z ? blocks[j] : make_int4(0, 0, 0, 0);
+    double rr[kNormChunk], bvv[kNormChunk];
+#pragma unroll
+    for (int j = 0; j < kNormChunk; ++j) {
+      rr[j] = 0.0;
+      bvv[j] = 0.0;
+      if (j >= ck.z) continue;
+      const int4 bk = bks[j];
       const int X = bk.x;
-      const bool leaf = !((bk.w >> mysub) & 1);
-      double r, bv;
       if (!defect) {
         const T *par = A.it_par + item * kParStride;
         const W5<T> w = weights<T>(A.wt, A.geom, bk.y, bk.z, x, y);
         const T Lu = apply5<T>(A.u + (int64_t)X * kSS, x, y, w, par[32 + l]);
         const T bb = A.b[(int64_t)X * kSS + o];
-        r = (double)(-(bb + Lu / par[l]));
-        bv = (double)bb;
+        rr[j] = (double)(-(bb + Lu / par[l]));
+        bvv[j] = (double)bb;
       } else {
         const double *par = A.mx.it_par64 + item * kParStride;
         const W5<double> w = weights<double>(A.mx.wt64, A.geom, bk.y, bk.z, x, y);
         const double Lu = apply5<double>(A.mx.u64 + (int64_t)X * kSS, x, y, w, par[32 + l]);
-        bv = A.mx.b64[(int64_t)X * kSS + o];
-        r = -(bv + Lu / par[l]);
+        bvv[j] = A.mx.b64[(int64_t)X * kSS + o];
+        rr[j] = -(bvv[j] + Lu / par[l]);
+      }
+    }
+    double v = 0.0, vb = 0.0;
+#pragma unroll
+    for (int j = 0; j < kNormChunk; ++j) {
+      if (j >= ck.z) continue;
+      const int4 bk = bks[j];
+      const int X = bk.x;
+      const double r = rr[j], bv = bvv[j];
+      if (defect) {
         A.b[(int64_t)X * kSS + o] = (T)(-r);
         if (A.bghost && (x <= 3 || x >= 16 || y <= 3 || y >= 16))
           copy_ghost<T>(A.b, X, A.tr.faces + 4 * X, x, y, (T)(-r));
@@ -1024,7 +1165,7 @@ __device__ void ph_blocknorm(const EngArgs<T> &A, bool defect, bool with_b, int 
         eb[t] = T(0);
         if (t < kSS - 256) eb[t + 256] = T(0);
       }
-      if (leaf) {
+      if (!((bk.w >> mysub) & 1)) {  // a leaf cell
         v = fma(r, r, v);
         vb = fma(bv, bv, vb);
       }
@@ -1060,7 +1201,7 @@ __device__ void ph_blocknorm(const EngArgs<T> &A, bool defect, bool with_b, int 
 // initial-norm entries), the item's V-cycle count, and freezes the item once its norm
 // is <= tol * |b| (|b| = 0 counts as 1) or not finite.  Items frozen before are skipped.
 template <typename T>
-__device__ void ph_itemnorm(const EngArgs<T> &A, bool first, int cycles, double *red) {
+__device__ void ph_itemnorm(const EngArgs<T> &A, bool first, int cycles, int steps, double *red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int k = blockIdx.x; k < A.nitems; k += gridDim.x) {
     if (A.frozen[k]) continue;
@@ -1086,13 +1227,16 @@ __device__ void ph_itemnorm(const EngArgs<T> &A, bool first, int cycles, double 
         sb += red[32 + q];
       }
       const double nrm = sqrt(sv);
-      double *io = A.inorm + 4 * k;
+      double *io = A.inorm + kItemRec * k;
       if (first) {
         io[1] = sqrt(sb);
         io[2] = nrm;
       }
       io[0] = nrm;
-      io[3] = (double)cycles;
+      // V-cycles run: the launch's count (FP64); in mixed mode the step bookkeeping
+      // counts them per item (items may run fewer V-cycles in a step than others)
+      if (first || A.mx.u64 == nullptr) io[3] = (double)cycles;
+      io[4] = (double)steps;
       const double bn = io[1] > 0.0 ? io[1] : 1.0;
       if (!(nrm > A.tol * bn) || !isfinite(nrm)) A.frozen[k] = 1;
     }
@@ -1252,10 +1396,11 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
 
   const int gslot = blockIdx.x * nslots + slot, gstep = gridDim.x * nslots;
   // Norm step: per-block partials, barrier, per-item sums and freezing, barrier.
+  int steps = 0;  // mixed: defect-correction steps run
   auto norm_step = [&](bool defect, bool first, int ncyc) -> bool {
     ph_blocknorm<T>(A, defect, first, t, slot, gslot, gstep, reinterpret_cast<double *>(&S.tile[0][0]));
     if (!sync(true, false, false)) return false;
-    ph_itemnorm<T>(A, first, ncyc, s_direct);
+    ph_itemnorm<T>(A, first, ncyc, steps, s_direct);
     return sync(true, false, false);
   };
   __shared__ int s_live;
@@ -1267,6 +1412,46 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
     }
     __syncthreads();
     return s_live != 0;
+  };
+  // Mixed: V-cycles of a defect-correction step, up to A.inner.  An item runs one per
+  // decade of its norm / (tol |b|) (a contraction of 0.1 per cycle), so a nearly
+  // converged solve runs no extra cycle; the step runs as many as the item furthest from
+  // its tolerance needs, and an item that has run its share is paused (frozen = 2) for
+  // the rest of the step.  An item's V-cycles are therefore those of its solo solve.
+  auto want_cycles = [&](int i) -> int {
+    const volatile double *io = A.inorm + kItemRec * i;
+    const double bn = io[1] > 0.0 ? io[1] : 1.0;
+    const double rho = io[0] / (A.tol * bn);
+    int k = 1;
+    for (double th = 10.0; k < A.inner && rho > th; th *= 10.0) ++k;
+    return k;
+  };
+  __shared__ int s_inner;
+  auto inner_now = [&]() -> int {
+    if (threadIdx.x == 0) {
+      int kmax = 1;
+      for (int i = 0; i < A.nitems; ++i)
+        if (*((volatile int *)A.frozen + i) == 0) kmax = max(kmax, want_cycles(i));
+      s_inner = min(kmax, max(1, A.inner));
+    }
+    __syncthreads();
+    return s_inner;
+  };
+  // After V-cycle k (0-based) of a step of nv: count it for every item that ran it, then
+  // pause the items whose share is done, or, after the last one, resume them (CTA 0; the
+  // caller's grid barrier publishes the flags).
+  auto step_books = [&](int k, int nv) {
+    if (!(cta0 && threadIdx.x == 0)) return;
+    for (int i = 0; i < A.nitems; ++i) {
+      volatile int *fz = (volatile int *)A.frozen + i;
+      volatile double *io = A.inorm + kItemRec * i;
+      if (*fz == 0) io[3] = io[3] + 1.0;
+      if (k + 1 < nv) {
+        if (*fz == 0 && want_cycles(i) <= k + 1) *fz = 2;
+      } else if (*fz == 2) {
+        *fz = 0;
+      }
+    }
   };
 
   // One FAS V-cycle (src/multigrid.jl:60-106) on the current fields.
@@ -1361,8 +1546,17 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
       if (!norm_step(true, iter == 0, cycles)) return;
     }
     if (loop && (!any_live() || cycles >= A.max_cycles)) break;
-    if (!vcycle_body()) return;
-    cycles++;
+    // mixed: up to A.inner FP32 V-cycles on the same defect, the correction carried over
+    const int nv = (mixed && loop) ? inner_now() : 1;
+    for (int k = 0; k < nv; ++k) {
+      if (!vcycle_body()) return;
+      cycles++;
+      if (mixed && loop) {
+        step_books(k, nv);
+        if (!sync(true, false, false)) return;
+      }
+    }
+    if (mixed) steps++;
     if (!loop) break;
     if (!mixed && !norm_step(false, false, cycles)) return;
   }

@@ -67,6 +67,7 @@ struct EngineRun {
   double *u64 = nullptr;             // mixed precision: FP64 iterate and right-hand side
   const double *b64 = nullptr;
   int apply_update = 0;
+  int inner = 1;                     // mixed: FP32 V-cycles per defect-correction step
   int max_cycles = 0;                // > 0: device-side loop until every item has converged
   double tol = 0.0;                  // relative to each item's leaf norm of b
 };
@@ -77,7 +78,8 @@ int engine_check(srmg_ctx *ctx);
 template <typename T>
 int engine_smooth(srmg_ctx *ctx, T *u, const T *b, const ItemTabs &tabs, int geom, int level, int n);
 // Copy the per-item results of the last device loop ({norm, |b|, initial, cycles} per
-// item, then the launch's V-cycle count) to ctx->h_items and check the error word.
+// item, kItemRec values each, then the launch's V-cycle count) to ctx->h_items and
+// check the error word.
 int read_items(srmg_ctx *ctx);
 int items_host_reserve(srmg_ctx *ctx);  // the pinned mirror (read_items calls it)
 int items_d2h(srmg_ctx *ctx);           // the copy alone, stream-ordered

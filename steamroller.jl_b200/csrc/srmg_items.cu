@@ -226,7 +226,7 @@ int srmg::prepare_items(srmg_ctx *ctx, const ItemSpec *specs, int geom, double o
 }
 
 int srmg::items_host_reserve(srmg_ctx *ctx) {
-  const size_t n = 4 * (size_t)ctx->nitems + 8;
+  const size_t n = kItemRec * (size_t)ctx->nitems + 8;
   if (ctx->h_items_n >= n) return SRMG_OK;
   if (ctx->h_items) cudaFreeHost(ctx->h_items);
   ctx->h_items = nullptr;
@@ -238,7 +238,7 @@ int srmg::items_host_reserve(srmg_ctx *ctx) {
 }
 
 int srmg::items_d2h(srmg_ctx *ctx) {
-  const size_t n = 4 * (size_t)ctx->nitems + 8;
+  const size_t n = kItemRec * (size_t)ctx->nitems + 8;
   CK(cudaMemcpyAsync(ctx->h_items, ctx->istat.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   return SRMG_OK;
 }

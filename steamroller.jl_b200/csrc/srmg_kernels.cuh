@@ -25,6 +25,9 @@ constexpr int kParStride = 96;
 // Blocks per norm chunk: the leaf norms are summed per chunk of up to this many
 // consecutive blocks of one item and level, then per item over its chunks.
 constexpr int kNormChunk = 4;
+// Per-item result record of a device solve loop: {norm, |b|, initial norm, V-cycles run,
+// defect-correction steps run (mixed mode; 0 in FP64 mode)}.
+constexpr int kItemRec = 5;
 
 // Face numbering (the four StarStencil directions): 0 = -r, 1 = +r, 2 = -z, 3 = +z.
 enum FaceType : int { FACE_NONE = 0, FACE_NEIGHBOR = 1, FACE_BOUNDARY = 2, FACE_REFBND = 3 };

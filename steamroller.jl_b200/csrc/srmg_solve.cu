@@ -197,18 +197,19 @@ extern "C" void srmg_solve_opts_default(srmg_solve_opts *o) {
   o->ntop = 4;
   o->nup = 2;
   o->omega = 1.0;
-  o->inner_cycles = 1;
+  o->inner_cycles = 2;
   o->warm_start = 0;
 }
 
 // Per-item statistics from the device loop's results (read_items).
 static void item_stats(srmg_ctx *ctx, int k, srmg_stats *st) {
-  const double *io = ctx->h_items + 4 * k;
+  const double *io = ctx->h_items + kItemRec * k;
   const double bn = io[1] > 0 ? io[1] : 1.0;
   st->bnorm = io[1];
   st->rel_residual = io[0] / bn;
   st->initial_rel = io[2] / bn;
   st->cycles = (int)io[3];
+  st->outer = (int)io[4];
   st->status = std::isfinite(st->rel_residual) ? SRMG_OK : SRMG_ERR_DIVERGED;
 }
 
@@ -252,13 +253,15 @@ int srmg::solve_enqueue(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_
   run.direct = true;
   run.u64 = u;
   run.b64 = b;
+  run.inner = std::max(1, o->inner_cycles);
+  // max_cycles caps defect-correction steps in mixed mode; the device loop counts V-cycles
+  run.max_cycles = (int)std::min<int64_t>((int64_t)run.max_cycles * run.inner, 1 << 30);
   return engine_vcycle<float>(ctx, e, be, u1, r, tabs, geom, 0, o->ndown, o->ntop, o->nup, &run);
 }
 
 void srmg::items_stats(srmg_ctx *ctx, const srmg_solve_opts *o, srmg_stats *st) {
   for (int k = 0; k < ctx->nitems; k++) {
     item_stats(ctx, k, &st[k]);
-    if (o->mode == SRMG_MODE_MIXED) st[k].outer = st[k].cycles;
   }
 }
 

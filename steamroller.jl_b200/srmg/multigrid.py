@@ -308,7 +308,7 @@ def fill_ghost_(ctx: Context, u, l, bc, mask=7):
 
 
 def solve(ctx: Context, u, b, s, geometry, bc, lpldisc=None, tol=1e-8, mode=MODE_FP64,
-          max_cycles=1000, ndown=2, ntop=4, nup=2, omega=1.0, inner_cycles=1, warm_start=0):
+          max_cycles=1000, ndown=2, ntop=4, nup=2, omega=1.0, inner_cycles=2, warm_start=0):
     """Solve L u + s b = 0 to resnorm(u)/leafnorm(b) <= tol; returns the stats dict."""
     op, k2 = _disc(lpldisc)
     bca = _bc(bc)
@@ -348,7 +348,7 @@ class Batch(Context):
         self.total_blocks = sum(self.nblks)
 
     def solve(self, us, bs, tol=1e-8, mode=MODE_FP64, max_cycles=1000, ndown=2, ntop=4, nup=2,
-              omega=1.0, inner_cycles=1, warm_start=0):
+              omega=1.0, inner_cycles=2, warm_start=0):
         """Solve every item; ``us``/``bs`` are per-item fields (numpy arrays: host entry
         point; torch tensors: device entry point).  Returns one stats dict per item."""
         assert len(us) == self.nitems and len(bs) == self.nitems
@@ -363,7 +363,7 @@ class Batch(Context):
         return [x.as_dict() for x in st]
 
     def solve_forest(self, u, b, tol=1e-8, mode=MODE_FP64, max_cycles=1000, ndown=2, ntop=4, nup=2,
-                     omega=1.0, inner_cycles=1, warm_start=0):
+                     omega=1.0, inner_cycles=2, warm_start=0):
         """Solve every item on device fields in the forest layout (no copies)."""
         o = SolveOpts(tol, max_cycles, mode, ndown, ntop, nup, omega, inner_cycles, warm_start)
         st = (Stats * self.nitems)()
