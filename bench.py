@@ -188,13 +188,17 @@ def main():
     ap.add_argument("--learned-pairs", type=int, default=20000, help="solve pairs generated for training")
     ap.add_argument("--no-config5", action="store_true", help="skip the full-size timestep (config-5) section")
     ap.add_argument("--config5-steps", type=int, default=200)
-    ap.add_argument("--only", default=None, choices=[None, "vcycle", "smooth"],
+    ap.add_argument("--only", default=None, choices=[None, "vcycle", "smooth", "cnn"],
                     help="vcycle: time plain FP64 V-cycles only; smooth: GS iterations on the finest "
-                         "level only (profiling runs)")
+                         "level only; cnn: the warm-start network's inference forward, mma.sync and "
+                         "tcgen05 (profiling runs)")
+    ap.add_argument("--samples", type=int, default=4096, help="--only cnn: block samples per forward")
     ap.add_argument("--config", default="config2", choices=["config1", "config2", "config5"])
     args = ap.parse_args()
     if args.only in ("vcycle", "smooth"):
         return vcycle_only(args)
+    if args.only == "cnn":
+        return cnn_only(args)
 
     from srmg import gen, model
     from srmg.tree import leaf_cells
@@ -527,6 +531,35 @@ def vcycle_only(args):
     print(json.dumps({"only": "vcycle", "config": args.config, "blocks": problem.tree.nblocks(),
                       "ms_per_vcycle": ms, "model_bytes": B, "model_GBps": B / (ms / 1e3) / 1e9}))
     ctx.close()
+
+
+def cnn_only(args):
+    """The warm-start network's inference forward on --samples random BF16 block samples:
+    W untimed calls, then K timed calls of each forward (mma.sync, tcgen05) with CUDA
+    events on the network's stream; prints one JSON line.  Used for ncu captures."""
+    import torch
+    from srmg import multigrid as mg
+    net = mg.Cnn(0, seed=7)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(SEED)
+    x = torch.randn((args.samples, 400, 2), generator=g, device="cuda").to(torch.bfloat16)
+    torch.cuda.synchronize()
+    out = {"only": "cnn", "samples": args.samples, "params": net.nparams,
+           "macs_per_sample": 2 * 9 * 32 * 400 + 4 * 9 * 32 * 32 * 400 + 9 * 32 * 400}
+    for name, fwd in (("mma_sync", net.forward), ("tcgen05", net.forward_tc)):
+        for _ in range(args.warmup):
+            fwd(x)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            y = fwd(x)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) / max(1, args.steps) * 1e3
+        # each call synchronises the network's stream, so the wall clock brackets the
+        # device work plus one launch and synchronisation
+        out[name] = {"ms_per_forward": ms, "tflops": 2 * out["macs_per_sample"] * args.samples / (ms / 1e3) / 1e12,
+                     "finite": bool(torch.isfinite(y).all()), "timing": "wall clock around synchronous calls"}
+    print(json.dumps(out))
 
 
 def fp64_cycle_count_estimate(problem):

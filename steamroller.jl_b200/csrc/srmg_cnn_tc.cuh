@@ -19,11 +19,12 @@
 // wait is bounded; on a timeout the kernel sets *err, frees its TMEM and returns.
 //
 // Measured against the mma.sync forward (k_cnn_fwd) on one B200 it is correct to the
-// same tolerance but slower (~140 vs ~190 TFLOP/s of useful MACs at 4096+ samples): with
-// N = 32 output channels an M=128 x N=32 x K=16 MMA reads ~5 KB of operands from shared
-// memory for 65k MACs, so the layer is operand-bandwidth bound, while the mma.sync
-// kernel reuses each A fragment across its 4 N-tiles in registers.  It is therefore an
-// opt-in path (srmg_cnn_use_tcgen05).
+// same tolerance but slower (0.92 vs 0.70 ms per 4096 samples).  It is latency-bound:
+// one sample per CTA is in flight, and per layer the MMAs, their commit and wait, and
+// the TMEM epilogue that writes the next layer's operands run one after another (tensor
+// pipe 9.6% active, 8 warps, long-scoreboard stalls leading).  Overlapping two samples
+// or two layers needs a second set of operand copies, which the 219 KB of copies and
+// weights leave no room for.  It is therefore an opt-in path (srmg_cnn_use_tcgen05).
 
 constexpr int kTcW = 24;                     // padded row length (a multiple of 8)
 constexpr int kTcRows = 560;                 // rows per shifted copy: 512 + 2 * 24
