@@ -369,7 +369,7 @@ int srmg_streamer_step_dev(srmg_ctx *ctx, double *ne, double *npos, double *nneg
  *   "engine"           1 = persistent one-launch V-cycle (default), 0 = one kernel per
  *                      reference operation;
  *   "local_max_blocks" coarse levels whose every coarser level has at most this many
- *                      blocks run inside one CTA of the persistent kernel (default 16);
+ *                      blocks run inside one CTA of the persistent kernel (default 4);
  *   "engine_ctas"      CTAs of the persistent kernel (0 = one per SM);
  *   "trace"            1 = record a %globaltimer stamp (ns) after every phase of the
  *                      persistent kernel, read back with srmg_get_trace;

@@ -81,7 +81,8 @@ struct srmg_ctx {
   srmg::DevBuf sync;         // {barrier counter, error word}
   int num_sms = 0;
   int engine_ctas = 0;       // cooperative grid size (0 = not yet known)
-  int local_max_blocks = 16; // levels whose every coarser level has <= this many blocks run in CTA 0
+  int local_max_blocks = 4;  // levels whose every coarser level has <= this many blocks run in CTA 0
+                             // (4 measured fastest on the 1.5M- and 10M-leaf trees)
   bool use_engine = true;
   unsigned refbnd_levels = 0;  // bit l: level l has refinement-boundary faces
   bool trace_on = false;

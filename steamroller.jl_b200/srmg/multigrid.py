@@ -373,13 +373,13 @@ class Batch(Context):
 
 
 def autotune(ctx: Context, u, b, s, geometry, bc, lpldisc=None, tol=1e-8, mode=MODE_MIXED,
-             max_cycles=1000, ndown=2, ntop=4, nup=2, omega=1.0):
+             max_cycles=1000, ndown=2, ntop=4, nup=2, omega=1.0, inner_cycles=2):
     """Autotune launch shape and sweep counts on this problem (device fields); returns
     (chosen options dict, list of trial dicts).  The chosen launch options stay set on
     the context."""
     op, k2 = _disc(lpldisc)
     bca = _bc(bc)
-    o = SolveOpts(tol, max_cycles, mode, ndown, ntop, nup, omega, 1, 0)
+    o = SolveOpts(tol, max_cycles, mode, ndown, ntop, nup, omega, inner_cycles, 0)
     tr = (TuneTrial * 64)()
     _order_after_torch(ctx, u, b)
     n = lib().srmg_autotune(ctx.handle, _ptr(u), _ptr(b), u.shape[0], s, op, k2, geometry, bca.ctypes.data,
@@ -391,9 +391,9 @@ def autotune(ctx: Context, u, b, s, geometry, bc, lpldisc=None, tol=1e-8, mode=M
 
 
 def batch_autotune(batch: "Batch", us, bs, tol=1e-8, mode=MODE_MIXED, max_cycles=1000, ndown=2, ntop=4,
-                   nup=2, omega=1.0):
+                   nup=2, omega=1.0, inner_cycles=2):
     """Autotune a batch on its items' device fields; returns (options, trials)."""
-    o = SolveOpts(tol, max_cycles, mode, ndown, ntop, nup, omega, 1, 0)
+    o = SolveOpts(tol, max_cycles, mode, ndown, ntop, nup, omega, inner_cycles, 0)
     tr = (TuneTrial * 64)()
     up = (_P * batch.nitems)(*[_ptr(x) for x in us])
     bp = (_P * batch.nitems)(*[_ptr(x) for x in bs])

@@ -157,7 +157,7 @@ def test_autotune_single_and_batch(setup):
     st = mg.solve(c, ug, bg, p.s, p.geom, p.bc, disc(p), tol=1e-8, mode=mg.MODE_MIXED,
                   ndown=chosen["ndown"], nup=chosen["nup"], ntop=chosen["ntop"])
     assert st["rel_residual"] <= 1e-8
-    c.set_option("engine_ctas", 0).set_option("local_max_blocks", 16)
+    c.set_option("engine_ctas", 0).set_option("local_max_blocks", 4)
     us = [torch_cuda(np.zeros_like(q.b)) for _, q in items]
     bs = [torch_cuda(q.b) for _, q in items]
     chosen, trials = mg.batch_autotune(batch, us, bs, tol=1e-8, mode=mg.MODE_MIXED)
@@ -165,4 +165,4 @@ def test_autotune_single_and_batch(setup):
     sts = batch.solve(us, bs, mode=mg.MODE_MIXED, tol=1e-8, ndown=chosen["ndown"], nup=chosen["nup"],
                       ntop=chosen["ntop"], max_cycles=400)
     assert all(s["rel_residual"] <= 1e-8 for s in sts)
-    batch.set_option("engine_ctas", 0).set_option("local_max_blocks", 16)
+    batch.set_option("engine_ctas", 0).set_option("local_max_blocks", 4)
