@@ -204,6 +204,30 @@ int srmg_residual_postrestrict_level_dev(srmg_ctx *ctx, double *b, const double 
                                          const double *r, int64_t nblk_alloc, int level,
                                          double s, int op, double k2, int geom);
 
+/* ---- stage preparation and post-processing on the device --------------------------
+ * The work around the field solve inside derivs! (src/streamer.jl:309-351), so that a
+ * time step can keep u, q and n on the device. */
+/* netcharge!(tree, q, n, chem) (src/streamer.jl:369-373) for the NetIonization
+ * chemistry (src/chemistry.jl:80: charges -1 for electrons, +1 for ions): q = -ne + nion
+ * on every valid cell of every block.  For order-2 discretisations rhs_level!
+ * (src/multigrid.jl:363-388) is the identity, so q is the solve's right-hand side. */
+int srmg_netcharge(srmg_ctx *ctx, double *q, const double *ne, const double *nion, int64_t nblk_alloc);
+int srmg_netcharge_dev(srmg_ctx *ctx, double *q, const double *ne, const double *nion, int64_t nblk_alloc);
+/* restrict_full!(u, conn) (src/restrict.jl:43-47): restrict_level! for levels L..2. */
+int srmg_restrict_full_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc);
+/* electric_field!(tree, e, eabs, u, h, t, e0) (src/multigrid.jl:421-449, the method for
+ * a constant background field e0 = (e0_r, e0_z), :451).  e is a VectorBlockField{2,16,2}:
+ * 21 x 21 x 2 doubles per block (component d at offset 441 d); for d = r, z and every
+ * face I of validindices(e, d) (src/blockfield.jl:403-405), e[I, d] = (u[I - e_d] -
+ * u[I]) / h_l + e0[d] with h_l = h / 2^(l-1); eabs (20 x 20 per block) at every valid
+ * cell = sqrt(sum_d (e[I, d] + e[I + e_d, d])^2 / 4).  u's ghosts must be filled.
+ * Bit-exact against the reference's arithmetic (IEEE division and square root, no
+ * fused multiply-add). */
+int srmg_electric_field(srmg_ctx *ctx, double *e, double *eabs, const double *u, int64_t nblk_alloc,
+                        double h, const double e0[2]);
+int srmg_electric_field_dev(srmg_ctx *ctx, double *e, double *eabs, const double *u, int64_t nblk_alloc,
+                            double h, const double e0[2]);
+
 /* Allocation-free residual norm.  No counterpart in the reference: it exists for
  * callers that cannot call cudaMalloc when they need the norm -- code inside CUDA
  * stream capture, hosts whose device memory belongs to their own pool allocator, or

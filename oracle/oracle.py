@@ -68,6 +68,8 @@ def lib():
             "orc_resnorm": (D, [PP, PP, PP, D, TP, OP]),
             "orc_leafnorm": (D, [PP, PP, TP]),
             "orc_solve": (I, [PP, PP, PP, PP, D, TP, OP, I, I, I, D, D, I, ctypes.POINTER(D)]),
+            "orc_netcharge": (None, [PP, PP, PP, TP]),
+            "orc_electric_field": (None, [PP, PP, PP, D, PP, TP]),
             "orc_set_threads": (None, [I]),
             "orc_get_threads": (I, []),
         }

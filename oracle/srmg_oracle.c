@@ -497,3 +497,62 @@ int orc_solve(double *u, double *b, double *r, double *u1, double s, const orc_t
     if (rel) *rel = x;
     return c;
 }
+
+/* ---- stage preparation and post-processing --------------------------------------- */
+
+/* netcharge! (src/streamer.jl:369-373): q[I] = dot(n[I], species_charge) over the valid
+ * cells of every block; NetIonization charges are (-1, +1) (src/chemistry.jl:80), so
+ * q = (n_e * -1) + (n_ion * 1), the products exact. */
+void orc_netcharge(double *q, const double *ne, const double *nion, const orc_tree *t) {
+    const int M = t->M, G = t->G, S = M + 2 * G;
+    for (int l = 1; l <= t->nlev; l++) {
+        const orc_pair *p = t->pairs[l - 1];
+        const int64_t n = t->npairs[l - 1];
+#pragma omp parallel for schedule(static)
+        for (int64_t k = 0; k < n; k++)
+            for (int j = G + 1; j <= G + M; j++)
+                for (int i = G + 1; i <= G + M; i++) {
+                    const int64_t o = IX(S, i, j, p[k].blk);
+                    q[o] = ne[o] * -1.0 + nion[o] * 1.0;
+                }
+    }
+}
+
+/* electric_field! (src/multigrid.jl:421-449) with a constant field e0 (the SVector
+ * method, :451).  e is a VectorBlockField (src/blockfield.jl:84-95): (S+1)^2 x 2 values
+ * per block, component d at offset d (S+1)^2.  h_l = h / (1 << (level - 1)).  For
+ * d = 1, 2 and I in validindices(e, d) (src/blockfield.jl:403-405: G+1..G+M+1 along d,
+ * G+1..G+M across): e[I, d] = (u[I - e_d] - u[I]) / h_l + e0[d].  Then for the valid
+ * cells: f2 = 0; f2 += (e[I, d] + e[I + e_d, d])^2 / 4 for d = 1, 2; eabs = sqrt(f2). */
+void orc_electric_field(double *e, double *eabs, const double *u, double h, const double e0[2],
+                        const orc_tree *t) {
+    const int M = t->M, G = t->G, S = M + 2 * G, SV = S + 1;
+    for (int l = 1; l <= t->nlev; l++) {
+        const orc_pair *p = t->pairs[l - 1];
+        const int64_t n = t->npairs[l - 1];
+        const double hl = h / (double)((int64_t)1 << (l - 1));
+#pragma omp parallel for schedule(static)
+        for (int64_t k = 0; k < n; k++) {
+            const int64_t blk = p[k].blk;
+            double *eb = e + (int64_t)2 * SV * SV * (blk - 1);
+            for (int d = 0; d < 2; d++)
+                for (int j = G + 1; j <= G + M + (d == 1); j++)
+                    for (int i = G + 1; i <= G + M + (d == 0); i++) {
+                        const int i1 = d == 0 ? i - 1 : i, j1 = d == 1 ? j - 1 : j;
+                        eb[(i - 1) + SV * (j - 1) + SV * SV * d] =
+                            (u[IX(S, i1, j1, blk)] - u[IX(S, i, j, blk)]) / hl + e0[d];
+                    }
+            for (int j = G + 1; j <= G + M; j++)
+                for (int i = G + 1; i <= G + M; i++) {
+                    double f2 = 0.0;
+                    for (int d = 0; d < 2; d++) {
+                        const int ip = d == 0 ? i + 1 : i, jp = d == 1 ? j + 1 : j;
+                        const double sum = eb[(i - 1) + SV * (j - 1) + SV * SV * d] +
+                                           eb[(ip - 1) + SV * (jp - 1) + SV * SV * d];
+                        f2 += sum * sum / 4;
+                    }
+                    eabs[IX(S, i, j, blk)] = sqrt(f2);
+                }
+        }
+    }
+}

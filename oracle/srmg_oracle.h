@@ -90,6 +90,11 @@ int orc_solve(double *u, double *b, double *r, double *u1, double s, const orc_t
               const orc_operator *op, int ndown, int ntop, int nup, double omega,
               double tol, int max_cycles, double *rel);
 
+/* Stage preparation and post-processing of derivs! (src/streamer.jl:309-351). */
+void orc_netcharge(double *q, const double *ne, const double *nion, const orc_tree *t);
+void orc_electric_field(double *e, double *eabs, const double *u, double h, const double e0[2],
+                        const orc_tree *t);
+
 void orc_set_threads(int n);
 int orc_get_threads(void);
 

@@ -20,9 +20,10 @@ enabled=true)`, or the environment variables SRMG_DEVICE and SRMG_DISABLE=1.
 module SteamrollerGPU
 
 using Steamroller
-using Steamroller: ScalarBlockField, LaplacianDiscretization, HelmholtzDiscretization,
+using Steamroller: ScalarBlockField, VectorBlockField, LaplacianDiscretization, HelmholtzDiscretization,
     CartesianGeometry, CylindricalGeometry, GeneralHomogeneousBoundaryConditions,
-    Neighbor, Boundary, RefBoundary, Child
+    Neighbor, Boundary, RefBoundary, Child, Tree, NetIonization
+using StaticArrays: SVector
 
 const libsrmg = get(ENV, "SRMG_LIB", joinpath(@__DIR__, "..", "srmg", "libsrmg.so"))
 
@@ -176,7 +177,7 @@ function solve!(u::GPUField, b::GPUField, s, tree, conn, geometry::GPUGeom,
     a = Ref(bc.a)
     # srmg_solve_opts / srmg_stats (include/srmg.h)
     opts = (Float64(tol), Cint(max_cycles), Cint(mixed ? 1 : 0), Cint(ndown), Cint(ntop), Cint(nup),
-            Float64(ω), Cint(1), Cint(0))
+            Float64(ω), Cint(2), Cint(0))
     optsref = Ref(opts)
     stats = Ref((Cint(0), Cint(0), Cint(0), 0.0, 0.0, 0.0, 0.0))
     GC.@preserve u b a optsref stats begin
@@ -189,6 +190,46 @@ function solve!(u::GPUField, b::GPUField, s, tree, conn, geometry::GPUGeom,
     end
     st = stats[]
     (st[2], st[4])
+end
+
+# ---- stage preparation and post-processing of derivs! (src/streamer.jl:309-351) ------
+
+# These receive no connectivity, so they run on the GPU only while the uploaded tree is
+# the one they are given (the solve of the previous stage uploaded it); after a
+# refinement they use the Julia methods until the next solve uploads the new tree.
+tree_current(tree) = STATE.enabled && STATE.ctx != C_NULL && fingerprint(tree) == STATE.fingerprint
+
+# netcharge!(tree, q, n, chem) (src/streamer.jl:369-373) for the NetIonization chemistry:
+# q = -n_e + n_ion on every valid cell, on the GPU (srmg_netcharge).
+function Steamroller.netcharge!(tree::Tree, q::GPUField, n::AbstractVector{<:GPUField}, chem::NetIonization)
+    if !tree_current(tree) || length(n) != 2
+        return invoke(Steamroller.netcharge!, Tuple{Tree,Any,Any,Any}, tree, q, n, chem)
+    end
+    ne, ni = n[1], n[2]
+    GC.@preserve q ne ni begin
+        check(ccall((:srmg_netcharge, libsrmg), Cint,
+                    (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int64),
+                    context(), pointer(q.u), pointer(ne.u), pointer(ni.u), size(q.u, 3)))
+    end
+    nothing
+end
+
+# electric_field!(tree, f, fabs, u, h, t, e0::SVector) (src/multigrid.jl:421-451) on the
+# GPU (srmg_electric_field): face fields and |E| of every block, bit-exact.
+function Steamroller.electric_field!(tree::Tree, f::VectorBlockField{2,16,2,Float64}, fabs::GPUField,
+                                     u::GPUField, h, t, e0::SVector{2})
+    if !tree_current(tree)
+        return invoke(Steamroller.electric_field!, Tuple{Tree,Any,Any,Any,Any,Any,SVector},
+                      tree, f, fabs, u, h, t, e0)
+    end
+    e0v = Ref((Float64(e0[1]), Float64(e0[2])))
+    GC.@preserve f fabs u e0v begin
+        check(ccall((:srmg_electric_field, libsrmg), Cint,
+                    (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int64, Float64, Ptr{Float64}),
+                    context(), pointer(f.u), pointer(fabs.u), pointer(u.u), size(u.u, 3), Float64(h),
+                    Base.unsafe_convert(Ptr{Float64}, e0v)))
+    end
+    nothing
 end
 
 end # module

@@ -95,6 +95,11 @@ SIGNATURES = {
     "srmg_gs_iter_dev": (_I, [_P, _P, _P, _I64, _I, _D, _D, _I, _I, _D, _I, _P]),
     "srmg_residual_level_dev": (_I, [_P, _P, _P, _P, _I64, _I, _D, _I, _D, _I]),
     "srmg_restrict_level_dev": (_I, [_P, _P, _I64, _I]),
+    "srmg_restrict_full_dev": (_I, [_P, _P, _I64]),
+    "srmg_netcharge": (_I, [_P, _P, _P, _P, _I64]),
+    "srmg_netcharge_dev": (_I, [_P, _P, _P, _P, _I64]),
+    "srmg_electric_field": (_I, [_P, _P, _P, _P, _I64, ctypes.c_double, _P]),
+    "srmg_electric_field_dev": (_I, [_P, _P, _P, _P, _I64, ctypes.c_double, _P]),
     "srmg_interp_add_level_dev": (_I, [_P, _P, _P, _I64, _I]),
     "srmg_residual_postrestrict_level_dev": (_I, [_P, _P, _P, _P, _I64, _I, _D, _I, _D, _I]),
     "srmg_resnorm_noalloc": (_I, [_P, _P, _P, _I64, _D, _I, _D, _I, _P]),
@@ -305,6 +310,36 @@ def fill_ghost_(ctx: Context, u, l, bc, mask=7):
     else:
         _order_after_torch(ctx, u)
         ctx.check(lib().srmg_fill_ghost_dev(ctx.handle, _ptr(u), u.shape[0], l, bca.ctypes.data, mask))
+
+
+def netcharge(ctx: Context, q, ne, nion):
+    """netcharge!(tree, q, n, chem) for NetIonization (src/streamer.jl:369-373): q = -ne + nion
+    on every valid cell.  numpy (host) or torch (device) fields of one kind."""
+    if isinstance(q, np.ndarray):
+        ctx.check(lib().srmg_netcharge(ctx.handle, _ptr(q), _ptr(ne), _ptr(nion), q.shape[0]))
+    else:
+        _order_after_torch(ctx, q, ne, nion)
+        ctx.check(lib().srmg_netcharge_dev(ctx.handle, _ptr(q), _ptr(ne), _ptr(nion), q.shape[0]))
+
+
+def restrict_full_(ctx: Context, u):
+    """restrict_full!(u, conn) (src/restrict.jl:43-47) on a device field."""
+    _order_after_torch(ctx, u)
+    ctx.check(lib().srmg_restrict_full_dev(ctx.handle, _ptr(u), u.shape[0]))
+
+
+def electric_field(ctx: Context, e, eabs, u, h, e0):
+    """electric_field!(tree, e, eabs, u, h, t, e0) with a constant background field e0 =
+    (e0_r, e0_z) (src/multigrid.jl:421-451).  e: [nblk, 2, 21, 21] (VectorBlockField
+    storage), eabs and u: [nblk, 20, 20]; numpy (host) or torch (device)."""
+    e0a = np.ascontiguousarray(e0, dtype=np.float64)
+    if isinstance(u, np.ndarray):
+        ctx.check(lib().srmg_electric_field(ctx.handle, _ptr(e), _ptr(eabs), _ptr(u), u.shape[0], float(h),
+                                            e0a.ctypes.data))
+    else:
+        _order_after_torch(ctx, e, eabs, u)
+        ctx.check(lib().srmg_electric_field_dev(ctx.handle, _ptr(e), _ptr(eabs), _ptr(u), u.shape[0], float(h),
+                                                e0a.ctypes.data))
 
 
 def solve(ctx: Context, u, b, s, geometry, bc, lpldisc=None, tol=1e-8, mode=MODE_FP64,

@@ -137,3 +137,36 @@ def test_vcycles_converge_to_manufactured_solution(which):
                 leaf[blk - 1, 2:18, 2:18] = True
     err = np.linalg.norm((u - ustar)[leaf]) / np.linalg.norm(ustar[leaf])
     assert err < 1e-8, err
+
+
+def test_netcharge_and_field_of_linear_potential(uniform3):
+    """netcharge! (src/streamer.jl:369-373) is nion - ne exactly; electric_field!
+    (src/multigrid.jl:421-449) of u = A r + B z (r, z cell centres of each level) is the
+    constant field (-A + e0_r, -B + e0_z) on every face and its magnitude on every cell."""
+    p = uniform3
+    ot = OracleTree(p.tree, p.conn, p.nblk)
+    rng = np.random.default_rng(4)
+    ne = rng.uniform(0, 1e20, (p.nblk, 20, 20))
+    ni = rng.uniform(0, 1e20, (p.nblk, 20, 20))
+    q = np.zeros_like(ne)
+    olib().orc_netcharge(_ptr(q), _ptr(ne), _ptr(ni), ot.ref)
+    vm = np.zeros(q.shape, dtype=bool)
+    vm[:, 2:18, 2:18] = True
+    assert np.array_equal(q[vm], (ni - ne)[vm])
+    assert np.all(q[~vm] == 0)
+
+    h, A, B, e0 = 7.8125e-4, 3.0e5, -1.25e6, np.array([250.0, 1.5e6])
+    u = np.zeros((p.nblk, 20, 20))
+    for l in range(1, len(p.tree) + 1):
+        I, J = cell_index_fields(p.tree, l, p.nblk)
+        hl = h / 2 ** (l - 1)
+        lev = ~np.isnan(I)
+        u = np.where(lev, A * (np.nan_to_num(I) - 0.5) * hl + B * (np.nan_to_num(J) - 0.5) * hl, u)
+    e = np.zeros((p.nblk, 2, 21, 21))
+    eabs = np.zeros((p.nblk, 20, 20))
+    olib().orc_electric_field(_ptr(e), _ptr(eabs), _ptr(u), h, _ptr(e0), ot.ref)
+    er = e[:, 0, 2:18, 2:19]   # faces 3..19 along r, cells 3..18 along z (1-based)
+    ez = e[:, 1, 2:19, 2:18]
+    np.testing.assert_allclose(er, -A + e0[0], rtol=1e-9)
+    np.testing.assert_allclose(ez, -B + e0[1], rtol=1e-9)
+    np.testing.assert_allclose(eabs[vm], np.hypot(-A + e0[0], -B + e0[1]), rtol=1e-9)
