@@ -273,6 +273,22 @@ def main():
     value = world * args.steps / (mixed_ms / 1e3)
     fp64_value = world * fp64_steps / (fp64_ms / 1e3)
 
+    # error of each result on the leaf cells against a tight FP64 solve (tol 1e-11; the
+    # FP64 GPU path matches the oracle to <= 1e-12 in the parity tests)
+    from srmg.timestep import leaf_mask
+    leaf = torch.from_numpy(leaf_mask(problem.tree, problem.nblk)).to(dev)
+    sols = {}
+    for name, mode, tol in (("reference", mg.MODE_FP64, 1e-11), ("mixed", mg.MODE_MIXED, TOL),
+                            ("fp64", mg.MODE_FP64, TOL)):
+        with torch.cuda.stream(stream):
+            u.zero_()
+        stream.synchronize()
+        mg.solve(ctx, u, b, s, geom, bc, tol=tol, mode=mode, max_cycles=5000)
+        sols[name] = u[leaf].clone()
+    nref = float(sols["reference"].norm())
+    err = {k: float((sols[k] - sols["reference"]).norm()) / nref for k in ("mixed", "fp64")}
+    err["reference"] = "FP64 GPU solve to 1e-11 (leaf cells, relative L2)"
+
     # roofline of the plain FP64 V-cycle (model bytes / event-timed V-cycle)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     r_, u1_ = torch.zeros_like(b), torch.zeros_like(b)
@@ -322,7 +338,7 @@ def main():
                          "peak_source": src,
                          "kernel": "plain FP64 V-cycle (whole cycle)", "bytes_per_launch": bytes_vc,
                          "ms_per_vcycle": vc_ms},
-            "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}
+            "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(), "error_vs_fp64": err}
     all_cells = sum(len(layer) for layer in problem.tree) * 256
     line["cells_vcycles_per_s"] = {
         "leaf": nleaf * mixed_st["cycles"] * value, "all_levels": all_cells * mixed_st["cycles"] * value,
