@@ -486,6 +486,33 @@ __device__ __forceinline__ HaloCell halo_cell(int t) {
   return h;
 }
 
+// The red halo cell m (0..31) handled by lane m % 8 of warp m / 8 of a half slot (the
+// cell 2 (m % 8) + (m / 8 % 2) of ghost face m / 8), packed into two ints once per CTA:
+// {hx | hy << 5 | nx << 10 | ny << 15 | f << 20 | nsub << 22, (cx + 1) | (cy + 1) << 6 |
+// (cnx + 1) << 12 | (cny + 1) << 18}, the corner fields all -1 where there is none.
+__device__ __forceinline__ int2 halo_pack(int m) {
+  const HaloCell h = halo_cell(16 * (m >> 3) + 2 * (m & 7) + ((m >> 3) & 1));
+  const int w0 = h.hx | (h.hy << 5) | (h.nx << 10) | (h.ny << 15) | (h.f << 20) | (h.nsub << 22);
+  const int w1 = h.cx < 0 ? 0 : (h.cx + 1) | ((h.cy + 1) << 6) | ((h.cnx + 1) << 12) | ((h.cny + 1) << 18);
+  return make_int2(w0, w1);
+}
+__device__ __forceinline__ HaloCell halo_unpack(int2 w) {
+  HaloCell h;
+  h.hx = w.x & 31;
+  h.hy = (w.x >> 5) & 31;
+  h.nx = (w.x >> 10) & 31;
+  h.ny = (w.x >> 15) & 31;
+  h.f = (w.x >> 20) & 3;
+  h.nsub = (w.x >> 22) & 3;
+  h.jj = 0;
+  h.red = true;
+  h.cx = (w.y & 63) - 1;
+  h.cy = ((w.y >> 6) & 63) - 1;
+  h.cnx = ((w.y >> 12) & 63) - 1;
+  h.cny = ((w.y >> 18) & 63) - 1;
+  return h;
+}
+
 // Vector access to the two cells (x, x+1), x even, of a tile row: 16 bytes (FP64) or 8
 // bytes (FP32), aligned because tiles and fields are 16-byte aligned and kS is even.
 template <typename T> struct Pair2;
@@ -586,7 +613,7 @@ __device__ __forceinline__ bool slot_and(int slot, bool ok) {
 template <typename T>
 __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T *esrc, bool copy_u1,
                        bool make_e, bool fas, int first, int step, int t, int slot, SlotSmem<T> &S,
-                       unsigned &pk) {
+                       unsigned &pk, const int2 *halo_tab) {
   const int n = A.tr.nblk[l - 1];
   const int4 *recs = A.tr.lvl_rec[l - 1];
   const int nmine = (first < n) ? (n - 1 - first) / step + 1 : 0;
@@ -602,14 +629,14 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
   const int mysub = ((x0 - 2) >> 3) + 2 * ((y - 2) >> 3);
   // lanes 0-7 of warp wv: the red cells 2 lane + (wv % 2) of ghost face wv
   const bool hthr = lane < 8;
-  const int hidx = 16 * wv + 2 * (lane & 7) + (wv & 1);
+  const int hm = 8 * wv + (lane & 7);  // this lane's entry of the halo table
   // neighbour values of the halo cell, loaded one iteration ahead
   // (b comes from b's ghost layer when A.bghost, except the FAS right-hand side of a
   // covered neighbour cell, formed here from the neighbour's restricted residual in e)
   T hvn = T(0), hcn = T(0);
   auto prefetch = [&](int j) {
     if (hthr) {
-      const HaloCell hc_ = halo_cell(hidx);
+      const HaloCell hc_ = halo_unpack(halo_tab[hm]);
       const int4 fi = S.recs[j][1 + hc_.f];
       if (fi.x == FACE_NEIGHBOR) {
         const int64_t nb = (int64_t)fi.y * kSS;
@@ -705,7 +732,7 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
       T halo_new = T(0);
       int halo_o = -1;
       if (act && ok && hthr) {
-        const HaloCell hc_ = halo_cell(hidx);
+        const HaloCell hc_ = halo_unpack(halo_tab[hm]);
         const int4 fi = fc[hc_.f];
         if (fi.x == FACE_NEIGHBOR) {
           auto at = [&](int a, int c) -> T { return (a == hc_.cx && c == hc_.cy) ? hc : tile[a + kS * c]; };
@@ -1341,6 +1368,8 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
     for (int q = 0; q < kBuf; ++q) mbar_init(&S.bar[q]);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  __shared__ int2 s_halo[32];  // the GS halo cells, packed (halo_pack)
+  if (threadIdx.x < 32) s_halo[threadIdx.x] = halo_pack(threadIdx.x);
   __syncthreads();
   unsigned pk = 0;  // items streamed through this slot's buffers so far
   unsigned epoch = 0;
@@ -1382,7 +1411,7 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
     const int l = A.smooth_level;
     for (int it = 0; it < A.smooth_n; ++it) {
       const bool ok = ph_gsi<T>(A, l, fld(l), oth(l), nullptr, false, false, false, first_of(false),
-                                step_of(false), t, slot, S, pk);
+                                step_of(false), t, slot, S, pk, s_halo);
       cur ^= 1u << l;
       if (!sync(ok, false, false)) return;
     }
@@ -1464,7 +1493,7 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
         bool ok = true;
         if (runs(loc))
           ok = ph_gsi<T>(A, l, fld(l), oth(l), nullptr, it == 0 && l < L, false, it == 0 && l < L, first_of(loc),
-                         step_of(loc), t, slot, S, pk);
+                         step_of(loc), t, slot, S, pk, s_halo);
         cur ^= 1u << l;
         if (!sync(ok, loc, loc)) return false;
       }
@@ -1484,7 +1513,7 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
         bool ok = true;
         if (runs(loc))
           ok = ph_gsi<T>(A, 1, fld(1), oth(1), nullptr, it == 0 && L > 1, last && L > 1, it == 0 && L > 1,
-                         first_of(loc), step_of(loc), t, slot, S, pk);
+                         first_of(loc), step_of(loc), t, slot, S, pk, s_halo);
         cur ^= 1u << 1;
         if (!sync(ok, loc, last ? (2 <= K || L < 2) : loc)) return false;
       }
@@ -1500,7 +1529,7 @@ __global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant
         bool ok = true;
         if (runs(loc))
           ok = ph_gsi<T>(A, l, fld(l), oth(l), A.e, false, last && l < L, false, first_of(loc), step_of(loc), t,
-                         slot, S, pk);
+                         slot, S, pk, s_halo);
         cur ^= 1u << l;
         const bool next_loc = last ? ((l + 1) <= K) : loc;
         if (!sync(ok, loc, l == L && last ? false : next_loc)) return false;
