@@ -395,6 +395,9 @@ int srmg_streamer_step_dev(srmg_ctx *ctx, double *ne, double *npos, double *nneg
  *   "local_max_blocks" coarse levels whose every coarser level has at most this many
  *                      blocks run inside one CTA of the persistent kernel (default 4);
  *   "engine_ctas"      CTAs of the persistent kernel (0 = one per SM);
+ *   "engine_threads"   threads per CTA of the persistent kernel: 768 (three slots, more
+ *                      registers per thread) or 1024 (four slots); 0 (default) picks 768
+ *                      for trees of up to 16384 blocks and 1024 above;
  *   "trace"            1 = record a %globaltimer stamp (ns) after every phase of the
  *                      persistent kernel, read back with srmg_get_trace;
  *   "graph"            1 = batched solves replay a captured CUDA graph;

@@ -825,6 +825,10 @@ extern "C" int srmg_set_option(srmg_ctx *ctx, const char *key, int64_t value) {
       if (value > nsm) return fail(ctx, SRMG_ERR_BADARG, "engine_ctas above the SM count (%d)", nsm);
     }
     ctx->engine_ctas = (int)value;
+  } else if (!strcmp(key, "engine_threads")) {
+    if (value != 0 && value != 768 && value != 1024)
+      return fail(ctx, SRMG_ERR_BADARG, "engine_threads must be 0 (by tree size), 768 or 1024");
+    ctx->engine_threads = (int)value;
   } else return fail(ctx, SRMG_ERR_BADARG, "unknown option '%s'", key);
   return SRMG_OK;
 }

@@ -224,6 +224,7 @@ static std::vector<const void *> graph_key_of(srmg_ctx *ctx, double *const *u, c
   memcpy(tb.data(), ctx->it_tab_host.data(), ctx->it_tab_host.size());
   k.insert(k.end(), tb.begin(), tb.end());
   k.push_back((const void *)(intptr_t)ctx->engine_ctas);
+  k.push_back((const void *)(intptr_t)ctx->engine_threads);
   k.push_back((const void *)(intptr_t)ctx->local_max_blocks);
   k.push_back((const void *)(intptr_t)ctx->trace_on);
   return k;

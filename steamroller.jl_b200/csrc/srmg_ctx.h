@@ -81,6 +81,7 @@ struct srmg_ctx {
   srmg::DevBuf sync;         // {barrier counter, error word}
   int num_sms = 0;
   int engine_ctas = 0;       // cooperative grid size (0 = not yet known)
+  int engine_threads = 0;    // threads per CTA of the persistent kernel: 768 or 1024 (0 = by tree size)
   int local_max_blocks = 4;  // levels whose every coarser level has <= this many blocks run in CTA 0
                              // (4 measured fastest on the 1.5M- and 10M-leaf trees)
   bool use_engine = true;

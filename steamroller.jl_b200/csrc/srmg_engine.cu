@@ -33,13 +33,26 @@ const double *wrow_of<double>(srmg_ctx *ctx) { return ctx->d_wrow64; }
 template <>
 const float *wrow_of<float>(srmg_ctx *ctx) { return ctx->d_wrow32; }
 
+// Threads per CTA for this context: the "engine_threads" option, else by tree size
+// (measured: 768 threads are faster up to ~16k blocks, 1024 above).
+int engine_threads_of(const srmg_ctx *ctx) {
+  if (ctx->engine_threads) return ctx->engine_threads;
+  return ctx->max_blk <= 16384 ? kEngineNarrow : kEngineWide;
+}
+
 template <typename T>
-int engine_grid(srmg_ctx *ctx, int *grid) {
+const void *engine_kernel(int threads) {
+  return threads == kEngineNarrow ? (const void *)k_engine_vcycle<T, kEngineNarrow>
+                                  : (const void *)k_engine_vcycle<T, kEngineWide>;
+}
+
+template <typename T>
+int engine_grid(srmg_ctx *ctx, int threads, int *grid) {
   if (ctx->num_sms == 0) CK(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
-  const size_t smem = engine_smem_bytes<T>();
-  CK(cudaFuncSetAttribute(k_engine_vcycle<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const size_t smem = engine_smem_bytes<T>(threads);
+  CK(cudaFuncSetAttribute(engine_kernel<T>(threads), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_engine_vcycle<T>, 1024, smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, engine_kernel<T>(threads), threads, smem));
   if (per_sm < 1) return fail(ctx, SRMG_ERR_CUDA, "engine kernel cannot be resident (occupancy 0)");
   *grid = ctx->num_sms * std::min(per_sm, 1);
   return SRMG_OK;
@@ -104,11 +117,12 @@ static int engine_common(srmg_ctx *ctx, EngArgs<T> &A, T *u, const ItemTabs &tab
 template <typename T>
 static int engine_launch(srmg_ctx *ctx, EngArgs<T> &A) {
   int grid = 0;
-  RC(engine_grid<T>(ctx, &grid));  // also raises the dynamic shared-memory limit
+  const int threads = engine_threads_of(ctx);
+  RC(engine_grid<T>(ctx, threads, &grid));  // also raises the dynamic shared-memory limit
   if (ctx->engine_ctas > 0 && ctx->engine_ctas < grid) grid = ctx->engine_ctas;
   void *args[] = {&A};
-  CK(cudaLaunchCooperativeKernel((const void *)k_engine_vcycle<T>, dim3(grid), dim3(1024), args,
-                                 engine_smem_bytes<T>(), ctx->stream));
+  CK(cudaLaunchCooperativeKernel(engine_kernel<T>(threads), dim3(grid), dim3(threads), args,
+                                 engine_smem_bytes<T>(threads), ctx->stream));
   ctx->launches++;
   return SRMG_OK;
 }

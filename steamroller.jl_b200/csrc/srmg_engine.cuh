@@ -1222,11 +1222,12 @@ __device__ void ph_blocknorm(const EngArgs<T> &A, bool defect, bool with_b, int 
   }
 }
 
-// Per-item norms from the chunk partials, one CTA (1024 threads) per item, in a fixed
-// order: thread-strided sums over the item's chunk partials, the warp sums, then the
-// 32 warp sums in order.  Writes inorm[4 k + 0] (and with `first` the |b| and
-// initial-norm entries), the item's V-cycle count, and freezes the item once its norm
-// is <= tol * |b| (|b| = 0 counts as 1) or not finite.  Items frozen before are skipped.
+// Per-item norms from the chunk partials, one CTA per item, in a fixed order: sums over
+// the item's chunk partials strided by kNormLanes lanes, the warp sums, then the
+// kNormLanes / 32 warp sums in order.  Writes the item's record (norm; with `first` |b|
+// and the initial norm; V-cycles and steps run) and freezes the item once its norm is
+// <= tol * |b| (|b| = 0 counts as 1) or not finite.  Items frozen before are skipped.
+constexpr int kNormLanes = 768;  // <= the smaller launch shape
 template <typename T>
 __device__ void ph_itemnorm(const EngArgs<T> &A, bool first, int cycles, int steps, double *red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1234,10 +1235,13 @@ __device__ void ph_itemnorm(const EngArgs<T> &A, bool first, int cycles, int ste
     if (A.frozen[k]) continue;
     double v = 0.0, vb = 0.0;
     const int2 rg = A.it_chunks[k];
-    for (int j = threadIdx.x; j < rg.y; j += blockDim.x) {
-      v += A.bpart[rg.x + j];
-      if (first) vb += A.bpart_b[rg.x + j];
-    }
+    // a fixed width of kNormLanes lanes, whatever the CTA size, so that an item's norm
+    // has the same rounding in every launch shape (a batch matches its solo solves)
+    if (threadIdx.x < kNormLanes)
+      for (int j = threadIdx.x; j < rg.y; j += kNormLanes) {
+        v += A.bpart[rg.x + j];
+        if (first) vb += A.bpart_b[rg.x + j];
+      }
     for (int off = 16; off > 0; off >>= 1) {
       v += __shfl_xor_sync(0xffffffffu, v, off);
       vb += __shfl_xor_sync(0xffffffffu, vb, off);
@@ -1249,7 +1253,7 @@ __device__ void ph_itemnorm(const EngArgs<T> &A, bool first, int cycles, int ste
     __syncthreads();
     if (threadIdx.x == 0) {
       double sv = 0.0, sb = 0.0;
-      for (int q = 0; q < 32; ++q) {
+      for (int q = 0; q < kNormLanes / 32; ++q) {
         sv += red[q];
         sb += red[32 + q];
       }
@@ -1351,13 +1355,19 @@ __device__ void ph_copy_back(const EngArgs<T> &A, int l, const T *src, T *dst, i
 
 // ------------------------------------------------------------------ the kernel
 
-template <typename T>
-constexpr size_t engine_smem_bytes() {
-  return 4 * sizeof(SlotSmem<T>);
-}
+// Threads per CTA of the persistent kernel: 1024 (four 256-thread slots, 64 registers a
+// thread) or 768 (three slots, 80 registers).  The wider CTA carries more blocks at a
+// time on large levels; the narrower one spills far less, which shortens the latency
+// chains that small trees are made of.
+constexpr int kEngineWide = 1024, kEngineNarrow = 768;
 
 template <typename T>
-__global__ void __launch_bounds__(1024, 1) k_engine_vcycle(const __grid_constant__ EngArgs<T> A) {
+constexpr size_t engine_smem_bytes(int threads) {
+  return (size_t)(threads / 256) * sizeof(SlotSmem<T>);
+}
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT, 1) k_engine_vcycle(const __grid_constant__ EngArgs<T> A) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   SlotSmem<T> *smem = reinterpret_cast<SlotSmem<T> *>(smem_raw);
   const int nslots = blockDim.x >> 8;

@@ -166,3 +166,29 @@ def test_autotune_single_and_batch(setup):
                       ntop=chosen["ntop"], max_cycles=400)
     assert all(s["rel_residual"] <= 1e-8 for s in sts)
     batch.set_option("engine_ctas", 0).set_option("local_max_blocks", 4)
+
+
+@pytest.mark.parametrize("mode", [mg.MODE_FP64, mg.MODE_MIXED])
+def test_launch_shape_independent(setup, mode):
+    """The persistent kernel runs with 768 or 1024 threads per CTA (option
+    "engine_threads"; by default chosen from the tree size): solo and batched results,
+    cycle counts and norms are bit-identical in both shapes."""
+    _, items, batch = setup
+    c, p = items[0]
+    out = {}
+    for nt in (768, 1024):
+        c.set_option("engine_threads", nt)
+        batch.set_option("engine_threads", nt)
+        u_solo, st_solo = solo(c, p, mode)
+        us = [torch_cuda(np.zeros_like(q.b)) for _, q in items]
+        sts = batch.solve(us, [torch_cuda(q.b) for _, q in items], mode=mode, **OPTS)
+        out[nt] = (u_solo, st_solo, [to_np(u) for u in us], sts)
+    c.set_option("engine_threads", 0)
+    batch.set_option("engine_threads", 0)
+    a, b = out[768], out[1024]
+    np.testing.assert_array_equal(a[0].view(np.uint64), b[0].view(np.uint64))
+    assert a[1]["cycles"] == b[1]["cycles"] and a[1]["rel_residual"] == b[1]["rel_residual"]
+    for k in range(len(items)):
+        np.testing.assert_array_equal(a[2][k].view(np.uint64), b[2][k].view(np.uint64))
+        assert a[3][k]["cycles"] == b[3][k]["cycles"]
+        assert a[3][k]["rel_residual"] == b[3][k]["rel_residual"]
