@@ -42,8 +42,8 @@ SEED = 2
 TARGET_LEAF = 1_500_000
 METRIC = "field solves/sec at 1e-8 rel residual (mixed-precision multigrid; plain FP64 GPU alongside)"
 # DRAM bytes of one plain FP64 V-cycle launch on the config-2 tree, from an ncu capture
-# (62.26 MB read + 56.06 MB written)
-TRAFFIC_VCYCLE_CONFIG2 = 118.32e6
+# (57.72 MB read + 41.05 MB written)
+TRAFFIC_VCYCLE_CONFIG2 = 98.77e6
 
 
 def peaks():
