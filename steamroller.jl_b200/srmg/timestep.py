@@ -134,7 +134,9 @@ def run(net, steps=200, sample_every=50, device=0, log=None, problem=None):
                           "photo_cycles_max": float(np.mean(rec["photo_cycles"])),
                           "kept": {"previous": float(np.mean(w == 0)), "extrapolated": float(np.mean(w == 1)),
                                    "learned": float(np.mean(w == 2))}},
-        "fp64_gpu": {"step_ms": float(fp64_ms), "poisson_cycles": float(fp64_cyc)},
+        "fp64_gpu": {"step_ms": float(fp64_ms), "poisson_cycles": float(fp64_cyc),
+                     "photo_cycles": [float(np.mean([x["fp64_photo_cycles"][j] for x in samples]))
+                                      for j in range(len(LAMBDAS))]},
         "speedup_vs_fp64_gpu": float(fp64_ms / step_ms.mean()),
         "error_vs_fp64": {"poisson_rel_l2_max": max(x["err_poisson"] for x in samples),
                           "photo_rel_l2_max": max(x["err_photo"] for x in samples)},
@@ -157,9 +159,11 @@ def fp64_sample(s, psi, psi_prev, src, phi_prev, stream, opts, mask_t):
         stream.synchronize()
         ev0.record(stream)
         st = mg.solve(s.ctx, u, s.b, s.s, s.geom, s.bc, mode=mg.MODE_FP64, **opts)
+        photo_cycles = []
         for j, lam in enumerate(LAMBDAS):
-            mg.solve(s.ctx, ps[j], src[j], batch_s(s), s.geom, gen.BC_PHOTO, ("helmholtz", lam * lam),
-                     mode=mg.MODE_FP64, **opts)
+            sth = mg.solve(s.ctx, ps[j], src[j], batch_s(s), s.geom, gen.BC_PHOTO, ("helmholtz", lam * lam),
+                           mode=mg.MODE_FP64, **opts)
+            photo_cycles.append(sth["cycles"])
         ev1.record(stream)
         ev1.synchronize()
         ms = ev0.elapsed_time(ev1)
@@ -173,7 +177,8 @@ def fp64_sample(s, psi, psi_prev, src, phi_prev, stream, opts, mask_t):
             n = ps[j][mask_t].norm()
             if n > 0:
                 err_h = max(err_h, float(((psi[j] - ps[j])[mask_t]).norm() / n))
-    return {"fp64_step_ms": ms, "fp64_poisson_cycles": st["cycles"], "err_poisson": err_p, "err_photo": err_h}
+    return {"fp64_step_ms": ms, "fp64_poisson_cycles": st["cycles"], "fp64_photo_cycles": photo_cycles,
+            "err_poisson": err_p, "err_photo": err_h}
 
 
 def batch_s(s):

@@ -328,12 +328,31 @@ def test_resnorm_matches_oracle(pair):
     assert abs(got - want) <= 1e-10 * abs(want)
 
 
-def test_fp64_solve_to_tolerance():
-    p = PROBS["refined"]
+def variant_problem(variant):
+    base = PROBS["refined"]
+    kw = dict(tree=base.tree, conn=base.conn, b=base.b.copy(), s=base.s, h1=base.h1, name=variant)
+    if variant == "helmholtz":
+        p = gen.Problem(**kw, op=gen.OP_HELMHOLTZ, k2=3.1e6, geom=gen.GEOM_CYL1, bc=gen.BC_PHOTO)
+        p.s = base.h1 ** 2
+        return p
+    if variant == "cartesian":
+        return gen.Problem(**kw, geom=gen.GEOM_CART)
+    if variant == "cyl2":
+        return gen.Problem(**kw, geom=gen.GEOM_CYL2)
+    return base
+
+
+@pytest.mark.parametrize("variant", ["poisson", "helmholtz", "cartesian", "cyl2"])
+def test_fp64_solve_to_tolerance(variant):
+    """The tolerance-driven FP64 solve (one persistent launch; its halo updates read the
+    neighbours' b from the engine copy's ghost layer) runs the oracle's cycle count and
+    ends on its iterate."""
+    p = variant_problem(variant)
     pr = Pair(p)
     u, b = _prepared(pr)
     ug = torch_cuda(u)
-    st = mg.solve(pr.ctx, ug, torch_cuda(b), p.s, p.geom, p.bc, tol=1e-8, mode=mg.MODE_FP64,
+    lpl = ("helmholtz", p.k2) if p.op == 1 else None
+    st = mg.solve(pr.ctx, ug, torch_cuda(b), p.s, p.geom, p.bc, lpldisc=lpl, tol=1e-8, mode=mg.MODE_FP64,
                   max_cycles=2000)
     uo = u.copy()
     c, rel = pr.orc.solve(uo, b.copy(), 1e-8, max_cycles=2000)
