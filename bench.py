@@ -10,9 +10,10 @@ data with the shapes of the reference's own setup (no published data exists).
              direct coarsest-level solve) with fields resident in HBM
   fp64       the plain FP64 GPU multigrid (the reference's V-cycle, repeated to the
              same tolerance) on the same tree
-  roofline   the plain FP64 V-cycle: algorithmic bytes of the multigrid model
-             (srmg.model.vcycle_bytes) / measured V-cycle time, against the measured
-             HBM copy peak
+  roofline   the timed kernel (one mixed-solve launch per step): algorithmic bytes
+             of the model (srmg.model.mixed_solve_bytes) / its event-timed duration,
+             against the measured HBM copy peak; roofline_fp64_vcycle the same for
+             one plain FP64 V-cycle (srmg.model.vcycle_bytes)
   e2e        the same solve through the C ABI with host arrays (H2D of u and b and
              D2H of u inside the timed region)
   cpu_baseline  the oracle (C restatement of the reference FP64 solve, OpenMP) on
@@ -44,6 +45,8 @@ METRIC = "field solves/sec at 1e-8 rel residual (mixed-precision multigrid; plai
 # DRAM bytes of one plain FP64 V-cycle launch on the config-2 tree, from an ncu capture
 # (57.72 MB read + 41.05 MB written)
 TRAFFIC_VCYCLE_CONFIG2 = 98.77e6
+# DRAM bytes of one mixed-solve launch on the config-2 tree, from an ncu capture
+TRAFFIC_MIXED_CONFIG2 = None
 
 
 def peaks():
@@ -56,52 +59,101 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled while the timed region runs."""
+    """SM clocks and clock-event (throttle) reasons sampled through NVML every 5 ms while
+    the timed region runs (nvidia-smi's fastest loop, 200 ms, would see one sample of a
+    40 ms region).  Falls back to `nvidia-smi -lms 200` when NVML is not importable."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits (nvml.h: nvmlClocksEventReason*)
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+            "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
 
-    def __init__(self, index):
+    def __init__(self, index, period_s=0.005):
         self.index = index
-        self.rows = []
+        self.period = period_s
+        self.sm, self.mx, self.reasons = [], [], set()
         self.proc = None
+        self.nvml = None
+        self.stop_ev = threading.Event()
+        self.t = None
 
-    def __enter__(self):
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def start(self):
+        self.stop_ev.clear()
+        try:
+            self.nvml, self.h = self._handle()
+            self.t = threading.Thread(target=self._poll, daemon=True)
             self.t.start()
         except Exception:
-            self.proc = None
+            self.nvml = None
+            try:
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                     "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.t = threading.Thread(target=self._read, daemon=True)
+                self.t.start()
+            except Exception:
+                self.proc = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+    def _poll(self):
+        nv = self.nvml
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        mx = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+        while True:
+            self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+            self.mx.append(float(mx))
+            bits = int(get_reasons(self.h))
+            for name, bit in self.BITS.items():
+                if bits & bit:
+                    self.reasons.add(name)
+            if self.stop_ev.wait(self.period):
+                break
 
-    def __exit__(self, *a):
+    def _read(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.proc.stdout:
+            r = [x.strip() for x in line.split(",")]
+            if len(r) > 8 and r[1].replace(".", "").isdigit():
+                self.sm.append(float(r[1]))
+                self.mx.append(float(r[2]))
+                for k, n in enumerate(names):
+                    if r[5 + k].lower() == "active":
+                        self.reasons.add(n)
+
+    def stop(self):
+        self.stop_ev.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.t is not None:
+            self.t.join(timeout=5)
+
+    def __enter__(self):
+        return self.start()
+
+    def __exit__(self, *a):
+        self.stop()
 
     def summary(self):
-        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
-        reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
-            if len(r) > 8:
-                for k, n in enumerate(names):
-                    if r[5 + k].lower() == "active":
-                        reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+        return {"sm_mhz": float(np.median(self.sm)) if self.sm else None,
+                "sm_max_mhz": max(self.mx) if self.mx else None, "reasons": sorted(self.reasons),
+                "samples": len(self.sm), "source": "nvml, 5 ms" if self.nvml else "nvidia-smi, 200 ms"}
 
 
 def dist_setup(backend=None):
@@ -246,13 +298,15 @@ def main():
         u.zero_()
         return mg.solve(ctx, u, b, s, geom, bc, tol=TOL, mode=mode, max_cycles=max_cycles)
 
-    def timed(mode, steps, warm):
+    def timed(mode, steps, warm, clk=None):
         for _ in range(warm):
             with torch.cuda.stream(stream):
                 st = one_solve(mode)
         barrier(pg, dev)
         total_ms, stats = 0.0, None
         l0 = ctx.launches()
+        if clk is not None:
+            clk.start()
         for _ in range(steps):
             with torch.cuda.stream(stream):
                 flush.fill_(1.0)
@@ -261,11 +315,13 @@ def main():
             st = mg.solve(ctx, u, b, s, geom, bc, tol=TOL, mode=mode, max_cycles=5000)
             total_ms += st["device_ms"]
             stats = st
+        if clk is not None:
+            clk.stop()
         barrier(pg, dev)
         return total_ms, stats, ctx.launches() - l0
 
-    with ClockSampler(local) as clk:
-        mixed_ms, mixed_st, launches = timed(mg.MODE_MIXED, args.steps, args.warmup)
+    clk = ClockSampler(local)
+    mixed_ms, mixed_st, launches = timed(mg.MODE_MIXED, args.steps, args.warmup, clk)
     fp64_steps = max(1, args.fp64_steps)
     fp64_ms, fp64_st, _ = timed(mg.MODE_FP64, fp64_steps, 1)
     mixed_ms = max_over_ranks(mixed_ms, pg, dev)
@@ -306,6 +362,9 @@ def main():
     bytes_vc = model.vcycle_bytes(problem.tree, 8, 2, 2, 4)
     hbm, src = peaks()
     achieved = bytes_vc / (vc_ms / 1e3) / 1e9
+    # the timed kernel: one mixed-solve launch per step, event-timed on the context's stream
+    bytes_mx = model.mixed_solve_bytes(problem.tree, mixed_st["cycles"], mixed_st["outer"])
+    achieved_mx = bytes_mx / (mixed_ms / args.steps / 1e3) / 1e9
 
     # e2e through the host-pointer C ABI, from page-locked host buffers
     uh = torch.zeros(problem.b.shape, dtype=torch.float64).pin_memory().numpy()
@@ -331,13 +390,21 @@ def main():
             "mixed": {"cycles_per_solve": mixed_st["cycles"], "outer_steps": mixed_st["outer"],
                       "rel_residual": mixed_st["rel_residual"]},
             "speedup_vs_fp64": value / fp64_value,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": TRAFFIC_VCYCLE_CONFIG2 if nleaf == 1503232 else None,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one V-cycle launch "
-                                           "on this tree (most of the working set stays in L2)",
+            "roofline": {"bound": "hbm", "achieved": achieved_mx, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved_mx / hbm,
+                         "traffic": TRAFFIC_MIXED_CONFIG2 if nleaf == 1503232 else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one mixed-solve "
+                                           "launch on this tree (most of the working set stays in L2)",
                          "peak_source": src,
-                         "kernel": "plain FP64 V-cycle (whole cycle)", "bytes_per_launch": bytes_vc,
-                         "ms_per_vcycle": vc_ms},
+                         "kernel": "mixed-precision solve (one persistent launch per solve: the timed kernel)",
+                         "bytes_per_launch": bytes_mx, "ms_per_launch": mixed_ms / args.steps,
+                         "bytes_model": "srmg.model.mixed_solve_bytes(tree, cycles=%d, steps=%d)"
+                                        % (mixed_st["cycles"], mixed_st["outer"])},
+            "roofline_fp64_vcycle": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                                     "frac": achieved / hbm,
+                                     "traffic": TRAFFIC_VCYCLE_CONFIG2 if nleaf == 1503232 else None,
+                                     "peak_source": src, "kernel": "plain FP64 V-cycle (whole cycle)",
+                                     "bytes_per_launch": bytes_vc, "ms_per_vcycle": vc_ms},
             "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(), "error_vs_fp64": err}
     all_cells = sum(len(layer) for layer in problem.tree) * 256
     line["cells_vcycles_per_s"] = {

@@ -27,3 +27,23 @@ def vcycle_bytes(tree, w=8, ndown=2, nup=2, ntop=4, M=16):
         total += w * n[l - 1] * (3 * (ndown + nup) + 8.5) + 5 * w * n[l - 2]
     total += 3 * w * ntop * (n[0] if n else 0)
     return total
+
+
+def mixed_solve_bytes(tree, cycles, steps, ndown=2, nup=2, ntop=4, M=16):
+    """Algorithmic bytes of one mixed-precision solve (one persistent launch).
+
+    `cycles` FP32 V-cycles (w = 4) plus the FP64 side of the defect correction, with N
+    the valid cells of all levels and N2 those of levels >= 2:
+      * steps + 1 defect passes: read u64 and b64, write the FP32 right-hand side and
+        zero the FP32 correction (24 B per cell);
+      * steps + 1 restrictions of u64 onto the covered subblocks (8 B read per fine
+        cell + 8/4 B written: 10 B per cell of levels >= 2);
+      * steps updates u64 += e: read u64 and e, write u64 (20 B per cell).
+    The coarsest level's direct solve (one 256 x 256 FP64 matrix-vector product per
+    item) replaces the ntop sweeps; both are negligible next to the finer levels.
+    """
+    n = level_cells(tree, M)
+    N = float(sum(n))
+    N2 = float(sum(n[1:]))
+    fp64 = (steps + 1) * (24.0 * N + 10.0 * N2) + steps * 20.0 * N
+    return cycles * vcycle_bytes(tree, 4, ndown, nup, ntop, M) + fp64
