@@ -17,11 +17,13 @@
  * Edge structs below are the isbits layouts of the Julia structs, so Julia vectors
  * are passed without conversion.  All block indices and coordinates are 1-based.
  *
- * Supported: D = 2, M = 16, G = 2, order-2 Laplacian / Helmholtz discretisations,
- * Cartesian and cylindrical geometries, homogeneous boundary conditions
- * (GeneralHomogeneousBoundaryConditions, src/boundary.jl:21-38) and a StarStencil
- * connectivity.  Anything else returns SRMG_ERR_UNSUPPORTED and the Julia shim keeps
- * the original Julia method.
+ * Supported: D = 2, M = 16, G = 2, order-2 Laplacian / Helmholtz discretisations
+ * and the compact order-4 Laplacian, Cartesian and cylindrical geometries,
+ * homogeneous boundary conditions (GeneralHomogeneousBoundaryConditions,
+ * src/boundary.jl:21-38), and a StarStencil or BoxStencil connectivity
+ * (src/connectivity.jl:106-149; the BoxStencil one adds diagonal edges that fill the
+ * 2 x 2 corner ghosts).  Anything else returns SRMG_ERR_UNSUPPORTED and the Julia shim
+ * keeps the original Julia method.
  *
  * Every entry point returns SRMG_OK (0) or a negative SRMG_ERR_* code;
  * srmg_last_error() gives the message.  A context is not thread-safe; distinct
@@ -47,9 +49,16 @@ extern "C" {
 #define SRMG_ERR_NOTREE      -8
 
 /* lpldisc: LaplacianDiscretization{2,2} / HelmholtzDiscretization{2,2}(k2)
- * (src/laplacian.jl:14, src/helmholtz.jl:9-11). */
+ * (src/laplacian.jl:14, src/helmholtz.jl:9-11), and LaplacianDiscretization{2,4}, the
+ * compact order-4 scheme (src/laplacian.jl:131-209): 9-point left-hand side, 5-point
+ * right-hand side applied by srmg_rhs_level, four-colour Gauss-Seidel
+ * (src/multigrid.jl:206-232, 268-295).  Order 4 needs a tree set with a BoxStencil
+ * connectivity and runs FP64 on the per-operation kernels (vcycle, fmg, resnorm,
+ * FP64 srmg_solve); mixed precision, batches and the autotuner return
+ * SRMG_ERR_UNSUPPORTED for it. */
 #define SRMG_OP_LAPLACIAN 0
 #define SRMG_OP_HELMHOLTZ 1
+#define SRMG_OP_LAPLACIAN4 2
 /* geometry: CartesianGeometry, CylindricalGeometry{1}, CylindricalGeometry{2}
  * (src/geometry.jl:14-20). */
 #define SRMG_GEOM_CARTESIAN 0
@@ -183,7 +192,9 @@ int srmg_solve_dev(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc
  * bit 1 = fill_ghost_bnd!, bit 2 = fill_ghost_interp!; 7 = fill_ghost!. */
 int srmg_fill_ghost_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level,
                         const int8_t bc[9], int mask);
-/* gauss_seidel_level!(..., RedBlack{parity}) (src/multigrid.jl:238-243). */
+/* gauss_seidel_level!(..., RedBlack{parity}) (src/multigrid.jl:238-243); for
+ * SRMG_OP_LAPLACIAN4, FourColors{parity >> 1, parity & 1} with parity 0..3
+ * (src/multigrid.jl:206-232). */
 int srmg_gs_level_dev(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, int level,
                       double omega, double sl, int op, double k2, int geom, int parity);
 /* gauss_seidel_iter! (src/multigrid.jl:250-265). */
@@ -215,6 +226,15 @@ int srmg_netcharge(srmg_ctx *ctx, double *q, const double *ne, const double *nio
 int srmg_netcharge_dev(srmg_ctx *ctx, double *q, const double *ne, const double *nion, int64_t nblk_alloc);
 /* restrict_full!(u, conn) (src/restrict.jl:43-47): restrict_level! for levels L..2. */
 int srmg_restrict_full_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc);
+/* rhs_level!(q1, q, tree[level], lpldisc, geometry) (src/multigrid.jl:363-388): q1 = R q
+ * on the valid cells of every block of the level; R is the identity for order 2 and
+ * the compact 5-point right-hand side (divided by 12) for SRMG_OP_LAPLACIAN4.  q's
+ * ghosts must be filled.  Bit-exact.  derivs! (src/streamer.jl:314-318) calls it per
+ * level between fill_ghost!(q) and fill_ghost!(q1). */
+int srmg_rhs_level(srmg_ctx *ctx, double *q1, const double *q, int64_t nblk_alloc, int level, int op,
+                   int geom);
+int srmg_rhs_level_dev(srmg_ctx *ctx, double *q1, const double *q, int64_t nblk_alloc, int level, int op,
+                       int geom);
 /* electric_field!(tree, e, eabs, u, h, t, e0) (src/multigrid.jl:421-449, the method for
  * a constant background field e0 = (e0_r, e0_z), :451).  e is a VectorBlockField{2,16,2}:
  * 21 x 21 x 2 doubles per block (component d at offset 441 d); for d = r, z and every

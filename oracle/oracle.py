@@ -60,7 +60,9 @@ def lib():
             "orc_copyto_level": (None, [PP, PP, TP, I]),
             "orc_diffto_level": (None, [PP, PP, PP, TP, I]),
             "orc_gs_level": (None, [PP, PP, D, D, TP, I, OP, I]),
+            "orc_gs4_level": (None, [PP, PP, D, D, TP, I, OP, I, I]),
             "orc_gs_iter": (None, [PP, PP, D, D, I, I, TP, OP]),
+            "orc_rhs_level": (None, [PP, PP, TP, I, OP]),
             "orc_residual_level": (None, [PP, PP, PP, D, TP, I, OP]),
             "orc_residual_postrestrict_level": (None, [PP, PP, PP, D, TP, I, OP]),
             "orc_vcycle": (None, [PP, PP, PP, PP, D, TP, OP, I, I, I, I, D]),
@@ -153,6 +155,9 @@ class Oracle:
     def fill_ghost_all(self, u):
         for l in range(1, self.ot.nlev + 1):
             self.fill_ghost(u, l)
+
+    def rhs_level(self, q1, q, l):
+        lib().orc_rhs_level(_ptr(q1), _ptr(q), self.ot.ref, l, ctypes.byref(self.op))
 
     def vcycle(self, u, b, r, u1, lmax=0, ndown=2, ntop=4, nup=2, omega=1.0, s=None):
         lib().orc_vcycle(_ptr(u), _ptr(b), _ptr(r), _ptr(u1), self.p.s if s is None else s,

@@ -282,6 +282,66 @@ static inline double diagelm(const orc_operator *op, double s) {
     return (op->op == 1) ? (-4 - s * op->k2) : -4.0;
 }
 
+/* ---- order-4 compact discretisation, LaplacianDiscretization{2,4} ------------------
+ * applystencil (src/laplacian.jl:133-202): @stencil over a 3x3 literal whose rows are
+ * offsets along dimension 1 and columns along dimension 2, walked column-major, so the
+ * coefficient k = (d1 + 1) + 3 (d2 + 1) is accumulated k = 0..8 (v = 0; v += c_k u),
+ * then divided by 6.  Cylindrical coefficients are integer polynomials of the 1-based
+ * global index i along the radial dimension, divided as Float64 (Int / Int). */
+static void coeffs9(int geom, int64_t ir, int64_t iz, double c[9]) {
+    if (geom == 0) {
+        static const double cart[9] = {1, 4, 1, 4, -20, 4, 1, 4, 1};
+        for (int k = 0; k < 9; k++) c[k] = cart[k];
+        return;
+    }
+    const int64_t i = (geom == 1) ? ir : iz;
+    const double am = (double)(2 * (i - 1)) / (double)(2 * i - 1);   /* 2(i-1)/(2i-1) */
+    const double ap = (double)(2 * i) / (double)(2 * i - 1);         /* 2i/(2i-1) */
+    const int64_t q = 2 * i - 1;
+    const int64_t p1 = -2 + 9 * i - 16 * i * i + 8 * i * i * i;
+    const int64_t p2 = 1 - 5 * i + 5 * i * i;
+    const int64_t p3 = 1 + i - 8 * i * i + 8 * i * i * i;
+    const double em = (double)(4 * p1) / (double)(q * q * q);        /* radial -1 neighbour */
+    const double cc = (double)(-16 * p2) / (double)((1 - 2 * i) * (1 - 2 * i));
+    const double ep = (double)(4 * p3) / (double)(q * q * q);        /* radial +1 neighbour */
+    if (geom == 1) {  /* r = dimension 1 (src/laplacian.jl:156-164) */
+        const double v[9] = {am, 4, ap, em, cc, ep, am, 4, ap};
+        for (int k = 0; k < 9; k++) c[k] = v[k];
+    } else {          /* r = dimension 2 (src/laplacian.jl:176-184) */
+        const double v[9] = {am, em, am, 4, cc, 4, ap, ep, ap};
+        for (int k = 0; k < 9; k++) c[k] = v[k];
+    }
+}
+
+static inline double apply9(const double *ub, int S, int i, int j, const double c[9]) {
+    double v = 0.0;
+    for (int d2 = -1; d2 <= 1; d2++)
+        for (int d1 = -1; d1 <= 1; d1++) v += c[(d1 + 1) + 3 * (d2 + 1)] * ub[IX(S, i + d1, j + d2, 1)];
+    return v / 6;
+}
+
+/* diagelm for order 4 (src/laplacian.jl:150-151, 205-209): -20/6, or
+ * -16 (1 - 5i + 5i^2) / (1 - 2i)^2 / 6 with i the radial global index. */
+static inline double diagelm4(int geom, int64_t ir, int64_t iz) {
+    if (geom == 0) return -20.0 / 6.0;
+    const int64_t i = (geom == 1) ? ir : iz;
+    return (double)(-16 * (1 - 5 * i + 5 * i * i)) / (double)((1 - 2 * i) * (1 - 2 * i)) / 6;
+}
+
+/* The :lhs stencil of any supported discretisation at 1-based (i, j) with global
+ * indices (J1, J2), scale s. */
+static inline double lhs_apply(const orc_operator *op, double s, const double *ub, int S, int i, int j,
+                               int64_t J1, int64_t J2) {
+    if (op->op == 2) {
+        double c[9];
+        coeffs9(op->geom, J1, J2, c);
+        return apply9(ub, S, i, j, c);
+    }
+    stencil5 w;
+    weights(op, s, J1, J2, &w);
+    return apply5(ub, S, i, j, &w);
+}
+
 /* gauss_seidel!(..., RedBlack{P}) (src/multigrid.jl:153-180) on every block of level l
  * (gauss_seidel_level!, :238-243).  Colour P updates the cells whose 1-based local
  * indices satisfy (I1 - G - 1) % 2 == P xor (I2 & 1). */
@@ -312,10 +372,49 @@ void orc_gs_level(double *u, const double *b, double omega, double s, const orc_
     }
 }
 
-/* gauss_seidel_iter! for order 2 (src/multigrid.jl:250-265): red, copy+bnd ghosts,
- * black, copy+bnd ghosts.  Refinement-boundary ghosts stay frozen. */
+/* gauss_seidel!(..., FourColors{P1,P2}) (src/multigrid.jl:206-232): the cells
+ * (G+1+2a+P1, G+1+2b+P2) of every block of level l, updated as
+ * u -= omega (Lu + s b) / c (no fused operations). */
+void orc_gs4_level(double *u, const double *b, double omega, double s, const orc_tree *t, int l,
+                   const orc_operator *op, int p1, int p2) {
+    const int M = t->M, G = t->G, S = M + 2 * G;
+    const orc_pair *p = t->pairs[l - 1];
+    const int64_t n = t->npairs[l - 1];
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < n; k++) {
+        const int64_t blk = p[k].blk;
+        const int64_t g0r = (int64_t)M * (p[k].coord[0] - 1) + 1;
+        const int64_t g0z = (int64_t)M * (p[k].coord[1] - 1) + 1;
+        double *ub = u + (int64_t)S * S * (blk - 1);
+        const double *bb = b + (int64_t)S * S * (blk - 1);
+        for (int i2 = G + 1; i2 <= G + M; i2 += 2)
+            for (int i1 = G + 1; i1 <= G + M; i1 += 2) {
+                const int I1 = i1 + p1, I2 = i2 + p2;
+                const int64_t J1 = I1 - G + g0r - 1, J2 = I2 - G + g0z - 1;
+                const double c = diagelm4(op->geom, J1, J2);
+                double cf[9];
+                coeffs9(op->geom, J1, J2, cf);
+                const double Lu = apply9(ub, S, I1, I2, cf);
+                const double upd = omega * (Lu + s * bb[IX(S, I1, I2, 1)]) / c;
+                ub[IX(S, I1, I2, 1)] = ub[IX(S, I1, I2, 1)] - upd;
+            }
+    }
+}
+
+/* gauss_seidel_iter! (src/multigrid.jl:250-295): order 2 runs red, copy+bnd ghosts,
+ * black, copy+bnd ghosts; order 4 the four colours {0,0}, {0,1}, {1,0}, {1,1}, each
+ * followed by copy+bnd ghosts.  Refinement-boundary ghosts stay frozen. */
 void orc_gs_iter(double *u, const double *b, double omega, double s, int n, int l,
                  const orc_tree *t, const orc_operator *op) {
+    if (op->op == 2) {
+        for (int it = 0; it < n; it++)
+            for (int c = 0; c < 4; c++) {
+                orc_gs4_level(u, b, omega, s, t, l, op, c >> 1, c & 1);
+                orc_fill_ghost_copy(u, t, l);
+                orc_fill_ghost_bnd(u, t, l, op->bc);
+            }
+        return;
+    }
     for (int it = 0; it < n; it++) {
         orc_gs_level(u, b, omega, s, t, l, op, 0);
         orc_fill_ghost_copy(u, t, l);
@@ -340,9 +439,7 @@ void orc_residual_level(double *r, const double *u, const double *b, double s,
         const double *ub = u + (int64_t)S * S * (blk - 1);
         for (int I2 = G + 1; I2 <= G + M; I2++)
             for (int I1 = G + 1; I1 <= G + M; I1++) {
-                stencil5 w;
-                weights(op, s, I1 - G + g0r - 1, I2 - G + g0z - 1, &w);
-                const double Lu = apply5(ub, S, I1, I2, &w);
+                const double Lu = lhs_apply(op, s, ub, S, I1, I2, I1 - G + g0r - 1, I2 - G + g0z - 1);
                 const int64_t o = IX(S, I1, I2, blk);
                 r[o] = -(b[o] + Lu / s);
             }
@@ -367,9 +464,7 @@ void orc_residual_postrestrict_level(double *bfield, const double *u, const doub
         const double *ub = u + (int64_t)S * S * (blk - 1);
         for (int I2 = lo[1]; I2 <= hi[1]; I2++)
             for (int I1 = lo[0]; I1 <= hi[0]; I1++) {
-                stencil5 w;
-                weights(op, s, I1 - G + g0r - 1, I2 - G + g0z - 1, &w);
-                const double Lu = apply5(ub, S, I1, I2, &w);
+                const double Lu = lhs_apply(op, s, ub, S, I1, I2, I1 - G + g0r - 1, I2 - G + g0z - 1);
                 const int64_t o = IX(S, I1, I2, blk);
                 bfield[o] = -(r[o] + Lu / s);
             }
@@ -499,6 +594,50 @@ int orc_solve(double *u, double *b, double *r, double *u1, double s, const orc_t
 }
 
 /* ---- stage preparation and post-processing --------------------------------------- */
+
+/* rhs_level! over rhs! (src/multigrid.jl:363-388): q1 = R q on the valid cells of every
+ * block of level l.  Order 2: the identity (src/laplacian.jl:86-91,120-125,
+ * src/helmholtz.jl:27-32,59-64).  Order 4: the compact right-hand side
+ * (src/laplacian.jl:141-148,166-173,186-193), a 3x3 literal walked column-major
+ * (v = 0; v += c u) over its nonzero entries, then divided by 12. */
+void orc_rhs_level(double *q1, const double *q, const orc_tree *t, int l, const orc_operator *op) {
+    const int M = t->M, G = t->G, S = M + 2 * G;
+    const orc_pair *p = t->pairs[l - 1];
+    const int64_t n = t->npairs[l - 1];
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < n; k++) {
+        const int64_t blk = p[k].blk;
+        const int64_t g0r = (int64_t)M * (p[k].coord[0] - 1) + 1;
+        const int64_t g0z = (int64_t)M * (p[k].coord[1] - 1) + 1;
+        const double *qb = q + (int64_t)S * S * (blk - 1);
+        for (int I2 = G + 1; I2 <= G + M; I2++)
+            for (int I1 = G + 1; I1 <= G + M; I1++) {
+                const int64_t o = IX(S, I1, I2, blk);
+                if (op->op != 2) {
+                    q1[o] = q[o];
+                    continue;
+                }
+                /* nonzero entries in walk order: (0,-1), (-1,0), (0,0), (1,0), (0,1) */
+                double wzm = 1, wrm = 1, wrp = 1, wzp = 1;
+                if (op->geom == 1) {
+                    const int64_t i = I1 - G + g0r - 1;
+                    wrm = (double)(2 * i - 2) / (double)(2 * i - 1);
+                    wrp = (double)(2 * i) / (double)(2 * i - 1);
+                } else if (op->geom == 2) {
+                    const int64_t i = I2 - G + g0z - 1;
+                    wzm = (double)(2 * i - 2) / (double)(2 * i - 1);
+                    wzp = (double)(2 * i) / (double)(2 * i - 1);
+                }
+                double v = 0.0;
+                v += wzm * qb[IX(S, I1, I2 - 1, 1)];
+                v += wrm * qb[IX(S, I1 - 1, I2, 1)];
+                v += 8 * qb[IX(S, I1, I2, 1)];
+                v += wrp * qb[IX(S, I1 + 1, I2, 1)];
+                v += wzp * qb[IX(S, I1, I2 + 1, 1)];
+                q1[o] = v / 12;
+            }
+    }
+}
 
 /* netcharge! (src/streamer.jl:369-373): q[I] = dot(n[I], species_charge) over the valid
  * cells of every block; NetIonization charges are (-1, +1) (src/chemistry.jl:80), so

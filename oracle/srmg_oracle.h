@@ -49,7 +49,8 @@ typedef struct {
     int64_t *coord_of;      /* 2 * nblk_alloc entries, owned by the caller */
 } orc_tree;
 
-/* Operator: op 0 = LaplacianDiscretization{2,2}, 1 = HelmholtzDiscretization{2,2}(k2).
+/* Operator: op 0 = LaplacianDiscretization{2,2}, 1 = HelmholtzDiscretization{2,2}(k2),
+ * 2 = LaplacianDiscretization{2,4} (compact order 4; needs a BoxStencil connectivity).
  * geom 0 = CartesianGeometry, 1 = CylindricalGeometry{1}, 2 = CylindricalGeometry{2}. */
 typedef struct { int op; double k2; int geom; int8_t bc[9]; } orc_operator;
 
@@ -68,6 +69,8 @@ void orc_diffto_level(double *dst, const double *a1, const double *a2, const orc
 
 void orc_gs_level(double *u, const double *b, double omega, double s, const orc_tree *t, int l,
                   const orc_operator *op, int parity);
+void orc_gs4_level(double *u, const double *b, double omega, double s, const orc_tree *t, int l,
+                   const orc_operator *op, int p1, int p2);
 void orc_gs_iter(double *u, const double *b, double omega, double s, int n, int l,
                  const orc_tree *t, const orc_operator *op);
 void orc_residual_level(double *r, const double *u, const double *b, double s,
@@ -91,6 +94,7 @@ int orc_solve(double *u, double *b, double *r, double *u1, double s, const orc_t
               double tol, int max_cycles, double *rel);
 
 /* Stage preparation and post-processing of derivs! (src/streamer.jl:309-351). */
+void orc_rhs_level(double *q1, const double *q, const orc_tree *t, int l, const orc_operator *op);
 void orc_netcharge(double *q, const double *ne, const double *nion, const orc_tree *t);
 void orc_electric_field(double *e, double *eabs, const double *u, double h, const double e0[2],
                         const orc_tree *t);

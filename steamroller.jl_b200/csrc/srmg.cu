@@ -146,6 +146,13 @@ static int face_of(const int64_t f[2]) {
   return -1;
 }
 
+// Corner index of a diagonal direction (both components +-1), else -1:
+// q = (fr + 1) / 2 + 2 (fz + 1) / 2.
+static int corner_of(const int64_t f[2]) {
+  if ((f[0] != -1 && f[0] != 1) || (f[1] != -1 && f[1] != 1)) return -1;
+  return (int)((f[0] + 1) / 2 + 2 * ((f[1] + 1) / 2));
+}
+
 // Validate and upload a tree (or a forest: item_of[blk] gives the item of every 1-based
 // block id, each item's blocks contiguous within every level's list).
 int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_pair *const *pairs,
@@ -193,11 +200,13 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
   std::vector<int4> binfo(max_blk + 1, make_int4(0, 0, 0, 0));
   std::vector<int4> bface(4 * (max_blk + 1), make_int4(FACE_NONE, 0, 0, -1));
   std::vector<int4> bkids(max_blk + 1, make_int4(-1, -1, -1, -1));
-  std::vector<std::vector<int4>> hb(nlev), hf(nlev), hc(nlev);
+  std::vector<std::vector<int4>> hb(nlev), hf(nlev), hc(nlev), hcf(nlev);
+  bool corners = false;
   for (int l = 0; l < nlev; l++) {
     const int lv = l + 1;
     hb[l].resize(npairs[l]);
     hf[l].assign(4 * npairs[l], make_int4(FACE_NONE, 0, 0, 0));
+    hcf[l].assign(4 * npairs[l], make_int4(FACE_NONE, 0, 0, 0));
     for (int64_t p = 0; p < npairs[l]; p++) {
       const srmg_pair &pr = pairs[l][p];
       hb[l][p] = make_int4((int)(pr.blk - 1), (int)pr.coord[0], (int)pr.coord[1], 0);
@@ -210,15 +219,30 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
       slot = v;
       return SRMG_OK;
     };
+    // diagonal edges of a BoxStencil connectivity: the 2 x 2 corner ghosts
+    auto set_corner = [&](int64_t blk, int q, int4 v) -> int {
+      int4 &slot = hcf[l][4 * idx_of[blk] + q];
+      if (slot.x != FACE_NONE)
+        return fail(ctx, SRMG_ERR_BADTREE, "level %d: corner %d of block %lld written by two edges",
+                    lv, q, (long long)blk);
+      slot = v;
+      corners = true;
+      return SRMG_OK;
+    };
     if (nnb[l] < 0 || (nnb[l] > 0 && !nb[l])) return fail(ctx, SRMG_ERR_BADTREE, "level %d: neighbours", lv);
     for (int64_t k = 0; k < nnb[l]; k++) {
       const srmg_neighbor &e = nb[l][k];
       const int64_t mf[2] = {-e.face[0], -e.face[1]};
       const int f = face_of(mf);
-      if (f < 0) return fail(ctx, SRMG_ERR_UNSUPPORTED, "level %d: neighbour face is not a star direction", lv);
       if (!at_level(e.from, lv) || !at_level(e.to, lv))
         return fail(ctx, SRMG_ERR_BADTREE, "level %d: neighbour edge %lld->%lld not on this level", lv,
                     (long long)e.from, (long long)e.to);
+      if (f < 0) {
+        const int q = corner_of(mf);
+        if (q < 0) return fail(ctx, SRMG_ERR_UNSUPPORTED, "level %d: neighbour face is not a box direction", lv);
+        RC(set_corner(e.to, q, make_int4(FACE_NEIGHBOR, (int)(e.from - 1), 0, 0)));
+        continue;
+      }
       RC(set_face(e.to, f, make_int4(FACE_NEIGHBOR, (int)(e.from - 1), 0, 0)));
       {
         int4 &pf = bface[4 * (e.to - 1) + f];
@@ -235,11 +259,20 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
     for (int64_t k = 0; k < nbd[l]; k++) {
       const srmg_boundary &e = bd[l][k];
       const int f = face_of(e.face);
-      if (f < 0 || e.bnd[0] != e.face[0] || e.bnd[1] != e.face[1])
-        return fail(ctx, SRMG_ERR_UNSUPPORTED, "level %d: boundary edge is not a star face", lv);
       if (!at_level(e.block, lv) || e.level != lv)
         return fail(ctx, SRMG_ERR_BADTREE, "level %d: boundary edge of block %lld not on this level",
                     lv, (long long)e.block);
+      if (f < 0) {
+        // a diagonal step leaves the domain along bnd's nonzero components
+        const int q = corner_of(e.face);
+        if (q < 0 || (e.bnd[0] != 0 && e.bnd[0] != e.face[0]) || (e.bnd[1] != 0 && e.bnd[1] != e.face[1]) ||
+            (e.bnd[0] == 0 && e.bnd[1] == 0))
+          return fail(ctx, SRMG_ERR_UNSUPPORTED, "level %d: malformed boundary corner", lv);
+        RC(set_corner(e.block, q, make_int4(FACE_BOUNDARY, 0, (int)e.bnd[0], (int)e.bnd[1])));
+        continue;
+      }
+      if (e.bnd[0] != e.face[0] || e.bnd[1] != e.face[1])
+        return fail(ctx, SRMG_ERR_UNSUPPORTED, "level %d: boundary edge is not a star face", lv);
       RC(set_face(e.block, f, make_int4(FACE_BOUNDARY, 0, 0, 0)));
       bface[4 * (e.block - 1) + f].x = FACE_BOUNDARY;
     }
@@ -247,11 +280,17 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
     for (int64_t k = 0; k < nrb[l]; k++) {
       const srmg_refbnd &e = rb[l][k];
       const int f = face_of(e.face);
-      if (f < 0) return fail(ctx, SRMG_ERR_UNSUPPORTED, "level %d: refinement face is not a star direction", lv);
       if (lv < 2 || !at_level(e.fine, lv) || !at_level(e.coarse, lv - 1) || e.subblock[0] < 1 ||
           e.subblock[0] > 2 || e.subblock[1] < 1 || e.subblock[1] > 2)
         return fail(ctx, SRMG_ERR_BADTREE, "level %d: malformed refinement boundary %lld/%lld", lv,
                     (long long)e.fine, (long long)e.coarse);
+      if (f < 0) {
+        const int q = corner_of(e.face);
+        if (q < 0) return fail(ctx, SRMG_ERR_UNSUPPORTED, "level %d: refinement face is not a box direction", lv);
+        RC(set_corner(e.fine, q, make_int4(FACE_REFBND, (int)(e.coarse - 1), (int)e.subblock[0],
+                                           (int)e.subblock[1])));
+        continue;
+      }
       RC(set_face(e.fine, f, make_int4(FACE_REFBND, (int)(e.coarse - 1), (int)e.subblock[0],
                                        (int)e.subblock[1])));
       {
@@ -381,12 +420,13 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
     off += (bytes + 255) & ~size_t(255);
     return o;
   };
-  std::vector<size_t> ob(nlev), of(nlev), oc(nlev), orr(nlev);
+  std::vector<size_t> ob(nlev), of(nlev), oc(nlev), orr(nlev), ocf(nlev, 0);
   for (int l = 0; l < nlev; l++) {
     orr[l] = take(hr[l].size() * sizeof(int4));
     ob[l] = take(hb[l].size() * sizeof(int4));
     of[l] = take(hf[l].size() * sizeof(int4));
     oc[l] = take(hc[l].size() * sizeof(int4));
+    if (corners) ocf[l] = take(hcf[l].size() * sizeof(int4));
   }
   const size_t ocoord = take((max_blk + 1) * sizeof(int2));
   const size_t owm = take(wn * sizeof(double)), owp = take(wn * sizeof(double));
@@ -405,6 +445,7 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
     memcpy(host.data() + ob[l], hb[l].data(), hb[l].size() * sizeof(int4));
     memcpy(host.data() + of[l], hf[l].data(), hf[l].size() * sizeof(int4));
     memcpy(host.data() + oc[l], hc[l].data(), hc[l].size() * sizeof(int4));
+    if (corners) memcpy(host.data() + ocf[l], hcf[l].data(), hcf[l].size() * sizeof(int4));
   }
   // coord_of indexed by 0-based block id
   std::vector<int2> c0(max_blk + 1, make_int2(0, 0));
@@ -444,6 +485,7 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
     ctx->lv[l].rec = (int4 *)(base + orr[l]);
     ctx->lv[l].faces = (int4 *)(base + of[l]);
     ctx->lv[l].child = (int4 *)(base + oc[l]);
+    ctx->lv[l].cfaces = corners ? (int4 *)(base + ocf[l]) : nullptr;
     ctx->nblk_host[l] = ctx->lv[l].nblk;
     ctx->nch_host[l] = ctx->lv[l].nch;
   }
@@ -454,6 +496,7 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
   ctx->d_wp32 = (float *)(base + owp32);
   ctx->d_wrow64 = (double *)(base + owr);
   ctx->d_wrow32 = (float *)(base + owr32);
+  ctx->has_corners = corners;
   ctx->refbnd_levels = 0;
   for (int l = 0; l < nlev; l++)
     if (nrb[l] > 0 && l + 1 < 32) ctx->refbnd_levels |= 1u << (l + 1);
@@ -516,8 +559,10 @@ int srmg::check_call(srmg_ctx *ctx, int64_t nblk_alloc, int op, int geom, const 
   if (nblk_alloc < ctx->max_blk)
     return fail(ctx, SRMG_ERR_BADARG, "field holds %lld blocks but the tree uses block %lld",
                 (long long)nblk_alloc, (long long)ctx->max_blk);
-  if (op != SRMG_OP_LAPLACIAN && op != SRMG_OP_HELMHOLTZ)
+  if (op != SRMG_OP_LAPLACIAN && op != SRMG_OP_HELMHOLTZ && op != SRMG_OP_LAPLACIAN4)
     return fail(ctx, SRMG_ERR_UNSUPPORTED, "unsupported discretisation %d", op);
+  if (op == SRMG_OP_LAPLACIAN4 && !ctx->has_corners)
+    return fail(ctx, SRMG_ERR_UNSUPPORTED, "the order-4 discretisation needs a BoxStencil connectivity");
   if (geom < 0 || geom > 2) return fail(ctx, SRMG_ERR_UNSUPPORTED, "unsupported geometry %d", geom);
   if (bc) {
     for (int i = 0; i < 9; i++)
@@ -565,8 +610,9 @@ OpParams<T> srmg::op_params(int op, int geom, double k2, double sl, double omega
   p.s = (T)sl;
   const double centre = (op == SRMG_OP_HELMHOLTZ) ? (-4.0 - sl * k2) : -4.0;
   p.centre = (T)centre;
-  const double c = (op == SRMG_OP_HELMHOLTZ) ? (-4 - sl * k2) : -4.0;  // diagelm
+  const double c = (op == SRMG_OP_HELMHOLTZ) ? (-4 - sl * k2) : -4.0;  // diagelm (order 2)
   p.nwc = (T)(-(omega / c));
+  p.omega = (T)omega;
   return p;
 }
 template OpParams<double> srmg::op_params<double>(int, int, double, double, double);
@@ -582,9 +628,24 @@ int srmg::L_fill_ghost(srmg_ctx *ctx, T *u, int l, const Signs &sg, int mask) {
   const DevLevel &L = ctx->lv[l - 1];
   if (L.nblk == 0) return SRMG_OK;
   const int threads = 256;
-  k_fill_ghost<T><<<grid_for((int64_t)L.nblk * 4 * 32, threads, kGridCap), threads, 0, ctx->stream>>>(
-      u, L.view(l), sg, mask);
-  ctx->launches++;
+  const int gf = grid_for((int64_t)L.nblk * 4 * 32, threads, kGridCap);
+  if (!L.cfaces) {
+    // star faces only: the three passes touch disjoint cells and read none of each
+    // other's results, so one launch does them all
+    k_fill_ghost<T><<<gf, threads, 0, ctx->stream>>>(u, L.view(l), sg, mask);
+    ctx->launches++;
+    return SRMG_OK;
+  }
+  // BoxStencil tree: a boundary corner whose bnd is zero along one dimension mirrors
+  // the adjacent face's ghost cells, so copy, boundary and interpolation run as three
+  // ordered passes (fill_ghost!, src/connectivity.jl:155-159), faces and corners each
+  const int gc = grid_for((int64_t)L.nblk * 16, threads, kGridCap);
+  for (int phase = 1; phase <= 4; phase <<= 1) {
+    if (!(mask & phase)) continue;
+    k_fill_ghost<T><<<gf, threads, 0, ctx->stream>>>(u, L.view(l), sg, phase);
+    k_fill_corner<T><<<gc, threads, 0, ctx->stream>>>(u, L.view(l), sg, phase);
+    ctx->launches += 2;
+  }
   return SRMG_OK;
 }
 
@@ -593,6 +654,13 @@ int srmg::L_gs_colour(srmg_ctx *ctx, T *u, const T *b, int l, const OpParams<T> 
   const DevLevel &L = ctx->lv[l - 1];
   if (L.nblk == 0) return SRMG_OK;
   const int threads = 128;
+  if (p.op == SRMG_OP_LAPLACIAN4) {
+    // FourColors{parity >> 1, parity & 1}
+    k_gs4<T><<<grid_for((int64_t)L.nblk * 64, threads, kGridCap), threads, 0, ctx->stream>>>(
+        u, b, L.view(l), p, parity >> 1, parity & 1);
+    ctx->launches++;
+    return SRMG_OK;
+  }
   k_gs_colour<T><<<grid_for((int64_t)L.nblk * 128, threads, kGridCap), threads, 0, ctx->stream>>>(
       u, b, L.view(l), p, wtab<T>(ctx), parity);
   ctx->launches++;
@@ -602,6 +670,16 @@ int srmg::L_gs_colour(srmg_ctx *ctx, T *u, const T *b, int l, const OpParams<T> 
 template <typename T>
 int srmg::L_gs_iter(srmg_ctx *ctx, T *u, const T *b, int l, const OpParams<T> &p, int n,
                     const Signs &sg) {
+  if (p.op == SRMG_OP_LAPLACIAN4) {
+    // four colours {0,0}, {0,1}, {1,0}, {1,1}, each followed by copy and boundary ghosts
+    // (src/multigrid.jl:268-295)
+    for (int i = 0; i < n; i++)
+      for (int c = 0; c < 4; c++) {
+        RC(L_gs_colour<T>(ctx, u, b, l, p, c));
+        RC(L_fill_ghost<T>(ctx, u, l, sg, 3));
+      }
+    return SRMG_OK;
+  }
   for (int i = 0; i < n; i++) {
     RC(L_gs_colour<T>(ctx, u, b, l, p, 0));
     RC(L_fill_ghost<T>(ctx, u, l, sg, 3));
@@ -682,7 +760,10 @@ int srmg::vcycle_dev(srmg_ctx *ctx, T *u, T *b, T *r, T *u1, double s, int op, d
   // Bulk copies need 16-byte aligned block tiles.
   const bool aligned = ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(b) |
                          reinterpret_cast<uintptr_t>(r) | reinterpret_cast<uintptr_t>(u1)) & 15) == 0;
-  if (ctx->use_engine && aligned && ndown >= 1 && ntop >= 1 && nup >= 1 && ctx->nlev <= 30) {
+  // The engine's ghost pushes cover the four star faces only; trees with corner ghosts
+  // (BoxStencil connectivity) and the order-4 stencil use the per-operation kernels.
+  if (ctx->use_engine && aligned && !ctx->has_corners && op != SRMG_OP_LAPLACIAN4 && ndown >= 1 &&
+      ntop >= 1 && nup >= 1 && ctx->nlev <= 30) {
     ItemTabs tabs;
     const std::vector<ItemSpec> specs = uniform_items(ctx, s, op, k2, bc_of(sg).data());
     RC(prepare_items(ctx, specs.data(), geom, omega, false, 0, 0.0, &tabs));
@@ -884,7 +965,8 @@ extern "C" int srmg_gs_level_dev(srmg_ctx *ctx, double *u, const double *b, int6
                                  int level, double omega, double sl, int op, double k2, int geom,
                                  int parity) {
   RC(check_call(ctx, nblk_alloc, op, geom, nullptr));
-  if (!u || !b || level < 1 || level > ctx->nlev || (parity != 0 && parity != 1))
+  const int ncol = op == SRMG_OP_LAPLACIAN4 ? 4 : 2;
+  if (!u || !b || level < 1 || level > ctx->nlev || parity < 0 || parity >= ncol)
     return fail(ctx, SRMG_ERR_BADARG, "gs_level: bad arguments");
   RC(L_gs_colour<double>(ctx, u, b, level, op_params<double>(op, geom, k2, sl, omega), parity));
   CK(cudaGetLastError());
@@ -898,7 +980,7 @@ extern "C" int srmg_gs_iter_dev(srmg_ctx *ctx, double *u, const double *b, int64
   if (!u || !b || level < 1 || level > ctx->nlev || n < 0)
     return fail(ctx, SRMG_ERR_BADARG, "gs_iter: bad arguments");
   const bool aligned = ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(b)) & 15) == 0;
-  if (ctx->use_engine && aligned) {
+  if (ctx->use_engine && aligned && !ctx->has_corners && op != SRMG_OP_LAPLACIAN4) {
     ItemTabs tabs;
     const std::vector<ItemSpec> specs = uniform_items(ctx, sl, op, k2, bc);
     RC(prepare_items(ctx, specs.data(), geom, omega, false, level, sl, &tabs));
@@ -924,6 +1006,20 @@ extern "C" int srmg_restrict_level_dev(srmg_ctx *ctx, double *u, int64_t nblk_al
   RC(check_call(ctx, nblk_alloc, 0, 0, nullptr));
   if (!u || level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "restrict_level: bad level");
   RC(L_restrict<double>(ctx, u, level));
+  CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+extern "C" int srmg_rhs_level_dev(srmg_ctx *ctx, double *q1, const double *q, int64_t nblk_alloc, int level,
+                                  int op, int geom) {
+  RC(check_call(ctx, nblk_alloc, op, geom, nullptr));
+  if (!q1 || !q || level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "rhs_level: bad arguments");
+  const DevLevel &L = ctx->lv[level - 1];
+  if (L.nblk > 0) {
+    k_rhs<double><<<grid_for((int64_t)L.nblk * 256, 256, kGridCap), 256, 0, ctx->stream>>>(q1, q, L.view(level),
+                                                                                         op, geom);
+    ctx->launches++;
+  }
   CK(cudaGetLastError());
   return SRMG_OK;
 }
@@ -1015,6 +1111,19 @@ extern "C" int srmg_resnorm(srmg_ctx *ctx, double *r, const double *b, const dou
   RC(stage_in(ctx, 0, u, nblk_alloc, &du));
   RC(stage_in(ctx, 1, b, nblk_alloc, &db));
   RC(srmg_resnorm_dev(ctx, r, db, du, nblk_alloc, s, op, k2, geom, bc, out));
+  return SRMG_OK;
+}
+
+extern "C" int srmg_rhs_level(srmg_ctx *ctx, double *q1, const double *q, int64_t nblk_alloc, int level, int op,
+                              int geom) {
+  RC(check_call(ctx, nblk_alloc, op, geom, nullptr));
+  if (!q1 || !q) return fail(ctx, SRMG_ERR_BADARG, "srmg_rhs_level: null field");
+  double *dq1, *dq;
+  RC(stage_in(ctx, 0, q1, nblk_alloc, &dq1));
+  RC(stage_in(ctx, 1, q, nblk_alloc, &dq));
+  RC(srmg_rhs_level_dev(ctx, dq1, dq, nblk_alloc, level, op, geom));
+  RC(stage_out(ctx, q1, dq1, nblk_alloc));
+  CK(cudaStreamSynchronize(ctx->stream));
   return SRMG_OK;
 }
 

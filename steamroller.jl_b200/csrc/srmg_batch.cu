@@ -40,6 +40,8 @@ extern "C" int srmg_batch_set(srmg_ctx *ctx, int nitems, const srmg_item *items,
       return fail(ctx, SRMG_ERR_NOTREE, "item %d: its context holds no tree", k);
     if (items[k].op != SRMG_OP_LAPLACIAN && items[k].op != SRMG_OP_HELMHOLTZ)
       return fail(ctx, SRMG_ERR_UNSUPPORTED, "item %d: unsupported discretisation %d", k, items[k].op);
+    if (t->has_corners)
+      return fail(ctx, SRMG_ERR_UNSUPPORTED, "item %d: batches need a StarStencil connectivity", k);
     for (int i = 0; i < 9; i++)
       if (items[k].bc[i] < -1 || items[k].bc[i] > 1)
         return fail(ctx, SRMG_ERR_BADARG, "item %d: boundary table entries must be -1, 0 or 1", k);

@@ -1070,6 +1070,8 @@ extern "C" int srmg_cnn_pack_dev(srmg_ctx *ctx, const double *f, const double *g
                                  int op, double k2, int geom, const int8_t bc[9], uint16_t *x, double *scale,
                                  int *blk, int max_samples) {
   RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  if (op == SRMG_OP_LAPLACIAN4)
+    return fail(ctx, SRMG_ERR_UNSUPPORTED, "the learned warm start supports order-2 discretisations");
   if (!f || !g || !x || !scale || !blk) return fail(ctx, SRMG_ERR_BADARG, "srmg_cnn_pack_dev: null argument");
   if (max_samples < ctx->nleaf)
     return fail(ctx, SRMG_ERR_BADARG, "srmg_cnn_pack_dev: room for %d samples, the tree has %d", max_samples,
@@ -1088,6 +1090,8 @@ extern "C" int srmg_cnn_predict_dev(srmg_ctx *ctx, srmg_cnn *net, double *u, con
                                     const double *phi2, const double *b2, int64_t nblk_alloc, double s, int op,
                                     double k2, int geom, const int8_t bc[9], int *which, double *resid) {
   RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  if (op == SRMG_OP_LAPLACIAN4)
+    return fail(ctx, SRMG_ERR_UNSUPPORTED, "the learned warm start supports order-2 discretisations");
   if (!net || !u || !b || !b1 || !phi2 || !b2) return fail(ctx, SRMG_ERR_BADARG, "srmg_cnn_predict_dev: null argument");
   if (net->device != ctx->device) return fail(ctx, SRMG_ERR_BADARG, "network and context on different devices");
   const int n = ctx->nleaf;

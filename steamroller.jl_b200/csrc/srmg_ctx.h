@@ -19,7 +19,8 @@ struct DevLevel {
   int4 *faces = nullptr;
   int4 *child = nullptr;
   int4 *rec = nullptr;   // engine records: 5 int4 per block ({blk, cr, cz, child_mask}, face 0..3)
-  LevelView view(int level) const { return LevelView{blocks, faces, child, nblk, nch, level}; }
+  int4 *cfaces = nullptr;  // BoxStencil trees: 4 corner faces per block, else null
+  LevelView view(int level) const { return LevelView{blocks, faces, child, nblk, nch, level, cfaces}; }
 };
 
 // A device buffer that only grows.
@@ -86,6 +87,7 @@ struct srmg_ctx {
                              // (4 measured fastest on the 1.5M- and 10M-leaf trees)
   bool use_engine = true;
   unsigned refbnd_levels = 0;  // bit l: level l has refinement-boundary faces
+  bool has_corners = false;    // the tree came with a BoxStencil connectivity (diagonal edges)
   bool trace_on = false;
   srmg::DevBuf trace;        // %globaltimer stamps after every engine phase (CTA 0)
 

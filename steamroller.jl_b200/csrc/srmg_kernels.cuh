@@ -40,16 +40,22 @@ struct LevelView {
   int nblk;
   int nch;
   int level;
+  // BoxStencil trees only (else null): [nblk*4] corner faces, corner q at direction
+  // (2 (q & 1) - 1, 2 (q >> 1) - 1); {type, src_blk, a, b} with (a, b) the subblock of a
+  // refinement corner or the boundary's bnd vector (components -1, 0, +1) of a
+  // boundary corner.
+  const int4 *cfaces;
 };
 
 // Operator parameters for one level.
 template <typename T>
 struct OpParams {
-  int op;        // 0 Laplacian, 1 Helmholtz
+  int op;        // 0 Laplacian, 1 Helmholtz, 2 compact order-4 Laplacian
   int geom;      // 0 Cartesian, 1 cylindrical r = dim 1, 2 cylindrical r = dim 2
   T s;           // level scale s_l
   T centre;      // -4 or -4 - s_l*k2 (stencil centre, src/helmholtz.jl:43-45)
   T nwc;         // -(omega / diagelm)  (src/multigrid.jl:177)
+  T omega;       // the relaxation factor itself (order 4 divides by a per-cell diagonal)
 };
 
 struct Signs { double v[9]; };  // boundary-condition table as doubles, column-major
@@ -101,6 +107,65 @@ __device__ __forceinline__ T apply5(const T *ub, int x, int y, const W5<T> &w, T
   v = v + w.rp * ub[o + 1];
   v = v + w.zp * ub[o + kS];
   return v;
+}
+
+// ---- compact order-4 Laplacian, LaplacianDiscretization{2,4} -------------------------
+// applystencil (src/laplacian.jl:133-202): a 3x3 literal, rows along dimension 1 and
+// columns along dimension 2, accumulated column-major (k = (d1 + 1) + 3 (d2 + 1),
+// v = 0; v += c_k u) and divided by 6.  The cylindrical coefficients are integer
+// polynomials of the radial 1-based global index i divided as doubles; every operation
+// is rounded on its own (no contraction), so results are bit-exact against the oracle.
+__device__ __forceinline__ void coeffs9(int geom, int64_t ir, int64_t iz, double c[9]) {
+  if (geom == 0) {
+    c[0] = 1; c[1] = 4; c[2] = 1; c[3] = 4; c[4] = -20; c[5] = 4; c[6] = 1; c[7] = 4; c[8] = 1;
+    return;
+  }
+  const int64_t i = geom == 1 ? ir : iz;
+  const int64_t q = 2 * i - 1;
+  const double am = __ddiv_rn((double)(2 * (i - 1)), (double)q);
+  const double ap = __ddiv_rn((double)(2 * i), (double)q);
+  const double q3 = (double)(q * q * q);
+  const double em = __ddiv_rn((double)(4 * (-2 + 9 * i - 16 * i * i + 8 * i * i * i)), q3);
+  const double cc = __ddiv_rn((double)(-16 * (1 - 5 * i + 5 * i * i)), (double)((1 - 2 * i) * (1 - 2 * i)));
+  const double ep = __ddiv_rn((double)(4 * (1 + i - 8 * i * i + 8 * i * i * i)), q3);
+  if (geom == 1) {  // r = dimension 1 (src/laplacian.jl:156-164)
+    c[0] = am; c[1] = 4; c[2] = ap; c[3] = em; c[4] = cc; c[5] = ep; c[6] = am; c[7] = 4; c[8] = ap;
+  } else {          // r = dimension 2 (src/laplacian.jl:176-184)
+    c[0] = am; c[1] = em; c[2] = am; c[3] = 4; c[4] = cc; c[5] = 4; c[6] = ap; c[7] = ep; c[8] = ap;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T apply9(const T *ub, int x, int y, int geom, int64_t ir, int64_t iz) {
+  double c[9];
+  coeffs9(geom, ir, iz, c);
+  T v = T(0);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const int d1 = k % 3 - 1, d2 = k / 3 - 1;
+    v = dadd<T>(v, dmul<T>(T(c[k]), ub[(x + d1) + kS * (y + d2)]));
+  }
+  return v / T(6);
+}
+
+// diagelm, order 4 (src/laplacian.jl:150-151, 205-209).
+__device__ __forceinline__ double diagelm4(int geom, int64_t ir, int64_t iz) {
+  if (geom == 0) return -20.0 / 6.0;
+  const int64_t i = geom == 1 ? ir : iz;
+  return __ddiv_rn(__ddiv_rn((double)(-16 * (1 - 5 * i + 5 * i * i)), (double)((1 - 2 * i) * (1 - 2 * i))), 6.0);
+}
+
+// 1-based global indices of local cell (x, y) of a block at 1-based coords (cr, cz)
+// (global_first, src/mesh.jl:76-78).
+__device__ __forceinline__ int64_t gidx(int c, int x) { return (int64_t)kM * (c - 1) + x - 1; }
+
+// The left-hand side of any supported discretisation at cell (x, y).
+template <typename T>
+__device__ __forceinline__ T lhs_apply(const T *ub, int x, int y, const OpParams<T> &p, const WTab<T> &wt,
+                                       int cr, int cz) {
+  if (p.op == 2) return apply9<T>(ub, x, y, p.geom, gidx(cr, x), gidx(cz, y));
+  const W5<T> w = weights<T>(wt, p.geom, cr, cz, x, y);
+  return apply5<T>(ub, x, y, w, p.centre);
 }
 
 // ---- ghost fill (src/connectivity.jl:155-258) --------------------------------------
@@ -199,8 +264,7 @@ __global__ void k_residual(T *__restrict__ r, const T *__restrict__ u, const T *
     const int x = 2 + (c & 15), y = 2 + (c >> 4);
     const int4 bk = lv.blocks[bi];
     const int64_t base = (int64_t)bk.x * kSS;
-    const W5<T> w = weights<T>(wt, p.geom, bk.y, bk.z, x, y);
-    const T Lu = apply5<T>(u + base, x, y, w, p.centre);
+    const T Lu = lhs_apply<T>(u + base, x, y, p, wt, bk.y, bk.z);
     const int64_t o = base + x + kS * y;
     r[o] = -(b[o] + Lu / p.s);
   }
@@ -221,8 +285,7 @@ __global__ void k_postrestrict(T *__restrict__ bf, const T *__restrict__ u, cons
     const int x = 2 + 8 * (ch.z - 1) + (c & 7), y = 2 + 8 * (ch.w - 1) + (c >> 3);
     const int2 cc = coord_of[cblk];
     const int64_t base = (int64_t)cblk * kSS;
-    const W5<T> w = weights<T>(wt, p.geom, cc.x, cc.y, x, y);
-    const T Lu = apply5<T>(u + base, x, y, w, p.centre);
+    const T Lu = lhs_apply<T>(u + base, x, y, p, wt, cc.x, cc.y);
     const int64_t o = base + x + kS * y;
     bf[o] = -(r[o] + Lu / p.s);
   }
@@ -316,8 +379,7 @@ __global__ void __launch_bounds__(NT) k_leafsq(double *__restrict__ part, const 
     const int64_t o = base + x + kS * y;
     double v;
     if (mode == 0) {
-      const W5<T> w = weights<T>(wt, p.geom, bk.y, bk.z, x, y);
-      const T Lu = apply5<T>(u + base, x, y, w, p.centre);
+      const T Lu = lhs_apply<T>(u + base, x, y, p, wt, bk.y, bk.z);
       v = (double)(-(b[o] + Lu / p.s));
     } else {
       v = (double)b[o];
@@ -349,6 +411,108 @@ __global__ void __launch_bounds__(NT) k_reduce_sqrt(double *__restrict__ out,
     double v = (threadIdx.x < NT / 32) ? sh[threadIdx.x] : 0.0;
     for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
     if (threadIdx.x == 0) out[0] = sqrt(v);
+  }
+}
+
+// gauss_seidel!(..., FourColors{P1,P2}) (src/multigrid.jl:206-232): cells
+// (2 + 2a + p1, 2 + 2b + p2), u -= omega (Lu + s b) / c, unfused.
+template <typename T>
+__global__ void k_gs4(T *__restrict__ u, const T *__restrict__ b, LevelView lv, OpParams<T> p, int p1, int p2) {
+  const int64_t total = (int64_t)lv.nblk * 64;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t >> 6), c = (int)(t & 63);
+    const int x = 2 + 2 * (c & 7) + p1, y = 2 + 2 * (c >> 3) + p2;
+    const int4 bk = lv.blocks[bi];
+    T *ub = u + (int64_t)bk.x * kSS;
+    const int64_t ir = gidx(bk.y, x), iz = gidx(bk.z, y);
+    const T Lu = apply9<T>(ub, x, y, p.geom, ir, iz);
+    const int o = x + kS * y;
+    const T cdiag = T(diagelm4(p.geom, ir, iz));
+    const T upd = dmul<T>(p.omega, dadd<T>(Lu, dmul<T>(p.s, b[(int64_t)bk.x * kSS + o]))) / cdiag;
+    ub[o] = ub[o] - upd;
+  }
+}
+
+// rhs! over rhs_level! (src/multigrid.jl:363-388): q1 = R q on the valid cells.  Order
+// 2: the identity (src/laplacian.jl:86-91,120-125).  Order 4: the literal
+// (src/laplacian.jl:141-148,166-173,186-193) walked over its nonzero entries
+// (0,-1), (-1,0), (0,0), (1,0), (0,1), then divided by 12.
+template <typename T>
+__global__ void k_rhs(T *__restrict__ q1, const T *__restrict__ q, LevelView lv, int op, int geom) {
+  const int64_t total = (int64_t)lv.nblk * 256;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t >> 8), c = (int)(t & 255);
+    const int x = 2 + (c & 15), y = 2 + (c >> 4);
+    const int4 bk = lv.blocks[bi];
+    const T *qb = q + (int64_t)bk.x * kSS;
+    const int o = x + kS * y;
+    if (op != 2) {
+      q1[(int64_t)bk.x * kSS + o] = qb[o];
+      continue;
+    }
+    T wzm = T(1), wrm = T(1), wrp = T(1), wzp = T(1);
+    if (geom != 0) {
+      const int64_t i = geom == 1 ? gidx(bk.y, x) : gidx(bk.z, y);
+      const T wm = __ddiv_rn((double)(2 * i - 2), (double)(2 * i - 1));
+      const T wp = __ddiv_rn((double)(2 * i), (double)(2 * i - 1));
+      if (geom == 1) { wrm = wm; wrp = wp; } else { wzm = wm; wzp = wp; }
+    }
+    T v = T(0);
+    v = dadd<T>(v, dmul<T>(wzm, qb[o - kS]));
+    v = dadd<T>(v, dmul<T>(wrm, qb[o - 1]));
+    v = dadd<T>(v, dmul<T>(T(8), qb[o]));
+    v = dadd<T>(v, dmul<T>(wrp, qb[o + 1]));
+    v = dadd<T>(v, dmul<T>(wzp, qb[o + kS]));
+    q1[(int64_t)bk.x * kSS + o] = v / T(12);
+  }
+}
+
+// Corner ghosts of a BoxStencil tree (src/connectivity.jl:155-258 with diagonal faces):
+// 2 x 2 cells per corner, one thread per cell.  phase 1 = copy from the diagonal
+// neighbour, 2 = boundary mirror (bnd may be zero along one dimension: then the mirror
+// reads the adjacent face's ghost cells), 4 = linear interpolation from the parent's
+// subblockbnd cell (src/blockfield.jl:416-434, src/interp.jl:24-63).  The three phases
+// run as separate launches in that order, as fill_ghost! runs its three passes.
+template <typename T>
+__global__ void k_fill_corner(T *__restrict__ u, LevelView lv, Signs sg, int phase) {
+  const int64_t total = (int64_t)lv.nblk * 16;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t >> 4), q = (int)((t >> 2) & 3), cell = (int)(t & 3);
+    const int4 fi = lv.cfaces[4 * bi + q];
+    const int type = fi.x;
+    if (type == FACE_NONE) continue;
+    if ((type == FACE_NEIGHBOR && phase != 1) || (type == FACE_BOUNDARY && phase != 2) ||
+        (type == FACE_REFBND && phase != 4))
+      continue;
+    const int fr = 2 * (q & 1) - 1, fz = 2 * (q >> 1) - 1;  // ghost direction
+    const int ir = cell & 1, iz = cell >> 1;
+    const int x = (fr < 0 ? 0 : kM + kG) + ir, y = (fz < 0 ? 0 : kM + kG) + iz;
+    T *ub = u + (int64_t)lv.blocks[bi].x * kSS;
+    if (type == FACE_NEIGHBOR) {
+      const T *src = u + (int64_t)fi.y * kSS;
+      ub[x + kS * y] = src[(x - kM * fr) + kS * (y - kM * fz)];
+    } else if (type == FACE_BOUNDARY) {
+      const int b0 = fi.z, b1 = fi.w;
+      const int mx = b0 < 0 ? 2 * kG - 1 - x : b0 > 0 ? 2 * (kG + kM) - 1 - x : x;
+      const int my = b1 < 0 ? 2 * kG - 1 - y : b1 > 0 ? 2 * (kG + kM) - 1 - y : y;
+      const T a = T(sg.v[(1 + b0) + 3 * (1 + b1)]);
+      ub[x + kS * y] = dmul<T>(a, ub[mx + kS * my]);
+    } else {
+      const T *cb = u + (int64_t)fi.y * kSS;
+      const int sbr = fi.z, sbz = fi.w;
+      // subblockbnd(subblock, -face): the last cell of the subblock along a dimension
+      // where the ghost lies below, the first where it lies above
+      const int jr = fr < 0 ? 1 + 8 * sbr : 2 + 8 * (sbr - 1);
+      const int jz = fz < 0 ? 1 + 8 * sbz : 2 + 8 * (sbz - 1);
+      const int o = jr + kS * jz;
+      T v = dmul<T>(T(0.5), cb[o]);
+      v = dadd<T>(v, dmul<T>(T(0.25), cb[o + (2 * ir - 1)]));
+      v = dadd<T>(v, dmul<T>(T(0.25), cb[o + kS * (2 * iz - 1)]));
+      ub[x + kS * y] = v;
+    }
   }
 }
 

@@ -62,8 +62,7 @@ __global__ void __launch_bounds__(NT) k_leafsq_per_block(double *__restrict__ pa
     const int x = 2 + (c & 15), y = 2 + (c >> 4);
     const int sub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
     if ((bk.w >> sub) & 1) continue;
-    const W5<double> w = weights<double>(wt, p.geom, bk.y, bk.z, x, y);
-    const double Lu = apply5<double>(u + base, x, y, w, p.centre);
+    const double Lu = lhs_apply<double>(u + base, x, y, p, wt, bk.y, bk.z);
     const int64_t o = base + x + kS * y;
     const double r = -(b[o] + Lu / p.s);
     acc = fma(r, r, acc);

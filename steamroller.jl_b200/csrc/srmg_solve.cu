@@ -216,7 +216,8 @@ static void item_stats(srmg_ctx *ctx, int k, srmg_stats *st) {
 bool srmg::engine_ok(srmg_ctx *ctx, const srmg_solve_opts *o, std::initializer_list<const void *> ptrs) {
   uintptr_t a = 0;
   for (const void *p : ptrs) a |= reinterpret_cast<uintptr_t>(p);
-  return ctx->use_engine && (a & 15) == 0 && o->ndown >= 1 && o->ntop >= 1 && o->nup >= 1 && ctx->nlev <= 30;
+  return ctx->use_engine && !ctx->has_corners && (a & 15) == 0 && o->ndown >= 1 && o->ntop >= 1 && o->nup >= 1 &&
+         ctx->nlev <= 30;
 }
 
 // Work buffers of a solve (allocated before any capture: nothing allocates later).
@@ -318,6 +319,9 @@ static int solve_fp64(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_al
 // item's defect norm is <= tol * leafnorm(b).
 static int solve_mixed(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, const ItemSpec *specs,
                        int geom, const srmg_solve_opts *o, srmg_stats *st) {
+  for (int k = 0; k < ctx->nitems; k++)
+    if (specs[k].op == SRMG_OP_LAPLACIAN4)
+      return fail(ctx, SRMG_ERR_UNSUPPORTED, "mixed precision supports order-2 discretisations; use FP64 mode");
   ItemTabs tabs;
   RC(prepare_items(ctx, specs, geom, o->omega, true, 0, 0.0, &tabs));
   if (engine_ok(ctx, o, {u, b})) {

@@ -102,6 +102,8 @@ extern "C" int srmg_autotune(srmg_ctx *ctx, double *u, const double *b, int64_t 
                              srmg_tune_trial *trials, int max_trials) {
   RC(check_call(ctx, nblk_alloc, op, geom, bc));
   if (!u || !b || !opts || max_trials < 0) return fail(ctx, SRMG_ERR_BADARG, "srmg_autotune: bad arguments");
+  if (op == SRMG_OP_LAPLACIAN4 || ctx->has_corners)
+    return fail(ctx, SRMG_ERR_UNSUPPORTED, "srmg_autotune tunes the persistent engine (StarStencil, order 2)");
   const size_t bytes = (size_t)nblk_alloc * kSS * sizeof(double);
   DevBuf u0;
   RC(ensure(ctx, u0, bytes));

@@ -23,7 +23,7 @@ import math
 import numpy as np
 
 from .tree import (Tree, Connectivity, boundaryconditions, connectivity, populate,
-                   refine_block, leaf_cells)
+                   refine_block, leaf_cells, STAR2, BOX2)
 
 ELEMENTARY_CHARGE = 1.6021766208e-19   # src/constants.jl:55
 EPSILON_0 = 8.854187817620389e-12      # src/constants.jl:56
@@ -32,7 +32,7 @@ M_BLOCK = 16
 G_GHOST = 2
 S_BLOCK = M_BLOCK + 2 * G_GHOST
 
-OP_LAPLACIAN, OP_HELMHOLTZ = 0, 1
+OP_LAPLACIAN, OP_HELMHOLTZ, OP_LAPLACIAN4 = 0, 1, 2
 GEOM_CART, GEOM_CYL1, GEOM_CYL2 = 0, 1, 2
 
 # Poisson BCs for the benchmark: Neumann on the axis and outer radius, Dirichlet at the
@@ -160,9 +160,10 @@ def channel_density(r, z, channels):
 
 
 def grow_tree(base_level: int, extra_levels: int, indicator, thr: float,
-              h1: float = L_DOMAIN / M_BLOCK, rootsize=(1, 1)) -> Tree:
+              h1: float = L_DOMAIN / M_BLOCK, rootsize=(1, 1), stencil=STAR2) -> Tree:
     """Uniform tree to ``base_level`` then refine, level by level, every leaf block
-    whose max indicator over its cells exceeds ``thr`` (with proper nesting)."""
+    whose max indicator over its cells exceeds ``thr`` (with proper nesting along
+    ``stencil``)."""
     tree = Tree(rootsize, base_level + extra_levels)
     populate(tree, base_level)
     for l in range(base_level, base_level + extra_levels):
@@ -174,7 +175,7 @@ def grow_tree(base_level: int, extra_levels: int, indicator, thr: float,
         for q in np.nonzero(mx > thr)[0]:
             c = coords[q]
             if tree.isleaf(l, c):
-                refine_block(tree, l, c)
+                refine_block(tree, l, c, stencil)
     tree.sync()
     return tree
 
@@ -337,3 +338,27 @@ def config3_tree_problems(seed: int = 3, ntrees: int = 16, lo=1e5, hi=3e6):
                                       bc=BC_PHOTO, name=f"cfg3-tree{t}-helm{j}", conn=conn))
         out.append((pois, terms))
     return out
+
+
+def order4_problem(seed: int = 7, geom: int = GEOM_CYL1, base_level: int = 3, extra: int = 3,
+                   thr_frac: float = 0.35) -> Problem:
+    """The compact order-4 Laplacian (LaplacianDiscretization{2,4}) on a refined tree
+    grown around a seeded channel with BoxStencil nesting and connectivity
+    (src/simulate.jl:258-262, src/streamer.jl:437).  ``b`` holds the net charge q; the
+    solve's right-hand side is rhs_level!(q1, q) of it (src/streamer.jl:313-318)."""
+    rng = np.random.default_rng(seed)
+    ch = seeded_channel(rng)
+    ind = lambda r, z: field_proxy(r, z, [ch])
+    blks, r, z, _, _ = block_cell_centres(_uniform(base_level), base_level, L_DOMAIN / M_BLOCK)
+    vals = ind(r, z)
+    thr = float(np.exp(np.log(vals.min()) + thr_frac * (np.log(vals.max()) - np.log(vals.min()))))
+    tree = grow_tree(base_level, extra, ind, thr, stencil=BOX2)
+    conn = connectivity(tree, BOX2)
+    # Neumann on the axis and the outer radius, Dirichlet at the electrodes, with the
+    # radial dimension chosen by the geometry; all Dirichlet for Cartesian
+    bc = {GEOM_CART: boundaryconditions(((-1, -1), (-1, -1))), GEOM_CYL1: BC_POISSON,
+          GEOM_CYL2: boundaryconditions(((-1, -1), (1, 1)))}[geom]
+    pr = make_problem(tree, channel_rhs([ch], seed), poisson_scale(), op=OP_LAPLACIAN4, bc=bc,
+                      name=f"order4-g{geom}-l{base_level}+{extra}", conn=conn)
+    pr.geom = geom
+    return pr

@@ -96,6 +96,8 @@ SIGNATURES = {
     "srmg_residual_level_dev": (_I, [_P, _P, _P, _P, _I64, _I, _D, _I, _D, _I]),
     "srmg_restrict_level_dev": (_I, [_P, _P, _I64, _I]),
     "srmg_restrict_full_dev": (_I, [_P, _P, _I64]),
+    "srmg_rhs_level": (_I, [_P, _P, _P, _I64, _I, _I, _I]),
+    "srmg_rhs_level_dev": (_I, [_P, _P, _P, _I64, _I, _I, _I]),
     "srmg_netcharge": (_I, [_P, _P, _P, _P, _I64]),
     "srmg_netcharge_dev": (_I, [_P, _P, _P, _P, _I64]),
     "srmg_electric_field": (_I, [_P, _P, _P, _P, _I64, ctypes.c_double, _P]),
@@ -257,9 +259,13 @@ def _bc(bc):
 
 
 def _disc(lpldisc):
-    """(op, k2) from a discretisation descriptor: None/'laplacian' or ('helmholtz', k2)."""
+    """(op, k2) from a discretisation descriptor: None/'laplacian' (LaplacianDiscretization
+    {2,2}), ('helmholtz', k2) (HelmholtzDiscretization{2,2}(k2)) or 'laplacian4'
+    (LaplacianDiscretization{2,4}, the compact order-4 scheme)."""
     if lpldisc is None or lpldisc == "laplacian" or lpldisc == 0:
         return 0, 0.0
+    if lpldisc == "laplacian4" or lpldisc == 2:
+        return 2, 0.0
     if isinstance(lpldisc, tuple) and lpldisc[0] in ("helmholtz", 1):
         return 1, float(lpldisc[1])
     raise ValueError(f"unsupported discretisation {lpldisc!r}")
@@ -320,6 +326,17 @@ def netcharge(ctx: Context, q, ne, nion):
     else:
         _order_after_torch(ctx, q, ne, nion)
         ctx.check(lib().srmg_netcharge_dev(ctx.handle, _ptr(q), _ptr(ne), _ptr(nion), q.shape[0]))
+
+
+def rhs_level_(ctx: Context, q1, q, l, geometry, lpldisc=None):
+    """rhs_level!(q1, q, tree[l], lpldisc, geometry) (src/multigrid.jl:363-388): q1 = R q
+    on level l (identity at order 2, the compact right-hand side at order 4)."""
+    op, _ = _disc(lpldisc)
+    if isinstance(q1, np.ndarray):
+        ctx.check(lib().srmg_rhs_level(ctx.handle, _ptr(q1), _ptr(q), q1.shape[0], l, op, geometry))
+    else:
+        _order_after_torch(ctx, q1, q)
+        ctx.check(lib().srmg_rhs_level_dev(ctx.handle, _ptr(q1), _ptr(q), q1.shape[0], l, op, geometry))
 
 
 def restrict_full_(ctx: Context, u):

@@ -11,7 +11,7 @@ Reference:
   * ``Tree`` / ``populate!`` / ``isleaf`` src/tree.jl:6-44, 105-115
   * ``parentcoord`` / ``subcoord``         src/mesh.jl:48-61
   * edge structs / ``connectivity!``      src/connectivity.jl:6-42, 106-149
-  * ``StarStencil`` iteration order       src/stencil.jl:16-32
+  * ``StarStencil`` / ``BoxStencil`` order src/stencil.jl:16-55
 """
 from __future__ import annotations
 
@@ -32,6 +32,9 @@ CHILD_DTYPE = np.dtype([("fine", "<i8"), ("coarse", "<i8"), ("subblock", "<i8", 
 
 # StarStencil{2} iteration order: (-1,0), (1,0), (0,-1), (0,1)  (src/stencil.jl:16-32)
 STAR2 = ((-1, 0), (1, 0), (0, -1), (0, 1))
+# BoxStencil{2} iteration order (src/stencil.jl:34-55, __incbox :72-90): dimension 1
+# fastest from (-1,-1), the origin skipped
+BOX2 = ((-1, -1), (0, -1), (1, -1), (-1, 0), (1, 0), (-1, 1), (0, 1), (1, 1))
 
 
 class BlockLayer:
@@ -143,12 +146,14 @@ def populate(tree: Tree, level: int) -> int:
     return tree.nblocks_created
 
 
-def refine_block(tree: Tree, l: int, c) -> None:
+def refine_block(tree: Tree, l: int, c, stencil=STAR2) -> None:
     """Refine leaf block ``c`` of level ``l`` keeping proper nesting: every in-domain
-    star neighbour of ``c`` must exist at level ``l`` first, so that the children's
-    missing neighbours always have a parent (the invariant asserted by
+    neighbour of ``c`` along ``stencil`` must exist at level ``l`` first, so that the
+    children's missing neighbours always have a parent (the invariant asserted by
     src/connectivity.jl:129,141 and maintained by ensure_proper_refine!,
-    src/refinement.jl:286-311)."""
+    src/refinement.jl:286-311).  The reference refines with a BoxStencil
+    (src/streamer.jl:437); ``BOX2`` reproduces that nesting, which a BoxStencil
+    connectivity needs."""
     if l >= len(tree):
         raise ValueError("cannot refine beyond the tree's maximum level")
     layer = tree[l - 1]
@@ -156,10 +161,10 @@ def refine_block(tree: Tree, l: int, c) -> None:
         raise KeyError(c)
     if not tree.isleaf(l, c):
         return
-    for s in STAR2:
+    for s in stencil:
         n = (c[0] + s[0], c[1] + s[1])
         if layer.in_domain(n) and n not in layer.index:
-            refine_block(tree, l - 1, parentcoord(n))
+            refine_block(tree, l - 1, parentcoord(n), stencil)
     nxt = tree[l]
     for cc in subblocks(c):
         if cc not in nxt.index:
@@ -176,14 +181,18 @@ class Connectivity:
         self.child = child
 
 
-def connectivity(tree: Tree) -> Connectivity:
-    """``connectivity!`` with a StarStencil (src/connectivity.jl:106-149)."""
+def connectivity(tree: Tree, stencil=STAR2) -> Connectivity:
+    """``connectivity!`` (src/connectivity.jl:106-149) with a StarStencil (``STAR2``,
+    order-2 discretisations) or a BoxStencil (``BOX2``, the order-4 compact
+    discretisation, src/simulate.jl:260-262), whose diagonal edges fill the 2 x 2
+    corner ghosts.  A diagonal step out of the domain along one dimension only gives a
+    Boundary whose ``bnd`` is zero along the other (src/connectivity.jl:112-115)."""
     nlev = len(tree)
     bd, nb, rb, ch = ([[] for _ in range(nlev)] for _ in range(4))
     for layer in tree:
         lv = layer.level
         for c, blk in layer.pairs:
-            for s in STAR2:
+            for s in stencil:
                 n = (c[0] + s[0], c[1] + s[1])
                 if not layer.in_domain(n):
                     bnd = tuple(0 if 1 <= n[d] <= layer.domain[d] else s[d] for d in range(2))
