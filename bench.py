@@ -46,7 +46,8 @@ METRIC = "field solves/sec at 1e-8 rel residual (mixed-precision multigrid; plai
 # (57.72 MB read + 41.05 MB written)
 TRAFFIC_VCYCLE_CONFIG2 = 98.77e6
 # DRAM bytes of one mixed-solve launch on the config-2 tree, from an ncu capture
-TRAFFIC_MIXED_CONFIG2 = None
+# (139.30 MB read + 182.13 MB written)
+TRAFFIC_MIXED_CONFIG2 = 321.43e6
 
 
 def peaks():
@@ -59,9 +60,10 @@ def peaks():
 
 
 class ClockSampler:
-    """SM clocks and clock-event (throttle) reasons sampled through NVML every 5 ms while
-    the timed region runs (nvidia-smi's fastest loop, 200 ms, would see one sample of a
-    40 ms region).  Falls back to `nvidia-smi -lms 200` when NVML is not importable."""
+    """SM clocks and clock-event (throttle) reasons while the timed region runs: NVML
+    polled every 5 ms (nvidia-smi's fastest loop, 200 ms, would see one sample of a
+    40 ms region) plus `nvidia-smi -lms 200` beside it for the reasons.  A failing NVML
+    call is recorded (`nvml_error`) and the other sources keep going."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -74,10 +76,12 @@ class ClockSampler:
         self.index = index
         self.period = period_s
         self.sm, self.mx, self.reasons = [], [], set()
+        self.smi_sm, self.smi_mx = [], []
         self.proc = None
         self.nvml = None
+        self.error = None
         self.stop_ev = threading.Event()
-        self.t = None
+        self.threads = []
 
     def _handle(self):
         import pynvml
@@ -89,36 +93,55 @@ class ClockSampler:
         except Exception:
             return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
+    def _note(self, e):
+        if self.error is None:
+            self.error = f"{type(e).__name__}: {e}"
+
     def start(self):
         self.stop_ev.clear()
         try:
             self.nvml, self.h = self._handle()
-            self.t = threading.Thread(target=self._poll, daemon=True)
-            self.t.start()
-        except Exception:
+            self.threads.append(threading.Thread(target=self._poll, daemon=True))
+        except Exception as e:
+            self._note(e)
             self.nvml = None
-            try:
-                self.proc = subprocess.Popen(
-                    ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                     "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-                self.t = threading.Thread(target=self._read, daemon=True)
-                self.t.start()
-            except Exception:
-                self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.threads.append(threading.Thread(target=self._read, daemon=True))
+        except Exception:
+            self.proc = None
+        for t in self.threads:
+            t.start()
         return self
 
     def _poll(self):
         nv = self.nvml
-        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
-            nv.nvmlDeviceGetCurrentClocksThrottleReasons
-        mx = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+        getters = [getattr(nv, n) for n in ("nvmlDeviceGetCurrentClocksEventReasons",
+                                             "nvmlDeviceGetCurrentClocksThrottleReasons") if hasattr(nv, n)]
+        try:
+            mx = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+        except Exception as e:
+            self._note(e)
+            mx = None
         while True:
-            self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
-            self.mx.append(float(mx))
-            bits = int(get_reasons(self.h))
-            for name, bit in self.BITS.items():
-                if bits & bit:
-                    self.reasons.add(name)
+            try:
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                if mx is not None:
+                    self.mx.append(mx)
+            except Exception as e:
+                self._note(e)
+            while getters:
+                try:
+                    bits = int(getters[0](self.h))
+                    for name, bit in self.BITS.items():
+                        if bits & bit:
+                            self.reasons.add(name)
+                    break
+                except Exception as e:
+                    self._note(e)
+                    getters.pop(0)
             if self.stop_ev.wait(self.period):
                 break
 
@@ -127,8 +150,8 @@ class ClockSampler:
         for line in self.proc.stdout:
             r = [x.strip() for x in line.split(",")]
             if len(r) > 8 and r[1].replace(".", "").isdigit():
-                self.sm.append(float(r[1]))
-                self.mx.append(float(r[2]))
+                self.smi_sm.append(float(r[1]))
+                self.smi_mx.append(float(r[2]))
                 for k, n in enumerate(names):
                     if r[5 + k].lower() == "active":
                         self.reasons.add(n)
@@ -141,8 +164,8 @@ class ClockSampler:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
-        if self.t is not None:
-            self.t.join(timeout=5)
+        for t in self.threads:
+            t.join(timeout=5)
 
     def __enter__(self):
         return self.start()
@@ -151,9 +174,14 @@ class ClockSampler:
         self.stop()
 
     def summary(self):
-        return {"sm_mhz": float(np.median(self.sm)) if self.sm else None,
-                "sm_max_mhz": max(self.mx) if self.mx else None, "reasons": sorted(self.reasons),
-                "samples": len(self.sm), "source": "nvml, 5 ms" if self.nvml else "nvidia-smi, 200 ms"}
+        sm = self.sm if self.sm else self.smi_sm
+        mx = self.mx + self.smi_mx
+        out = {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+               "reasons": sorted(self.reasons), "samples": len(self.sm), "smi_samples": len(self.smi_sm),
+               "source": "nvml every 5 ms + nvidia-smi every 200 ms"}
+        if self.error:
+            out["nvml_error"] = self.error
+        return out
 
 
 def dist_setup(backend=None):
