@@ -6,7 +6,8 @@ Drop-in GPU field solve for Steamroller.jl.  `using SteamrollerGPU` after
 `Steamroller.fmg!` for the supported combination
 
     ScalarBlockField{2,16,2,Float64} (contiguous storage),
-    LaplacianDiscretization{2,2} / HelmholtzDiscretization{2,2},
+    LaplacianDiscretization{2,2} / HelmholtzDiscretization{2,2} /
+    LaplacianDiscretization{2,4} (poisson_order = 4, on its BoxStencil connectivity),
     CartesianGeometry / CylindricalGeometry{1} / CylindricalGeometry{2},
     GeneralHomogeneousBoundaryConditions{2},
 
@@ -35,10 +36,11 @@ mutable struct State
     enabled::Bool
     fingerprint::UInt64
     generation::UInt64
+    levelfp::Vector{UInt64}   # per-level fingerprints of the uploaded tree
 end
 
 const STATE = State(C_NULL, parse(Int, get(ENV, "SRMG_DEVICE", "0")),
-                    get(ENV, "SRMG_DISABLE", "0") != "1", 0, 0)
+                    get(ENV, "SRMG_DISABLE", "0") != "1", 0, 0, UInt64[])
 
 function configure!(; device=STATE.device, enabled=STATE.enabled)
     if device != STATE.device && STATE.ctx != C_NULL
@@ -71,13 +73,18 @@ end
 # A cheap fingerprint of the tree: refine!/connectivity! (src/streamer.jl:545-549)
 # change at least one level's block set, so a checksum of every level's pairs decides
 # whether the device copy of the tree is stale.
+function layer_fingerprint(layer)
+    h = UInt64(length(layer.pairs))
+    for (c, blk) in layer.pairs
+        h += UInt64(blk) * 0x9e3779b97f4a7c15 + UInt64(c[1]) * 1000003 + UInt64(c[2])
+    end
+    h
+end
+
 function fingerprint(tree)
     h = UInt64(length(tree))
     for layer in tree
-        h = h * 0x100000001b3 + UInt64(length(layer.pairs))
-        for (c, blk) in layer.pairs
-            h += UInt64(blk) * 0x9e3779b97f4a7c15 + UInt64(c[1]) * 1000003 + UInt64(c[2])
-        end
+        h = h * 0x100000001b3 + layer_fingerprint(layer)
     end
     h
 end
@@ -103,6 +110,7 @@ function upload!(tree, conn)
                     lens(conn.child), ptrs(conn.child), STATE.generation))
     end
     STATE.fingerprint = fp
+    STATE.levelfp = UInt64[layer_fingerprint(l) for l in tree]
     nothing
 end
 
@@ -111,10 +119,11 @@ geomcode(::CylindricalGeometry{1}) = Cint(1)
 geomcode(::CylindricalGeometry{2}) = Cint(2)
 opcode(::LaplacianDiscretization{2,2}) = (Cint(0), 0.0)
 opcode(h::HelmholtzDiscretization{2,2}) = (Cint(1), Float64(h.k2))
+opcode(::LaplacianDiscretization{2,4}) = (Cint(2), 0.0)
 
 const GPUField = ScalarBlockField{2,16,2,Float64}
 const GPUGeom = Union{CartesianGeometry, CylindricalGeometry{1}, CylindricalGeometry{2}}
-const GPUDisc = Union{LaplacianDiscretization{2,2}, HelmholtzDiscretization{2,2}}
+const GPUDisc = Union{LaplacianDiscretization{2,2}, HelmholtzDiscretization{2,2}, LaplacianDiscretization{2,4}}
 
 function Steamroller.vcycle!(u::GPUField, b::GPUField, r::GPUField, u1::GPUField, s,
                              tree, conn, geometry::GPUGeom,
@@ -210,6 +219,26 @@ function Steamroller.netcharge!(tree::Tree, q::GPUField, n::AbstractVector{<:GPU
         check(ccall((:srmg_netcharge, libsrmg), Cint,
                     (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int64),
                     context(), pointer(q.u), pointer(ne.u), pointer(ni.u), size(q.u, 3)))
+    end
+    nothing
+end
+
+# rhs_level!(q1, q, layer, ld, geometry) (src/multigrid.jl:380-388) for the order-4
+# discretisation on the GPU (srmg_rhs_level, bit-exact): the compact right-hand side of
+# derivs! (src/streamer.jl:314-318).  Only the layer is given, so it runs on the GPU
+# while that level of the uploaded tree has the same blocks.
+function Steamroller.rhs_level!(q1::GPUField, q::GPUField, layer, ld::LaplacianDiscretization{2,4},
+                                geometry::GPUGeom)
+    lv = layer.level
+    if !(STATE.enabled && STATE.ctx != C_NULL && 1 <= lv <= length(STATE.levelfp) &&
+         layer_fingerprint(layer) == STATE.levelfp[lv])
+        return invoke(Steamroller.rhs_level!, Tuple{Any,Any,Any,Any,Any}, q1, q, layer, ld, geometry)
+    end
+    GC.@preserve q1 q begin
+        check(ccall((:srmg_rhs_level, libsrmg), Cint,
+                    (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int64, Cint, Cint, Cint),
+                    context(), pointer(q1.u), pointer(q.u), size(q.u, 3), Cint(lv), Cint(2),
+                    geomcode(geometry)))
     end
     nothing
 end
