@@ -233,6 +233,30 @@ int srmg_restrict_full_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc);
  * level between fill_ghost!(q) and fill_ghost!(q1). */
 int srmg_rhs_level(srmg_ctx *ctx, double *q1, const double *q, int64_t nblk_alloc, int level, int op,
                    int geom);
+
+/* ---- free boundary conditions on the radial boundary (FreeBC, src/freebc.jl) --------
+ * derivs! (src/streamer.jl:320) solves the homogeneous potential uh (srmg_vcycle /
+ * srmg_fmg with the same right-hand side), then freebc! adds boundary sources to the
+ * right-hand side; after the main solve fill_ghost_free! (src/streamer.jl:348) adds the
+ * boundary values to u's first outer ghost layer.  The tree of the context must be one
+ * tree (not a forest) with no level above `level`.
+ * srmg_freebc_set: FreeBC(CylindricalGeometry{dim}, u, level, rootsize, h)
+ * (src/freebc.jl:29-53) -- dim 1 or 2 is the radial dimension, rootsize the root block
+ * grid, f the transform kernel FreeBC computes (n = rootsize[other] 2^(level-1) 16
+ * values).  The library keeps a copy; call again when the FreeBC changes. */
+int srmg_freebc_set(srmg_ctx *ctx, int dim, int level, const int64_t rootsize[2], const double *f, int64_t n);
+/* freebc!(q, u, h, s, tree, conn, conf) (src/freebc.jl:83-105): q += the boundary
+ * sources computed from u's outer cells (getouter!, DST-II, times f, DST-III,
+ * setouter! with its refinement-boundary corrections).  b_out (n doubles, may be NULL)
+ * receives conf.b; the library keeps b for srmg_fill_ghost_free.  The transforms run
+ * as direct FP64 sums (n <= 131072). */
+int srmg_freebc(srmg_ctx *ctx, double *q, const double *u, int64_t nblk_alloc, double h, double s, double *b_out);
+int srmg_freebc_dev(srmg_ctx *ctx, double *q, const double *u, int64_t nblk_alloc, double h, double s,
+                    double *b_out);
+/* fill_ghost_free!(u, conf, tree, level) (src/freebc.jl:224-243) with the b of the last
+ * srmg_freebc call. */
+int srmg_fill_ghost_free(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level);
+int srmg_fill_ghost_free_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level);
 int srmg_rhs_level_dev(srmg_ctx *ctx, double *q1, const double *q, int64_t nblk_alloc, int level, int op,
                        int geom);
 /* electric_field!(tree, e, eabs, u, h, t, e0) (src/multigrid.jl:421-449, the method for

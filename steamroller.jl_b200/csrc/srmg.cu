@@ -109,6 +109,7 @@ extern "C" void srmg_destroy(srmg_ctx *ctx) {
   for (auto &b : ctx->cnn_work) if (b.p) cudaFree(b.p);
   if (ctx->sync.p) cudaFree(ctx->sync.p);
   if (ctx->trace.p) cudaFree(ctx->trace.p);
+  if (ctx->fbc.p) cudaFree(ctx->fbc.p);
   if (ctx->h_small) cudaFreeHost(ctx->h_small);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);

@@ -132,6 +132,12 @@ struct srmg_ctx {
   std::vector<const void *> graph_key;  // field pointers and options the graph was captured for
   bool use_graph = false;
 
+  // free boundary conditions (srmg_freebc_set): f [n], sin table [4n], work [n], b [n]
+  srmg::DevBuf fbc;
+  int64_t fbc_n = 0;
+  int fbc_dim = 0, fbc_level = 0;
+  int64_t fbc_root[2] = {1, 1};
+
   // coarsest-level direct inverses, by operator and level-1 structure
   std::map<std::vector<double>, srmg::DevBuf> coarse_cache;
 };

@@ -1,0 +1,371 @@
+// srmg_freebc.cu -- free boundary conditions on the radial boundary (FreeBC,
+// src/freebc.jl, after Malagon-Romero 2018), on the device.
+//
+// derivs! (src/streamer.jl:320) solves the homogeneous potential uh with the same
+// right-hand side and calls freebc!(q1, uh, ...), which adds boundary sources to q1;
+// after the main solve, fill_ghost_free! (src/streamer.jl:348) adds the boundary
+// values to u's first ghost layer before the field is evaluated.  The transform in
+// between works on the outer column at the finest level `level`:
+//   u1 = outer valid cells of uh / h_l (getouter!, src/freebc.jl:108-140)
+//   b  = DST-III(f .* DST-II(u1)) * h / 2^(level-1) / 2          (src/freebc.jl:93-102)
+// with FFTW's unnormalised RODFT10 (DST-II) and RODFT01 (DST-III):
+//   DST-II:  Y_k = 2 sum_{j=0}^{n-1} X_j sin(pi (2j+1)(k+1) / (2n))
+//   DST-III: Y_k = (-1)^k X_{n-1} + 2 sum_{j=0}^{n-2} X_j sin(pi (j+1)(2k+1) / (2n)).
+// n is at most a few ten thousand, so both run as direct sums, one CTA per output in a
+// fixed order, with the sine of every argument from a table of sin(pi t / (2n)),
+// t = 0..4n-1 (the integer argument reduced exactly modulo 4n).  f, the transform's
+// kernel (modified Bessel functions of the domain's aspect), is computed by the caller
+// as FreeBC does and handed over once (srmg_freebc_set).
+#include <cmath>
+
+#include "srmg_ctx.h"
+#include "srmg_internal.h"
+
+using namespace srmg;
+
+#define CK(call)                                              \
+  do {                                                        \
+    int _rc = cuda_check(ctx, (call), #call);                 \
+    if (_rc) return _rc;                                      \
+  } while (0)
+#define RC(call)               \
+  do {                         \
+    int _rc = (call);          \
+    if (_rc) return _rc;       \
+  } while (0)
+
+namespace {
+
+constexpr int64_t kFreeMaxN = 1 << 17;  // transform length limit (direct sums are O(n^2))
+constexpr int kDstThreads = 256;
+
+// Local 0-based (x, y) of a cell `a` cells along `dim` and `o` along the other dimension.
+__device__ __forceinline__ int cell_off(int dim, int a, int o) { return dim == 1 ? a + kS * o : o + kS * a; }
+
+__global__ void k_sin_table(double *tab, int64_t n) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 4 * n; t += (int64_t)gridDim.x * blockDim.x)
+    tab[t] = sinpi((double)t / (double)(2 * n));
+}
+
+// getouter! for one level (levels run in increasing order, so finer blocks overwrite).
+__global__ void k_getouter(double *__restrict__ u1, const double *__restrict__ u, LevelView lv, int dim, int kext,
+                           int p, double hl) {
+  const int64_t total = (int64_t)lv.nblk * kM;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t / kM), i = (int)(t % kM);
+    const int4 bk = lv.blocks[bi];
+    const int cd = dim == 1 ? bk.y : bk.z, co = dim == 1 ? bk.z : bk.y;
+    if (cd != kext) continue;
+    const double v = u[(int64_t)bk.x * kSS + cell_off(dim, kG + kM - 1, kG + i)] / hl;
+    const int64_t i0 = (int64_t)(co - 1) * kM;
+    for (int m = 0; m < p; ++m) u1[p * (i0 + i) + m] = v;
+  }
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double sh[kDstThreads / 32];
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x < 32) {
+    r = threadIdx.x < kDstThreads / 32 ? sh[threadIdx.x] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) r += __shfl_xor_sync(0xffffffffu, r, off);
+  }
+  return r;  // valid in thread 0
+}
+
+// y = DST-II(x)
+__global__ void __launch_bounds__(kDstThreads) k_dst2(double *__restrict__ y, const double *__restrict__ x,
+                                                      const double *__restrict__ tab, int64_t n) {
+  const int64_t m4 = 4 * n;
+  for (int64_t k = blockIdx.x; k < n; k += gridDim.x) {
+    double acc = 0.0;
+    for (int64_t j = threadIdx.x; j < n; j += kDstThreads) acc += x[j] * tab[((2 * j + 1) * (k + 1)) % m4];
+    const double s = block_sum(acc);
+    if (threadIdx.x == 0) y[k] = 2.0 * s;
+    __syncthreads();
+  }
+}
+
+// b = DST-III(f .* a) * h / 2^(level-1) / 2, the product f a rounded once per element
+__global__ void __launch_bounds__(kDstThreads) k_dst3_scale(double *__restrict__ b, const double *__restrict__ a,
+                                                            const double *__restrict__ f,
+                                                            const double *__restrict__ tab, int64_t n, double h,
+                                                            double p2) {
+  const int64_t m4 = 4 * n;
+  for (int64_t k = blockIdx.x; k < n; k += gridDim.x) {
+    double acc = 0.0;
+    for (int64_t j = threadIdx.x; j < n - 1; j += kDstThreads) acc += (f[j] * a[j]) * tab[((j + 1) * (2 * k + 1)) % m4];
+    const double s = block_sum(acc);
+    if (threadIdx.x == 0) {
+      const double last = f[n - 1] * a[n - 1];
+      const double yk = ((k & 1) ? -last : last) + 2.0 * s;
+      b[k] = yk * h / p2 / 2.0;
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ double seg_mean(const double *b, int64_t first, int64_t count) {
+  double v = 0.0;
+  for (int64_t m = 0; m < count; ++m) v = __dadd_rn(v, b[first + m]);
+  return v / (double)count;
+}
+
+// factor(CylindricalGeometry{D}, J, delta) with delta along D (src/geometry.jl:27-29)
+__device__ __forceinline__ double cyl_factor(int64_t J) { return fabs(1.0 + 1.0 / (double)(2 * J - 1)); }
+
+// setouter! boundary sources of one level (src/freebc.jl:157-176): every block with a
+// boundary face at +dim.
+__global__ void k_setouter_bnd(double *__restrict__ q, const double *__restrict__ b, LevelView lv, int dim, int p,
+                               double sl) {
+  const int fidx = dim == 1 ? 1 : 3;
+  const int64_t total = (int64_t)lv.nblk * kM;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t / kM), i = (int)(t % kM);
+    if (lv.faces[4 * bi + fidx].x != FACE_BOUNDARY) continue;
+    const int4 bk = lv.blocks[bi];
+    const int cd = dim == 1 ? bk.y : bk.z, co = dim == 1 ? bk.z : bk.y;
+    const int64_t i0 = (int64_t)(co - 1) * kM;
+    const int64_t Jd = (int64_t)kM * (cd - 1) + kM;
+    const double bmean = seg_mean(b, p * (i0 + i), p);
+    double *qc = q + (int64_t)bk.x * kSS + cell_off(dim, kG + kM - 1, kG + i);
+    *qc = *qc + 2.0 * cyl_factor(Jd) * bmean / sl;
+  }
+}
+
+// setouter! corrections at refinement boundaries of one level (src/freebc.jl:178-219):
+// one thread per block on the outer boundary walks its refinement faces in the
+// connectivity's direction order (`order` lists face codes: 0..3 star faces, 4..7 the
+// corners), so that additions to one cell happen in the reference's order.
+__global__ void k_setouter_ref(double *__restrict__ q, const double *__restrict__ b, LevelView lv, int dim, int kext,
+                               int p, double sl, int4 order_lo, int4 order_hi, int norder) {
+  const int order[8] = {order_lo.x, order_lo.y, order_lo.z, order_lo.w, order_hi.x, order_hi.y, order_hi.z, order_hi.w};
+  for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < lv.nblk; bi += gridDim.x * blockDim.x) {
+    const int4 bk = lv.blocks[bi];
+    const int cd = dim == 1 ? bk.y : bk.z, co = dim == 1 ? bk.z : bk.y;
+    if (cd != kext) continue;
+    for (int r = 0; r < norder; ++r) {
+      const int code = order[r];
+      int type, fr, fz;
+      if (code < 4) {
+        type = lv.faces[4 * bi + code].x;
+        fr = code == 0 ? -1 : code == 1 ? 1 : 0;
+        fz = code == 2 ? -1 : code == 3 ? 1 : 0;
+      } else {
+        const int qd = code - 4;
+        type = lv.cfaces ? lv.cfaces[4 * bi + qd].x : FACE_NONE;
+        fr = 2 * (qd & 1) - 1;
+        fz = 2 * (qd >> 1) - 1;
+      }
+      if (type != FACE_REFBND) continue;
+      const int dir = dim == 1 ? fz : fr;  // the face's component along the other dimension
+      const int i1 = dir == -1 ? kG + 1 : kM + kG;  // 1-based index along the other dimension
+      const int64_t j = (int64_t)(co - 1) * kM + i1 - kG;
+      const int64_t Jd = (int64_t)kM * (cd - 1) + kM;
+      const int64_t J1d = (Jd - 1) / 2 + 1;
+      // 0-based first element: dir = 1 reads b[p j + 1 : p (j + 2)], otherwise
+      // b[p (j - 3) : p (j - 1) - 1] (1-based, as written in the reference)
+      const int64_t first = dir == 1 ? p * j : p * (j - 3) - 1;
+      const double bmean = seg_mean(b, first, 2 * (int64_t)p);
+      double *qc = q + (int64_t)bk.x * kSS + cell_off(dim, kG + kM - 1, i1 - 1);
+      *qc = *qc + 2.0 * 0.25 * cyl_factor(J1d) * bmean / sl;
+    }
+  }
+}
+
+// fill_ghost_free! of one level (src/freebc.jl:224-243)
+__global__ void k_fill_ghost_free(double *__restrict__ u, const double *__restrict__ b, LevelView lv, int dim,
+                                  int kext, int p) {
+  const int64_t total = (int64_t)lv.nblk * kM;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t / kM), i = (int)(t % kM);
+    const int4 bk = lv.blocks[bi];
+    const int cd = dim == 1 ? bk.y : bk.z, co = dim == 1 ? bk.z : bk.y;
+    if (cd != kext) continue;
+    const int64_t i0 = (int64_t)(co - 1) * kM;
+    const double bmean = seg_mean(b, p * (i0 + i), p);
+    double *uc = u + (int64_t)bk.x * kSS + cell_off(dim, kG + kM, kG + i);
+    *uc = *uc + 2.0 * bmean;
+  }
+}
+
+int gridfor(int64_t work, int threads) {
+  const int64_t g = (work + threads - 1) / threads;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 8));
+}
+
+double *fbc_f(srmg_ctx *ctx) { return (double *)ctx->fbc.p; }
+double *fbc_tab(srmg_ctx *ctx) { return fbc_f(ctx) + ctx->fbc_n; }
+double *fbc_u1(srmg_ctx *ctx) { return fbc_tab(ctx) + 4 * ctx->fbc_n; }
+double *fbc_b(srmg_ctx *ctx) { return fbc_u1(ctx) + ctx->fbc_n; }
+
+// Levels the boundary work visits, and the checks freebc! makes.
+int fbc_ready(srmg_ctx *ctx, int64_t nblk_alloc, const char *who) {
+  RC(check_call(ctx, nblk_alloc, 0, 0, nullptr));
+  if (ctx->fbc_n <= 0) return fail(ctx, SRMG_ERR_BADARG, "%s: call srmg_freebc_set first", who);
+  if (ctx->nitems != 1) return fail(ctx, SRMG_ERR_UNSUPPORTED, "%s: one tree per context", who);
+  for (int l = ctx->fbc_level + 1; l <= ctx->nlev; ++l)
+    if (ctx->nblk_host[l - 1] > 0)
+      return fail(ctx, SRMG_ERR_BADARG, "%s: the tree has level %d above the free-boundary level %d", who, l,
+                  ctx->fbc_level);
+  return SRMG_OK;
+}
+
+// The extent of level l along `dim`, in blocks (tree[l].domain, src/blocklayer.jl:111-115).
+int extent(srmg_ctx *ctx, int l, int dim) { return (int)(ctx->fbc_root[dim - 1] << (l - 1)); }
+
+// Host checks on the uploaded tree: every block lies inside the level's extent given by
+// rootsize (so the gathers and means index inside b), and every refinement correction
+// reads inside b (Julia would throw a BoundsError there), with the same index
+// arithmetic as k_setouter_ref.
+int check_tree_fits(srmg_ctx *ctx) {
+  const int dim = ctx->fbc_dim, od = dim == 1 ? 2 : 1;
+  const int L = std::min(ctx->fbc_level, ctx->htree.nlev);
+  for (int l = 1; l <= L; ++l) {
+    const int kext = extent(ctx, l, dim), kexo = extent(ctx, l, od);
+    const int64_t p = (int64_t)1 << (ctx->fbc_level - l);
+    std::vector<int> cd(ctx->htree.max_blk + 1, 0), co(ctx->htree.max_blk + 1, 0);
+    for (const srmg_pair &pr : ctx->htree.pairs[l - 1]) {
+      if (pr.coord[dim - 1] > kext || pr.coord[od - 1] > kexo)
+        return fail(ctx, SRMG_ERR_BADARG, "freebc: block %lld of level %d lies outside the rootsize extent",
+                    (long long)pr.blk, l);
+      cd[pr.blk] = (int)pr.coord[dim - 1];
+      co[pr.blk] = (int)pr.coord[od - 1];
+    }
+    for (const srmg_refbnd &e : ctx->htree.rb[l - 1]) {
+      if (cd[e.fine] != kext) continue;
+      const int dir = (int)e.face[od - 1];
+      const int i1 = dir == -1 ? kG + 1 : kM + kG;
+      const int64_t j = (int64_t)(co[e.fine] - 1) * kM + i1 - kG;
+      const int64_t first = dir == 1 ? p * j : p * (j - 3) - 1;
+      if (first < 0 || first + 2 * p > ctx->fbc_n)
+        return fail(ctx, SRMG_ERR_BADTREE, "freebc: refinement correction of block %lld reads outside b",
+                    (long long)e.fine);
+    }
+  }
+  return SRMG_OK;
+}
+
+}  // namespace
+
+extern "C" int srmg_freebc_set(srmg_ctx *ctx, int dim, int level, const int64_t rootsize[2], const double *f,
+                               int64_t n) {
+  if (!ctx) return SRMG_ERR_BADARG;
+  if (dim != 1 && dim != 2) return fail(ctx, SRMG_ERR_UNSUPPORTED, "srmg_freebc_set: dim must be 1 or 2");
+  if (level < 1 || level > 30 || !rootsize || rootsize[0] < 1 || rootsize[1] < 1 || !f)
+    return fail(ctx, SRMG_ERR_BADARG, "srmg_freebc_set: bad arguments");
+  const int od = dim == 1 ? 2 : 1;
+  const int64_t want = rootsize[od - 1] * ((int64_t)1 << (level - 1)) * kM;
+  if (n != want)
+    return fail(ctx, SRMG_ERR_BADARG, "srmg_freebc_set: n = %lld, FreeBC has %lld", (long long)n, (long long)want);
+  if (n > kFreeMaxN)
+    return fail(ctx, SRMG_ERR_UNSUPPORTED, "srmg_freebc_set: transform length %lld above %lld", (long long)n,
+                (long long)kFreeMaxN);
+  cudaSetDevice(ctx->device);
+  RC(ensure(ctx, ctx->fbc, (size_t)7 * n * sizeof(double)));
+  ctx->fbc_n = n;
+  ctx->fbc_dim = dim;
+  ctx->fbc_level = level;
+  ctx->fbc_root[0] = rootsize[0];
+  ctx->fbc_root[1] = rootsize[1];
+  CK(cudaMemcpyAsync(fbc_f(ctx), f, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  k_sin_table<<<gridfor(4 * n, 256), 256, 0, ctx->stream>>>(fbc_tab(ctx), n);
+  ctx->launches++;
+  CK(cudaMemsetAsync(fbc_b(ctx), 0, n * sizeof(double), ctx->stream));
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SRMG_OK;
+}
+
+extern "C" int srmg_freebc_dev(srmg_ctx *ctx, double *q, const double *u, int64_t nblk_alloc, double h, double s,
+                               double *b_out) {
+  RC(fbc_ready(ctx, nblk_alloc, "srmg_freebc"));
+  if (!q || !u) return fail(ctx, SRMG_ERR_BADARG, "srmg_freebc: null field");
+  if (!(h > 0.0) || !std::isfinite(h) || !std::isfinite(s) || s == 0.0)
+    return fail(ctx, SRMG_ERR_BADARG, "srmg_freebc: bad h or s");
+  RC(check_tree_fits(ctx));
+  const int dim = ctx->fbc_dim, level = ctx->fbc_level;
+  const int64_t n = ctx->fbc_n;
+  const int L = std::min(level, ctx->nlev);
+  double *u1 = fbc_u1(ctx), *b = fbc_b(ctx), *am = b;  // DST-II output shares b's storage until the end
+  CK(cudaMemsetAsync(u1, 0, n * sizeof(double), ctx->stream));
+  for (int l = 1; l <= L; ++l) {
+    const int nb = ctx->nblk_host[l - 1];
+    if (!nb) continue;
+    const double hl = h / (double)((int64_t)1 << (l - 1));
+    k_getouter<<<gridfor((int64_t)nb * kM, 256), 256, 0, ctx->stream>>>(u1, u, ctx->lv[l - 1].view(l), dim,
+                                                                       extent(ctx, l, dim), 1 << (level - l), hl);
+    ctx->launches++;
+  }
+  const int g = (int)std::min<int64_t>(n, 148 * 16);
+  k_dst2<<<g, kDstThreads, 0, ctx->stream>>>(am, u1, fbc_tab(ctx), n);
+  // DST-III reads am and writes b: keep them apart (u1 is free again)
+  CK(cudaMemcpyAsync(u1, am, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  k_dst3_scale<<<g, kDstThreads, 0, ctx->stream>>>(b, u1, fbc_f(ctx), fbc_tab(ctx), n, h,
+                                                   (double)((int64_t)1 << (level - 1)));
+  ctx->launches += 2;
+  const int order_star[4] = {0, 1, 2, 3};                 // StarStencil order (src/stencil.jl:16-32)
+  const int order_box[8] = {4, 2, 5, 0, 1, 6, 3, 7};      // BoxStencil order (src/stencil.jl:34-90)
+  const int *ord = ctx->has_corners ? order_box : order_star;
+  const int nord = ctx->has_corners ? 8 : 4;
+  const int4 olo = make_int4(ord[0], ord[1], ord[2], ord[3]);
+  const int4 ohi = nord == 8 ? make_int4(ord[4], ord[5], ord[6], ord[7]) : make_int4(0, 0, 0, 0);
+  for (int l = 1; l <= L; ++l) {
+    const int nb = ctx->nblk_host[l - 1];
+    if (!nb) continue;
+    const int64_t f = (int64_t)1 << (l - 1);
+    const double sl = s / (double)(f * f);
+    const int p = 1 << (level - l);
+    k_setouter_bnd<<<gridfor((int64_t)nb * kM, 256), 256, 0, ctx->stream>>>(q, b, ctx->lv[l - 1].view(l), dim, p,
+                                                                           sl);
+    k_setouter_ref<<<gridfor(nb, 128), 128, 0, ctx->stream>>>(q, b, ctx->lv[l - 1].view(l), dim,
+                                                            extent(ctx, l, dim), p, sl, olo, ohi, nord);
+    ctx->launches += 2;
+  }
+  if (b_out) CK(cudaMemcpyAsync(b_out, b, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+extern "C" int srmg_fill_ghost_free_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level) {
+  RC(fbc_ready(ctx, nblk_alloc, "srmg_fill_ghost_free"));
+  if (!u || level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "srmg_fill_ghost_free: bad level");
+  if (level > ctx->fbc_level) return SRMG_OK;
+  const int nb = ctx->nblk_host[level - 1];
+  if (nb) {
+    k_fill_ghost_free<<<gridfor((int64_t)nb * kM, 256), 256, 0, ctx->stream>>>(
+        u, fbc_b(ctx), ctx->lv[level - 1].view(level), ctx->fbc_dim, extent(ctx, level, ctx->fbc_dim),
+        1 << (ctx->fbc_level - level));
+    ctx->launches++;
+  }
+  CK(cudaGetLastError());
+  return SRMG_OK;
+}
+
+// Host-array variants (the ccall boundary).
+extern "C" int srmg_freebc(srmg_ctx *ctx, double *q, const double *u, int64_t nblk_alloc, double h, double s,
+                           double *b_out) {
+  RC(fbc_ready(ctx, nblk_alloc, "srmg_freebc"));
+  if (!q || !u) return fail(ctx, SRMG_ERR_BADARG, "srmg_freebc: null field");
+  double *dq, *du;
+  RC(stage_in(ctx, 0, q, nblk_alloc, &dq));
+  RC(stage_in(ctx, 1, u, nblk_alloc, &du));
+  RC(srmg_freebc_dev(ctx, dq, du, nblk_alloc, h, s, nullptr));
+  RC(stage_out(ctx, q, dq, nblk_alloc));
+  if (b_out) CK(cudaMemcpyAsync(b_out, fbc_b(ctx), ctx->fbc_n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SRMG_OK;
+}
+
+extern "C" int srmg_fill_ghost_free(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level) {
+  RC(fbc_ready(ctx, nblk_alloc, "srmg_fill_ghost_free"));
+  if (!u) return fail(ctx, SRMG_ERR_BADARG, "srmg_fill_ghost_free: null field");
+  double *du;
+  RC(stage_in(ctx, 0, u, nblk_alloc, &du));
+  RC(srmg_fill_ghost_free_dev(ctx, du, nblk_alloc, level));
+  RC(stage_out(ctx, u, du, nblk_alloc));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SRMG_OK;
+}

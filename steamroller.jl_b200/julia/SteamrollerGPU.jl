@@ -23,7 +23,7 @@ module SteamrollerGPU
 using Steamroller
 using Steamroller: ScalarBlockField, VectorBlockField, LaplacianDiscretization, HelmholtzDiscretization,
     CartesianGeometry, CylindricalGeometry, GeneralHomogeneousBoundaryConditions,
-    Neighbor, Boundary, RefBoundary, Child, Tree, NetIonization
+    Neighbor, Boundary, RefBoundary, Child, Tree, NetIonization, FreeBC
 using StaticArrays: SVector
 
 const libsrmg = get(ENV, "SRMG_LIB", joinpath(@__DIR__, "..", "srmg", "libsrmg.so"))
@@ -37,16 +37,18 @@ mutable struct State
     fingerprint::UInt64
     generation::UInt64
     levelfp::Vector{UInt64}   # per-level fingerprints of the uploaded tree
+    fbc::UInt64               # objectid of the FreeBC whose kernel the library holds (0: none)
 end
 
 const STATE = State(C_NULL, parse(Int, get(ENV, "SRMG_DEVICE", "0")),
-                    get(ENV, "SRMG_DISABLE", "0") != "1", 0, 0, UInt64[])
+                    get(ENV, "SRMG_DISABLE", "0") != "1", 0, 0, UInt64[], 0)
 
 function configure!(; device=STATE.device, enabled=STATE.enabled)
     if device != STATE.device && STATE.ctx != C_NULL
         ccall((:srmg_destroy, libsrmg), Cvoid, (Ptr{Cvoid},), STATE.ctx)
         STATE.ctx = C_NULL
         STATE.fingerprint = 0
+        STATE.fbc = 0
     end
     STATE.device = device
     STATE.enabled = enabled
@@ -239,6 +241,45 @@ function Steamroller.rhs_level!(q1::GPUField, q::GPUField, layer, ld::LaplacianD
                     (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int64, Cint, Cint, Cint),
                     context(), pointer(q1.u), pointer(q.u), size(q.u, 3), Cint(lv), Cint(2),
                     geomcode(geometry)))
+    end
+    nothing
+end
+
+# Free boundary conditions (FreeBC, src/freebc.jl).  freebc! runs after setfreebc!'s
+# homogeneous solve (already on the GPU through vcycle!/fmg!); the library keeps conf.b
+# for fill_ghost_free!.  The transform kernel conf.f is handed over once per FreeBC.
+function Steamroller.freebc!(q::GPUField, u::GPUField, h, s, tree, conn, conf::FreeBC{2})
+    if !STATE.enabled
+        return invoke(Steamroller.freebc!, Tuple{Any,Any,Any,Any,Any,Any,FreeBC}, q, u, h, s, tree, conn, conf)
+    end
+    upload!(tree, conn)
+    id = objectid(conf)
+    if STATE.fbc != id
+        root = Int64[size(tree[1].domain)...]
+        GC.@preserve root conf begin
+            check(ccall((:srmg_freebc_set, libsrmg), Cint,
+                        (Ptr{Cvoid}, Cint, Cint, Ptr{Int64}, Ptr{Float64}, Int64),
+                        context(), Cint(Steamroller._perpdim(conf)), Cint(conf.level), root,
+                        pointer(conf.f), length(conf.f)))
+        end
+        STATE.fbc = id
+    end
+    GC.@preserve q u conf begin
+        check(ccall((:srmg_freebc, libsrmg), Cint,
+                    (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int64, Float64, Float64, Ptr{Float64}),
+                    context(), pointer(q.u), pointer(u.u), size(q.u, 3), Float64(h), Float64(s),
+                    pointer(conf.b)))
+    end
+    nothing
+end
+
+function Steamroller.fill_ghost_free!(u::GPUField, conf::FreeBC{2}, tree, l)
+    if !(tree_current(tree) && STATE.fbc == objectid(conf))
+        return invoke(Steamroller.fill_ghost_free!, Tuple{Any,FreeBC,Any,Any}, u, conf, tree, l)
+    end
+    GC.@preserve u begin
+        check(ccall((:srmg_fill_ghost_free, libsrmg), Cint, (Ptr{Cvoid}, Ptr{Float64}, Int64, Cint),
+                    context(), pointer(u.u), size(u.u, 3), Cint(l)))
     end
     nothing
 end

@@ -362,3 +362,34 @@ def order4_problem(seed: int = 7, geom: int = GEOM_CYL1, base_level: int = 3, ex
                       name=f"order4-g{geom}-l{base_level}+{extra}", conn=conn)
     pr.geom = geom
     return pr
+
+
+def outer_refined_problem(dim: int = 1, stencil=STAR2, seed: int = 9) -> Problem:
+    """A tree refined at the outer radial boundary, for the free boundary conditions
+    (FreeBC, src/freebc.jl): uniform to level 4 (8 x 8 blocks), two outer-edge blocks
+    refined to level 5 and one of their outer-edge children to level 6, so that the
+    outer boundary has refinement boundaries along it (the corrections of setouter!,
+    src/freebc.jl:178-219).  ``dim`` is the radial dimension (CylindricalGeometry{dim});
+    b is a seeded Gaussian charge on the axis."""
+    rng = np.random.default_rng(seed)
+    t = Tree((1, 1), 7)
+    populate(t, 4)
+
+    def at(r, z):
+        return (r, z) if dim == 1 else (z, r)
+    refine_block(t, 4, at(8, 4), stencil)
+    refine_block(t, 4, at(8, 5), stencil)
+    refine_block(t, 5, at(16, 9), stencil)
+    t.sync()
+    conn = connectivity(t, stencil)
+    z0 = L_DOMAIN * rng.uniform(0.35, 0.65)
+    w = 0.08 * L_DOMAIN
+
+    def rhs(r, z, l, gi, gj):
+        rr, zz = (r, z) if dim == 1 else (z, r)
+        return 1e18 * np.exp(-(rr * rr + (zz - z0) ** 2) / (w * w))
+
+    bc = boundaryconditions(((1, -1), (-1, -1))) if dim == 1 else boundaryconditions(((-1, -1), (1, -1)))
+    pr = make_problem(t, rhs, poisson_scale(), bc=bc, name=f"outer-refined-dim{dim}", conn=conn)
+    pr.geom = GEOM_CYL1 if dim == 1 else GEOM_CYL2
+    return pr

@@ -97,6 +97,11 @@ SIGNATURES = {
     "srmg_restrict_level_dev": (_I, [_P, _P, _I64, _I]),
     "srmg_restrict_full_dev": (_I, [_P, _P, _I64]),
     "srmg_rhs_level": (_I, [_P, _P, _P, _I64, _I, _I, _I]),
+    "srmg_freebc_set": (_I, [_P, _I, _I, _P, _P, _I64]),
+    "srmg_freebc": (_I, [_P, _P, _P, _I64, _D, _D, _P]),
+    "srmg_freebc_dev": (_I, [_P, _P, _P, _I64, _D, _D, _P]),
+    "srmg_fill_ghost_free": (_I, [_P, _P, _I64, _I]),
+    "srmg_fill_ghost_free_dev": (_I, [_P, _P, _I64, _I]),
     "srmg_rhs_level_dev": (_I, [_P, _P, _P, _I64, _I, _I, _I]),
     "srmg_netcharge": (_I, [_P, _P, _P, _P, _I64]),
     "srmg_netcharge_dev": (_I, [_P, _P, _P, _P, _I64]),
@@ -337,6 +342,36 @@ def rhs_level_(ctx: Context, q1, q, l, geometry, lpldisc=None):
     else:
         _order_after_torch(ctx, q1, q)
         ctx.check(lib().srmg_rhs_level_dev(ctx.handle, _ptr(q1), _ptr(q), q1.shape[0], l, op, geometry))
+
+
+def freebc_set(ctx: Context, dim, level, rootsize, f):
+    """FreeBC(CylindricalGeometry{dim}, u, level, rootsize, h) (src/freebc.jl:29-53): hand
+    the library the transform kernel f (computed as FreeBC does)."""
+    fa = np.ascontiguousarray(f, dtype=np.float64)
+    ra = np.ascontiguousarray(rootsize, dtype=np.int64)
+    ctx.check(lib().srmg_freebc_set(ctx.handle, dim, level, ra.ctypes.data, fa.ctypes.data, len(fa)))
+
+
+def freebc_(ctx: Context, q, u, h, s, b_out=None):
+    """freebc!(q, u, h, s, tree, conn, conf) (src/freebc.jl:83-105): q += boundary sources
+    from the homogeneous potential u.  numpy (host) or torch (device) fields; b_out
+    receives conf.b (numpy for host fields, a torch tensor for device fields)."""
+    if isinstance(q, np.ndarray):
+        bp = b_out.ctypes.data if b_out is not None else None
+        ctx.check(lib().srmg_freebc(ctx.handle, _ptr(q), _ptr(u), q.shape[0], h, s, bp))
+    else:
+        _order_after_torch(ctx, q, u)
+        bp = b_out.data_ptr() if b_out is not None else None
+        ctx.check(lib().srmg_freebc_dev(ctx.handle, _ptr(q), _ptr(u), q.shape[0], h, s, bp))
+
+
+def fill_ghost_free_(ctx: Context, u, l):
+    """fill_ghost_free!(u, conf, tree, l) (src/freebc.jl:224-243)."""
+    if isinstance(u, np.ndarray):
+        ctx.check(lib().srmg_fill_ghost_free(ctx.handle, _ptr(u), u.shape[0], l))
+    else:
+        _order_after_torch(ctx, u)
+        ctx.check(lib().srmg_fill_ghost_free_dev(ctx.handle, _ptr(u), u.shape[0], l))
 
 
 def restrict_full_(ctx: Context, u):

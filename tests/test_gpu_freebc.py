@@ -1,0 +1,145 @@
+"""Parity of the free boundary conditions on the GPU (srmg_freebc, srmg_fill_ghost_free,
+through the C ABI) with the oracle (oracle/freebc_oracle.py restating src/freebc.jl).
+
+Bar: the boundary sources added to q, conf.b and the ghost values agree with the
+oracle to <= 1e-12 relative L2: the GPU runs both sine transforms as direct FP64
+sums, the oracle through FFTs, so the two round differently.  Every other cell is
+untouched (bit-exact).  End to end (homogeneous solve, free boundary, main solve) the
+potential matches the oracle's to <= 1e-10.
+"""
+import numpy as np
+import pytest
+
+import freebc_oracle as fo
+from conftest import gpu_available
+from oracle import Oracle
+from srmg import gen, multigrid as mg
+from srmg.tree import STAR2, BOX2
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not gpu_available(), reason="needs a CUDA GPU")]
+
+REL = 1e-12
+SRMG_ERR_BADARG = -1
+
+
+def torch_cuda(a):
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    torch.cuda.synchronize()
+    return t
+
+
+def rel_l2(a, b):
+    n = np.linalg.norm(np.ravel(b))
+    return np.linalg.norm(np.ravel(a - b)) / (n if n > 0 else 1.0)
+
+
+CASES = [(d, st) for d in (1, 2) for st in ("star", "box")]
+
+
+def setup(dim, stencil):
+    p = gen.outer_refined_problem(dim, STAR2 if stencil == "star" else BOX2)
+    level = len(p.tree)
+    n, H, R, f = fo.kernel(dim, level, (1, 1), p.h1)
+    ctx = mg.Context(0).set_tree(p.tree, p.conn)
+    mg.freebc_set(ctx, dim, level, (1, 1), f)
+    return p, ctx, level, f
+
+
+@pytest.mark.parametrize("dim,stencil", CASES)
+def test_freebc_sources_and_b(dim, stencil):
+    p, ctx, level, f = setup(dim, stencil)
+    rng = np.random.default_rng(3)
+    u = rng.standard_normal(p.b.shape)
+    q = rng.standard_normal(p.b.shape)
+    qo = q.copy()
+    bo = fo.freebc(qo, u, p.h1, p.s, p.tree, p.conn, dim, level, f)
+    import torch
+    qg, ug = torch_cuda(q), torch_cuda(u)
+    bg = torch.zeros(len(f), dtype=torch.float64, device="cuda")
+    mg.freebc_(ctx, qg, ug, p.h1, p.s, b_out=bg)
+    ctx.synchronize()
+    qn = qg.cpu().numpy()
+    assert rel_l2(bg.cpu().numpy(), bo) <= REL
+    changed = qo != q
+    assert changed.any()
+    np.testing.assert_array_equal(qn[~changed], q[~changed])
+    assert rel_l2(qn[changed] - q[changed], qo[changed] - q[changed]) <= REL
+    # the host-array entry point gives the same result
+    qh = q.copy()
+    bh = np.zeros(len(f))
+    mg.freebc_(ctx, qh, u, p.h1, p.s, b_out=bh)
+    np.testing.assert_array_equal(qh, qn)
+    np.testing.assert_array_equal(bh, bg.cpu().numpy())
+    ctx.close()
+
+
+@pytest.mark.parametrize("dim,stencil", CASES)
+def test_fill_ghost_free(dim, stencil):
+    p, ctx, level, f = setup(dim, stencil)
+    rng = np.random.default_rng(4)
+    u = rng.standard_normal(p.b.shape)
+    q = rng.standard_normal(p.b.shape)
+    bo = fo.freebc(q.copy(), u, p.h1, p.s, p.tree, p.conn, dim, level, f)
+    mg.freebc_(ctx, q.copy(), u, p.h1, p.s)
+    w = rng.standard_normal(p.b.shape)
+    for l in range(1, len(p.tree) + 1):
+        wo = w.copy()
+        fo.fill_ghost_free(wo, bo, p.tree, dim, level, l)
+        wg = torch_cuda(w)
+        mg.fill_ghost_free_(ctx, wg, l)
+        ctx.synchronize()
+        wn = wg.cpu().numpy()
+        changed = wo != w
+        np.testing.assert_array_equal(wn[~changed], w[~changed])
+        if changed.any():
+            assert rel_l2(wn[changed] - w[changed], wo[changed] - w[changed]) <= REL, l
+    ctx.close()
+
+
+@pytest.mark.parametrize("dim", [1, 2])
+def test_free_boundary_end_to_end(dim):
+    """derivs!'s sequence (src/streamer.jl:320-334): homogeneous solve, freebc!, main
+    solve, on the GPU against the oracle."""
+    p, ctx, level, f = setup(dim, "star")
+    o = Oracle(p)
+    q = p.b.copy()
+    o.fill_ghost_all(q)
+    uh = np.zeros_like(q)
+    st = mg.solve(ctx, uh, q.copy(), p.s, p.geom, p.bc, tol=1e-12, mode=mg.MODE_FP64, max_cycles=3000)
+    assert st["rel_residual"] <= 1e-12
+    q1 = q.copy()
+    mg.freebc_(ctx, q1, uh, p.h1, p.s)
+    u = np.zeros_like(q)
+    st = mg.solve(ctx, u, q1, p.s, p.geom, p.bc, tol=1e-12, mode=mg.MODE_FP64, max_cycles=3000)
+    assert st["rel_residual"] <= 1e-12
+    uho = np.zeros_like(q)
+    o.solve(uho, q.copy(), 1e-12, 3000)
+    q1o = q.copy()
+    fo.freebc(q1o, uho, p.h1, p.s, p.tree, p.conn, dim, level, f)
+    uo = np.zeros_like(q)
+    o.solve(uo, q1o, 1e-12, 3000)
+    used = np.zeros(p.nblk, dtype=bool)
+    for layer in p.tree:
+        for _, blk in layer.pairs:
+            used[blk - 1] = True
+    assert rel_l2(u[used][:, 2:18, 2:18], uo[used][:, 2:18, 2:18]) <= 1e-10
+    ctx.close()
+
+
+def test_freebc_refuses_bad_use():
+    p = gen.outer_refined_problem(1, STAR2)
+    ctx = mg.Context(0).set_tree(p.tree, p.conn)
+    q = np.zeros_like(p.b)
+    with pytest.raises(mg.SrmgError) as ei:           # no srmg_freebc_set yet
+        mg.freebc_(ctx, q, q.copy(), p.h1, p.s)
+    assert ei.value.code == SRMG_ERR_BADARG
+    n, H, R, f = fo.kernel(1, 5, (1, 1), p.h1)          # level 5 < the tree's finest (6)
+    mg.freebc_set(ctx, 1, 5, (1, 1), f)
+    with pytest.raises(mg.SrmgError) as ei:
+        mg.freebc_(ctx, q, q.copy(), p.h1, p.s)
+    assert ei.value.code == SRMG_ERR_BADARG
+    with pytest.raises(mg.SrmgError):                   # n does not match FreeBC's length
+        mg.freebc_set(ctx, 1, 7, (1, 1), f)
+    ctx.close()
