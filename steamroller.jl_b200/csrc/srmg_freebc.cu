@@ -75,13 +75,20 @@ __device__ __forceinline__ double block_sum(double v) {
   return r;  // valid in thread 0
 }
 
-// y = DST-II(x)
+// y = DST-II(x).  The table index (2j + 1)(k + 1) mod 4n advances by a fixed step per
+// iteration of a thread, reduced by one conditional subtraction (4n < 2^31).
 __global__ void __launch_bounds__(kDstThreads) k_dst2(double *__restrict__ y, const double *__restrict__ x,
                                                       const double *__restrict__ tab, int64_t n) {
-  const int64_t m4 = 4 * n;
+  const int m4 = (int)(4 * n);
   for (int64_t k = blockIdx.x; k < n; k += gridDim.x) {
     double acc = 0.0;
-    for (int64_t j = threadIdx.x; j < n; j += kDstThreads) acc += x[j] * tab[((2 * j + 1) * (k + 1)) % m4];
+    int t = (int)(((2 * (int64_t)threadIdx.x + 1) * (k + 1)) % m4);
+    const int step = (int)((2 * (int64_t)kDstThreads * (k + 1)) % m4);
+    for (int64_t j = threadIdx.x; j < n; j += kDstThreads) {
+      acc += x[j] * tab[t];
+      t += step;
+      if (t >= m4) t -= m4;
+    }
     const double s = block_sum(acc);
     if (threadIdx.x == 0) y[k] = 2.0 * s;
     __syncthreads();
@@ -93,10 +100,16 @@ __global__ void __launch_bounds__(kDstThreads) k_dst3_scale(double *__restrict__
                                                             const double *__restrict__ f,
                                                             const double *__restrict__ tab, int64_t n, double h,
                                                             double p2) {
-  const int64_t m4 = 4 * n;
+  const int m4 = (int)(4 * n);
   for (int64_t k = blockIdx.x; k < n; k += gridDim.x) {
     double acc = 0.0;
-    for (int64_t j = threadIdx.x; j < n - 1; j += kDstThreads) acc += (f[j] * a[j]) * tab[((j + 1) * (2 * k + 1)) % m4];
+    int t = (int)(((int64_t)threadIdx.x + 1) * (2 * k + 1) % m4);
+    const int step = (int)((int64_t)kDstThreads * (2 * k + 1) % m4);
+    for (int64_t j = threadIdx.x; j < n - 1; j += kDstThreads) {
+      acc += (f[j] * a[j]) * tab[t];
+      t += step;
+      if (t >= m4) t -= m4;
+    }
     const double s = block_sum(acc);
     if (threadIdx.x == 0) {
       const double last = f[n - 1] * a[n - 1];
