@@ -32,7 +32,7 @@ class _Tree(ctypes.Structure):
 
 class _Op(ctypes.Structure):
     _fields_ = [("op", ctypes.c_int), ("k2", ctypes.c_double), ("geom", ctypes.c_int),
-                ("bc", ctypes.c_int8 * 9)]
+                ("bc", ctypes.c_int8 * 9), ("bc27", ctypes.c_int8 * 27)]
 
 
 def build():
@@ -72,6 +72,24 @@ def lib():
             "orc_solve": (I, [PP, PP, PP, PP, D, TP, OP, I, I, I, D, D, I, ctypes.POINTER(D)]),
             "orc_netcharge": (None, [PP, PP, PP, TP]),
             "orc_electric_field": (None, [PP, PP, PP, D, PP, TP]),
+            "orc3_tree_index": (None, [TP]),
+            "orc3_fill_ghost_copy": (None, [PP, TP, I]),
+            "orc3_fill_ghost_bnd": (None, [PP, TP, I, PP]),
+            "orc3_fill_ghost_interp": (None, [PP, TP, I]),
+            "orc3_fill_ghost": (None, [PP, TP, I, PP]),
+            "orc3_restrict_level": (None, [PP, TP, I]),
+            "orc3_interp_add_level": (None, [PP, PP, TP, I]),
+            "orc3_gs_level": (None, [PP, PP, D, D, TP, I, OP, I]),
+            "orc3_gs4_level": (None, [PP, PP, D, D, TP, I, OP, I, I]),
+            "orc3_gs_iter": (None, [PP, PP, D, D, I, I, TP, OP]),
+            "orc3_residual_level": (None, [PP, PP, PP, D, TP, I, OP]),
+            "orc3_residual_postrestrict_level": (None, [PP, PP, PP, D, TP, I, OP]),
+            "orc3_rhs_level": (None, [PP, PP, TP, I, OP]),
+            "orc3_vcycle": (None, [PP, PP, PP, PP, D, TP, OP, I, I, I, I, D]),
+            "orc3_fmg": (None, [PP, PP, PP, PP, D, TP, OP, I, I, I, D]),
+            "orc3_resnorm": (D, [PP, PP, PP, D, TP, OP]),
+            "orc3_leafnorm": (D, [PP, PP, TP]),
+            "orc3_solve": (I, [PP, PP, PP, PP, D, TP, OP, I, I, I, D, D, I, ctypes.POINTER(D)]),
             "orc_set_threads": (None, [I]),
             "orc_get_threads": (I, []),
         }
@@ -93,6 +111,7 @@ class OracleTree:
 
     def __init__(self, tree, conn, nblk_alloc, M=16, G=2):
         nlev = len(tree)
+        D = getattr(tree, "D", 2)
         self._keep = []
         pairs = [np.ascontiguousarray(layer.pairs_array()) for layer in tree]
 
@@ -113,12 +132,13 @@ class OracleTree:
             n, p = arrs(lists)
             setattr(t, "n" + field, ctypes.cast(n, _I64P))
             setattr(t, field, ctypes.cast(p, ctypes.POINTER(_P)))
-        self.coord_of = np.zeros(2 * nblk_alloc, dtype=np.int64)
+        # orc3_tree has orc_tree's layout; only the edge records and coord_of differ
+        self.coord_of = np.zeros(D * nblk_alloc, dtype=np.int64)
         t.nblk_alloc = nblk_alloc
         t.coord_of = self.coord_of.ctypes.data_as(_I64P)
         self.t = t
         self.nlev = nlev
-        lib().orc_tree_index(ctypes.byref(t))
+        (lib().orc3_tree_index if D == 3 else lib().orc_tree_index)(ctypes.byref(t))
 
     @property
     def ref(self):
@@ -128,8 +148,12 @@ class OracleTree:
 def make_op(op, k2, geom, bc):
     o = _Op()
     o.op, o.k2, o.geom = op, k2, geom
-    for i in range(9):
-        o.bc[i] = int(bc[i])
+    if len(bc) == 27:
+        for i in range(27):
+            o.bc27[i] = int(bc[i])
+    else:
+        for i in range(9):
+            o.bc[i] = int(bc[i])
     return o
 
 
@@ -181,4 +205,49 @@ class Oracle:
         c = lib().orc_solve(_ptr(u), _ptr(b), _ptr(r), _ptr(u1), self.p.s, self.ot.ref,
                             ctypes.byref(self.op), ndown, ntop, nup, omega, tol, max_cycles,
                             ctypes.byref(rel))
+        return c, rel.value
+
+
+class Oracle3:
+    """The D = 3 oracle (srmg_oracle3.c) for a Problem3-like object with tree, conn, b
+    ([nblk, 20, 20, 20]), s, op, k2 and a 27-entry bc."""
+
+    def __init__(self, problem, threads=None):
+        self.p = problem
+        self.ot = OracleTree(problem.tree, problem.conn, problem.nblk)
+        self.op = make_op(problem.op, problem.k2, 0, problem.bc)
+        self._bc, self._bcp = bc_ptr(problem.bc)
+        if threads:
+            lib().orc_set_threads(threads)
+
+    def fill_ghost(self, u, l):
+        lib().orc3_fill_ghost(_ptr(u), self.ot.ref, l, self._bcp)
+
+    def fill_ghost_all(self, u):
+        for l in range(1, self.ot.nlev + 1):
+            self.fill_ghost(u, l)
+
+    def rhs_level(self, q1, q, l):
+        lib().orc3_rhs_level(_ptr(q1), _ptr(q), self.ot.ref, l, ctypes.byref(self.op))
+
+    def vcycle(self, u, b, r, u1, lmax=0, ndown=2, ntop=4, nup=2, omega=1.0, s=None):
+        lib().orc3_vcycle(_ptr(u), _ptr(b), _ptr(r), _ptr(u1), self.p.s if s is None else s, self.ot.ref,
+                          ctypes.byref(self.op), lmax, ndown, ntop, nup, omega)
+
+    def fmg(self, u, b, r, u1, ndown=2, ntop=4, nup=2, omega=1.25):
+        lib().orc3_fmg(_ptr(u), _ptr(b), _ptr(r), _ptr(u1), self.p.s, self.ot.ref, ctypes.byref(self.op),
+                       ndown, ntop, nup, omega)
+
+    def resnorm(self, r, b, u):
+        return lib().orc3_resnorm(_ptr(r), _ptr(b), _ptr(u), self.p.s, self.ot.ref, ctypes.byref(self.op))
+
+    def leafnorm(self, f):
+        scratch = np.empty_like(f)
+        return lib().orc3_leafnorm(_ptr(scratch), _ptr(f), self.ot.ref)
+
+    def solve(self, u, b, tol, max_cycles=500, ndown=2, ntop=4, nup=2, omega=1.0):
+        r, u1 = np.zeros_like(u), np.zeros_like(u)
+        rel = ctypes.c_double()
+        c = lib().orc3_solve(_ptr(u), _ptr(b), _ptr(r), _ptr(u1), self.p.s, self.ot.ref, ctypes.byref(self.op),
+                             ndown, ntop, nup, omega, tol, max_cycles, ctypes.byref(rel))
         return c, rel.value
