@@ -78,10 +78,18 @@ typedef struct { int64_t fine, coarse; int64_t subblock[2]; } srmg_child;
 
 typedef struct srmg_ctx srmg_ctx;
 
-/* Create a context on CUDA device `device` (D, M, G must be 2, 16, 2).  The context
- * owns a CUDA stream, the device copy of the tree and the device mirrors of fields
- * passed through the host-pointer entry points.  No counterpart in the reference
- * (its state lives in Julia objects). */
+/* Create a context on CUDA device `device` (M = 16, G = 2; D = 2, or D = 3 for a
+ * three-dimensional tree).  The context owns a CUDA stream, the device copy of the tree
+ * and the device mirrors of fields passed through the host-pointer entry points.  No
+ * counterpart in the reference (its state lives in Julia objects).
+ * D = 3 (Cartesian, the only geometry with 3D stencils in the reference,
+ * src/laplacian.jl:274-340, src/helmholtz.jl:74-100): the tree is set with
+ * srmg_set_tree3; fields are 20^3 doubles per block (i fastest, then j, then k);
+ * boundary tables have 27 entries (a[2+b1, 2+b2, 2+b3], column-major); ops 0, 1 and 2
+ * (order 4 needs a BoxStencil{3} connectivity).  The multigrid entry points (vcycle,
+ * fmg, resnorm, the ghost fills and per-level operations, rhs_level, FP64 srmg_solve)
+ * run on the per-operation kernels in FP64; the other entry points return
+ * SRMG_ERR_UNSUPPORTED for a D = 3 context. */
 int srmg_create(srmg_ctx **ctx, int D, int M, int G, int device);
 void srmg_destroy(srmg_ctx *ctx);
 const char *srmg_last_error(const srmg_ctx *ctx);
@@ -104,6 +112,23 @@ int srmg_set_tree(srmg_ctx *ctx, int nlev,
                   const int64_t *nchild, const srmg_child *const *child,
                   uint64_t generation);
 uint64_t srmg_tree_generation(const srmg_ctx *ctx);
+
+/* D = 3: the isbits layouts of Pair{CartesianIndex{3},Int}, Neighbor{3}, Boundary{3},
+ * RefBoundary{3} and Child{3} (src/blocklayer.jl:23, src/connectivity.jl:6-42). */
+typedef struct { int64_t coord[3]; int64_t blk; } srmg_pair3;
+typedef struct { int64_t from, to; int64_t face[3]; } srmg_neighbor3;
+typedef struct { int64_t block; int64_t face[3]; int64_t bnd[3]; int64_t level; } srmg_boundary3;
+typedef struct { int64_t fine, coarse; int64_t face[3]; int64_t subblock[3]; } srmg_refbnd3;
+typedef struct { int64_t fine, coarse; int64_t subblock[3]; } srmg_child3;
+/* srmg_set_tree for a context created with D = 3 (any face in {-1,0,1}^3 but the
+ * origin: StarStencil{3} or BoxStencil{3} connectivity). */
+int srmg_set_tree3(srmg_ctx *ctx, int nlev,
+                   const int64_t *npairs, const srmg_pair3 *const *pairs,
+                   const int64_t *nneighbor, const srmg_neighbor3 *const *neighbor,
+                   const int64_t *nboundary, const srmg_boundary3 *const *boundary,
+                   const int64_t *nrefbnd, const srmg_refbnd3 *const *refbnd,
+                   const int64_t *nchild, const srmg_child3 *const *child,
+                   uint64_t generation);
 
 /* ---- the ccall boundary: HOST pointers (Julia-owned arrays) --------------------- */
 

@@ -60,7 +60,7 @@ int srmg::ensure(srmg_ctx *ctx, DevBuf &b, size_t bytes) {
 extern "C" int srmg_create(srmg_ctx **out, int D, int M, int G, int device) {
   if (!out) return SRMG_ERR_BADARG;
   *out = nullptr;
-  if (D != 2 || M != kM || G != kG) return SRMG_ERR_UNSUPPORTED;
+  if ((D != 2 && D != 3) || M != kM || G != kG) return SRMG_ERR_UNSUPPORTED;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
     return SRMG_ERR_CUDA;
@@ -74,6 +74,7 @@ extern "C" int srmg_create(srmg_ctx **out, int D, int M, int G, int device) {
     return SRMG_ERR_CUDA;
   }
   ctx->stream = ctx->own_stream;
+  ctx->D = D;
   if (ensure(ctx, ctx->small, 64 * sizeof(double))) {
     delete ctx;
     return SRMG_ERR_NOMEM;
@@ -82,10 +83,11 @@ extern "C" int srmg_create(srmg_ctx **out, int D, int M, int G, int device) {
   return SRMG_OK;
 }
 
-static void free_tree(srmg_ctx *ctx) {
+void srmg::free_tree(srmg_ctx *ctx) {
   if (ctx->d_tree) cudaFree(ctx->d_tree);
   ctx->d_tree = nullptr;
   ctx->lv.clear();
+  ctx->lv3.clear();
   ctx->nblk_host.clear();
   ctx->nch_host.clear();
   ctx->has_tree = false;
@@ -162,6 +164,7 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
                      const int64_t *nch, const srmg_child *const *ch, uint64_t generation,
                      const std::vector<int> *item_of, int nitems) {
   if (!ctx) return SRMG_ERR_BADARG;
+  if (ctx->D != 2) return fail(ctx, SRMG_ERR_BADARG, "a context created with D = 3 takes srmg_set_tree3");
   if (nlev < 1 || nlev > 30 || !npairs || !pairs || !nnb || !nb || !nbd || !bd || !nrb || !rb ||
       !nch || !ch)
     return fail(ctx, SRMG_ERR_BADARG, "srmg_set_tree: bad level count or null arrays");
@@ -556,6 +559,13 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
 
 int srmg::check_call(srmg_ctx *ctx, int64_t nblk_alloc, int op, int geom, const int8_t *bc) {
   if (!ctx) return SRMG_ERR_BADARG;
+  if (ctx->D != 2)
+    return fail(ctx, SRMG_ERR_UNSUPPORTED, "three-dimensional trees support the multigrid entry points only");
+  return check_call_any(ctx, nblk_alloc, op, geom, bc);
+}
+
+int srmg::check_call_any(srmg_ctx *ctx, int64_t nblk_alloc, int op, int geom, const int8_t *bc) {
+  if (!ctx) return SRMG_ERR_BADARG;
   if (!ctx->has_tree) return fail(ctx, SRMG_ERR_NOTREE, "no tree: call srmg_set_tree first");
   if (nblk_alloc < ctx->max_blk)
     return fail(ctx, SRMG_ERR_BADARG, "field holds %lld blocks but the tree uses block %lld",
@@ -565,8 +575,10 @@ int srmg::check_call(srmg_ctx *ctx, int64_t nblk_alloc, int op, int geom, const 
   if (op == SRMG_OP_LAPLACIAN4 && !ctx->has_corners)
     return fail(ctx, SRMG_ERR_UNSUPPORTED, "the order-4 discretisation needs a BoxStencil connectivity");
   if (geom < 0 || geom > 2) return fail(ctx, SRMG_ERR_UNSUPPORTED, "unsupported geometry %d", geom);
+  if (ctx->D == 3 && geom != 0)
+    return fail(ctx, SRMG_ERR_UNSUPPORTED, "three-dimensional trees take the Cartesian geometry only");
   if (bc) {
-    for (int i = 0; i < 9; i++)
+    for (int i = 0; i < (ctx->D == 3 ? 27 : 9); i++)
       if (bc[i] < -1 || bc[i] > 1) return fail(ctx, SRMG_ERR_BADARG, "boundary table entries must be -1, 0 or 1");
   }
   cudaSetDevice(ctx->device);
@@ -921,9 +933,14 @@ extern "C" int srmg_vcycle_dev(srmg_ctx *ctx, double *u, double *b, double *r, d
                                int64_t nblk_alloc, double s, int op, double k2, int geom,
                                const int8_t bc[9], int lmax, int ndown, int ntop, int nup,
                                double omega, int ncycles) {
-  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  RC(check_call_any(ctx, nblk_alloc, op, geom, bc));
   if (!u || !b || !r || !u1 || ndown < 0 || ntop < 0 || nup < 0 || ncycles < 0)
     return fail(ctx, SRMG_ERR_BADARG, "srmg_vcycle: bad arguments");
+  if (ctx->D == 3) {
+    for (int c = 0; c < ncycles; c++) RC(d3_vcycle(ctx, u, b, r, u1, s, op, k2, bc, lmax, ndown, ntop, nup, omega));
+    CK(cudaGetLastError());
+    return SRMG_OK;
+  }
   const Signs sg = make_signs(bc);
   for (int c = 0; c < ncycles; c++)
     RC(vcycle_dev<double>(ctx, u, b, r, u1, s, op, k2, geom, sg, lmax, ndown, ntop, nup, omega));
@@ -934,9 +951,10 @@ extern "C" int srmg_vcycle_dev(srmg_ctx *ctx, double *u, double *b, double *r, d
 extern "C" int srmg_fmg_dev(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
                             int64_t nblk_alloc, double s, int op, double k2, int geom,
                             const int8_t bc[9], int ndown, int ntop, int nup, double omega) {
-  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  RC(check_call_any(ctx, nblk_alloc, op, geom, bc));
   if (!u || !b || !r || !u1) return fail(ctx, SRMG_ERR_BADARG, "srmg_fmg: null field");
-  RC(fmg_dev_t<double>(ctx, u, b, r, u1, s, op, k2, geom, make_signs(bc), ndown, ntop, nup, omega));
+  if (ctx->D == 3) RC(d3_fmg(ctx, u, b, r, u1, s, op, k2, bc, ndown, ntop, nup, omega));
+  else RC(fmg_dev_t<double>(ctx, u, b, r, u1, s, op, k2, geom, make_signs(bc), ndown, ntop, nup, omega));
   CK(cudaGetLastError());
   return SRMG_OK;
 }
@@ -944,10 +962,11 @@ extern "C" int srmg_fmg_dev(srmg_ctx *ctx, double *u, double *b, double *r, doub
 extern "C" int srmg_resnorm_dev(srmg_ctx *ctx, double *r, const double *b, const double *u,
                                 int64_t nblk_alloc, double s, int op, double k2, int geom,
                                 const int8_t bc[9], double *out) {
-  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  RC(check_call_any(ctx, nblk_alloc, op, geom, bc));
   (void)r;
   if (!b || !u || !out) return fail(ctx, SRMG_ERR_BADARG, "srmg_resnorm: null argument");
-  RC(leafnorm_dev<double>(ctx, u, b, s, op, k2, geom, 0, 0));
+  if (ctx->D == 3) RC(d3_leafnorm(ctx, u, b, s, op, k2, 0, 0));
+  else RC(leafnorm_dev<double>(ctx, u, b, s, op, k2, geom, 0, 0));
   RC(read_small(ctx, 1));
   *out = ctx->h_small[0];
   return SRMG_OK;
@@ -955,9 +974,10 @@ extern "C" int srmg_resnorm_dev(srmg_ctx *ctx, double *r, const double *b, const
 
 extern "C" int srmg_fill_ghost_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level,
                                    const int8_t bc[9], int mask) {
-  RC(check_call(ctx, nblk_alloc, 0, 0, bc));
+  RC(check_call_any(ctx, nblk_alloc, 0, 0, bc));
   if (!u || level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "fill_ghost: bad level");
-  RC(L_fill_ghost<double>(ctx, u, level, make_signs(bc), mask));
+  if (ctx->D == 3) RC(d3_fill_ghost(ctx, u, level, bc, mask));
+  else RC(L_fill_ghost<double>(ctx, u, level, make_signs(bc), mask));
   CK(cudaGetLastError());
   return SRMG_OK;
 }
@@ -965,10 +985,15 @@ extern "C" int srmg_fill_ghost_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc,
 extern "C" int srmg_gs_level_dev(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc,
                                  int level, double omega, double sl, int op, double k2, int geom,
                                  int parity) {
-  RC(check_call(ctx, nblk_alloc, op, geom, nullptr));
+  RC(check_call_any(ctx, nblk_alloc, op, geom, nullptr));
   const int ncol = op == SRMG_OP_LAPLACIAN4 ? 4 : 2;
   if (!u || !b || level < 1 || level > ctx->nlev || parity < 0 || parity >= ncol)
     return fail(ctx, SRMG_ERR_BADARG, "gs_level: bad arguments");
+  if (ctx->D == 3) {
+    RC(d3_gs_level(ctx, u, b, level, omega, sl, op, k2, parity));
+    CK(cudaGetLastError());
+    return SRMG_OK;
+  }
   RC(L_gs_colour<double>(ctx, u, b, level, op_params<double>(op, geom, k2, sl, omega), parity));
   CK(cudaGetLastError());
   return SRMG_OK;
@@ -977,9 +1002,14 @@ extern "C" int srmg_gs_level_dev(srmg_ctx *ctx, double *u, const double *b, int6
 extern "C" int srmg_gs_iter_dev(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc,
                                 int level, double omega, double sl, int n, int op, double k2,
                                 int geom, const int8_t bc[9]) {
-  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  RC(check_call_any(ctx, nblk_alloc, op, geom, bc));
   if (!u || !b || level < 1 || level > ctx->nlev || n < 0)
     return fail(ctx, SRMG_ERR_BADARG, "gs_iter: bad arguments");
+  if (ctx->D == 3) {
+    RC(d3_gs_iter(ctx, u, b, level, omega, sl, n, op, k2, bc));
+    CK(cudaGetLastError());
+    return SRMG_OK;
+  }
   const bool aligned = ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(b)) & 15) == 0;
   if (ctx->use_engine && aligned && !ctx->has_corners && op != SRMG_OP_LAPLACIAN4) {
     ItemTabs tabs;
@@ -995,26 +1025,33 @@ extern "C" int srmg_gs_iter_dev(srmg_ctx *ctx, double *u, const double *b, int64
 extern "C" int srmg_residual_level_dev(srmg_ctx *ctx, double *r, const double *u, const double *b,
                                        int64_t nblk_alloc, int level, double sl, int op, double k2,
                                        int geom) {
-  RC(check_call(ctx, nblk_alloc, op, geom, nullptr));
+  RC(check_call_any(ctx, nblk_alloc, op, geom, nullptr));
   if (!r || !u || !b || level < 1 || level > ctx->nlev)
     return fail(ctx, SRMG_ERR_BADARG, "residual_level: bad arguments");
-  RC(L_residual<double>(ctx, r, u, b, level, op_params<double>(op, geom, k2, sl, 1.0)));
+  if (ctx->D == 3) RC(d3_residual_level(ctx, r, u, b, level, sl, op, k2));
+  else RC(L_residual<double>(ctx, r, u, b, level, op_params<double>(op, geom, k2, sl, 1.0)));
   CK(cudaGetLastError());
   return SRMG_OK;
 }
 
 extern "C" int srmg_restrict_level_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level) {
-  RC(check_call(ctx, nblk_alloc, 0, 0, nullptr));
+  RC(check_call_any(ctx, nblk_alloc, 0, 0, nullptr));
   if (!u || level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "restrict_level: bad level");
-  RC(L_restrict<double>(ctx, u, level));
+  if (ctx->D == 3) RC(d3_restrict_level(ctx, u, level));
+  else RC(L_restrict<double>(ctx, u, level));
   CK(cudaGetLastError());
   return SRMG_OK;
 }
 
 extern "C" int srmg_rhs_level_dev(srmg_ctx *ctx, double *q1, const double *q, int64_t nblk_alloc, int level,
                                   int op, int geom) {
-  RC(check_call(ctx, nblk_alloc, op, geom, nullptr));
+  RC(check_call_any(ctx, nblk_alloc, op, geom, nullptr));
   if (!q1 || !q || level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "rhs_level: bad arguments");
+  if (ctx->D == 3) {
+    RC(d3_rhs_level(ctx, q1, q, level, op));
+    CK(cudaGetLastError());
+    return SRMG_OK;
+  }
   const DevLevel &L = ctx->lv[level - 1];
   if (L.nblk > 0) {
     k_rhs<double><<<grid_for((int64_t)L.nblk * 256, 256, kGridCap), 256, 0, ctx->stream>>>(q1, q, L.view(level),
@@ -1027,10 +1064,11 @@ extern "C" int srmg_rhs_level_dev(srmg_ctx *ctx, double *q1, const double *q, in
 
 extern "C" int srmg_interp_add_level_dev(srmg_ctx *ctx, double *u, const double *u1,
                                          int64_t nblk_alloc, int level) {
-  RC(check_call(ctx, nblk_alloc, 0, 0, nullptr));
+  RC(check_call_any(ctx, nblk_alloc, 0, 0, nullptr));
   if (!u || !u1 || level < 1 || level > ctx->nlev)
     return fail(ctx, SRMG_ERR_BADARG, "interp_add_level: bad level");
-  RC(L_interp_add<double>(ctx, u, u1, level));
+  if (ctx->D == 3) RC(d3_interp_add_level(ctx, u, u1, level));
+  else RC(L_interp_add<double>(ctx, u, u1, level));
   CK(cudaGetLastError());
   return SRMG_OK;
 }
@@ -1038,10 +1076,11 @@ extern "C" int srmg_interp_add_level_dev(srmg_ctx *ctx, double *u, const double 
 extern "C" int srmg_residual_postrestrict_level_dev(srmg_ctx *ctx, double *b, const double *u,
                                                     const double *r, int64_t nblk_alloc, int level,
                                                     double s, int op, double k2, int geom) {
-  RC(check_call(ctx, nblk_alloc, op, geom, nullptr));
+  RC(check_call_any(ctx, nblk_alloc, op, geom, nullptr));
   if (!b || !u || !r || level < 1 || level > ctx->nlev)
     return fail(ctx, SRMG_ERR_BADARG, "postrestrict: bad arguments");
-  RC(L_postrestrict<double>(ctx, b, u, r, level, op_params<double>(op, geom, k2, s, 1.0)));
+  if (ctx->D == 3) RC(d3_postrestrict_level(ctx, b, u, r, level, s, op, k2));
+  else RC(L_postrestrict<double>(ctx, b, u, r, level, op_params<double>(op, geom, k2, s, 1.0)));
   CK(cudaGetLastError());
   return SRMG_OK;
 }
@@ -1050,7 +1089,7 @@ extern "C" int srmg_residual_postrestrict_level_dev(srmg_ctx *ctx, double *b, co
 
 // Copy host fields into the context's device mirrors (slot i of f64).
 int srmg::stage_in(srmg_ctx *ctx, int slot, const double *h, int64_t nblk_alloc, double **d) {
-  const size_t bytes = (size_t)nblk_alloc * kSS * sizeof(double);
+  const size_t bytes = (size_t)nblk_alloc * block_elems(ctx) * sizeof(double);
   RC(ensure(ctx, ctx->f64[slot], bytes));
   *d = (double *)ctx->f64[slot].p;
   if (h) CK(cudaMemcpyAsync(*d, h, bytes, cudaMemcpyHostToDevice, ctx->stream));
@@ -1058,7 +1097,7 @@ int srmg::stage_in(srmg_ctx *ctx, int slot, const double *h, int64_t nblk_alloc,
 }
 
 int srmg::stage_out(srmg_ctx *ctx, double *h, const double *d, int64_t nblk_alloc) {
-  const size_t bytes = (size_t)nblk_alloc * kSS * sizeof(double);
+  const size_t bytes = (size_t)nblk_alloc * block_elems(ctx) * sizeof(double);
   CK(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
   return SRMG_OK;
 }
@@ -1067,7 +1106,7 @@ extern "C" int srmg_vcycle(srmg_ctx *ctx, double *u, double *b, double *r, doubl
                            int64_t nblk_alloc, double s, int op, double k2, int geom,
                            const int8_t bc[9], int lmax, int ndown, int ntop, int nup, double omega,
                            int ncycles) {
-  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  RC(check_call_any(ctx, nblk_alloc, op, geom, bc));
   if (!u || !b) return fail(ctx, SRMG_ERR_BADARG, "srmg_vcycle: null field");
   (void)r;
   (void)u1;
@@ -1087,7 +1126,7 @@ extern "C" int srmg_vcycle(srmg_ctx *ctx, double *u, double *b, double *r, doubl
 extern "C" int srmg_fmg(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
                         int64_t nblk_alloc, double s, int op, double k2, int geom,
                         const int8_t bc[9], int ndown, int ntop, int nup, double omega) {
-  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  RC(check_call_any(ctx, nblk_alloc, op, geom, bc));
   if (!u || !b) return fail(ctx, SRMG_ERR_BADARG, "srmg_fmg: null field");
   (void)r;
   (void)u1;
@@ -1106,7 +1145,7 @@ extern "C" int srmg_fmg(srmg_ctx *ctx, double *u, double *b, double *r, double *
 extern "C" int srmg_resnorm(srmg_ctx *ctx, double *r, const double *b, const double *u,
                             int64_t nblk_alloc, double s, int op, double k2, int geom,
                             const int8_t bc[9], double *out) {
-  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  RC(check_call_any(ctx, nblk_alloc, op, geom, bc));
   if (!b || !u || !out) return fail(ctx, SRMG_ERR_BADARG, "srmg_resnorm: null argument");
   double *du, *db;
   RC(stage_in(ctx, 0, u, nblk_alloc, &du));
@@ -1117,7 +1156,7 @@ extern "C" int srmg_resnorm(srmg_ctx *ctx, double *r, const double *b, const dou
 
 extern "C" int srmg_rhs_level(srmg_ctx *ctx, double *q1, const double *q, int64_t nblk_alloc, int level, int op,
                               int geom) {
-  RC(check_call(ctx, nblk_alloc, op, geom, nullptr));
+  RC(check_call_any(ctx, nblk_alloc, op, geom, nullptr));
   if (!q1 || !q) return fail(ctx, SRMG_ERR_BADARG, "srmg_rhs_level: null field");
   double *dq1, *dq;
   RC(stage_in(ctx, 0, q1, nblk_alloc, &dq1));
@@ -1130,7 +1169,7 @@ extern "C" int srmg_rhs_level(srmg_ctx *ctx, double *q1, const double *q, int64_
 
 extern "C" int srmg_fill_ghost(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level,
                                const int8_t bc[9]) {
-  RC(check_call(ctx, nblk_alloc, 0, 0, bc));
+  RC(check_call_any(ctx, nblk_alloc, 0, 0, bc));
   if (!u) return fail(ctx, SRMG_ERR_BADARG, "srmg_fill_ghost: null field");
   double *du;
   RC(stage_in(ctx, 0, u, nblk_alloc, &du));

@@ -1,0 +1,746 @@
+// srmg3.cu -- the multigrid field solve on three-dimensional block trees (D = 3,
+// CartesianGeometry: the only geometry with 3D stencils in the reference,
+// src/laplacian.jl:274-340, src/helmholtz.jl:74-100).
+//
+// A 3D context (srmg_create with D = 3) holds an octree uploaded by srmg_set_tree3 and
+// runs the per-operation path in FP64: every generic entry point (vcycle, fmg,
+// resnorm, the ghost fills, the per-level operations, rhs_level, FP64 solve) checks
+// the context's dimension and lands here.  Blocks are 20^3 doubles (16^3 valid cells
+// and 2 ghost layers), dimension 1 fastest; Julia passes pointer(u.u) as in 2D.
+//
+// Device tree, per level: blocks {blk, c1, c2, c3} (0-based id, 1-based coords), the
+// child mask per block (bit (s1-1) + 2(s2-1) + 4(s3-1) set when that octant has a
+// child), a pull table of 27 faces per block indexed by the ghost direction
+// (f1+1) + 3(f2+1) + 9(f3+1) (entry 13 unused): {type, source block, packed vector},
+// the packed vector holding a boundary's bnd or a refinement face's subblock as
+// 2-bit fields (component + 1), and the child edges {fine, coarse, packed subblock}.
+//
+// Operation order follows the dimension-generic reference code written out for
+// D = 3 (Base.Cartesian loops, first index innermost): ghost copies, mirrors and
+// interpolation (weights 1/4, src/interp.jl:7-11) and restriction (8 cells, / 8) are
+// bit-exact; stencils are accumulated in the reference's order without contraction.
+#include <cmath>
+#include <cstring>
+
+#include "srmg_ctx.h"
+#include "srmg_internal.h"
+
+using namespace srmg;
+
+#define CK(call)                                              \
+  do {                                                        \
+    int _rc = cuda_check(ctx, (call), #call);                 \
+    if (_rc) return _rc;                                      \
+  } while (0)
+#define RC(call)               \
+  do {                         \
+    int _rc = (call);          \
+    if (_rc) return _rc;       \
+  } while (0)
+
+namespace {
+
+constexpr int S = kS, S2 = kS * kS, S3 = kS * kS * kS;
+
+struct Signs27 { double v[27]; };
+
+__device__ __forceinline__ int o3(int x, int y, int z) { return x + S * y + S2 * z; }
+__device__ __forceinline__ int unpack(int packed, int d) { return ((packed >> (2 * d)) & 3) - 1; }
+
+// ---- ghost fills (src/connectivity.jl:155-258), one thread per ghost cell -----------
+// phase 1 copies from neighbours, 2 mirrors at the domain boundary, 4 interpolates from
+// the parent; fill_ghost! runs them in that order as three launches.
+__global__ void k3_fill(double *__restrict__ u, Level3View L, Signs27 sg, int phase) {
+  const int64_t total = (int64_t)L.nblk * S3;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t / S3), c = (int)(t % S3);
+    const int x = c % S, y = (c / S) % S, z = c / S2;
+    const int f1 = x < kG ? -1 : x >= kG + kM ? 1 : 0;
+    const int f2 = y < kG ? -1 : y >= kG + kM ? 1 : 0;
+    const int f3 = z < kG ? -1 : z >= kG + kM ? 1 : 0;
+    if (!f1 && !f2 && !f3) continue;
+    const int4 fi = L.faces[27 * bi + (f1 + 1) + 3 * (f2 + 1) + 9 * (f3 + 1)];
+    const int type = fi.x;
+    if ((type == FACE_NEIGHBOR && phase != 1) || (type == FACE_BOUNDARY && phase != 2) ||
+        (type == FACE_REFBND && phase != 4) || type == FACE_NONE)
+      continue;
+    double *ub = u + (int64_t)L.blocks[bi].x * S3;
+    if (type == FACE_NEIGHBOR) {
+      const double *src = u + (int64_t)fi.y * S3;
+      ub[c] = src[o3(x - kM * f1, y - kM * f2, z - kM * f3)];
+    } else if (type == FACE_BOUNDARY) {
+      const int b1 = unpack(fi.z, 0), b2 = unpack(fi.z, 1), b3 = unpack(fi.z, 2);
+      auto mir = [](int i, int b) { return b < 0 ? 2 * kG - 1 - i : b > 0 ? 2 * (kG + kM) - 1 - i : i; };
+      ub[c] = __dmul_rn(sg.v[(1 + b1) + 3 * (1 + b2) + 9 * (1 + b3)], ub[o3(mir(x, b1), mir(y, b2), mir(z, b3))]);
+    } else {
+      // interp! from the parent's subblockbnd cell: along a face dimension the parent's
+      // last (ghost below) or first (ghost above) subblock cell, else the subblock cell
+      // over this one; i_d is the child offset
+      const double *cb = u + (int64_t)fi.y * S3;
+      const int p[3] = {x, y, z}, f[3] = {f1, f2, f3};
+      int js[3], ii[3];
+      for (int d = 0; d < 3; ++d) {
+        const int sb = unpack(fi.z, d) + 1;
+        if (f[d] < 0) { js[d] = 1 + 8 * sb; ii[d] = p[d]; }
+        else if (f[d] > 0) { js[d] = 2 + 8 * (sb - 1); ii[d] = p[d] - (kG + kM); }
+        else { js[d] = 2 + 8 * (sb - 1) + ((p[d] - kG) >> 1); ii[d] = (p[d] - kG) & 1; }
+      }
+      const int o = o3(js[0], js[1], js[2]);
+      double v = __dmul_rn(0.25, cb[o]);
+      v = __dadd_rn(v, __dmul_rn(0.25, cb[o + (2 * ii[0] - 1)]));
+      v = __dadd_rn(v, __dmul_rn(0.25, cb[o + S * (2 * ii[1] - 1)]));
+      v = __dadd_rn(v, __dmul_rn(0.25, cb[o + S2 * (2 * ii[2] - 1)]));
+      ub[c] = v;
+    }
+  }
+}
+
+// ---- stencils: @stencil over the 3x3x3 literal, slab (third offset) slowest ---------
+__device__ __forceinline__ double lhs3(const double *ub, int o, int op, double centre) {
+  if (op == 2) {  // order 4: faces 2, edges 1, centre -24, corners absent; / 6
+    double v = 0.0;
+#pragma unroll
+    for (int d3 = -1; d3 <= 1; ++d3)
+#pragma unroll
+      for (int d2 = -1; d2 <= 1; ++d2)
+#pragma unroll
+        for (int d1 = -1; d1 <= 1; ++d1) {
+          const int nz = (d1 != 0) + (d2 != 0) + (d3 != 0);
+          if (nz == 3) continue;
+          const double c = nz == 0 ? -24.0 : nz == 1 ? 2.0 : 1.0;
+          v = __dadd_rn(v, __dmul_rn(c, ub[o + d1 + S * d2 + S2 * d3]));
+        }
+    return v / 6.0;
+  }
+  double v = 0.0;  // order 2: (0,0,-1), (0,-1,0), (-1,0,0), centre, (1,0,0), (0,1,0), (0,0,1)
+  v = __dadd_rn(v, ub[o - S2]);
+  v = __dadd_rn(v, ub[o - S]);
+  v = __dadd_rn(v, ub[o - 1]);
+  v = __dadd_rn(v, __dmul_rn(centre, ub[o]));
+  v = __dadd_rn(v, ub[o + 1]);
+  v = __dadd_rn(v, ub[o + S]);
+  v = __dadd_rn(v, ub[o + S2]);
+  return v;
+}
+
+struct Op3 { int op; double s, centre, diag, omega; };
+
+// RedBlack{P} (src/multigrid.jl:153-180): x steps by 2, parity P xor (y+1 & 1) xor (z+1 & 1)
+// in 1-based terms; two fused multiply-adds as the reference's muladds.
+__global__ void k3_gs_rb(double *__restrict__ u, const double *__restrict__ b, Level3View L, Op3 p, int parity) {
+  const int64_t total = (int64_t)L.nblk * (kM * kM * kM / 2);
+  const double nwc = -(p.omega / p.diag);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t / 2048), c = (int)(t % 2048);
+    const int z = kG + c / 128, y = kG + (c / 8) % 16, k = c % 8;
+    const int pp = parity ^ ((y + 1) & 1) ^ ((z + 1) & 1);
+    const int x = kG + 2 * k + pp;
+    const int64_t base = (int64_t)L.blocks[bi].x * S3;
+    const int o = o3(x, y, z);
+    const double Lu = lhs3(u + base, o, p.op, p.centre);
+    const double v = fma(p.s, b[base + o], Lu);
+    u[base + o] = fma(nwc, v, u[base + o]);
+  }
+}
+
+// FourColors{P1,P2} (src/multigrid.jl:206-232) for D = 3: cells (x + p1, y + p2, z) on
+// the even grid of the first two dimensions, p_a = (P_a + z + 1) mod 2 (1-based z);
+// u -= omega (Lu + s b) / c, unfused.
+__global__ void k3_gs4(double *__restrict__ u, const double *__restrict__ b, Level3View L, Op3 p, int P1, int P2) {
+  const int64_t total = (int64_t)L.nblk * 1024;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t / 1024), c = (int)(t % 1024);
+    const int z = kG + c / 64;
+    const int p1 = (P1 + z + 1) & 1, p2 = (P2 + z + 1) & 1;
+    const int x = kG + 2 * (c % 8) + p1, y = kG + 2 * ((c / 8) % 8) + p2;
+    const int64_t base = (int64_t)L.blocks[bi].x * S3;
+    const int o = o3(x, y, z);
+    const double Lu = lhs3(u + base, o, p.op, p.centre);
+    const double upd = __dmul_rn(p.omega, __dadd_rn(Lu, __dmul_rn(p.s, b[base + o]))) / p.diag;
+    u[base + o] = u[base + o] - upd;
+  }
+}
+
+__global__ void k3_residual(double *__restrict__ r, const double *__restrict__ u, const double *__restrict__ b,
+                            Level3View L, Op3 p) {
+  const int64_t total = (int64_t)L.nblk * 4096;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t / 4096), c = (int)(t % 4096);
+    const int o = o3(kG + c % 16, kG + (c / 16) % 16, kG + c / 256);
+    const int64_t base = (int64_t)L.blocks[bi].x * S3;
+    r[base + o] = -(b[base + o] + lhs3(u + base, o, p.op, p.centre) / p.s);
+  }
+}
+
+// residual_subblock! on the coarse subblock of every child edge of this level
+__global__ void k3_postrestrict(double *__restrict__ bf, const double *__restrict__ u, const double *__restrict__ r,
+                                Level3View L, Op3 pc) {
+  const int64_t total = (int64_t)L.nch * 512;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(t / 512), c = (int)(t % 512);
+    const int4 ch = L.child[e];
+    const int x = kG + 8 * unpack(ch.z, 0) + c % 8;
+    const int y = kG + 8 * unpack(ch.z, 1) + (c / 8) % 8;
+    const int z = kG + 8 * unpack(ch.z, 2) + c / 64;
+    const int o = o3(x, y, z);
+    const int64_t base = (int64_t)ch.y * S3;
+    bf[base + o] = -(r[base + o] + lhs3(u + base, o, pc.op, pc.centre) / pc.s);
+  }
+}
+
+// restrict! (src/restrict.jl:5-25): f = 0; f += the 8 fine cells (first offset
+// innermost); coarse = f / 8
+__global__ void k3_restrict(double *__restrict__ u, Level3View L) {
+  const int64_t total = (int64_t)L.nch * 512;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(t / 512), c = (int)(t % 512);
+    const int4 ch = L.child[e];
+    const int kx = c % 8, ky = (c / 8) % 8, kz = c / 64;
+    const double *fb = u + (int64_t)ch.x * S3 + o3(kG + 2 * kx, kG + 2 * ky, kG + 2 * kz);
+    double f = 0.0;
+#pragma unroll
+    for (int i3 = 0; i3 <= 1; ++i3)
+#pragma unroll
+      for (int i2 = 0; i2 <= 1; ++i2)
+#pragma unroll
+        for (int i1 = 0; i1 <= 1; ++i1) f = __dadd_rn(f, fb[i1 + S * i2 + S2 * i3]);
+    u[(int64_t)ch.y * S3 + o3(kG + 8 * unpack(ch.z, 0) + kx, kG + 8 * unpack(ch.z, 1) + ky,
+                              kG + 8 * unpack(ch.z, 2) + kz)] = f / 8.0;
+  }
+}
+
+// interp_add_level! (src/interp.jl:107-115): u_fine += P(u1 over the parent's subblock)
+__global__ void k3_interp_add(double *__restrict__ u, const double *__restrict__ u1, Level3View L) {
+  const int64_t total = (int64_t)L.nch * 4096;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(t / 4096), c = (int)(t % 4096);
+    const int4 ch = L.child[e];
+    const int dx = c % 16, dy = (c / 16) % 16, dz = c / 256;
+    const int o = o3(kG + 8 * unpack(ch.z, 0) + (dx >> 1), kG + 8 * unpack(ch.z, 1) + (dy >> 1),
+                     kG + 8 * unpack(ch.z, 2) + (dz >> 1));
+    const double *cb = u1 + (int64_t)ch.y * S3;
+    double v = __dmul_rn(0.25, cb[o]);
+    v = __dadd_rn(v, __dmul_rn(0.25, cb[o + (2 * (dx & 1) - 1)]));
+    v = __dadd_rn(v, __dmul_rn(0.25, cb[o + S * (2 * (dy & 1) - 1)]));
+    v = __dadd_rn(v, __dmul_rn(0.25, cb[o + S2 * (2 * (dz & 1) - 1)]));
+    double *d = u + (int64_t)ch.x * S3 + o3(kG + dx, kG + dy, kG + dz);
+    *d = __dadd_rn(v, *d);
+  }
+}
+
+__global__ void k3_copy(double *__restrict__ dst, const double *__restrict__ a1, const double *__restrict__ a2,
+                        Level3View L) {
+  const int64_t total = (int64_t)L.nblk * S3;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t o = (int64_t)L.blocks[t / S3].x * S3 + t % S3;
+    dst[o] = a2 ? a1[o] - a2[o] : a1[o];
+  }
+}
+
+// rhs! (src/multigrid.jl:363-388): identity at order 2, the 7-point right-hand side
+// (centre 6) / 12 at order 4 (src/laplacian.jl:322-337)
+__global__ void k3_rhs(double *__restrict__ q1, const double *__restrict__ q, Level3View L, int op) {
+  const int64_t total = (int64_t)L.nblk * 4096;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t / 4096), c = (int)(t % 4096);
+    const int o = o3(kG + c % 16, kG + (c / 16) % 16, kG + c / 256);
+    const int64_t base = (int64_t)L.blocks[bi].x * S3;
+    const double *qb = q + base;
+    if (op != 2) {
+      q1[base + o] = qb[o];
+      continue;
+    }
+    double v = 0.0;
+    v = __dadd_rn(v, qb[o - S2]);
+    v = __dadd_rn(v, qb[o - S]);
+    v = __dadd_rn(v, qb[o - 1]);
+    v = __dadd_rn(v, __dmul_rn(6.0, qb[o]));
+    v = __dadd_rn(v, qb[o + 1]);
+    v = __dadd_rn(v, qb[o + S]);
+    v = __dadd_rn(v, qb[o + S2]);
+    q1[base + o] = v / 12.0;
+  }
+}
+
+// Sum over the level's leaf cells of w_l f^2 (f = residual, or b itself), one partial per
+// CTA; a leaf cell of level l carries 8^-(l-1), what resnorm!'s restriction of squares
+// gives it (src/multigrid.jl:391-417).
+template <int NT>
+__global__ void __launch_bounds__(NT) k3_leafsq(double *__restrict__ part, const double *__restrict__ u,
+                                                const double *__restrict__ b, Level3View L, Op3 p, double wl,
+                                                int mode) {
+  double acc = 0.0;
+  const int64_t total = (int64_t)L.nblk * 4096;
+  for (int64_t t = blockIdx.x * (int64_t)NT + threadIdx.x; t < total; t += (int64_t)gridDim.x * NT) {
+    const int bi = (int)(t / 4096), c = (int)(t % 4096);
+    const int cx = c % 16, cy = (c / 16) % 16, cz = c / 256;
+    const int oct = (cx >> 3) + 2 * (cy >> 3) + 4 * (cz >> 3);
+    if ((L.mask[bi] >> oct) & 1) continue;
+    const int o = o3(kG + cx, kG + cy, kG + cz);
+    const int64_t base = (int64_t)L.blocks[bi].x * S3;
+    const double v = mode == 0 ? -(b[base + o] + lhs3(u + base, o, p.op, p.centre) / p.s) : b[base + o];
+    acc = fma(v, v, acc);
+  }
+  __shared__ double sh[NT / 32];
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < NT / 32 ? sh[threadIdx.x] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if (threadIdx.x == 0) part[blockIdx.x] = v * wl;
+  }
+}
+
+int grid3(int64_t work, int threads) {
+  const int64_t g = (work + threads - 1) / threads;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 16));
+}
+
+Signs27 signs27(const int8_t *bc) {
+  Signs27 s;
+  for (int i = 0; i < 27; ++i) s.v[i] = bc ? (double)bc[i] : 1.0;
+  return s;
+}
+
+Op3 op3(int op, double k2, double sl, double omega) {
+  Op3 p;
+  p.op = op;
+  p.s = sl;
+  p.centre = op == SRMG_OP_HELMHOLTZ ? -6.0 - sl * k2 : -6.0;
+  p.diag = op == SRMG_OP_LAPLACIAN4 ? -4.0 : p.centre;  // diagelm (src/laplacian.jl:299,339)
+  p.omega = omega;
+  return p;
+}
+
+Level3View view(srmg_ctx *ctx, int l) { return ctx->lv3[l - 1].view(); }
+
+int fill(srmg_ctx *ctx, double *u, int l, const Signs27 &sg, int mask) {
+  const int n = ctx->nblk_host[l - 1];
+  if (!n) return SRMG_OK;
+  for (int phase = 1; phase <= 4; phase <<= 1) {
+    if (!(mask & phase)) continue;
+    k3_fill<<<grid3((int64_t)n * S3, 256), 256, 0, ctx->stream>>>(u, view(ctx, l), sg, phase);
+    ctx->launches++;
+  }
+  return SRMG_OK;
+}
+
+int gs_colour(srmg_ctx *ctx, double *u, const double *b, int l, const Op3 &p, int colour) {
+  const int n = ctx->nblk_host[l - 1];
+  if (!n) return SRMG_OK;
+  if (p.op == SRMG_OP_LAPLACIAN4)
+    k3_gs4<<<grid3((int64_t)n * 1024, 256), 256, 0, ctx->stream>>>(u, b, view(ctx, l), p, colour >> 1, colour & 1);
+  else
+    k3_gs_rb<<<grid3((int64_t)n * 2048, 256), 256, 0, ctx->stream>>>(u, b, view(ctx, l), p, colour);
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+// gauss_seidel_iter! (src/multigrid.jl:250-295): each colour followed by copy and
+// boundary ghosts
+int gs_iter(srmg_ctx *ctx, double *u, const double *b, int l, const Op3 &p, int n, const Signs27 &sg) {
+  const int ncol = p.op == SRMG_OP_LAPLACIAN4 ? 4 : 2;
+  for (int i = 0; i < n; ++i)
+    for (int c = 0; c < ncol; ++c) {
+      RC(gs_colour(ctx, u, b, l, p, c));
+      RC(fill(ctx, u, l, sg, 3));
+    }
+  return SRMG_OK;
+}
+
+int residual(srmg_ctx *ctx, double *r, const double *u, const double *b, int l, const Op3 &p) {
+  const int n = ctx->nblk_host[l - 1];
+  if (!n) return SRMG_OK;
+  k3_residual<<<grid3((int64_t)n * 4096, 256), 256, 0, ctx->stream>>>(r, u, b, view(ctx, l), p);
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+int postrestrict(srmg_ctx *ctx, double *bf, const double *u, const double *r, int l, const Op3 &pc) {
+  const int n = ctx->nch_host[l - 1];
+  if (!n) return SRMG_OK;
+  k3_postrestrict<<<grid3((int64_t)n * 512, 256), 256, 0, ctx->stream>>>(bf, u, r, view(ctx, l), pc);
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+int restrict_l(srmg_ctx *ctx, double *u, int l) {
+  const int n = ctx->nch_host[l - 1];
+  if (!n) return SRMG_OK;
+  k3_restrict<<<grid3((int64_t)n * 512, 256), 256, 0, ctx->stream>>>(u, view(ctx, l));
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+int interp_add(srmg_ctx *ctx, double *u, const double *u1, int l) {
+  const int n = ctx->nch_host[l - 1];
+  if (!n) return SRMG_OK;
+  k3_interp_add<<<grid3((int64_t)n * 4096, 256), 256, 0, ctx->stream>>>(u, u1, view(ctx, l));
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+int copy_l(srmg_ctx *ctx, double *dst, const double *a1, const double *a2, int l) {
+  const int n = ctx->nblk_host[l - 1];
+  if (!n) return SRMG_OK;
+  k3_copy<<<grid3((int64_t)n * S3, 256), 256, 0, ctx->stream>>>(dst, a1, a2, view(ctx, l));
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+int vcycle(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, double s, int op, double k2,
+           const Signs27 &sg, int lmax, int ndown, int ntop, int nup, double omega) {
+  if (lmax == 0) lmax = ctx->nlev;
+  if (lmax < 1 || lmax > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "lmax %d out of range", lmax);
+  for (int l = lmax; l >= 2; --l) {
+    const double sl = level_scale(s, l);
+    const Op3 p = op3(op, k2, sl, omega), pc = op3(op, k2, 4 * sl, omega);
+    RC(gs_iter(ctx, u, b, l, p, ndown, sg));
+    RC(restrict_l(ctx, u, l));
+    RC(fill(ctx, u, l - 1, sg, 7));
+    RC(copy_l(ctx, u1, u, nullptr, l - 1));
+    RC(residual(ctx, r, u, b, l, p));
+    // r's ghost fills (src/multigrid.jl:80,83) are not read by any later operation
+    RC(restrict_l(ctx, r, l));
+    RC(postrestrict(ctx, b, u, r, l, pc));
+  }
+  RC(gs_iter(ctx, u, b, 1, op3(op, k2, s, omega), ntop, sg));
+  for (int l = 2; l <= lmax; ++l) {
+    const Op3 p = op3(op, k2, level_scale(s, l), omega);
+    RC(copy_l(ctx, u1, u, u1, l - 1));
+    RC(fill(ctx, u1, l - 1, sg, 7));
+    RC(interp_add(ctx, u, u1, l));
+    RC(fill(ctx, u, l, sg, 7));
+    RC(gs_iter(ctx, u, b, l, p, nup, sg));
+    RC(fill(ctx, u, l, sg, 7));
+  }
+  return SRMG_OK;
+}
+
+int leafnorm(srmg_ctx *ctx, const double *u, const double *b, double s, int op, double k2, int mode, int slot) {
+  constexpr int NT = 256;
+  int total = 0;
+  std::vector<int> grids(ctx->nlev);
+  for (int l = 1; l <= ctx->nlev; ++l) {
+    const int n = ctx->nblk_host[l - 1];
+    grids[l - 1] = n ? std::min(grid3((int64_t)n * 4096, NT), 148 * 4) : 0;
+    total += grids[l - 1];
+  }
+  RC(ensure(ctx, ctx->part, sizeof(double) * std::max(total, 1)));
+  double *part = (double *)ctx->part.p;
+  int off = 0;
+  for (int l = 1; l <= ctx->nlev; ++l) {
+    if (!grids[l - 1]) continue;
+    const double wl = 1.0 / (double)((int64_t)1 << (3 * (l - 1)));
+    k3_leafsq<NT><<<grids[l - 1], NT, 0, ctx->stream>>>(part + off, u, b, view(ctx, l),
+                                                       op3(op, k2, level_scale(s, l), 1.0), wl, mode);
+    ctx->launches++;
+    off += grids[l - 1];
+  }
+  double *out = (double *)ctx->small.p + slot;
+  if (total == 0) {
+    CK(cudaMemsetAsync(out, 0, sizeof(double), ctx->stream));
+    return SRMG_OK;
+  }
+  k_reduce_sqrt<1024><<<1, 1024, 0, ctx->stream>>>(out, part, total);
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+int corner_code(const int64_t f[3]) {
+  for (int d = 0; d < 3; ++d)
+    if (f[d] < -1 || f[d] > 1) return -1;
+  if (!f[0] && !f[1] && !f[2]) return -1;
+  return (int)((f[0] + 1) + 3 * (f[1] + 1) + 9 * (f[2] + 1));
+}
+
+int pack3(const int64_t v[3], int add) {
+  return (int)((v[0] + add) | ((v[1] + add) << 2) | ((v[2] + add) << 4));
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ tree upload
+
+extern "C" int srmg_set_tree3(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_pair3 *const *pairs,
+                              const int64_t *nnb, const srmg_neighbor3 *const *nb, const int64_t *nbd,
+                              const srmg_boundary3 *const *bd, const int64_t *nrb, const srmg_refbnd3 *const *rb,
+                              const int64_t *nch, const srmg_child3 *const *ch, uint64_t generation) {
+  if (!ctx) return SRMG_ERR_BADARG;
+  if (ctx->D != 3) return fail(ctx, SRMG_ERR_BADARG, "srmg_set_tree3 needs a context created with D = 3");
+  if (nlev < 1 || nlev > 20 || !npairs || !pairs || !nnb || !nb || !nbd || !bd || !nrb || !rb || !nch || !ch)
+    return fail(ctx, SRMG_ERR_BADARG, "srmg_set_tree3: bad level count or null arrays");
+  cudaSetDevice(ctx->device);
+  int64_t max_blk = 0;
+  for (int l = 0; l < nlev; ++l) {
+    if (npairs[l] < 0 || (npairs[l] > 0 && !pairs[l]) || npairs[l] > (int64_t)INT32_MAX / 32)
+      return fail(ctx, SRMG_ERR_BADTREE, "level %d: bad block count", l + 1);
+    for (int64_t p = 0; p < npairs[l]; ++p) {
+      const srmg_pair3 &pr = pairs[l][p];
+      if (pr.blk < 1 || pr.blk >= INT32_MAX / 2)
+        return fail(ctx, SRMG_ERR_BADTREE, "level %d: block index out of range", l + 1);
+      for (int d = 0; d < 3; ++d)
+        if (pr.coord[d] < 1 || pr.coord[d] > (1 << 22))
+          return fail(ctx, SRMG_ERR_BADTREE, "level %d: block coordinate out of range", l + 1);
+      max_blk = std::max(max_blk, pr.blk);
+    }
+  }
+  std::vector<int> lev_of(max_blk + 1, 0), idx_of(max_blk + 1, -1);
+  for (int l = 0; l < nlev; ++l)
+    for (int64_t p = 0; p < npairs[l]; ++p) {
+      const int64_t b = pairs[l][p].blk;
+      if (lev_of[b]) return fail(ctx, SRMG_ERR_BADTREE, "block %lld appears twice in the tree", (long long)b);
+      lev_of[b] = l + 1;
+      idx_of[b] = (int)p;
+    }
+  auto at = [&](int64_t b, int l) { return b >= 1 && b <= max_blk && lev_of[b] == l; };
+  std::vector<std::vector<int4>> hb(nlev), hf(nlev), hc(nlev);
+  std::vector<std::vector<int>> hm(nlev);
+  bool corners = false;
+  for (int l = 0; l < nlev; ++l) {
+    const int lv = l + 1;
+    hb[l].resize(npairs[l]);
+    hm[l].assign(npairs[l], 0);
+    hf[l].assign(27 * npairs[l], make_int4(FACE_NONE, 0, 0, 0));
+    for (int64_t p = 0; p < npairs[l]; ++p) {
+      const srmg_pair3 &pr = pairs[l][p];
+      hb[l][p] = make_int4((int)(pr.blk - 1), (int)pr.coord[0], (int)pr.coord[1], (int)pr.coord[2]);
+    }
+    auto set = [&](int64_t blk, int code, int4 v) -> int {
+      int4 &slot = hf[l][27 * idx_of[blk] + code];
+      if (slot.x != FACE_NONE)
+        return fail(ctx, SRMG_ERR_BADTREE, "level %d: ghost direction %d of block %lld written twice", lv, code,
+                    (long long)blk);
+      slot = v;
+      const int nz = (code % 3 != 1) + ((code / 3) % 3 != 1) + (code / 9 != 1);
+      if (nz > 1) corners = true;
+      return SRMG_OK;
+    };
+    if (nnb[l] < 0 || (nnb[l] > 0 && !nb[l])) return fail(ctx, SRMG_ERR_BADTREE, "level %d: neighbours", lv);
+    for (int64_t k = 0; k < nnb[l]; ++k) {
+      const srmg_neighbor3 &e = nb[l][k];
+      const int64_t mf[3] = {-e.face[0], -e.face[1], -e.face[2]};
+      const int code = corner_code(mf);
+      if (code < 0 || !at(e.from, lv) || !at(e.to, lv))
+        return fail(ctx, SRMG_ERR_BADTREE, "level %d: malformed neighbour edge", lv);
+      RC(set(e.to, code, make_int4(FACE_NEIGHBOR, (int)(e.from - 1), 0, 0)));
+    }
+    if (nbd[l] < 0 || (nbd[l] > 0 && !bd[l])) return fail(ctx, SRMG_ERR_BADTREE, "level %d: boundaries", lv);
+    for (int64_t k = 0; k < nbd[l]; ++k) {
+      const srmg_boundary3 &e = bd[l][k];
+      const int code = corner_code(e.face);
+      bool ok = code >= 0 && at(e.block, lv) && e.level == lv && (e.bnd[0] || e.bnd[1] || e.bnd[2]);
+      for (int d = 0; d < 3 && ok; ++d) ok = e.bnd[d] == 0 || e.bnd[d] == e.face[d];
+      if (!ok) return fail(ctx, SRMG_ERR_BADTREE, "level %d: malformed boundary edge", lv);
+      RC(set(e.block, code, make_int4(FACE_BOUNDARY, 0, pack3(e.bnd, 1), 0)));
+    }
+    if (nrb[l] < 0 || (nrb[l] > 0 && !rb[l])) return fail(ctx, SRMG_ERR_BADTREE, "level %d: refboundaries", lv);
+    for (int64_t k = 0; k < nrb[l]; ++k) {
+      const srmg_refbnd3 &e = rb[l][k];
+      const int code = corner_code(e.face);
+      bool ok = code >= 0 && lv >= 2 && at(e.fine, lv) && at(e.coarse, lv - 1);
+      for (int d = 0; d < 3 && ok; ++d) ok = e.subblock[d] == 1 || e.subblock[d] == 2;
+      if (!ok) return fail(ctx, SRMG_ERR_BADTREE, "level %d: malformed refinement boundary", lv);
+      RC(set(e.fine, code, make_int4(FACE_REFBND, (int)(e.coarse - 1), pack3(e.subblock, 0), 0)));
+    }
+    if (nch[l] < 0 || (nch[l] > 0 && !ch[l])) return fail(ctx, SRMG_ERR_BADTREE, "level %d: children", lv);
+    hc[l].resize(nch[l]);
+    for (int64_t k = 0; k < nch[l]; ++k) {
+      const srmg_child3 &e = ch[l][k];
+      bool ok = lv >= 2 && at(e.fine, lv) && at(e.coarse, lv - 1);
+      for (int d = 0; d < 3 && ok; ++d) ok = e.subblock[d] == 1 || e.subblock[d] == 2;
+      if (!ok) return fail(ctx, SRMG_ERR_BADTREE, "level %d: malformed child edge", lv);
+      hc[l][k] = make_int4((int)(e.fine - 1), (int)(e.coarse - 1), pack3(e.subblock, 0), 0);
+      const int bit = 1 << ((int)(e.subblock[0] - 1) + 2 * (int)(e.subblock[1] - 1) + 4 * (int)(e.subblock[2] - 1));
+      int &m = hm[l - 1][idx_of[e.coarse]];
+      if (m & bit) return fail(ctx, SRMG_ERR_BADTREE, "level %d: two children cover one octant", lv);
+      m |= bit;
+    }
+  }
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off += (bytes + 255) & ~size_t(255);
+    return o;
+  };
+  std::vector<size_t> ob(nlev), om(nlev), of(nlev), oc(nlev);
+  for (int l = 0; l < nlev; ++l) {
+    ob[l] = take(hb[l].size() * sizeof(int4));
+    om[l] = take(hm[l].size() * sizeof(int));
+    of[l] = take(hf[l].size() * sizeof(int4));
+    oc[l] = take(hc[l].size() * sizeof(int4));
+  }
+  std::vector<char> host(std::max<size_t>(off, 256), 0);
+  for (int l = 0; l < nlev; ++l) {
+    memcpy(host.data() + ob[l], hb[l].data(), hb[l].size() * sizeof(int4));
+    memcpy(host.data() + om[l], hm[l].data(), hm[l].size() * sizeof(int));
+    memcpy(host.data() + of[l], hf[l].data(), hf[l].size() * sizeof(int4));
+    memcpy(host.data() + oc[l], hc[l].data(), hc[l].size() * sizeof(int4));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  free_tree(ctx);
+  void *d = nullptr;
+  if (cudaMalloc(&d, host.size()) != cudaSuccess)
+    return fail(ctx, SRMG_ERR_NOMEM, "tree allocation of %zu bytes", host.size());
+  ctx->d_tree = d;
+  CK(cudaMemcpyAsync(d, host.data(), host.size(), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  char *base = (char *)d;
+  ctx->nlev = nlev;
+  ctx->lv3.assign(nlev, Dev3Level{});
+  ctx->nblk_host.resize(nlev);
+  ctx->nch_host.resize(nlev);
+  for (int l = 0; l < nlev; ++l) {
+    Dev3Level &L = ctx->lv3[l];
+    L.nblk = (int)hb[l].size();
+    L.nch = (int)hc[l].size();
+    L.blocks = (int4 *)(base + ob[l]);
+    L.mask = (int *)(base + om[l]);
+    L.faces = (int4 *)(base + of[l]);
+    L.child = (int4 *)(base + oc[l]);
+    ctx->nblk_host[l] = L.nblk;
+    ctx->nch_host[l] = L.nch;
+  }
+  ctx->lv.clear();
+  ctx->max_blk = max_blk;
+  ctx->generation = generation;
+  ctx->has_corners = corners;
+  ctx->nitems = 1;
+  ctx->has_tree = true;
+  return SRMG_OK;
+}
+
+// ------------------------------------------------------------------ entry-point bodies
+
+int srmg::d3_fill_ghost(srmg_ctx *ctx, double *u, int level, const int8_t *bc, int mask) {
+  if (level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "fill_ghost: bad level");
+  return fill(ctx, u, level, signs27(bc), mask);
+}
+
+int srmg::d3_gs_level(srmg_ctx *ctx, double *u, const double *b, int level, double omega, double sl, int op,
+                      double k2, int colour) {
+  const int ncol = op == SRMG_OP_LAPLACIAN4 ? 4 : 2;
+  if (level < 1 || level > ctx->nlev || colour < 0 || colour >= ncol)
+    return fail(ctx, SRMG_ERR_BADARG, "gs_level: bad arguments");
+  return gs_colour(ctx, u, b, level, op3(op, k2, sl, omega), colour);
+}
+
+int srmg::d3_gs_iter(srmg_ctx *ctx, double *u, const double *b, int level, double omega, double sl, int n, int op,
+                     double k2, const int8_t *bc) {
+  if (level < 1 || level > ctx->nlev || n < 0) return fail(ctx, SRMG_ERR_BADARG, "gs_iter: bad arguments");
+  return gs_iter(ctx, u, b, level, op3(op, k2, sl, omega), n, signs27(bc));
+}
+
+int srmg::d3_residual_level(srmg_ctx *ctx, double *r, const double *u, const double *b, int level, double sl,
+                            int op, double k2) {
+  if (level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "residual_level: bad level");
+  return residual(ctx, r, u, b, level, op3(op, k2, sl, 1.0));
+}
+
+int srmg::d3_restrict_level(srmg_ctx *ctx, double *u, int level) {
+  if (level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "restrict_level: bad level");
+  return restrict_l(ctx, u, level);
+}
+
+int srmg::d3_interp_add_level(srmg_ctx *ctx, double *u, const double *u1, int level) {
+  if (level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "interp_add_level: bad level");
+  return interp_add(ctx, u, u1, level);
+}
+
+int srmg::d3_postrestrict_level(srmg_ctx *ctx, double *b, const double *u, const double *r, int level, double s,
+                                int op, double k2) {
+  if (level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "postrestrict: bad level");
+  return postrestrict(ctx, b, u, r, level, op3(op, k2, s, 1.0));
+}
+
+int srmg::d3_rhs_level(srmg_ctx *ctx, double *q1, const double *q, int level, int op) {
+  if (level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "rhs_level: bad level");
+  const int n = ctx->nblk_host[level - 1];
+  if (n) {
+    k3_rhs<<<grid3((int64_t)n * 4096, 256), 256, 0, ctx->stream>>>(q1, q, view(ctx, level), op);
+    ctx->launches++;
+  }
+  return SRMG_OK;
+}
+
+int srmg::d3_vcycle(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, double s, int op, double k2,
+                    const int8_t *bc, int lmax, int ndown, int ntop, int nup, double omega) {
+  return vcycle(ctx, u, b, r, u1, s, op, k2, signs27(bc), lmax, ndown, ntop, nup, omega);
+}
+
+int srmg::d3_fmg(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, double s, int op, double k2,
+                 const int8_t *bc, int ndown, int ntop, int nup, double omega) {
+  const Signs27 sg = signs27(bc);
+  int lmax = 0;
+  for (int l = 1; l <= ctx->nlev; ++l)
+    if (ctx->nblk_host[l - 1] > 0) lmax = l;
+  for (int l = lmax; l >= 2; --l) {
+    const double sl = level_scale(s, l);
+    RC(restrict_l(ctx, u, l));
+    RC(fill(ctx, u, l - 1, sg, 7));
+    RC(residual(ctx, r, u, b, l, op3(op, k2, sl, omega)));
+    RC(restrict_l(ctx, r, l));
+    RC(postrestrict(ctx, b, u, r, l, op3(op, k2, 4 * sl, omega)));
+  }
+  for (int l = 1; l <= lmax; ++l) {
+    RC(copy_l(ctx, u1, u, nullptr, l));
+    if (l > 1) {
+      RC(copy_l(ctx, u1, u, u1, l - 1));
+      RC(fill(ctx, u1, l - 1, sg, 7));
+      RC(interp_add(ctx, u, u1, l));
+    }
+    RC(fill(ctx, u, l, sg, 7));
+    RC(vcycle(ctx, u, b, r, u1, s, op, k2, sg, l, ndown, ntop, nup, omega));
+  }
+  return SRMG_OK;
+}
+
+int srmg::d3_leafnorm(srmg_ctx *ctx, const double *u, const double *b, double s, int op, double k2, int mode,
+                      int slot) {
+  return leafnorm(ctx, u, b, s, op, k2, mode, slot);
+}
+
+// FP64 tolerance loop on the per-operation V-cycle (srmg_solve for D = 3).
+int srmg::d3_solve(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, double s, int op, double k2,
+                   const int8_t *bc, const srmg_solve_opts *o, srmg_stats *st) {
+  if (o->mode != SRMG_MODE_FP64)
+    return fail(ctx, SRMG_ERR_UNSUPPORTED, "three-dimensional solves run in FP64 mode");
+  if (!(o->tol > 0) || o->max_cycles < 0 || o->ndown < 0 || o->nup < 0 || o->ntop < 0)
+    return fail(ctx, SRMG_ERR_BADARG, "srmg_solve: bad options");
+  memset(st, 0, sizeof(*st));
+  const size_t bytes = (size_t)nblk_alloc * S3 * sizeof(double);
+  for (int i : {2, 3, 4}) RC(ensure(ctx, ctx->f64[i], bytes));
+  double *r = (double *)ctx->f64[2].p, *u1 = (double *)ctx->f64[3].p, *bw = (double *)ctx->f64[4].p;
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  CK(cudaMemcpyAsync(bw, b, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  const Signs27 sg = signs27(bc);
+  RC(leafnorm(ctx, u, b, s, op, k2, 1, 1));
+  RC(leafnorm(ctx, u, bw, s, op, k2, 0, 0));
+  RC(read_small(ctx, 2));
+  const double bn = ctx->h_small[1] > 0 ? ctx->h_small[1] : 1.0;
+  st->bnorm = ctx->h_small[1];
+  double rel = ctx->h_small[0] / bn;
+  st->initial_rel = rel;
+  int c = 0;
+  while (rel > o->tol && c < o->max_cycles) {
+    RC(vcycle(ctx, u, bw, r, u1, s, op, k2, sg, 0, o->ndown, o->ntop, o->nup, o->omega));
+    ++c;
+    RC(leafnorm(ctx, u, bw, s, op, k2, 0, 0));
+    RC(read_small(ctx, 1));
+    rel = ctx->h_small[0] / bn;
+    if (!std::isfinite(rel)) {
+      st->status = SRMG_ERR_DIVERGED;
+      break;
+    }
+  }
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  CK(cudaEventSynchronize(ctx->ev1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  st->device_ms = ms;
+  st->cycles = c;
+  st->rel_residual = rel;
+  if (st->status) return fail(ctx, st->status, "residual is not finite after %d cycles", c);
+  return SRMG_OK;
+}

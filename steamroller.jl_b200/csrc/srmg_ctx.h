@@ -23,6 +23,28 @@ struct DevLevel {
   LevelView view(int level) const { return LevelView{blocks, faces, child, nblk, nch, level, cfaces}; }
 };
 
+// Per-level device view of a three-dimensional tree (srmg_set_tree3): blocks
+// {blk, c1, c2, c3}, child-octant masks, 27 pull faces per block by ghost direction
+// (f1+1) + 3(f2+1) + 9(f3+1), child edges {fine, coarse, packed subblock}.
+struct Level3View {
+  const int4 *blocks;
+  const int *mask;
+  const int4 *faces;
+  const int4 *child;
+  int nblk;
+  int nch;
+};
+
+struct Dev3Level {
+  int nblk = 0;
+  int nch = 0;
+  int4 *blocks = nullptr;
+  int *mask = nullptr;
+  int4 *faces = nullptr;
+  int4 *child = nullptr;
+  Level3View view() const { return Level3View{blocks, mask, faces, child, nblk, nch}; }
+};
+
 // A device buffer that only grows.
 struct DevBuf {
   void *p = nullptr;
@@ -53,6 +75,7 @@ struct HostTree {
 
 struct srmg_ctx {
   int device = 0;
+  int D = 2;                 // dimension of the tree: 2, or 3 (per-operation FP64 path only)
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
@@ -65,6 +88,7 @@ struct srmg_ctx {
   int64_t max_blk = 0;      // largest 1-based block id in the tree
   int wtab_n = 0;           // entries of the radial weight tables
   std::vector<srmg::DevLevel> lv;      // index l-1
+  std::vector<srmg::Dev3Level> lv3;    // D = 3 trees, index l-1
   std::vector<int> nblk_host;          // per level
   std::vector<int> nch_host;
   void *d_tree = nullptr;              // one allocation for all tree arrays

@@ -11,6 +11,32 @@ int fail(srmg_ctx *c, int code, const char *fmt, ...);
 int cuda_check(srmg_ctx *c, cudaError_t e, const char *what);
 int ensure(srmg_ctx *ctx, DevBuf &b, size_t bytes);
 int check_call(srmg_ctx *ctx, int64_t nblk_alloc, int op, int geom, const int8_t *bc);
+// check_call for the entry points that also run on three-dimensional trees (3^D-entry
+// boundary table, Cartesian geometry there); check_call refuses D = 3 contexts.
+int check_call_any(srmg_ctx *ctx, int64_t nblk_alloc, int op, int geom, const int8_t *bc);
+// values per block of the context's fields: 20^D
+inline int64_t block_elems(const srmg_ctx *ctx) { return ctx->D == 3 ? (int64_t)kS * kS * kS : (int64_t)kSS; }
+void free_tree(srmg_ctx *ctx);
+// the D = 3 bodies of the generic entry points (srmg3.cu)
+int d3_fill_ghost(srmg_ctx *ctx, double *u, int level, const int8_t *bc, int mask);
+int d3_gs_level(srmg_ctx *ctx, double *u, const double *b, int level, double omega, double sl, int op, double k2,
+                int colour);
+int d3_gs_iter(srmg_ctx *ctx, double *u, const double *b, int level, double omega, double sl, int n, int op, double k2,
+               const int8_t *bc);
+int d3_residual_level(srmg_ctx *ctx, double *r, const double *u, const double *b, int level, double sl, int op,
+                      double k2);
+int d3_restrict_level(srmg_ctx *ctx, double *u, int level);
+int d3_interp_add_level(srmg_ctx *ctx, double *u, const double *u1, int level);
+int d3_postrestrict_level(srmg_ctx *ctx, double *b, const double *u, const double *r, int level, double s, int op,
+                          double k2);
+int d3_rhs_level(srmg_ctx *ctx, double *q1, const double *q, int level, int op);
+int d3_vcycle(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, double s, int op, double k2,
+              const int8_t *bc, int lmax, int ndown, int ntop, int nup, double omega);
+int d3_fmg(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, double s, int op, double k2, const int8_t *bc,
+           int ndown, int ntop, int nup, double omega);
+int d3_leafnorm(srmg_ctx *ctx, const double *u, const double *b, double s, int op, double k2, int mode, int slot);
+int d3_solve(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, double s, int op, double k2,
+             const int8_t *bc, const srmg_solve_opts *o, srmg_stats *st);
 Signs make_signs(const int8_t *bc);
 std::vector<int8_t> bc_of(const Signs &sg);
 int build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_pair *const *pairs,

@@ -410,8 +410,16 @@ int srmg::solve_items(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_al
 extern "C" int srmg_solve_dev(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, double s,
                               int op, double k2, int geom, const int8_t bc[9],
                               const srmg_solve_opts *opts, srmg_stats *stats) {
-  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  RC(check_call_any(ctx, nblk_alloc, op, geom, bc));
   if (!u || !b) return fail(ctx, SRMG_ERR_BADARG, "srmg_solve: null field");
+  if (ctx->D == 3) {
+    srmg_solve_opts o;
+    if (opts) o = *opts; else srmg_solve_opts_default(&o);
+    srmg_stats st;
+    const int rc = d3_solve(ctx, u, b, nblk_alloc, s, op, k2, bc, &o, &st);
+    if (stats) *stats = st;
+    return rc;
+  }
   const std::vector<ItemSpec> specs = uniform_items(ctx, s, op, k2, bc);
   std::vector<srmg_stats> st((size_t)ctx->nitems);
   const int rc = solve_items(ctx, u, b, nblk_alloc, specs.data(), geom, opts, st.data());
@@ -435,7 +443,7 @@ extern "C" int srmg_solve_dev(srmg_ctx *ctx, double *u, const double *b, int64_t
 extern "C" int srmg_solve(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, double s, int op,
                           double k2, int geom, const int8_t bc[9], const srmg_solve_opts *opts,
                           srmg_stats *stats) {
-  RC(check_call(ctx, nblk_alloc, op, geom, bc));
+  RC(check_call_any(ctx, nblk_alloc, op, geom, bc));
   if (!u || !b) return fail(ctx, SRMG_ERR_BADARG, "srmg_solve: null field");
   double *du, *db;
   RC(stage_in(ctx, 0, u, nblk_alloc, &du));

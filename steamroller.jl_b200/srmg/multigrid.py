@@ -77,6 +77,7 @@ SIGNATURES = {
     "srmg_set_stream": (_I, [_P, _P]),
     "srmg_synchronize": (_I, [_P]),
     "srmg_set_tree": (_I, [_P, _I] + [_P] * 10 + [ctypes.c_uint64]),
+    "srmg_set_tree3": (_I, [_P, _I] + [_P] * 10 + [ctypes.c_uint64]),
     "srmg_tree_generation": (ctypes.c_uint64, [_P]),
     "srmg_vcycle": (_I, [_P, _P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, _I, _I, _I, _I, _D, _I]),
     "srmg_fmg": (_I, [_P, _P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, _I, _I, _I, _D]),
@@ -184,9 +185,10 @@ def _ptr(a):
 class Context:
     """An srmg context bound to one device with a tree uploaded."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, D: int = 2):
         self._h = _P()
-        rc = lib().srmg_create(ctypes.byref(self._h), 2, 16, 2, device)
+        self.D = D
+        rc = lib().srmg_create(ctypes.byref(self._h), D, 16, 2, device)
         if rc != SRMG_OK:
             raise SrmgError(rc, "srmg_create failed")
         self._tree_keep = None
@@ -231,7 +233,8 @@ class Context:
         rb = arrs(conn.refboundary)
         ch = arrs(conn.child)
         self.generation = (self.generation + 1) if generation is None else generation
-        self.check(lib().srmg_set_tree(self._h, nlev, *pairs, *nb, *bd, *rb, *ch, self.generation))
+        f = lib().srmg_set_tree3 if getattr(tree, "D", 2) == 3 else lib().srmg_set_tree
+        self.check(f(self._h, nlev, *pairs, *nb, *bd, *rb, *ch, self.generation))
         self._tree_keep = keep
         return self
 
@@ -259,7 +262,10 @@ class Context:
 
 
 def _bc(bc):
-    a = np.ascontiguousarray(np.asarray(bc, dtype=np.int8).reshape(9))
+    """The boundary table: 9 entries (D = 2) or 27 (D = 3), column-major."""
+    a = np.ascontiguousarray(np.asarray(bc, dtype=np.int8).reshape(-1))
+    if a.size not in (9, 27):
+        raise ValueError("a boundary table has 9 (D = 2) or 27 (D = 3) entries")
     return a
 
 

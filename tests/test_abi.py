@@ -49,5 +49,7 @@ def test_create_without_gpu_fails_cleanly():
 
 def test_unsupported_shapes_rejected():
     h = ctypes.c_void_p()
-    assert mg.lib().srmg_create(ctypes.byref(h), 3, 16, 2, 0) == -6
+    assert mg.lib().srmg_create(ctypes.byref(h), 4, 16, 2, 0) == -6
+    assert mg.lib().srmg_create(ctypes.byref(h), 1, 16, 2, 0) == -6
     assert mg.lib().srmg_create(ctypes.byref(h), 2, 8, 2, 0) == -6
+    assert mg.lib().srmg_create(ctypes.byref(h), 3, 16, 4, 0) == -6
