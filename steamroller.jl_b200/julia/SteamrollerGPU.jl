@@ -8,6 +8,8 @@ Drop-in GPU field solve for Steamroller.jl.  `using SteamrollerGPU` after
     ScalarBlockField{2,16,2,Float64} (contiguous storage),
     LaplacianDiscretization{2,2} / HelmholtzDiscretization{2,2} /
     LaplacianDiscretization{2,4} (poisson_order = 4, on its BoxStencil connectivity),
+    and in 3D ScalarBlockField{3,16,2,Float64} with LaplacianDiscretization{3,2},
+    HelmholtzDiscretization{3,2} or LaplacianDiscretization{3,4} (CartesianGeometry),
     CartesianGeometry / CylindricalGeometry{1} / CylindricalGeometry{2},
     GeneralHomogeneousBoundaryConditions{2},
 
@@ -49,6 +51,11 @@ function configure!(; device=STATE.device, enabled=STATE.enabled)
         STATE.ctx = C_NULL
         STATE.fingerprint = 0
         STATE.fbc = 0
+    end
+    if device != STATE.device && STATE3.ctx != C_NULL
+        ccall((:srmg_destroy, libsrmg), Cvoid, (Ptr{Cvoid},), STATE3.ctx)
+        STATE3.ctx = C_NULL
+        STATE3.fingerprint = 0
     end
     STATE.device = device
     STATE.enabled = enabled
@@ -201,6 +208,116 @@ function solve!(u::GPUField, b::GPUField, s, tree, conn, geometry::GPUGeom,
     end
     st = stats[]
     (st[2], st[4])
+end
+
+# ---- three-dimensional trees: a second context created with D = 3 ----------------------
+
+mutable struct State3
+    ctx::Ptr{Cvoid}
+    fingerprint::UInt64
+    generation::UInt64
+end
+const STATE3 = State3(C_NULL, 0, 0)
+
+function context3()
+    if STATE3.ctx == C_NULL
+        r = Ref{Ptr{Cvoid}}(C_NULL)
+        rc = ccall((:srmg_create, libsrmg), Cint, (Ptr{Ptr{Cvoid}}, Cint, Cint, Cint, Cint),
+                   r, 3, 16, 2, STATE.device)
+        rc == SRMG_OK || error("srmg_create(D = 3) failed ($rc)")
+        STATE3.ctx = r[]
+    end
+    STATE3.ctx
+end
+
+function check3(rc)
+    rc == SRMG_OK && return nothing
+    msg = unsafe_string(ccall((:srmg_last_error, libsrmg), Cstring, (Ptr{Cvoid},), STATE3.ctx))
+    error("libsrmg error $rc: $msg")
+end
+
+function fingerprint3(tree)
+    h = UInt64(length(tree))
+    for layer in tree
+        h = h * 0x100000001b3 + UInt64(length(layer.pairs))
+        for (c, blk) in layer.pairs
+            h += UInt64(blk) * 0x9e3779b97f4a7c15 + UInt64(c[1]) * 1000003 + UInt64(c[2]) * 7919 + UInt64(c[3])
+        end
+    end
+    h
+end
+
+# srmg_set_tree3 takes the same per-level pointers as srmg_set_tree; the isbits layouts
+# of Pair{CartesianIndex{3},Int} and Neighbor{3}/Boundary{3}/RefBoundary{3}/Child{3}
+# are the srmg_*3 structs of include/srmg.h.
+function upload3!(tree, conn)
+    fp = fingerprint3(tree)
+    fp == STATE3.fingerprint && return nothing
+    lens(v) = Int64[length(x) for x in v]
+    ptrs(v) = Ptr{Cvoid}[pointer(x) for x in v]
+    STATE3.generation += 1
+    GC.@preserve tree conn begin
+        check3(ccall((:srmg_set_tree3, libsrmg), Cint,
+                     (Ptr{Cvoid}, Cint, Ptr{Int64}, Ptr{Ptr{Cvoid}}, Ptr{Int64}, Ptr{Ptr{Cvoid}},
+                      Ptr{Int64}, Ptr{Ptr{Cvoid}}, Ptr{Int64}, Ptr{Ptr{Cvoid}}, Ptr{Int64},
+                      Ptr{Ptr{Cvoid}}, UInt64),
+                     context3(), length(tree), Int64[length(l.pairs) for l in tree],
+                     Ptr{Cvoid}[pointer(l.pairs) for l in tree],
+                     lens(conn.neighbor), ptrs(conn.neighbor), lens(conn.boundary), ptrs(conn.boundary),
+                     lens(conn.refboundary), ptrs(conn.refboundary), lens(conn.child), ptrs(conn.child),
+                     STATE3.generation))
+    end
+    STATE3.fingerprint = fp
+    nothing
+end
+
+const GPUField3 = ScalarBlockField{3,16,2,Float64}
+const GPUDisc3 = Union{LaplacianDiscretization{3,2}, HelmholtzDiscretization{3,2}, LaplacianDiscretization{3,4}}
+opcode(::LaplacianDiscretization{3,2}) = (Cint(0), 0.0)
+opcode(h::HelmholtzDiscretization{3,2}) = (Cint(1), Float64(h.k2))
+opcode(::LaplacianDiscretization{3,4}) = (Cint(2), 0.0)
+
+function Steamroller.vcycle!(u::GPUField3, b::GPUField3, r::GPUField3, u1::GPUField3, s,
+                             tree, conn, geometry::CartesianGeometry,
+                             bc::GeneralHomogeneousBoundaryConditions{3}, lpldisc::GPUDisc3;
+                             lmax=0, ndown=3, ntop=5, nup=3, ω=1.0)
+    if !STATE.enabled
+        return invoke(Steamroller.vcycle!, Tuple{Any,Any,Any,Any,Any,Any,Any,Any,Any,Any},
+                      u, b, r, u1, s, tree, conn, geometry, bc, lpldisc; lmax, ndown, ntop, nup, ω)
+    end
+    upload3!(tree, conn)
+    op, k2 = opcode(lpldisc)
+    a = Ref(bc.a)
+    GC.@preserve u b r u1 a begin
+        check3(ccall((:srmg_vcycle, libsrmg), Cint,
+                     (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int64,
+                      Float64, Cint, Float64, Cint, Ptr{Int8}, Cint, Cint, Cint, Cint, Float64, Cint),
+                     context3(), pointer(u.u), pointer(b.u), pointer(r.u), pointer(u1.u), size(u.u, 4),
+                     Float64(s), op, k2, Cint(0), Base.unsafe_convert(Ptr{Int8}, a), lmax, ndown, ntop, nup,
+                     Float64(ω), 1))
+    end
+    nothing
+end
+
+function Steamroller.fmg!(u::GPUField3, b::GPUField3, r::GPUField3, u1::GPUField3, s,
+                          tree, conn, geometry::CartesianGeometry,
+                          bc::GeneralHomogeneousBoundaryConditions{3}, lpldisc::GPUDisc3;
+                          lmax=0, ndown=3, ntop=5, nup=3, ω=1.25)
+    if !STATE.enabled
+        return invoke(Steamroller.fmg!, Tuple{Any,Any,Any,Any,Any,Any,Any,Any,Any,Any},
+                      u, b, r, u1, s, tree, conn, geometry, bc, lpldisc; lmax, ndown, ntop, nup, ω)
+    end
+    upload3!(tree, conn)
+    op, k2 = opcode(lpldisc)
+    a = Ref(bc.a)
+    GC.@preserve u b r u1 a begin
+        check3(ccall((:srmg_fmg, libsrmg), Cint,
+                     (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int64,
+                      Float64, Cint, Float64, Cint, Ptr{Int8}, Cint, Cint, Cint, Float64),
+                     context3(), pointer(u.u), pointer(b.u), pointer(r.u), pointer(u1.u), size(u.u, 4),
+                     Float64(s), op, k2, Cint(0), Base.unsafe_convert(Ptr{Int8}, a), ndown, ntop, nup, Float64(ω)))
+    end
+    nothing
 end
 
 # ---- stage preparation and post-processing of derivs! (src/streamer.jl:309-351) ------
