@@ -268,6 +268,7 @@ def main():
     ap.add_argument("--learned-pairs", type=int, default=20000, help="solve pairs generated for training")
     ap.add_argument("--no-config5", action="store_true", help="skip the full-size timestep (config-5) section")
     ap.add_argument("--config5-steps", type=int, default=200)
+    ap.add_argument("--no-rows", action="store_true", help="skip the order-4, 3D and free-boundary section")
     ap.add_argument("--only", default=None, choices=[None, "vcycle", "smooth", "cnn"],
                     help="vcycle: time plain FP64 V-cycles only; smooth: GS iterations on the finest "
                          "level only; cnn: the warm-start network's inference forward, mma.sync and "
@@ -445,6 +446,8 @@ def main():
         if not args.no_config5:
             line["config5"] = run_config5(local, net, args.config5_steps, cpu=(rank == 0 and not args.no_cpu))
         net.close()
+    if not args.no_rows:
+        line["rows"] = run_rows(local)
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = run_cpu_reference(problem, fp64_st["cycles"])
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -590,6 +593,90 @@ def run_config5(local, net, steps, cpu=True):
                                "kind": "port", "s_per_vcycle": spv,
                                "sample": f"2 oracle FP64 V-cycles on this tree, scaled by the {cyc:.0f} cycles of "
                                          "the FP64 Poisson solve from the previous potential"}
+    return out
+
+
+def run_rows(local):
+    """The widened rows, FP64 on the per-operation kernels, event-timed on one stream:
+    the compact order-4 Laplacian on a refined BoxStencil tree (beside the order-2
+    Laplacian on the same tree and path), a uniform level-4 octree (512 finest blocks,
+    order-2 and order-4), and the free-boundary step on the config-2 tree at the
+    transform lengths of a level-9 and a level-11 tree.  Roofline: the V-cycle byte
+    model (srmg.model.vcycle_bytes, 3w per cell per GS iteration whatever the stencil)
+    against the measured copy peak."""
+    import torch
+    from srmg import gen, gen3, model, multigrid as mg
+    from srmg.tree3 import Tree3, populate, connectivity as connectivity3, STAR3, BOX3
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    hbm, _ = peaks()
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+
+    def time_vcycles(ctx, b_np, s, geom, bc, lpl, n=8):
+        ctx.set_stream(stream.cuda_stream)
+        b = torch.from_numpy(b_np).to(dev)
+        u, r, u1 = torch.zeros_like(b), torch.zeros_like(b), torch.zeros_like(b)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            mg.vcycle_(ctx, u, b, r, u1, s, geom, bc, lpl, ndown=2, ntop=4, nup=2, ncycles=3)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            l0 = ctx.launches()
+            e0.record(stream)
+            mg.vcycle_(ctx, u, b, r, u1, s, geom, bc, lpl, ndown=2, ntop=4, nup=2, ncycles=n)
+            e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / n, (ctx.launches() - l0) / n
+
+    def line(tree, ms, launches, extra=None):
+        B = model.vcycle_bytes(tree, 8, 2, 2, 4)
+        d = {"blocks": tree.nblocks(), "ms_per_vcycle": ms, "launches_per_vcycle": launches, "model_bytes": B,
+             "achieved_GBps": B / (ms / 1e3) / 1e9, "frac_of_measured_hbm": B / (ms / 1e3) / 1e9 / hbm}
+        d.update(extra or {})
+        return d
+
+    out = {}
+    p = gen.order4_problem(seed=41, geom=gen.GEOM_CYL1, base_level=6, extra=3)
+    ctx = mg.Context(local).set_tree(p.tree, p.conn)
+    ms4, l4 = time_vcycles(ctx, p.b, p.s, p.geom, p.bc, "laplacian4")
+    ms2, l2 = time_vcycles(ctx, p.b, p.s, p.geom, p.bc, None)
+    out["order4_2d"] = {"workload": f"{p.name}: compact order-4 Laplacian, cylindrical r-z, BoxStencil tree",
+                        "order4": line(p.tree, ms4, l4), "order2_same_tree_per_op": line(p.tree, ms2, l2)}
+    ctx.close()
+    t = Tree3((1, 1, 1), 4)
+    populate(t, 4)
+    for name, op, st in (("order2", 0, STAR3), ("order4", 2, BOX3)):
+        conn = connectivity3(t, st)
+        p3 = gen3.make_problem3(t, conn, lambda x, y, z: np.sin(3 * x) * np.cos(2 * y) * z, (1.0 / 16) ** 2, op=op)
+        ctx = mg.Context(local, D=3).set_tree(t, conn)
+        ms, ln = time_vcycles(ctx, p3.b, p3.s, 0, p3.bc, {0: None, 2: "laplacian4"}[op])
+        out.setdefault("octree_3d", {"workload": "uniform level-4 octree (585 blocks, 2.1M finest cells), "
+                                                 "Cartesian, Dirichlet"})[name] = line(t, ms, ln)
+        ctx.close()
+    import freebc_oracle as fo
+    p = gen.config2(seed=2, target_leaf=1_500_000)
+    ctx = mg.Context(local).set_tree(p.tree, p.conn)
+    ctx.set_stream(stream.cuda_stream)
+    q = torch.from_numpy(p.b).to(dev)
+    u = torch.from_numpy(np.random.default_rng(0).standard_normal(p.b.shape)).to(dev)
+    torch.cuda.synchronize()
+    fb = {}
+    for level in (9, 11):
+        n, _, _, f = fo.kernel(1, level, (1, 1), p.h1)
+        mg.freebc_set(ctx, 1, level, (1, 1), f)
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                mg.freebc_(ctx, q, u, p.h1, p.s)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(5):
+                mg.freebc_(ctx, q, u, p.h1, p.s)
+            e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / 5
+        fb[str(n)] = {"ms": ms, "fp64_GFLOPs": 4.0 * n * n / (ms / 1e3) / 1e9}
+    out["freebc"] = {"workload": "freebc! on the config-2 tree (outer column gather, DST-II, times f, DST-III, "
+                                 "setouter), transform length n", "by_n": fb}
+    ctx.close()
     return out
 
 

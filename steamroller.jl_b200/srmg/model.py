@@ -16,7 +16,9 @@ from __future__ import annotations
 
 
 def level_cells(tree, M=16):
-    return [len(layer.index) * M * M for layer in tree]
+    """Valid cells per level: M^D per block (D from the tree, 2 by default)."""
+    D = getattr(tree, "D", 2)
+    return [len(layer.index) * M ** D for layer in tree]
 
 
 def vcycle_bytes(tree, w=8, ndown=2, nup=2, ntop=4, M=16):
