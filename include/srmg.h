@@ -470,6 +470,11 @@ int srmg_streamer_step_dev(srmg_ctx *ctx, double *ne, double *npos, double *nneg
  *   "trace"            1 = record a %globaltimer stamp (ns) after every phase of the
  *                      persistent kernel, read back with srmg_get_trace;
  *   "graph"            1 = batched solves replay a captured CUDA graph;
+ *   "op_graphs"        1 (default) = V-cycles on the per-operation kernels (3D trees,
+ *                      BoxStencil trees, order 4, or "engine" 0) are captured once per
+ *                      (fields, operator, sweep counts, tree, stream) into a CUDA graph
+ *                      and replayed (bit-identical results; up to 8 graphs kept, all
+ *                      dropped when the tree changes); 0 = launch kernel by kernel;
  *   "cnn_active_ppm"   the learned warm start runs the network only on blocks whose
  *                      share of (b_n - 2 b_{n-1} + b_{n-2})^2 is at least this many
  *                      millionths of the largest block's (default 0 = every

@@ -83,7 +83,14 @@ extern "C" int srmg_create(srmg_ctx **out, int D, int M, int G, int device) {
   return SRMG_OK;
 }
 
+void srmg::drop_op_graphs(srmg_ctx *ctx) {
+  for (auto &g : ctx->op_graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  ctx->op_graphs.clear();
+}
+
 void srmg::free_tree(srmg_ctx *ctx) {
+  drop_op_graphs(ctx);
   if (ctx->d_tree) cudaFree(ctx->d_tree);
   ctx->d_tree = nullptr;
   ctx->lv.clear();
@@ -107,6 +114,7 @@ extern "C" void srmg_destroy(srmg_ctx *ctx) {
   if (ctx->istat.p) cudaFree(ctx->istat.p);
   if (ctx->h_items) cudaFreeHost(ctx->h_items);
   if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+  drop_op_graphs(ctx);
   for (auto &b : ctx->forest) if (b.p) cudaFree(b.p);
   for (auto &b : ctx->cnn_work) if (b.p) cudaFree(b.p);
   if (ctx->sync.p) cudaFree(ctx->sync.p);
@@ -904,6 +912,10 @@ extern "C" int srmg_set_option(srmg_ctx *ctx, const char *key, int64_t value) {
   if (!strcmp(key, "engine")) ctx->use_engine = value != 0;
   else if (!strcmp(key, "trace")) ctx->trace_on = value != 0;
   else if (!strcmp(key, "graph")) ctx->use_graph = value != 0;
+  else if (!strcmp(key, "op_graphs")) {
+    ctx->use_op_graphs = value != 0;
+    if (!ctx->use_op_graphs) drop_op_graphs(ctx);
+  }
   else if (!strcmp(key, "cnn_active_ppm")) {
     if (value < 0 || value > 1000000) return fail(ctx, SRMG_ERR_BADARG, "cnn_active_ppm out of range");
     ctx->cnn_active_ppm = (int)value;
@@ -927,6 +939,77 @@ extern "C" int srmg_set_option(srmg_ctx *ctx, const char *key, int64_t value) {
   return SRMG_OK;
 }
 
+// ------------------------------------------------------------------ graphed per-operation V-cycles
+
+namespace {
+constexpr size_t kOpGraphs = 8;
+
+template <typename V>
+void put(std::vector<char> &k, const V &v) {
+  const char *p = reinterpret_cast<const char *>(&v);
+  k.insert(k.end(), p, p + sizeof(V));
+}
+
+int run_vcycles(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, double s, int op, double k2, int geom,
+                const int8_t *bc, int lmax, int ndown, int ntop, int nup, double omega, int ncycles) {
+  if (ctx->D == 3) {
+    for (int c = 0; c < ncycles; c++) RC(d3_vcycle(ctx, u, b, r, u1, s, op, k2, bc, lmax, ndown, ntop, nup, omega));
+    return SRMG_OK;
+  }
+  const Signs sg = make_signs(bc);
+  for (int c = 0; c < ncycles; c++)
+    RC(vcycle_dev<double>(ctx, u, b, r, u1, s, op, k2, geom, sg, lmax, ndown, ntop, nup, omega));
+  return SRMG_OK;
+}
+}  // namespace
+
+// A per-operation V-cycle is a fixed sequence of several hundred small launches with no
+// host work in between, so it is captured once into a CUDA graph and replayed: the
+// kernels are the same, only their launch overhead changes.  The graph bakes in the
+// field pointers, the operator, the sweep counts and the tree's device arrays, all of
+// which are part of the key; a new tree drops every graph.
+int srmg::vcycle_ops(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, double s, int op, double k2,
+                     int geom, const int8_t *bc, int lmax, int ndown, int ntop, int nup, double omega, int ncycles) {
+  if (!ctx->use_op_graphs || ncycles <= 0)
+    return run_vcycles(ctx, u, b, r, u1, s, op, k2, geom, bc, lmax, ndown, ntop, nup, omega, ncycles);
+  std::vector<char> key;
+  for (const void *p : {(const void *)u, (const void *)b, (const void *)r, (const void *)u1, (const void *)ctx->d_tree,
+                        (const void *)ctx->stream})
+    put(key, p);
+  for (double v : {s, k2, omega}) put(key, v);
+  for (int v : {op, geom, lmax, ndown, ntop, nup, ncycles, ctx->D}) put(key, v);
+  put(key, ctx->generation);
+  const int nbc = ctx->D == 3 ? 27 : 9;
+  for (int i = 0; i < nbc; i++) put(key, (int8_t)(bc ? bc[i] : 1));
+  for (auto &g : ctx->op_graphs)
+    if (g.key == key) {
+      CK(cudaGraphLaunch(g.exec, ctx->stream));
+      ctx->launches += g.launches;
+      return SRMG_OK;
+    }
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  const int64_t l0 = ctx->launches;
+  const int rc = run_vcycles(ctx, u, b, r, u1, s, op, k2, geom, bc, lmax, ndown, ntop, nup, omega, ncycles);
+  const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &graph);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (ec != cudaSuccess) return cuda_check(ctx, ec, "cudaStreamEndCapture");
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ei != cudaSuccess) return cuda_check(ctx, ei, "cudaGraphInstantiate");
+  if (ctx->op_graphs.size() >= kOpGraphs) {
+    cudaGraphExecDestroy(ctx->op_graphs.front().exec);
+    ctx->op_graphs.erase(ctx->op_graphs.begin());
+  }
+  ctx->op_graphs.push_back({key, exec, ctx->launches - l0});
+  CK(cudaGraphLaunch(exec, ctx->stream));
+  return SRMG_OK;
+}
+
 // ------------------------------------------------------------------ device entry points
 
 extern "C" int srmg_vcycle_dev(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
@@ -936,8 +1019,15 @@ extern "C" int srmg_vcycle_dev(srmg_ctx *ctx, double *u, double *b, double *r, d
   RC(check_call_any(ctx, nblk_alloc, op, geom, bc));
   if (!u || !b || !r || !u1 || ndown < 0 || ntop < 0 || nup < 0 || ncycles < 0)
     return fail(ctx, SRMG_ERR_BADARG, "srmg_vcycle: bad arguments");
-  if (ctx->D == 3) {
-    for (int c = 0; c < ncycles; c++) RC(d3_vcycle(ctx, u, b, r, u1, s, op, k2, bc, lmax, ndown, ntop, nup, omega));
+  // the per-operation path (3D trees, BoxStencil trees, order 4, or the engine switched
+  // off) runs from a captured graph; the persistent engine is one launch already
+  const bool aligned = ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(b) |
+                         reinterpret_cast<uintptr_t>(r) | reinterpret_cast<uintptr_t>(u1)) & 15) == 0;
+  const bool engine = ctx->D == 2 && ctx->use_engine && aligned && !ctx->has_corners && op != SRMG_OP_LAPLACIAN4 &&
+                      ndown >= 1 && ntop >= 1 && nup >= 1 && ctx->nlev <= 30;
+  if (!engine) {
+    if (lmax < 0 || lmax > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "lmax %d out of range", lmax);
+    RC(vcycle_ops(ctx, u, b, r, u1, s, op, k2, geom, bc, lmax, ndown, ntop, nup, omega, ncycles));
     CK(cudaGetLastError());
     return SRMG_OK;
   }

@@ -714,7 +714,6 @@ int srmg::d3_solve(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc
   double *r = (double *)ctx->f64[2].p, *u1 = (double *)ctx->f64[3].p, *bw = (double *)ctx->f64[4].p;
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   CK(cudaMemcpyAsync(bw, b, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
-  const Signs27 sg = signs27(bc);
   RC(leafnorm(ctx, u, b, s, op, k2, 1, 1));
   RC(leafnorm(ctx, u, bw, s, op, k2, 0, 0));
   RC(read_small(ctx, 2));
@@ -724,7 +723,7 @@ int srmg::d3_solve(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc
   st->initial_rel = rel;
   int c = 0;
   while (rel > o->tol && c < o->max_cycles) {
-    RC(vcycle(ctx, u, bw, r, u1, s, op, k2, sg, 0, o->ndown, o->ntop, o->nup, o->omega));
+    RC(vcycle_ops(ctx, u, bw, r, u1, s, op, k2, 0, bc, 0, o->ndown, o->ntop, o->nup, o->omega, 1));
     ++c;
     RC(leafnorm(ctx, u, bw, s, op, k2, 0, 0));
     RC(read_small(ctx, 1));

@@ -155,6 +155,15 @@ struct srmg_ctx {
   cudaGraphExec_t graph_exec = nullptr;
   std::vector<const void *> graph_key;  // field pointers and options the graph was captured for
   bool use_graph = false;
+  // per-operation V-cycles replayed from captured graphs, by (fields, operator, sweep
+  // counts, tree, stream); at most kOpGraphs kept, the oldest replaced first
+  struct OpGraph {
+    std::vector<char> key;
+    cudaGraphExec_t exec = nullptr;
+    int64_t launches = 0;
+  };
+  std::vector<OpGraph> op_graphs;
+  bool use_op_graphs = true;
 
   // free boundary conditions (srmg_freebc_set): f [n], sin table [4n], work [n], b [n]
   srmg::DevBuf fbc;

@@ -17,6 +17,11 @@ int check_call_any(srmg_ctx *ctx, int64_t nblk_alloc, int op, int geom, const in
 // values per block of the context's fields: 20^D
 inline int64_t block_elems(const srmg_ctx *ctx) { return ctx->D == 3 ? (int64_t)kS * kS * kS : (int64_t)kSS; }
 void free_tree(srmg_ctx *ctx);
+void drop_op_graphs(srmg_ctx *ctx);
+// `ncycles` per-operation FP64 V-cycles (2D trees off the persistent engine, or 3D),
+// replayed from a captured CUDA graph when the option `op_graphs` is on (default).
+int vcycle_ops(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, double s, int op, double k2, int geom,
+               const int8_t *bc, int lmax, int ndown, int ntop, int nup, double omega, int ncycles);
 // the D = 3 bodies of the generic entry points (srmg3.cu)
 int d3_fill_ghost(srmg_ctx *ctx, double *u, int level, const int8_t *bc, int mask);
 int d3_gs_level(srmg_ctx *ctx, double *u, const double *b, int level, double omega, double sl, int op, double k2,

@@ -284,7 +284,6 @@ static int solve_fp64(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_al
   // per-operation kernels, host loop (one item)
   if (ctx->nitems != 1) return fail(ctx, SRMG_ERR_UNSUPPORTED, "batched solves need the persistent engine");
   const ItemSpec &sp = specs[0];
-  const Signs sg = make_signs(sp.bc);
   RC(leafnorm_dev<double>(ctx, u, b, sp.s, sp.op, sp.k2, geom, 1, 1));
   RC(leafnorm_dev<double>(ctx, u, bw, sp.s, sp.op, sp.k2, geom, 0, 0));
   RC(read_small(ctx, 2));
@@ -294,8 +293,7 @@ static int solve_fp64(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_al
   st->initial_rel = rel;
   int c = 0;
   while (rel > o->tol && c < o->max_cycles) {
-    RC(vcycle_dev<double>(ctx, u, bw, r, u1, sp.s, sp.op, sp.k2, geom, sg, 0, o->ndown, o->ntop, o->nup,
-                          o->omega));
+    RC(vcycle_ops(ctx, u, bw, r, u1, sp.s, sp.op, sp.k2, geom, sp.bc, 0, o->ndown, o->ntop, o->nup, o->omega, 1));
     c++;
     RC(leafnorm_dev<double>(ctx, u, bw, sp.s, sp.op, sp.k2, geom, 0, 0));
     RC(read_small(ctx, 1));
