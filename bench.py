@@ -269,10 +269,10 @@ def main():
     ap.add_argument("--no-config5", action="store_true", help="skip the full-size timestep (config-5) section")
     ap.add_argument("--config5-steps", type=int, default=200)
     ap.add_argument("--no-rows", action="store_true", help="skip the order-4, 3D and free-boundary section")
-    ap.add_argument("--only", default=None, choices=[None, "vcycle", "smooth", "cnn"],
+    ap.add_argument("--only", default=None, choices=[None, "vcycle", "smooth", "cnn", "rows"],
                     help="vcycle: time plain FP64 V-cycles only; smooth: GS iterations on the finest "
                          "level only; cnn: the warm-start network's inference forward, mma.sync and "
-                         "tcgen05 (profiling runs)")
+                         "tcgen05 (profiling runs); rows: the order-4, 3D and free-boundary section")
     ap.add_argument("--samples", type=int, default=4096, help="--only cnn: block samples per forward")
     ap.add_argument("--config", default="config2", choices=["config1", "config2", "config5"])
     args = ap.parse_args()
@@ -280,6 +280,9 @@ def main():
         return vcycle_only(args)
     if args.only == "cnn":
         return cnn_only(args)
+    if args.only == "rows":
+        print(json.dumps({"only": "rows", **run_rows(0)}))
+        return
 
     from srmg import gen, model
     from srmg.tree import leaf_cells

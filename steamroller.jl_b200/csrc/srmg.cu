@@ -659,13 +659,12 @@ int srmg::L_fill_ghost(srmg_ctx *ctx, T *u, int l, const Signs &sg, int mask) {
   }
   // BoxStencil tree: a boundary corner whose bnd is zero along one dimension mirrors
   // the adjacent face's ghost cells, so copy, boundary and interpolation run as three
-  // ordered passes (fill_ghost!, src/connectivity.jl:155-159), faces and corners each
-  const int gc = grid_for((int64_t)L.nblk * 16, threads, kGridCap);
+  // ordered passes (fill_ghost!, src/connectivity.jl:155-159), each launch filling the
+  // faces and corners of its pass
   for (int phase = 1; phase <= 4; phase <<= 1) {
     if (!(mask & phase)) continue;
     k_fill_ghost<T><<<gf, threads, 0, ctx->stream>>>(u, L.view(l), sg, phase);
-    k_fill_corner<T><<<gc, threads, 0, ctx->stream>>>(u, L.view(l), sg, phase);
-    ctx->launches += 2;
+    ctx->launches++;
   }
   return SRMG_OK;
 }

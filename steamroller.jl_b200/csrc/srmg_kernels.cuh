@@ -169,7 +169,13 @@ __device__ __forceinline__ T lhs_apply(const T *ub, int x, int y, const OpParams
 }
 
 // ---- ghost fill (src/connectivity.jl:155-258) --------------------------------------
-// One warp per (block, face): lane -> (layer g = lane/16, position k = lane%16).
+template <typename T>
+__device__ __forceinline__ void fill_corner_cell(T *__restrict__ u, const LevelView &lv, const Signs &sg, int phase,
+                                                 int64_t t);
+
+// One warp per (block, face): lane -> (layer g = lane/16, position k = lane%16).  On a
+// BoxStencil tree (lv.cfaces set) the launch covers one pass (mask 1, 2 or 4) and also
+// fills the corner cells of that pass: within one pass no cell reads another's result.
 template <typename T>
 __global__ void k_fill_ghost(T *__restrict__ u, LevelView lv, Signs sg, int mask) {
   const int lane = threadIdx.x & 31;
@@ -229,6 +235,11 @@ __global__ void k_fill_ghost(T *__restrict__ u, LevelView lv, Signs sg, int mask
       v = dadd<T>(v, dmul<T>(T(0.25), cb[o + kS * (2 * iz - 1)]));
       ub[x + kS * y] = v;
     }
+  }
+  if (lv.cfaces && (mask == 1 || mask == 2 || mask == 4)) {
+    const int64_t ct = (int64_t)lv.nblk * 16;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ct; t += (int64_t)gridDim.x * blockDim.x)
+      fill_corner_cell<T>(u, lv, sg, mask, t);
   }
 }
 
@@ -470,23 +481,23 @@ __global__ void k_rhs(T *__restrict__ q1, const T *__restrict__ q, LevelView lv,
 }
 
 // Corner ghosts of a BoxStencil tree (src/connectivity.jl:155-258 with diagonal faces):
-// 2 x 2 cells per corner, one thread per cell.  phase 1 = copy from the diagonal
-// neighbour, 2 = boundary mirror (bnd may be zero along one dimension: then the mirror
-// reads the adjacent face's ghost cells), 4 = linear interpolation from the parent's
-// subblockbnd cell (src/blockfield.jl:416-434, src/interp.jl:24-63).  The three phases
-// run as separate launches in that order, as fill_ghost! runs its three passes.
+// 2 x 2 cells per corner, one thread (index t) per cell.  phase 1 = copy from the
+// diagonal neighbour, 2 = boundary mirror (bnd may be zero along one dimension: then the
+// mirror reads the adjacent face's ghost cells, written by an earlier pass), 4 = linear
+// interpolation from the parent's subblockbnd cell (src/blockfield.jl:416-434,
+// src/interp.jl:24-63).  The three passes run as separate launches of k_fill_ghost in
+// that order, as fill_ghost! runs them.
 template <typename T>
-__global__ void k_fill_corner(T *__restrict__ u, LevelView lv, Signs sg, int phase) {
-  const int64_t total = (int64_t)lv.nblk * 16;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
+__device__ __forceinline__ void fill_corner_cell(T *__restrict__ u, const LevelView &lv, const Signs &sg, int phase,
+                                                 int64_t t) {
+  {
     const int bi = (int)(t >> 4), q = (int)((t >> 2) & 3), cell = (int)(t & 3);
     const int4 fi = lv.cfaces[4 * bi + q];
     const int type = fi.x;
-    if (type == FACE_NONE) continue;
+    if (type == FACE_NONE) return;
     if ((type == FACE_NEIGHBOR && phase != 1) || (type == FACE_BOUNDARY && phase != 2) ||
         (type == FACE_REFBND && phase != 4))
-      continue;
+      return;
     const int fr = 2 * (q & 1) - 1, fz = 2 * (q >> 1) - 1;  // ghost direction
     const int ir = cell & 1, iz = cell >> 1;
     const int x = (fr < 0 ? 0 : kM + kG) + ir, y = (fz < 0 ? 0 : kM + kG) + iz;
