@@ -11,7 +11,7 @@
 // with FFTW's unnormalised RODFT10 (DST-II) and RODFT01 (DST-III):
 //   DST-II:  Y_k = 2 sum_{j=0}^{n-1} X_j sin(pi (2j+1)(k+1) / (2n))
 //   DST-III: Y_k = (-1)^k X_{n-1} + 2 sum_{j=0}^{n-2} X_j sin(pi (j+1)(2k+1) / (2n)).
-// n is at most a few ten thousand, so both run as two-level direct sums (k_dst) in a
+// n is at most a few ten thousand, so both run as direct sums, one CTA per output in a
 // fixed order, with the sine of every argument from a table of sin(pi t / (2n)),
 // t = 0..4n-1 (the integer argument reduced exactly modulo 4n).  f, the transform's
 // kernel (modified Bessel functions of the domain's aspect), is computed by the caller
@@ -62,85 +62,59 @@ __global__ void k_getouter(double *__restrict__ u1, const double *__restrict__ u
   }
 }
 
-// Both transforms as two-level direct sums.  With the index of a term split as
-// j = j0 + 16 jb, the angle splits as alpha(j0) + beta(jb), and
-//   sin(alpha + beta) = sin(alpha) cos(beta) + cos(alpha) sin(beta),
-// so Y_k = sum_jb [cos(beta_jb) P_jb + sin(beta_jb) Q_jb] with the 16-term inner products
-// P_jb = sum_j0 z_j sin(alpha_j0), Q_jb = sum_j0 z_j cos(alpha_j0).  The sines and cosines
-// of alpha for the CTA's kDstK outputs sit in shared memory (read as broadcasts) and
-// two table gathers serve 16 terms.  Every angle is pi t / (2n) with the integer t
-// reduced exactly modulo 4n; cos(pi t / (2n)) = sin(pi (t + n) / (2n)).
-//   V = 2 (DST-II of x):   z_j = x_j, alpha = (k+1)(2 j0 + 1), beta = 32 (k+1) jb;
-//   V = 3 (DST-III of f x): z_m = f_{m-1} x_{m-1} for 1 <= m <= n-1 (z_0 = 0),
-//                           alpha = (2k+1) m0, beta = 16 (2k+1) mb, plus the (-1)^k term,
-//                           scaled by h / 2^(level-1) / 2.
-constexpr int kDstB = 16;  // inner block (n is a multiple of 16)
-constexpr int kDstK = 8;   // outputs per CTA pass
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double sh[kDstThreads / 32];
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x < 32) {
+    r = threadIdx.x < kDstThreads / 32 ? sh[threadIdx.x] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) r += __shfl_xor_sync(0xffffffffu, r, off);
+  }
+  return r;  // valid in thread 0
+}
 
-template <int V>
-__global__ void __launch_bounds__(kDstThreads) k_dst(double *__restrict__ y, const double *__restrict__ x,
-                                                     const double *__restrict__ f, const double *__restrict__ tab,
-                                                     int64_t n, double h, double p2) {
-  __shared__ double s_in[kDstK][kDstB], c_in[kDstK][kDstB];
-  __shared__ double red[kDstThreads / 32][kDstK];
-  const int64_t m4 = 4 * n, nb = n / kDstB;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int64_t k0 = (int64_t)blockIdx.x * kDstK; k0 < n; k0 += (int64_t)gridDim.x * kDstK) {
-    for (int q = threadIdx.x; q < kDstK * kDstB; q += kDstThreads) {
-      const int kk = q / kDstB, j0 = q % kDstB;
-      const int64_t k = k0 + kk;
-      const int64_t t = k < n ? (V == 2 ? (k + 1) * (2 * j0 + 1) : (2 * k + 1) * j0) % m4 : 0;
-      s_in[kk][j0] = tab[t];
-      c_in[kk][j0] = tab[(t + n) % m4];
+// y = DST-II(x).  The table index (2j + 1)(k + 1) mod 4n advances by a fixed step per
+// iteration of a thread, reduced by one conditional subtraction (4n < 2^31).
+__global__ void __launch_bounds__(kDstThreads) k_dst2(double *__restrict__ y, const double *__restrict__ x,
+                                                      const double *__restrict__ tab, int64_t n) {
+  const int m4 = (int)(4 * n);
+  for (int64_t k = blockIdx.x; k < n; k += gridDim.x) {
+    double acc = 0.0;
+    int t = (int)(((2 * (int64_t)threadIdx.x + 1) * (k + 1)) % m4);
+    const int step = (int)((2 * (int64_t)kDstThreads * (k + 1)) % m4);
+    for (int64_t j = threadIdx.x; j < n; j += kDstThreads) {
+      acc += x[j] * tab[t];
+      t += step;
+      if (t >= m4) t -= m4;
     }
+    const double s = block_sum(acc);
+    if (threadIdx.x == 0) y[k] = 2.0 * s;
     __syncthreads();
-    double acc[kDstK];
-#pragma unroll
-    for (int kk = 0; kk < kDstK; ++kk) acc[kk] = 0.0;
-    for (int64_t jb = threadIdx.x; jb < nb; jb += kDstThreads) {
-      double z[kDstB];
-#pragma unroll
-      for (int j0 = 0; j0 < kDstB; ++j0) {
-        const int64_t j = j0 + kDstB * jb;
-        if (V == 2) z[j0] = x[j];
-        else z[j0] = (j >= 1 && j <= n - 1) ? f[j - 1] * x[j - 1] : 0.0;
-      }
-#pragma unroll
-      for (int kk = 0; kk < kDstK; ++kk) {
-        const int64_t k = k0 + kk;
-        double P = 0.0, Q = 0.0;
-#pragma unroll
-        for (int j0 = 0; j0 < kDstB; ++j0) {
-          P = fma(z[j0], s_in[kk][j0], P);
-          Q = fma(z[j0], c_in[kk][j0], Q);
-        }
-        const int64_t to = k < n ? (V == 2 ? 2 * kDstB * (k + 1) * jb : kDstB * (2 * k + 1) * jb) % m4 : 0;
-        acc[kk] = fma(tab[(to + n) % m4], P, acc[kk]);
-        acc[kk] = fma(tab[to], Q, acc[kk]);
-      }
+  }
+}
+
+// b = DST-III(f .* a) * h / 2^(level-1) / 2, the product f a rounded once per element
+__global__ void __launch_bounds__(kDstThreads) k_dst3_scale(double *__restrict__ b, const double *__restrict__ a,
+                                                            const double *__restrict__ f,
+                                                            const double *__restrict__ tab, int64_t n, double h,
+                                                            double p2) {
+  const int m4 = (int)(4 * n);
+  for (int64_t k = blockIdx.x; k < n; k += gridDim.x) {
+    double acc = 0.0;
+    int t = (int)(((int64_t)threadIdx.x + 1) * (2 * k + 1) % m4);
+    const int step = (int)((int64_t)kDstThreads * (2 * k + 1) % m4);
+    for (int64_t j = threadIdx.x; j < n - 1; j += kDstThreads) {
+      acc += (f[j] * a[j]) * tab[t];
+      t += step;
+      if (t >= m4) t -= m4;
     }
-    // fixed-order reduction: warp shuffles, then the warps' partials in order
-#pragma unroll
-    for (int kk = 0; kk < kDstK; ++kk) {
-      double v = acc[kk];
-      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-      if (lane == 0) red[warp][kk] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x < kDstK) {
-      const int kk = threadIdx.x;
-      const int64_t k = k0 + kk;
-      double sum = 0.0;
-      for (int w = 0; w < kDstThreads / 32; ++w) sum += red[w][kk];
-      if (k < n) {
-        if (V == 2) {
-          y[k] = 2.0 * sum;
-        } else {
-          const double last = f[n - 1] * x[n - 1];
-          const double yk = ((k & 1) ? -last : last) + 2.0 * sum;
-          y[k] = yk * h / p2 / 2.0;
-        }
-      }
+    const double s = block_sum(acc);
+    if (threadIdx.x == 0) {
+      const double last = f[n - 1] * a[n - 1];
+      const double yk = ((k & 1) ? -last : last) + 2.0 * s;
+      b[k] = yk * h / p2 / 2.0;
     }
     __syncthreads();
   }
@@ -338,12 +312,12 @@ extern "C" int srmg_freebc_dev(srmg_ctx *ctx, double *q, const double *u, int64_
                                                                        extent(ctx, l, dim), 1 << (level - l), hl);
     ctx->launches++;
   }
-  const int g = (int)std::min<int64_t>((n + kDstK - 1) / kDstK, 148 * 16);
-  k_dst<2><<<g, kDstThreads, 0, ctx->stream>>>(am, u1, nullptr, fbc_tab(ctx), n, 0.0, 1.0);
+  const int g = (int)std::min<int64_t>(n, 148 * 16);
+  k_dst2<<<g, kDstThreads, 0, ctx->stream>>>(am, u1, fbc_tab(ctx), n);
   // DST-III reads am and writes b: keep them apart (u1 is free again)
   CK(cudaMemcpyAsync(u1, am, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-  k_dst<3><<<g, kDstThreads, 0, ctx->stream>>>(b, u1, fbc_f(ctx), fbc_tab(ctx), n, h,
-                                               (double)((int64_t)1 << (level - 1)));
+  k_dst3_scale<<<g, kDstThreads, 0, ctx->stream>>>(b, u1, fbc_f(ctx), fbc_tab(ctx), n, h,
+                                                   (double)((int64_t)1 << (level - 1)));
   ctx->launches += 2;
   const int order_star[4] = {0, 1, 2, 3};                 // StarStencil order (src/stencil.jl:16-32)
   const int order_box[8] = {4, 2, 5, 0, 1, 6, 3, 7};      // BoxStencil order (src/stencil.jl:34-90)
