@@ -30,12 +30,15 @@ using namespace srmg;
 
 extern "C" int srmg_batch_set(srmg_ctx *ctx, int nitems, const srmg_item *items, int geom) {
   if (!ctx) return SRMG_ERR_BADARG;
+  if (ctx->D != 2) return fail(ctx, SRMG_ERR_UNSUPPORTED, "srmg_batch_set: batches take two-dimensional trees");
   if (nitems < 1 || nitems > (1 << 22) || !items) return fail(ctx, SRMG_ERR_BADARG, "srmg_batch_set: bad item list");
   if (geom < 0 || geom > 2) return fail(ctx, SRMG_ERR_UNSUPPORTED, "unsupported geometry %d", geom);
   int nlev = 0;
   int64_t total = 0;
   for (int k = 0; k < nitems; k++) {
     const srmg_ctx *t = items[k].tree;
+    if (t && t->D != 2)
+      return fail(ctx, SRMG_ERR_UNSUPPORTED, "item %d: batches take two-dimensional trees", k);
     if (!t || !t->has_tree || t->htree.nlev < 1)
       return fail(ctx, SRMG_ERR_NOTREE, "item %d: its context holds no tree", k);
     if (items[k].op != SRMG_OP_LAPLACIAN && items[k].op != SRMG_OP_HELMHOLTZ)

@@ -216,8 +216,9 @@ mutable struct State3
     ctx::Ptr{Cvoid}
     fingerprint::UInt64
     generation::UInt64
+    levelfp::Vector{UInt64}
 end
-const STATE3 = State3(C_NULL, 0, 0)
+const STATE3 = State3(C_NULL, 0, 0, UInt64[])
 
 function context3()
     if STATE3.ctx == C_NULL
@@ -236,13 +237,18 @@ function check3(rc)
     error("libsrmg error $rc: $msg")
 end
 
+function layer_fingerprint3(layer)
+    h = UInt64(length(layer.pairs))
+    for (c, blk) in layer.pairs
+        h += UInt64(blk) * 0x9e3779b97f4a7c15 + UInt64(c[1]) * 1000003 + UInt64(c[2]) * 7919 + UInt64(c[3])
+    end
+    h
+end
+
 function fingerprint3(tree)
     h = UInt64(length(tree))
     for layer in tree
-        h = h * 0x100000001b3 + UInt64(length(layer.pairs))
-        for (c, blk) in layer.pairs
-            h += UInt64(blk) * 0x9e3779b97f4a7c15 + UInt64(c[1]) * 1000003 + UInt64(c[2]) * 7919 + UInt64(c[3])
-        end
+        h = h * 0x100000001b3 + layer_fingerprint3(layer)
     end
     h
 end
@@ -268,6 +274,7 @@ function upload3!(tree, conn)
                      STATE3.generation))
     end
     STATE3.fingerprint = fp
+    STATE3.levelfp = UInt64[layer_fingerprint3(l) for l in tree]
     nothing
 end
 
@@ -316,6 +323,23 @@ function Steamroller.fmg!(u::GPUField3, b::GPUField3, r::GPUField3, u1::GPUField
                       Float64, Cint, Float64, Cint, Ptr{Int8}, Cint, Cint, Cint, Float64),
                      context3(), pointer(u.u), pointer(b.u), pointer(r.u), pointer(u1.u), size(u.u, 4),
                      Float64(s), op, k2, Cint(0), Base.unsafe_convert(Ptr{Int8}, a), ndown, ntop, nup, Float64(ω)))
+    end
+    nothing
+end
+
+# rhs_level! for the 3D order-4 discretisation (src/multigrid.jl:380-388), while the level
+# matches the uploaded octree
+function Steamroller.rhs_level!(q1::GPUField3, q::GPUField3, layer, ld::LaplacianDiscretization{3,4},
+                                geometry::CartesianGeometry)
+    lv = layer.level
+    if !(STATE.enabled && STATE3.ctx != C_NULL && 1 <= lv <= length(STATE3.levelfp) &&
+         layer_fingerprint3(layer) == STATE3.levelfp[lv])
+        return invoke(Steamroller.rhs_level!, Tuple{Any,Any,Any,Any,Any}, q1, q, layer, ld, geometry)
+    end
+    GC.@preserve q1 q begin
+        check3(ccall((:srmg_rhs_level, libsrmg), Cint,
+                     (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int64, Cint, Cint, Cint),
+                     context3(), pointer(q1.u), pointer(q.u), size(q.u, 4), Cint(lv), Cint(2), Cint(0)))
     end
     nothing
 end
