@@ -53,3 +53,15 @@ def test_unsupported_shapes_rejected():
     assert mg.lib().srmg_create(ctypes.byref(h), 1, 16, 2, 0) == -6
     assert mg.lib().srmg_create(ctypes.byref(h), 2, 8, 2, 0) == -6
     assert mg.lib().srmg_create(ctypes.byref(h), 3, 16, 4, 0) == -6
+
+
+def test_three_dimensional_struct_layouts():
+    """The D = 3 edge records the Python builder emits have the isbits sizes of
+    Pair{CartesianIndex{3},Int}, Neighbor{3}, Boundary{3}, RefBoundary{3}, Child{3}
+    (the srmg_*3 structs of include/srmg.h)."""
+    from srmg import tree3
+    assert tree3.PAIR3_DTYPE.itemsize == 32
+    assert tree3.NEIGHBOR3_DTYPE.itemsize == 40
+    assert tree3.BOUNDARY3_DTYPE.itemsize == 64
+    assert tree3.REFBND3_DTYPE.itemsize == 64
+    assert tree3.CHILD3_DTYPE.itemsize == 40

@@ -9,6 +9,8 @@ src/restrict.jl:5-25):
     second and fourth order;
   * V-cycles on a refined octree drive the residual norm below 1e-10.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -110,3 +112,23 @@ def test_vcycles_converge_on_refined_octree(op):
     u = np.zeros_like(b)
     c, rel = o.solve(u, b, 1e-10, max_cycles=300)
     assert rel <= 1e-10, (c, rel)
+
+
+@pytest.mark.parametrize("op", [0, 2])
+def test_colours_cover_every_cell_once(op):
+    """RedBlack (2 colours) and FourColors (4) for D = 3: with u = 0, b = 1 each colour
+    changes a disjoint set of valid cells and together they change all of them."""
+    p = gen3.refined3(seed=6, op=op)
+    o = Oracle3(p)
+    ncol = 4 if op == 2 else 2
+    blk = p.tree[0].pairs[0][1] - 1
+    seen = np.zeros((16, 16, 16), dtype=int)
+    for c in range(ncol):
+        u = np.zeros_like(p.b)
+        b = np.ones_like(p.b)
+        if op == 2:
+            olib().orc3_gs4_level(_ptr(u), _ptr(b), 1.0, 1.0, o.ot.ref, 1, ctypes.byref(o.op), c >> 1, c & 1)
+        else:
+            olib().orc3_gs_level(_ptr(u), _ptr(b), 1.0, 1.0, o.ot.ref, 1, ctypes.byref(o.op), c)
+        seen += (u[blk, 2:18, 2:18, 2:18] != 0)
+    assert np.all(seen == 1)

@@ -161,3 +161,18 @@ def test_rhs_level_order2_is_identity():
         for _, blk in layer.pairs:
             used[blk - 1] = True
     assert np.array_equal(q1[used][:, 2:18, 2:18].view(np.uint64), q[used][:, 2:18, 2:18].view(np.uint64))
+
+
+def test_four_colours_cover_every_cell_once():
+    """FourColors {0,0}, {0,1}, {1,0}, {1,1} (src/multigrid.jl:206-232): with u = 0 and
+    b = 1, each colour changes a disjoint quarter of the valid cells."""
+    p = gen.order4_problem(seed=12, geom=gen.GEOM_CART)
+    o = Oracle(p)
+    blk = p.tree[0].pairs[0][1] - 1
+    seen = np.zeros((16, 16), dtype=int)
+    for c in range(4):
+        u = np.zeros_like(p.b)
+        b = np.ones_like(p.b)
+        olib().orc_gs4_level(_ptr(u), _ptr(b), 1.0, 1.0, o.ot.ref, 1, ctypes.byref(o.op), c >> 1, c & 1)
+        seen += (u[blk, 2:18, 2:18] != 0)
+    assert np.all(seen == 1)
