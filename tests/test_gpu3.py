@@ -16,7 +16,7 @@ import pytest
 from conftest import gpu_available
 from oracle import Oracle3, lib as olib, _ptr
 from srmg import gen3, multigrid as mg
-from srmg.tree3 import connectivity, STAR3, BOX3
+from srmg.tree3 import Tree3, populate, connectivity, STAR3, BOX3
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not gpu_available(), reason="needs a CUDA GPU")]
@@ -245,3 +245,28 @@ def test_three_dimensional_limits(pair):
     with pytest.raises(mg.SrmgError) as ei:     # cylindrical geometry
         mg.vcycle_(pair.ctx, u.copy(), b0.copy(), u.copy(), u.copy(), p.s, 1, p.bc, lpl(p))
     assert ei.value.code == SRMG_ERR_UNSUPPORTED
+
+
+def test_oblong_root_and_partial_vcycle():
+    """An octree on a (2, 1, 1) root grid with refinement, and V-cycles that stop at a
+    level below the finest (lmax)."""
+    from srmg.tree3 import refine_block
+    t = Tree3((2, 1, 1), 4)
+    populate(t, 2)
+    refine_block(t, 2, (3, 2, 1))
+    t.sync()
+    conn = connectivity(t, STAR3)
+    p = gen3.make_problem3(t, conn, lambda x, y, z: np.exp(-((x - 1.2) ** 2 + (y - 0.6) ** 2 + z ** 2) / 0.05),
+                           (1.0 / 16) ** 2)
+    pr = Pair(p)
+    b0 = pr.rhs()
+    z0 = np.zeros_like(b0)
+    for lmax in (0, 2):
+        ug, bg, rg, u1g = torch_cuda(z0), torch_cuda(b0), torch_cuda(z0), torch_cuda(z0)
+        mg.vcycle_(pr.ctx, ug, bg, rg, u1g, p.s, 0, p.bc, None, lmax=lmax, ndown=2, ntop=4, nup=2, ncycles=2)
+        pr.ctx.synchronize()
+        uo, bo = z0.copy(), b0.copy()
+        for _ in range(2):
+            pr.orc.vcycle(uo, bo, z0.copy(), z0.copy(), lmax=lmax, ndown=2, ntop=4, nup=2)
+        assert rel_l2(ug.cpu().numpy(), uo) <= REL, lmax
+    pr.ctx.close()

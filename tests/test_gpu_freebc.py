@@ -143,3 +143,33 @@ def test_freebc_refuses_bad_use():
     with pytest.raises(mg.SrmgError):                   # n does not match FreeBC's length
         mg.freebc_set(ctx, 1, 7, (1, 1), f)
     ctx.close()
+
+
+def test_freebc_oblong_root():
+    """A (1, 2) root grid: the outer column is twice as long (n = 2 * 16 * 2^(level-1))."""
+    from srmg.tree import Tree, populate, connectivity, boundaryconditions, refine_block
+    t = Tree((1, 2), 4)
+    populate(t, 2)
+    refine_block(t, 2, (2, 3))
+    t.sync()
+    conn = connectivity(t)
+    p = gen.make_problem(t, lambda r, z, l, gi, gj: np.exp(-(r * r + (z - 0.012) ** 2) / 2e-5), gen.poisson_scale(),
+                         bc=boundaryconditions(((1, -1), (-1, -1))), conn=conn)
+    level = len(t)
+    n, H, R, f = fo.kernel(1, level, (1, 2), p.h1)
+    assert n == 2 * 16 * 2 ** (level - 1)
+    ctx = mg.Context(0).set_tree(p.tree, p.conn)
+    mg.freebc_set(ctx, 1, level, (1, 2), f)
+    rng = np.random.default_rng(8)
+    u = rng.standard_normal(p.b.shape)
+    q = rng.standard_normal(p.b.shape)
+    qo = q.copy()
+    bo = fo.freebc(qo, u, p.h1, p.s, p.tree, p.conn, 1, level, f)
+    qh = q.copy()
+    bh = np.zeros(n)
+    mg.freebc_(ctx, qh, u, p.h1, p.s, b_out=bh)
+    assert rel_l2(bh, bo) <= REL
+    changed = qo != q
+    np.testing.assert_array_equal(qh[~changed], q[~changed])
+    assert rel_l2(qh[changed] - q[changed], qo[changed] - q[changed]) <= REL
+    ctx.close()

@@ -284,3 +284,30 @@ def test_unsupported_combinations(pair):
         mg.vcycle_(star, u.copy(), b0.copy(), u.copy(), u.copy(), p.s, p.geom, p.bc, "laplacian4")
     assert ei.value.code == SRMG_ERR_UNSUPPORTED
     star.close()
+
+
+@pytest.mark.parametrize("root,levels,geom", [((1, 1), 1, gen.GEOM_CART), ((2, 1), 3, gen.GEOM_CYL1),
+                                              ((1, 2), 3, gen.GEOM_CYL2)])
+def test_small_and_oblong_trees(root, levels, geom):
+    """Edge cases: a single block (every ghost, corners included, from the boundary) and
+    oblong root grids, uniform trees with BoxStencil connectivity."""
+    from srmg.tree import Tree, populate
+    t = Tree(root, levels)
+    populate(t, levels)
+    conn = connectivity(t, BOX2)
+    bc = {gen.GEOM_CART: gen.boundaryconditions(((-1, -1), (-1, -1))), gen.GEOM_CYL1: gen.BC_POISSON,
+          gen.GEOM_CYL2: gen.boundaryconditions(((-1, -1), (1, 1)))}[geom]
+    p = gen.make_problem(t, lambda r, z, l, gi, gj: np.exp(-((r - 0.004) ** 2 + (z - 0.006) ** 2) / 1e-5) * 1e18,
+                         gen.poisson_scale(), op=gen.OP_LAPLACIAN4, bc=bc, conn=conn)
+    p.geom = geom
+    pr = Pair(p)
+    b0 = pr.rhs()
+    z = np.zeros_like(b0)
+    ug, bg, rg, u1g = torch_cuda(z), torch_cuda(b0), torch_cuda(z), torch_cuda(z)
+    mg.vcycle_(pr.ctx, ug, bg, rg, u1g, p.s, p.geom, p.bc, "laplacian4", ndown=2, ntop=4, nup=2, ncycles=2)
+    pr.ctx.synchronize()
+    uo, bo = z.copy(), b0.copy()
+    for _ in range(2):
+        pr.orc.vcycle(uo, bo, z.copy(), z.copy(), ndown=2, ntop=4, nup=2)
+    assert rel_l2(to_np(ug), uo) <= REL
+    pr.ctx.close()
