@@ -86,10 +86,16 @@ CASES = {
                     lambda r, z: (-A * A * np.cos(A * r) - A * np.sin(A * r) / r - B * B * np.cos(A * r))
                     * np.sin(B * z),
                     boundaryconditions(((1, -1), (-1, -1)))),
+    # the same with the radial dimension second (CylindricalGeometry{2}): the block
+    # coordinates' first component is then the axial one
+    gen.GEOM_CYL2: (lambda a, r: np.cos(A * r) * np.sin(B * a),
+                    lambda a, r: (-A * A * np.cos(A * r) - A * np.sin(A * r) / r - B * B * np.cos(A * r))
+                    * np.sin(B * a),
+                    boundaryconditions(((-1, -1), (1, -1)))),
 }
 
 
-@pytest.mark.parametrize("geom", [gen.GEOM_CART, gen.GEOM_CYL1])
+@pytest.mark.parametrize("geom", [gen.GEOM_CART, gen.GEOM_CYL1, gen.GEOM_CYL2])
 def test_order4_interior_truncation_is_fourth_order(geom):
     ex, lap, bc = CASES[geom]
     errs = []
