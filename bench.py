@@ -454,6 +454,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = run_cpu_reference(problem, fp64_st["cycles"])
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        # the same on one host core (the oracle's OpenMP loops with one thread)
+        cpu1 = run_cpu_reference(problem, fp64_st["cycles"], budget_s=8.0, threads=1)
+        line["cpu_baseline_1core"] = {k: cpu1[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if rank == 0:
         print(json.dumps(line))
     ctx.close()
