@@ -969,7 +969,10 @@ int run_vcycles(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, doub
 // which are part of the key; a new tree drops every graph.
 int srmg::vcycle_ops(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, double s, int op, double k2,
                      int geom, const int8_t *bc, int lmax, int ndown, int ntop, int nup, double omega, int ncycles) {
-  if (!ctx->use_op_graphs || ncycles <= 0)
+  // a caller already capturing the stream records the launches into its own graph
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(ctx->stream, &cap));
+  if (!ctx->use_op_graphs || ncycles <= 0 || cap != cudaStreamCaptureStatusNone)
     return run_vcycles(ctx, u, b, r, u1, s, op, k2, geom, bc, lmax, ndown, ntop, nup, omega, ncycles);
   std::vector<char> key;
   for (const void *p : {(const void *)u, (const void *)b, (const void *)r, (const void *)u1, (const void *)ctx->d_tree,
