@@ -391,7 +391,8 @@ end
 # for fill_ghost_free!.  The transform kernel conf.f is handed over once per FreeBC.
 function Steamroller.freebc!(q::GPUField, u::GPUField, h, s, tree, conn, conf::FreeBC{2})
     if !STATE.enabled
-        return invoke(Steamroller.freebc!, Tuple{Any,Any,Any,Any,Any,Any,FreeBC}, q, u, h, s, tree, conn, conf)
+        return invoke(Steamroller.freebc!, Tuple{ScalarBlockField,ScalarBlockField,Any,Any,Any,Any,FreeBC},
+                      q, u, h, s, tree, conn, conf)
     end
     upload!(tree, conn)
     id = objectid(conf)
@@ -416,7 +417,7 @@ end
 
 function Steamroller.fill_ghost_free!(u::GPUField, conf::FreeBC{2}, tree, l)
     if !(tree_current(tree) && STATE.fbc == objectid(conf))
-        return invoke(Steamroller.fill_ghost_free!, Tuple{Any,FreeBC,Any,Any}, u, conf, tree, l)
+        return invoke(Steamroller.fill_ghost_free!, Tuple{ScalarBlockField,FreeBC,Any,Any}, u, conf, tree, l)
     end
     GC.@preserve u begin
         check(ccall((:srmg_fill_ghost_free, libsrmg), Cint, (Ptr{Cvoid}, Ptr{Float64}, Int64, Cint),
