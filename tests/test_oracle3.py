@@ -132,3 +132,34 @@ def test_colours_cover_every_cell_once(op):
             olib().orc3_gs_level(_ptr(u), _ptr(b), 1.0, 1.0, o.ot.ref, 1, ctypes.byref(o.op), c)
         seen += (u[blk, 2:18, 2:18, 2:18] != 0)
     assert np.all(seen == 1)
+
+
+def test_boundary_table_is_column_major():
+    """boundaryconditions (src/boundary.jl:28-38) for D = 3: entry a[2+b1, 2+b2, 2+b3]
+    is the product of the per-dimension signs of the nonzero b_d, at flat index
+    (1+b1) + 3(1+b2) + 9(1+b3)."""
+    from srmg.tree3 import boundaryconditions
+    desc = ((1, -1), (-1, -1), (1, -1))
+    a = boundaryconditions(desc)
+    for b1 in (-1, 0, 1):
+        for b2 in (-1, 0, 1):
+            for b3 in (-1, 0, 1):
+                want = 1
+                for d, b in enumerate((b1, b2, b3)):
+                    if b:
+                        want *= desc[d][0] if b < 0 else desc[d][1]
+                assert a[(1 + b1) + 3 * (1 + b2) + 9 * (1 + b3)] == want
+
+
+def test_generator_restriction_matches_oracle():
+    """The problem generator's numpy restrict_full! sums the 8 fine cells in the
+    reference's order, so it matches the oracle's restriction chain bit for bit."""
+    p = gen3.refined3(seed=8)
+    o = Oracle3(p)
+    f = np.random.default_rng(3).standard_normal(p.b.shape)
+    a = f.copy()
+    gen3.restrict_full3(a, p.tree, p.conn)
+    b = f.copy()
+    for l in range(len(p.tree), 1, -1):
+        olib().orc3_restrict_level(_ptr(b), o.ot.ref, l)
+    np.testing.assert_array_equal(a.view(np.uint64), b.view(np.uint64))
