@@ -170,3 +170,21 @@ def test_netcharge_and_field_of_linear_potential(uniform3):
     np.testing.assert_allclose(er, -A + e0[0], rtol=1e-9)
     np.testing.assert_allclose(ez, -B + e0[1], rtol=1e-9)
     np.testing.assert_allclose(eabs[vm], np.hypot(-A + e0[0], -B + e0[1]), rtol=1e-9)
+
+
+def test_generator_restriction_matches_oracle():
+    """The problem generators restrict right-hand sides onto parent blocks the way
+    restrict_full! does (src/restrict.jl:43-47); checked bit for bit against the
+    oracle's restriction chain on a refined tree."""
+    import numpy as np
+    from oracle import Oracle, lib as olib, _ptr
+    from srmg import gen
+    p = gen.order4_problem(seed=13, geom=gen.GEOM_CYL1)
+    o = Oracle(p)
+    f = np.random.default_rng(5).standard_normal(p.b.shape)
+    a = f.copy()
+    gen.restrict_full_np(a, p.tree, p.conn)
+    b = f.copy()
+    for l in range(len(p.tree), 1, -1):
+        olib().orc_restrict_level(_ptr(b), o.ot.ref, l)
+    np.testing.assert_array_equal(a.view(np.uint64), b.view(np.uint64))
