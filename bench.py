@@ -17,7 +17,9 @@ data with the shapes of the reference's own setup (no published data exists).
   e2e        the same solve through the C ABI with host arrays (H2D of u and b and
              D2H of u inside the timed region)
   cpu_baseline  the oracle (C restatement of the reference FP64 solve, OpenMP) on
-             the host cores, on a bounded sample of V-cycles
+             the host cores: complete solves from a zero guess to the tolerance
+  error_vs_fp64  each GPU result's relative L2 error on the leaf cells against the
+             oracle's FP64 solution of the same problem to 1e-11
 
 `--impl reference` times the reference's CPU algorithm (the oracle, since Julia is not
 available) on the same workload.  Multi-GPU: replicas (independent solves per rank,
@@ -223,35 +225,52 @@ def shard(n, rank, world):
     return list(range(rank, n, world))
 
 
-def run_cpu_reference(problem, fp64_cycles, budget_s=12.0, threads=None, warm=1):
-    """Time reference-algorithm V-cycles (the oracle, OpenMP) on the host cores and
-    scale to solves/s with the FP64 cycle count of the same solve."""
+def _oracle(problem, threads):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc_mod
     orc_mod.build() if not os.path.exists(orc_mod._LIB_PATH) else None
-    threads = threads or os.cpu_count()
-    orc = orc_mod.Oracle(problem, threads=threads)
-    u = np.zeros_like(problem.b)
+    return orc_mod.Oracle(problem, threads=threads)
+
+
+def oracle_solve(problem, tol, threads=None, u0=None, max_cycles=5000):
+    """One complete reference-algorithm FP64 solve (the oracle: V-cycles (2, 2, 4) with
+    resnorm after each, src/multigrid.jl:60-106, 391-417) from u0 (zero if None) to
+    resnorm/leafnorm(b) <= tol.  Returns (u, cycles, rel_residual, wall seconds)."""
+    orc = _oracle(problem, threads or os.cpu_count())
+    u = np.zeros_like(problem.b) if u0 is None else u0.copy()
     b = problem.b.copy()
-    r, u1 = np.zeros_like(u), np.zeros_like(u)
+    t0 = time.perf_counter()
+    c, rel = orc.solve(u, b, tol, max_cycles=max_cycles, ndown=2, ntop=4, nup=2)
+    return u, c, rel, time.perf_counter() - t0
+
+
+def run_cpu_reference(problem, steps=1, warm=0, threads=None, budget_s=None):
+    """Time complete reference-algorithm solves (the oracle, OpenMP over blocks per
+    level, as the reference's @batch loops) from a zero guess to 1e-8 on the host cores:
+    `warm` untimed solves, then `steps` timed ones (with budget_s: as many as fit, at
+    least one).  Every solve is run to the tolerance; nothing is extrapolated."""
+    threads = threads or os.cpu_count()
     for _ in range(warm):
-        orc.vcycle(u, b, r, u1, ndown=2, ntop=4, nup=2)
-    n, t0 = 0, time.perf_counter()
+        oracle_solve(problem, TOL, threads)
+    times, cycles, rels = [], [], []
+    t_start = time.perf_counter()
     while True:
-        orc.vcycle(u, b, r, u1, ndown=2, ntop=4, nup=2)
-        n += 1
-        if time.perf_counter() - t0 > budget_s:
+        _, c, rel, dt = oracle_solve(problem, TOL, threads)
+        times.append(dt)
+        cycles.append(c)
+        rels.append(rel)
+        if budget_s is None:
+            if len(times) >= steps:
+                break
+        elif time.perf_counter() - t_start + dt > budget_s:
             break
-    dt = (time.perf_counter() - t0) / n
-    # one resnorm per cycle, as the solve loop does
-    t1 = time.perf_counter()
-    orc.resnorm(r, b, u)
-    dt += time.perf_counter() - t1
-    solves_per_s = 1.0 / (fp64_cycles * dt)
-    return {"value": solves_per_s, "unit": "solves/s", "cores": threads, "kind": "port",
-            "sample": f"{n} FP64 V-cycles (+resnorm) of the same tree timed ({n * dt:.1f} s), "
-                      f"scaled by the {fp64_cycles} cycles one solve takes",
-            "s_per_vcycle": dt}
+    total = float(np.sum(times))
+    n = len(times)
+    return {"value": n / total, "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{n} complete FP64 solves of this tree from a zero guess to rel. residual {TOL:g} "
+                      f"({cycles[0]} V-cycles each, {total:.1f} s)",
+            "ms_per_solve": 1e3 * total / n, "cycles_per_solve": int(cycles[0]),
+            "rel_residual": float(max(rels)), "solves": n}
 
 
 def main():
@@ -298,18 +317,18 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        # FP64 cycle count of this solve: the reference algorithm converges identically on
-        # the GPU path; count cycles with the oracle on a bounded sample instead.
-        cyc = fp64_cycle_count_estimate(problem)
-        cpu = run_cpu_reference(problem, cyc["cycles"], budget_s=max(5.0, 2.0 * args.steps))
+        # one step = one complete FP64 solve of the reference algorithm (the oracle) from
+        # a zero guess to the tolerance, wall-timed on the host cores
+        cpu = run_cpu_reference(problem, steps=args.steps, warm=args.warmup)
         line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": "solves/s",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": 1e3 / cpu["value"], "higher_is_better": True, "scaling": "weak",
+                "ms_per_step": cpu["ms_per_solve"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
                 "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "e2e": {"value": cpu["value"], "unit": "solves/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0},
-                "fp64_cycles_per_solve": cyc}
+                "fp64_cycles_per_solve": {"cycles": cpu["cycles_per_solve"], "extrapolated": False,
+                                          "rel_residual": cpu["rel_residual"]}}
         print(json.dumps(line))
         return
 
@@ -361,21 +380,31 @@ def main():
     value = world * args.steps / (mixed_ms / 1e3)
     fp64_value = world * fp64_steps / (fp64_ms / 1e3)
 
-    # error of each result on the leaf cells against a tight FP64 solve (tol 1e-11; the
-    # FP64 GPU path matches the oracle to <= 1e-12 in the parity tests)
+    # error of each result on the leaf cells against the FP64 oracle's solution of the
+    # same problem to 1e-11 (the oracle's complete solve on the host cores, rank 0); with
+    # --no-cpu, against the plain FP64 GPU path's solve to 1e-11 instead
     from srmg.timestep import leaf_mask
-    leaf = torch.from_numpy(leaf_mask(problem.tree, problem.nblk)).to(dev)
+    leaf_np = leaf_mask(problem.tree, problem.nblk)
+    leaf = torch.from_numpy(leaf_np).to(dev)
     sols = {}
-    for name, mode, tol in (("reference", mg.MODE_FP64, 1e-11), ("mixed", mg.MODE_MIXED, TOL),
+    for name, mode, tol in (("fp64_tight", mg.MODE_FP64, 1e-11), ("mixed", mg.MODE_MIXED, TOL),
                             ("fp64", mg.MODE_FP64, TOL)):
         with torch.cuda.stream(stream):
             u.zero_()
         stream.synchronize()
         mg.solve(ctx, u, b, s, geom, bc, tol=tol, mode=mode, max_cycles=5000)
-        sols[name] = u[leaf].clone()
-    nref = float(sols["reference"].norm())
-    err = {k: float((sols[k] - sols["reference"]).norm()) / nref for k in ("mixed", "fp64")}
-    err["reference"] = "FP64 GPU solve to 1e-11 (leaf cells, relative L2)"
+        sols[name] = u[leaf].cpu().numpy()
+    if rank == 0 and not args.no_cpu:
+        uo, oc, orel, ot = oracle_solve(problem, 1e-11)
+        ref = uo[leaf_np]
+        ref_name = (f"FP64 oracle solve to 1e-11 from zero ({oc} V-cycles, rel. residual {orel:.2e}, "
+                    f"{ot:.1f} s on {os.cpu_count()} host cores); leaf cells, relative L2")
+    else:
+        ref = sols["fp64_tight"]
+        ref_name = "FP64 GPU solve to 1e-11 (leaf cells, relative L2)"
+    nref = float(np.linalg.norm(ref))
+    err = {k: float(np.linalg.norm(sols[k] - ref)) / nref for k in ("mixed", "fp64", "fp64_tight")}
+    err["reference"] = ref_name
 
     # roofline of the plain FP64 V-cycle (model bytes / event-timed V-cycle)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -452,10 +481,12 @@ def main():
     if not args.no_rows:
         line["rows"] = run_rows(local)
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = run_cpu_reference(problem, fp64_st["cycles"])
+        # complete oracle solves from zero to 1e-8 for about 20 s (at least one)
+        cpu = run_cpu_reference(problem, budget_s=20.0)
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
-        # the same on one host core (the oracle's OpenMP loops with one thread)
-        cpu1 = run_cpu_reference(problem, fp64_st["cycles"], budget_s=8.0, threads=1)
+        line["cpu_baseline"]["cycles_per_solve"] = cpu["cycles_per_solve"]
+        # the same on one host core (the oracle's OpenMP loops with one thread): one solve
+        cpu1 = run_cpu_reference(problem, steps=1, threads=1)
         line["cpu_baseline_1core"] = {k: cpu1[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if rank == 0:
         print(json.dumps(line))
@@ -578,27 +609,16 @@ def run_learned(local, npairs):
 def run_config5(local, net, steps, cpu=True):
     """Config 5: the full-size timestep field solve (Poisson + 3 Helmholtz per step,
     learned warm start + mixed precision) on the 8-12M-leaf tree, beside the plain FP64
-    GPU solves of sampled steps and, on rank 0, the oracle's FP64 V-cycle time on the
-    host cores (a bounded sample of 2 V-cycles scaled by the FP64 cycle count)."""
+    GPU solves of sampled steps and, on rank 0, one complete oracle FP64 Poisson solve of
+    the same tree on the host cores (from a zero guess to 1e-8)."""
     from srmg import timestep
     out, problem = timestep.run(net, steps=steps, device=local)
     if cpu:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle as orc_mod
-        orc = orc_mod.Oracle(problem, threads=os.cpu_count())
-        u = np.zeros_like(problem.b)
-        b = problem.b.copy()
-        r, u1 = np.zeros_like(u), np.zeros_like(u)
-        orc.vcycle(u, b, r, u1, ndown=2, ntop=4, nup=2)
-        t0 = time.perf_counter()
-        for _ in range(2):
-            orc.vcycle(u, b, r, u1, ndown=2, ntop=4, nup=2)
-        spv = (time.perf_counter() - t0) / 2
-        cyc = out["fp64_gpu"]["poisson_cycles"]
-        out["cpu_baseline"] = {"value": 1.0 / (spv * cyc), "unit": "Poisson solves/s", "cores": os.cpu_count(),
-                               "kind": "port", "s_per_vcycle": spv,
-                               "sample": f"2 oracle FP64 V-cycles on this tree, scaled by the {cyc:.0f} cycles of "
-                                         "the FP64 Poisson solve from the previous potential"}
+        _, c, rel, dt = oracle_solve(problem, TOL)
+        out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "Poisson solves/s", "cores": os.cpu_count(),
+                               "kind": "port", "cycles": c, "rel_residual": rel, "s_per_solve": dt,
+                               "sample": f"one complete oracle FP64 Poisson solve of this tree from a zero guess "
+                                         f"to {TOL:g} ({c} V-cycles, {dt:.1f} s)"}
     return out
 
 
@@ -764,27 +784,6 @@ def cnn_only(args):
         out[name] = {"ms_per_forward": ms, "tflops": 2 * out["macs_per_sample"] * args.samples / (ms / 1e3) / 1e12,
                      "finite": bool(torch.isfinite(y).all()), "timing": "wall clock around synchronous calls"}
     print(json.dumps(out))
-
-
-def fp64_cycle_count_estimate(problem):
-    """Cycle count of the reference FP64 solve: the oracle's V-cycle contraction over a
-    bounded number of cycles, extrapolated geometrically to the tolerance."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as orc_mod
-    orc = orc_mod.Oracle(problem, threads=os.cpu_count())
-    u = np.zeros_like(problem.b)
-    b = problem.b.copy()
-    r, u1 = np.zeros_like(u), np.zeros_like(u)
-    bn = orc.leafnorm(b)
-    hist = [orc.resnorm(r, b, u) / bn]
-    for _ in range(12):
-        orc.vcycle(u, b, r, u1, ndown=2, ntop=4, nup=2)
-        hist.append(orc.resnorm(r, b, u) / bn)
-        if hist[-1] <= TOL:
-            return {"cycles": len(hist) - 1, "extrapolated": False}
-    rho = (hist[-1] / hist[-5]) ** 0.25
-    extra = int(np.ceil(np.log(TOL / hist[-1]) / np.log(rho)))
-    return {"cycles": len(hist) - 1 + extra, "extrapolated": True, "rho": rho}
 
 
 if __name__ == "__main__":

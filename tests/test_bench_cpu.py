@@ -25,6 +25,10 @@ def test_reference_arm_json_line():
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == line["value"] and cb["sample"]
     e2e = line["e2e"]
     assert e2e["value"] == line["value"] and e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+    # every step is a complete solve to the tolerance: measured, not extrapolated
+    cyc = line["fp64_cycles_per_solve"]
+    assert cyc["extrapolated"] is False and cyc["cycles"] > 0 and cyc["rel_residual"] <= 1e-8
+    assert abs(line["ms_per_step"] - 1e3 / line["value"]) <= 1e-6 * line["ms_per_step"]
 
 
 def test_byte_model_figures():
