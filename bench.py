@@ -375,10 +375,14 @@ def main():
     mixed_ms, mixed_st, launches = timed(mg.MODE_MIXED, args.steps, args.warmup, clk)
     fp64_steps = max(1, args.fp64_steps)
     fp64_ms, fp64_st, _ = timed(mg.MODE_FP64, fp64_steps, 1)
+    # FP64 V-cycles with the mixed mode's direct coarsest solve: the precision effect alone
+    fpd_ms, fpd_st, _ = timed(mg.MODE_FP64_DIRECT, args.steps, 1)
     mixed_ms = max_over_ranks(mixed_ms, pg, dev)
     fp64_ms = max_over_ranks(fp64_ms, pg, dev)
+    fpd_ms = max_over_ranks(fpd_ms, pg, dev)
     value = world * args.steps / (mixed_ms / 1e3)
     fp64_value = world * fp64_steps / (fp64_ms / 1e3)
+    fpd_value = world * args.steps / (fpd_ms / 1e3)
 
     # error of each result on the leaf cells against the FP64 oracle's solution of the
     # same problem to 1e-11 (the oracle's complete solve on the host cores, rank 0); with
@@ -450,7 +454,11 @@ def main():
                      "ms_per_solve": fp64_ms / fp64_steps, "rel_residual": fp64_st["rel_residual"]},
             "mixed": {"cycles_per_solve": mixed_st["cycles"], "outer_steps": mixed_st["outer"],
                       "rel_residual": mixed_st["rel_residual"]},
+            "fp64_direct_coarse": {"value": fpd_value, "unit": "solves/s", "cycles_per_solve": fpd_st["cycles"],
+                                   "ms_per_solve": fpd_ms / args.steps, "rel_residual": fpd_st["rel_residual"],
+                                   "what": "FP64 V-cycles with the mixed mode's direct FP64 coarsest solve"},
             "speedup_vs_fp64": value / fp64_value,
+            "speedup_split": {"coarse_solve": fpd_value / fp64_value, "precision": value / fpd_value},
             "roofline": {"bound": "hbm", "achieved": achieved_mx, "peak": hbm, "unit": "GB/s",
                          "frac": achieved_mx / hbm,
                          "traffic": TRAFFIC_MIXED_CONFIG2 if nleaf == 1503232 else None,
@@ -471,6 +479,8 @@ def main():
     line["cells_vcycles_per_s"] = {
         "leaf": nleaf * mixed_st["cycles"] * value, "all_levels": all_cells * mixed_st["cycles"] * value,
         "fp64_leaf": nleaf * fp64_st["cycles"] * fp64_value, "note": "cells x V-cycles per second"}
+    line["config1"] = run_config1(local, args.steps, args.warmup, cpu=(rank == 0 and not args.no_cpu))
+    line["dropin_vcycle"] = run_dropin(ctx, problem, args.steps, args.warmup, stream)
     if not args.no_batch:
         line["batch"] = run_batch(local, stream, min(args.steps, 3), rank, world, pg, dev)
     if not args.no_learned:
@@ -493,6 +503,90 @@ def main():
     ctx.close()
     if pg is not None:
         pg.destroy_process_group()
+
+
+def run_dropin(ctx, problem, steps, warm, stream):
+    """The drop-in call as run_from_input makes it: derivs! runs poisson_iter = 2
+    vcycle! per stage (src/streamer.jl:322-334) on Julia-owned, pageable host arrays,
+    which the shim hands to srmg_vcycle.  Wall time per call (H2D of u and b, 2 V-cycles,
+    D2H of u), from pageable numpy arrays: with b copied back (the reference's in/out
+    b), without it (the default), and with the arrays page-locked by srmg_host_register;
+    beside it the device time of the same 2 V-cycles."""
+    from srmg import multigrid as mg
+    p = problem
+    u0 = np.zeros_like(p.b)
+    out = {"workload": "config2 tree, srmg_vcycle x 2 V-cycles (poisson_iter = 2) on pageable host arrays",
+           "bytes_per_call": {"h2d": 2 * p.b.nbytes, "d2h_u": p.b.nbytes}}
+    cases = (("pageable_b_copied_back", 1, False), ("pageable", 0, False), ("registered", 0, True))
+    for name, copy_back, register in cases:
+        ctx.set_option("b_copy_back", copy_back)
+        u, b = u0.copy(), p.b.copy()
+        r, u1 = np.zeros_like(u), np.zeros_like(u)
+        if register:
+            for a in (u, b):
+                ctx.check(mg.lib().srmg_host_register(ctx.handle, a.ctypes.data, a.nbytes))
+        ts = []
+        for i in range(warm + steps):
+            t0 = time.perf_counter()
+            mg.vcycle_(ctx, u, b, r, u1, p.s, p.geom, p.bc, ndown=2, ntop=4, nup=2, ncycles=2)
+            if i >= warm:
+                ts.append(time.perf_counter() - t0)
+        if register:
+            for a in (u, b):
+                ctx.check(mg.lib().srmg_host_unregister(ctx.handle, a.ctypes.data))
+        out[name] = {"ms_per_call": 1e3 * float(np.mean(ts)), "ms_min": 1e3 * float(np.min(ts))}
+    ctx.set_option("b_copy_back", 0)
+    import torch
+    bg = torch.from_numpy(p.b).cuda()
+    ug = torch.zeros_like(bg)
+    rg, u1g = torch.zeros_like(bg), torch.zeros_like(bg)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    cur = torch.cuda.current_stream()
+    ctx.set_stream(cur.cuda_stream)
+    mg.vcycle_(ctx, ug, bg, rg, u1g, p.s, p.geom, p.bc, ndown=2, ntop=4, nup=2, ncycles=2)
+    ev0.record(cur)
+    for _ in range(steps):
+        mg.vcycle_(ctx, ug, bg, rg, u1g, p.s, p.geom, p.bc, ndown=2, ntop=4, nup=2, ncycles=2)
+    ev1.record(cur)
+    ev1.synchronize()
+    out["device_ms_per_call"] = ev0.elapsed_time(ev1) / steps
+    ctx.set_stream(stream.cuda_stream)
+    return out
+
+
+def run_config1(local, steps, warm, cpu=True):
+    """Config 1: the uniform level-5 tree (256 x 256 cells, 341 blocks), FP64 Poisson
+    solve from a zero guess to 1e-10 (the reference's own CPU-runnable case), through
+    the persistent engine in plain FP64, FP64 with the direct coarsest solve, and mixed
+    precision; event-timed per solve on the context's stream; beside it one complete
+    oracle solve on the host cores."""
+    import torch
+    from srmg import gen, multigrid as mg
+    p = gen.config1()
+    tol = 1e-10
+    ctx = mg.Context(local).set_tree(p.tree, p.conn)
+    b = torch.from_numpy(p.b).cuda(local)
+    u = torch.zeros_like(b)
+    out = {"workload": "config1: uniform level-5 tree (256 x 256 cells, 341 blocks), Poisson, cylindrical r-z, "
+                       "tol 1e-10", "blocks": p.tree.nblocks(), "tol": tol}
+    for mode, name in ((mg.MODE_FP64, "fp64"), (mg.MODE_FP64_DIRECT, "fp64_direct_coarse"), (mg.MODE_MIXED, "mixed")):
+        ms, st = [], None
+        for i in range(warm + steps):
+            u.zero_()
+            torch.cuda.synchronize()
+            st = mg.solve(ctx, u, b, p.s, p.geom, p.bc, tol=tol, mode=mode, max_cycles=5000)
+            if i >= warm:
+                ms.append(st["device_ms"])
+        out[name] = {"value": 1e3 / float(np.mean(ms)), "unit": "solves/s", "ms_per_solve": float(np.mean(ms)),
+                     "cycles": st["cycles"], "rel_residual": st["rel_residual"]}
+    if cpu:
+        _, c, rel, dt = oracle_solve(p, tol)
+        out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+                               "cycles": c, "rel_residual": rel,
+                               "sample": f"one complete oracle FP64 solve from a zero guess to {tol:g} ({c} V-cycles)"}
+    ctx.close()
+    return out
 
 
 def run_batch(local, stream, steps, rank=0, world=1, pg=None, dev=None):

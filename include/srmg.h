@@ -133,18 +133,36 @@ int srmg_set_tree3(srmg_ctx *ctx, int nlev,
 /* ---- the ccall boundary: HOST pointers (Julia-owned arrays) --------------------- */
 
 /* `ncycles` x vcycle! (src/multigrid.jl:60-106) on host arrays of nblk_alloc blocks.
- * u and b are in/out exactly as in the reference (b's non-leaf blocks receive the FAS
- * right-hand side); r and u1 are scratch and are not written back.  Blocks until u
- * and b are back in host memory.  bc is the 3x3 Int8 table of
+ * u is in/out exactly as in the reference, ghosts included.  b: its leaf cells are
+ * never written; the reference leaves the FAS right-hand side in the covered cells of
+ * the coarse levels, which none of its callers reads (derivs! re-restricts q before
+ * every solve, src/streamer.jl:313-318, and vcycle! overwrites those cells before it
+ * reads them), so by default b is not copied back and its covered cells keep the
+ * caller's values (option "b_copy_back" 1 copies the FAS values back as the reference
+ * leaves them).  r and u1 are scratch and are not written back.  Blocks until u is
+ * back in host memory.  Host ranges registered with srmg_host_register are copied by
+ * DMA at full bandwidth.  bc is the 3x3 Int8 table of
  * GeneralHomogeneousBoundaryConditions, column-major (src/boundary.jl:28-38). */
 int srmg_vcycle(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, int64_t nblk_alloc,
                 double s, int op, double k2, int geom, const int8_t bc[9],
                 int lmax, int ndown, int ntop, int nup, double omega, int ncycles);
 
-/* fmg! (src/multigrid.jl:17-51) on host arrays; u and b in/out, r and u1 scratch. */
+/* fmg! (src/multigrid.jl:17-51) on host arrays; u in/out, b as in srmg_vcycle, r and
+ * u1 scratch. */
 int srmg_fmg(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, int64_t nblk_alloc,
              double s, int op, double k2, int geom, const int8_t bc[9],
              int ndown, int ntop, int nup, double omega);
+
+/* Page-lock a host range of the caller (cudaHostRegister) so that the host-array entry
+ * points copy it by DMA at full bandwidth instead of staging it through the driver's
+ * pageable-copy buffer.  Meant for the Julia-owned field storage (the ElasticArray
+ * data of a ScalarBlockField, src/blockfield.jl:33-40) that srmg_vcycle / srmg_fmg
+ * receive on every call.  The range stays registered until srmg_host_unregister or
+ * srmg_destroy; the caller must not free it before (when newblock! resizes a field,
+ * src/blockfield.jl:255-260, unregister the old pointer).  Registering the same
+ * (ptr, bytes) twice is a no-op. */
+int srmg_host_register(srmg_ctx *ctx, void *ptr, int64_t bytes);
+int srmg_host_unregister(srmg_ctx *ctx, void *ptr);
 
 /* resnorm! (src/multigrid.jl:391-417): *out = sqrt(sum over leaf cells of r^2 scaled
  * by 4^-(l-1)), with r = -(b + L u / s_l) on every level.  r is scratch. */
@@ -162,11 +180,18 @@ int srmg_fill_ghost(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level, con
  *                         vcycle! algorithm), residual checked after each cycle;
  *   mode SRMG_MODE_MIXED: FP64 defect correction around FP32 V-cycles (smoothing,
  *                         restriction, prolongation in FP32), FP64 residual, FP64
- *                         coarsest-level direct solve and FP64 norms.
+ *                         coarsest-level direct solve and FP64 norms;
+ *   mode SRMG_MODE_FP64_DIRECT: the FP64 V-cycles of SRMG_MODE_FP64 with the
+ *                         coarsest level solved directly by the same FP64 inverse as
+ *                         the mixed mode, in place of the ntop sweeps (not the
+ *                         reference's algorithm: it separates the effect of the
+ *                         precision from that of the coarse solve; order 2, 2D, the
+ *                         persistent engine only).
  * u holds the initial guess on entry (ghosts filled) and the solution on exit
- * (ghosts filled); b is read-only in both modes. */
+ * (ghosts filled); b is read-only in every mode. */
 #define SRMG_MODE_FP64  0
 #define SRMG_MODE_MIXED 1
+#define SRMG_MODE_FP64_DIRECT 2
 typedef struct {
     double tol;          /* relative residual target, e.g. 1e-8 */
     int max_cycles;      /* cap on V-cycles (FP64) or outer steps (mixed) */
@@ -214,7 +239,10 @@ int srmg_solve_dev(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc
 
 /* Single reference routines on device fields (used for per-operation parity). */
 /* fill_ghost! parts (src/connectivity.jl:155-159): mask bit 0 = fill_ghost_copy!,
- * bit 1 = fill_ghost_bnd!, bit 2 = fill_ghost_interp!; 7 = fill_ghost!. */
+ * bit 1 = fill_ghost_bnd!, bit 2 = fill_ghost_interp!; 7 = fill_ghost!.  Bit 3 with bit
+ * 2 makes the refinement ghosts InterpCopy ones (src/interp.jl:66-85: each coarse
+ * cell's value copied into the 2 x 2 fine ghosts it covers), as derivs! fills the
+ * electron density (src/streamer.jl:343); StarStencil trees only. */
 int srmg_fill_ghost_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc, int level,
                         const int8_t bc[9], int mask);
 /* gauss_seidel_level!(..., RedBlack{parity}) (src/multigrid.jl:238-243); for
@@ -445,18 +473,51 @@ int srmg_cnn_predict_dev(srmg_ctx *ctx, srmg_cnn *net, double *u, const double *
                          int64_t nblk_alloc, double s, int op, double k2, int geom,
                          const int8_t bc[9], int *which, double *resid);
 
-/* ---- streamer stepper for training data (no single reference counterpart) -------
- * One forward-Euler step of electron, positive-ion and negative-ion densities on the
- * leaf-holding blocks: electrons drift in E = -grad phi + E0 z^ and diffuse, with
- * Koren-limited upwind face values (src/fluid.jl:8-94); ionisation
- * alpha = alpha_A exp(-alpha_B / |E|) and attachment eta feed the immobile ions
- * (src/chemistry.jl:29-82 drifts electrons only).  ne and phi need their ghosts.
- * dt = min(dt_max, cfl h/max|v|, cfl h^2/(4 D), cfl eps0/(e mu max ne)) -> *dt_out.
- * work: DEVICE scratch of 3 * nblk_alloc * 400 + 2 doubles. */
-int srmg_streamer_step_dev(srmg_ctx *ctx, double *ne, double *npos, double *nneg, const double *phi,
-                           int64_t nblk_alloc, double h1, double E0, double mu, double D,
-                           double alpha_A, double alpha_B, double eta, double cfl, double dt_max,
-                           double *work, double *dt_out);
+/* ---- streamer transport for training data (derivs! and step!, src/streamer.jl) ----
+ * The electron transport and chemistry inside derivs! (src/streamer.jl:292-366) with
+ * the reference's default models, NetIonization (src/chemistry.jl:29-82, species
+ * electrons and net positive ions, charges -1 and +1) over the MinimalTransportModel
+ * (src/transport.jl:9-35) and a uniform gas density; no photoionization (the default
+ * empty model).  The caller composes a stage as derivs! does: netcharge, restrict_full,
+ * the Poisson solve, restrict_full(ne), ghost fills of ne (copy, fill_ghost_bnd! with the
+ * fluid table, InterpCopy refinement ghosts: srmg_fill_ghost_dev mask 1|2|4|8) and of u,
+ * srmg_electric_field_dev, fill_ghost!(eabs, ExtrapolateConst) (a table of +1 signs),
+ * then srmg_streamer_flux_dev and srmg_streamer_rates_dev. */
+typedef struct srmg_transport {
+  double mu;   /* mobility (m^2 / V s) */
+  double D;    /* diffusion coefficient (m^2 / s) */
+  double ai;   /* ionisation: townsend = ai exp(-Ei / |E|) (1/m, V/m) */
+  double Ei;
+  double aa;   /* attachment = aa exp(-Ea / |E|) (1/m, V/m) */
+  double Ea;
+} srmg_transport;
+
+/* flux!(tree, FluxSchemeKoren(), flux, ne, e, eabs, h, trans, dens, maxdt)
+ * (src/fluid.jl:44-94) followed by restrict_flux!(flux, conn)
+ * (src/connectivity.jl:327-360).  flux and e are VectorBlockField{2,16,2} (882
+ * doubles per block, as srmg_electric_field_dev writes e); every face of every leaf
+ * block is written, then each coarse face at a refinement boundary becomes the mean of
+ * the two fine faces.  ne needs 2 ghost layers, eabs 1.  maxdt_blk (DEVICE, nblk_alloc
+ * doubles, may be NULL) receives each leaf block's min(h/|v|, h^2/D/4, Maxwell time)
+ * over its faces; maxdt_min (DEVICE, 1 double, may be NULL) their minimum over the leaf
+ * blocks.  Fluxes and time steps are bit-exact against IEEE double arithmetic. */
+int srmg_streamer_flux_dev(srmg_ctx *ctx, double *flux, double *maxdt_blk, double *maxdt_min,
+                           const double *ne, const double *e, const double *eabs, int64_t nblk_alloc,
+                           double h, const srmg_transport *tr);
+/* chemderivs! (pre, init; post, add; src/chemistry.jl:29-82) and
+ * fluxderivs!(tree, dne, flux, h, geom) (src/fluid.jl:8-30) on the valid cells of every
+ * leaf block: dni = ionisation + attachment rate, dne = the same plus the flux
+ * divergence with the geometry factors of src/geometry.jl:27-29 (geom as in
+ * srmg_vcycle). */
+int srmg_streamer_rates_dev(srmg_ctx *ctx, double *dne, double *dni, const double *ne, const double *eabs,
+                            const double *flux, int64_t nblk_alloc, double h, int geom,
+                            const srmg_transport *tr);
+/* The SSPRK3 combinations of step! (src/streamer.jl:400-413), elementwise over `count`
+ * doubles: stage 1 out = n + dn1 dt; stage 2 out = n + (dn1 dt/4 + dn2 dt/4); stage 3
+ * out = n + ((dn1 dt/6 + dn2 dt/6) + dn3 (2 dt)/3).  Bit-exact (no fused
+ * multiply-add).  out may alias n. */
+int srmg_ssprk3_stage_dev(srmg_ctx *ctx, double *out, const double *n, const double *dn1, const double *dn2,
+                          const double *dn3, int64_t count, double dt, int stage);
 
 /* Tuning knobs (no reference counterpart; the autotuner drives them):
  *   "engine"           1 = persistent one-launch V-cycle (default), 0 = one kernel per
@@ -475,6 +536,9 @@ int srmg_streamer_step_dev(srmg_ctx *ctx, double *ne, double *npos, double *nneg
  *                      (fields, operator, sweep counts, tree, stream) into a CUDA graph
  *                      and replayed (bit-identical results; up to 8 graphs kept, all
  *                      dropped when the tree changes); 0 = launch kernel by kernel;
+ *   "b_copy_back"      1 = srmg_vcycle / srmg_fmg copy b back to the host (the FAS
+ *                      values in its covered cells, as the reference leaves them);
+ *                      0 (default) = b is not copied back;
  *   "cnn_active_ppm"   the learned warm start runs the network only on blocks whose
  *                      share of (b_n - 2 b_{n-1} + b_{n-2})^2 is at least this many
  *                      millionths of the largest block's (default 0 = every

@@ -124,7 +124,42 @@ extern "C" void srmg_destroy(srmg_ctx *ctx) {
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  for (auto &r : ctx->host_reg) cudaHostUnregister(r.first);
   delete ctx;
+}
+
+// Page-lock a caller's host range so that the host-array entry points copy it by DMA
+// at full bandwidth (a pageable range is staged through a driver buffer).  The range
+// stays registered until srmg_host_unregister or srmg_destroy; the caller must not free
+// it before.
+extern "C" int srmg_host_register(srmg_ctx *ctx, void *ptr, int64_t bytes) {
+  if (!ctx) return SRMG_ERR_BADARG;
+  if (!ptr || bytes <= 0) return fail(ctx, SRMG_ERR_BADARG, "srmg_host_register: null range");
+  for (auto &r : ctx->host_reg)
+    if (r.first == ptr) {
+      if (r.second == (size_t)bytes) return SRMG_OK;
+      return fail(ctx, SRMG_ERR_BADARG, "srmg_host_register: %p already registered with another size", ptr);
+    }
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterDefault));
+  ctx->host_reg.emplace_back(ptr, (size_t)bytes);
+  return SRMG_OK;
+}
+
+extern "C" int srmg_host_unregister(srmg_ctx *ctx, void *ptr) {
+  if (!ctx) return SRMG_ERR_BADARG;
+  for (size_t k = 0; k < ctx->host_reg.size(); k++)
+    if (ctx->host_reg[k].first == ptr) {
+      CK(cudaSetDevice(ctx->device));
+      const cudaError_t e = cudaHostUnregister(ptr);
+      ctx->host_reg.erase(ctx->host_reg.begin() + k);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, SRMG_ERR_CUDA, "srmg_host_unregister: %s", cudaGetErrorString(e));
+      }
+      return SRMG_OK;
+    }
+  return fail(ctx, SRMG_ERR_BADARG, "srmg_host_unregister: %p was not registered", ptr);
 }
 
 extern "C" const char *srmg_last_error(const srmg_ctx *ctx) {
@@ -910,6 +945,8 @@ extern "C" int srmg_set_option(srmg_ctx *ctx, const char *key, int64_t value) {
   if (!ctx || !key) return SRMG_ERR_BADARG;
   if (!strcmp(key, "engine")) ctx->use_engine = value != 0;
   else if (!strcmp(key, "trace")) ctx->trace_on = value != 0;
+  else if (!strcmp(key, "b_copy_back")) ctx->b_copy_back = value != 0;
+  else if (!strcmp(key, "freebc_direct")) ctx->fbc_direct = value != 0;
   else if (!strcmp(key, "graph")) ctx->use_graph = value != 0;
   else if (!strcmp(key, "op_graphs")) {
     ctx->use_op_graphs = value != 0;
@@ -1068,6 +1105,12 @@ extern "C" int srmg_fill_ghost_dev(srmg_ctx *ctx, double *u, int64_t nblk_alloc,
                                    const int8_t bc[9], int mask) {
   RC(check_call_any(ctx, nblk_alloc, 0, 0, bc));
   if (!u || level < 1 || level > ctx->nlev) return fail(ctx, SRMG_ERR_BADARG, "fill_ghost: bad level");
+  if (mask & 8) {
+    // InterpCopy refinement ghosts: one launch over the star faces only
+    if (ctx->D == 3 || ctx->has_corners)
+      return fail(ctx, SRMG_ERR_UNSUPPORTED, "fill_ghost: InterpCopy ghosts (mask bit 3) on 2D StarStencil trees only");
+    if (!(mask & 4)) return fail(ctx, SRMG_ERR_BADARG, "fill_ghost: mask bit 3 needs bit 2");
+  }
   if (ctx->D == 3) RC(d3_fill_ghost(ctx, u, level, bc, mask));
   else RC(L_fill_ghost<double>(ctx, u, level, make_signs(bc), mask));
   CK(cudaGetLastError());
@@ -1210,7 +1253,7 @@ extern "C" int srmg_vcycle(srmg_ctx *ctx, double *u, double *b, double *r, doubl
   RC(srmg_vcycle_dev(ctx, du, db, dr, du1, nblk_alloc, s, op, k2, geom, bc, lmax, ndown, ntop, nup,
                      omega, ncycles));
   RC(stage_out(ctx, u, du, nblk_alloc));
-  RC(stage_out(ctx, b, db, nblk_alloc));
+  if (ctx->b_copy_back) RC(stage_out(ctx, b, db, nblk_alloc));
   CK(cudaStreamSynchronize(ctx->stream));
   return engine_check(ctx);
 }
@@ -1229,7 +1272,7 @@ extern "C" int srmg_fmg(srmg_ctx *ctx, double *u, double *b, double *r, double *
   RC(stage_in(ctx, 3, nullptr, nblk_alloc, &du1));
   RC(srmg_fmg_dev(ctx, du, db, dr, du1, nblk_alloc, s, op, k2, geom, bc, ndown, ntop, nup, omega));
   RC(stage_out(ctx, u, du, nblk_alloc));
-  RC(stage_out(ctx, b, db, nblk_alloc));
+  if (ctx->b_copy_back) RC(stage_out(ctx, b, db, nblk_alloc));
   CK(cudaStreamSynchronize(ctx->stream));
   return engine_check(ctx);
 }

@@ -162,7 +162,7 @@ static int opts_of(srmg_ctx *ctx, const srmg_solve_opts *opts, srmg_solve_opts *
   if (opts) *o = *opts; else srmg_solve_opts_default(o);
   if (!(o->tol > 0) || o->max_cycles < 0 || o->ndown < 0 || o->nup < 0 || o->ntop < 0)
     return fail(ctx, SRMG_ERR_BADARG, "srmg_batch_solve: bad options");
-  if (o->mode != SRMG_MODE_FP64 && o->mode != SRMG_MODE_MIXED)
+  if (o->mode != SRMG_MODE_FP64 && o->mode != SRMG_MODE_MIXED && o->mode != SRMG_MODE_FP64_DIRECT)
     return fail(ctx, SRMG_ERR_BADARG, "unknown solve mode %d", o->mode);
   return SRMG_OK;
 }
@@ -258,7 +258,7 @@ static int batch_solve(srmg_ctx *ctx, double *const *u, const double *const *b, 
   // CUDA graph: gathers, the persistent solve, the result copy and the scatters are
   // captured once per key and replayed.
   ItemTabs tabs;
-  RC(prepare_items(ctx, ctx->batch_items.data(), ctx->geom_forest, o.omega, o.mode == SRMG_MODE_MIXED, 0, 0.0,
+  RC(prepare_items(ctx, ctx->batch_items.data(), ctx->geom_forest, o.omega, o.mode != SRMG_MODE_FP64, 0, 0.0,
                    &tabs));
   RC(solve_reserve(ctx, ctx->max_blk, o.mode));
   RC(items_host_reserve(ctx));

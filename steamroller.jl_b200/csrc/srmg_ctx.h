@@ -170,6 +170,13 @@ struct srmg_ctx {
   int64_t fbc_n = 0;
   int fbc_dim = 0, fbc_level = 0;
   int64_t fbc_root[2] = {1, 1};
+  bool fbc_direct = false;  // option "freebc_direct": direct-sum transforms even for power-of-two n
+
+  // host-array entry points: b copied back to the host (off by default: leaf cells of b
+  // are never written, and non-leaf b is unspecified after a V-cycle), and the host
+  // ranges page-locked through srmg_host_register {address, bytes}
+  bool b_copy_back = false;
+  std::vector<std::pair<void *, size_t>> host_reg;
 
   // coarsest-level direct inverses, by operator and level-1 structure
   std::map<std::vector<double>, srmg::DevBuf> coarse_cache;

@@ -11,11 +11,19 @@
 // with FFTW's unnormalised RODFT10 (DST-II) and RODFT01 (DST-III):
 //   DST-II:  Y_k = 2 sum_{j=0}^{n-1} X_j sin(pi (2j+1)(k+1) / (2n))
 //   DST-III: Y_k = (-1)^k X_{n-1} + 2 sum_{j=0}^{n-2} X_j sin(pi (j+1)(2k+1) / (2n)).
-// n is at most a few ten thousand, so both run as direct sums, one CTA per output in a
-// fixed order, with the sine of every argument from a table of sin(pi t / (2n)),
-// t = 0..4n-1 (the integer argument reduced exactly modulo 4n).  f, the transform's
-// kernel (modified Bessel functions of the domain's aspect), is computed by the caller
-// as FreeBC does and handed over once (srmg_freebc_set).
+// When n is a power of two (n = 16 2^(level-1) rootsize: rootsize a power of two along
+// the other dimension, the usual (1, 1) root included) both transforms go through one
+// complex FFT of length n each, O(n log n): DST-II(x)[k] = DCT-II(x')[n-1-k] with
+// x'_j = (-1)^j x_j, and DCT-II through Makhoul's reordering v = (x_0, x_2, ..., x_3,
+// x_1) and C_k = 2 Re(e^{-i pi k / 2n} V_k); DST-III(X)[k] = (-1)^k DCT-III(X'')[k] with
+// X''_j = X_{n-1-j}, and DCT-III through the inverse reordering of an unnormalised
+// inverse FFT of W^{-k} (X''_k - i X''_{n-k}).  The FFT is radix-2 in shared memory for
+// n <= 8192 and a four-step n = n1 n2 split (n2 column FFTs with twiddles, then n1 row
+// FFTs) above, twiddles from a table of e^{-2 pi i k / n}.  Other n run as direct
+// sums, one CTA per output in a fixed order, with the sine of every argument from a
+// table of sin(pi t / (2n)), t = 0..4n-1 (the integer argument reduced exactly modulo
+// 4n).  f, the transform's kernel (modified Bessel functions of the domain's aspect),
+// is computed by the caller as FreeBC does and handed over once (srmg_freebc_set).
 #include <cmath>
 
 #include "srmg_ctx.h"
@@ -73,6 +81,125 @@ __device__ __forceinline__ double block_sum(double v) {
     for (int off = 16; off > 0; off >>= 1) r += __shfl_xor_sync(0xffffffffu, r, off);
   }
   return r;  // valid in thread 0
+}
+
+// ---- FFT path (n a power of two) ----------------------------------------------------
+
+constexpr int kFftMaxLocal = 8192;  // one CTA's shared-memory FFT (128 KB of complex doubles)
+constexpr int kFftThreads = 512;
+
+__global__ void k_twiddles(double2 *tw, int64_t n) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    double sn, cs;
+    sincospi(-2.0 * (double)k / (double)n, &sn, &cs);  // e^{-2 pi i k / n}
+    tw[k] = make_double2(cs, sn);
+  }
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// `count` forward FFTs of length len (a power of two, <= kFftMaxLocal), one per CTA
+// pass: element j of transform t is in[t * in_t + j * in_j]; output k goes to
+// out[t * out_t + k * out_k], multiplied by tw[(t * k * tw_mul) mod n] when tw_mul > 0
+// (the four-step twiddles).  The table tw holds e^{-2 pi i k / n}; a length-len
+// transform uses every (n / len)-th entry.  Iterative radix-2, bit-reversed load.
+__global__ void __launch_bounds__(kFftThreads) k_fft(double2 *__restrict__ out, const double2 *__restrict__ in,
+                                                     const double2 *__restrict__ tw, int64_t n, int len, int logl,
+                                                     int count, int64_t in_t, int64_t in_j, int64_t out_t,
+                                                     int64_t out_k, int64_t tw_mul) {
+  extern __shared__ double2 sbuf[];
+  const int64_t stride_n = n / len;
+  for (int t = blockIdx.x; t < count; t += gridDim.x) {
+    for (int j = threadIdx.x; j < len; j += blockDim.x) {
+      const int r = (int)(__brev((unsigned)j) >> (32 - logl));
+      sbuf[r] = in[t * in_t + j * in_j];
+    }
+    __syncthreads();
+    for (int half = 1; half < len; half <<= 1) {
+      const int64_t tstep = stride_n * (len / (2 * half));
+      for (int idx = threadIdx.x; idx < len / 2; idx += blockDim.x) {
+        const int pos = idx & (half - 1), i = (idx - pos) * 2 + pos;
+        const double2 w = tw[pos * tstep];
+        const double2 a = sbuf[i], b = cmul(sbuf[i + half], w);
+        sbuf[i] = make_double2(a.x + b.x, a.y + b.y);
+        sbuf[i + half] = make_double2(a.x - b.x, a.y - b.y);
+      }
+      __syncthreads();
+    }
+    for (int k = threadIdx.x; k < len; k += blockDim.x) {
+      double2 v = sbuf[k];
+      if (tw_mul > 0) v = cmul(v, tw[((int64_t)t * k * tw_mul) % n]);
+      out[t * out_t + k * out_k] = v;
+    }
+    __syncthreads();
+  }
+}
+
+// The length-n forward FFT of `a` into `b` (a is left modified), one or two launches.
+int fft_forward(srmg_ctx *ctx, double2 *b, double2 *a, double2 *tmp, const double2 *tw, int64_t n) {
+  int logn = 0;
+  while (((int64_t)1 << logn) < n) ++logn;
+  if (n <= kFftMaxLocal) {
+    k_fft<<<1, kFftThreads, n * sizeof(double2), ctx->stream>>>(b, a, tw, n, (int)n, logn, 1, 0, 1, 0, 1, 0);
+    ctx->launches++;
+    return SRMG_OK;
+  }
+  // four-step: j = j1 + n1 j2, k = k2 + n2 k1
+  const int l2 = logn / 2, l1 = logn - l2;
+  const int n1 = 1 << l1, n2 = 1 << l2;
+  // step 1: for every j1, the FFT over j2 (stride n1), times W_n^{j1 k2}, into tmp[j1 + n1 k2]
+  k_fft<<<std::min(n1, 148 * 4), kFftThreads, n2 * sizeof(double2), ctx->stream>>>(tmp, a, tw, n, n2, l2, n1, 1,
+                                                                                  n1, 1, n1, 1);
+  // step 2: for every k2, the FFT over j1 (contiguous), into b[k2 + n2 k1]
+  k_fft<<<std::min(n2, 148 * 4), kFftThreads, n1 * sizeof(double2), ctx->stream>>>(b, tmp, tw, n, n1, l1, n2, n1,
+                                                                                  1, 1, n2, 0);
+  ctx->launches += 2;
+  return SRMG_OK;
+}
+
+// DST-II, step 1: v = Makhoul reordering of x'_j = (-1)^j x_j, as complex values.
+__global__ void k_dst2_pre(double2 *__restrict__ v, const double *__restrict__ x, int64_t n) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n / 2; j += (int64_t)gridDim.x * blockDim.x) {
+    v[j] = make_double2(x[2 * j], 0.0);                   // (-1)^(2j) = 1
+    v[n - 1 - j] = make_double2(-x[2 * j + 1], 0.0);      // (-1)^(2j+1) = -1
+  }
+}
+
+// DST-II, step 2: y[k] = C[n-1-k], C[m] = 2 Re(e^{-i pi m / 2n} V[m]); then the DST-III
+// input X_j = f_j y_j (rounded once) reversed, X''_m = X_{n-1-m}, and
+// V'[m] = e^{+i pi m / 2n} (X''_m - i X''_{n-m}) (X''_n = 0), conjugated for the
+// inverse transform done as a forward FFT.  With y_out the DST-II output is kept.
+__global__ void k_dst_mid(double2 *__restrict__ vp, double *__restrict__ y_out, const double2 *__restrict__ V,
+                          const double *__restrict__ f, int64_t n) {
+  auto C = [&](int64_t m) {  // DCT-II of x' at m
+    double sn, cs;
+    sincospi(-(double)m / (double)(2 * n), &sn, &cs);
+    const double2 z = V[m];
+    return 2.0 * (z.x * cs - z.y * sn);
+  };
+  for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < n; m += (int64_t)gridDim.x * blockDim.x) {
+    // y_k = C[n-1-k]; X''_m = f_{n-1-m} y_{n-1-m} = f_{n-1-m} C[m]
+    const double xm = f[n - 1 - m] * C(m);
+    if (y_out) y_out[n - 1 - m] = C(m);
+    const double xnm = m == 0 ? 0.0 : f[m - 1] * C(n - m);  // X''_{n-m} = f_{m-1} y_{m-1} = f_{m-1} C[n-m]
+    double sn, cs;
+    sincospi((double)m / (double)(2 * n), &sn, &cs);  // e^{+i pi m / 2n}
+    // (cs + i sn)(xm - i xnm) = (cs xm + sn xnm) + i (sn xm - cs xnm); conjugated
+    vp[m] = make_double2(cs * xm + sn * xnm, -(sn * xm - cs * xnm));
+  }
+}
+
+// DST-III, last step: the unnormalised inverse FFT is conj(FFT(conj V')): w = conj of
+// the forward result; y[2j] = Re w[j], y[2j+1] = Re w[n-1-j]; DST-III[k] = (-1)^k y[k];
+// b[k] = DST-III[k] h / 2^(level-1) / 2.
+__global__ void k_dst3_post(double *__restrict__ b, const double2 *__restrict__ w, int64_t n, double h, double p2) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n / 2; j += (int64_t)gridDim.x * blockDim.x) {
+    const double ye = w[j].x, yo = w[n - 1 - j].x;  // Re(conj z) = Re z
+    b[2 * j] = ye * h / p2 / 2.0;                   // (-1)^(2j) = 1
+    b[2 * j + 1] = -yo * h / p2 / 2.0;
+  }
 }
 
 // y = DST-II(x).  The table index (2j + 1)(k + 1) mod 4n advances by a fixed step per
@@ -209,10 +336,16 @@ int gridfor(int64_t work, int threads) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 8));
 }
 
+// The context's free-boundary buffer: f [n], the sine table [4n], u1 [n], b [n], and for
+// the FFT path the twiddles [n complex] and three complex work arrays [n each].
+constexpr int64_t kFbcDoubles = 13;
 double *fbc_f(srmg_ctx *ctx) { return (double *)ctx->fbc.p; }
 double *fbc_tab(srmg_ctx *ctx) { return fbc_f(ctx) + ctx->fbc_n; }
 double *fbc_u1(srmg_ctx *ctx) { return fbc_tab(ctx) + 4 * ctx->fbc_n; }
 double *fbc_b(srmg_ctx *ctx) { return fbc_u1(ctx) + ctx->fbc_n; }
+double2 *fbc_tw(srmg_ctx *ctx) { return (double2 *)(fbc_b(ctx) + ctx->fbc_n); }
+double2 *fbc_work(srmg_ctx *ctx, int k) { return fbc_tw(ctx) + (1 + k) * ctx->fbc_n; }
+bool fbc_pow2(int64_t n) { return n >= 2 && (n & (n - 1)) == 0; }
 
 // Levels the boundary work visits, and the checks freebc! makes.
 int fbc_ready(srmg_ctx *ctx, int64_t nblk_alloc, const char *who) {
@@ -277,7 +410,7 @@ extern "C" int srmg_freebc_set(srmg_ctx *ctx, int dim, int level, const int64_t 
     return fail(ctx, SRMG_ERR_UNSUPPORTED, "srmg_freebc_set: transform length %lld above %lld", (long long)n,
                 (long long)kFreeMaxN);
   cudaSetDevice(ctx->device);
-  RC(ensure(ctx, ctx->fbc, (size_t)7 * n * sizeof(double)));
+  RC(ensure(ctx, ctx->fbc, (size_t)kFbcDoubles * n * sizeof(double)));
   ctx->fbc_n = n;
   ctx->fbc_dim = dim;
   ctx->fbc_level = level;
@@ -286,6 +419,13 @@ extern "C" int srmg_freebc_set(srmg_ctx *ctx, int dim, int level, const int64_t 
   CK(cudaMemcpyAsync(fbc_f(ctx), f, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   k_sin_table<<<gridfor(4 * n, 256), 256, 0, ctx->stream>>>(fbc_tab(ctx), n);
   ctx->launches++;
+  if (fbc_pow2(n)) {
+    // the FFT kernel holds up to kFftMaxLocal complex doubles in dynamic shared memory
+    CK(cudaFuncSetAttribute(k_fft, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)(kFftMaxLocal * sizeof(double2))));
+    k_twiddles<<<gridfor(n, 256), 256, 0, ctx->stream>>>(fbc_tw(ctx), n);
+    ctx->launches++;
+  }
   CK(cudaMemsetAsync(fbc_b(ctx), 0, n * sizeof(double), ctx->stream));
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
@@ -312,13 +452,23 @@ extern "C" int srmg_freebc_dev(srmg_ctx *ctx, double *q, const double *u, int64_
                                                                        extent(ctx, l, dim), 1 << (level - l), hl);
     ctx->launches++;
   }
-  const int g = (int)std::min<int64_t>(n, 148 * 16);
-  k_dst2<<<g, kDstThreads, 0, ctx->stream>>>(am, u1, fbc_tab(ctx), n);
-  // DST-III reads am and writes b: keep them apart (u1 is free again)
-  CK(cudaMemcpyAsync(u1, am, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-  k_dst3_scale<<<g, kDstThreads, 0, ctx->stream>>>(b, u1, fbc_f(ctx), fbc_tab(ctx), n, h,
-                                                   (double)((int64_t)1 << (level - 1)));
-  ctx->launches += 2;
+  const double p2 = (double)((int64_t)1 << (level - 1));
+  if (fbc_pow2(n) && !ctx->fbc_direct) {
+    double2 *w0 = fbc_work(ctx, 0), *w1 = fbc_work(ctx, 1), *w2 = fbc_work(ctx, 2);
+    k_dst2_pre<<<gridfor(n / 2, 256), 256, 0, ctx->stream>>>(w0, u1, n);
+    RC(fft_forward(ctx, w1, w0, w2, fbc_tw(ctx), n));
+    k_dst_mid<<<gridfor(n, 256), 256, 0, ctx->stream>>>(w0, nullptr, w1, fbc_f(ctx), n);
+    RC(fft_forward(ctx, w1, w0, w2, fbc_tw(ctx), n));
+    k_dst3_post<<<gridfor(n / 2, 256), 256, 0, ctx->stream>>>(b, w1, n, h, p2);
+    ctx->launches += 3;
+  } else {
+    const int g = (int)std::min<int64_t>(n, 148 * 16);
+    k_dst2<<<g, kDstThreads, 0, ctx->stream>>>(am, u1, fbc_tab(ctx), n);
+    // DST-III reads am and writes b: keep them apart (u1 is free again)
+    CK(cudaMemcpyAsync(u1, am, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    k_dst3_scale<<<g, kDstThreads, 0, ctx->stream>>>(b, u1, fbc_f(ctx), fbc_tab(ctx), n, h, p2);
+    ctx->launches += 2;
+  }
   const int order_star[4] = {0, 1, 2, 3};                 // StarStencil order (src/stencil.jl:16-32)
   const int order_box[8] = {4, 2, 5, 0, 1, 6, 3, 7};      // BoxStencil order (src/stencil.jl:34-90)
   const int *ord = ctx->has_corners ? order_box : order_star;

@@ -230,6 +230,10 @@ __global__ void k_fill_ghost(T *__restrict__ u, LevelView lv, Signs sg, int mask
         ir = k & 1;
       }
       const int o = jr + kS * jz;
+      if (mask & 8) {  // InterpCopy (src/interp.jl:66-85): the coarse cell's value itself
+        ub[x + kS * y] = cb[o];
+        continue;
+      }
       T v = dmul<T>(T(0.5), cb[o]);
       v = dadd<T>(v, dmul<T>(T(0.25), cb[o + (2 * ir - 1)]));
       v = dadd<T>(v, dmul<T>(T(0.25), cb[o + kS * (2 * iz - 1)]));

@@ -222,7 +222,7 @@ bool srmg::engine_ok(srmg_ctx *ctx, const srmg_solve_opts *o, std::initializer_l
 
 // Work buffers of a solve (allocated before any capture: nothing allocates later).
 int srmg::solve_reserve(srmg_ctx *ctx, int64_t nblk_alloc, int mode) {
-  if (mode == SRMG_MODE_FP64) {
+  if (mode != SRMG_MODE_MIXED) {
     const size_t bytes = (size_t)nblk_alloc * kSS * sizeof(double);
     for (int i : {2, 3, 4}) RC(ensure(ctx, ctx->f64[i], bytes));
   } else {
@@ -240,10 +240,11 @@ int srmg::solve_enqueue(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_
   EngineRun run;
   run.max_cycles = std::max(1, o->max_cycles);
   run.tol = o->tol;
-  if (o->mode == SRMG_MODE_FP64) {
+  if (o->mode != SRMG_MODE_MIXED) {
     const size_t bytes = (size_t)nblk_alloc * kSS * sizeof(double);
     double *bw = (double *)ctx->f64[4].p, *r = (double *)ctx->f64[2].p, *u1 = (double *)ctx->f64[3].p;
     CK(cudaMemcpyAsync(bw, b, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    run.direct = o->mode == SRMG_MODE_FP64_DIRECT;
     return engine_vcycle<double>(ctx, u, bw, u1, r, tabs, geom, 0, o->ndown, o->ntop, o->nup, &run);
   }
   const size_t b32 = (size_t)nblk_alloc * kSS * sizeof(float);
@@ -271,14 +272,20 @@ static int solve_fp64(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_al
                       int geom, const srmg_solve_opts *o, srmg_stats *st) {
   RC(solve_reserve(ctx, nblk_alloc, SRMG_MODE_FP64));
   double *bw = (double *)ctx->f64[4].p, *r = (double *)ctx->f64[2].p, *u1 = (double *)ctx->f64[3].p;
+  const bool direct = o->mode == SRMG_MODE_FP64_DIRECT;
+  if (direct)
+    for (int k = 0; k < ctx->nitems; k++)
+      if (specs[k].op == SRMG_OP_LAPLACIAN4)
+        return fail(ctx, SRMG_ERR_UNSUPPORTED, "the direct coarsest solve supports order-2 discretisations");
   if (engine_ok(ctx, o, {u, b, bw, r, u1})) {
     ItemTabs tabs;
-    RC(prepare_items(ctx, specs, geom, o->omega, false, 0, 0.0, &tabs));
+    RC(prepare_items(ctx, specs, geom, o->omega, direct, 0, 0.0, &tabs));
     RC(solve_enqueue(ctx, u, b, nblk_alloc, tabs, geom, o));
     RC(read_items(ctx));
     items_stats(ctx, o, st);
     return SRMG_OK;
   }
+  if (direct) return fail(ctx, SRMG_ERR_UNSUPPORTED, "SRMG_MODE_FP64_DIRECT needs the persistent engine");
   const size_t bytes = (size_t)nblk_alloc * kSS * sizeof(double);
   CK(cudaMemcpyAsync(bw, b, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
   // per-operation kernels, host loop (one item)
@@ -392,7 +399,7 @@ int srmg::solve_items(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_al
   for (int k = 0; k < ctx->nitems; k++) memset(&st[k], 0, sizeof(srmg_stats));
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   int rc;
-  if (o.mode == SRMG_MODE_FP64) rc = solve_fp64(ctx, u, b, nblk_alloc, specs, geom, &o, st);
+  if (o.mode == SRMG_MODE_FP64 || o.mode == SRMG_MODE_FP64_DIRECT) rc = solve_fp64(ctx, u, b, nblk_alloc, specs, geom, &o, st);
   else if (o.mode == SRMG_MODE_MIXED) rc = solve_mixed(ctx, u, b, nblk_alloc, specs, geom, &o, st);
   else rc = fail(ctx, SRMG_ERR_BADARG, "unknown solve mode %d", o.mode);
   cudaEventRecord(ctx->ev1, ctx->stream);

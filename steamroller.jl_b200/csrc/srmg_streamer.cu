@@ -1,17 +1,29 @@
-// srmg_streamer.cu -- a minimal streamer stepper that produces the solve pairs the
-// learned warm start trains on: electrons drift and diffuse in the field of the
-// solved potential plus a uniform applied field, with Koren-limited upwind fluxes
-// (src/fluid.jl:8-94: flux!, fluxderivs!), and ionisation/attachment feed two immobile
-// ion species (the reference's NetIonization chemistry drifts only electrons,
-// src/chemistry.jl:29-82; here positive and negative ions are both kept).
+// srmg_streamer.cu -- the electron transport and chemistry inside derivs!
+// (src/streamer.jl:292-366) and the SSPRK3 stage combinations of step!
+// (src/streamer.jl:386-425), on the device, for the streamer runs that generate the
+// learned warm start's training pairs:
+//   * flux! with the Koren scheme (src/fluid.jl:44-94): per leaf block and per face of
+//     validindices(e, d), the upwind value n_u + koren_limited(n_u - n_u2, n_d - n_u)
+//     (src/fluid.jl:265-280) times the drift velocity -mu E, plus the diffusion flux, and
+//     the block's largest stable time step (CFL, diffusion, Maxwell relaxation);
+//   * restrict_flux! (src/connectivity.jl:327-360): at every refinement boundary the
+//     coarse block's face flux is the mean of the two fine face fluxes it covers;
+//   * chemderivs! for NetIonization (src/chemistry.jl:29-82) with the MinimalTransportModel
+//     (src/transport.jl:9-35): ionisation before the (empty) photoionization, attachment
+//     after it, for both species (electrons and net positive ions);
+//   * fluxderivs! (src/fluid.jl:8-30): the flux divergence with the geometry factors of
+//     src/geometry.jl:27-29, accumulated face by face in the reference's order;
+//   * the three SSPRK3 combinations n + dn1 dt, n + (dn1 dt/4 + dn2 dt/4),
+//     n + ((dn1 dt/6 + dn2 dt/6) + dn3 2dt/3).
+// Every operation is rounded on its own (no fused multiply-add), as in the reference,
+// so fluxes, time steps and stage combinations are bit-exact against a restatement with
+// IEEE double arithmetic; the chemistry calls exp(), which may differ in the last bit.
 //
-// Geometry: cylindrical (r = dim 1, z = dim 2), cell centres r_i = (i - 1/2) h.  The
-// divergence of a face flux F is (r_{i+1/2} F_{i+1/2} - r_{i-1/2} F_{i-1/2}) / (r_i h)
-// + (F_{j+1/2} - F_{j-1/2}) / h; the axis face has r = 0.  Every block needs its 2-cell
-// ghost halo of n_e and of phi filled (the face at a block edge reads 2 cells on each
-// side).  Rates are computed on the valid cells of every leaf-holding block.
+// The vector fields (e, flux) use the VectorBlockField{2, 16, 2} storage
+// (src/blockfield.jl:84-95): 21 x 21 values per component, component d at offset 441 d,
+// 882 values per block; face (x, y) of component d (0-based local indices) is the face
+// between cell (x, y) - e_d and cell (x, y).
 #include <cmath>
-#include <vector>
 
 #include "srmg_ctx.h"
 #include "srmg_internal.h"
@@ -31,139 +43,241 @@ using namespace srmg;
 
 namespace {
 
-constexpr double kE = 1.6021766208e-19;      // elementary charge (src/constants.jl:55)
-constexpr double kEps0 = 8.854187817620389e-12;  // (src/constants.jl:56)
+constexpr int kSV = kS + 1;
+constexpr int kSSV = kSV * kSV;
+constexpr int kFacesPerDim = (kM + 1) * kM;  // 17 x 16 faces of validindices(e, d)
 
-// Koren limiter psi(r) = max(0, min(2r, (1 + 2r)/3, 2)) on the slope ratio r.
-__device__ __forceinline__ double koren(double r) { return fmax(0.0, fmin(fmin(2.0 * r, (1.0 + 2.0 * r) / 3.0), 2.0)); }
+constexpr double kElemCharge = 1.6021766208e-19;  // src/constants.jl:55
+constexpr double kEpsilon0 = 8.854187817620389e-12;  // src/constants.jl:56
 
-// Face value of n upwind of a face between cells a (left) and b (right), velocity v:
-// second-order reconstruction limited by Koren (n0 = left of a, n3 = right of b).
-__device__ __forceinline__ double face_value(double v, double n0, double na, double nb, double n3) {
-  if (v >= 0.0) {
-    const double d = nb - na;
-    const double r = d != 0.0 ? (na - n0) / d : 0.0;
-    return na + 0.5 * koren(r) * d;
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dvd(double a, double b) { return __ddiv_rn(a, b); }
+
+// koren_limited(a, b) = psi(a / b) b (src/fluid.jl:274-280).
+__device__ __forceinline__ double koren_limited(double a, double b) {
+  if (mul(a, b) < 0.0) return 0.0;
+  if (fabs(a) > fabs(mul(4.0, b))) return b;
+  if (fabs(mul(10.0, a)) > fabs(mul(4.0, b))) return add(dvd(b, 3.0), dvd(a, 6.0));
+  return a;
+}
+
+// Leaf blocks (no child in any subblock: isleaf, src/tree.jl:105-115) among the blocks
+// holding a leaf cell.
+__device__ __forceinline__ bool leaf_block(const int4 *info, int X) { return (info[X].z & 15) == 0; }
+
+// Non-negative doubles order like their bit patterns as unsigned integers.
+__device__ __forceinline__ void atomic_min_nonneg(double *addr, double v) {
+  atomicMin(reinterpret_cast<unsigned long long *>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+// flux! (Koren) on the leaf blocks: one 256-thread CTA per block pass, the 544 faces of
+// the block strided over its threads.  ne needs 2 ghost layers, eabs 1.
+__global__ void k_streamer_flux(double *__restrict__ flux, double *__restrict__ maxdt_blk,
+                                double *__restrict__ maxdt_min, const double *__restrict__ ne,
+                                const double *__restrict__ e, const double *__restrict__ eabs,
+                                const int2 *__restrict__ leaf, int nleaf, const int4 *__restrict__ info,
+                                double h1, srmg_transport tr) {
+  __shared__ double s_min[8];
+  const double maxwell = kEpsilon0 / kElemCharge;  // (co.epsilon_0 / co.elementary_charge)
+  for (int k = blockIdx.x; k < nleaf; k += gridDim.x) {
+    const int X = leaf[k].x;
+    if (!leaf_block(info, X)) continue;  // uniform per CTA
+    const double h = dvd(h1, (double)((int64_t)1 << (leaf[k].y - 1)));  // h /= 1 << (level - 1)
+    const double *n = ne + (int64_t)X * kSS;
+    const double *ea = eabs + (int64_t)X * kSS;
+    const double *eb = e + (int64_t)X * 2 * kSSV;
+    double *fb = flux + (int64_t)X * 2 * kSSV;
+    double md = INFINITY;
+    for (int q = threadIdx.x; q < 2 * kFacesPerDim; q += blockDim.x) {
+      const int d = q >= kFacesPerDim;
+      const int r = q - d * kFacesPerDim;
+      // face I = (x, y) of component d; I1 = I - e_d
+      const int x = d ? 2 + (r & 15) : 2 + r % 17;
+      const int y = d ? 2 + (r >> 4) : 2 + r / 17;
+      const int st = d ? kS : 1;  // e_d in tile offsets
+      const int o = x + kS * y;
+      const double ed = eb[d * kSSV + x + kSV * y];
+      const double eabs1 = dvd(add(ea[o], ea[o - st]), 2.0);
+      const double mu = tr.mu, diff = tr.D;  // mobility / diffusion of the minimal model, theta = 1
+      const double v = mul(-ed, mu);
+      const int sv = signbit(v) ? -1 : 1;
+      // downstream, upstream and twice-upstream cells along d
+      const int od = o + st * (sv == 1 ? 0 : -1);
+      const int ou = o + st * (sv == 1 ? -1 : 0);
+      const int ou2 = o + st * (sv == 1 ? -2 : 1);
+      double F = mul(v, add(n[ou], koren_limited(sub(n[ou], n[ou2]), sub(n[od], n[ou]))));
+      const double tmaxwell = dvd(mul(maxwell, eabs1), fabs(F));
+      F = add(F, dvd(mul(diff, sub(n[o - st], n[o])), h));
+      fb[d * kSSV + x + kSV * y] = F;
+      md = fmin(md, fmin(fmin(dvd(h, fabs(v)), dvd(dvd(mul(h, h), diff), 4.0)), tmaxwell));
+    }
+    for (int off = 16; off > 0; off >>= 1) md = fmin(md, __shfl_xor_sync(0xffffffffu, md, off));
+    if ((threadIdx.x & 31) == 0) s_min[threadIdx.x >> 5] = md;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = s_min[0];
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmin(m, s_min[w]);
+      if (maxdt_blk) maxdt_blk[X] = m;
+      if (maxdt_min) atomic_min_nonneg(maxdt_min, m);
+    }
+    __syncthreads();
   }
-  const double d = na - nb;
-  const double r = d != 0.0 ? (nb - n3) / d : 0.0;
-  return nb + 0.5 * koren(r) * d;
 }
 
-__device__ __forceinline__ void atomic_max_pos(double *addr, double v) {
-  // non-negative doubles order like their bit patterns as signed integers
-  atomicMax(reinterpret_cast<unsigned long long *>(addr), (unsigned long long)__double_as_longlong(v));
+// restrict_flux! over one level's refinement-boundary faces: thread (block, face, k)
+// sets the coarse block's face k (0..7) of the half `subblock` covers to the mean of
+// the two fine faces 2k, 2k + 1: f = ((0 + f_2k) + f_2k+1) / 2.
+__global__ void k_restrict_flux(double *__restrict__ flux, LevelView lv) {
+  const int64_t total = (int64_t)lv.nblk * 32;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t >> 5), f = (int)(t >> 3) & 3, k = (int)(t & 7);
+    const int4 fi = lv.faces[4 * bi + f];
+    if (fi.x != FACE_REFBND) continue;
+    const int d = f >> 1;  // the face's dimension: 0 for -r/+r, 1 for -z/+z
+    const int fine_n = (f & 1) ? 2 + kM : 2, coarse_n = (f & 1) ? 2 : 2 + kM;  // normal face index
+    const int sb = d == 0 ? fi.w : fi.z;  // the tangential half
+    const int ct = 2 + 8 * (sb - 1) + k, ft = 2 + 2 * k;
+    const double *src = flux + (int64_t)lv.blocks[bi].x * 2 * kSSV + d * kSSV;
+    double *dst = flux + (int64_t)fi.y * 2 * kSSV + d * kSSV;
+    auto at = [&](int nrm, int tan) { return d == 0 ? nrm + kSV * tan : tan + kSV * nrm; };
+    const double s = add(add(0.0, src[at(fine_n, ft)]), src[at(fine_n, ft + 1)]);
+    dst[at(coarse_n, ct)] = dvd(s, 2.0);
+  }
 }
 
-struct Phys {
-  double mu, D;        // electron mobility (m^2/Vs) and diffusion (m^2/s)
-  double E0;           // applied field along +z (V/m)
-  double alpha_A, alpha_B;  // ionisation alpha = A exp(-B/|E|) (1/m, V/m)
-  double eta;          // attachment (1/m)
-};
-
-// Rates on the valid cells of the leaf-holding blocks; maxima of |v| and n_e into mx.
-__global__ void k_streamer_rates(const double *__restrict__ ne, const double *__restrict__ phi, const int2 *leaf,
-                                 int nleaf, const int4 *__restrict__ info, double h1, Phys P,
-                                 double *__restrict__ dne, double *__restrict__ dnp, double *__restrict__ dnn,
-                                 double *__restrict__ mx) {
+// chemderivs! (init, then add) and fluxderivs! on the valid cells of the leaf blocks:
+// dni = pre + post; dne = (((pre + post) + lower-r) - upper-r) + lower-z) - upper-z,
+// each face term (factor F) / h, factor = |1 + delta / (2 J - 1)| along the radial
+// dimension (1 along the others and in Cartesian geometry).
+__global__ void k_streamer_rates(double *__restrict__ dne, double *__restrict__ dni,
+                                 const double *__restrict__ ne, const double *__restrict__ eabs,
+                                 const double *__restrict__ flux, const int2 *__restrict__ leaf, int nleaf,
+                                 const int4 *__restrict__ info, double h1, int geom, srmg_transport tr) {
   const int64_t total = (int64_t)nleaf * 256;
-  double vmax = 0.0, nmax = 0.0;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
     const int k = (int)(t >> 8), c = (int)(t & 255);
-    const int2 lb = leaf[k];
-    const int4 bi = info[lb.x];
-    const double h = h1 / (double)((int64_t)1 << (lb.y - 1));
+    const int X = leaf[k].x;
+    const int4 bi = info[X];
+    if ((bi.z & 15) != 0) continue;
+    const double h = dvd(h1, (double)((int64_t)1 << (leaf[k].y - 1)));
     const int x = 2 + (c & 15), y = 2 + (c >> 4);
-    const int64_t base = (int64_t)lb.x * kSS;
-    const double *n = ne + base, *f = phi + base;
-    auto N = [&](int a, int b) { return n[a + kS * b]; };
-    auto F = [&](int a, int b) { return f[a + kS * b]; };
-    // global 1-based r index of this cell; face radii r_{i-1/2} = (i - 1) h, r_{i+1/2} = i h
-    const int64_t ig = x - 1 + 16 * (int64_t)(bi.x - 1);
-    const double rc = ((double)ig - 0.5) * h, rm = (double)(ig - 1) * h, rp = (double)ig * h;
-    // fields at the four faces (E = -grad phi, plus the applied field on z faces)
-    const double Erm = -(F(x, y) - F(x - 1, y)) / h, Erp = -(F(x + 1, y) - F(x, y)) / h;
-    const double Ezm = -(F(x, y) - F(x, y - 1)) / h + P.E0, Ezp = -(F(x, y + 1) - F(x, y)) / h + P.E0;
-    const double vrm = -P.mu * Erm, vrp = -P.mu * Erp, vzm = -P.mu * Ezm, vzp = -P.mu * Ezp;
-    const double Frm = vrm * face_value(vrm, N(x - 2, y), N(x - 1, y), N(x, y), N(x + 1, y)) -
-                       P.D * (N(x, y) - N(x - 1, y)) / h;
-    const double Frp = vrp * face_value(vrp, N(x - 1, y), N(x, y), N(x + 1, y), N(x + 2, y)) -
-                       P.D * (N(x + 1, y) - N(x, y)) / h;
-    const double Fzm = vzm * face_value(vzm, N(x, y - 2), N(x, y - 1), N(x, y), N(x, y + 1)) -
-                       P.D * (N(x, y) - N(x, y - 1)) / h;
-    const double Fzp = vzp * face_value(vzp, N(x, y - 1), N(x, y), N(x, y + 1), N(x, y + 2)) -
-                       P.D * (N(x, y + 1) - N(x, y)) / h;
-    const double div = (rp * Frp - rm * Frm) / (rc * h) + (Fzp - Fzm) / h;
-    // cell-centred field magnitude for the sources
-    const double Er = 0.5 * (Erm + Erp), Ez = 0.5 * (Ezm + Ezp);
-    const double Em = sqrt(Er * Er + Ez * Ez);
-    const double ion = P.alpha_A * exp(-P.alpha_B / fmax(Em, 1.0)) * P.mu * Em * N(x, y);
-    const double att = P.eta * P.mu * Em * N(x, y);
-    const int64_t o = base + x + kS * y;
-    dne[o] = -div + ion - att;
-    dnp[o] = ion;
-    dnn[o] = att;
-    vmax = fmax(vmax, fmax(fmax(fabs(vrm), fabs(vrp)), fmax(fabs(vzm), fabs(vzp))));
-    nmax = fmax(nmax, N(x, y));
-  }
-  for (int off = 16; off > 0; off >>= 1) {
-    vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, off));
-    nmax = fmax(nmax, __shfl_xor_sync(0xffffffffu, nmax, off));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomic_max_pos(mx, vmax);
-    atomic_max_pos(mx + 1, nmax);
+    const int64_t o = (int64_t)X * kSS + x + kS * y;
+    const double n1 = ne[o], E = eabs[o];
+    // NetIonization, MinimalTransportModel: mobility mu, townsend ai exp(-Ei / E),
+    // attachment aa exp(-Ea / E)
+    const double pre = mul(mul(mul(tr.mu, E), n1), mul(tr.ai, exp(dvd(-tr.Ei, E))));
+    const double post = mul(mul(mul(-tr.mu, E), n1), mul(tr.aa, exp(dvd(-tr.Ea, E))));
+    const double chem = add(pre, post);
+    dni[o] = chem;
+    const double *fb = flux + (int64_t)X * 2 * kSSV;
+    const int64_t Jr = gidx(bi.x, x), Jz = gidx(bi.y, y);
+    auto fac = [&](int dim, int delta) -> double {  // factor(geom, J, delta e_dim)
+      const bool radial = (geom == 1 && dim == 0) || (geom == 2 && dim == 1);
+      if (geom == 0) return 1.0;
+      const int64_t J = dim == 0 ? Jr : Jz;
+      const double q = radial ? dvd((double)delta, (double)(2 * J - 1)) : 0.0;
+      return fabs(add(1.0, q));
+    };
+    double v = chem;
+    v = add(v, dvd(mul(fac(0, -1), fb[x + kSV * y]), h));
+    v = sub(v, dvd(mul(fac(0, 1), fb[(x + 1) + kSV * y]), h));
+    v = add(v, dvd(mul(fac(1, -1), fb[kSSV + x + kSV * y]), h));
+    v = sub(v, dvd(mul(fac(1, 1), fb[kSSV + x + kSV * (y + 1)]), h));
+    dne[o] = v;
   }
 }
 
-__global__ void k_streamer_update(double *__restrict__ ne, double *__restrict__ np, double *__restrict__ nn,
-                                  const double *__restrict__ dne, const double *__restrict__ dnp,
-                                  const double *__restrict__ dnn, const int2 *leaf, int nleaf, double dt) {
-  const int64_t total = (int64_t)nleaf * 256;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)(t >> 8), c = (int)(t & 255);
-    const int64_t o = (int64_t)leaf[k].x * kSS + (2 + (c & 15)) + kS * (2 + (c >> 4));
-    ne[o] = fmax(0.0, ne[o] + dt * dne[o]);
-    np[o] = np[o] + dt * dnp[o];
-    nn[o] = nn[o] + dt * dnn[o];
+__global__ void k_init_min(double *m) { *m = INFINITY; }
+
+// The SSPRK3 stage combinations of step! (src/streamer.jl:400-413), elementwise.
+__global__ void k_ssprk3(double *__restrict__ out, const double *__restrict__ n, const double *__restrict__ d1,
+                         const double *__restrict__ d2, const double *__restrict__ d3, int64_t count, double dt,
+                         int stage) {
+  const double dt1 = dvd(dt, 4.0), dt6 = dvd(dt, 6.0), dt23 = dvd(mul(2.0, dt), 3.0);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
+    double inc;
+    if (stage == 1) inc = mul(d1[i], dt);
+    else if (stage == 2) inc = add(mul(d1[i], dt1), mul(d2[i], dt1));
+    else inc = add(add(mul(d1[i], dt6), mul(d2[i], dt6)), mul(d3[i], dt23));
+    out[i] = add(n[i], inc);
   }
+}
+
+int grid_of(int64_t work, int threads, int cap) {
+  const int64_t g = (work + threads - 1) / threads;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, cap));
+}
+
+int check_transport(srmg_ctx *ctx, const srmg_transport *tr, const char *who) {
+  if (!tr) return fail(ctx, SRMG_ERR_BADARG, "%s: null transport model", who);
+  const double v[6] = {tr->mu, tr->D, tr->ai, tr->Ei, tr->aa, tr->Ea};
+  for (double a : v)
+    if (!std::isfinite(a)) return fail(ctx, SRMG_ERR_BADARG, "%s: transport values must be finite", who);
+  if (!(tr->D > 0)) return fail(ctx, SRMG_ERR_BADARG, "%s: diffusion must be > 0", who);
+  return SRMG_OK;
 }
 
 }  // namespace
 
-// One forward-Euler step of the densities (n_e, n_+, n_-) on the leaf-holding blocks.
-// n_e and phi must have their ghosts filled.  dt = min(dt_max, cfl * h_min / max|v|,
-// cfl * h_min^2 / (4 D), cfl * eps0 / (e mu max n_e)) is returned in *dt_out.  work:
-// 3 device fields of nblk_alloc blocks (rates), 2 doubles (maxima).
-extern "C" int srmg_streamer_step_dev(srmg_ctx *ctx, double *ne, double *npos, double *nneg, const double *phi,
-                                      int64_t nblk_alloc, double h1, double E0, double mu, double D,
-                                      double alpha_A, double alpha_B, double eta, double cfl, double dt_max,
-                                      double *work, double *dt_out) {
+extern "C" int srmg_streamer_flux_dev(srmg_ctx *ctx, double *flux, double *maxdt_blk, double *maxdt_min,
+                                      const double *ne, const double *e, const double *eabs, int64_t nblk_alloc,
+                                      double h, const srmg_transport *tr) {
   RC(check_call(ctx, nblk_alloc, 0, 0, nullptr));
-  if (!ne || !npos || !nneg || !phi || !work || !dt_out || !(h1 > 0) || !(cfl > 0) || !(dt_max > 0))
-    return fail(ctx, SRMG_ERR_BADARG, "srmg_streamer_step_dev: bad arguments");
-  const int64_t nval = nblk_alloc * (int64_t)kSS;
-  double *dne = work, *dnp = work + nval, *dnn = work + 2 * nval, *mx = work + 3 * nval;
-  CK(cudaMemsetAsync(mx, 0, 2 * sizeof(double), ctx->stream));
-  Phys P{mu, D, E0, alpha_A, alpha_B, eta};
-  const int n = ctx->nleaf;
-  const int grid = (int)std::min<int64_t>(4096, ((int64_t)n * 256 + 255) / 256);
-  k_streamer_rates<<<grid, 256, 0, ctx->stream>>>(ne, phi, ctx->d_leaf, n, ctx->d_info, h1, P, dne, dnp, dnn, mx);
+  if (!flux || !ne || !e || !eabs) return fail(ctx, SRMG_ERR_BADARG, "srmg_streamer_flux_dev: null field");
+  if (!(h > 0.0) || !std::isfinite(h)) return fail(ctx, SRMG_ERR_BADARG, "srmg_streamer_flux_dev: h must be > 0");
+  RC(check_transport(ctx, tr, "srmg_streamer_flux_dev"));
+  if (maxdt_min) {
+    k_init_min<<<1, 1, 0, ctx->stream>>>(maxdt_min);
+    ctx->launches++;
+  }
+  if (ctx->nleaf > 0) {
+    k_streamer_flux<<<std::min(ctx->nleaf, 148 * 8), 256, 0, ctx->stream>>>(
+        flux, maxdt_blk, maxdt_min, ne, e, eabs, ctx->d_leaf, ctx->nleaf, ctx->d_info, h, *tr);
+    ctx->launches++;
+  }
+  for (int l = 2; l <= ctx->nlev; l++) {
+    if (!((ctx->refbnd_levels >> l) & 1)) continue;
+    const int n = ctx->nblk_host[l - 1];
+    k_restrict_flux<<<grid_of((int64_t)n * 32, 256, 148 * 8), 256, 0, ctx->stream>>>(flux, ctx->lv[l - 1].view(l));
+    ctx->launches++;
+  }
   CK(cudaGetLastError());
-  double hmx[2];
-  CK(cudaMemcpyAsync(hmx, mx, sizeof hmx, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  int lmax = 1;
-  for (int l = 1; l <= ctx->nlev; l++)
-    if (ctx->nblk_host[l - 1] > 0) lmax = l;
-  const double hmin = h1 / (double)((int64_t)1 << (lmax - 1));
-  double dt = dt_max;
-  if (hmx[0] > 0) dt = std::min(dt, cfl * hmin / hmx[0]);
-  if (D > 0) dt = std::min(dt, cfl * hmin * hmin / (4.0 * D));
-  if (hmx[1] > 0) dt = std::min(dt, cfl * kEps0 / (kE * mu * hmx[1]));
-  k_streamer_update<<<grid, 256, 0, ctx->stream>>>(ne, npos, nneg, dne, dnp, dnn, ctx->d_leaf, n, dt);
+  return SRMG_OK;
+}
+
+extern "C" int srmg_streamer_rates_dev(srmg_ctx *ctx, double *dne, double *dni, const double *ne,
+                                       const double *eabs, const double *flux, int64_t nblk_alloc, double h,
+                                       int geom, const srmg_transport *tr) {
+  RC(check_call(ctx, nblk_alloc, 0, 0, nullptr));
+  if (!dne || !dni || !ne || !eabs || !flux) return fail(ctx, SRMG_ERR_BADARG, "srmg_streamer_rates_dev: null field");
+  if (!(h > 0.0) || !std::isfinite(h)) return fail(ctx, SRMG_ERR_BADARG, "srmg_streamer_rates_dev: h must be > 0");
+  if (geom < 0 || geom > 2) return fail(ctx, SRMG_ERR_BADARG, "srmg_streamer_rates_dev: geom must be 0, 1 or 2");
+  RC(check_transport(ctx, tr, "srmg_streamer_rates_dev"));
+  if (ctx->nleaf > 0) {
+    k_streamer_rates<<<grid_of((int64_t)ctx->nleaf * 256, 256, 148 * 16), 256, 0, ctx->stream>>>(
+        dne, dni, ne, eabs, flux, ctx->d_leaf, ctx->nleaf, ctx->d_info, h, geom, *tr);
+    ctx->launches++;
+  }
   CK(cudaGetLastError());
-  *dt_out = dt;
+  return SRMG_OK;
+}
+
+extern "C" int srmg_ssprk3_stage_dev(srmg_ctx *ctx, double *out, const double *n, const double *dn1,
+                                     const double *dn2, const double *dn3, int64_t count, double dt, int stage) {
+  if (!ctx) return SRMG_ERR_BADARG;
+  if (stage < 1 || stage > 3) return fail(ctx, SRMG_ERR_BADARG, "srmg_ssprk3_stage_dev: stage must be 1, 2 or 3");
+  if (!out || !n || !dn1 || (stage >= 2 && !dn2) || (stage == 3 && !dn3) || count < 0)
+    return fail(ctx, SRMG_ERR_BADARG, "srmg_ssprk3_stage_dev: bad arguments");
+  if (!std::isfinite(dt)) return fail(ctx, SRMG_ERR_BADARG, "srmg_ssprk3_stage_dev: dt must be finite");
+  CK(cudaSetDevice(ctx->device));
+  if (count > 0) {
+    k_ssprk3<<<grid_of(count, 256, 148 * 16), 256, 0, ctx->stream>>>(out, n, dn1, dn2, dn3, count, dt, stage);
+    ctx->launches++;
+  }
+  CK(cudaGetLastError());
   return SRMG_OK;
 }

@@ -47,7 +47,8 @@ const STATE = State(C_NULL, parse(Int, get(ENV, "SRMG_DEVICE", "0")),
 
 function configure!(; device=STATE.device, enabled=STATE.enabled)
     if device != STATE.device && STATE.ctx != C_NULL
-        ccall((:srmg_destroy, libsrmg), Cvoid, (Ptr{Cvoid},), STATE.ctx)
+        ccall((:srmg_destroy, libsrmg), Cvoid, (Ptr{Cvoid},), STATE.ctx)  # also unregisters
+        empty!(REGISTERED)
         STATE.ctx = C_NULL
         STATE.fingerprint = 0
         STATE.fbc = 0
@@ -79,15 +80,47 @@ function context()
     STATE.ctx
 end
 
-# A cheap fingerprint of the tree: refine!/connectivity! (src/streamer.jl:545-549)
-# change at least one level's block set, so a checksum of every level's pairs decides
-# whether the device copy of the tree is stale.
+# A fingerprint of the tree: refine!/connectivity! (src/streamer.jl:545-549) change
+# at least one level's block set or block numbering, so a hash of every level's pairs,
+# in order, decides whether the device copy of the tree is stale.  FNV-1a over the
+# sequence (coord1, coord2, blk) of each pair: swapping the block ids of two
+# coordinates, or moving a pair, changes it.  `invalidate!()` forces the next upload.
+@inline fnv(h::UInt64, x) = (h ⊻ (reinterpret(UInt64, Int64(x)))) * 0x100000001b3
+
 function layer_fingerprint(layer)
-    h = UInt64(length(layer.pairs))
+    h = fnv(0xcbf29ce484222325, length(layer.pairs))
     for (c, blk) in layer.pairs
-        h += UInt64(blk) * 0x9e3779b97f4a7c15 + UInt64(c[1]) * 1000003 + UInt64(c[2])
+        h = fnv(fnv(fnv(h, c[1]), c[2]), blk)
     end
     h
+end
+
+"""
+    invalidate!()
+
+Forget the uploaded tree, so that the next solve uploads the tree and connectivity
+again (for callers that rebuild the tree in place in a way the fingerprint might not
+see)."""
+invalidate!() = (STATE.fingerprint = 0; STATE3.fingerprint = 0; nothing)
+
+# Host ranges page-locked for the fields passed to srmg_vcycle / srmg_fmg, keyed by the
+# ElasticArray object: when newblock! resizes a field (src/blockfield.jl:255-260) its
+# data moves, so the old range is unregistered before the new one is registered.
+const REGISTERED = Dict{UInt64, Tuple{Ptr{Cvoid}, Int}}()
+
+function register!(f)
+    ptr, n = Ptr{Cvoid}(pointer(f.u)), sizeof(f.u)
+    key = objectid(f.u)
+    old = get(REGISTERED, key, nothing)
+    old == (ptr, n) && return nothing
+    if old !== nothing
+        # the old range may already be gone: the result is not checked
+        ccall((:srmg_host_unregister, libsrmg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), context(), old[1])
+        delete!(REGISTERED, key)
+    end
+    rc = ccall((:srmg_host_register, libsrmg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Int64), context(), ptr, n)
+    rc == SRMG_OK && (REGISTERED[key] = (ptr, n))  # unregistered ranges still work, staged
+    nothing
 end
 
 function fingerprint(tree)
@@ -144,6 +177,8 @@ function Steamroller.vcycle!(u::GPUField, b::GPUField, r::GPUField, u1::GPUField
                       lmax, ndown, ntop, nup, ω)
     end
     upload!(tree, conn)
+    register!(u)
+    register!(b)
     op, k2 = opcode(lpldisc)
     a = Ref(bc.a)
     GC.@preserve u b r u1 a begin
@@ -167,6 +202,8 @@ function Steamroller.fmg!(u::GPUField, b::GPUField, r::GPUField, u1::GPUField, s
                       lmax, ndown, ntop, nup, ω)
     end
     upload!(tree, conn)
+    register!(u)
+    register!(b)
     op, k2 = opcode(lpldisc)
     a = Ref(bc.a)
     GC.@preserve u b r u1 a begin
@@ -238,9 +275,9 @@ function check3(rc)
 end
 
 function layer_fingerprint3(layer)
-    h = UInt64(length(layer.pairs))
+    h = fnv(0xcbf29ce484222325, length(layer.pairs))
     for (c, blk) in layer.pairs
-        h += UInt64(blk) * 0x9e3779b97f4a7c15 + UInt64(c[1]) * 1000003 + UInt64(c[2]) * 7919 + UInt64(c[3])
+        h = fnv(fnv(fnv(fnv(h, c[1]), c[2]), c[3]), blk)
     end
     h
 end

@@ -24,7 +24,7 @@ LIB_PATH = os.path.join(_HERE, "libsrmg.so")
 SRMG_OK = 0
 ERRORS = {-1: "BADARG", -2: "BADTREE", -3: "CUDA", -4: "TIMEOUT", -5: "DIVERGED",
           -6: "UNSUPPORTED", -7: "NOMEM", -8: "NOTREE"}
-MODE_FP64, MODE_MIXED = 0, 1
+MODE_FP64, MODE_MIXED, MODE_FP64_DIRECT = 0, 1, 2
 
 
 class SrmgError(RuntimeError):
@@ -70,6 +70,11 @@ _I64 = ctypes.c_int64
 _D = ctypes.c_double
 
 # name -> (restype, argtypes); the complete exported surface of include/srmg.h
+class Transport(ctypes.Structure):
+    """srmg_transport: the MinimalTransportModel (src/transport.jl:9-35)."""
+    _fields_ = [("mu", _D), ("D", _D), ("ai", _D), ("Ei", _D), ("aa", _D), ("Ea", _D)]
+
+
 SIGNATURES = {
     "srmg_create": (_I, [ctypes.POINTER(_P), _I, _I, _I, _I]),
     "srmg_destroy": (None, [_P]),
@@ -112,6 +117,8 @@ SIGNATURES = {
     "srmg_residual_postrestrict_level_dev": (_I, [_P, _P, _P, _P, _I64, _I, _D, _I, _D, _I]),
     "srmg_resnorm_noalloc": (_I, [_P, _P, _P, _I64, _D, _I, _D, _I, _P]),
     "srmg_set_option": (_I, [_P, ctypes.c_char_p, _I64]),
+    "srmg_host_register": (_I, [_P, _P, _I64]),
+    "srmg_host_unregister": (_I, [_P, _P]),
     "srmg_get_trace": (_I, [_P, _P, _I]),
     "srmg_launch_count": (_I64, [_P]),
     "srmg_batch_set": (_I, [_P, _I, ctypes.POINTER(Item), _I]),
@@ -144,7 +151,9 @@ SIGNATURES = {
     "srmg_cnn_pack_dev": (_I, [_P, _P, _P, _I64, _D, _I, _D, _I, _P, _P, _P, _P, _I]),
     "srmg_cnn_predict_dev": (_I, [_P, _P, _P, _P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, ctypes.POINTER(_I),
                                   ctypes.POINTER(_D)]),
-    "srmg_streamer_step_dev": (_I, [_P, _P, _P, _P, _P, _I64] + [_D] * 9 + [_P, ctypes.POINTER(_D)]),
+    "srmg_streamer_flux_dev": (_I, [_P, _P, _P, _P, _P, _P, _P, _I64, _D, ctypes.POINTER(Transport)]),
+    "srmg_streamer_rates_dev": (_I, [_P, _P, _P, _P, _P, _P, _I64, _D, _I, ctypes.POINTER(Transport)]),
+    "srmg_ssprk3_stage_dev": (_I, [_P, _P, _P, _P, _P, _P, _I64, _D, _I]),
 }
 
 

@@ -2,8 +2,9 @@
 through the C ABI) with the oracle (oracle/freebc_oracle.py restating src/freebc.jl).
 
 Bar: the boundary sources added to q, conf.b and the ghost values agree with the
-oracle to <= 1e-12 relative L2: the GPU runs both sine transforms as direct FP64
-sums, the oracle through FFTs, so the two round differently.  Every other cell is
+oracle to <= 1e-12 relative L2: the GPU runs both sine transforms through its own FFT
+(power-of-two lengths) or as direct FP64 sums (other lengths), the oracle through
+scipy's FFTs, so the two round differently.  Every other cell is
 untouched (bit-exact).  End to end (homogeneous solve, free boundary, main solve) the
 potential matches the oracle's to <= 1e-10.
 """
@@ -145,10 +146,13 @@ def test_freebc_refuses_bad_use():
     ctx.close()
 
 
-def test_freebc_oblong_root():
-    """A (1, 2) root grid: the outer column is twice as long (n = 2 * 16 * 2^(level-1))."""
+@pytest.mark.parametrize("rows", [2, 3])
+def test_freebc_oblong_root(rows):
+    """A (1, 2) root grid: the outer column is twice as long (n = 2 * 16 * 2^(level-1)),
+    a power of two (the FFT path); a (1, 3) root: n = 3 * 16 * 2^(level-1), the direct
+    sums."""
     from srmg.tree import Tree, populate, connectivity, boundaryconditions, refine_block
-    t = Tree((1, 2), 4)
+    t = Tree((1, rows), 4)
     populate(t, 2)
     refine_block(t, 2, (2, 3))
     t.sync()
@@ -156,10 +160,10 @@ def test_freebc_oblong_root():
     p = gen.make_problem(t, lambda r, z, l, gi, gj: np.exp(-(r * r + (z - 0.012) ** 2) / 2e-5), gen.poisson_scale(),
                          bc=boundaryconditions(((1, -1), (-1, -1))), conn=conn)
     level = len(t)
-    n, H, R, f = fo.kernel(1, level, (1, 2), p.h1)
-    assert n == 2 * 16 * 2 ** (level - 1)
+    n, H, R, f = fo.kernel(1, level, (1, rows), p.h1)
+    assert n == rows * 16 * 2 ** (level - 1)
     ctx = mg.Context(0).set_tree(p.tree, p.conn)
-    mg.freebc_set(ctx, 1, level, (1, 2), f)
+    mg.freebc_set(ctx, 1, level, (1, rows), f)
     rng = np.random.default_rng(8)
     u = rng.standard_normal(p.b.shape)
     q = rng.standard_normal(p.b.shape)
@@ -172,4 +176,35 @@ def test_freebc_oblong_root():
     changed = qo != q
     np.testing.assert_array_equal(qh[~changed], q[~changed])
     assert rel_l2(qh[changed] - q[changed], qo[changed] - q[changed]) <= REL
+    ctx.close()
+
+
+@pytest.mark.parametrize("level", [9, 11, 13])
+def test_freebc_fft_matches_direct_sums(level):
+    """At the lengths of a 9-, 11- and 13-level tree (n = 4096, 16384, 65536: the last
+    two through the four-step FFT) the FFT transforms give conf.b and the sources of
+    the direct sums and of the oracle to <= 1e-12."""
+    import torch
+    p = gen.config2(seed=5, target_leaf=40_000, extra=3)
+    n, H, R, f = fo.kernel(1, level, (1, 1), p.h1)
+    ctx = mg.Context(0).set_tree(p.tree, p.conn)
+    mg.freebc_set(ctx, 1, level, (1, 1), f)
+    rng = np.random.default_rng(level)
+    u = rng.standard_normal(p.b.shape)
+    q = rng.standard_normal(p.b.shape)
+    out = {}
+    for direct in (0, 1):
+        ctx.set_option("freebc_direct", direct)
+        qg, ug = torch_cuda(q), torch_cuda(u)
+        bg = torch.zeros(n, dtype=torch.float64, device="cuda")
+        mg.freebc_(ctx, qg, ug, p.h1, p.s, b_out=bg)
+        ctx.synchronize()
+        out[direct] = (qg.cpu().numpy(), bg.cpu().numpy())
+    qo = q.copy()
+    bo = fo.freebc(qo, u, p.h1, p.s, p.tree, p.conn, 1, level, f)
+    for direct in (0, 1):
+        assert rel_l2(out[direct][1], bo) <= REL, direct
+        changed = qo != q
+        assert rel_l2(out[direct][0][changed] - q[changed], qo[changed] - q[changed]) <= REL
+    assert rel_l2(out[0][1], out[1][1]) <= REL
     ctx.close()

@@ -260,18 +260,34 @@ def test_engine_local_levels(local_max):
 
 
 def test_vcycle_host_pointer_entry_point(pair):
-    """srmg_vcycle (host arrays, the ccall boundary) == the device entry point."""
+    """srmg_vcycle (host arrays, the ccall boundary) == the device entry point.  b is
+    not copied back by default (its leaf cells are never written); with "b_copy_back"
+    it returns the FAS values of the covered cells as the device path leaves them.
+    Page-locked (registered) host arrays give the same results."""
     p = pair.p
     u, b = _prepared(pair)
-    uh, bh = u.copy(), b.copy()
-    mg.vcycle_(pair.ctx, uh, bh, np.zeros_like(u), np.zeros_like(u), p.s, p.geom, p.bc,
-               ndown=2, ntop=4, nup=2, ncycles=2)
     ug, bg = torch_cuda(u), torch_cuda(b)
     mg.vcycle_(pair.ctx, ug, bg, torch_cuda(np.zeros_like(u)), torch_cuda(np.zeros_like(u)), p.s,
                p.geom, p.bc, ndown=2, ntop=4, nup=2, ncycles=2)
     pair.ctx.synchronize()
-    assert np.array_equal(uh.view(np.uint64), to_np(ug).view(np.uint64))
-    assert np.array_equal(bh.view(np.uint64), to_np(bg).view(np.uint64))
+    for copy_back, register in ((0, False), (1, False), (0, True)):
+        pair.ctx.set_option("b_copy_back", copy_back)
+        uh, bh = u.copy(), b.copy()
+        if register:
+            for a in (uh, bh):
+                pair.ctx.check(mg.lib().srmg_host_register(pair.ctx.handle, a.ctypes.data, a.nbytes))
+        mg.vcycle_(pair.ctx, uh, bh, np.zeros_like(u), np.zeros_like(u), p.s, p.geom, p.bc,
+                   ndown=2, ntop=4, nup=2, ncycles=2)
+        assert np.array_equal(uh.view(np.uint64), to_np(ug).view(np.uint64))
+        want_b = to_np(bg) if copy_back else b
+        assert np.array_equal(bh.view(np.uint64), want_b.view(np.uint64))
+        if register:
+            for a in (uh, bh):
+                pair.ctx.check(mg.lib().srmg_host_unregister(pair.ctx.handle, a.ctypes.data))
+    pair.ctx.set_option("b_copy_back", 0)
+    # the leaf cells of b are the same either way
+    leaf = leaf_mask(p)
+    assert np.array_equal(to_np(bg)[leaf], b[leaf])
 
 
 @pytest.mark.parametrize("variant", ["helmholtz", "cartesian", "cyl2", "default_bc", "omega"])
@@ -390,3 +406,24 @@ def leaf_mask(p):
             if p.tree.isleaf(layer.level, c):
                 m[blk - 1, 2:18, 2:18] = True
     return m
+
+
+def test_fp64_direct_mode_reaches_the_oracle_solution():
+    """SRMG_MODE_FP64_DIRECT: FP64 V-cycles with the direct FP64 coarsest solve converge
+    to the oracle's FP64 solution in far fewer cycles than the reference's 4 top sweeps,
+    and to the same solution as the mixed mode."""
+    p = PROBS["refined"]
+    pr = Pair(p)
+    u, b = _prepared(pr)
+    out = {}
+    for mode in (mg.MODE_FP64, mg.MODE_FP64_DIRECT, mg.MODE_MIXED):
+        ug = torch_cuda(u)
+        st = mg.solve(pr.ctx, ug, torch_cuda(b), p.s, p.geom, p.bc, tol=1e-8, mode=mode, max_cycles=2000)
+        assert st["rel_residual"] <= 1e-8
+        out[mode] = (st["cycles"], to_np(ug))
+    assert out[mg.MODE_FP64_DIRECT][0] < out[mg.MODE_FP64][0]
+    uo = u.copy()
+    pr.orc.solve(uo, b.copy(), 1e-11, max_cycles=5000)
+    leaf = leaf_mask(p)
+    assert rel_l2(out[mg.MODE_FP64_DIRECT][1], uo, leaf) < 1e-6
+    assert rel_l2(out[mg.MODE_FP64_DIRECT][1], out[mg.MODE_MIXED][1], leaf) < 1e-6
