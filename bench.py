@@ -345,9 +345,21 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     s, geom, bc = problem.s, problem.geom, problem.bc
 
+    # the project's autotuner picks the launch shape, sweep counts and Gauss-Seidel
+    # relaxation factor of the mixed solve on this problem (untimed; the plain FP64 leg
+    # keeps the reference's V(2,2) cycle with 4 top sweeps and omega = 1)
+    with torch.cuda.stream(stream):
+        u.zero_()
+    stream.synchronize()
+    chosen, _ = mg.autotune(ctx, u, b, s, geom, bc, tol=TOL, mode=mg.MODE_MIXED)
+    tuned = {k: chosen[k] for k in ("ndown", "nup", "ntop", "omega")}
+    cfg["tuned"] = tuned
+    ref_cycle = dict(ndown=2, nup=2, ntop=4, omega=1.0)
+    opts_of = {mg.MODE_MIXED: tuned, mg.MODE_FP64_DIRECT: tuned, mg.MODE_FP64: ref_cycle}
+
     def one_solve(mode, max_cycles=5000):
         u.zero_()
-        return mg.solve(ctx, u, b, s, geom, bc, tol=TOL, mode=mode, max_cycles=max_cycles)
+        return mg.solve(ctx, u, b, s, geom, bc, tol=TOL, mode=mode, max_cycles=max_cycles, **opts_of[mode])
 
     def timed(mode, steps, warm, clk=None):
         for _ in range(warm):
@@ -363,7 +375,7 @@ def main():
                 flush.fill_(1.0)
                 u.zero_()
             stream.synchronize()
-            st = mg.solve(ctx, u, b, s, geom, bc, tol=TOL, mode=mode, max_cycles=5000)
+            st = mg.solve(ctx, u, b, s, geom, bc, tol=TOL, mode=mode, max_cycles=5000, **opts_of[mode])
             total_ms += st["device_ms"]
             stats = st
         if clk is not None:
@@ -396,7 +408,7 @@ def main():
         with torch.cuda.stream(stream):
             u.zero_()
         stream.synchronize()
-        mg.solve(ctx, u, b, s, geom, bc, tol=tol, mode=mode, max_cycles=5000)
+        mg.solve(ctx, u, b, s, geom, bc, tol=tol, mode=mode, max_cycles=5000, **opts_of[mode])
         sols[name] = u[leaf].cpu().numpy()
     if rank == 0 and not args.no_cpu:
         uo, oc, orel, ot = oracle_solve(problem, 1e-11)
@@ -428,7 +440,8 @@ def main():
     hbm, src = peaks()
     achieved = bytes_vc / (vc_ms / 1e3) / 1e9
     # the timed kernel: one mixed-solve launch per step, event-timed on the context's stream
-    bytes_mx = model.mixed_solve_bytes(problem.tree, mixed_st["cycles"], mixed_st["outer"])
+    bytes_mx = model.mixed_solve_bytes(problem.tree, mixed_st["cycles"], mixed_st["outer"], ndown=tuned["ndown"],
+                                       nup=tuned["nup"])
     achieved_mx = bytes_mx / (mixed_ms / args.steps / 1e3) / 1e9
 
     # e2e through the host-pointer C ABI, from page-locked host buffers
@@ -438,7 +451,7 @@ def main():
     for i in range(args.warmup + args.steps):
         uh[:] = 0.0
         t0 = time.perf_counter()
-        mg.solve(ctx, uh, bh, s, geom, bc, tol=TOL, mode=mg.MODE_MIXED)
+        mg.solve(ctx, uh, bh, s, geom, bc, tol=TOL, mode=mg.MODE_MIXED, **tuned)
         if i >= args.warmup:
             e2e_t.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(float(np.sum(e2e_t)), pg, dev)
@@ -467,8 +480,8 @@ def main():
                          "peak_source": src,
                          "kernel": "mixed-precision solve (one persistent launch per solve: the timed kernel)",
                          "bytes_per_launch": bytes_mx, "ms_per_launch": mixed_ms / args.steps,
-                         "bytes_model": "srmg.model.mixed_solve_bytes(tree, cycles=%d, steps=%d)"
-                                        % (mixed_st["cycles"], mixed_st["outer"])},
+                         "bytes_model": "srmg.model.mixed_solve_bytes(tree, cycles=%d, steps=%d, ndown=%d, nup=%d)"
+                                        % (mixed_st["cycles"], mixed_st["outer"], tuned["ndown"], tuned["nup"])},
             "roofline_fp64_vcycle": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                                      "frac": achieved / hbm,
                                      "traffic": TRAFFIC_VCYCLE_CONFIG2 if nleaf == 1503232 else None,
@@ -542,16 +555,14 @@ def run_dropin(ctx, problem, steps, warm, stream):
     rg, u1g = torch.zeros_like(bg), torch.zeros_like(bg)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    cur = torch.cuda.current_stream()
-    ctx.set_stream(cur.cuda_stream)
-    mg.vcycle_(ctx, ug, bg, rg, u1g, p.s, p.geom, p.bc, ndown=2, ntop=4, nup=2, ncycles=2)
-    ev0.record(cur)
-    for _ in range(steps):
+    with torch.cuda.stream(stream):  # the context's stream: the events bracket its launches
         mg.vcycle_(ctx, ug, bg, rg, u1g, p.s, p.geom, p.bc, ndown=2, ntop=4, nup=2, ncycles=2)
-    ev1.record(cur)
+        ev0.record(stream)
+        for _ in range(steps):
+            mg.vcycle_(ctx, ug, bg, rg, u1g, p.s, p.geom, p.bc, ndown=2, ntop=4, nup=2, ncycles=2)
+        ev1.record(stream)
     ev1.synchronize()
     out["device_ms_per_call"] = ev0.elapsed_time(ev1) / steps
-    ctx.set_stream(stream.cuda_stream)
     return out
 
 
@@ -616,7 +627,9 @@ def run_batch(local, stream, steps, rank=0, world=1, pg=None, dev=None):
         us = [torch.zeros(p.b.shape, dtype=torch.float64, device="cuda") for _, p in items]
         bs = [torch.from_numpy(p.b).cuda() for _, p in items]
     stream.synchronize()
-    opts = dict(tol=TOL, ndown=2, ntop=4, nup=2, max_cycles=5000)
+    ref_opts = dict(tol=TOL, ndown=2, ntop=4, nup=2, max_cycles=5000)   # plain FP64: the reference's cycle
+    tuned_opts = dict(tol=TOL, max_cycles=5000, **mg.TUNED)               # mixed: the tuned smoother
+    opts_of = {mg.MODE_MIXED: tuned_opts, mg.MODE_FP64: ref_opts}
 
     def zero():
         with torch.cuda.stream(stream):
@@ -628,12 +641,12 @@ def run_batch(local, stream, steps, rank=0, world=1, pg=None, dev=None):
     res = {}
     for mode, name in ((mg.MODE_MIXED, "mixed"), (mg.MODE_FP64, "fp64")):
         zero()
-        batch.solve(us, bs, mode=mode, **opts)  # warm-up (capture)
+        batch.solve(us, bs, mode=mode, **opts_of[mode])  # warm-up (capture)
         ms = []
         n = steps if mode == mg.MODE_MIXED else 1
         for _ in range(n):
             zero()
-            st = batch.solve(us, bs, mode=mode, **opts)
+            st = batch.solve(us, bs, mode=mode, **opts_of[mode])
             ms.append(st[0]["device_ms"])
         t = max_over_ranks(float(np.mean(ms)), pg, dev)
         res[name + "_batched"] = {"value": n_total / (t / 1e3), "unit": "solves/s",
@@ -646,7 +659,7 @@ def run_batch(local, stream, steps, rank=0, world=1, pg=None, dev=None):
             with torch.cuda.stream(stream):
                 us[k].zero_()
             stream.synchronize()
-            st = mg.solve(c, us[k], bs[k], p.s, p.geom, p.bc, disc(p), mode=mode, **opts)
+            st = mg.solve(c, us[k], bs[k], p.s, p.geom, p.bc, disc(p), mode=mode, **opts_of[mode])
             tot += st["device_ms"]
         tot = max_over_ranks(tot, pg, dev)
         res[name + "_solo"] = {"value": n_total / (tot / 1e3), "unit": "solves/s", "ms_total": tot}

@@ -326,19 +326,20 @@ int srmg_electric_field_dev(srmg_ctx *ctx, double *e, double *eabs, const double
                             double h, const double e0[2]);
 
 /* Allocation-free residual norm.  No counterpart in the reference: it exists for
- * callers that cannot call cudaMalloc when they need the norm -- code inside CUDA
- * stream capture, hosts whose device memory belongs to their own pool allocator, or
- * loops that cannot take an allocation's implicit synchronisation.  Same value as
- * srmg_resnorm_dev (resnorm!, src/multigrid.jl:391-417) up to summation order, but
- * it calls no cudaMalloc/cudaFree or allocating library routine: its scratch (one
- * partial sum per tree block) is a static device array of 65536 doubles (512 KiB),
- * held by every GPU that loads the library until the process exits.  Trees of more
- * than 65536 blocks are rejected with SRMG_ERR_BADARG.  `out` is a DEVICE address
- * that receives the norm, stream-ordered on the context's stream; nothing is copied
- * to the host.  The array is shared by all calls and keeps the last call's
- * contents; calls that overlap on the GPU (several streams or contexts at once)
- * race on it.  The first call on each device looks up the array's device address;
- * make that first call before any stream capture begins. */
+ * callers that cannot call cudaMalloc when they need the norm -- hosts whose device
+ * memory belongs to their own pool allocator, or loops that cannot take an
+ * allocation's implicit synchronisation.  Same value as srmg_resnorm_dev up to
+ * summation order, but it calls no cudaMalloc/cudaFree or allocating library routine:
+ * its scratch (one partial sum per tree block) is a static device array of 65536
+ * doubles (512 KiB), held by every GPU that loads the library until the process
+ * exits.  Trees of more than 65536 blocks are rejected with SRMG_ERR_BADARG; 2D trees
+ * only (SRMG_ERR_UNSUPPORTED for D = 3).  `out` is a DEVICE address that receives the
+ * norm, stream-ordered on the context's stream; nothing is copied to the host.  The
+ * array is shared by all calls and keeps the last call's contents; calls that overlap
+ * on the GPU (several streams or contexts at once) race on it.  The first call on each
+ * device looks up the array's device address and keeps it for the life of the process
+ * (the device's primary context must outlive the calls: no use after a
+ * cudaDeviceReset); make that first call before any stream capture begins. */
 int srmg_resnorm_noalloc(srmg_ctx *ctx, const double *b, const double *u, int64_t nblk_alloc,
                          double s, int op, double k2, int geom, double *out);
 
@@ -387,17 +388,20 @@ int srmg_batch_solve_forest_dev(srmg_ctx *batch, double *u, const double *b,
 
 /* ---- autotuner (no reference counterpart) ----------------------------------------
  * Times complete solves to opts->tol from the caller's initial guess for a set of
- * candidate launch shapes and sweep counts (30 candidates, each solved twice):
- * engine_ctas (one CTA per SM or half as many: blocks per CTA), local_max_blocks
- * (4, 16, 64: coarse levels kept inside one CTA) and (ndown, nup) in {(2,2), (1,1),
- * (1,2), (2,1), (3,3)}.  The fastest candidate's options are set on the context and
- * its sweep counts written to *opts; u is restored to its initial content.  Trials
- * are reported in `trials` (up to max_trials).  Returns the number of trials run or
- * an error code.  The tile shape is fixed: one 20 x 20 block per 256-thread slot. */
+ * candidates, each solved twice: first the launch shape at the caller's sweeps and
+ * omega -- engine_ctas (one CTA per SM or half as many: blocks per CTA) x
+ * local_max_blocks (4, 16, 64: coarse levels kept inside one CTA), 6 candidates --
+ * then, at the fastest shape, (ndown, nup) in {(2,2), (1,1), (1,2), (2,1), (3,3)} x the
+ * Gauss-Seidel relaxation factor omega in {1, 1.1, 1.2}, 15 candidates.  The fastest
+ * candidate's options are set on the context and its sweep counts and omega written to
+ * *opts; u is restored to its initial content.  Trials are reported in `trials` (up to
+ * max_trials).  Returns the number of trials run or an error code.  The tile shape is
+ * fixed: one 20 x 20 block per 256-thread slot. */
 typedef struct {
     int engine_ctas, local_max_blocks, ndown, nup, ntop;
     int cycles;          /* V-cycles (FP64) or defect-correction steps (mixed), worst item */
     double ms;           /* best device time of the trial, -1 if it missed the tolerance */
+    double omega;        /* relaxation factor of the trial */
 } srmg_tune_trial;
 int srmg_autotune(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc,
                   double s, int op, double k2, int geom, const int8_t bc[9],

@@ -141,15 +141,19 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err, unsigned &
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
     int ok = 1;
     const long long t0 = gtimer();
-    while (true) {
+    // the error word and the clock are read every 32 polls only: each read is another
+    // memory round trip between two polls (measured: 1.42 -> 1.29 us per barrier)
+    for (unsigned it = 1;; ++it) {
       unsigned v;
       asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
       if (v >= target) break;
-      if (*(volatile int *)err) { ok = 0; break; }
-      if (gtimer() - t0 > timeout_ns) {
-        atomicCAS(err, 0, 1);
-        ok = 0;
-        break;
+      if ((it & 31u) == 0) {
+        if (*(volatile int *)err) { ok = 0; break; }
+        if (gtimer() - t0 > timeout_ns) {
+          atomicCAS(err, 0, 1);
+          ok = 0;
+          break;
+        }
       }
       __nanosleep(20);
     }
@@ -225,15 +229,24 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
 constexpr int kBuf = 4;
 constexpr int kChunk = 32;
 constexpr int kWRow = 2 * kS;  // a weight row: wm, then wp, at the tile positions 0..19
+// Levels 1..kLevCache whose GS phases give a slot at most two blocks keep those blocks'
+// records in the slot's shared memory for the whole launch (loaded once at the start),
+// so that the phase issues its tile copies at once instead of after a record load.
+constexpr int kLevCache = 12;
 template <typename T>
 struct SlotSmem {
   T tile[kBuf][kSS];
   T tile2[kBuf][kSS];  // the second tile of a pair: b (GS, restriction) or the parent's e (prolongation)
   T wst[kBuf][kWRow];  // the block's weight row (GS, restriction)
   int4 recs[kChunk][6];
+  int4 rgs[kLevCache][2][6];  // cached GS records of the small levels (rows of 6 like recs)
+  int4 rres[kLevCache][2][6];  // cached restriction records (child edge, fine info, coarse faces)
+  int4 rpro[kLevCache][2][6];  // cached prolongation records (child edge, fine faces)
   uint64_t bar[kBuf];
   int sel[kChunk];  // list positions of the chunk's blocks that take part
   int cnt;
+  unsigned gs_cached;  // bit l: the GS records of level l are in rgs[l - 1]
+  unsigned ch_cached;  // bit l: the restriction and prolongation records of level l are cached
 };
 // Bulk copies land on 16-byte boundaries: every tile buffer of every slot.
 static_assert(sizeof(SlotSmem<double>) % 16 == 0 && sizeof(SlotSmem<float>) % 16 == 0, "slot size");
@@ -634,10 +647,13 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
   // (b comes from b's ghost layer when A.bghost, except the FAS right-hand side of a
   // covered neighbour cell, formed here from the neighbour's restricted residual in e)
   T hvn = T(0), hcn = T(0);
+  // the records: the launch-long cache of a small level, or the chunk staged in recs
+  const bool cached = A.nitems == 1 && l <= kLevCache && ((S.gs_cached >> l) & 1u);
+  int4(*R)[6] = cached ? S.rgs[l - 1] : S.recs;
   auto prefetch = [&](int j) {
     if (hthr) {
       const HaloCell hc_ = halo_unpack(halo_tab[hm]);
-      const int4 fi = S.recs[j][1 + hc_.f];
+      const int4 fi = R[j][1 + hc_.f];
       if (fi.x == FACE_NEIGHBOR) {
         const int64_t nb = (int64_t)fi.y * kSS;
         const bool covn = fas && ((fi.z >> hc_.nsub) & 1);
@@ -648,14 +664,16 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
     }
   };
   auto issue = [&](int j) {
-    const int4 bk = S.recs[j][0];
+    const int4 bk = R[j][0];
     issue_block<T>(A, S, (pk + j) % kBuf, src, bk.x, bk.y, bk.z);
   };
   // one item: the operator values stay in registers for the whole level
   T s = A.it_par[l], centre = A.it_par[32 + l], nwc = A.it_par[64 + l];
   for (int c0 = 0; c0 < nmine; c0 += kChunk) {
     int cn;
-    if (A.nitems == 1) {
+    if (cached) {
+      cn = nmine;  // <= 2, one chunk
+    } else if (A.nitems == 1) {
       cn = min(kChunk, nmine - c0);
       for (int i = t; i < 5 * cn; i += 256) {
         const int q = i / 5, k = i - 5 * q;
@@ -684,8 +702,8 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
       const int buf = kb % kBuf;
       const T hv = hvn, hc = hcn;
       if (j + 2 < cn) prefetch(j + 2);
-      const int4 bk = S.recs[act ? j : 0][0];
-      const int4 *fc = &S.recs[act ? j : 0][1];
+      const int4 bk = R[act ? j : 0][0];
+      const int4 *fc = &R[act ? j : 0][1];
       const int64_t xo = (int64_t)bk.x * kSS + o0;
       const bool cov = fas && ((bk.w >> mysub) & 1);
       // the covered cells' restricted residual (FAS), loaded while the tiles arrive
@@ -818,25 +836,32 @@ __device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
   const int half = t >> 7, h = t & 127;
   const int x0 = 2 + 2 * (h & 7), y = 2 + (h >> 3);
   const int o0 = x0 + kS * y;
+  const bool cached = A.nitems == 1 && l <= kLevCache && ((S.ch_cached >> l) & 1u);
+  int4(*R)[6] = cached ? S.rres[l - 1] : S.recs;
   auto issue = [&](int j) {
-    const int4 fi = S.recs[j][1];
-    issue_block<T>(A, S, (pk + j) % kBuf, uf, S.recs[j][0].x, fi.x, fi.y);
+    const int4 fi = R[j][1];
+    issue_block<T>(A, S, (pk + j) % kBuf, uf, R[j][0].x, fi.x, fi.y);
   };
   for (int c0 = 0; c0 < nmine; c0 += kChunk) {
     // the chunk's next child edges, without those of frozen items: recs[q][0] = {fine,
     // coarse, sb_r, sb_z}, recs[q][1] = info of the fine block, recs[q][2..5] = the
-    // coarse block's faces
-    select_chunk<T>(S, t, c0, nmine, first, step,
-                    [&](int gi) { return A.nitems == 1 || !A.frozen[A.tr.info[ch[gi].x].z >> 8]; });
-    slot_sync(slot);
-    const int cn = S.cnt;
-    for (int i = t; i < 6 * cn; i += 256) {
-      const int q = i / 6, k = i - 6 * q;
-      const int4 e = ch[S.sel[q]];
-      S.recs[q][k] = k == 0 ? e : k == 1 ? A.tr.info[e.x] : A.tr.faces[4 * e.y + k - 2];
+    // coarse block's faces (or the launch-long cache of a small level)
+    int cn;
+    if (cached) {
+      cn = nmine;  // <= 2, one chunk
+    } else {
+      select_chunk<T>(S, t, c0, nmine, first, step,
+                      [&](int gi) { return A.nitems == 1 || !A.frozen[A.tr.info[ch[gi].x].z >> 8]; });
+      slot_sync(slot);
+      cn = S.cnt;
+      for (int i = t; i < 6 * cn; i += 256) {
+        const int q = i / 6, k = i - 6 * q;
+        const int4 e = ch[S.sel[q]];
+        S.recs[q][k] = k == 0 ? e : k == 1 ? A.tr.info[e.x] : A.tr.faces[4 * e.y + k - 2];
+      }
+      slot_sync(slot);
+      if (cn == 0) continue;
     }
-    slot_sync(slot);
-    if (cn == 0) continue;
     if (t == 0)
       for (int q = 0; q < kBuf && q < cn; ++q) issue(q);
     for (int i = 0; 2 * i < cn; ++i) {
@@ -848,7 +873,7 @@ __device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
       if (act) ok = mbar_wait(&S.bar[buf], (kb / kBuf) & 1, A.err, A.timeout_ns);
       const T *tile = S.tile[buf];
       const int jj = act ? j : 0;
-      const int4 e = S.recs[jj][0], fi = S.recs[jj][1];
+      const int4 e = R[jj][0], fi = R[jj][1];
       const int item = fi.z >> 8;
       if (act && ok) {
         const T *par = A.it_par + item * kParStride;
@@ -883,7 +908,7 @@ __device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
         const T cu = restrict4<T>(tile, 2 + 2 * kx, 2 + 2 * ky);
         const T cr = restrict4<T>(S.tile2[buf], 2 + 2 * kx, 2 + 2 * ky);
         uc[(int64_t)C * kSS + cx + kS * cy] = cu;
-        push_f<T>((unsigned)A.it_sgbits[item], uc, C, &S.recs[j][2], cx, cy, cu);
+        push_f<T>((unsigned)A.it_sgbits[item], uc, C, &R[j][2], cx, cy, cu);
         A.e[(int64_t)C * kSS + cx + kS * cy] = cr;
       }
     }
@@ -908,28 +933,36 @@ __device__ bool ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int f
   const int dx = t & 15, dy = t >> 4;
   const int x = 2 + dx, y = 2 + dy;
   const int ir = dx & 1, iz = dy & 1;
-  auto issue = [&](unsigned kb, int j) { issue_pair<T>(S, kb % kBuf, uf, S.recs[j][0].x, A.e, S.recs[j][0].y); };
+  const bool cached = A.nitems == 1 && l <= kLevCache && ((S.ch_cached >> l) & 1u);
+  int4(*R)[6] = cached ? S.rpro[l - 1] : S.recs;
+  auto issue = [&](unsigned kb, int j) { issue_pair<T>(S, kb % kBuf, uf, R[j][0].x, A.e, R[j][0].y); };
   for (int c0 = 0; c0 < nmine; c0 += kChunk) {
     // the chunk's next child edges, without those of frozen items:
     // recs[q][0] = {fine, coarse, sb_r, sb_z}, recs[q][1..4] = the fine block's faces
-    select_chunk<T>(S, t, c0, nmine, first, step,
-                    [&](int gi) { return A.nitems == 1 || !A.frozen[A.tr.info[ch[gi].x].z >> 8]; });
-    slot_sync(slot);
-    const int cn = S.cnt;
-    for (int i = t; i < 5 * cn; i += 256) {
-      const int q = i / 5, k = i - 5 * q;
-      const int4 e = ch[S.sel[q]];
-      S.recs[q][k] = k == 0 ? e : A.tr.faces[4 * e.x + k - 1];
+    // (or the launch-long cache of a small level)
+    int cn;
+    if (cached) {
+      cn = nmine;  // <= 2, one chunk
+    } else {
+      select_chunk<T>(S, t, c0, nmine, first, step,
+                      [&](int gi) { return A.nitems == 1 || !A.frozen[A.tr.info[ch[gi].x].z >> 8]; });
+      slot_sync(slot);
+      cn = S.cnt;
+      for (int i = t; i < 5 * cn; i += 256) {
+        const int q = i / 5, k = i - 5 * q;
+        const int4 e = ch[S.sel[q]];
+        S.recs[q][k] = k == 0 ? e : A.tr.faces[4 * e.x + k - 1];
+      }
+      slot_sync(slot);
+      if (cn == 0) continue;
     }
-    slot_sync(slot);
-    if (cn == 0) continue;
     if (t == 0)
       for (int q = 0; q < kBuf - 1 && q < cn; ++q) issue(pk + q, q);
     for (int j = 0; j < cn; ++j) {
       const unsigned kb = pk + j;
       const int buf = kb % kBuf;
-      const int4 e = S.recs[j][0];
-      const int4 *fc = &S.recs[j][1];
+      const int4 e = R[j][0];
+      const int4 *fc = &R[j][1];
       const int F = e.x;
       if (t == 0 && j + kBuf - 1 < cn) issue(kb + kBuf - 1, j + kBuf - 1);
       if (!mbar_wait(&S.bar[buf], (kb / kBuf) & 1, A.err, A.timeout_ns)) {
@@ -1281,7 +1314,7 @@ __device__ void ph_itemnorm(const EngArgs<T> &A, bool first, int cycles, int ste
 // correction e = u_1 - u1 of the level.  An item's level 1 has <= 4 blocks.
 template <typename T>
 __device__ void ph_direct_top(const EngArgs<T> &A, T *u, bool make_e, int first, int step, int t, int slot,
-                              double *sol) {
+                              double *sol, double *rhs) {
   const int x = 2 + (t & 15), y = 2 + (t >> 4);
   const int o = x + kS * y;
   const int mysub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
@@ -1307,16 +1340,29 @@ __device__ void ph_direct_top(const EngArgs<T> &A, T *u, bool make_e, int first,
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int n = 256 * n1;
     const double *P = A.it_P[k];
-    for (int q = warp; q < n; q += nw) {
-      const double *pr = P + (int64_t)q * n;
-      double acc = 0.0;
+    // the level's right-hand side once into shared memory, then every warp four rows of
+    // P at a time (four independent accumulators keep more of P's loads in flight);
+    // each row sums lane-strided partials, then the warp, in a fixed order
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+      const int c = j & 255;
+      rhs[j] = (double)A.b[(int64_t)blocks[j >> 8].x * kSS + (2 + (c & 15)) + kS * (2 + (c >> 4))];
+    }
+    __syncthreads();
+    for (int q0 = 4 * warp; q0 < n; q0 += 4 * nw) {  // n is a multiple of 256: all four rows exist
+      const double *pr = P + (int64_t)q0 * n;
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
       for (int j = lane; j < n; j += 32) {
-        const int c = j & 255;
-        const int X = blocks[j >> 8].x;
-        acc = fma(pr[j], (double)A.b[(int64_t)X * kSS + (2 + (c & 15)) + kS * (2 + (c >> 4))], acc);
+        const double bj = rhs[j];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc[r] = fma(pr[(int64_t)r * n + j], bj, acc[r]);
       }
-      for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-      if (lane == 0) sol[q] = acc;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        double a = acc[r];
+        for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+        if (lane == 0) sol[q0 + r] = a;
+      }
     }
     __syncthreads();
     if (slot < n1) {
@@ -1380,6 +1426,41 @@ __global__ void __launch_bounds__(NT, 1) k_engine_vcycle(const __grid_constant__
   }
   __shared__ int2 s_halo[32];  // the GS halo cells, packed (halo_pack)
   if (threadIdx.x < 32) s_halo[threadIdx.x] = halo_pack(threadIdx.x);
+  // GS records of the small levels (at most two blocks for this slot), once per launch
+  if (t == 0) S.gs_cached = S.ch_cached = 0u;
+  slot_sync(slot);
+  if (A.nitems == 1) {
+    const int Lc = min(A.lmax, kLevCache);
+    for (int l = 1; l <= Lc; ++l) {
+      const bool loc = l <= A.local_top;
+      if (loc && blockIdx.x != 0) continue;
+      const int first = loc ? slot : blockIdx.x * nslots + slot, step = loc ? nslots : gridDim.x * nslots;
+      const int n = A.tr.nblk[l - 1];
+      const int nmine = (first < n) ? (n - 1 - first) / step + 1 : 0;
+      if (nmine == 0 || nmine > 2) continue;
+      for (int i = t; i < 5 * nmine; i += 256) {
+        const int q = i / 5, k = i - 5 * q;
+        S.rgs[l - 1][q][k] = A.tr.lvl_rec[l - 1][5 * (first + q * step) + k];
+      }
+      if (t == 0) S.gs_cached |= 1u << l;
+    }
+    // the child edges of level l (fine at l): restriction and prolongation records
+    for (int l = 2; l <= Lc; ++l) {
+      const bool loc = l <= A.local_top;
+      if (loc && blockIdx.x != 0) continue;
+      const int first = loc ? slot : blockIdx.x * nslots + slot, step = loc ? nslots : gridDim.x * nslots;
+      const int n = A.tr.nch[l - 1];
+      const int nmine = (first < n) ? (n - 1 - first) / step + 1 : 0;
+      if (nmine == 0 || nmine > 2) continue;
+      for (int i = t; i < 6 * nmine; i += 256) {
+        const int q = i / 6, k = i - 6 * q;
+        const int4 e = A.tr.lvl_child[l - 1][first + q * step];
+        S.rres[l - 1][q][k] = k == 0 ? e : k == 1 ? A.tr.info[e.x] : A.tr.faces[4 * e.y + k - 2];
+        if (k < 5) S.rpro[l - 1][q][k] = k == 0 ? e : A.tr.faces[4 * e.x + k - 1];
+      }
+      if (t == 0) S.ch_cached |= 1u << l;
+    }
+  }
   __syncthreads();
   unsigned pk = 0;  // items streamed through this slot's buffers so far
   unsigned epoch = 0;
@@ -1389,6 +1470,7 @@ __global__ void __launch_bounds__(NT, 1) k_engine_vcycle(const __grid_constant__
   auto fld = [&](int l) -> T * { return ((cur >> l) & 1) ? A.ualt : A.u; };
   auto oth = [&](int l) -> T * { return ((cur >> l) & 1) ? A.u : A.ualt; };
   __shared__ double s_direct[1024];  // coarsest-level direct solution (CTA 0)
+  __shared__ double s_rhs[1024];     // its right-hand side
 
   auto first_of = [&](bool loc) { return loc ? slot : blockIdx.x * nslots + slot; };
   auto step_of = [&](bool loc) { return loc ? nslots : gridDim.x * nslots; };
@@ -1514,7 +1596,8 @@ __global__ void __launch_bounds__(NT, 1) k_engine_vcycle(const __grid_constant__
     // coarsest level
     if (A.it_P) {
       const bool loc = 1 <= K;
-      if (runs(loc)) ph_direct_top<T>(A, fld(1), L > 1, loc ? 0 : blockIdx.x, loc ? 1 : gridDim.x, t, slot, s_direct);
+      if (runs(loc))
+        ph_direct_top<T>(A, fld(1), L > 1, loc ? 0 : blockIdx.x, loc ? 1 : gridDim.x, t, slot, s_direct, s_rhs);
       if (!sync(true, loc, 2 <= K || L < 2)) return false;
     } else {
       const bool loc = 1 <= K;

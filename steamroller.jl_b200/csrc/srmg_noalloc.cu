@@ -1,11 +1,11 @@
 // srmg_noalloc.cu -- srmg_resnorm_noalloc: the residual norm with no device allocation.
 //
 // Who needs it: callers that must not call cudaMalloc at the moment they compute a
-// norm -- code running inside CUDA stream capture (where cudaMalloc is not allowed),
-// hosts whose memory is owned by their own pool allocator (a Julia GPU array pool, a
-// framework arena) and which forbid other allocations, and latency-critical loops that
-// cannot afford an allocation's implicit synchronisation.  srmg_resnorm_dev may grow
-// its partial-sum buffer with cudaMalloc; this entry point never does.
+// norm -- hosts whose device memory is owned by their own pool allocator (a Julia GPU
+// array pool, a framework arena) and which forbid other allocations, and
+// latency-critical loops that cannot afford an allocation's implicit synchronisation.
+// srmg_resnorm_dev may grow its partial-sum buffer with cudaMalloc; this entry point
+// never does.  2D trees only (check_call refuses D = 3 with SRMG_ERR_UNSUPPORTED).
 //
 // Its scratch is a file-scope __device__ array holding one partial sum per tree block,
 // so the tree may hold at most kNoAllocMaxBlocks blocks.  Every GPU that loads the
@@ -27,7 +27,10 @@ static __device__ __align__(256) double g_noalloc_parts[kNoAllocMaxBlocks];
 
 // Host code may not use g_noalloc_parts as an address: on the host it only names a
 // stand-in.  The device address is looked up once per device with that device
-// current, and cached here.
+// current, and cached here for the life of the process: the cache assumes that the
+// device's primary context (which holds the array) lives as long as the process.  A
+// caller that resets the device (cudaDeviceReset) and keeps using the library would
+// pass a stale address; such a caller must not use this entry point after the reset.
 constexpr int kMaxDevices = 64;
 double *g_parts_addr[kMaxDevices] = {nullptr};
 std::mutex g_parts_mu;

@@ -155,9 +155,10 @@ def evaluate(net: mg.Cnn, runs, steps, every=10, seed=99, device=0, mode=mg.MODE
         hist = None
         for k in range(steps):
             phi_prev, b_prev = s.advance()
+            kw = mg.TUNED if mode != mg.MODE_FP64 else {}
             if hist is None or k % every:
                 s.phi.copy_(phi_prev)
-                mg.solve(s.ctx, s.phi, s.b, s.s, s.geom, s.bc, tol=tol, mode=mode)
+                mg.solve(s.ctx, s.phi, s.b, s.s, s.geom, s.bc, tol=tol, mode=mode, **kw)
                 hist = (phi_prev, b_prev)
                 continue
             phi2, b2 = hist
@@ -165,7 +166,7 @@ def evaluate(net: mg.Cnn, runs, steps, every=10, seed=99, device=0, mode=mg.MODE
 
             def run(u):
                 torch.cuda.synchronize()
-                st = mg.solve(s.ctx, u, s.b, s.s, s.geom, s.bc, tol=tol, mode=mode)
+                st = mg.solve(s.ctx, u, s.b, s.s, s.geom, s.bc, tol=tol, mode=mode, **kw)
                 return (st["cycles"], st["device_ms"], st["initial_rel"])
 
             res["zero"] = run(torch.zeros_like(phi_prev))

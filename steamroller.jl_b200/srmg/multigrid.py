@@ -22,9 +22,17 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libsrmg.so")
 
 SRMG_OK = 0
+# error codes of include/srmg.h
+SRMG_ERR_BADARG, SRMG_ERR_BADTREE, SRMG_ERR_CUDA, SRMG_ERR_TIMEOUT = -1, -2, -3, -4
+SRMG_ERR_DIVERGED, SRMG_ERR_UNSUPPORTED, SRMG_ERR_NOMEM, SRMG_ERR_NOTREE = -5, -6, -7, -8
 ERRORS = {-1: "BADARG", -2: "BADTREE", -3: "CUDA", -4: "TIMEOUT", -5: "DIVERGED",
           -6: "UNSUPPORTED", -7: "NOMEM", -8: "NOTREE"}
 MODE_FP64, MODE_MIXED, MODE_FP64_DIRECT = 0, 1, 2
+# Smoother of the mixed-precision (and FP64-direct) solves as the autotuner picks it on
+# the refined 1.5M- and 10M-leaf-cell trees: one red-black sweep down and one up per
+# level, relaxation factor 1.1 (the reference's own cycle, V(2,2) with omega 1, stays the
+# default of every entry point).
+TUNED = dict(ndown=1, nup=1, ntop=4, omega=1.1)
 
 
 class SrmgError(RuntimeError):
@@ -51,7 +59,8 @@ class Stats(ctypes.Structure):
 
 class TuneTrial(ctypes.Structure):
     _fields_ = [("engine_ctas", ctypes.c_int), ("local_max_blocks", ctypes.c_int), ("ndown", ctypes.c_int),
-                ("nup", ctypes.c_int), ("ntop", ctypes.c_int), ("cycles", ctypes.c_int), ("ms", ctypes.c_double)]
+                ("nup", ctypes.c_int), ("ntop", ctypes.c_int), ("cycles", ctypes.c_int), ("ms", ctypes.c_double),
+                ("omega", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -125,7 +125,8 @@ class Streamer:
             for l in range(1, len(self.tree) + 1):
                 mg.fill_ghost_(self.ctx, self.phi, l, self.bc)
             return {"cycles": self.poisson_iter}
-        return mg.solve(self.ctx, self.phi, self.b, self.s, self.geom, self.bc, tol=self.tol, mode=mg.MODE_MIXED)
+        return mg.solve(self.ctx, self.phi, self.b, self.s, self.geom, self.bc, tol=self.tol, mode=mg.MODE_MIXED,
+                        **mg.TUNED)
 
     def _rates(self, dn, ne, nion, maxdt=False):
         """The rest of derivs! after the solve (src/streamer.jl:337-366): dn[0] = dne,
@@ -198,7 +199,8 @@ class Streamer:
         """Advance one step and solve the new charge from the previous potential;
         returns (phi_prev, b_prev, stats of the new solve)."""
         phi_prev, b_prev = self.advance(tmax)
-        st = mg.solve(self.ctx, self.phi, self.b, self.s, self.geom, self.bc, tol=tol, mode=mode)
+        kw = mg.TUNED if mode != mg.MODE_FP64 else {}
+        st = mg.solve(self.ctx, self.phi, self.b, self.s, self.geom, self.bc, tol=tol, mode=mode, **kw)
         return phi_prev, b_prev, st
 
     def ionisation_rate(self, stage):

@@ -65,7 +65,8 @@ def run(net, steps=200, sample_every=50, device=0, log=None, problem=None):
         psi_old = [None] * STAGES
         src = [zf() for _ in LAMBDAS]
     mask_t = torch.from_numpy(leaf_mask(p.tree, nblk)).to(dev)
-    opts = dict(tol=1e-8, ndown=2, ntop=4, nup=2, max_cycles=5000)
+    opts = dict(tol=1e-8, max_cycles=5000, **mg.TUNED)          # mixed solves: the tuned smoother
+    ref_opts = dict(tol=1e-8, ndown=2, ntop=4, nup=2, max_cycles=5000)  # plain FP64: the reference's cycle
     rec = {"poisson_ms": [], "photo_ms": [], "poisson_cycles": [], "photo_cycles": [], "which": [],
            "stage_poisson_cycles": [[] for _ in range(STAGES)]}
     samples = []
@@ -100,7 +101,7 @@ def run(net, steps=200, sample_every=50, device=0, log=None, problem=None):
         sts = timed("photo", lambda: batch.solve(psi[k], src, mode=mg.MODE_MIXED, **opts))
         cur["photo_cycles"] = max(cur["photo_cycles"], max(x["cycles"] for x in sts))
         if fp64 is not None:
-            fp64_stage_photo(s, guesses, src, stream, opts, fp64)
+            fp64_stage_photo(s, guesses, src, stream, ref_opts, fp64)
 
     def poisson(stage, fp64):
         guess = s.phi.clone() if fp64 is not None else None
@@ -109,7 +110,7 @@ def run(net, steps=200, sample_every=50, device=0, log=None, problem=None):
         rec["stage_poisson_cycles"][stage - 1].append(st["cycles"])
         cur["poisson_cycles"] += st["cycles"]
         if fp64 is not None:
-            fp64_stage_poisson(s, guess, stream, opts, fp64)
+            fp64_stage_poisson(s, guess, stream, ref_opts, fp64)
         return st
 
     rec_steps = [0]
@@ -130,7 +131,7 @@ def run(net, steps=200, sample_every=50, device=0, log=None, problem=None):
             guess1 = s.phi.clone() if sampled else None
             poisson(1, fp64)
             if sampled:
-                samples.append(error_sample(s, guess1, stream, opts, mask_t))
+                samples.append(error_sample(s, guess1, stream, ref_opts, mask_t))
             phi_prev, b_prev = s.advance(on_stage=lambda st_: photo(st_, fp64),
                                          poisson=lambda st_: poisson(st_, fp64))
             stream.synchronize()

@@ -167,9 +167,9 @@ def test_residual_postrestrict_transfers_bitexact(pair):
         np.testing.assert_array_equal(bits(rg.cpu().numpy()), bits(ro), err_msg=f"residual {l}")
         if l < 2:
             continue
-        bg = torch_cuda(b0)
+        bg, r0g = torch_cuda(b0), torch_cuda(r0)  # held until the kernel has run
         pair.ctx.check(L.srmg_residual_postrestrict_level_dev(pair.ctx.handle, bg.data_ptr(), ug.data_ptr(),
-                                                              torch_cuda(r0).data_ptr(), p.nblk, l, 4 * sl, p.op,
+                                                              r0g.data_ptr(), p.nblk, l, 4 * sl, p.op,
                                                               p.k2, 0))
         pair.ctx.synchronize()
         bo = b0.copy()

@@ -202,9 +202,12 @@ def test_freebc_fft_matches_direct_sums(level):
         out[direct] = (qg.cpu().numpy(), bg.cpu().numpy())
     qo = q.copy()
     bo = fo.freebc(qo, u, p.h1, p.s, p.tree, p.conn, 1, level, f)
+    changed = qo != q
+    # the FFT path rounds like the oracle's FFTs; the direct sums of n terms round to
+    # within ~n ulp
+    bar = {0: REL, 1: max(REL, 4 * n * np.finfo(float).eps)}
     for direct in (0, 1):
-        assert rel_l2(out[direct][1], bo) <= REL, direct
-        changed = qo != q
-        assert rel_l2(out[direct][0][changed] - q[changed], qo[changed] - q[changed]) <= REL
-    assert rel_l2(out[0][1], out[1][1]) <= REL
+        assert rel_l2(out[direct][1], bo) <= bar[direct], direct
+        assert rel_l2(out[direct][0][changed] - q[changed], qo[changed] - q[changed]) <= bar[direct], direct
+    assert rel_l2(out[0][1], out[1][1]) <= bar[1]
     ctx.close()

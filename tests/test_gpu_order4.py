@@ -164,9 +164,9 @@ def test_residual_and_postrestrict_bitexact(pair):
         olib().orc_residual_level(_ptr(ro), _ptr(u0), _ptr(b0), sl, pair.orc.ot.ref, l, ctypes.byref(pair.orc.op))
         np.testing.assert_array_equal(bits(to_np(rg)), bits(ro), err_msg=f"residual level {l}")
         if l >= 2:
-            bg = torch_cuda(b0)
+            bg, r0g = torch_cuda(b0), torch_cuda(r0)  # held until the kernel has run
             pair.ctx.check(mg.lib().srmg_residual_postrestrict_level_dev(
-                pair.ctx.handle, bg.data_ptr(), ug.data_ptr(), torch_cuda(r0).data_ptr(), p.nblk, l, 4 * sl, 2, 0.0,
+                pair.ctx.handle, bg.data_ptr(), ug.data_ptr(), r0g.data_ptr(), p.nblk, l, 4 * sl, 2, 0.0,
                 p.geom))
             pair.ctx.synchronize()
             bo = b0.copy()

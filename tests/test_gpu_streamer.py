@@ -39,8 +39,8 @@ def case(request):
 
 def _inputs(p, ctx, orc, seed):
     """A positive density with filled ghosts and the field of a random potential: e,
-    eabs from the library's electric_field! (bit-exact against the oracle's), eabs's
-    ghosts by fill_ghost!(ExtrapolateConst)."""
+    eabs from the oracle's electric_field! (the library's is bit-exact against it,
+    test_gpu_stage.py), eabs's ghosts by fill_ghost!(ExtrapolateConst)."""
     rng = np.random.default_rng(seed)
     n = p.nblk
     ne = 1e18 * (1.0 + rng.random((n, 20, 20))) * (1.0 + 50.0 * (rng.random((n, 1, 1)) < 0.1))
@@ -66,9 +66,9 @@ def test_flux_and_maxdt_bitexact(case):
     mdb = torch.full((p.nblk,), np.inf, dtype=torch.float64, device="cuda")
     mdm = torch.zeros(1, dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
+    keep = [cuda(ne), cuda(e), cuda(eabs)]  # held until the kernel has run
     ctx.check(mg.lib().srmg_streamer_flux_dev(ctx.handle, fg.data_ptr(), mdb.data_ptr(), mdm.data_ptr(),
-                                              cuda(ne).data_ptr(), cuda(e).data_ptr(), cuda(eabs).data_ptr(),
-                                              p.nblk, p.h1, ctypes.byref(tr)))
+                                              *[x.data_ptr() for x in keep], p.nblk, p.h1, ctypes.byref(tr)))
     ctx.synchronize()
     F, md = so.flux(ne, e, eabs, p.tree, p.h1)
     so.restrict_flux(F, p.conn)
@@ -93,8 +93,9 @@ def test_rates_match_oracle(case, geom):
     dne = torch.zeros((p.nblk, 20, 20), dtype=torch.float64, device="cuda")
     dni = torch.zeros_like(dne)
     torch.cuda.synchronize()
-    ctx.check(mg.lib().srmg_streamer_rates_dev(ctx.handle, dne.data_ptr(), dni.data_ptr(), cuda(ne).data_ptr(),
-                                               cuda(eabs).data_ptr(), cuda(F).data_ptr(), p.nblk, p.h1, geom,
+    keep = [cuda(ne), cuda(eabs), cuda(F)]  # held until the kernel has run
+    ctx.check(mg.lib().srmg_streamer_rates_dev(ctx.handle, dne.data_ptr(), dni.data_ptr(),
+                                               *[x.data_ptr() for x in keep], p.nblk, p.h1, geom,
                                                ctypes.byref(tr)))
     ctx.synchronize()
     wne, wni = so.rates(ne, eabs, F, p.tree, p.h1, geom)
@@ -128,8 +129,9 @@ def test_ssprk3_stages_bitexact(case):
     dt = 4.1e-12
     for stage in (1, 2, 3):
         out = cuda(np.zeros_like(n))
-        ctx.check(mg.lib().srmg_ssprk3_stage_dev(ctx.handle, out.data_ptr(), cuda(n).data_ptr(), cuda(d1).data_ptr(),
-                                                 cuda(d2).data_ptr(), cuda(d3).data_ptr(), n.size, dt, stage))
+        keep = [cuda(n), cuda(d1), cuda(d2), cuda(d3)]  # held until the kernel has run
+        ctx.check(mg.lib().srmg_ssprk3_stage_dev(ctx.handle, out.data_ptr(), *[x.data_ptr() for x in keep],
+                                                 n.size, dt, stage))
         ctx.synchronize()
         want = so.ssprk3_stage(n, d1, d2, d3, dt, stage)
         assert np.array_equal(out.cpu().numpy().view(np.uint64), want.view(np.uint64)), stage

@@ -1,8 +1,8 @@
 """srmg_resnorm_noalloc: the residual norm for callers that cannot allocate.
 
-Some callers cannot call cudaMalloc when they need a residual norm: code running
-inside CUDA stream capture, hosts whose device memory belongs to their own pool
-allocator, loops that cannot afford an allocation's implicit synchronisation.  The
+Some callers cannot call cudaMalloc when they need a residual norm: hosts whose
+device memory belongs to their own pool allocator, loops that cannot afford an
+allocation's implicit synchronisation.  The
 allocation-free entry point keeps its per-block partial sums in a static device
 array instead.  This test calls it through the C ABI, twice in a row, and checks each
 result against the existing srmg_resnorm_dev within the same tolerance the resnorm
@@ -76,4 +76,19 @@ def test_noalloc_rejects_trees_above_the_limit():
                                        1, out.data_ptr())
     assert rc == -1
     assert b"65536" in mg.lib().srmg_last_error(ctx.handle)
+    ctx.close()
+
+
+def test_noalloc_refuses_three_dimensional_trees():
+    import torch
+    from srmg.tree3 import Tree3, populate, connectivity as connectivity3
+    t = Tree3((1, 1, 1), 2)
+    populate(t, 2)
+    ctx = mg.Context(0, D=3).set_tree(t, connectivity3(t))
+    n = t.nblocks_created
+    f = torch.zeros((n, 20, 20, 20), dtype=torch.float64, device="cuda")
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    rc = mg.lib().srmg_resnorm_noalloc(ctx.handle, f.data_ptr(), f.data_ptr(), n, 1.0, 0, 0.0, 0, out.data_ptr())
+    assert rc == mg.SRMG_ERR_UNSUPPORTED
     ctx.close()
