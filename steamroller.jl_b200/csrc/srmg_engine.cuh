@@ -1081,7 +1081,7 @@ __device__ void ph_update64(const EngArgs<T> &A, int t, int gslot, int gstep) {
 // The four 64-thread quarters of a slot take one child edge each, two rounds per pass
 // with every load issued before the stores.
 template <typename T>
-__device__ void ph_restrict64(const EngArgs<T> &A, int l, int t, int gslot, int gstep) {
+__device__ void ph_restrict64(const EngArgs<T> &A, int l, int t, int gslot, int gstep, bool all = false) {
   constexpr int R = 2;
   const int n = A.tr.nch[l - 1];
   const int4 *ch = A.tr.lvl_child[l - 1];
@@ -1113,7 +1113,7 @@ __device__ void ph_restrict64(const EngArgs<T> &A, int l, int t, int gslot, int 
     }
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-      if (!on[k] || is_frozen(A, item[k])) continue;
+      if (!on[k] || (!all && is_frozen(A, item[k]))) continue;
       const int cx = 2 + 8 * (e[k].z - 1) + kx, cy = 2 + 8 * (e[k].w - 1) + ky;
       A.mx.u64[(int64_t)e[k].y * kSS + cx + kS * cy] = v[k];
       push_tw<double>((unsigned)A.it_sgbits[item[k]], A.mx.u64, e[k].y, fx[k], fy[k], cx, cy, v[k]);
@@ -1121,10 +1121,48 @@ __device__ void ph_restrict64(const EngArgs<T> &A, int l, int t, int gslot, int 
   }
 }
 
+// The restriction of u64 onto every covered cell whose four children are leaf cells,
+// for all levels in one phase: a 64-thread quarter of a slot takes one child edge (of
+// any level), each thread one 2 x 2 group of the fine block, skipped when the fine
+// block has a child over that group.  It reads only leaf cells, which no thread of the
+// phase writes, so the levels need no order.  These are the only covered cells a leaf
+// cell's stencil reads (directly, through a neighbour's copy ghost, or through the
+// refinement ghosts of a finer block): under the tree's 2:1 nesting a covered cell next
+// to a leaf region, or next to a refinement boundary, has leaf children.  So the
+// defect of the mixed solve needs only this phase between two defects; the deeper
+// covered cells keep stale values until the full chain (ph_restrict64, level by level)
+// at the end of the solve makes u64 a composite-grid function again.  The values are
+// the chain's own (same order of the four additions), so the iterates do not change.
+template <typename T>
+__device__ void ph_restrict64_leaf(const EngArgs<T> &A, int t, int gslot, int gstep) {
+  const int quarter = t >> 6, c = t & 63, kx = c & 7, ky = c >> 3;
+  int total = 0;
+  for (int l = 2; l <= A.lmax; ++l) total += A.tr.nch[l - 1];
+  for (int i = 4 * gslot + quarter; i < total; i += 4 * gstep) {
+    int l = 2, off = i;
+    while (off >= A.tr.nch[l - 1]) {
+      off -= A.tr.nch[l - 1];
+      ++l;
+    }
+    const int4 e = A.tr.lvl_child[l - 1][off];  // {fine, coarse, sb_r, sb_z}
+    const int fsub = (kx >> 2) + 2 * (ky >> 2);
+    if ((A.tr.info[e.x].z >> fsub) & 1) continue;  // the fine block has a child over this group
+    const int item = A.tr.info[e.y].z >> 8;
+    if (is_frozen(A, item)) continue;
+    const double v = restrict4<double>(A.mx.u64 + (int64_t)e.x * kSS, 2 + 2 * kx, 2 + 2 * ky);
+    const int cx = 2 + 8 * (e.z - 1) + kx, cy = 2 + 8 * (e.w - 1) + ky;
+    int2 fx = make_int2(FACE_NONE, -1), fy = make_int2(FACE_NONE, -1);
+    if (cx <= 3 || cx >= 16) fx = face_tw(A.tr.faces + 4 * e.y, cx <= 3 ? 0 : 1);
+    if (cy <= 3 || cy >= 16) fy = face_tw(A.tr.faces + 4 * e.y, cy <= 3 ? 2 : 3);
+    A.mx.u64[(int64_t)e.y * kSS + cx + kS * cy] = v;
+    push_tw<double>((unsigned)A.it_sgbits[item], A.mx.u64, e.y, fx, fy, cx, cy, v);
+  }
+}
+
 // Refinement-boundary ghosts of u64 on level l from level l - 1: the two halves of a slot
 // take one block each, two rounds per pass, loads before stores.
 template <typename T>
-__device__ void ph_refbnd64(const EngArgs<T> &A, int l, int t, int gslot, int gstep) {
+__device__ void ph_refbnd64(const EngArgs<T> &A, int l, int t, int gslot, int gstep, bool all = false) {
   constexpr int R = 2;
   const int n = A.tr.nblk[l - 1];
   const int4 *blocks = A.tr.lvl_blocks[l - 1];
@@ -1139,7 +1177,7 @@ __device__ void ph_refbnd64(const EngArgs<T> &A, int l, int t, int gslot, int gs
       fi[k] = make_int4(FACE_NONE, 0, 0, -1);
       if (ik < n) {
         const int4 bk = blocks[ik];
-        if (!is_frozen(A, item_of(bk))) {
+        if (all || !is_frozen(A, item_of(bk))) {
           X[k] = bk.x;
           fi[k] = A.tr.faces[4 * bk.x + (q >> 5)];
         }
@@ -1656,8 +1694,8 @@ __global__ void __launch_bounds__(NT, 1) k_engine_vcycle(const __grid_constant__
         ph_update64<T>(A, t, gslot, gstep);
         if (!sync(true, false, false)) return;
       }
-      for (int l = L; l >= 2; --l) {
-        ph_restrict64<T>(A, l, t, gslot, gstep);
+      if (L >= 2) {
+        ph_restrict64_leaf<T>(A, t, gslot, gstep);
         if (!sync(true, false, false)) return;
       }
       for (int l = 2; l <= L; ++l)
@@ -1667,7 +1705,22 @@ __global__ void __launch_bounds__(NT, 1) k_engine_vcycle(const __grid_constant__
         }
       if (!norm_step(true, iter == 0, cycles)) return;
     }
-    if (loop && (!any_live() || cycles >= A.max_cycles)) break;
+    if (loop && (!any_live() || cycles >= A.max_cycles)) {
+      if (mixed) {
+        // u64 a composite-grid function of its leaves again, every item: the full
+        // restriction chain, level by level, and the refinement ghosts
+        for (int l = L; l >= 2; --l) {
+          ph_restrict64<T>(A, l, t, gslot, gstep, true);
+          if (!sync(true, false, false)) return;
+        }
+        for (int l = 2; l <= L; ++l)
+          if ((A.mx.refbnd_levels >> l) & 1) {
+            ph_refbnd64<T>(A, l, t, gslot, gstep, true);
+            if (!sync(true, false, false)) return;
+          }
+      }
+      break;
+    }
     // mixed: up to A.inner FP32 V-cycles on the same defect, the correction carried over
     const int nv = (mixed && loop) ? inner_now() : 1;
     for (int k = 0; k < nv; ++k) {

@@ -336,9 +336,11 @@ int gridfor(int64_t work, int threads) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 8));
 }
 
-// The context's free-boundary buffer: f [n], the sine table [4n], u1 [n], b [n], and for
-// the FFT path the twiddles [n complex] and three complex work arrays [n each].
-constexpr int64_t kFbcDoubles = 13;
+// The context's free-boundary buffer: f [n], the sine table [4n], u1 [n], b [n] (7n
+// doubles), and for the FFT path the twiddles [n complex] and three complex work arrays
+// [n complex each] (8n doubles): 15n doubles in all.
+constexpr int64_t kFbcDoubles = 7 + 2 * (1 + 3);
+static_assert(kFbcDoubles == 15, "free-boundary buffer layout");
 double *fbc_f(srmg_ctx *ctx) { return (double *)ctx->fbc.p; }
 double *fbc_tab(srmg_ctx *ctx) { return fbc_f(ctx) + ctx->fbc_n; }
 double *fbc_u1(srmg_ctx *ctx) { return fbc_tab(ctx) + 4 * ctx->fbc_n; }
