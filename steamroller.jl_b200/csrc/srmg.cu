@@ -10,6 +10,7 @@
 
 #include "srmg_ctx.h"
 #include "srmg_internal.h"
+#include "srmg_seq.cuh"
 
 using namespace srmg;
 
@@ -84,6 +85,9 @@ extern "C" int srmg_create(srmg_ctx **out, int D, int M, int G, int device) {
 }
 
 void srmg::drop_op_graphs(srmg_ctx *ctx) {
+  for (auto &q : ctx->op_seqs)
+    if (q.ops.p) cudaFree(q.ops.p);
+  ctx->op_seqs.clear();
   for (auto &g : ctx->op_graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   ctx->op_graphs.clear();
@@ -98,6 +102,7 @@ void srmg::free_tree(srmg_ctx *ctx) {
   ctx->nblk_host.clear();
   ctx->nch_host.clear();
   ctx->has_tree = false;
+  ctx->fbc_built = false;
 }
 
 extern "C" void srmg_destroy(srmg_ctx *ctx) {
@@ -120,6 +125,7 @@ extern "C" void srmg_destroy(srmg_ctx *ctx) {
   if (ctx->sync.p) cudaFree(ctx->sync.p);
   if (ctx->trace.p) cudaFree(ctx->trace.p);
   if (ctx->fbc.p) cudaFree(ctx->fbc.p);
+  if (ctx->fbc_tabs.p) cudaFree(ctx->fbc_tabs.p);
   if (ctx->h_small) cudaFreeHost(ctx->h_small);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -679,6 +685,30 @@ double srmg::level_scale(double s, int l) {
   return s / (double)(f * f);
 }
 
+// While a sequence is being recorded (ctx->seq_rec set, FP64 only) the launchers below
+// append their operation instead of launching it.
+template <typename T>
+static bool seq_push(srmg_ctx *ctx, int kind, int i0, int i1, T *a, const T *b, const T *c, const LevelView &lv,
+                     const OpParams<T> *p, const Signs *sg) {
+  if (!ctx->seq_rec) return false;
+  if (sizeof(T) != sizeof(double)) return false;  // only FP64 cycles are recorded
+  SeqOp<T> op;
+  memset(&op, 0, sizeof op);
+  op.kind = kind;
+  op.i0 = i0;
+  op.i1 = i1;
+  op.a = a;
+  op.b = b;
+  op.c = c;
+  op.lv = lv;
+  if (p) op.p = *p;
+  if (sg) op.sg = *sg;
+  const char *q = reinterpret_cast<const char *>(&op);
+  ctx->seq_rec->insert(ctx->seq_rec->end(), q, q + sizeof op);
+  ctx->launches++;
+  return true;
+}
+
 template <typename T>
 int srmg::L_fill_ghost(srmg_ctx *ctx, T *u, int l, const Signs &sg, int mask) {
   const DevLevel &L = ctx->lv[l - 1];
@@ -688,6 +718,7 @@ int srmg::L_fill_ghost(srmg_ctx *ctx, T *u, int l, const Signs &sg, int mask) {
   if (!L.cfaces) {
     // star faces only: the three passes touch disjoint cells and read none of each
     // other's results, so one launch does them all
+    if (seq_push<T>(ctx, SEQ_FILL, mask, 0, u, nullptr, nullptr, L.view(l), nullptr, &sg)) return SRMG_OK;
     k_fill_ghost<T><<<gf, threads, 0, ctx->stream>>>(u, L.view(l), sg, mask);
     ctx->launches++;
     return SRMG_OK;
@@ -698,6 +729,7 @@ int srmg::L_fill_ghost(srmg_ctx *ctx, T *u, int l, const Signs &sg, int mask) {
   // faces and corners of its pass
   for (int phase = 1; phase <= 4; phase <<= 1) {
     if (!(mask & phase)) continue;
+    if (seq_push<T>(ctx, SEQ_FILL, phase, 0, u, nullptr, nullptr, L.view(l), nullptr, &sg)) continue;
     k_fill_ghost<T><<<gf, threads, 0, ctx->stream>>>(u, L.view(l), sg, phase);
     ctx->launches++;
   }
@@ -711,11 +743,13 @@ int srmg::L_gs_colour(srmg_ctx *ctx, T *u, const T *b, int l, const OpParams<T> 
   const int threads = 128;
   if (p.op == SRMG_OP_LAPLACIAN4) {
     // FourColors{parity >> 1, parity & 1}
+    if (seq_push<T>(ctx, SEQ_GS4, parity >> 1, parity & 1, u, b, nullptr, L.view(l), &p, nullptr)) return SRMG_OK;
     k_gs4<T><<<grid_for((int64_t)L.nblk * 64, threads, kGridCap), threads, 0, ctx->stream>>>(
         u, b, L.view(l), p, parity >> 1, parity & 1);
     ctx->launches++;
     return SRMG_OK;
   }
+  if (seq_push<T>(ctx, SEQ_GS_COLOUR, parity, 0, u, b, nullptr, L.view(l), &p, nullptr)) return SRMG_OK;
   k_gs_colour<T><<<grid_for((int64_t)L.nblk * 128, threads, kGridCap), threads, 0, ctx->stream>>>(
       u, b, L.view(l), p, wtab<T>(ctx), parity);
   ctx->launches++;
@@ -748,6 +782,7 @@ template <typename T>
 int srmg::L_residual(srmg_ctx *ctx, T *r, const T *u, const T *b, int l, const OpParams<T> &p) {
   const DevLevel &L = ctx->lv[l - 1];
   if (L.nblk == 0) return SRMG_OK;
+  if (seq_push<T>(ctx, SEQ_RESIDUAL, 0, 0, r, u, b, L.view(l), &p, nullptr)) return SRMG_OK;
   k_residual<T><<<grid_for((int64_t)L.nblk * 256, 256, kGridCap), 256, 0, ctx->stream>>>(
       r, u, b, L.view(l), p, wtab<T>(ctx));
   ctx->launches++;
@@ -758,6 +793,7 @@ template <typename T>
 int srmg::L_postrestrict(srmg_ctx *ctx, T *bf, const T *u, const T *r, int l, const OpParams<T> &pc) {
   const DevLevel &L = ctx->lv[l - 1];
   if (L.nch == 0) return SRMG_OK;
+  if (seq_push<T>(ctx, SEQ_POSTRESTRICT, 0, 0, bf, u, r, L.view(l), &pc, nullptr)) return SRMG_OK;
   k_postrestrict<T><<<grid_for((int64_t)L.nch * 64, 256, kGridCap), 256, 0, ctx->stream>>>(
       bf, u, r, L.view(l), ctx->d_coord_of, pc, wtab<T>(ctx));
   ctx->launches++;
@@ -768,6 +804,7 @@ template <typename T>
 int srmg::L_restrict(srmg_ctx *ctx, T *u, int l) {
   const DevLevel &L = ctx->lv[l - 1];
   if (L.nch == 0) return SRMG_OK;
+  if (seq_push<T>(ctx, SEQ_RESTRICT, 0, 0, u, nullptr, nullptr, L.view(l), nullptr, nullptr)) return SRMG_OK;
   k_restrict<T><<<grid_for((int64_t)L.nch * 64, 256, kGridCap), 256, 0, ctx->stream>>>(u, L.view(l));
   ctx->launches++;
   return SRMG_OK;
@@ -777,6 +814,7 @@ template <typename T>
 int srmg::L_interp_add(srmg_ctx *ctx, T *u, const T *u1, int l) {
   const DevLevel &L = ctx->lv[l - 1];
   if (L.nch == 0) return SRMG_OK;
+  if (seq_push<T>(ctx, SEQ_INTERP_ADD, 0, 0, u, u1, nullptr, L.view(l), nullptr, nullptr)) return SRMG_OK;
   k_interp_add<T><<<grid_for((int64_t)L.nch * 256, 256, kGridCap), 256, 0, ctx->stream>>>(
       u, u1, L.view(l));
   ctx->launches++;
@@ -787,6 +825,7 @@ template <typename T>
 int srmg::L_copy(srmg_ctx *ctx, T *dst, const T *src, int l) {
   const DevLevel &L = ctx->lv[l - 1];
   if (L.nblk == 0) return SRMG_OK;
+  if (seq_push<T>(ctx, SEQ_COPY, 0, 0, dst, src, nullptr, L.view(l), nullptr, nullptr)) return SRMG_OK;
   k_copy_level<T><<<grid_for((int64_t)L.nblk * kSS, 256, kGridCap), 256, 0, ctx->stream>>>(
       dst, src, L.view(l));
   ctx->launches++;
@@ -797,6 +836,7 @@ template <typename T>
 int srmg::L_diff(srmg_ctx *ctx, T *dst, const T *a1, const T *a2, int l) {
   const DevLevel &L = ctx->lv[l - 1];
   if (L.nblk == 0) return SRMG_OK;
+  if (seq_push<T>(ctx, SEQ_DIFF, 0, 0, dst, a1, a2, L.view(l), nullptr, nullptr)) return SRMG_OK;
   k_diff_level<T><<<grid_for((int64_t)L.nblk * kSS, 256, kGridCap), 256, 0, ctx->stream>>>(
       dst, a1, a2, L.view(l));
   ctx->launches++;
@@ -817,8 +857,9 @@ int srmg::vcycle_dev(srmg_ctx *ctx, T *u, T *b, T *r, T *u1, double s, int op, d
                          reinterpret_cast<uintptr_t>(r) | reinterpret_cast<uintptr_t>(u1)) & 15) == 0;
   // The engine's ghost pushes cover the four star faces only; trees with corner ghosts
   // (BoxStencil connectivity) and the order-4 stencil use the per-operation kernels.
+  // (a sequence being recorded holds per-operation records only)
   if (ctx->use_engine && aligned && !ctx->has_corners && op != SRMG_OP_LAPLACIAN4 && ndown >= 1 &&
-      ntop >= 1 && nup >= 1 && ctx->nlev <= 30) {
+      ntop >= 1 && nup >= 1 && ctx->nlev <= 30 && !ctx->seq_rec) {
     ItemTabs tabs;
     const std::vector<ItemSpec> specs = uniform_items(ctx, s, op, k2, bc_of(sg).data());
     RC(prepare_items(ctx, specs.data(), geom, omega, false, 0, 0.0, &tabs));
@@ -948,6 +989,10 @@ extern "C" int srmg_set_option(srmg_ctx *ctx, const char *key, int64_t value) {
   else if (!strcmp(key, "b_copy_back")) ctx->b_copy_back = value != 0;
   else if (!strcmp(key, "freebc_direct")) ctx->fbc_direct = value != 0;
   else if (!strcmp(key, "graph")) ctx->use_graph = value != 0;
+  else if (!strcmp(key, "op_sequencer")) {
+    ctx->use_op_seq = value != 0;
+    if (!ctx->use_op_seq) drop_op_graphs(ctx);
+  }
   else if (!strcmp(key, "op_graphs")) {
     ctx->use_op_graphs = value != 0;
     if (!ctx->use_op_graphs) drop_op_graphs(ctx);
@@ -1009,7 +1054,8 @@ int srmg::vcycle_ops(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
   // a caller already capturing the stream records the launches into its own graph
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   CK(cudaStreamIsCapturing(ctx->stream, &cap));
-  if (!ctx->use_op_graphs || ncycles <= 0 || cap != cudaStreamCaptureStatusNone)
+  const bool seq = ctx->use_op_seq && ctx->D == 2;
+  if (!(ctx->use_op_graphs || seq) || ncycles <= 0 || cap != cudaStreamCaptureStatusNone)
     return run_vcycles(ctx, u, b, r, u1, s, op, k2, geom, bc, lmax, ndown, ntop, nup, omega, ncycles);
   std::vector<char> key;
   for (const void *p : {(const void *)u, (const void *)b, (const void *)r, (const void *)u1, (const void *)ctx->d_tree,
@@ -1020,6 +1066,35 @@ int srmg::vcycle_ops(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
   put(key, ctx->generation);
   const int nbc = ctx->D == 3 ? 27 : 9;
   for (int i = 0; i < nbc; i++) put(key, (int8_t)(bc ? bc[i] : 1));
+  if (seq) {
+    // the whole sequence as one cooperative launch of the sequencer: record it once per
+    // key (the launchers append their operations instead of launching), keep it on the
+    // device, launch it
+    for (auto &q : ctx->op_seqs)
+      if (q.key == key) return seq_launch(ctx, q.ops.p, q.nops);
+    std::vector<char> rec;
+    const int64_t l0 = ctx->launches;
+    ctx->seq_rec = &rec;
+    const int rc = run_vcycles(ctx, u, b, r, u1, s, op, k2, geom, bc, lmax, ndown, ntop, nup, omega, ncycles);
+    ctx->seq_rec = nullptr;
+    ctx->launches = l0;
+    if (rc) return rc;
+    if (ctx->op_seqs.size() >= kOpGraphs) {
+      if (ctx->op_seqs.front().ops.p) cudaFree(ctx->op_seqs.front().ops.p);
+      ctx->op_seqs.erase(ctx->op_seqs.begin());
+    }
+    srmg_ctx::OpSeq q;
+    q.key = key;
+    q.nops = (int)(rec.size() / seq_op_bytes());
+    if (q.nops > 0) {
+      RC(ensure(ctx, q.ops, rec.size()));
+      // on the context's stream: the launch below is ordered after the copy (pageable
+      // source, staged before the call returns)
+      CK(cudaMemcpyAsync(q.ops.p, rec.data(), rec.size(), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    ctx->op_seqs.push_back(q);
+    return seq_launch(ctx, q.ops.p, q.nops);
+  }
   for (auto &g : ctx->op_graphs)
     if (g.key == key) {
       CK(cudaGraphLaunch(g.exec, ctx->stream));

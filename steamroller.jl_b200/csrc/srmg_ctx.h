@@ -164,6 +164,17 @@ struct srmg_ctx {
   };
   std::vector<OpGraph> op_graphs;
   bool use_op_graphs = true;
+  // the same V-cycles as one cooperative launch of the sequencer (srmg_seq.cu): the
+  // recorded operations by key, at most kOpGraphs kept; while seq_rec is set the
+  // per-operation launchers append records (SeqOp<double>) to it instead of launching
+  struct OpSeq {
+    std::vector<char> key;
+    srmg::DevBuf ops;
+    int nops = 0;
+  };
+  std::vector<OpSeq> op_seqs;
+  bool use_op_seq = true;
+  std::vector<char> *seq_rec = nullptr;
 
   // free boundary conditions (srmg_freebc_set): f [n], sin table [4n], work [n], b [n]
   srmg::DevBuf fbc;
@@ -171,6 +182,12 @@ struct srmg_ctx {
   int fbc_dim = 0, fbc_level = 0;
   int64_t fbc_root[2] = {1, 1};
   bool fbc_direct = false;  // option "freebc_direct": direct-sum transforms even for power-of-two n
+  // per-tree tables of srmg_freebc_dev (the outer-column gather, the level views and the
+  // outer blocks), built on first use after srmg_freebc_set or a new tree
+  srmg::DevBuf fbc_tabs;
+  bool fbc_built = false;
+  int fbc_nent = 0;
+  size_t fbc_off_lvs = 0, fbc_off_ent = 0;
 
   // host-array entry points: b copied back to the host (off by default: leaf cells of b
   // are never written, and non-leaf b is unspecified after a V-cycle), and the host

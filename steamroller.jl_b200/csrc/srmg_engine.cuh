@@ -546,7 +546,8 @@ __device__ __forceinline__ void st_pair(T *p, T a, T b) {
 }
 
 // The order-2 stencil of applystencil (src/laplacian.jl:25-49,78-118) on values already
-// loaded: the same products and sums, in the same order, as apply5.
+// loaded: the same products and sums, in the same order, as apply5, here free to be
+// contracted into FMAs (the engine agrees with the per-operation kernels to rounding).
 template <typename T>
 __device__ __forceinline__ T sten5(const W5<T> &w, T centre, T zm, T rm, T c, T rp, T zp) {
   T v = w.zm * zm;

@@ -17,9 +17,11 @@
 // x'_j = (-1)^j x_j, and DCT-II through Makhoul's reordering v = (x_0, x_2, ..., x_3,
 // x_1) and C_k = 2 Re(e^{-i pi k / 2n} V_k); DST-III(X)[k] = (-1)^k DCT-III(X'')[k] with
 // X''_j = X_{n-1-j}, and DCT-III through the inverse reordering of an unnormalised
-// inverse FFT of W^{-k} (X''_k - i X''_{n-k}).  The FFT is radix-2 in shared memory for
-// n <= 8192 and a four-step n = n1 n2 split (n2 column FFTs with twiddles, then n1 row
-// FFTs) above, twiddles from a table of e^{-2 pi i k / n}.  Other n run as direct
+// inverse FFT of W^{-k} (X''_k - i X''_{n-k}).  For n <= 8192 the gather, both FFTs
+// (radix-2 stages, two per pass over shared memory) and the steps between them run in
+// one CTA in shared memory; above, a
+// four-step n = n1 n2 split (n2 column FFTs with twiddles, then n1 row FFTs) per
+// transform, twiddles from a table of e^{-2 pi i k / n}.  Other n run as direct
 // sums, one CTA per output in a fixed order, with the sine of every argument from a
 // table of sin(pi t / (2n)), t = 0..4n-1 (the integer argument reduced exactly modulo
 // 4n).  f, the transform's kernel (modified Bessel functions of the domain's aspect),
@@ -55,19 +57,29 @@ __global__ void k_sin_table(double *tab, int64_t n) {
     tab[t] = sinpi((double)t / (double)(2 * n));
 }
 
-// getouter! for one level (levels run in increasing order, so finer blocks overwrite).
-__global__ void k_getouter(double *__restrict__ u1, const double *__restrict__ u, LevelView lv, int dim, int kext,
-                           int p, double hl) {
-  const int64_t total = (int64_t)lv.nblk * kM;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    const int bi = (int)(t / kM), i = (int)(t % kM);
-    const int4 bk = lv.blocks[bi];
-    const int cd = dim == 1 ? bk.y : bk.z, co = dim == 1 ? bk.z : bk.y;
-    if (cd != kext) continue;
-    const double v = u[(int64_t)bk.x * kSS + cell_off(dim, kG + kM - 1, kG + i)] / hl;
-    const int64_t i0 = (int64_t)(co - 1) * kM;
-    for (int m = 0; m < p; ++m) u1[p * (i0 + i) + m] = v;
-  }
+// One position of the outer column: the element of u that getouter! (src/freebc.jl:108-140)
+// reads for it -- levels walked in increasing order, so the finest level at the outer
+// extent that covers the position wins -- and that level, or off = -1 where no block
+// covers it (the column stays zero there).  Built on the host once per tree.
+struct FbcSrc {
+  long long off;
+  int level;
+  int pad;
+};
+
+// getouter!'s value at position j: u / h_l, h_l = h / 2^(l-1).
+__device__ __forceinline__ double outer_value(const FbcSrc *__restrict__ src, const double *__restrict__ u, double h,
+                                              int64_t j) {
+  const FbcSrc sj = src[j];
+  if (sj.off < 0) return 0.0;
+  return u[sj.off] / (h / (double)((int64_t)1 << (sj.level - 1)));
+}
+
+// u1 = getouter! over every level, one launch (direct-sum path).
+__global__ void k_fbc_gather(double *__restrict__ u1, const FbcSrc *__restrict__ src, const double *__restrict__ u,
+                             double h, int64_t n) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
+    u1[j] = outer_value(src, u, h, j);
 }
 
 __device__ __forceinline__ double block_sum(double v) {
@@ -159,35 +171,48 @@ int fft_forward(srmg_ctx *ctx, double2 *b, double2 *a, double2 *tmp, const doubl
   return SRMG_OK;
 }
 
-// DST-II, step 1: v = Makhoul reordering of x'_j = (-1)^j x_j, as complex values.
-__global__ void k_dst2_pre(double2 *__restrict__ v, const double *__restrict__ x, int64_t n) {
-  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n / 2; j += (int64_t)gridDim.x * blockDim.x) {
-    v[j] = make_double2(x[2 * j], 0.0);                   // (-1)^(2j) = 1
-    v[n - 1 - j] = make_double2(-x[2 * j + 1], 0.0);      // (-1)^(2j+1) = -1
+// DST-II, step 1: the Makhoul position of x_j in v (x'_j = (-1)^j x_j; v = (x'_0, x'_2,
+// ..., x'_3, x'_1)) and its sign.
+__device__ __forceinline__ int64_t makhoul_pos(int64_t j, int64_t n) { return (j & 1) ? n - 1 - (j >> 1) : (j >> 1); }
+
+// getouter! and the reordering in one launch (four-step FFT path): v[pos(j)] = +-u1_j.
+__global__ void k_fbc_gather_pre(double2 *__restrict__ v, const FbcSrc *__restrict__ src, const double *__restrict__ u,
+                                 double h, int64_t n) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+    const double x = outer_value(src, u, h, j);
+    v[makhoul_pos(j, n)] = make_double2((j & 1) ? -x : x, 0.0);
   }
 }
 
-// DST-II, step 2: y[k] = C[n-1-k], C[m] = 2 Re(e^{-i pi m / 2n} V[m]); then the DST-III
-// input X_j = f_j y_j (rounded once) reversed, X''_m = X_{n-1-m}, and
-// V'[m] = e^{+i pi m / 2n} (X''_m - i X''_{n-m}) (X''_n = 0), conjugated for the
-// inverse transform done as a forward FFT.  With y_out the DST-II output is kept.
+// DST-II, step 2, at m: C[m] = 2 Re(e^{-i pi m / 2n} V[m]), the DCT-II of x' (y_k =
+// C[n-1-k] is the DST-II).  Every product and sum rounded on its own.
+__device__ __forceinline__ double dct2_at(double2 z, int64_t m, int64_t n) {
+  double sn, cs;
+  sincospi(-(double)m / (double)(2 * n), &sn, &cs);
+  return 2.0 * __dadd_rn(__dmul_rn(z.x, cs), -__dmul_rn(z.y, sn));
+}
+
+// The DST-III input at m from the DST-II output: X_j = f_j y_j (rounded once) reversed,
+// X''_m = X_{n-1-m} = f_{n-1-m} C[m], X''_{n-m} = f_{m-1} C[n-m] (X''_n = 0), and
+// V'[m] = e^{+i pi m / 2n} (X''_m - i X''_{n-m}), conjugated for the inverse transform
+// done as a forward FFT: (cs xm + sn xnm) - i (sn xm - cs xnm).
+__device__ __forceinline__ double2 dst3_in(double xm, double xnm, int64_t m, int64_t n) {
+  double sn, cs;
+  sincospi((double)m / (double)(2 * n), &sn, &cs);
+  return make_double2(__dadd_rn(__dmul_rn(cs, xm), __dmul_rn(sn, xnm)),
+                      -__dadd_rn(__dmul_rn(sn, xm), -__dmul_rn(cs, xnm)));
+}
+
+// DST-II step 2 and the DST-III input over all m (four-step FFT path).  With y_out the
+// DST-II output is kept.
 __global__ void k_dst_mid(double2 *__restrict__ vp, double *__restrict__ y_out, const double2 *__restrict__ V,
                           const double *__restrict__ f, int64_t n) {
-  auto C = [&](int64_t m) {  // DCT-II of x' at m
-    double sn, cs;
-    sincospi(-(double)m / (double)(2 * n), &sn, &cs);
-    const double2 z = V[m];
-    return 2.0 * (z.x * cs - z.y * sn);
-  };
   for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < n; m += (int64_t)gridDim.x * blockDim.x) {
-    // y_k = C[n-1-k]; X''_m = f_{n-1-m} y_{n-1-m} = f_{n-1-m} C[m]
-    const double xm = f[n - 1 - m] * C(m);
-    if (y_out) y_out[n - 1 - m] = C(m);
-    const double xnm = m == 0 ? 0.0 : f[m - 1] * C(n - m);  // X''_{n-m} = f_{m-1} y_{m-1} = f_{m-1} C[n-m]
-    double sn, cs;
-    sincospi((double)m / (double)(2 * n), &sn, &cs);  // e^{+i pi m / 2n}
-    // (cs + i sn)(xm - i xnm) = (cs xm + sn xnm) + i (sn xm - cs xnm); conjugated
-    vp[m] = make_double2(cs * xm + sn * xnm, -(sn * xm - cs * xnm));
+    const double cm = dct2_at(V[m], m, n);
+    if (y_out) y_out[n - 1 - m] = cm;
+    const double xm = __dmul_rn(f[n - 1 - m], cm);
+    const double xnm = m == 0 ? 0.0 : __dmul_rn(f[m - 1], dct2_at(V[n - m], n - m, n));
+    vp[m] = dst3_in(xm, xnm, m, n);
   }
 }
 
@@ -198,6 +223,102 @@ __global__ void k_dst3_post(double *__restrict__ b, const double2 *__restrict__ 
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n / 2; j += (int64_t)gridDim.x * blockDim.x) {
     const double ye = w[j].x, yo = w[n - 1 - j].x;  // Re(conj z) = Re z
     b[2 * j] = ye * h / p2 / 2.0;                   // (-1)^(2j) = 1
+    b[2 * j + 1] = -yo * h / p2 / 2.0;
+  }
+}
+
+// ---- the whole transform in one CTA (n a power of two, n <= kFftMaxLocal) -----------
+
+constexpr int kLocalThreads = 1024;
+
+__device__ __forceinline__ void bfly(double2 &a, double2 &c, double2 w) {
+  const double2 t = cmul(c, w);
+  c = make_double2(a.x - t.x, a.y - t.y);
+  a = make_double2(a.x + t.x, a.y + t.y);
+}
+
+// In-place radix-2 FFT of buf (loaded in bit-reversed order) with the twiddles
+// e^{-2 pi i k / n}, k < n / 2, in shared memory: the butterflies of k_fft, two stages
+// (half = h, then 2h) per pass over shared memory where they pair up.  A thread holds
+// the four elements g + pos + {0, h, 2h, 3h} (g a multiple of 4h, pos < h) in registers:
+// stage h pairs (0, h) and (2h, 3h) with twiddle pos n / 2h, stage 2h pairs (0, 2h)
+// with twiddle pos n / 4h and (h, 3h) with (pos + h) n / 4h -- the same operations on
+// the same values as two radix-2 passes.
+__device__ __forceinline__ void local_fft(double2 *buf, const double2 *stw, int n, int logn) {
+  int half = 1;
+  if (logn & 1) {  // one radix-2 stage first when the stage count is odd
+    for (int idx = threadIdx.x; idx < n / 2; idx += blockDim.x) {
+      double2 a = buf[2 * idx], c = buf[2 * idx + 1];
+      bfly(a, c, stw[0]);
+      buf[2 * idx] = a;
+      buf[2 * idx + 1] = c;
+    }
+    __syncthreads();
+    half = 2;
+  }
+  for (; half < n; half <<= 2) {
+    const int t1 = n / (2 * half), t2 = n / (4 * half);
+    for (int idx = threadIdx.x; idx < n / 4; idx += blockDim.x) {
+      const int pos = idx & (half - 1), i = (idx - pos) * 4 + pos;
+      double2 a0 = buf[i], a1 = buf[i + half], a2 = buf[i + 2 * half], a3 = buf[i + 3 * half];
+      const double2 w1 = stw[pos * t1];
+      bfly(a0, a1, w1);
+      bfly(a2, a3, w1);
+      bfly(a0, a2, stw[pos * t2]);
+      bfly(a1, a3, stw[(pos + half) * t2]);
+      buf[i] = a0;
+      buf[i + half] = a1;
+      buf[i + 2 * half] = a2;
+      buf[i + 3 * half] = a3;
+    }
+    __syncthreads();
+  }
+}
+
+// b = DST-III(f .* DST-II(getouter!(u))) h / 2^(level-1) / 2 in one CTA: the gather and
+// the Makhoul reordering loaded bit-reversed into shared memory, the forward FFT, the
+// DST-III input formed in place one (m, n - m) pair per thread, a bit-reversal
+// permutation, the second FFT and the output reordering.  Dynamic shared memory: n
+// complex values and n / 2 twiddles (24 n bytes, 192 KB at n = 8192).
+__global__ void __launch_bounds__(kLocalThreads, 1)
+    k_dst_local(double *__restrict__ b, const FbcSrc *__restrict__ src, const double *__restrict__ u, double h,
+                const double2 *__restrict__ tw, const double *__restrict__ f, int n, int logn, double p2) {
+  extern __shared__ double2 sm[];
+  double2 *buf = sm, *stw = sm + n;
+  for (int k = threadIdx.x; k < n / 2; k += blockDim.x) stw[k] = tw[k];
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const double x = outer_value(src, u, h, j);
+    const unsigned pos = (unsigned)makhoul_pos(j, n);
+    buf[__brev(pos) >> (32 - logn)] = make_double2((j & 1) ? -x : x, 0.0);
+  }
+  __syncthreads();
+  local_fft(buf, stw, n, logn);
+  for (int m = threadIdx.x; m <= n / 2; m += blockDim.x) {
+    const int mm = n - m;  // the partner position (m = 0 has none, m = n / 2 is its own)
+    const double cm = dct2_at(buf[m], m, n);
+    if (m == 0) {
+      buf[0] = dst3_in(__dmul_rn(f[n - 1], cm), 0.0, 0, n);
+      continue;
+    }
+    const double cmm = dct2_at(buf[mm], mm, n);
+    const double2 vm = dst3_in(__dmul_rn(f[n - 1 - m], cm), __dmul_rn(f[m - 1], cmm), m, n);
+    if (mm != m) buf[mm] = dst3_in(__dmul_rn(f[n - 1 - mm], cmm), __dmul_rn(f[mm - 1], cm), mm, n);
+    buf[m] = vm;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int r = (int)(__brev((unsigned)i) >> (32 - logn));
+    if (i < r) {
+      const double2 t = buf[i];
+      buf[i] = buf[r];
+      buf[r] = t;
+    }
+  }
+  __syncthreads();
+  local_fft(buf, stw, n, logn);
+  for (int j = threadIdx.x; j < n / 2; j += blockDim.x) {
+    const double ye = buf[j].x, yo = buf[n - 1 - j].x;  // as k_dst3_post
+    b[2 * j] = ye * h / p2 / 2.0;
     b[2 * j + 1] = -yo * h / p2 / 2.0;
   }
 }
@@ -256,36 +377,38 @@ __device__ __forceinline__ double seg_mean(const double *b, int64_t first, int64
 // factor(CylindricalGeometry{D}, J, delta) with delta along D (src/geometry.jl:27-29)
 __device__ __forceinline__ double cyl_factor(int64_t J) { return fabs(1.0 + 1.0 / (double)(2 * J - 1)); }
 
-// setouter! boundary sources of one level (src/freebc.jl:157-176): every block with a
-// boundary face at +dim.
-__global__ void k_setouter_bnd(double *__restrict__ q, const double *__restrict__ b, LevelView lv, int dim, int p,
-                               double sl) {
-  const int fidx = dim == 1 ? 1 : 3;
-  const int64_t total = (int64_t)lv.nblk * kM;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    const int bi = (int)(t / kM), i = (int)(t % kM);
-    if (lv.faces[4 * bi + fidx].x != FACE_BOUNDARY) continue;
-    const int4 bk = lv.blocks[bi];
-    const int cd = dim == 1 ? bk.y : bk.z, co = dim == 1 ? bk.z : bk.y;
-    const int64_t i0 = (int64_t)(co - 1) * kM;
-    const int64_t Jd = (int64_t)kM * (cd - 1) + kM;
-    const double bmean = seg_mean(b, p * (i0 + i), p);
-    double *qc = q + (int64_t)bk.x * kSS + cell_off(dim, kG + kM - 1, kG + i);
-    *qc = *qc + 2.0 * cyl_factor(Jd) * bmean / sl;
-  }
-}
-
-// setouter! corrections at refinement boundaries of one level (src/freebc.jl:178-219):
-// one thread per block on the outer boundary walks its refinement faces in the
-// connectivity's direction order (`order` lists face codes: 0..3 star faces, 4..7 the
-// corners), so that additions to one cell happen in the reference's order.
-__global__ void k_setouter_ref(double *__restrict__ q, const double *__restrict__ b, LevelView lv, int dim, int kext,
-                               int p, double sl, int4 order_lo, int4 order_hi, int norder) {
+// setouter! (src/freebc.jl:157-219) over every level in one launch: one thread per cell
+// of the outer valid column of each listed block (the blocks at the level's outer
+// extent, or with a boundary face at +dim).  The thread adds the boundary source
+// (src/freebc.jl:157-176) when the block's +dim face is a boundary, then -- for the
+// first and last cell of the column -- the refinement-boundary corrections that land
+// on it (src/freebc.jl:178-219), walking the connectivity's direction order (`order`
+// lists face codes: 0..3 star faces, 4..7 the corners).  Each cell belongs to one
+// block and one thread, so its additions happen in the reference's order: the level's
+// boundary sources before its refinement corrections, those in direction order.
+__global__ void k_setouter_all(double *__restrict__ q, const double *__restrict__ b, const LevelView *__restrict__ lvs,
+                               const int2 *__restrict__ ent, int nent, int dim, int level, long long root_dim,
+                               double s, int4 order_lo, int4 order_hi, int norder) {
   const int order[8] = {order_lo.x, order_lo.y, order_lo.z, order_lo.w, order_hi.x, order_hi.y, order_hi.z, order_hi.w};
-  for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < lv.nblk; bi += gridDim.x * blockDim.x) {
+  const int fidx = dim == 1 ? 1 : 3;
+  const int64_t total = (int64_t)nent * kM;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(t / kM), i = (int)(t % kM);
+    const int l = ent[e].x, bi = ent[e].y;
+    const LevelView &lv = lvs[l - 1];
     const int4 bk = lv.blocks[bi];
     const int cd = dim == 1 ? bk.y : bk.z, co = dim == 1 ? bk.z : bk.y;
-    if (cd != kext) continue;
+    const int64_t fl = (int64_t)1 << (l - 1);
+    const double sl = s / (double)(fl * fl);
+    const int64_t p = (int64_t)1 << (level - l);
+    const int64_t Jd = (int64_t)kM * (cd - 1) + kM;
+    if (lv.faces[4 * bi + fidx].x == FACE_BOUNDARY) {
+      const int64_t i0 = (int64_t)(co - 1) * kM;
+      const double bmean = seg_mean(b, p * (i0 + i), p);
+      double *qc = q + (int64_t)bk.x * kSS + cell_off(dim, kG + kM - 1, kG + i);
+      *qc = *qc + 2.0 * cyl_factor(Jd) * bmean / sl;
+    }
+    if ((i != 0 && i != kM - 1) || cd != (int)(root_dim << (l - 1))) continue;
     for (int r = 0; r < norder; ++r) {
       const int code = order[r];
       int type, fr, fz;
@@ -302,13 +425,13 @@ __global__ void k_setouter_ref(double *__restrict__ q, const double *__restrict_
       if (type != FACE_REFBND) continue;
       const int dir = dim == 1 ? fz : fr;  // the face's component along the other dimension
       const int i1 = dir == -1 ? kG + 1 : kM + kG;  // 1-based index along the other dimension
+      if (i1 - 1 - kG != i) continue;                // another cell's correction
       const int64_t j = (int64_t)(co - 1) * kM + i1 - kG;
-      const int64_t Jd = (int64_t)kM * (cd - 1) + kM;
       const int64_t J1d = (Jd - 1) / 2 + 1;
       // 0-based first element: dir = 1 reads b[p j + 1 : p (j + 2)], otherwise
       // b[p (j - 3) : p (j - 1) - 1] (1-based, as written in the reference)
       const int64_t first = dir == 1 ? p * j : p * (j - 3) - 1;
-      const double bmean = seg_mean(b, first, 2 * (int64_t)p);
+      const double bmean = seg_mean(b, first, 2 * p);
       double *qc = q + (int64_t)bk.x * kSS + cell_off(dim, kG + kM - 1, i1 - 1);
       *qc = *qc + 2.0 * 0.25 * cyl_factor(J1d) * bmean / sl;
     }
@@ -354,6 +477,7 @@ int fbc_ready(srmg_ctx *ctx, int64_t nblk_alloc, const char *who) {
   RC(check_call(ctx, nblk_alloc, 0, 0, nullptr));
   if (ctx->fbc_n <= 0) return fail(ctx, SRMG_ERR_BADARG, "%s: call srmg_freebc_set first", who);
   if (ctx->nitems != 1) return fail(ctx, SRMG_ERR_UNSUPPORTED, "%s: one tree per context", who);
+  if (ctx->D != 2) return fail(ctx, SRMG_ERR_UNSUPPORTED, "%s: two-dimensional trees only", who);
   for (int l = ctx->fbc_level + 1; l <= ctx->nlev; ++l)
     if (ctx->nblk_host[l - 1] > 0)
       return fail(ctx, SRMG_ERR_BADARG, "%s: the tree has level %d above the free-boundary level %d", who, l,
@@ -367,7 +491,7 @@ int extent(srmg_ctx *ctx, int l, int dim) { return (int)(ctx->fbc_root[dim - 1] 
 // Host checks on the uploaded tree: every block lies inside the level's extent given by
 // rootsize (so the gathers and means index inside b), and every refinement correction
 // reads inside b (Julia would throw a BoundsError there), with the same index
-// arithmetic as k_setouter_ref.
+// arithmetic as k_setouter_all.
 int check_tree_fits(srmg_ctx *ctx) {
   const int dim = ctx->fbc_dim, od = dim == 1 ? 2 : 1;
   const int L = std::min(ctx->fbc_level, ctx->htree.nlev);
@@ -396,6 +520,70 @@ int check_tree_fits(srmg_ctx *ctx) {
   return SRMG_OK;
 }
 
+
+// The tables of srmg_freebc_dev for the current tree and free-boundary setting, built
+// once (check_tree_fits included): the outer-column source of every transform position
+// (getouter!'s level loop run on the host), the device level views, and the (level,
+// index) of every block at its level's outer extent or with a boundary face at +dim.
+int fbc_build(srmg_ctx *ctx) {
+  if (ctx->fbc_built) return SRMG_OK;
+  RC(check_tree_fits(ctx));
+  const int dim = ctx->fbc_dim, od = dim == 1 ? 2 : 1, level = ctx->fbc_level;
+  const int64_t n = ctx->fbc_n;
+  const int L = std::min(level, ctx->nlev);
+  std::vector<FbcSrc> src((size_t)n, FbcSrc{-1, 0, 0});
+  std::vector<LevelView> lvs((size_t)std::max(L, 1));
+  std::vector<int2> ent;
+  for (int l = 1; l <= L; ++l) {
+    lvs[l - 1] = ctx->lv[l - 1].view(l);
+    const int kext = extent(ctx, l, dim);
+    const int64_t p = (int64_t)1 << (level - l);
+    const auto &pairs = ctx->htree.pairs[l - 1];
+    std::vector<char> at_bnd(pairs.size(), 0);
+    std::vector<int> idx(ctx->htree.max_blk + 1, -1);
+    for (size_t bi = 0; bi < pairs.size(); ++bi) idx[pairs[bi].blk] = (int)bi;
+    for (const srmg_boundary &e : ctx->htree.bd[l - 1])
+      if (e.face[dim - 1] == 1 && e.face[od - 1] == 0 && e.block >= 1 && e.block <= ctx->htree.max_blk &&
+          idx[e.block] >= 0)
+        at_bnd[idx[e.block]] = 1;
+    for (size_t bi = 0; bi < pairs.size(); ++bi) {
+      const srmg_pair &pr = pairs[bi];
+      const bool outer = pr.coord[dim - 1] == kext;
+      if (outer || at_bnd[bi]) ent.push_back(make_int2(l, (int)bi));
+      if (!outer) continue;
+      if (pr.coord[od - 1] < 1)
+        return fail(ctx, SRMG_ERR_BADARG, "freebc: block %lld of level %d has a coordinate below 1",
+                    (long long)pr.blk, l);
+      const int64_t i0 = (pr.coord[od - 1] - 1) * kM;
+      for (int i = 0; i < kM; ++i) {
+        const long long off = (long long)(pr.blk - 1) * kSS +
+                              (dim == 1 ? (kG + kM - 1) + kS * (kG + i) : (kG + i) + kS * (kG + kM - 1));
+        for (int64_t m = 0; m < p; ++m) src[(size_t)(p * (i0 + i) + m)] = FbcSrc{off, l, 0};
+      }
+    }
+  }
+  const size_t b_src = src.size() * sizeof(FbcSrc);
+  const size_t o_lvs = (b_src + 255) & ~size_t(255);
+  const size_t o_ent = (o_lvs + lvs.size() * sizeof(LevelView) + 255) & ~size_t(255);
+  const size_t total = o_ent + std::max<size_t>(ent.size(), 1) * sizeof(int2);
+  RC(ensure(ctx, ctx->fbc_tabs, total));
+  char *d = (char *)ctx->fbc_tabs.p;
+  // on the context's stream (pageable sources, staged before each call returns)
+  CK(cudaMemcpyAsync(d, src.data(), b_src, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(d + o_lvs, lvs.data(), lvs.size() * sizeof(LevelView), cudaMemcpyHostToDevice, ctx->stream));
+  if (!ent.empty())
+    CK(cudaMemcpyAsync(d + o_ent, ent.data(), ent.size() * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->fbc_off_lvs = o_lvs;
+  ctx->fbc_off_ent = o_ent;
+  ctx->fbc_nent = (int)ent.size();
+  ctx->fbc_built = true;
+  return SRMG_OK;
+}
+
+const FbcSrc *fbc_src(srmg_ctx *ctx) { return (const FbcSrc *)ctx->fbc_tabs.p; }
+const LevelView *fbc_lvs(srmg_ctx *ctx) { return (const LevelView *)((char *)ctx->fbc_tabs.p + ctx->fbc_off_lvs); }
+const int2 *fbc_ent(srmg_ctx *ctx) { return (const int2 *)((char *)ctx->fbc_tabs.p + ctx->fbc_off_ent); }
+
 }  // namespace
 
 extern "C" int srmg_freebc_set(srmg_ctx *ctx, int dim, int level, const int64_t rootsize[2], const double *f,
@@ -418,6 +606,7 @@ extern "C" int srmg_freebc_set(srmg_ctx *ctx, int dim, int level, const int64_t 
   ctx->fbc_level = level;
   ctx->fbc_root[0] = rootsize[0];
   ctx->fbc_root[1] = rootsize[1];
+  ctx->fbc_built = false;
   CK(cudaMemcpyAsync(fbc_f(ctx), f, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   k_sin_table<<<gridfor(4 * n, 256), 256, 0, ctx->stream>>>(fbc_tab(ctx), n);
   ctx->launches++;
@@ -425,6 +614,9 @@ extern "C" int srmg_freebc_set(srmg_ctx *ctx, int dim, int level, const int64_t 
     // the FFT kernel holds up to kFftMaxLocal complex doubles in dynamic shared memory
     CK(cudaFuncSetAttribute(k_fft, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)(kFftMaxLocal * sizeof(double2))));
+    // k_dst_local: the transform and n / 2 twiddles
+    CK(cudaFuncSetAttribute(k_dst_local, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)(kFftMaxLocal * sizeof(double2) * 3 / 2)));
     k_twiddles<<<gridfor(n, 256), 256, 0, ctx->stream>>>(fbc_tw(ctx), n);
     ctx->launches++;
   }
@@ -440,36 +632,34 @@ extern "C" int srmg_freebc_dev(srmg_ctx *ctx, double *q, const double *u, int64_
   if (!q || !u) return fail(ctx, SRMG_ERR_BADARG, "srmg_freebc: null field");
   if (!(h > 0.0) || !std::isfinite(h) || !std::isfinite(s) || s == 0.0)
     return fail(ctx, SRMG_ERR_BADARG, "srmg_freebc: bad h or s");
-  RC(check_tree_fits(ctx));
+  RC(fbc_build(ctx));
   const int dim = ctx->fbc_dim, level = ctx->fbc_level;
   const int64_t n = ctx->fbc_n;
-  const int L = std::min(level, ctx->nlev);
   double *u1 = fbc_u1(ctx), *b = fbc_b(ctx), *am = b;  // DST-II output shares b's storage until the end
-  CK(cudaMemsetAsync(u1, 0, n * sizeof(double), ctx->stream));
-  for (int l = 1; l <= L; ++l) {
-    const int nb = ctx->nblk_host[l - 1];
-    if (!nb) continue;
-    const double hl = h / (double)((int64_t)1 << (l - 1));
-    k_getouter<<<gridfor((int64_t)nb * kM, 256), 256, 0, ctx->stream>>>(u1, u, ctx->lv[l - 1].view(l), dim,
-                                                                       extent(ctx, l, dim), 1 << (level - l), hl);
-    ctx->launches++;
-  }
   const double p2 = (double)((int64_t)1 << (level - 1));
-  if (fbc_pow2(n) && !ctx->fbc_direct) {
+  if (fbc_pow2(n) && !ctx->fbc_direct && n <= kFftMaxLocal) {
+    // gather, DST-II, times f, DST-III: one CTA
+    int logn = 0;
+    while (((int64_t)1 << logn) < n) ++logn;
+    k_dst_local<<<1, kLocalThreads, 24 * n, ctx->stream>>>(b, fbc_src(ctx), u, h, fbc_tw(ctx), fbc_f(ctx), (int)n,
+                                                          logn, p2);
+    ctx->launches++;
+  } else if (fbc_pow2(n) && !ctx->fbc_direct) {
     double2 *w0 = fbc_work(ctx, 0), *w1 = fbc_work(ctx, 1), *w2 = fbc_work(ctx, 2);
-    k_dst2_pre<<<gridfor(n / 2, 256), 256, 0, ctx->stream>>>(w0, u1, n);
+    k_fbc_gather_pre<<<gridfor(n, 256), 256, 0, ctx->stream>>>(w0, fbc_src(ctx), u, h, n);
     RC(fft_forward(ctx, w1, w0, w2, fbc_tw(ctx), n));
     k_dst_mid<<<gridfor(n, 256), 256, 0, ctx->stream>>>(w0, nullptr, w1, fbc_f(ctx), n);
     RC(fft_forward(ctx, w1, w0, w2, fbc_tw(ctx), n));
     k_dst3_post<<<gridfor(n / 2, 256), 256, 0, ctx->stream>>>(b, w1, n, h, p2);
     ctx->launches += 3;
   } else {
+    k_fbc_gather<<<gridfor(n, 256), 256, 0, ctx->stream>>>(u1, fbc_src(ctx), u, h, n);
     const int g = (int)std::min<int64_t>(n, 148 * 16);
     k_dst2<<<g, kDstThreads, 0, ctx->stream>>>(am, u1, fbc_tab(ctx), n);
     // DST-III reads am and writes b: keep them apart (u1 is free again)
     CK(cudaMemcpyAsync(u1, am, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     k_dst3_scale<<<g, kDstThreads, 0, ctx->stream>>>(b, u1, fbc_f(ctx), fbc_tab(ctx), n, h, p2);
-    ctx->launches += 2;
+    ctx->launches += 3;
   }
   const int order_star[4] = {0, 1, 2, 3};                 // StarStencil order (src/stencil.jl:16-32)
   const int order_box[8] = {4, 2, 5, 0, 1, 6, 3, 7};      // BoxStencil order (src/stencil.jl:34-90)
@@ -477,17 +667,11 @@ extern "C" int srmg_freebc_dev(srmg_ctx *ctx, double *q, const double *u, int64_
   const int nord = ctx->has_corners ? 8 : 4;
   const int4 olo = make_int4(ord[0], ord[1], ord[2], ord[3]);
   const int4 ohi = nord == 8 ? make_int4(ord[4], ord[5], ord[6], ord[7]) : make_int4(0, 0, 0, 0);
-  for (int l = 1; l <= L; ++l) {
-    const int nb = ctx->nblk_host[l - 1];
-    if (!nb) continue;
-    const int64_t f = (int64_t)1 << (l - 1);
-    const double sl = s / (double)(f * f);
-    const int p = 1 << (level - l);
-    k_setouter_bnd<<<gridfor((int64_t)nb * kM, 256), 256, 0, ctx->stream>>>(q, b, ctx->lv[l - 1].view(l), dim, p,
-                                                                           sl);
-    k_setouter_ref<<<gridfor(nb, 128), 128, 0, ctx->stream>>>(q, b, ctx->lv[l - 1].view(l), dim,
-                                                            extent(ctx, l, dim), p, sl, olo, ohi, nord);
-    ctx->launches += 2;
+  if (ctx->fbc_nent > 0) {
+    k_setouter_all<<<gridfor((int64_t)ctx->fbc_nent * kM, 128), 128, 0, ctx->stream>>>(
+        q, b, fbc_lvs(ctx), fbc_ent(ctx), ctx->fbc_nent, dim, level, (long long)ctx->fbc_root[dim - 1], s, olo, ohi,
+        nord);
+    ctx->launches++;
   }
   if (b_out) CK(cudaMemcpyAsync(b_out, b, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
   CK(cudaGetLastError());

@@ -18,6 +18,9 @@ int check_call_any(srmg_ctx *ctx, int64_t nblk_alloc, int op, int geom, const in
 inline int64_t block_elems(const srmg_ctx *ctx) { return ctx->D == 3 ? (int64_t)kS * kS * kS : (int64_t)kSS; }
 void free_tree(srmg_ctx *ctx);
 void drop_op_graphs(srmg_ctx *ctx);
+// One cooperative launch of the sequencer over `nops` recorded operations (srmg_seq.cu).
+int seq_launch(srmg_ctx *ctx, const void *d_ops, int nops);
+size_t seq_op_bytes();
 // `ncycles` per-operation FP64 V-cycles (2D trees off the persistent engine, or 3D),
 // replayed from a captured CUDA graph when the option `op_graphs` is on (default).
 int vcycle_ops(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, double s, int op, double k2, int geom,

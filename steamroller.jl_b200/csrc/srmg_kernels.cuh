@@ -7,8 +7,10 @@
 //
 // Each kernel restates one reference routine and keeps its floating-point operation
 // order where the result must be bit-exact (ghost copies, mirrors, linear
-// interpolation, restriction); __dadd_rn/__dmul_rn stop the compiler from contracting
-// those into FMAs.  Stencil arithmetic only has to agree to rounding.
+// interpolation, restriction, and the stencils of the smoother and the residual);
+// __dadd_rn/__dmul_rn stop the compiler from contracting those into FMAs, and fma()
+// stands where the reference calls muladd.  The same bodies run as separate kernels
+// and inside the sequencer's single launch, with identical results.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -97,15 +99,18 @@ __device__ __forceinline__ W5<T> weights(const WTab<T> &wt, int geom, int cr, in
 }
 
 // applystencil, order 2 (src/laplacian.jl:25-49,78-118; src/helmholtz.jl:17-57):
-// v = 0; v += c * u[I+S] over S = (0,-1), (-1,0), (0,0), (1,0), (0,1).
+// v = 0; v += c * u[I+S] over S = (0,-1), (-1,0), (0,0), (1,0), (0,1), each product and
+// sum rounded on its own: the uncontracted reading of the reference's @fastmath
+// stencil, and a rounding that does not depend on the context the body is inlined
+// into (the compiler's choice of FMAs would).
 template <typename T>
 __device__ __forceinline__ T apply5(const T *ub, int x, int y, const W5<T> &w, T centre) {
   const int o = x + kS * y;
-  T v = w.zm * ub[o - kS];
-  v = v + w.rm * ub[o - 1];
-  v = v + centre * ub[o];
-  v = v + w.rp * ub[o + 1];
-  v = v + w.zp * ub[o + kS];
+  T v = dadd<T>(T(0), dmul<T>(w.zm, ub[o - kS]));
+  v = dadd<T>(v, dmul<T>(w.rm, ub[o - 1]));
+  v = dadd<T>(v, dmul<T>(centre, ub[o]));
+  v = dadd<T>(v, dmul<T>(w.rp, ub[o + 1]));
+  v = dadd<T>(v, dmul<T>(w.zp, ub[o + kS]));
   return v;
 }
 
@@ -177,7 +182,7 @@ __device__ __forceinline__ void fill_corner_cell(T *__restrict__ u, const LevelV
 // BoxStencil tree (lv.cfaces set) the launch covers one pass (mask 1, 2 or 4) and also
 // fills the corner cells of that pass: within one pass no cell reads another's result.
 template <typename T>
-__global__ void k_fill_ghost(T *__restrict__ u, LevelView lv, Signs sg, int mask) {
+__device__ __forceinline__ void d_fill_ghost(T *__restrict__ u, LevelView lv, Signs sg, int mask) {
   const int lane = threadIdx.x & 31;
   const int warps_per_cta = blockDim.x >> 5;
   const int g = lane >> 4, k = lane & 15;
@@ -250,7 +255,7 @@ __global__ void k_fill_ghost(T *__restrict__ u, LevelView lv, Signs sg, int mask
 // ---- red-black Gauss-Seidel colour sweep (src/multigrid.jl:153-180, 238-243) ------
 // Colour P updates valid cells with (x + y + 1) & 1 == P (0-based local indices).
 template <typename T>
-__global__ void k_gs_colour(T *__restrict__ u, const T *__restrict__ b, LevelView lv,
+__device__ __forceinline__ void d_gs_colour(T *__restrict__ u, const T *__restrict__ b, LevelView lv,
                             OpParams<T> p, WTab<T> wt, int parity) {
   const int64_t total = (int64_t)lv.nblk * 128;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
@@ -270,7 +275,7 @@ __global__ void k_gs_colour(T *__restrict__ u, const T *__restrict__ b, LevelVie
 
 // ---- residual (src/multigrid.jl:309-323, 349-354): r = -(b + Lu/s) ---------------
 template <typename T>
-__global__ void k_residual(T *__restrict__ r, const T *__restrict__ u, const T *__restrict__ b,
+__device__ __forceinline__ void d_residual(T *__restrict__ r, const T *__restrict__ u, const T *__restrict__ b,
                            LevelView lv, OpParams<T> p, WTab<T> wt) {
   const int64_t total = (int64_t)lv.nblk * 256;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
@@ -288,7 +293,7 @@ __global__ void k_residual(T *__restrict__ r, const T *__restrict__ u, const T *
 // ---- FAS coarse RHS (src/multigrid.jl:112-119, 331-344) ----------------------------
 // For each Child edge of this level, on the coarse subblock: bf = -(r + L(u)/s_c).
 template <typename T>
-__global__ void k_postrestrict(T *__restrict__ bf, const T *__restrict__ u, const T *__restrict__ r,
+__device__ __forceinline__ void d_postrestrict(T *__restrict__ bf, const T *__restrict__ u, const T *__restrict__ r,
                                LevelView lv, const int2 *__restrict__ coord_of, OpParams<T> p,
                                WTab<T> wt) {
   const int64_t total = (int64_t)lv.nch * 64;
@@ -309,7 +314,7 @@ __global__ void k_postrestrict(T *__restrict__ bf, const T *__restrict__ u, cons
 // ---- restriction (src/restrict.jl:5-37) --------------------------------------------
 // coarse = ((((0 + f00) + f10) + f01) + f11) / 4 for each Child edge of this level.
 template <typename T>
-__global__ void k_restrict(T *__restrict__ u, LevelView lv) {
+__device__ __forceinline__ void d_restrict(T *__restrict__ u, LevelView lv) {
   const int64_t total = (int64_t)lv.nch * 64;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
@@ -328,7 +333,7 @@ __global__ void k_restrict(T *__restrict__ u, LevelView lv) {
 
 // ---- prolongation-add (src/interp.jl:24-63, 107-115): u_f += P(u1_c) -------------
 template <typename T>
-__global__ void k_interp_add(T *__restrict__ u, const T *__restrict__ u1, LevelView lv) {
+__device__ __forceinline__ void d_interp_add(T *__restrict__ u, const T *__restrict__ u1, LevelView lv) {
   const int64_t total = (int64_t)lv.nch * 256;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
@@ -349,7 +354,7 @@ __global__ void k_interp_add(T *__restrict__ u, const T *__restrict__ u1, LevelV
 
 // ---- whole-block copy / difference over a level (src/blockfield.jl:557-576) ------
 template <typename T>
-__global__ void k_copy_level(T *__restrict__ dst, const T *__restrict__ src, LevelView lv) {
+__device__ __forceinline__ void d_copy_level(T *__restrict__ dst, const T *__restrict__ src, LevelView lv) {
   const int64_t total = (int64_t)lv.nblk * kSS;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
@@ -360,7 +365,7 @@ __global__ void k_copy_level(T *__restrict__ dst, const T *__restrict__ src, Lev
 }
 
 template <typename T>
-__global__ void k_diff_level(T *__restrict__ dst, const T *__restrict__ a1, const T *a2,
+__device__ __forceinline__ void d_diff_level(T *__restrict__ dst, const T *__restrict__ a1, const T *a2,
                              LevelView lv) {
   const int64_t total = (int64_t)lv.nblk * kSS;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
@@ -432,7 +437,7 @@ __global__ void __launch_bounds__(NT) k_reduce_sqrt(double *__restrict__ out,
 // gauss_seidel!(..., FourColors{P1,P2}) (src/multigrid.jl:206-232): cells
 // (2 + 2a + p1, 2 + 2b + p2), u -= omega (Lu + s b) / c, unfused.
 template <typename T>
-__global__ void k_gs4(T *__restrict__ u, const T *__restrict__ b, LevelView lv, OpParams<T> p, int p1, int p2) {
+__device__ __forceinline__ void d_gs4(T *__restrict__ u, const T *__restrict__ b, LevelView lv, OpParams<T> p, int p1, int p2) {
   const int64_t total = (int64_t)lv.nblk * 64;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
@@ -529,6 +534,59 @@ __device__ __forceinline__ void fill_corner_cell(T *__restrict__ u, const LevelV
       ub[x + kS * y] = v;
     }
   }
+}
+
+
+// The kernels of the per-operation path: each a grid-stride loop over its work, so the
+// same bodies also run as the operations of one cooperative launch (srmg_seq.cu).
+template <typename T>
+__global__ void k_fill_ghost(T *__restrict__ u, LevelView lv, Signs sg, int mask) {
+  d_fill_ghost<T>(u, lv, sg, mask);
+}
+
+template <typename T>
+__global__ void k_gs_colour(T *__restrict__ u, const T *__restrict__ b, LevelView lv,
+                            OpParams<T> p, WTab<T> wt, int parity) {
+  d_gs_colour<T>(u, b, lv, p, wt, parity);
+}
+
+template <typename T>
+__global__ void k_residual(T *__restrict__ r, const T *__restrict__ u, const T *__restrict__ b,
+                           LevelView lv, OpParams<T> p, WTab<T> wt) {
+  d_residual<T>(r, u, b, lv, p, wt);
+}
+
+template <typename T>
+__global__ void k_postrestrict(T *__restrict__ bf, const T *__restrict__ u, const T *__restrict__ r,
+                               LevelView lv, const int2 *__restrict__ coord_of, OpParams<T> p,
+                               WTab<T> wt) {
+  d_postrestrict<T>(bf, u, r, lv, coord_of, p, wt);
+}
+
+template <typename T>
+__global__ void k_restrict(T *__restrict__ u, LevelView lv) {
+  d_restrict<T>(u, lv);
+}
+
+template <typename T>
+__global__ void k_interp_add(T *__restrict__ u, const T *__restrict__ u1, LevelView lv) {
+  d_interp_add<T>(u, u1, lv);
+}
+
+template <typename T>
+__global__ void k_copy_level(T *__restrict__ dst, const T *__restrict__ src, LevelView lv) {
+  d_copy_level<T>(dst, src, lv);
+}
+
+template <typename T>
+__global__ void k_diff_level(T *__restrict__ dst, const T *__restrict__ a1, const T *a2,
+                             LevelView lv) {
+  d_diff_level<T>(dst, a1, a2, lv);
+}
+
+template <typename T>
+__global__ void k_gs4(T *__restrict__ u, const T *__restrict__ b, LevelView lv, OpParams<T> p, int p1, int p2) {
+  d_gs4<T>(u, b, lv, p, p1, p2);
 }
 
 }  // namespace srmg

@@ -1,0 +1,90 @@
+// srmg_seq.cu -- the sequencer: a recorded per-operation V-cycle (srmg_seq.cuh) as one
+// cooperative launch.
+//
+// The V-cycles that cannot use the persistent engine (order-4 stencils, BoxStencil
+// trees with corner ghosts, the engine switched off) are several hundred small
+// dependent operations per cycle: GS colours, ghost-fill passes, residuals,
+// restrictions, prolongations.  Launched one by one (or replayed from a CUDA graph)
+// each costs a kernel launch of ~7 us for a few microseconds of work.  The sequencer
+// runs the same operations, the same grid-stride bodies, inside one launch: a record
+// per operation, a grid barrier (release/acquire on a counter, bounded wait) between
+// consecutive records.  The barrier orders the operations and makes each one's writes
+// visible to the next as two stream-ordered launches would, so the results are
+// bit-identical to the launches they replace.
+#include <cstring>
+
+#include "srmg_ctx.h"
+#include "srmg_engine.cuh"
+#include "srmg_internal.h"
+#include "srmg_seq.cuh"
+
+using namespace srmg;
+
+#define CK(call)                                              \
+  do {                                                        \
+    int _rc = cuda_check(ctx, (call), #call);                 \
+    if (_rc) return _rc;                                      \
+  } while (0)
+#define RC(call)               \
+  do {                         \
+    int _rc = (call);          \
+    if (_rc) return _rc;       \
+  } while (0)
+
+namespace {
+
+constexpr int kSeqThreads = 512;
+
+template <typename T>
+__global__ void __launch_bounds__(kSeqThreads, 1)
+    k_sequencer(const SeqOp<T> *__restrict__ ops, int nops, WTab<T> wt, const int2 *__restrict__ coord_of,
+                unsigned *bar, int *err, long long timeout_ns) {
+  unsigned epoch = 0;
+  for (int i = 0; i < nops; ++i) {
+    const SeqOp<T> &op = ops[i];
+    switch (op.kind) {
+      case SEQ_FILL: d_fill_ghost<T>(op.a, op.lv, op.sg, op.i0); break;
+      case SEQ_GS_COLOUR: d_gs_colour<T>(op.a, op.b, op.lv, op.p, wt, op.i0); break;
+      case SEQ_GS4: d_gs4<T>(op.a, op.b, op.lv, op.p, op.i0, op.i1); break;
+      case SEQ_RESIDUAL: d_residual<T>(op.a, op.b, op.c, op.lv, op.p, wt); break;
+      case SEQ_POSTRESTRICT: d_postrestrict<T>(op.a, op.b, op.c, op.lv, coord_of, op.p, wt); break;
+      case SEQ_RESTRICT: d_restrict<T>(op.a, op.lv); break;
+      case SEQ_INTERP_ADD: d_interp_add<T>(op.a, op.b, op.lv); break;
+      case SEQ_COPY: d_copy_level<T>(op.a, op.b, op.lv); break;
+      case SEQ_DIFF: d_diff_level<T>(op.a, op.b, op.c, op.lv); break;
+      default:
+        if (threadIdx.x == 0) atomicCAS(err, 0, 4);
+        return;
+    }
+    if (i + 1 < nops && !grid_barrier(bar, err, epoch, timeout_ns)) return;
+  }
+}
+
+}  // namespace
+
+// One launch of the sequencer over `nops` records at d_ops (device memory), on the
+// context's stream.  The barrier counter and error word are the persistent engine's
+// (zeroed here, read by engine_check).
+int srmg::seq_launch(srmg_ctx *ctx, const void *d_ops, int nops) {
+  if (nops <= 0) return SRMG_OK;
+  const void *fn = (const void *)k_sequencer<double>;
+  if (ctx->num_sms == 0) CK(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSeqThreads, 0));
+  if (per_sm < 1) return fail(ctx, SRMG_ERR_CUDA, "sequencer kernel cannot be resident (occupancy 0)");
+  const size_t sync_bytes = 256 + sizeof(int) * (size_t)ctx->nitems;
+  RC(ensure(ctx, ctx->sync, sync_bytes));
+  CK(cudaMemsetAsync(ctx->sync.p, 0, 256, ctx->stream));
+  const SeqOp<double> *ops = (const SeqOp<double> *)d_ops;
+  WTab<double> wt{ctx->d_wm64, ctx->d_wp64};
+  const int2 *coord_of = ctx->d_coord_of;
+  unsigned *bar = (unsigned *)ctx->sync.p;
+  int *err = (int *)((char *)ctx->sync.p + 128);
+  long long timeout = 2000000000LL;  // 2 s per barrier wait
+  void *args[] = {&ops, &nops, &wt, &coord_of, &bar, &err, &timeout};
+  CK(cudaLaunchCooperativeKernel(fn, dim3(ctx->num_sms), dim3(kSeqThreads), args, 0, ctx->stream));
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+size_t srmg::seq_op_bytes() { return sizeof(SeqOp<double>); }

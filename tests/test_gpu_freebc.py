@@ -59,8 +59,12 @@ def test_freebc_sources_and_b(dim, stencil):
     import torch
     qg, ug = torch_cuda(q), torch_cuda(u)
     bg = torch.zeros(len(f), dtype=torch.float64, device="cuda")
+    l0 = ctx.launches()
     mg.freebc_(ctx, qg, ug, p.h1, p.s, b_out=bg)
     ctx.synchronize()
+    # n <= 8192, a power of two: the transform pair in one CTA, then the sources of all
+    # levels in one launch
+    assert ctx.launches() - l0 == 2
     qn = qg.cpu().numpy()
     assert rel_l2(bg.cpu().numpy(), bo) <= REL
     changed = qo != q

@@ -1,7 +1,9 @@
-"""Per-operation V-cycles replayed from captured CUDA graphs (option `op_graphs`, on by
-default) give bit-identical results to the same kernels launched one by one, for every
-key (fields, operator, sweep counts, tree): a BoxStencil order-4 tree, a StarStencil
-tree with the persistent engine off, and an octree."""
+"""Per-operation V-cycles run three ways -- kernel by kernel, replayed from a captured
+CUDA graph (option `op_graphs`), and as one cooperative launch of the sequencer (option
+`op_sequencer`, on by default for 2D trees) -- give bit-identical results for every key
+(fields, operator, sweep counts, tree): a BoxStencil order-4 tree, a StarStencil tree
+with the persistent engine off, and an octree (graphs only: the sequencer records 2D
+cycles)."""
 import numpy as np
 import pytest
 
@@ -28,23 +30,33 @@ def cases():
     yield "octree", (lambda: mg.Context(0, D=3).set_tree(t, conn)), p3.b, p3.s, 0, p3.bc, None
 
 
+MODES = {"kernels": dict(op_graphs=0, op_sequencer=0), "graphs": dict(op_graphs=1, op_sequencer=0),
+         "sequencer": dict(op_graphs=0, op_sequencer=1)}
+
+
 @pytest.mark.parametrize("case", list(cases()), ids=lambda c: c[0])
-def test_graph_replay_is_bit_identical(case):
+def test_replay_and_sequencer_are_bit_identical(case):
     import torch
     _, make, b0, s, geom, bc, lpl = case
     results = {}
-    for graphs in (0, 1):
-        ctx = make().set_option("op_graphs", graphs)
+    for mode, opts in MODES.items():
+        ctx = make()
+        for k, v in opts.items():
+            ctx.set_option(k, v)
         b = torch.from_numpy(b0).cuda()
         u, r, u1 = torch.zeros_like(b), torch.zeros_like(b), torch.zeros_like(b)
         torch.cuda.synchronize()
         outs = []
-        # two calls of the same key (capture, then replay), then a new key (other s)
+        l0 = ctx.launches()
+        # two calls of the same key (record / capture, then replay), then a new key (other s)
         for ss in (s, s, 0.5 * s):
             mg.vcycle_(ctx, u, b, r, u1, ss, geom, bc, lpl, ndown=2, ntop=4, nup=2, ncycles=2)
             ctx.synchronize()
             outs.append(u.cpu().numpy().copy())
-        results[graphs] = outs
+        results[mode] = (outs, ctx.launches() - l0)
         ctx.close()
-    for a, g in zip(results[0], results[1]):
-        np.testing.assert_array_equal(a.view(np.uint64), g.view(np.uint64))
+    for mode in ("graphs", "sequencer"):
+        for a, g in zip(results["kernels"][0], results[mode][0]):
+            np.testing.assert_array_equal(a.view(np.uint64), g.view(np.uint64), err_msg=mode)
+    if case[0] != "octree":
+        assert results["sequencer"][1] == 3  # one launch per call
