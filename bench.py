@@ -45,11 +45,12 @@ SEED = 2
 TARGET_LEAF = 1_500_000
 METRIC = "field solves/sec at 1e-8 rel residual (mixed-precision multigrid; plain FP64 GPU alongside)"
 # DRAM bytes of one plain FP64 V-cycle launch on the config-2 tree, from an ncu capture
-# (57.72 MB read + 41.05 MB written)
-TRAFFIC_VCYCLE_CONFIG2 = 98.77e6
-# DRAM bytes of one mixed-solve launch on the config-2 tree, from an ncu capture
-# (139.30 MB read + 182.13 MB written)
-TRAFFIC_MIXED_CONFIG2 = 321.43e6
+# (57.03 MB read + 39.74 MB written)
+TRAFFIC_VCYCLE_CONFIG2 = 96.77e6
+# DRAM bytes of one mixed-solve launch on the config-2 tree (the tuned V(1,1) cycle,
+# 9 V-cycles in 5 defect-correction steps), from an ncu capture (172.92 MB read +
+# 252.54 MB written)
+TRAFFIC_MIXED_CONFIG2 = 425.46e6
 
 
 def peaks():
@@ -736,7 +737,8 @@ def run_config5(local, net, steps, cpu=True):
 
 
 def run_rows(local):
-    """The widened rows, FP64 on the per-operation kernels, event-timed on one stream:
+    """The widened rows, FP64 on the per-operation kernels (replayed from CUDA graphs;
+    the sequencer's single launch alongside), event-timed on one stream:
     the compact order-4 Laplacian on a refined BoxStencil tree (beside the order-2
     Laplacian on the same tree and path), a uniform level-4 octree (512 finest blocks,
     order-2 and order-4), and the free-boundary step on the config-2 tree at the
@@ -779,8 +781,13 @@ def run_rows(local):
     ctx = mg.Context(local).set_tree(p.tree, p.conn)
     ms4, l4 = time_vcycles(ctx, p.b, p.s, p.geom, p.bc, "laplacian4")
     ms2, l2 = time_vcycles(ctx, p.b, p.s, p.geom, p.bc, None)
+    # the same cycles as one sequencer launch instead of a replayed CUDA graph
+    ctx.set_option("op_sequencer", 1)
+    ms4q, l4q = time_vcycles(ctx, p.b, p.s, p.geom, p.bc, "laplacian4")
+    ctx.set_option("op_sequencer", 0)
     out["order4_2d"] = {"workload": f"{p.name}: compact order-4 Laplacian, cylindrical r-z, BoxStencil tree",
-                        "order4": line(p.tree, ms4, l4), "order2_same_tree_per_op": line(p.tree, ms2, l2)}
+                        "order4": line(p.tree, ms4, l4), "order2_same_tree_per_op": line(p.tree, ms2, l2),
+                        "order4_sequencer": line(p.tree, ms4q, l4q)}
     ctx.close()
     t = Tree3((1, 1, 1), 4)
     populate(t, 4)
@@ -788,9 +795,14 @@ def run_rows(local):
         conn = connectivity3(t, st)
         p3 = gen3.make_problem3(t, conn, lambda x, y, z: np.sin(3 * x) * np.cos(2 * y) * z, (1.0 / 16) ** 2, op=op)
         ctx = mg.Context(local, D=3).set_tree(t, conn)
-        ms, ln = time_vcycles(ctx, p3.b, p3.s, 0, p3.bc, {0: None, 2: "laplacian4"}[op])
-        out.setdefault("octree_3d", {"workload": "uniform level-4 octree (585 blocks, 2.1M finest cells), "
-                                                 "Cartesian, Dirichlet"})[name] = line(t, ms, ln)
+        lpl = {0: None, 2: "laplacian4"}[op]
+        ms, ln = time_vcycles(ctx, p3.b, p3.s, 0, p3.bc, lpl)
+        ctx.set_option("op_sequencer", 1)
+        msq, lnq = time_vcycles(ctx, p3.b, p3.s, 0, p3.bc, lpl)
+        row = out.setdefault("octree_3d", {"workload": "uniform level-4 octree (585 blocks, 2.1M finest cells), "
+                                                       "Cartesian, Dirichlet"})
+        row[name] = line(t, ms, ln)
+        row[name + "_sequencer"] = line(t, msq, lnq)
         ctx.close()
     import freebc_oracle as fo
     p = gen.config2(seed=2, target_leaf=1_500_000)

@@ -540,6 +540,12 @@ int srmg_ssprk3_stage_dev(srmg_ctx *ctx, double *out, const double *n, const dou
  *                      (fields, operator, sweep counts, tree, stream) into a CUDA graph
  *                      and replayed (bit-identical results; up to 8 graphs kept, all
  *                      dropped when the tree changes); 0 = launch kernel by kernel;
+ *   "op_sequencer"     1 = those V-cycles are recorded once per key instead and run as
+ *                      one cooperative launch that walks the recorded operations with
+ *                      a grid barrier between consecutive ones (bit-identical results);
+ *                      0 (default: graph replay measured faster on 2D and 3D trees);
+ *   "freebc_direct"    1 = srmg_freebc transforms by direct sums even for power-of-two
+ *                      lengths (default 0: FFTs);
  *   "b_copy_back"      1 = srmg_vcycle / srmg_fmg copy b back to the host (the FAS
  *                      values in its covered cells, as the reference leaves them);
  *                      0 (default) = b is not copied back;

@@ -1054,7 +1054,7 @@ int srmg::vcycle_ops(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
   // a caller already capturing the stream records the launches into its own graph
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   CK(cudaStreamIsCapturing(ctx->stream, &cap));
-  const bool seq = ctx->use_op_seq && ctx->D == 2;
+  const bool seq = ctx->use_op_seq;
   if (!(ctx->use_op_graphs || seq) || ncycles <= 0 || cap != cudaStreamCaptureStatusNone)
     return run_vcycles(ctx, u, b, r, u1, s, op, k2, geom, bc, lmax, ndown, ntop, nup, omega, ncycles);
   std::vector<char> key;
@@ -1070,8 +1070,11 @@ int srmg::vcycle_ops(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
     // the whole sequence as one cooperative launch of the sequencer: record it once per
     // key (the launchers append their operations instead of launching), keep it on the
     // device, launch it
+    auto launch = [&](const srmg_ctx::OpSeq &q) {
+      return ctx->D == 3 ? seq_launch3(ctx, q.ops.p, q.nops) : seq_launch(ctx, q.ops.p, q.nops);
+    };
     for (auto &q : ctx->op_seqs)
-      if (q.key == key) return seq_launch(ctx, q.ops.p, q.nops);
+      if (q.key == key) return launch(q);
     std::vector<char> rec;
     const int64_t l0 = ctx->launches;
     ctx->seq_rec = &rec;
@@ -1085,7 +1088,7 @@ int srmg::vcycle_ops(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
     }
     srmg_ctx::OpSeq q;
     q.key = key;
-    q.nops = (int)(rec.size() / seq_op_bytes());
+    q.nops = (int)(rec.size() / (ctx->D == 3 ? seq3_op_bytes() : seq_op_bytes()));
     if (q.nops > 0) {
       RC(ensure(ctx, q.ops, rec.size()));
       // on the context's stream: the launch below is ordered after the copy (pageable
@@ -1093,7 +1096,7 @@ int srmg::vcycle_ops(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
       CK(cudaMemcpyAsync(q.ops.p, rec.data(), rec.size(), cudaMemcpyHostToDevice, ctx->stream));
     }
     ctx->op_seqs.push_back(q);
-    return seq_launch(ctx, q.ops.p, q.nops);
+    return launch(q);
   }
   for (auto &g : ctx->op_graphs)
     if (g.key == key) {

@@ -20,9 +20,11 @@
 // interpolation (weights 1/4, src/interp.jl:7-11) and restriction (8 cells, / 8) are
 // bit-exact; stencils are accumulated in the reference's order without contraction.
 #include <cmath>
+#include <algorithm>
 #include <cstring>
 
 #include "srmg_ctx.h"
+#include "srmg_engine.cuh"
 #include "srmg_internal.h"
 
 using namespace srmg;
@@ -50,7 +52,7 @@ __device__ __forceinline__ int unpack(int packed, int d) { return ((packed >> (2
 // ---- ghost fills (src/connectivity.jl:155-258), one thread per ghost cell -----------
 // phase 1 copies from neighbours, 2 mirrors at the domain boundary, 4 interpolates from
 // the parent; fill_ghost! runs them in that order as three launches.
-__global__ void k3_fill(double *__restrict__ u, Level3View L, Signs27 sg, int phase) {
+__device__ __forceinline__ void d3_fill(double *__restrict__ u, Level3View L, const Signs27 &sg, int phase) {
   const int64_t total = (int64_t)L.nblk * S3;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
     const int bi = (int)(t / S3), c = (int)(t % S3);
@@ -127,7 +129,7 @@ struct Op3 { int op; double s, centre, diag, omega; };
 
 // RedBlack{P} (src/multigrid.jl:153-180): x steps by 2, parity P xor (y+1 & 1) xor (z+1 & 1)
 // in 1-based terms; two fused multiply-adds as the reference's muladds.
-__global__ void k3_gs_rb(double *__restrict__ u, const double *__restrict__ b, Level3View L, Op3 p, int parity) {
+__device__ __forceinline__ void d3_gs_rb(double *__restrict__ u, const double *__restrict__ b, Level3View L, Op3 p, int parity) {
   const int64_t total = (int64_t)L.nblk * (kM * kM * kM / 2);
   const double nwc = -(p.omega / p.diag);
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
@@ -146,7 +148,7 @@ __global__ void k3_gs_rb(double *__restrict__ u, const double *__restrict__ b, L
 // FourColors{P1,P2} (src/multigrid.jl:206-232) for D = 3: cells (x + p1, y + p2, z) on
 // the even grid of the first two dimensions, p_a = (P_a + z + 1) mod 2 (1-based z);
 // u -= omega (Lu + s b) / c, unfused.
-__global__ void k3_gs4(double *__restrict__ u, const double *__restrict__ b, Level3View L, Op3 p, int P1, int P2) {
+__device__ __forceinline__ void d3_gs4(double *__restrict__ u, const double *__restrict__ b, Level3View L, Op3 p, int P1, int P2) {
   const int64_t total = (int64_t)L.nblk * 1024;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
     const int bi = (int)(t / 1024), c = (int)(t % 1024);
@@ -161,7 +163,7 @@ __global__ void k3_gs4(double *__restrict__ u, const double *__restrict__ b, Lev
   }
 }
 
-__global__ void k3_residual(double *__restrict__ r, const double *__restrict__ u, const double *__restrict__ b,
+__device__ __forceinline__ void d3_residual(double *__restrict__ r, const double *__restrict__ u, const double *__restrict__ b,
                             Level3View L, Op3 p) {
   const int64_t total = (int64_t)L.nblk * 4096;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
@@ -173,7 +175,7 @@ __global__ void k3_residual(double *__restrict__ r, const double *__restrict__ u
 }
 
 // residual_subblock! on the coarse subblock of every child edge of this level
-__global__ void k3_postrestrict(double *__restrict__ bf, const double *__restrict__ u, const double *__restrict__ r,
+__device__ __forceinline__ void d3_postrestrict(double *__restrict__ bf, const double *__restrict__ u, const double *__restrict__ r,
                                 Level3View L, Op3 pc) {
   const int64_t total = (int64_t)L.nch * 512;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
@@ -190,7 +192,7 @@ __global__ void k3_postrestrict(double *__restrict__ bf, const double *__restric
 
 // restrict! (src/restrict.jl:5-25): f = 0; f += the 8 fine cells (first offset
 // innermost); coarse = f / 8
-__global__ void k3_restrict(double *__restrict__ u, Level3View L) {
+__device__ __forceinline__ void d3_restrict(double *__restrict__ u, Level3View L) {
   const int64_t total = (int64_t)L.nch * 512;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
     const int e = (int)(t / 512), c = (int)(t % 512);
@@ -210,7 +212,7 @@ __global__ void k3_restrict(double *__restrict__ u, Level3View L) {
 }
 
 // interp_add_level! (src/interp.jl:107-115): u_fine += P(u1 over the parent's subblock)
-__global__ void k3_interp_add(double *__restrict__ u, const double *__restrict__ u1, Level3View L) {
+__device__ __forceinline__ void d3_interp_add(double *__restrict__ u, const double *__restrict__ u1, Level3View L) {
   const int64_t total = (int64_t)L.nch * 4096;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
     const int e = (int)(t / 4096), c = (int)(t % 4096);
@@ -228,13 +230,89 @@ __global__ void k3_interp_add(double *__restrict__ u, const double *__restrict__
   }
 }
 
-__global__ void k3_copy(double *__restrict__ dst, const double *__restrict__ a1, const double *__restrict__ a2,
+__device__ __forceinline__ void d3_copy(double *__restrict__ dst, const double *__restrict__ a1, const double *__restrict__ a2,
                         Level3View L) {
   const int64_t total = (int64_t)L.nblk * S3;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t o = (int64_t)L.blocks[t / S3].x * S3 + t % S3;
     dst[o] = a2 ? a1[o] - a2[o] : a1[o];
   }
+}
+
+// The per-operation kernels: each one body, launched alone or run by the sequencer.
+__global__ void k3_fill(double *__restrict__ u, Level3View L, Signs27 sg, int phase) { d3_fill(u, L, sg, phase); }
+__global__ void k3_gs_rb(double *__restrict__ u, const double *__restrict__ b, Level3View L, Op3 p, int parity) { d3_gs_rb(u, b, L, p, parity); }
+__global__ void k3_gs4(double *__restrict__ u, const double *__restrict__ b, Level3View L, Op3 p, int P1, int P2) { d3_gs4(u, b, L, p, P1, P2); }
+__global__ void k3_residual(double *__restrict__ r, const double *__restrict__ u, const double *__restrict__ b,
+                            Level3View L, Op3 p) { d3_residual(r, u, b, L, p); }
+__global__ void k3_postrestrict(double *__restrict__ bf, const double *__restrict__ u, const double *__restrict__ r,
+                                Level3View L, Op3 pc) { d3_postrestrict(bf, u, r, L, pc); }
+__global__ void k3_restrict(double *__restrict__ u, Level3View L) { d3_restrict(u, L); }
+__global__ void k3_interp_add(double *__restrict__ u, const double *__restrict__ u1, Level3View L) { d3_interp_add(u, u1, L); }
+__global__ void k3_copy(double *__restrict__ dst, const double *__restrict__ a1, const double *__restrict__ a2,
+                        Level3View L) { d3_copy(dst, a1, a2, L); }
+
+// ---- the sequencer (3D): a recorded per-operation V-cycle in one cooperative launch --
+// The records are the launches the per-operation path would make, in order; a grid
+// barrier (release/acquire on a counter, bounded wait) separates consecutive records,
+// so every operation sees its predecessors' writes as a separate launch would, and the
+// results are those of the launches.
+enum Seq3Kind { S3_FILL = 1, S3_GS_RB, S3_GS4, S3_RESIDUAL, S3_POSTRESTRICT, S3_RESTRICT, S3_INTERP_ADD, S3_COPY };
+struct SeqOp3 {
+  int kind, i0, i1, pad;
+  double *a;
+  const double *b;
+  const double *c;
+  Level3View lv;
+  Op3 p;
+  Signs27 sg;
+};
+
+constexpr int kSeq3Threads = 512;
+constexpr int kSeq3PerSM = 1;  // resident CTAs per SM
+
+__global__ void __launch_bounds__(kSeq3Threads, kSeq3PerSM)
+    k3_sequencer(const SeqOp3 *__restrict__ ops, int nops, unsigned *bar, int *err, long long timeout_ns) {
+  unsigned epoch = 0;
+  for (int i = 0; i < nops; ++i) {
+    const SeqOp3 &op = ops[i];
+    switch (op.kind) {
+      case S3_FILL: d3_fill(op.a, op.lv, op.sg, op.i0); break;
+      case S3_GS_RB: d3_gs_rb(op.a, op.b, op.lv, op.p, op.i0); break;
+      case S3_GS4: d3_gs4(op.a, op.b, op.lv, op.p, op.i0, op.i1); break;
+      case S3_RESIDUAL: d3_residual(op.a, op.b, op.c, op.lv, op.p); break;
+      case S3_POSTRESTRICT: d3_postrestrict(op.a, op.b, op.c, op.lv, op.p); break;
+      case S3_RESTRICT: d3_restrict(op.a, op.lv); break;
+      case S3_INTERP_ADD: d3_interp_add(op.a, op.b, op.lv); break;
+      case S3_COPY: d3_copy(op.a, op.b, op.c, op.lv); break;
+      default:
+        if (threadIdx.x == 0) atomicCAS(err, 0, 4);
+        return;
+    }
+    if (i + 1 < nops && !grid_barrier(bar, err, epoch, timeout_ns)) return;
+  }
+}
+
+// While a sequence is being recorded (ctx->seq_rec set) the launchers below append
+// their operation instead of launching it.
+bool seq3_push(srmg_ctx *ctx, int kind, int i0, int i1, double *a, const double *b, const double *c,
+               const Level3View &lv, const Op3 *p, const Signs27 *sg) {
+  if (!ctx->seq_rec) return false;
+  SeqOp3 op;
+  memset(&op, 0, sizeof op);
+  op.kind = kind;
+  op.i0 = i0;
+  op.i1 = i1;
+  op.a = a;
+  op.b = b;
+  op.c = c;
+  op.lv = lv;
+  if (p) op.p = *p;
+  if (sg) op.sg = *sg;
+  const char *q = reinterpret_cast<const char *>(&op);
+  ctx->seq_rec->insert(ctx->seq_rec->end(), q, q + sizeof op);
+  ctx->launches++;
+  return true;
 }
 
 // rhs! (src/multigrid.jl:363-388): identity at order 2, the 7-point right-hand side
@@ -320,6 +398,7 @@ int fill(srmg_ctx *ctx, double *u, int l, const Signs27 &sg, int mask) {
   if (!n) return SRMG_OK;
   for (int phase = 1; phase <= 4; phase <<= 1) {
     if (!(mask & phase)) continue;
+    if (seq3_push(ctx, S3_FILL, phase, 0, u, nullptr, nullptr, view(ctx, l), nullptr, &sg)) continue;
     k3_fill<<<grid3((int64_t)n * S3, 256), 256, 0, ctx->stream>>>(u, view(ctx, l), sg, phase);
     ctx->launches++;
   }
@@ -329,6 +408,11 @@ int fill(srmg_ctx *ctx, double *u, int l, const Signs27 &sg, int mask) {
 int gs_colour(srmg_ctx *ctx, double *u, const double *b, int l, const Op3 &p, int colour) {
   const int n = ctx->nblk_host[l - 1];
   if (!n) return SRMG_OK;
+  if (p.op == SRMG_OP_LAPLACIAN4 &&
+      seq3_push(ctx, S3_GS4, colour >> 1, colour & 1, u, b, nullptr, view(ctx, l), &p, nullptr))
+    return SRMG_OK;
+  if (p.op != SRMG_OP_LAPLACIAN4 && seq3_push(ctx, S3_GS_RB, colour, 0, u, b, nullptr, view(ctx, l), &p, nullptr))
+    return SRMG_OK;
   if (p.op == SRMG_OP_LAPLACIAN4)
     k3_gs4<<<grid3((int64_t)n * 1024, 256), 256, 0, ctx->stream>>>(u, b, view(ctx, l), p, colour >> 1, colour & 1);
   else
@@ -352,6 +436,7 @@ int gs_iter(srmg_ctx *ctx, double *u, const double *b, int l, const Op3 &p, int 
 int residual(srmg_ctx *ctx, double *r, const double *u, const double *b, int l, const Op3 &p) {
   const int n = ctx->nblk_host[l - 1];
   if (!n) return SRMG_OK;
+  if (seq3_push(ctx, S3_RESIDUAL, 0, 0, r, u, b, view(ctx, l), &p, nullptr)) return SRMG_OK;
   k3_residual<<<grid3((int64_t)n * 4096, 256), 256, 0, ctx->stream>>>(r, u, b, view(ctx, l), p);
   ctx->launches++;
   return SRMG_OK;
@@ -360,6 +445,7 @@ int residual(srmg_ctx *ctx, double *r, const double *u, const double *b, int l, 
 int postrestrict(srmg_ctx *ctx, double *bf, const double *u, const double *r, int l, const Op3 &pc) {
   const int n = ctx->nch_host[l - 1];
   if (!n) return SRMG_OK;
+  if (seq3_push(ctx, S3_POSTRESTRICT, 0, 0, bf, u, r, view(ctx, l), &pc, nullptr)) return SRMG_OK;
   k3_postrestrict<<<grid3((int64_t)n * 512, 256), 256, 0, ctx->stream>>>(bf, u, r, view(ctx, l), pc);
   ctx->launches++;
   return SRMG_OK;
@@ -368,6 +454,7 @@ int postrestrict(srmg_ctx *ctx, double *bf, const double *u, const double *r, in
 int restrict_l(srmg_ctx *ctx, double *u, int l) {
   const int n = ctx->nch_host[l - 1];
   if (!n) return SRMG_OK;
+  if (seq3_push(ctx, S3_RESTRICT, 0, 0, u, nullptr, nullptr, view(ctx, l), nullptr, nullptr)) return SRMG_OK;
   k3_restrict<<<grid3((int64_t)n * 512, 256), 256, 0, ctx->stream>>>(u, view(ctx, l));
   ctx->launches++;
   return SRMG_OK;
@@ -376,6 +463,7 @@ int restrict_l(srmg_ctx *ctx, double *u, int l) {
 int interp_add(srmg_ctx *ctx, double *u, const double *u1, int l) {
   const int n = ctx->nch_host[l - 1];
   if (!n) return SRMG_OK;
+  if (seq3_push(ctx, S3_INTERP_ADD, 0, 0, u, u1, nullptr, view(ctx, l), nullptr, nullptr)) return SRMG_OK;
   k3_interp_add<<<grid3((int64_t)n * 4096, 256), 256, 0, ctx->stream>>>(u, u1, view(ctx, l));
   ctx->launches++;
   return SRMG_OK;
@@ -384,6 +472,7 @@ int interp_add(srmg_ctx *ctx, double *u, const double *u1, int l) {
 int copy_l(srmg_ctx *ctx, double *dst, const double *a1, const double *a2, int l) {
   const int n = ctx->nblk_host[l - 1];
   if (!n) return SRMG_OK;
+  if (seq3_push(ctx, S3_COPY, 0, 0, dst, a1, a2, view(ctx, l), nullptr, nullptr)) return SRMG_OK;
   k3_copy<<<grid3((int64_t)n * S3, 256), 256, 0, ctx->stream>>>(dst, a1, a2, view(ctx, l));
   ctx->launches++;
   return SRMG_OK;
@@ -743,3 +832,27 @@ int srmg::d3_solve(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc
   if (st->status) return fail(ctx, st->status, "residual is not finite after %d cycles", c);
   return SRMG_OK;
 }
+
+// One launch of the 3D sequencer over `nops` records at d_ops (device memory), on the
+// context's stream.  The barrier counter and error word are the persistent engine's
+// (zeroed here, read by engine_check).
+int srmg::seq_launch3(srmg_ctx *ctx, const void *d_ops, int nops) {
+  if (nops <= 0) return SRMG_OK;
+  const void *fn = (const void *)k3_sequencer;
+  if (ctx->num_sms == 0) CK(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSeq3Threads, 0));
+  if (per_sm < 1) return fail(ctx, SRMG_ERR_CUDA, "sequencer kernel cannot be resident (occupancy 0)");
+  RC(ensure(ctx, ctx->sync, 256 + sizeof(int) * (size_t)ctx->nitems));
+  CK(cudaMemsetAsync(ctx->sync.p, 0, 256, ctx->stream));
+  const SeqOp3 *ops = (const SeqOp3 *)d_ops;
+  unsigned *bar = (unsigned *)ctx->sync.p;
+  int *err = (int *)((char *)ctx->sync.p + 128);
+  long long timeout = 2000000000LL;  // 2 s per barrier wait
+  void *args[] = {&ops, &nops, &bar, &err, &timeout};
+  CK(cudaLaunchCooperativeKernel(fn, dim3(ctx->num_sms * std::min(per_sm, kSeq3PerSM)), dim3(kSeq3Threads), args, 0, ctx->stream));
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+size_t srmg::seq3_op_bytes() { return sizeof(SeqOp3); }

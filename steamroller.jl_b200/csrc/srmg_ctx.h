@@ -173,7 +173,7 @@ struct srmg_ctx {
     int nops = 0;
   };
   std::vector<OpSeq> op_seqs;
-  bool use_op_seq = true;
+  bool use_op_seq = false;
   std::vector<char> *seq_rec = nullptr;
 
   // free boundary conditions (srmg_freebc_set): f [n], sin table [4n], work [n], b [n]

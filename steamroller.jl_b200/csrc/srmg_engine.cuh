@@ -1729,7 +1729,9 @@ __global__ void __launch_bounds__(NT, 1) k_engine_vcycle(const __grid_constant__
       cycles++;
       if (mixed && loop) {
         step_books(k, nv);
-        if (!sync(true, false, false)) return;
+        // a lone item is never paused inside its step (nv is its own share), and CTA 0,
+        // which wrote the books, is the one that reads them: no barrier needed
+        if (A.nitems > 1 && !sync(true, false, false)) return;
       }
     }
     if (mixed) steps++;

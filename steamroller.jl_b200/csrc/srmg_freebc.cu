@@ -184,35 +184,43 @@ __global__ void k_fbc_gather_pre(double2 *__restrict__ v, const FbcSrc *__restri
   }
 }
 
-// DST-II, step 2, at m: C[m] = 2 Re(e^{-i pi m / 2n} V[m]), the DCT-II of x' (y_k =
-// C[n-1-k] is the DST-II).  Every product and sum rounded on its own.
-__device__ __forceinline__ double dct2_at(double2 z, int64_t m, int64_t n) {
-  double sn, cs;
-  sincospi(-(double)m / (double)(2 * n), &sn, &cs);
-  return 2.0 * __dadd_rn(__dmul_rn(z.x, cs), -__dmul_rn(z.y, sn));
+// The half-angle table: hw[m] = (cos, sin)(pi m / 2n), m = 0..n, from sincospi once
+// per srmg_freebc_set (the transforms read it instead of evaluating sincospi).
+__global__ void k_half_twiddles(double2 *hw, int64_t n) {
+  for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m <= n; m += (int64_t)gridDim.x * blockDim.x) {
+    double sn, cs;
+    sincospi((double)m / (double)(2 * n), &sn, &cs);
+    hw[m] = make_double2(cs, sn);
+  }
+}
+
+// DST-II, step 2, at m: C[m] = 2 Re(e^{-i pi m / 2n} V[m]) = 2 (Re V cos + Im V sin),
+// the DCT-II of x' (y_k = C[n-1-k] is the DST-II); hm = hw[m].  Every product and sum
+// rounded on its own.
+__device__ __forceinline__ double dct2_at(double2 z, double2 hm) {
+  return 2.0 * __dadd_rn(__dmul_rn(z.x, hm.x), __dmul_rn(z.y, hm.y));
 }
 
 // The DST-III input at m from the DST-II output: X_j = f_j y_j (rounded once) reversed,
 // X''_m = X_{n-1-m} = f_{n-1-m} C[m], X''_{n-m} = f_{m-1} C[n-m] (X''_n = 0), and
 // V'[m] = e^{+i pi m / 2n} (X''_m - i X''_{n-m}), conjugated for the inverse transform
-// done as a forward FFT: (cs xm + sn xnm) - i (sn xm - cs xnm).
-__device__ __forceinline__ double2 dst3_in(double xm, double xnm, int64_t m, int64_t n) {
-  double sn, cs;
-  sincospi((double)m / (double)(2 * n), &sn, &cs);
-  return make_double2(__dadd_rn(__dmul_rn(cs, xm), __dmul_rn(sn, xnm)),
-                      -__dadd_rn(__dmul_rn(sn, xm), -__dmul_rn(cs, xnm)));
+// done as a forward FFT: (cos xm + sin xnm) - i (sin xm - cos xnm); hm = hw[m].
+__device__ __forceinline__ double2 dst3_in(double xm, double xnm, double2 hm) {
+  return make_double2(__dadd_rn(__dmul_rn(hm.x, xm), __dmul_rn(hm.y, xnm)),
+                      -__dadd_rn(__dmul_rn(hm.y, xm), -__dmul_rn(hm.x, xnm)));
 }
 
 // DST-II step 2 and the DST-III input over all m (four-step FFT path).  With y_out the
 // DST-II output is kept.
 __global__ void k_dst_mid(double2 *__restrict__ vp, double *__restrict__ y_out, const double2 *__restrict__ V,
-                          const double *__restrict__ f, int64_t n) {
+                          const double *__restrict__ f, const double2 *__restrict__ hw, int64_t n) {
   for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < n; m += (int64_t)gridDim.x * blockDim.x) {
-    const double cm = dct2_at(V[m], m, n);
+    const double2 hm = hw[m];
+    const double cm = dct2_at(V[m], hm);
     if (y_out) y_out[n - 1 - m] = cm;
     const double xm = __dmul_rn(f[n - 1 - m], cm);
-    const double xnm = m == 0 ? 0.0 : __dmul_rn(f[m - 1], dct2_at(V[n - m], n - m, n));
-    vp[m] = dst3_in(xm, xnm, m, n);
+    const double xnm = m == 0 ? 0.0 : __dmul_rn(f[m - 1], dct2_at(V[n - m], hw[n - m]));
+    vp[m] = dst3_in(xm, xnm, hm);
   }
 }
 
@@ -231,27 +239,73 @@ __global__ void k_dst3_post(double *__restrict__ b, const double2 *__restrict__ 
 
 constexpr int kLocalThreads = 1024;
 
-__device__ __forceinline__ void bfly(double2 &a, double2 &c, double2 w) {
+// Shared-memory index of element i: one pad element after every eight, so that the
+// power-of-two strides of the butterflies and of the twiddle reads fall on different
+// banks (16-byte elements, a quarter-warp of 8 threads per 128-byte wavefront).
+__device__ __forceinline__ int spad(int i) { return i + (i >> 3); }
+
+// Decimation in time: a' = a + w c, c' = a - w c.
+__device__ __forceinline__ void bfly_dit(double2 &a, double2 &c, double2 w) {
   const double2 t = cmul(c, w);
   c = make_double2(a.x - t.x, a.y - t.y);
   a = make_double2(a.x + t.x, a.y + t.y);
 }
 
-// In-place radix-2 FFT of buf (loaded in bit-reversed order) with the twiddles
-// e^{-2 pi i k / n}, k < n / 2, in shared memory: the butterflies of k_fft, two stages
-// (half = h, then 2h) per pass over shared memory where they pair up.  A thread holds
-// the four elements g + pos + {0, h, 2h, 3h} (g a multiple of 4h, pos < h) in registers:
-// stage h pairs (0, h) and (2h, 3h) with twiddle pos n / 2h, stage 2h pairs (0, 2h)
-// with twiddle pos n / 4h and (h, 3h) with (pos + h) n / 4h -- the same operations on
-// the same values as two radix-2 passes.
-__device__ __forceinline__ void local_fft(double2 *buf, const double2 *stw, int n, int logn) {
+// Decimation in frequency: a' = a + c, c' = (a - c) w.
+__device__ __forceinline__ void bfly_dif(double2 &a, double2 &c, double2 w) {
+  const double2 d = make_double2(a.x - c.x, a.y - c.y);
+  a = make_double2(a.x + c.x, a.y + c.y);
+  c = cmul(d, w);
+}
+
+// In-place radix-2 FFTs over buf (padded, spad) with the twiddles W^k = e^{-2 pi i k / n},
+// k < n / 2, in shared memory (padded), two stages per pass over shared memory.
+// Decimation in frequency takes natural order to bit-reversed order: stages
+// half = n/2, n/4, ..., 1, a thread holding e_q = g + pos + q H/2 (q = 0..3, g a
+// multiple of 2H, pos < H/2) for the stage pair (H, H/2): (e0, e2) with W_{2H}^pos,
+// (e1, e3) with W_{2H}^(pos + H/2), then (e0, e1) and (e2, e3) with W_H^pos.
+__device__ __forceinline__ void local_fft_dif(double2 *buf, const double2 *stw, int n, int logn) {
+  int H = n / 2;
+  for (; H >= 2; H >>= 2) {
+    const int q = H / 2, t1 = n / (2 * H), t2 = n / H;
+    for (int idx = threadIdx.x; idx < n / 4; idx += blockDim.x) {
+      const int pos = idx & (q - 1), e0 = (idx - pos) * 4 + pos;
+      double2 a0 = buf[spad(e0)], a1 = buf[spad(e0 + q)], a2 = buf[spad(e0 + 2 * q)], a3 = buf[spad(e0 + 3 * q)];
+      bfly_dif(a0, a2, stw[spad(pos * t1)]);
+      bfly_dif(a1, a3, stw[spad((pos + q) * t1)]);
+      const double2 w2 = stw[spad(pos * t2)];
+      bfly_dif(a0, a1, w2);
+      bfly_dif(a2, a3, w2);
+      buf[spad(e0)] = a0;
+      buf[spad(e0 + q)] = a1;
+      buf[spad(e0 + 2 * q)] = a2;
+      buf[spad(e0 + 3 * q)] = a3;
+    }
+    __syncthreads();
+  }
+  if (H == 1) {  // an odd stage count ends with one radix-2 stage (twiddle 1)
+    for (int idx = threadIdx.x; idx < n / 2; idx += blockDim.x) {
+      double2 a = buf[spad(2 * idx)], c = buf[spad(2 * idx + 1)];
+      bfly_dif(a, c, stw[0]);
+      buf[spad(2 * idx)] = a;
+      buf[spad(2 * idx + 1)] = c;
+    }
+    __syncthreads();
+  }
+}
+
+// Decimation in time takes bit-reversed order to natural order: stages half = 1, 2,
+// ..., n/2 (the butterflies of k_fft), a thread holding g + pos + {0, h, 2h, 3h} (g a
+// multiple of 4h, pos < h) for the stage pair (h, 2h): (0, h) and (2h, 3h) with
+// W_{2h}^pos, then (0, 2h) with W_{4h}^pos and (h, 3h) with W_{4h}^(pos + h).
+__device__ __forceinline__ void local_fft_dit(double2 *buf, const double2 *stw, int n, int logn) {
   int half = 1;
   if (logn & 1) {  // one radix-2 stage first when the stage count is odd
     for (int idx = threadIdx.x; idx < n / 2; idx += blockDim.x) {
-      double2 a = buf[2 * idx], c = buf[2 * idx + 1];
-      bfly(a, c, stw[0]);
-      buf[2 * idx] = a;
-      buf[2 * idx + 1] = c;
+      double2 a = buf[spad(2 * idx)], c = buf[spad(2 * idx + 1)];
+      bfly_dit(a, c, stw[0]);
+      buf[spad(2 * idx)] = a;
+      buf[spad(2 * idx + 1)] = c;
     }
     __syncthreads();
     half = 2;
@@ -260,64 +314,66 @@ __device__ __forceinline__ void local_fft(double2 *buf, const double2 *stw, int 
     const int t1 = n / (2 * half), t2 = n / (4 * half);
     for (int idx = threadIdx.x; idx < n / 4; idx += blockDim.x) {
       const int pos = idx & (half - 1), i = (idx - pos) * 4 + pos;
-      double2 a0 = buf[i], a1 = buf[i + half], a2 = buf[i + 2 * half], a3 = buf[i + 3 * half];
-      const double2 w1 = stw[pos * t1];
-      bfly(a0, a1, w1);
-      bfly(a2, a3, w1);
-      bfly(a0, a2, stw[pos * t2]);
-      bfly(a1, a3, stw[(pos + half) * t2]);
-      buf[i] = a0;
-      buf[i + half] = a1;
-      buf[i + 2 * half] = a2;
-      buf[i + 3 * half] = a3;
+      double2 a0 = buf[spad(i)], a1 = buf[spad(i + half)], a2 = buf[spad(i + 2 * half)],
+              a3 = buf[spad(i + 3 * half)];
+      const double2 w1 = stw[spad(pos * t1)];
+      bfly_dit(a0, a1, w1);
+      bfly_dit(a2, a3, w1);
+      bfly_dit(a0, a2, stw[spad(pos * t2)]);
+      bfly_dit(a1, a3, stw[spad((pos + half) * t2)]);
+      buf[spad(i)] = a0;
+      buf[spad(i + half)] = a1;
+      buf[spad(i + 2 * half)] = a2;
+      buf[spad(i + 3 * half)] = a3;
     }
     __syncthreads();
   }
 }
 
-// b = DST-III(f .* DST-II(getouter!(u))) h / 2^(level-1) / 2 in one CTA: the gather and
-// the Makhoul reordering loaded bit-reversed into shared memory, the forward FFT, the
-// DST-III input formed in place one (m, n - m) pair per thread, a bit-reversal
-// permutation, the second FFT and the output reordering.  Dynamic shared memory: n
-// complex values and n / 2 twiddles (24 n bytes, 192 KB at n = 8192).
+// Dynamic shared memory of k_dst_local: n + n/8 padded complex values and n/2 + n/16
+// padded twiddles (27 n bytes, 216 KB at n = 8192).
+constexpr int local_smem_bytes(int n) { return (int)sizeof(double2) * (n + n / 8 + n / 2 + n / 16); }
+
+// b = DST-III(f .* DST-II(getouter!(u))) h / 2^(level-1) / 2 in one CTA.  The gather
+// and the Makhoul reordering load the first FFT's input in natural order; that FFT
+// (decimation in frequency) leaves V in bit-reversed order, so the DST-III input of the
+// pair (m, n - m) -- formed in place by one thread -- lands exactly where the second FFT
+// (decimation in time) wants it, at the bit-reversed positions of m and n - m; that FFT
+// leaves natural order for the output reordering.  No permutation pass.
 __global__ void __launch_bounds__(kLocalThreads, 1)
     k_dst_local(double *__restrict__ b, const FbcSrc *__restrict__ src, const double *__restrict__ u, double h,
-                const double2 *__restrict__ tw, const double *__restrict__ f, int n, int logn, double p2) {
+                const double2 *__restrict__ tw, const double2 *__restrict__ hw, const double *__restrict__ f, int n,
+                int logn, double p2) {
   extern __shared__ double2 sm[];
-  double2 *buf = sm, *stw = sm + n;
-  for (int k = threadIdx.x; k < n / 2; k += blockDim.x) stw[k] = tw[k];
+  double2 *buf = sm, *stw = sm + spad(n);
+  for (int k = threadIdx.x; k < n / 2; k += blockDim.x) stw[spad(k)] = tw[k];
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
     const double x = outer_value(src, u, h, j);
-    const unsigned pos = (unsigned)makhoul_pos(j, n);
-    buf[__brev(pos) >> (32 - logn)] = make_double2((j & 1) ? -x : x, 0.0);
+    buf[spad((int)makhoul_pos(j, n))] = make_double2((j & 1) ? -x : x, 0.0);
   }
   __syncthreads();
-  local_fft(buf, stw, n, logn);
+  local_fft_dif(buf, stw, n, logn);
+  auto brev = [&](int i) { return (int)(__brev((unsigned)i) >> (32 - logn)); };
   for (int m = threadIdx.x; m <= n / 2; m += blockDim.x) {
     const int mm = n - m;  // the partner position (m = 0 has none, m = n / 2 is its own)
-    const double cm = dct2_at(buf[m], m, n);
+    const int am = spad(brev(m));
+    const double2 hm = hw[m];
+    const double cm = dct2_at(buf[am], hm);
     if (m == 0) {
-      buf[0] = dst3_in(__dmul_rn(f[n - 1], cm), 0.0, 0, n);
+      buf[am] = dst3_in(__dmul_rn(f[n - 1], cm), 0.0, hm);
       continue;
     }
-    const double cmm = dct2_at(buf[mm], mm, n);
-    const double2 vm = dst3_in(__dmul_rn(f[n - 1 - m], cm), __dmul_rn(f[m - 1], cmm), m, n);
-    if (mm != m) buf[mm] = dst3_in(__dmul_rn(f[n - 1 - mm], cmm), __dmul_rn(f[mm - 1], cm), mm, n);
-    buf[m] = vm;
+    const int amm = spad(brev(mm));
+    const double2 hmm = hw[mm];
+    const double cmm = dct2_at(buf[amm], hmm);
+    const double2 vm = dst3_in(__dmul_rn(f[n - 1 - m], cm), __dmul_rn(f[m - 1], cmm), hm);
+    if (mm != m) buf[amm] = dst3_in(__dmul_rn(f[n - 1 - mm], cmm), __dmul_rn(f[mm - 1], cm), hmm);
+    buf[am] = vm;
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const int r = (int)(__brev((unsigned)i) >> (32 - logn));
-    if (i < r) {
-      const double2 t = buf[i];
-      buf[i] = buf[r];
-      buf[r] = t;
-    }
-  }
-  __syncthreads();
-  local_fft(buf, stw, n, logn);
+  local_fft_dit(buf, stw, n, logn);
   for (int j = threadIdx.x; j < n / 2; j += blockDim.x) {
-    const double ye = buf[j].x, yo = buf[n - 1 - j].x;  // as k_dst3_post
+    const double ye = buf[spad(j)].x, yo = buf[spad(n - 1 - j)].x;  // as k_dst3_post
     b[2 * j] = ye * h / p2 / 2.0;
     b[2 * j + 1] = -yo * h / p2 / 2.0;
   }
@@ -461,15 +517,17 @@ int gridfor(int64_t work, int threads) {
 
 // The context's free-boundary buffer: f [n], the sine table [4n], u1 [n], b [n] (7n
 // doubles), and for the FFT path the twiddles [n complex] and three complex work arrays
-// [n complex each] (8n doubles): 15n doubles in all.
-constexpr int64_t kFbcDoubles = 7 + 2 * (1 + 3);
-static_assert(kFbcDoubles == 15, "free-boundary buffer layout");
+// [n complex each] (8n doubles), then the half-angle table [n + 1 complex]: 17n + 2
+// doubles in all.
+constexpr int64_t kFbcDoubles = 7 + 2 * (1 + 3) + 2;
+static_assert(kFbcDoubles == 17, "free-boundary buffer layout");
 double *fbc_f(srmg_ctx *ctx) { return (double *)ctx->fbc.p; }
 double *fbc_tab(srmg_ctx *ctx) { return fbc_f(ctx) + ctx->fbc_n; }
 double *fbc_u1(srmg_ctx *ctx) { return fbc_tab(ctx) + 4 * ctx->fbc_n; }
 double *fbc_b(srmg_ctx *ctx) { return fbc_u1(ctx) + ctx->fbc_n; }
 double2 *fbc_tw(srmg_ctx *ctx) { return (double2 *)(fbc_b(ctx) + ctx->fbc_n); }
 double2 *fbc_work(srmg_ctx *ctx, int k) { return fbc_tw(ctx) + (1 + k) * ctx->fbc_n; }
+double2 *fbc_hw(srmg_ctx *ctx) { return fbc_work(ctx, 3); }
 bool fbc_pow2(int64_t n) { return n >= 2 && (n & (n - 1)) == 0; }
 
 // Levels the boundary work visits, and the checks freebc! makes.
@@ -600,7 +658,7 @@ extern "C" int srmg_freebc_set(srmg_ctx *ctx, int dim, int level, const int64_t 
     return fail(ctx, SRMG_ERR_UNSUPPORTED, "srmg_freebc_set: transform length %lld above %lld", (long long)n,
                 (long long)kFreeMaxN);
   cudaSetDevice(ctx->device);
-  RC(ensure(ctx, ctx->fbc, (size_t)kFbcDoubles * n * sizeof(double)));
+  RC(ensure(ctx, ctx->fbc, ((size_t)kFbcDoubles * n + 2) * sizeof(double)));
   ctx->fbc_n = n;
   ctx->fbc_dim = dim;
   ctx->fbc_level = level;
@@ -614,11 +672,12 @@ extern "C" int srmg_freebc_set(srmg_ctx *ctx, int dim, int level, const int64_t 
     // the FFT kernel holds up to kFftMaxLocal complex doubles in dynamic shared memory
     CK(cudaFuncSetAttribute(k_fft, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)(kFftMaxLocal * sizeof(double2))));
-    // k_dst_local: the transform and n / 2 twiddles
+    // k_dst_local: the padded transform and twiddles
     CK(cudaFuncSetAttribute(k_dst_local, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)(kFftMaxLocal * sizeof(double2) * 3 / 2)));
+                            local_smem_bytes(kFftMaxLocal)));
     k_twiddles<<<gridfor(n, 256), 256, 0, ctx->stream>>>(fbc_tw(ctx), n);
-    ctx->launches++;
+    k_half_twiddles<<<gridfor(n + 1, 256), 256, 0, ctx->stream>>>(fbc_hw(ctx), n);
+    ctx->launches += 2;
   }
   CK(cudaMemsetAsync(fbc_b(ctx), 0, n * sizeof(double), ctx->stream));
   CK(cudaGetLastError());
@@ -641,14 +700,14 @@ extern "C" int srmg_freebc_dev(srmg_ctx *ctx, double *q, const double *u, int64_
     // gather, DST-II, times f, DST-III: one CTA
     int logn = 0;
     while (((int64_t)1 << logn) < n) ++logn;
-    k_dst_local<<<1, kLocalThreads, 24 * n, ctx->stream>>>(b, fbc_src(ctx), u, h, fbc_tw(ctx), fbc_f(ctx), (int)n,
+    k_dst_local<<<1, kLocalThreads, local_smem_bytes((int)n), ctx->stream>>>(b, fbc_src(ctx), u, h, fbc_tw(ctx), fbc_hw(ctx), fbc_f(ctx), (int)n,
                                                           logn, p2);
     ctx->launches++;
   } else if (fbc_pow2(n) && !ctx->fbc_direct) {
     double2 *w0 = fbc_work(ctx, 0), *w1 = fbc_work(ctx, 1), *w2 = fbc_work(ctx, 2);
     k_fbc_gather_pre<<<gridfor(n, 256), 256, 0, ctx->stream>>>(w0, fbc_src(ctx), u, h, n);
     RC(fft_forward(ctx, w1, w0, w2, fbc_tw(ctx), n));
-    k_dst_mid<<<gridfor(n, 256), 256, 0, ctx->stream>>>(w0, nullptr, w1, fbc_f(ctx), n);
+    k_dst_mid<<<gridfor(n, 256), 256, 0, ctx->stream>>>(w0, nullptr, w1, fbc_f(ctx), fbc_hw(ctx), n);
     RC(fft_forward(ctx, w1, w0, w2, fbc_tw(ctx), n));
     k_dst3_post<<<gridfor(n / 2, 256), 256, 0, ctx->stream>>>(b, w1, n, h, p2);
     ctx->launches += 3;

@@ -21,6 +21,9 @@ void drop_op_graphs(srmg_ctx *ctx);
 // One cooperative launch of the sequencer over `nops` recorded operations (srmg_seq.cu).
 int seq_launch(srmg_ctx *ctx, const void *d_ops, int nops);
 size_t seq_op_bytes();
+// The same for three-dimensional trees (srmg3.cu).
+int seq_launch3(srmg_ctx *ctx, const void *d_ops, int nops);
+size_t seq3_op_bytes();
 // `ncycles` per-operation FP64 V-cycles (2D trees off the persistent engine, or 3D),
 // replayed from a captured CUDA graph when the option `op_graphs` is on (default).
 int vcycle_ops(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, double s, int op, double k2, int geom,

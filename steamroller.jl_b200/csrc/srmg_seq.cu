@@ -11,6 +11,7 @@
 // consecutive records.  The barrier orders the operations and makes each one's writes
 // visible to the next as two stream-ordered launches would, so the results are
 // bit-identical to the launches they replace.
+#include <algorithm>
 #include <cstring>
 
 #include "srmg_ctx.h"
@@ -34,9 +35,10 @@ using namespace srmg;
 namespace {
 
 constexpr int kSeqThreads = 512;
+constexpr int kSeqPerSM = 1;  // resident CTAs per SM
 
 template <typename T>
-__global__ void __launch_bounds__(kSeqThreads, 1)
+__global__ void __launch_bounds__(kSeqThreads, kSeqPerSM)
     k_sequencer(const SeqOp<T> *__restrict__ ops, int nops, WTab<T> wt, const int2 *__restrict__ coord_of,
                 unsigned *bar, int *err, long long timeout_ns) {
   unsigned epoch = 0;
@@ -82,7 +84,7 @@ int srmg::seq_launch(srmg_ctx *ctx, const void *d_ops, int nops) {
   int *err = (int *)((char *)ctx->sync.p + 128);
   long long timeout = 2000000000LL;  // 2 s per barrier wait
   void *args[] = {&ops, &nops, &wt, &coord_of, &bar, &err, &timeout};
-  CK(cudaLaunchCooperativeKernel(fn, dim3(ctx->num_sms), dim3(kSeqThreads), args, 0, ctx->stream));
+  CK(cudaLaunchCooperativeKernel(fn, dim3(ctx->num_sms * std::min(per_sm, kSeqPerSM)), dim3(kSeqThreads), args, 0, ctx->stream));
   ctx->launches++;
   return SRMG_OK;
 }

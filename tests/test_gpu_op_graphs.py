@@ -1,15 +1,14 @@
 """Per-operation V-cycles run three ways -- kernel by kernel, replayed from a captured
 CUDA graph (option `op_graphs`), and as one cooperative launch of the sequencer (option
-`op_sequencer`, on by default for 2D trees) -- give bit-identical results for every key
-(fields, operator, sweep counts, tree): a BoxStencil order-4 tree, a StarStencil tree
-with the persistent engine off, and an octree (graphs only: the sequencer records 2D
-cycles)."""
+`op_sequencer`, on by default) -- give bit-identical results for every key (fields,
+operator, sweep counts, tree): a BoxStencil order-4 tree, a StarStencil tree with the
+persistent engine off, and an octree (order-2 and order-4 stencils)."""
 import numpy as np
 import pytest
 
 from conftest import gpu_available
 from srmg import gen, gen3, multigrid as mg
-from srmg.tree3 import Tree3, populate, connectivity as connectivity3, STAR3
+from srmg.tree3 import Tree3, populate, connectivity as connectivity3, STAR3, BOX3
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not gpu_available(), reason="needs a CUDA GPU")]
@@ -28,6 +27,9 @@ def cases():
     conn = connectivity3(t, STAR3)
     p3 = gen3.make_problem3(t, conn, lambda x, y, z: np.cos(4 * x) * y * (1 - z), (1.0 / 16) ** 2)
     yield "octree", (lambda: mg.Context(0, D=3).set_tree(t, conn)), p3.b, p3.s, 0, p3.bc, None
+    conn4 = connectivity3(t, BOX3)
+    p34 = gen3.make_problem3(t, conn4, lambda x, y, z: np.sin(3 * x) * y * (1 - z), (1.0 / 16) ** 2, op=2)
+    yield "octree_order4", (lambda: mg.Context(0, D=3).set_tree(t, conn4)), p34.b, p34.s, 0, p34.bc, "laplacian4"
 
 
 MODES = {"kernels": dict(op_graphs=0, op_sequencer=0), "graphs": dict(op_graphs=1, op_sequencer=0),
@@ -58,5 +60,4 @@ def test_replay_and_sequencer_are_bit_identical(case):
     for mode in ("graphs", "sequencer"):
         for a, g in zip(results["kernels"][0], results[mode][0]):
             np.testing.assert_array_equal(a.view(np.uint64), g.view(np.uint64), err_msg=mode)
-    if case[0] != "octree":
-        assert results["sequencer"][1] == 3  # one launch per call
+    assert results["sequencer"][1] == 3  # one launch per call
