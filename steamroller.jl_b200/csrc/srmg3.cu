@@ -50,21 +50,50 @@ __device__ __forceinline__ int o3(int x, int y, int z) { return x + S * y + S2 *
 __device__ __forceinline__ int unpack(int packed, int d) { return ((packed >> (2 * d)) & 3) - 1; }
 
 // ---- ghost fills (src/connectivity.jl:155-258), one thread per ghost cell -----------
-// phase 1 copies from neighbours, 2 mirrors at the domain boundary, 4 interpolates from
-// the parent; fill_ghost! runs them in that order as three launches.
+// `phase` is a mask: 1 copies from neighbours, 2 mirrors at the domain boundary, 4
+// interpolates from the parent.  fill_ghost! runs them in that order; on BoxStencil{3}
+// trees an edge or corner ghost can mirror a face ghost that the copy pass writes, so
+// the passes are three launches there.  On StarStencil{3} trees only face ghosts are
+// filled, each reads valid cells of its own level or cells of the parent level, and no
+// ghost reads another: one launch does all three passes with the same results.
+// The ghost cells of a 20^3 block, enumerated: the four z-planes z = 0, 1, 18, 19 whole
+// (4 x 400 cells), then for each of the 16 valid z the rows y = 0, 1, 18, 19 whole
+// (4 x 20) and, on the 16 valid rows, the columns x = 0, 1, 18, 19 -- 3904 cells.
+constexpr int kGhost3 = 4 * S2 + kM * (4 * S + kM * 4);
+__device__ __forceinline__ int ghost_side(int i) { return i < 2 ? i : kS - 4 + i; }  // 0, 1, 18, 19
+__device__ __forceinline__ void ghost_cell(int g, int &x, int &y, int &z) {
+  if (g < 4 * S2) {
+    z = ghost_side(g / S2);
+    x = g % S;
+    y = (g / S) % S;
+    return;
+  }
+  g -= 4 * S2;
+  z = kG + g / (4 * S + 4 * kM);
+  const int r = g % (4 * S + 4 * kM);
+  if (r < 4 * S) {
+    y = ghost_side(r / S);
+    x = r % S;
+  } else {
+    y = kG + (r - 4 * S) / 4;
+    x = ghost_side((r - 4 * S) % 4);
+  }
+}
+
 __device__ __forceinline__ void d3_fill(double *__restrict__ u, Level3View L, const Signs27 &sg, int phase) {
-  const int64_t total = (int64_t)L.nblk * S3;
+  const int64_t total = (int64_t)L.nblk * kGhost3;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    const int bi = (int)(t / S3), c = (int)(t % S3);
-    const int x = c % S, y = (c / S) % S, z = c / S2;
+    const int bi = (int)(t / kGhost3);
+    int x, y, z;
+    ghost_cell((int)(t % kGhost3), x, y, z);
+    const int c = o3(x, y, z);
     const int f1 = x < kG ? -1 : x >= kG + kM ? 1 : 0;
     const int f2 = y < kG ? -1 : y >= kG + kM ? 1 : 0;
     const int f3 = z < kG ? -1 : z >= kG + kM ? 1 : 0;
-    if (!f1 && !f2 && !f3) continue;
     const int4 fi = L.faces[27 * bi + (f1 + 1) + 3 * (f2 + 1) + 9 * (f3 + 1)];
     const int type = fi.x;
-    if ((type == FACE_NEIGHBOR && phase != 1) || (type == FACE_BOUNDARY && phase != 2) ||
-        (type == FACE_REFBND && phase != 4) || type == FACE_NONE)
+    if ((type == FACE_NEIGHBOR && !(phase & 1)) || (type == FACE_BOUNDARY && !(phase & 2)) ||
+        (type == FACE_REFBND && !(phase & 4)) || type == FACE_NONE)
       continue;
     double *ub = u + (int64_t)L.blocks[bi].x * S3;
     if (type == FACE_NEIGHBOR) {
@@ -396,10 +425,16 @@ Level3View view(srmg_ctx *ctx, int l) { return ctx->lv3[l - 1].view(); }
 int fill(srmg_ctx *ctx, double *u, int l, const Signs27 &sg, int mask) {
   const int n = ctx->nblk_host[l - 1];
   if (!n) return SRMG_OK;
+  if (!ctx->has_corners) {
+    if (seq3_push(ctx, S3_FILL, mask, 0, u, nullptr, nullptr, view(ctx, l), nullptr, &sg)) return SRMG_OK;
+    k3_fill<<<grid3((int64_t)n * kGhost3, 256), 256, 0, ctx->stream>>>(u, view(ctx, l), sg, mask);
+    ctx->launches++;
+    return SRMG_OK;
+  }
   for (int phase = 1; phase <= 4; phase <<= 1) {
     if (!(mask & phase)) continue;
     if (seq3_push(ctx, S3_FILL, phase, 0, u, nullptr, nullptr, view(ctx, l), nullptr, &sg)) continue;
-    k3_fill<<<grid3((int64_t)n * S3, 256), 256, 0, ctx->stream>>>(u, view(ctx, l), sg, phase);
+    k3_fill<<<grid3((int64_t)n * kGhost3, 256), 256, 0, ctx->stream>>>(u, view(ctx, l), sg, phase);
     ctx->launches++;
   }
   return SRMG_OK;
