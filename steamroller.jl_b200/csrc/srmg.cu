@@ -723,10 +723,17 @@ int srmg::L_fill_ghost(srmg_ctx *ctx, T *u, int l, const Signs &sg, int mask) {
     ctx->launches++;
     return SRMG_OK;
   }
-  // BoxStencil tree: a boundary corner whose bnd is zero along one dimension mirrors
-  // the adjacent face's ghost cells, so copy, boundary and interpolation run as three
-  // ordered passes (fill_ghost!, src/connectivity.jl:155-159), each launch filling the
-  // faces and corners of its pass
+  // BoxStencil tree: copy, boundary and interpolation are ordered passes (fill_ghost!,
+  // src/connectivity.jl:155-159), each launch filling the faces and corners of its
+  // passes.  Copy and boundary share one launch (a boundary corner evaluates the face
+  // ghost it mirrors itself, fill_corner_cell); interpolation follows on its own.
+  if ((mask & 3) == 3) {
+    if (!seq_push<T>(ctx, SEQ_FILL, 3, 0, u, nullptr, nullptr, L.view(l), nullptr, &sg)) {
+      k_fill_ghost<T><<<gf, threads, 0, ctx->stream>>>(u, L.view(l), sg, 3);
+      ctx->launches++;
+    }
+    mask &= ~3;
+  }
   for (int phase = 1; phase <= 4; phase <<= 1) {
     if (!(mask & phase)) continue;
     if (seq_push<T>(ctx, SEQ_FILL, phase, 0, u, nullptr, nullptr, L.view(l), nullptr, &sg)) continue;

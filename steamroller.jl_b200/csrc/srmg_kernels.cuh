@@ -179,8 +179,9 @@ __device__ __forceinline__ void fill_corner_cell(T *__restrict__ u, const LevelV
                                                  int64_t t);
 
 // One warp per (block, face): lane -> (layer g = lane/16, position k = lane%16).  On a
-// BoxStencil tree (lv.cfaces set) the launch covers one pass (mask 1, 2 or 4) and also
-// fills the corner cells of that pass: within one pass no cell reads another's result.
+// BoxStencil tree (lv.cfaces set) the launch covers one pass (mask 1, 2 or 4) or the
+// copy and boundary passes together (mask 3), and also fills the corner cells of those
+// passes (fill_corner_cell).
 template <typename T>
 __device__ __forceinline__ void d_fill_ghost(T *__restrict__ u, LevelView lv, Signs sg, int mask) {
   const int lane = threadIdx.x & 31;
@@ -245,7 +246,7 @@ __device__ __forceinline__ void d_fill_ghost(T *__restrict__ u, LevelView lv, Si
       ub[x + kS * y] = v;
     }
   }
-  if (lv.cfaces && (mask == 1 || mask == 2 || mask == 4)) {
+  if (lv.cfaces && (mask == 1 || mask == 2 || mask == 3 || mask == 4)) {
     const int64_t ct = (int64_t)lv.nblk * 16;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ct; t += (int64_t)gridDim.x * blockDim.x)
       fill_corner_cell<T>(u, lv, sg, mask, t);
@@ -490,22 +491,47 @@ __global__ void k_rhs(T *__restrict__ q1, const T *__restrict__ q, LevelView lv,
 }
 
 // Corner ghosts of a BoxStencil tree (src/connectivity.jl:155-258 with diagonal faces):
-// 2 x 2 cells per corner, one thread (index t) per cell.  phase 1 = copy from the
-// diagonal neighbour, 2 = boundary mirror (bnd may be zero along one dimension: then the
-// mirror reads the adjacent face's ghost cells, written by an earlier pass), 4 = linear
-// interpolation from the parent's subblockbnd cell (src/blockfield.jl:416-434,
-// src/interp.jl:24-63).  The three passes run as separate launches of k_fill_ghost in
-// that order, as fill_ghost! runs them.
+// 2 x 2 cells per corner, one thread (index t) per cell.  `mask` selects the passes:
+// 1 = copy from the diagonal neighbour, 2 = boundary mirror, 4 = linear interpolation
+// from the parent's subblockbnd cell (src/blockfield.jl:416-434, src/interp.jl:24-63).
+// A boundary corner whose bnd is zero along one dimension mirrors the adjacent face's
+// ghost cells, which fill_ghost! writes in an earlier pass.  fill_ghost! runs copy,
+// boundary and interpolation in that order; here copy and boundary may share one launch
+// (mask 3): such a corner then evaluates the face ghost it mirrors from that face's own
+// source -- the neighbour's valid cell, or the mirrored valid cell -- with the same
+// operations as the face pass, instead of reading it.  Interpolation (mask 4) stays a
+// launch of its own after them: the boundary pass reads a refinement face's ghosts as
+// they were before this fill.
 template <typename T>
-__device__ __forceinline__ void fill_corner_cell(T *__restrict__ u, const LevelView &lv, const Signs &sg, int phase,
+__device__ __forceinline__ T face_ghost_value(const T *__restrict__ u, const T *ub, const LevelView &lv,
+                                              const Signs &sg, int bi, int f, int x, int y) {
+  const int4 ff = lv.faces[4 * bi + f];
+  if (ff.x == FACE_NEIGHBOR) {  // as the copy pass of d_fill_ghost
+    const T *src = u + (int64_t)ff.y * kSS;
+    int sx = x, sy = y;
+    if (f == 0) sx = x + kM; else if (f == 1) sx = x - kM;
+    else if (f == 2) sy = y + kM; else sy = y - kM;
+    return src[sx + kS * sy];
+  }
+  if (ff.x == FACE_BOUNDARY) {  // as the boundary pass of d_fill_ghost
+    int mx = x, my = y;
+    if (f == 0) mx = 2 * kG - 1 - x; else if (f == 1) mx = 2 * (kG + kM) - 1 - x;
+    else if (f == 2) my = 2 * kG - 1 - y; else my = 2 * (kG + kM) - 1 - y;
+    return dmul<T>(T(sg.v[face_sign_index(f)]), ub[mx + kS * my]);
+  }
+  return ub[x + kS * y];  // a refinement face: not written by the copy and boundary passes
+}
+
+template <typename T>
+__device__ __forceinline__ void fill_corner_cell(T *__restrict__ u, const LevelView &lv, const Signs &sg, int mask,
                                                  int64_t t) {
   {
     const int bi = (int)(t >> 4), q = (int)((t >> 2) & 3), cell = (int)(t & 3);
     const int4 fi = lv.cfaces[4 * bi + q];
     const int type = fi.x;
     if (type == FACE_NONE) return;
-    if ((type == FACE_NEIGHBOR && phase != 1) || (type == FACE_BOUNDARY && phase != 2) ||
-        (type == FACE_REFBND && phase != 4))
+    if ((type == FACE_NEIGHBOR && !(mask & 1)) || (type == FACE_BOUNDARY && !(mask & 2)) ||
+        (type == FACE_REFBND && !(mask & 4)))
       return;
     const int fr = 2 * (q & 1) - 1, fz = 2 * (q >> 1) - 1;  // ghost direction
     const int ir = cell & 1, iz = cell >> 1;
@@ -519,7 +545,16 @@ __device__ __forceinline__ void fill_corner_cell(T *__restrict__ u, const LevelV
       const int mx = b0 < 0 ? 2 * kG - 1 - x : b0 > 0 ? 2 * (kG + kM) - 1 - x : x;
       const int my = b1 < 0 ? 2 * kG - 1 - y : b1 > 0 ? 2 * (kG + kM) - 1 - y : y;
       const T a = T(sg.v[(1 + b0) + 3 * (1 + b1)]);
-      ub[x + kS * y] = dmul<T>(a, ub[mx + kS * my]);
+      T src;
+      if ((mask & 1) && (b0 == 0) != (b1 == 0)) {
+        // the mirror lands in the ghost cells of the face along the zero component,
+        // which the copy part of this launch writes: evaluate that cell directly
+        const int f = b0 == 0 ? (fr < 0 ? 0 : 1) : (fz < 0 ? 2 : 3);
+        src = face_ghost_value<T>(u, ub, lv, sg, bi, f, mx, my);
+      } else {
+        src = ub[mx + kS * my];
+      }
+      ub[x + kS * y] = dmul<T>(a, src);
     } else {
       const T *cb = u + (int64_t)fi.y * kSS;
       const int sbr = fi.z, sbz = fi.w;
