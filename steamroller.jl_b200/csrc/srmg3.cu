@@ -52,10 +52,13 @@ __device__ __forceinline__ int unpack(int packed, int d) { return ((packed >> (2
 // ---- ghost fills (src/connectivity.jl:155-258), one thread per ghost cell -----------
 // `phase` is a mask: 1 copies from neighbours, 2 mirrors at the domain boundary, 4
 // interpolates from the parent.  fill_ghost! runs them in that order; on BoxStencil{3}
-// trees an edge or corner ghost can mirror a face ghost that the copy pass writes, so
-// the passes are three launches there.  On StarStencil{3} trees only face ghosts are
-// filled, each reads valid cells of its own level or cells of the parent level, and no
-// ghost reads another: one launch does all three passes with the same results.
+// trees an edge or corner boundary ghost can mirror a face or edge ghost that the copy
+// pass writes (its bnd is zero along the directions where it is not on the domain
+// boundary), so there copy and boundary share one launch -- such a ghost takes the
+// neighbour's valid cell the copy would write -- and interpolation, which rewrites
+// ghosts the boundary pass reads as they were, follows in a second.  On StarStencil{3}
+// trees only face ghosts are filled, each reads valid cells of its own level or cells
+// of the parent level, and no ghost reads another: one launch does all three passes.
 // The ghost cells of a 20^3 block, enumerated: the four z-planes z = 0, 1, 18, 19 whole
 // (4 x 400 cells), then for each of the 16 valid z the rows y = 0, 1, 18, 19 whole
 // (4 x 20) and, on the 16 valid rows, the columns x = 0, 1, 18, 19 -- 3904 cells.
@@ -102,7 +105,20 @@ __device__ __forceinline__ void d3_fill(double *__restrict__ u, Level3View L, co
     } else if (type == FACE_BOUNDARY) {
       const int b1 = unpack(fi.z, 0), b2 = unpack(fi.z, 1), b3 = unpack(fi.z, 2);
       auto mir = [](int i, int b) { return b < 0 ? 2 * kG - 1 - i : b > 0 ? 2 * (kG + kM) - 1 - i : i; };
-      ub[c] = __dmul_rn(sg.v[(1 + b1) + 3 * (1 + b2) + 9 * (1 + b3)], ub[o3(mir(x, b1), mir(y, b2), mir(z, b3))]);
+      const int mx = mir(x, b1), my = mir(y, b2), mz = mir(z, b3);
+      // the mirrored cell is still a ghost along the directions where bnd is zero; when
+      // this launch also runs the copy pass and that ghost is a neighbour copy, take the
+      // neighbour's valid cell itself (the copy pass's own operation) instead of the
+      // ghost the copy writes
+      const int g1 = b1 ? 0 : f1, g2 = b2 ? 0 : f2, g3 = b3 ? 0 : f3;
+      double src;
+      const int4 gi = (phase & 1) && (g1 || g2 || g3) ? L.faces[27 * bi + (g1 + 1) + 3 * (g2 + 1) + 9 * (g3 + 1)]
+                                                       : make_int4(FACE_NONE, 0, 0, 0);
+      if (gi.x == FACE_NEIGHBOR)
+        src = u[(int64_t)gi.y * S3 + o3(mx - kM * g1, my - kM * g2, mz - kM * g3)];
+      else
+        src = ub[o3(mx, my, mz)];
+      ub[c] = __dmul_rn(sg.v[(1 + b1) + 3 * (1 + b2) + 9 * (1 + b3)], src);
     } else {
       // interp! from the parent's subblockbnd cell: along a face dimension the parent's
       // last (ghost below) or first (ghost above) subblock cell, else the subblock cell
@@ -431,6 +447,13 @@ int fill(srmg_ctx *ctx, double *u, int l, const Signs27 &sg, int mask) {
     ctx->launches++;
     return SRMG_OK;
   }
+  if ((mask & 3) == 3 && ctx->merge_fill) {
+    if (!seq3_push(ctx, S3_FILL, 3, 0, u, nullptr, nullptr, view(ctx, l), nullptr, &sg)) {
+      k3_fill<<<grid3((int64_t)n * kGhost3, 256), 256, 0, ctx->stream>>>(u, view(ctx, l), sg, 3);
+      ctx->launches++;
+    }
+    mask &= ~3;
+  }
   for (int phase = 1; phase <= 4; phase <<= 1) {
     if (!(mask & phase)) continue;
     if (seq3_push(ctx, S3_FILL, phase, 0, u, nullptr, nullptr, view(ctx, l), nullptr, &sg)) continue;
@@ -622,6 +645,7 @@ extern "C" int srmg_set_tree3(srmg_ctx *ctx, int nlev, const int64_t *npairs, co
   std::vector<std::vector<int4>> hb(nlev), hf(nlev), hc(nlev);
   std::vector<std::vector<int>> hm(nlev);
   bool corners = false;
+  bool merge_fill = true;
   for (int l = 0; l < nlev; ++l) {
     const int lv = l + 1;
     hb[l].resize(npairs[l]);
@@ -667,6 +691,18 @@ extern "C" int srmg_set_tree3(srmg_ctx *ctx, int nlev, const int64_t *npairs, co
       for (int d = 0; d < 3 && ok; ++d) ok = e.subblock[d] == 1 || e.subblock[d] == 2;
       if (!ok) return fail(ctx, SRMG_ERR_BADTREE, "level %d: malformed refinement boundary", lv);
       RC(set(e.fine, code, make_int4(FACE_REFBND, (int)(e.coarse - 1), pack3(e.subblock, 0), 0)));
+    }
+    // a boundary ghost mirrors, along the directions where its bnd is zero, a ghost that
+    // must not itself be a boundary ghost for copy and boundary to share a launch
+    for (size_t k = 0; k < hf[l].size(); ++k) {
+      const int4 v = hf[l][k];
+      if (v.x != FACE_BOUNDARY) continue;
+      const int code = (int)(k % 27);
+      const int f[3] = {code % 3 - 1, (code / 3) % 3 - 1, code / 9 - 1};
+      int g[3];
+      for (int d = 0; d < 3; ++d) g[d] = ((v.z >> (2 * d)) & 3) - 1 ? 0 : f[d];
+      if (!g[0] && !g[1] && !g[2]) continue;
+      if (hf[l][k - code + (g[0] + 1) + 3 * (g[1] + 1) + 9 * (g[2] + 1)].x == FACE_BOUNDARY) merge_fill = false;
     }
     if (nch[l] < 0 || (nch[l] > 0 && !ch[l])) return fail(ctx, SRMG_ERR_BADTREE, "level %d: children", lv);
     hc[l].resize(nch[l]);
@@ -730,6 +766,7 @@ extern "C" int srmg_set_tree3(srmg_ctx *ctx, int nlev, const int64_t *npairs, co
   ctx->max_blk = max_blk;
   ctx->generation = generation;
   ctx->has_corners = corners;
+  ctx->merge_fill = merge_fill;
   ctx->nitems = 1;
   ctx->has_tree = true;
   return SRMG_OK;

@@ -112,6 +112,7 @@ struct srmg_ctx {
   bool use_engine = true;
   unsigned refbnd_levels = 0;  // bit l: level l has refinement-boundary faces
   bool has_corners = false;    // the tree came with a BoxStencil connectivity (diagonal edges)
+  bool merge_fill = true;      // 3D: copy and boundary fill passes may share a launch
   bool trace_on = false;
   srmg::DevBuf trace;        // %globaltimer stamps after every engine phase (CTA 0)
 

@@ -100,7 +100,7 @@ def rand(p, seed):
     return np.random.default_rng(seed).standard_normal(p.b.shape)
 
 
-@pytest.mark.parametrize("mask", [1, 2, 4, 7])
+@pytest.mark.parametrize("mask", [1, 2, 3, 4, 5, 6, 7])
 def test_fill_ghost_bitexact(pair, mask):
     p = pair.p
     u0 = rand(p, 1)
