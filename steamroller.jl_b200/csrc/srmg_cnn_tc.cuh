@@ -191,7 +191,7 @@ k_cnn_fwd_tc(const __nv_bfloat16 *__restrict__ x, int n, const unsigned char *__
         }
         tc_commit(&S.mbar);
       }
-      // every thread waits for the layer's MMAs (bounded); the verdict is made uniform
+      // every thread waits for the layer's MMAs (bounded); the outcome is made uniform
       const bool done = tc_mbar_wait(&S.mbar, phase, 1000000000LL);
       ok = __syncthreads_and(done) != 0;
       if (!ok && tid == 0) atomicCAS(err, 0, 1);
