@@ -544,6 +544,14 @@ int srmg_ssprk3_stage_dev(srmg_ctx *ctx, double *out, const double *n, const dou
  *                      one cooperative launch that walks the recorded operations with
  *                      a grid barrier between consecutive ones (bit-identical results);
  *                      0 (default: graph replay measured faster on 2D and 3D trees);
+ *   "direct_level"     the level of the FP64 direct coarsest solve of mixed and
+ *                      SRMG_MODE_FP64_DIRECT solves on the persistent kernel: 0 (default)
+ *                      = level 2 for a lone tree whose level 2 holds 1..4 blocks and has no
+ *                      refinement boundary (its 256..1024-row inverse is built on the host
+ *                      once per operator, ~0.5 s at 1024 rows, and applied by every CTA),
+ *                      else level 1 (one CTA); 1 = level 1 always (batches always use
+ *                      level 1, so a solo solve matches its batched twin bit for bit only
+ *                      with 1); 2 = level 2 where possible;
  *   "freebc_direct"    1 = srmg_freebc transforms by direct sums even for power-of-two
  *                      lengths (default 0: FFTs);
  *   "b_copy_back"      1 = srmg_vcycle / srmg_fmg copy b back to the host (the FAS

@@ -566,6 +566,8 @@ int srmg::build_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs, const srmg_
   ctx->nitems = nitems;
   ctx->l1_blocks = hb[0];
   ctx->l1_faces = hf[0];
+  ctx->l2_blocks = nlev >= 2 ? hb[1] : std::vector<int4>();
+  ctx->l2_faces = nlev >= 2 ? hf[1] : std::vector<int4>();
   ctx->wtab_n = wn;
   ctx->max_blk = max_blk;
   ctx->generation = generation;
@@ -996,7 +998,10 @@ extern "C" int srmg_set_option(srmg_ctx *ctx, const char *key, int64_t value) {
   else if (!strcmp(key, "b_copy_back")) ctx->b_copy_back = value != 0;
   else if (!strcmp(key, "freebc_direct")) ctx->fbc_direct = value != 0;
   else if (!strcmp(key, "graph")) ctx->use_graph = value != 0;
-  else if (!strcmp(key, "op_sequencer")) {
+  else if (!strcmp(key, "direct_level")) {
+    if (value < 0 || value > 2) return fail(ctx, SRMG_ERR_BADARG, "direct_level must be 0, 1 or 2");
+    ctx->direct_level = (int)value;
+  } else if (!strcmp(key, "op_sequencer")) {
     ctx->use_op_seq = value != 0;
     if (!ctx->use_op_seq) drop_op_graphs(ctx);
   }

@@ -141,6 +141,8 @@ struct srmg_ctx {
   int cnn_active_ppm = 0;               // > 0: network only on blocks with g energy >= ppm 1e-6 x max
   int cnn_last_active = 0;              // active blocks of the last prediction (when read back)
   std::vector<int4> l1_blocks, l1_faces;  // level 1 as uploaded (direct coarsest solve)
+  std::vector<int4> l2_blocks, l2_faces;  // level 2 as uploaded (a lone tree's direct solve there)
+  int direct_level = 0;                   // option "direct_level": 0 = 2 where possible, 1 or 2
   std::vector<srmg::ItemSpec> batch_items;       // operators given to srmg_batch_set
 
   // per-item operator tables of the persistent engine

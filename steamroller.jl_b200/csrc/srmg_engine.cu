@@ -153,7 +153,16 @@ int srmg::engine_vcycle(srmg_ctx *ctx, T *u, T *b, T *u1, T *e, const ItemTabs &
   A.ntop = ntop;
   A.nup = nup;
   A.local_top = engine_local_top(ctx, L);
-  if (run->direct && tabs.P) A.it_P = tabs.P;
+  A.top = 1;
+  if (run->direct && tabs.P) {
+    A.it_P = tabs.P;
+    if (tabs.top == 2 && L >= 2) {
+      // level 2 is solved directly by every CTA: no level below it is visited, and none
+      // runs CTA-locally
+      A.top = 2;
+      A.local_top = 0;
+    }
+  }
   A.max_cycles = run->max_cycles;
   A.tol = run->tol;
   if (run->max_cycles > 0) {

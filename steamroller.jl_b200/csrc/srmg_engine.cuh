@@ -83,13 +83,14 @@ struct EngArgs {
   int lmax;          // finest non-empty level taking part
   int ndown, ntop, nup;
   int local_top;     // levels 1..local_top run inside CTA 0
+  int top;           // the coarsest level a V-cycle visits: 1, or 2 (a lone item's direct solve there)
   int smooth_level;  // > 0: run smooth_n GS iterations on this level only (gauss_seidel_iter!)
   int smooth_n;
   int nitems;
   int nlev_tab;                // row length of it_lrange
   const T *it_par;             // per item: kParStride operator values (s_l, centre_l, nwc_l)
   const int *it_sgbits;        // per item: the 3x3 boundary table, entry k as (bc_k + 1) << 2k
-  const double *const *it_P;   // per item: P = -s A_1^{-1} of its level 1 (row-major), or null
+  const double *const *it_P;   // per item: P = -s_t A_t^{-1} of its level t = top (row-major), or null
   const int2 *it_lrange;       // [item * nlev_tab + l - 1]: {first, count} in level l's block list
   int *frozen;                 // per item: nonzero once it has stopped iterating (zero at launch)
   unsigned *bar;     // barrier counter, zero at launch
@@ -1421,6 +1422,73 @@ __device__ void ph_direct_top(const EngArgs<T> &A, T *u, bool make_e, int first,
   }
 }
 
+// The direct solve on level 2 of a lone item (<= 4 blocks, n <= 1024 unknowns), spread
+// over every CTA in two phases with a grid barrier between them.  First half: every CTA
+// forms the level's whole FAS right-hand side in shared memory -- b = -(e + L(u)/s) on
+// covered cells (e holds the restricted residual), b itself on leaf cells, as
+// ph_direct_top does on level 1 -- and keeps the old u of the rows it will solve.  No
+// CTA writes u or e before the barrier, so every one reads the same old values.
+template <typename T>
+__device__ void ph_direct2_rhs(const EngArgs<T> &A, const T *u, int lt, double *rhs, double *uold) {
+  const int2 rg = A.it_lrange[lt - 1];  // item 0
+  const int n = 256 * rg.y;
+  const int4 *blocks = A.tr.lvl_blocks[lt - 1] + rg.x;
+  const T s = A.it_par[lt], centre = A.it_par[32 + lt];
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const int c = j & 255, x = 2 + (c & 15), y = 2 + (c >> 4);
+    const int4 bk = blocks[j >> 8];
+    const int64_t o = (int64_t)bk.x * kSS + x + kS * y;
+    const int mysub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
+    T bv;
+    if ((bk.w >> mysub) & 1) {
+      const W5<T> w = weights<T>(A.wt, A.geom, bk.y, bk.z, x, y);
+      const T Lu = apply5<T>(u + (int64_t)bk.x * kSS, x, y, w, centre);
+      bv = -(A.e[o] + Lu / s);
+    } else {
+      bv = A.b[o];
+    }
+    rhs[j] = (double)bv;
+  }
+  const int rpc = (n + gridDim.x - 1) / gridDim.x, r0 = blockIdx.x * rpc;
+  for (int q = threadIdx.x; q < rpc && r0 + q < n; q += blockDim.x) {
+    const int j = r0 + q, c = j & 255;
+    uold[q] = (double)u[(int64_t)blocks[j >> 8].x * kSS + (2 + (c & 15)) + kS * (2 + (c >> 4))];
+  }
+}
+
+// Second half: CTA c solves rows [c rpc, (c + 1) rpc) of u = P rhs in FP64, one warp per
+// row (lane-strided partial sums, then the warp, in a fixed order), and writes the row's
+// new u, the correction e = u - u_old and their ghost pushes in place.
+template <typename T>
+__device__ void ph_direct2_rows(const EngArgs<T> &A, T *u, int lt, bool make_e, const double *rhs,
+                                const double *uold) {
+  const int2 rg = A.it_lrange[lt - 1];
+  const int n = 256 * rg.y;
+  const int4 *blocks = A.tr.lvl_blocks[lt - 1] + rg.x;
+  const double *P = A.it_P[0];
+  const int rpc = (n + gridDim.x - 1) / gridDim.x, r0 = blockIdx.x * rpc, r1 = min(n, r0 + rpc);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int q = r0 + warp; q < r1; q += nw) {
+    const double *pr = P + (int64_t)q * n;
+    double acc = 0.0;
+    for (int j = lane; j < n; j += 32) acc = fma(pr[j], rhs[j], acc);
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (lane == 0) {
+      const int c = q & 255, x = 2 + (c & 15), y = 2 + (c >> 4);
+      const int X = blocks[q >> 8].x;
+      const int4 *fc = A.tr.faces + 4 * X;
+      const T nu = (T)acc;
+      u[(int64_t)X * kSS + x + kS * y] = nu;
+      push<T>(A, 0, u, X, fc, x, y, nu);
+      if (make_e) {
+        const T ev = nu - (T)uold[q - r0];
+        A.e[(int64_t)X * kSS + x + kS * y] = ev;
+        push<T>(A, 0, A.e, X, fc, x, y, ev);
+      }
+    }
+  }
+}
+
 // Copy level l's blocks (valid cells and face ghosts) from src to dst.
 template <typename T>
 __device__ void ph_copy_back(const EngArgs<T> &A, int l, const T *src, T *dst, int first, int step, int t) {
@@ -1617,8 +1685,9 @@ __global__ void __launch_bounds__(NT, 1) k_engine_vcycle(const __grid_constant__
   // One FAS V-cycle (src/multigrid.jl:60-106) on the current fields.
   auto vcycle_body = [&]() -> bool {
     cur = 0;
-    // descending leg
-    for (int l = L; l >= 2; --l) {
+    // descending leg, down to the level above the coarsest one visited
+    const int lt = A.top;
+    for (int l = L; l >= lt + 1; --l) {
       const bool loc = l <= K;
       for (int it = 0; it < A.ndown; ++it) {
         bool ok = true;
@@ -1633,7 +1702,13 @@ __global__ void __launch_bounds__(NT, 1) k_engine_vcycle(const __grid_constant__
       if (!sync(okr, loc, (l - 1) <= K)) return false;
     }
     // coarsest level
-    if (A.it_P) {
+    if (A.it_P && lt == 2) {
+      // a lone item's direct solve on level 2, grid-wide (never CTA-local: local_top = 0)
+      ph_direct2_rhs<T>(A, fld(2), 2, s_rhs, s_direct);
+      if (!sync(true, false, false)) return false;
+      ph_direct2_rows<T>(A, fld(2), 2, L > 2, s_rhs, s_direct);
+      if (!sync(true, false, false)) return false;
+    } else if (A.it_P) {
       const bool loc = 1 <= K;
       if (runs(loc))
         ph_direct_top<T>(A, fld(1), L > 1, loc ? 0 : blockIdx.x, loc ? 1 : gridDim.x, t, slot, s_direct, s_rhs);
@@ -1651,7 +1726,7 @@ __global__ void __launch_bounds__(NT, 1) k_engine_vcycle(const __grid_constant__
       }
     }
     // ascending leg
-    for (int l = 2; l <= L; ++l) {
+    for (int l = lt + 1; l <= L; ++l) {
       const bool loc = l <= K;
       bool okp = true;
       if (runs(loc)) okp = ph_prolong<T>(A, l, fld(l), fld(l - 1), first_of(loc), step_of(loc), t, slot, S, pk);

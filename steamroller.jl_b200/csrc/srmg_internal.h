@@ -88,13 +88,20 @@ struct ItemTabs {
   const double *const *P = nullptr;  // per item direct coarsest-level inverse, or null
   const double *P0 = nullptr;        // item 0's inverse (per-operation kernels)
   int n0 = 0;                        // its unknowns
+  int top = 1;                       // the level the inverses belong to (1, or 2 for a lone tree)
 };
 // Upload the per-item tables for operators `specs` (ctx->nitems entries).  With
 // smooth_level > 0 the level's entries use the scale smooth_sl instead of s_l.  With
-// want_P the coarsest-level inverse of every item is prepared (cached); tabs->P stays
-// null when some item's level 1 has more than 4 blocks or its operator is singular.
+// want_P the direct-solve inverse of every item on level `top` is prepared (cached);
+// with top = 2 and no usable level-2 inverse it falls back to level 1; tabs->P stays
+// null when some item's level has more than 4 blocks, a face without a ghost source on
+// that level, or a singular operator.
 int prepare_items(srmg_ctx *ctx, const ItemSpec *specs, int geom, double omega, bool want_P,
-                  int smooth_level, double smooth_sl, ItemTabs *tabs);
+                  int smooth_level, double smooth_sl, ItemTabs *tabs, int top = 1);
+// The level of the persistent engine's direct solve for this context: 2 for a lone
+// two-dimensional tree whose level 2 holds 1..4 blocks (option "direct_level" not 1),
+// else 1.
+int direct_top(srmg_ctx *ctx);
 // The same operator for every item.
 std::vector<ItemSpec> uniform_items(srmg_ctx *ctx, double s, int op, double k2, const int8_t *bc);
 

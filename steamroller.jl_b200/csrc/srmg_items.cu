@@ -64,29 +64,34 @@ bool invert(std::vector<double> &a, int n) {
   return true;
 }
 
-// P = -s A_1^{-1} for one item: the level-1 operator over the item's level-1 blocks,
-// ghosts resolved through neighbour copies and boundary mirrors, assembled on the host,
-// inverted and uploaded (cached by operator and structure).  *P stays null when the
-// item's level 1 has more than 4 blocks or A_1 is singular.
-int item_inverse(srmg_ctx *ctx, int item, const ItemSpec &sp, int geom, const double **P) {
+// P = -s_t A_t^{-1} for one item on level t = lt (1 or 2): the level's operator over
+// the item's blocks of that level, ghosts resolved through neighbour copies and boundary
+// mirrors, assembled on the host, inverted and uploaded (cached by level, operator and
+// structure).  *P stays null when the item's level has more than 4 blocks, a face with
+// no ghost source on the level (a refinement boundary) or a singular operator.
+int item_inverse(srmg_ctx *ctx, int item, const ItemSpec &sp, int geom, int lt, const double **P) {
   *P = nullptr;
-  const int2 rg = ctx->it_lrange_host[(size_t)item * ctx->nlev];
+  if (lt < 1 || lt > 2 || lt > ctx->nlev) return SRMG_OK;
+  const std::vector<int4> &hb = lt == 1 ? ctx->l1_blocks : ctx->l2_blocks;
+  const std::vector<int4> &hf = lt == 1 ? ctx->l1_faces : ctx->l2_faces;
+  const int2 rg = ctx->it_lrange_host[(size_t)item * ctx->nlev + lt - 1];
   const int nb = rg.y;
   const int n = nb * 256;
   if (nb < 1 || nb > 4) return SRMG_OK;
   auto local = [&](int blk) {
     for (int i = 0; i < nb; i++)
-      if (ctx->l1_blocks[rg.x + i].x == blk) return i;
+      if (hb[rg.x + i].x == blk) return i;
     return -1;
   };
-  std::vector<double> key = {sp.s, (double)sp.op, sp.k2, (double)geom, (double)nb};
+  const double s = level_scale(sp.s, lt);  // s_l = s / 4^(l-1)
+  std::vector<double> key = {(double)lt, s, (double)sp.op, sp.k2, (double)geom, (double)nb};
   for (int i = 0; i < 9; i++) key.push_back(sp.bc[i]);
   for (int i = 0; i < nb; i++) {
-    const int4 bk = ctx->l1_blocks[rg.x + i];
+    const int4 bk = hb[rg.x + i];
     key.push_back(bk.y);
     key.push_back(bk.z);
     for (int f = 0; f < 4; f++) {
-      const int4 fi = ctx->l1_faces[4 * (rg.x + i) + f];
+      const int4 fi = hf[4 * (rg.x + i) + f];
       key.push_back(fi.x);
       key.push_back(fi.x == FACE_NEIGHBOR ? local(fi.y) : -1);
     }
@@ -97,11 +102,10 @@ int item_inverse(srmg_ctx *ctx, int item, const ItemSpec &sp, int geom, const do
     return SRMG_OK;
   }
   std::vector<double> A((size_t)n * n, 0.0);
-  const double s = sp.s;
   const double centre = (sp.op == SRMG_OP_HELMHOLTZ) ? (-4.0 - s * sp.k2) : -4.0;
   static const int sidx[4] = {3, 5, 1, 7};
   for (int bi = 0; bi < nb; bi++) {
-    const int4 bk = ctx->l1_blocks[rg.x + bi];
+    const int4 bk = hb[rg.x + bi];
     for (int y = 2; y < 18; y++)
       for (int x = 2; x < 18; x++) {
         const int row = bi * 256 + (y - 2) * 16 + (x - 2);
@@ -125,7 +129,7 @@ int item_inverse(srmg_ctx *ctx, int item, const ItemSpec &sp, int geom, const do
           int cb = bi;
           if (cx < 2 || cx > 17 || cy < 2 || cy > 17) {
             const int f = q;  // the face crossed: 0 -r, 1 +r, 2 -z, 3 +z
-            const int4 fi = ctx->l1_faces[4 * (rg.x + bi) + f];
+            const int4 fi = hf[4 * (rg.x + bi) + f];
             if (fi.x == FACE_NEIGHBOR) {
               cb = local(fi.y);
               if (cb < 0) return SRMG_OK;  // neighbour outside the item: no direct solve
@@ -135,7 +139,7 @@ int item_inverse(srmg_ctx *ctx, int item, const ItemSpec &sp, int geom, const do
               if (f == 0) cx = 3 - cx; else if (f == 1) cx = 35 - cx;
               else if (f == 2) cy = 3 - cy; else cy = 35 - cy;
             } else {
-              return SRMG_OK;  // no ghost source at level 1
+              return SRMG_OK;  // no ghost source on this level
             }
           }
           const int col = cb * 256 + (cy - 2) * 16 + (cx - 2);
@@ -173,8 +177,14 @@ std::vector<ItemSpec> srmg::uniform_items(srmg_ctx *ctx, double s, int op, doubl
   return std::vector<ItemSpec>((size_t)ctx->nitems, sp);
 }
 
+int srmg::direct_top(srmg_ctx *ctx) {
+  if (ctx->direct_level == 1 || ctx->nitems != 1 || ctx->D != 2 || ctx->nlev < 2) return 1;
+  const int nb2 = ctx->nblk_host[1];
+  return nb2 >= 1 && nb2 <= 4 ? 2 : 1;
+}
+
 int srmg::prepare_items(srmg_ctx *ctx, const ItemSpec *specs, int geom, double omega, bool want_P,
-                        int smooth_level, double smooth_sl, ItemTabs *tabs) {
+                        int smooth_level, double smooth_sl, ItemTabs *tabs, int top) {
   const int ni = ctx->nitems;
   const size_t o64 = 0;
   const size_t o32 = align8(o64 + sizeof(double) * kParStride * ni);
@@ -203,9 +213,19 @@ int srmg::prepare_items(srmg_ctx *ctx, const ItemSpec *specs, int geom, double o
     sg[k] = 0;
     for (int i = 0; i < 9; i++) sg[k] |= (sp.bc[i] + 1) << (2 * i);
     pp[k] = nullptr;
-    if (all_P) {
-      RC(item_inverse(ctx, k, sp, geom, &pp[k]));
+  }
+  if (all_P) {
+    for (int k = 0; k < ni && all_P; k++) {
+      RC(item_inverse(ctx, k, specs[k], geom, top, &pp[k]));
       if (!pp[k]) all_P = false;
+    }
+    if (!all_P && top == 2) {  // no usable level-2 inverse: the level-1 solve
+      top = 1;
+      all_P = true;
+      for (int k = 0; k < ni && all_P; k++) {
+        RC(item_inverse(ctx, k, specs[k], geom, top, &pp[k]));
+        if (!pp[k]) all_P = false;
+      }
     }
   }
   if (!all_P)
@@ -221,7 +241,8 @@ int srmg::prepare_items(srmg_ctx *ctx, const ItemSpec *specs, int geom, double o
   tabs->sgbits = (const int *)(d + osg);
   tabs->P = all_P ? (const double *const *)(d + oP) : nullptr;
   tabs->P0 = all_P ? pp[0] : nullptr;
-  tabs->n0 = all_P ? 256 * ctx->it_lrange_host[0].y : 0;
+  tabs->n0 = all_P ? 256 * ctx->it_lrange_host[top - 1].y : 0;
+  tabs->top = all_P ? top : 1;
   return SRMG_OK;
 }
 

@@ -279,7 +279,7 @@ static int solve_fp64(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_al
         return fail(ctx, SRMG_ERR_UNSUPPORTED, "the direct coarsest solve supports order-2 discretisations");
   if (engine_ok(ctx, o, {u, b, bw, r, u1})) {
     ItemTabs tabs;
-    RC(prepare_items(ctx, specs, geom, o->omega, direct, 0, 0.0, &tabs));
+    RC(prepare_items(ctx, specs, geom, o->omega, direct, 0, 0.0, &tabs, direct_top(ctx)));
     RC(solve_enqueue(ctx, u, b, nblk_alloc, tabs, geom, o));
     RC(read_items(ctx));
     items_stats(ctx, o, st);
@@ -328,8 +328,11 @@ static int solve_mixed(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_a
     if (specs[k].op == SRMG_OP_LAPLACIAN4)
       return fail(ctx, SRMG_ERR_UNSUPPORTED, "mixed precision supports order-2 discretisations; use FP64 mode");
   ItemTabs tabs;
-  RC(prepare_items(ctx, specs, geom, o->omega, true, 0, 0.0, &tabs));
-  if (engine_ok(ctx, o, {u, b})) {
+  // the persistent engine solves directly on level 2 where it can (direct_top), the
+  // per-operation path on level 1
+  const bool engine = engine_ok(ctx, o, {u, b});
+  RC(prepare_items(ctx, specs, geom, o->omega, true, 0, 0.0, &tabs, engine ? direct_top(ctx) : 1));
+  if (engine) {
     RC(solve_enqueue(ctx, u, b, nblk_alloc, tabs, geom, o));
     RC(read_items(ctx));
     items_stats(ctx, o, st);

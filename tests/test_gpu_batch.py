@@ -4,8 +4,10 @@ Poisson potential and photoionization Helmholtz terms) in one persistent launch.
 Every item of a batch must end exactly where a solo solve of the same problem ends:
 same V-cycle count and bit-identical potential (the engine's per-block arithmetic and
 per-item norms do not depend on the other items, and a converged item is frozen while
-the others iterate).  The solo solves themselves are held to the oracle by
-test_gpu_parity.py.
+the others iterate).  A batch solves the coarsest level directly on level 1; a lone
+tree's solve uses level 2 where it can (option "direct_level"), so the solo contexts
+compared here are set to level 1.  The solo solves themselves are held to the oracle
+by test_gpu_parity.py.
 """
 import numpy as np
 import pytest
@@ -42,13 +44,13 @@ def setup():
     items = []
     ctxs = []
     for pois, terms in trees:
-        c = mg.Context(0).set_tree(pois.tree, pois.conn)
+        c = mg.Context(0).set_tree(pois.tree, pois.conn).set_option("direct_level", 1)
         ctxs.append(c)
         for p in [pois] + terms[:2]:
             items.append((c, p))
     uni = gen.make_problem(gen._uniform(4), lambda r, z, l, gi, gj: np.sin(r * 900) * np.cos(z * 700) * 1e19,
                            gen.poisson_scale(), name="uniform4")
-    cu = mg.Context(0).set_tree(uni.tree, uni.conn)
+    cu = mg.Context(0).set_tree(uni.tree, uni.conn).set_option("direct_level", 1)
     ctxs.append(cu)
     items.append((cu, uni))
     batch = mg.Batch([(c, p.s, disc(p), p.bc) for c, p in items], gen.GEOM_CYL1)

@@ -453,12 +453,16 @@ def leaf_mask(p):
     return m
 
 
-def test_fp64_direct_mode_reaches_the_oracle_solution():
+@pytest.mark.parametrize("direct_level", [1, 2])
+def test_fp64_direct_mode_reaches_the_oracle_solution(direct_level):
     """SRMG_MODE_FP64_DIRECT: FP64 V-cycles with the direct FP64 coarsest solve converge
     to the oracle's FP64 solution in far fewer cycles than the reference's 4 top sweeps,
-    and to the same solution as the mixed mode."""
+    and to the same solution as the mixed mode; with the direct solve on level 1 (one
+    CTA) and on level 2 (every CTA; the default for a lone tree)."""
     p = PROBS["refined"]
+    assert len(p.tree[1]) <= 4  # level 2 can be solved directly
     pr = Pair(p)
+    pr.ctx.set_option("direct_level", direct_level)
     u, b = _prepared(pr)
     out = {}
     for mode in (mg.MODE_FP64, mg.MODE_FP64_DIRECT, mg.MODE_MIXED):
