@@ -392,16 +392,19 @@ int srmg_batch_solve_forest_dev(srmg_ctx *batch, double *u, const double *b,
  * omega -- engine_ctas (one CTA per SM or half as many: blocks per CTA) x
  * local_max_blocks (4, 16, 64: coarse levels kept inside one CTA), 6 candidates --
  * then, at the fastest shape, (ndown, nup) in {(2,2), (1,1), (1,2), (2,1), (3,3)} x the
- * Gauss-Seidel relaxation factor omega in {1, 1.1, 1.2}, 15 candidates.  The fastest
- * candidate's options are set on the context and its sweep counts and omega written to
- * *opts; u is restored to its initial content.  Trials are reported in `trials` (up to
- * max_trials).  Returns the number of trials run or an error code.  The tile shape is
- * fixed: one 20 x 20 block per 256-thread slot. */
+ * Gauss-Seidel relaxation factor omega in {1, 1.1, 1.2}, 15 candidates; and for mixed
+ * solves, at the fastest of those, the FP32 V-cycles per defect-correction step
+ * (inner_cycles) in {1, 2, 3, 4}, 4 candidates.  The fastest candidate's options are set
+ * on the context and its sweep counts, omega and inner_cycles written to *opts; u is
+ * restored to its initial content.  Trials are reported in `trials` (up to max_trials).
+ * Returns the number of trials run or an error code.  The tile shape is fixed: one
+ * 20 x 20 block per 256-thread slot. */
 typedef struct {
     int engine_ctas, local_max_blocks, ndown, nup, ntop;
     int cycles;          /* V-cycles (FP64) or defect-correction steps (mixed), worst item */
     double ms;           /* best device time of the trial, -1 if it missed the tolerance */
     double omega;        /* relaxation factor of the trial */
+    int inner_cycles;    /* FP32 V-cycles per defect-correction step (mixed) */
 } srmg_tune_trial;
 int srmg_autotune(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc,
                   double s, int op, double k2, int geom, const int8_t bc[9],

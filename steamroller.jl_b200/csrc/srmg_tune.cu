@@ -14,8 +14,13 @@
 //   * the relaxation factor omega of the red-black Gauss-Seidel sweeps (1, 1.1, 1.2):
 //     over-relaxed smoothing contracts more per V-cycle (measured on the 1.5M-leaf
 //     tree: 7 instead of 8 FP64-direct cycles at (2, 2), 9 instead of 12 at (1, 1)).
+//   * mixed solves: FP32 V-cycles per defect-correction step (inner_cycles 1..4): more
+//     cycles per step mean fewer FP64 update/defect passes, until the FP32 correction
+//     stops contracting (measured on the 1.5M-leaf tree with the level-2 direct solve:
+//     9 cycles in 3 steps, 1.97 ms, against 9 in 5, 2.16 ms, at 2 per step).
 // The launch shape is tuned first at the caller's sweeps and omega (6 candidates), then
-// the sweeps and omega at that shape (15 candidates).
+// the sweeps and omega at that shape (15 candidates), then for mixed solves the inner
+// cycles at those (4 candidates).
 // The tile shape is fixed by the data layout (one 20 x 20 block per 256-thread slot,
 // four slots per CTA).  The fastest trial's settings are applied to the context and
 // written to *opts; the caller's fields are restored after every trial.
@@ -45,6 +50,7 @@ namespace {
 struct Cand {
   int ctas, local_max, ndown, nup;
   double omega;
+  int inner;
 };
 
 // Run every candidate with `solve` (which restores its own inputs), keep the fastest.
@@ -56,16 +62,19 @@ int tune(srmg_ctx *ctx, srmg_solve_opts *opts, srmg_tune_trial *trials, int max_
   const double omegas[] = {1.0, 1.1, 1.2};
   const int save_ctas = ctx->engine_ctas, save_lm = ctx->local_max_blocks;
   double best = 1e300;
-  Cand pick{save_ctas, save_lm, opts->ndown, opts->nup, opts->omega};
+  Cand pick{save_ctas, save_lm, opts->ndown, opts->nup, opts->omega, std::max(1, opts->inner_cycles)};
   int n = 0;
-  for (int stage = 0; stage < 2; ++stage) {
+  const int nstage = opts->mode == SRMG_MODE_MIXED ? 3 : 2;
+  for (int stage = 0; stage < nstage; ++stage) {
   std::vector<Cand> cands;
   if (stage == 0) {
     for (int ctas : {0, nsm / 2})
-      for (int lm : {4, 16, 64}) cands.push_back({ctas, lm, opts->ndown, opts->nup, opts->omega});
-  } else {
+      for (int lm : {4, 16, 64}) cands.push_back({ctas, lm, opts->ndown, opts->nup, opts->omega, pick.inner});
+  } else if (stage == 1) {
     for (const auto &sw : sweeps)
-      for (double om : omegas) cands.push_back({pick.ctas, pick.local_max, sw[0], sw[1], om});
+      for (double om : omegas) cands.push_back({pick.ctas, pick.local_max, sw[0], sw[1], om, pick.inner});
+  } else {
+    for (int in : {1, 2, 3, 4}) cands.push_back({pick.ctas, pick.local_max, pick.ndown, pick.nup, pick.omega, in});
   }
   for (const Cand &c : cands) {
     ctx->engine_ctas = c.ctas;
@@ -74,6 +83,7 @@ int tune(srmg_ctx *ctx, srmg_solve_opts *opts, srmg_tune_trial *trials, int max_
     o.ndown = c.ndown;
     o.nup = c.nup;
     o.omega = c.omega;
+    o.inner_cycles = c.inner;
     double ms = 0.0, ms2 = 0.0;
     int cyc = 0;
     bool ok = false;
@@ -95,6 +105,7 @@ int tune(srmg_ctx *ctx, srmg_solve_opts *opts, srmg_tune_trial *trials, int max_
       tr.ms = ok ? t : -1.0;
       tr.cycles = cyc;
       tr.omega = c.omega;
+      tr.inner_cycles = c.inner;
     }
     n++;
     if (ok && t < best) {
@@ -108,6 +119,7 @@ int tune(srmg_ctx *ctx, srmg_solve_opts *opts, srmg_tune_trial *trials, int max_
   opts->ndown = pick.ndown;
   opts->nup = pick.nup;
   opts->omega = pick.omega;
+  opts->inner_cycles = pick.inner;
   return n;
 }
 

@@ -60,7 +60,7 @@ class Stats(ctypes.Structure):
 class TuneTrial(ctypes.Structure):
     _fields_ = [("engine_ctas", ctypes.c_int), ("local_max_blocks", ctypes.c_int), ("ndown", ctypes.c_int),
                 ("nup", ctypes.c_int), ("ntop", ctypes.c_int), ("cycles", ctypes.c_int), ("ms", ctypes.c_double),
-                ("omega", ctypes.c_double)]
+                ("omega", ctypes.c_double), ("inner_cycles", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -145,30 +145,38 @@ def test_batch_rejects_bad_items(setup):
 
 def test_autotune_single_and_batch(setup):
     """The autotuner times every candidate to the tolerance (6 launch shapes, then 15
-    sweep-count and relaxation-factor pairs at the fastest shape), restores the
-    caller's initial guess, and leaves the fastest launch shape, sweep counts and omega
-    in force."""
+    sweep-count and relaxation-factor pairs at the fastest shape, then for mixed solves
+    4 inner-cycle counts at the fastest pair), restores the caller's initial guess, and
+    leaves the fastest launch shape, sweep counts, omega and inner cycles in force; an
+    FP64-direct tuning has no inner-cycle stage."""
     ctxs, items, batch = setup
     c, p = items[0]
     u0 = np.zeros_like(p.b)
     ug, bg = torch_cuda(u0), torch_cuda(p.b)
     chosen, trials = mg.autotune(c, ug, bg, p.s, p.geom, p.bc, disc(p), tol=1e-8, mode=mg.MODE_MIXED)
-    assert len(trials) == 21
+    assert len(trials) == 25
     assert all(t["ms"] > 0 for t in trials)
-    assert {t["omega"] for t in trials[6:]} == {1.0, 1.1, 1.2}
+    assert {t["omega"] for t in trials[6:21]} == {1.0, 1.1, 1.2}
+    assert [t["inner_cycles"] for t in trials[21:]] == [1, 2, 3, 4]
     best = min(trials, key=lambda t: t["ms"])
-    assert (chosen["ndown"], chosen["nup"], chosen["omega"]) == (best["ndown"], best["nup"], best["omega"])
+    assert (chosen["ndown"], chosen["nup"], chosen["omega"], chosen["inner_cycles"]) == \
+        (best["ndown"], best["nup"], best["omega"], best["inner_cycles"])
     np.testing.assert_array_equal(to_np(ug), u0)  # initial guess restored
     st = mg.solve(c, ug, bg, p.s, p.geom, p.bc, disc(p), tol=1e-8, mode=mg.MODE_MIXED,
-                  ndown=chosen["ndown"], nup=chosen["nup"], ntop=chosen["ntop"], omega=chosen["omega"])
+                  ndown=chosen["ndown"], nup=chosen["nup"], ntop=chosen["ntop"], omega=chosen["omega"],
+                  inner_cycles=chosen["inner_cycles"])
     assert st["rel_residual"] <= 1e-8
+    c.set_option("engine_ctas", 0).set_option("local_max_blocks", 4)
+    _, trials_d = mg.autotune(c, ug, bg, p.s, p.geom, p.bc, disc(p), tol=1e-8, mode=mg.MODE_FP64_DIRECT)
+    assert len(trials_d) == 21
     c.set_option("engine_ctas", 0).set_option("local_max_blocks", 4)
     us = [torch_cuda(np.zeros_like(q.b)) for _, q in items]
     bs = [torch_cuda(q.b) for _, q in items]
     chosen, trials = mg.batch_autotune(batch, us, bs, tol=1e-8, mode=mg.MODE_MIXED)
-    assert len(trials) == 21 and all(t["ms"] > 0 for t in trials)
+    assert len(trials) == 25 and all(t["ms"] > 0 for t in trials)
     sts = batch.solve(us, bs, mode=mg.MODE_MIXED, tol=1e-8, ndown=chosen["ndown"], nup=chosen["nup"],
-                      ntop=chosen["ntop"], omega=chosen["omega"], max_cycles=400)
+                      ntop=chosen["ntop"], omega=chosen["omega"], inner_cycles=chosen["inner_cycles"],
+                      max_cycles=400)
     assert all(s["rel_residual"] <= 1e-8 for s in sts)
     batch.set_option("engine_ctas", 0).set_option("local_max_blocks", 4)
 
