@@ -48,9 +48,9 @@ METRIC = "field solves/sec at 1e-8 rel residual (mixed-precision multigrid; plai
 # (57.03 MB read + 39.74 MB written)
 TRAFFIC_VCYCLE_CONFIG2 = 96.77e6
 # DRAM bytes of one mixed-solve launch on the config-2 tree (the tuned V(1,1) cycle,
-# 9 V-cycles in 5 defect-correction steps), from an ncu capture (172.92 MB read +
-# 252.54 MB written)
-TRAFFIC_MIXED_CONFIG2 = 425.46e6
+# 9 V-cycles in 3 defect-correction steps, the direct solve on level 2), from an ncu
+# capture (171.37 MB read + 151.77 MB written)
+TRAFFIC_MIXED_CONFIG2 = 323.15e6
 
 
 def peaks():

@@ -66,6 +66,12 @@ def run(net, steps=200, sample_every=50, device=0, log=None, problem=None):
         src = [zf() for _ in LAMBDAS]
     mask_t = torch.from_numpy(leaf_mask(p.tree, nblk)).to(dev)
     opts = dict(tol=1e-8, max_cycles=5000, **mg.TUNED)          # mixed solves: the tuned smoother
+    # one untimed solve of each kind first: a context builds the inverse of its direct
+    # coarsest solve (per operator, on the host) the first time it solves
+    with torch.cuda.stream(stream):
+        mg.solve(s.ctx, s.phi.clone(), s.b.clone(), s.s, s.geom, s.bc, mode=mg.MODE_MIXED, **dict(opts, max_cycles=1))
+        batch.solve([zf() for _ in LAMBDAS], [zf() for _ in LAMBDAS], mode=mg.MODE_MIXED, **dict(opts, max_cycles=1))
+    stream.synchronize()
     ref_opts = dict(tol=1e-8, ndown=2, ntop=4, nup=2, max_cycles=5000)  # plain FP64: the reference's cycle
     rec = {"poisson_ms": [], "photo_ms": [], "poisson_cycles": [], "photo_cycles": [], "which": [],
            "stage_poisson_cycles": [[] for _ in range(STAGES)]}
