@@ -444,6 +444,31 @@ def test_mixed_solve_reaches_fp64_solution(engine):
     assert err < 1e-6, err
 
 
+@pytest.mark.parametrize("variant", ["helmholtz", "cartesian", "cyl2"])
+@pytest.mark.parametrize("direct_level", [1, 2])
+def test_mixed_solve_direct_levels_operator_variants(variant, direct_level):
+    """The mixed solve with the direct FP64 solve on level 1 (one CTA) or level 2 (every
+    CTA) reaches the oracle's FP64 solution for the Helmholtz operator (photoionization
+    boundary table) and the Cartesian and r = dim 2 geometries, with the autotuner's
+    smoother and 3 V-cycles per defect-correction step."""
+    p = variant_problem(variant)
+    pr = Pair(p)
+    pr.ctx.set_option("direct_level", direct_level)
+    u, b = _prepared(pr)
+    ug = torch_cuda(u)
+    lpl = ("helmholtz", p.k2) if p.op == 1 else None
+    st = mg.solve(pr.ctx, ug, torch_cuda(b), p.s, p.geom, p.bc, lpldisc=lpl, tol=1e-8, mode=mg.MODE_MIXED,
+                  max_cycles=200, inner_cycles=3, **mg.TUNED)
+    assert st["rel_residual"] <= 1e-8
+    # the smoother was tuned on r = dim 1 trees; with r = dim 2 and the level-1 solve
+    # this tree needs 49 cycles
+    assert st["cycles"] < 80
+    uo = u.copy()
+    pr.orc.solve(uo, b.copy(), 1e-11, max_cycles=5000)
+    err = rel_l2(to_np(ug), uo, leaf_mask(p))
+    assert err < 1e-6, err
+
+
 def leaf_mask(p):
     m = np.zeros(p.b.shape, dtype=bool)
     for layer in p.tree:
