@@ -749,7 +749,6 @@ def run_rows(local):
     import torch
     from srmg import gen, gen3, model, multigrid as mg
     from srmg.tree3 import Tree3, populate, connectivity as connectivity3, STAR3, BOX3
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
     hbm, _ = peaks()
     dev = torch.device("cuda", local)
     stream = torch.cuda.Stream(device=dev)
@@ -805,7 +804,7 @@ def run_rows(local):
         row[name] = line(t, ms, ln)
         row[name + "_sequencer"] = line(t, msq, lnq)
         ctx.close()
-    import freebc_oracle as fo
+    from srmg import freebc as fbc
     p = gen.config2(seed=2, target_leaf=1_500_000)
     ctx = mg.Context(local).set_tree(p.tree, p.conn)
     ctx.set_stream(stream.cuda_stream)
@@ -814,7 +813,7 @@ def run_rows(local):
     torch.cuda.synchronize()
     fb = {}
     for level in (9, 11):
-        n, _, _, f = fo.kernel(1, level, (1, 1), p.h1)
+        n, _, _, f = fbc.kernel(1, level, (1, 1), p.h1)
         mg.freebc_set(ctx, 1, level, (1, 1), f)
         with torch.cuda.stream(stream):
             for _ in range(2):
