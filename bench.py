@@ -187,8 +187,10 @@ class ClockSampler:
         return out
 
 
-def dist_setup(backend=None):
-    """One process per GPU (torchrun env); NCCL on GPUs, gloo on the host (tests)."""
+def dist_setup(backend=None, timeout_s=120):
+    """One process per GPU (torchrun env); NCCL on GPUs, gloo on the host (tests).  A
+    rank that dies or never joins makes the others' next collective end with an error
+    within timeout_s instead of waiting for good."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -196,7 +198,7 @@ def dist_setup(backend=None):
     if world > 1:
         import torch.distributed as dist
         import datetime
-        dist.init_process_group(backend or "nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(backend or "nccl", timeout=datetime.timedelta(seconds=timeout_s))
         pg = dist
     return world, rank, local, pg
 

@@ -325,6 +325,14 @@ int srmg_electric_field(srmg_ctx *ctx, double *e, double *eabs, const double *u,
 int srmg_electric_field_dev(srmg_ctx *ctx, double *e, double *eabs, const double *u, int64_t nblk_alloc,
                             double h, const double e0[2]);
 
+/* Self-test of the failure path of the persistent kernels' grid barrier (no reference
+ * counterpart): one cooperative launch in which every CTA but one enters a grid
+ * barrier whose bounded wait is limited to timeout_ms (1..2000); the missing CTA makes
+ * the wait run out, the kernel records it in the context's error word and returns.
+ * Returns SRMG_ERR_TIMEOUT (the status a stuck barrier of a solve reports), or
+ * SRMG_ERR_BADARG.  Nothing faults or hangs; the context stays usable. */
+int srmg_selftest_barrier_timeout(srmg_ctx *ctx, int timeout_ms);
+
 /* Allocation-free residual norm.  No counterpart in the reference: it exists for
  * callers that cannot call cudaMalloc when they need the norm -- hosts whose device
  * memory belongs to their own pool allocator, or loops that cannot take an

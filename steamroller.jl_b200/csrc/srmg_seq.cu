@@ -62,7 +62,37 @@ __global__ void __launch_bounds__(kSeqThreads, kSeqPerSM)
   }
 }
 
+// Self-test of the barrier's failure path: every CTA but `absent` enters one grid
+// barrier; the absent CTA returns at once, so the others' bounded wait runs out, the
+// first to give up records error 1 and all of them return.
+__global__ void k_barrier_selftest(unsigned *bar, int *err, long long timeout_ns, int absent) {
+  if ((int)blockIdx.x == absent) return;
+  unsigned epoch = 0;
+  grid_barrier(bar, err, epoch, timeout_ns);
+}
+
 }  // namespace
+
+extern "C" int srmg_selftest_barrier_timeout(srmg_ctx *ctx, int timeout_ms) {
+  if (!ctx || timeout_ms < 1 || timeout_ms > 2000) return SRMG_ERR_BADARG;
+  cudaSetDevice(ctx->device);
+  if (ctx->num_sms == 0) CK(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  RC(ensure(ctx, ctx->sync, 256 + sizeof(int) * (size_t)std::max(ctx->nitems, 1)));
+  CK(cudaMemsetAsync(ctx->sync.p, 0, 256, ctx->stream));
+  unsigned *bar = (unsigned *)ctx->sync.p;
+  int *err = (int *)((char *)ctx->sync.p + 128);
+  long long timeout = (long long)timeout_ms * 1000000LL;
+  int absent = 0;
+  void *args[] = {&bar, &err, &timeout, &absent};
+  CK(cudaLaunchCooperativeKernel((const void *)k_barrier_selftest, dim3(ctx->num_sms), dim3(128), args, 0,
+                                 ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const int rc = engine_check(ctx);  // SRMG_ERR_TIMEOUT when the wait ran out
+  // leave the barrier state clean for the next launch
+  CK(cudaMemsetAsync(ctx->sync.p, 0, 256, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return rc;
+}
 
 // One launch of the sequencer over `nops` records at d_ops (device memory), on the
 // context's stream.  The barrier counter and error word are the persistent engine's

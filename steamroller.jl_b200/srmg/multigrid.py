@@ -125,6 +125,7 @@ SIGNATURES = {
     "srmg_interp_add_level_dev": (_I, [_P, _P, _P, _I64, _I]),
     "srmg_residual_postrestrict_level_dev": (_I, [_P, _P, _P, _P, _I64, _I, _D, _I, _D, _I]),
     "srmg_resnorm_noalloc": (_I, [_P, _P, _P, _I64, _D, _I, _D, _I, _P]),
+    "srmg_selftest_barrier_timeout": (_I, [_P, _I]),
     "srmg_set_option": (_I, [_P, ctypes.c_char_p, _I64]),
     "srmg_host_register": (_I, [_P, _P, _I64]),
     "srmg_host_unregister": (_I, [_P, _P]),
