@@ -222,33 +222,42 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
 }
 
 // Per-slot staging: kBuf buffers of block tiles and the records of a chunk of up to
-// kChunk blocks.  The GS and restriction phases take two blocks per iteration (one per
-// half slot), so four buffers hold the current pair and the next; the prolongation
-// phase runs kBuf - 1 blocks ahead.  Shared memory is kept small on purpose: what the
-// CTA does not claim stays L1 cache for the scattered loads (face records, coarse
-// values of refinement ghosts, spills), and a larger staging area measured slower.
+// kChunk blocks.  The GS, restriction and prolongation phases take two blocks per
+// iteration (one per half slot), so four buffers hold the current pair and the next.
+// Shared memory is kept small on purpose: what the CTA does not claim stays L1 cache for
+// the scattered loads (face records, coarse values of refinement ghosts, spills), and a
+// larger staging area measured slower.
 constexpr int kBuf = 4;
 constexpr int kChunk = 32;
 constexpr int kWRow = 2 * kS;  // a weight row: wm, then wp, at the tile positions 0..19
-// Levels 1..kLevCache whose GS phases give a slot at most two blocks keep those blocks'
-// records in the slot's shared memory for the whole launch (loaded once at the start),
-// so that the phase issues its tile copies at once instead of after a record load.
-constexpr int kLevCache = 12;
+// Launch-long record cache: a single-item launch loads, once at its start and level by
+// level from the coarsest, a slot's whole share of a level's GS, restriction and
+// prolongation records into kRecRows rows of the slot's shared memory while it fits (at
+// most one chunk per level and kind), so that those phases issue their tile copies at
+// once instead of after one or two dependent record loads.  FP64 keeps the footprint of
+// two blocks per level on twelve levels (the 1024-thread FP64 shape is sensitive to the
+// L1 it leaves); FP32 takes a third more.
+template <typename T>
+constexpr int kRecRows = sizeof(T) == 4 ? 96 : 72;
 template <typename T>
 struct SlotSmem {
   T tile[kBuf][kSS];
   T tile2[kBuf][kSS];  // the second tile of a pair: b (GS, restriction) or the parent's e (prolongation)
   T wst[kBuf][kWRow];  // the block's weight row (GS, restriction)
   int4 recs[kChunk][6];
-  int4 rgs[kLevCache][2][6];  // cached GS records of the small levels (rows of 6 like recs)
-  int4 rres[kLevCache][2][6];  // cached restriction records (child edge, fine info, coarse faces)
-  int4 rpro[kLevCache][2][6];  // cached prolongation records (child edge, fine faces)
+  // cached rows: GS {blk, cr, cz, mask} + 4 faces; restriction {child edge}, fine info,
+  // 4 coarse faces; prolongation {child edge} + 4 fine faces
+  int4 rc[kRecRows<T>][6];
   uint64_t bar[kBuf];
   int sel[kChunk];  // list positions of the chunk's blocks that take part
   int cnt;
-  unsigned gs_cached;  // bit l: the GS records of level l are in rgs[l - 1]
-  unsigned ch_cached;  // bit l: the restriction and prolongation records of level l are cached
+  int cstep[kMaxLev];                  // the list step the level's cached rows were taken with
+  signed char off_gs[kMaxLev];         // first cached row of level l's GS records, or -1
+  signed char off_res[kMaxLev];        // ... of its restriction records (child edges at level l)
+  signed char off_pro[kMaxLev];        // ... of its prolongation records
+  signed char pad_[(16 - (3 * kMaxLev + 4) % 16) % 16];
 };
+static_assert(kRecRows<float> <= 127 && kRecRows<double> <= 127, "row offsets are signed chars");
 // Bulk copies land on 16-byte boundaries: every tile buffer of every slot.
 static_assert(sizeof(SlotSmem<double>) % 16 == 0 && sizeof(SlotSmem<float>) % 16 == 0, "slot size");
 static_assert((kSS * sizeof(float)) % 16 == 0 && (kBuf * kSS * sizeof(float)) % 16 == 0, "tile offsets");
@@ -500,7 +509,7 @@ __device__ __forceinline__ HaloCell halo_cell(int t) {
   return h;
 }
 
-// The red halo cell m (0..31) handled by lane m % 8 of warp m / 8 of a half slot (the
+// Red halo cell m (0..31) of a block, handled by lane m of warp 0 of a half slot (the
 // cell 2 (m % 8) + (m / 8 % 2) of ghost face m / 8), packed into two ints once per CTA:
 // {hx | hy << 5 | nx << 10 | ny << 15 | f << 20 | nsub << 22, (cx + 1) | (cy + 1) << 6 |
 // (cnx + 1) << 12 | (cny + 1) << 18}, the corner fields all -1 where there is none.
@@ -642,16 +651,18 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
   const bool yodd = (y & 1) != 0;  // red (colour 0 of RedBlack{0}, updated first) is x0 if y is odd
   const int xr = yodd ? x0 : x0 + 1, xbk = yodd ? x0 + 1 : x0;  // the pair's red and black cells
   const int mysub = ((x0 - 2) >> 3) + 2 * ((y - 2) >> 3);
-  // lanes 0-7 of warp wv: the red cells 2 lane + (wv % 2) of ghost face wv
-  const bool hthr = lane < 8;
-  const int hm = 8 * wv + (lane & 7);  // this lane's entry of the halo table
+  // warp 0 of a half: the 32 red halo cells, lane m taking entry m of the halo table (one
+  // warp issues the halo code instead of a quarter of every warp's lanes)
+  const bool hthr = wv == 0;
+  const int hm = lane;  // this lane's entry of the halo table
   // neighbour values of the halo cell, loaded one iteration ahead
   // (b comes from b's ghost layer when A.bghost, except the FAS right-hand side of a
   // covered neighbour cell, formed here from the neighbour's restricted residual in e)
   T hvn = T(0), hcn = T(0);
   // the records: the launch-long cache of a small level, or the chunk staged in recs
-  const bool cached = A.nitems == 1 && l <= kLevCache && ((S.gs_cached >> l) & 1u);
-  int4(*R)[6] = cached ? S.rgs[l - 1] : S.recs;
+  const int co = A.nitems == 1 && step == S.cstep[l - 1] ? S.off_gs[l - 1] : -1;
+  const bool cached = co >= 0;
+  int4(*R)[6] = cached ? &S.rc[co] : S.recs;
   auto prefetch = [&](int j) {
     if (hthr) {
       const HaloCell hc_ = halo_unpack(halo_tab[hm]);
@@ -669,12 +680,14 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
     const int4 bk = R[j][0];
     issue_block<T>(A, S, (pk + j) % kBuf, src, bk.x, bk.y, bk.z);
   };
-  // one item: the operator values stay in registers for the whole level
+  // one item: the operator values and the boundary table stay in registers for the
+  // whole level
   T s = A.it_par[l], centre = A.it_par[32 + l], nwc = A.it_par[64 + l];
+  const unsigned sgb1 = (unsigned)A.it_sgbits[0];
   for (int c0 = 0; c0 < nmine; c0 += kChunk) {
     int cn;
     if (cached) {
-      cn = nmine;  // <= 2, one chunk
+      cn = nmine;  // <= kChunk, one chunk
     } else if (A.nitems == 1) {
       cn = min(kChunk, nmine - c0);
       for (int i = t; i < 5 * cn; i += 256) {
@@ -708,9 +721,11 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
       const int4 *fc = &R[act ? j : 0][1];
       const int64_t xo = (int64_t)bk.x * kSS + o0;
       const bool cov = fas && ((bk.w >> mysub) & 1);
-      // the covered cells' restricted residual (FAS), loaded while the tiles arrive
-      T ex0 = T(0), ex1 = T(0);
+      // the covered cells' restricted residual (FAS), loaded while the tiles arrive, and
+      // in FP32 the pair's u1 (for e) as well (the register-capped FP64 shape would spill)
+      T ex0 = T(0), ex1 = T(0), uo0 = T(0), uo1 = T(0);
       if (act && cov) ld_pair<T>(A.e + xo, ex0, ex1);
+      if (sizeof(T) == 4 && act && make_e) ld_pair<T>(A.u1 + xo, uo0, uo1);
       bool ok = true;
       if (act) ok = mbar_wait(&S.bar[buf], (kb / kBuf) & 1, A.err, A.timeout_ns);
       T *tile = S.tile[buf];
@@ -794,7 +809,7 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
         const T black_new = fma(nwc, fma(s, bb, Lb), cb);
         const T nu0 = yodd ? red_new : black_new, nu1 = yodd ? black_new : red_new;
         const int X = bk.x;
-        const unsigned sgb = (unsigned)A.it_sgbits[item_of(bk)];
+        const unsigned sgb = A.nitems == 1 ? sgb1 : (unsigned)A.it_sgbits[item_of(bk)];
         st_pair<T>(dst + xo, nu0, nu1);
         push_pair<T>(sgb, dst, X, fc, x0, y, nu0, nu1);
         if (fc[wv].x == FACE_REFBND) {  // warp wv: the 32 ghost cells of face wv
@@ -803,8 +818,7 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
           dst[(int64_t)X * kSS + gx + kS * gy] = tile[gx + kS * gy];  // frozen during smoothing
         }
         if (make_e) {
-          T uo0, uo1;
-          ld_pair<T>(A.u1 + xo, uo0, uo1);
+          if (sizeof(T) == 8) ld_pair<T>(A.u1 + xo, uo0, uo1);
           const T ev0 = nu0 - uo0, ev1 = nu1 - uo1;
           st_pair<T>(A.e + xo, ev0, ev1);
           push_pair<T>(sgb, A.e, X, fc, x0, y, ev0, ev1);
@@ -838,8 +852,12 @@ __device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
   const int half = t >> 7, h = t & 127;
   const int x0 = 2 + 2 * (h & 7), y = 2 + (h >> 3);
   const int o0 = x0 + kS * y;
-  const bool cached = A.nitems == 1 && l <= kLevCache && ((S.ch_cached >> l) & 1u);
-  int4(*R)[6] = cached ? S.rres[l - 1] : S.recs;
+  const int co = A.nitems == 1 && step == S.cstep[l - 1] ? S.off_res[l - 1] : -1;
+  const bool cached = co >= 0;
+  int4(*R)[6] = cached ? &S.rc[co] : S.recs;
+  // one item: its operator values and boundary table, loaded before the first tile wait
+  const T s1 = A.it_par[l], centre1 = A.it_par[32 + l];
+  const unsigned sgb1 = (unsigned)A.it_sgbits[0];
   auto issue = [&](int j) {
     const int4 fi = R[j][1];
     issue_block<T>(A, S, (pk + j) % kBuf, uf, R[j][0].x, fi.x, fi.y);
@@ -850,7 +868,7 @@ __device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
     // coarse block's faces (or the launch-long cache of a small level)
     int cn;
     if (cached) {
-      cn = nmine;  // <= 2, one chunk
+      cn = nmine;  // <= kChunk, one chunk
     } else {
       select_chunk<T>(S, t, c0, nmine, first, step,
                       [&](int gi) { return A.nitems == 1 || !A.frozen[A.tr.info[ch[gi].x].z >> 8]; });
@@ -879,7 +897,7 @@ __device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
       const int item = fi.z >> 8;
       if (act && ok) {
         const T *par = A.it_par + item * kParStride;
-        const T s = par[l], centre = par[32 + l];
+        const T s = A.nitems == 1 ? s1 : par[l], centre = A.nitems == 1 ? centre1 : par[32 + l];
         const W5<T> w0 = wrow_w<T>(A.geom, S.wst[buf], x0, y);
         const W5<T> w1 = wrow_w<T>(A.geom, S.wst[buf], x0 + 1, y);
         T c0v, c1v, b0, b1, dn0, dn1, up0, up1;
@@ -910,7 +928,7 @@ __device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
         const T cu = restrict4<T>(tile, 2 + 2 * kx, 2 + 2 * ky);
         const T cr = restrict4<T>(S.tile2[buf], 2 + 2 * kx, 2 + 2 * ky);
         uc[(int64_t)C * kSS + cx + kS * cy] = cu;
-        push_f<T>((unsigned)A.it_sgbits[item], uc, C, &R[j][2], cx, cy, cu);
+        push_f<T>(A.nitems == 1 ? sgb1 : (unsigned)A.it_sgbits[item], uc, C, &R[j][2], cx, cy, cu);
         A.e[(int64_t)C * kSS + cx + kS * cy] = cr;
       }
     }
@@ -922,9 +940,12 @@ __device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
 
 // u_fine += P(e_coarse) on every valid cell (in place in uf), pushes of the new edge
 // values, and the fine block's refinement-boundary ghosts from uc (final coarse level).
-// Per child edge the fine block's u tile and its parent's e tile arrive together by
-// two bulk copies on one mbarrier of the slot's kBuf-deep pipeline, and the child's
-// face records are staged in shared memory.  Children of frozen items are skipped.
+// A slot's halves take one child edge each per iteration; per child edge the fine
+// block's u tile and its parent's e tile arrive together by two bulk copies on one
+// mbarrier of the slot's kBuf-deep pipeline, and thread h of a half updates the cell
+// pair (x0, y), (x0 + 1, y), x0 = 2 + 2 (h % 8), y = 2 + h / 8, and computes refinement
+// ghost h, whose coarse values it loads while the tiles arrive.  The child's face records
+// are staged in shared memory.  Children of frozen items are skipped.
 template <typename T>
 __device__ bool ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int first, int step, int t, int slot,
                            SlotSmem<T> &S, unsigned &pk) {
@@ -932,19 +953,22 @@ __device__ bool ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int f
   const int4 *ch = A.tr.lvl_child[l - 1];
   const int nmine = (first < n) ? (n - 1 - first) / step + 1 : 0;
   if (nmine == 0) return true;
-  const int dx = t & 15, dy = t >> 4;
-  const int x = 2 + dx, y = 2 + dy;
-  const int ir = dx & 1, iz = dy & 1;
-  const bool cached = A.nitems == 1 && l <= kLevCache && ((S.ch_cached >> l) & 1u);
-  int4(*R)[6] = cached ? S.rpro[l - 1] : S.recs;
-  auto issue = [&](unsigned kb, int j) { issue_pair<T>(S, kb % kBuf, uf, R[j][0].x, A.e, R[j][0].y); };
+  const int half = t >> 7, h = t & 127;
+  const int x0 = 2 + 2 * (h & 7), y = 2 + (h >> 3);
+  const int o0 = x0 + kS * y;
+  const int iz = (y - 2) & 1;  // the pair's coarse cell: column h % 8, row (y - 2) / 2 of the subblock
+  const int co = A.nitems == 1 && step == S.cstep[l - 1] ? S.off_pro[l - 1] : -1;
+  const bool cached = co >= 0;
+  int4(*R)[6] = cached ? &S.rc[co] : S.recs;
+  const unsigned sgb1 = (unsigned)A.it_sgbits[0];
+  auto issue = [&](int j) { issue_pair<T>(S, (pk + j) % kBuf, uf, R[j][0].x, A.e, R[j][0].y); };
   for (int c0 = 0; c0 < nmine; c0 += kChunk) {
     // the chunk's next child edges, without those of frozen items:
     // recs[q][0] = {fine, coarse, sb_r, sb_z}, recs[q][1..4] = the fine block's faces
     // (or the launch-long cache of a small level)
     int cn;
     if (cached) {
-      cn = nmine;  // <= 2, one chunk
+      cn = nmine;  // <= kChunk, one chunk
     } else {
       select_chunk<T>(S, t, c0, nmine, first, step,
                       [&](int gi) { return A.nitems == 1 || !A.frozen[A.tr.info[ch[gi].x].z >> 8]; });
@@ -959,30 +983,52 @@ __device__ bool ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int f
       if (cn == 0) continue;
     }
     if (t == 0)
-      for (int q = 0; q < kBuf - 1 && q < cn; ++q) issue(pk + q, q);
-    for (int j = 0; j < cn; ++j) {
+      for (int q = 0; q < kBuf && q < cn; ++q) issue(q);
+    for (int i = 0; 2 * i < cn; ++i) {
+      const int j = 2 * i + half;
+      const bool act = j < cn;
       const unsigned kb = pk + j;
       const int buf = kb % kBuf;
-      const int4 e = R[j][0];
-      const int4 *fc = &R[j][1];
+      const int4 e = R[act ? j : 0][0];
+      const int4 *fc = &R[act ? j : 0][1];
       const int F = e.x;
-      if (t == 0 && j + kBuf - 1 < cn) issue(kb + kBuf - 1, j + kBuf - 1);
-      if (!mbar_wait(&S.bar[buf], (kb / kBuf) & 1, A.err, A.timeout_ns)) {
-        drain_slot<T>(A, S, kb, j, cn);
+      // loaded while the tiles arrive: refinement ghost h from the coarse level, the
+      // item's boundary table
+      const int4 gf = fc[h >> 5];
+      const bool rb = act && gf.x == FACE_REFBND;
+      T gv = T(0);
+      int gx = 0, gy = 0;
+      if (rb) gv = refbnd_val<T>(uc, gf, h, gx, gy);
+      const unsigned sgb = (A.nitems == 1 || !act) ? sgb1 : (unsigned)A.it_sgbits[A.tr.info[F].z >> 8];
+      bool ok = true;
+      if (act) ok = mbar_wait(&S.bar[buf], (kb / kBuf) & 1, A.err, A.timeout_ns);
+      if (act && ok) {
+        const T *ut = S.tile[buf], *cb = S.tile2[buf];
+        const int jr = 2 + 8 * (e.z - 1) + (h & 7), jz = 2 + 8 * (e.w - 1) + ((y - 2) >> 1);
+        const int oc = jr + kS * jz;
+        // interp (src/interp.jl:24-63): 1/2 of the parent cell, 1/4 of its r and z
+        // neighbours on the child cell's side, in that order
+        const T cc = dmul<T>(T(0.5), cb[oc]);
+        const T cz = dmul<T>(T(0.25), cb[oc + kS * (2 * iz - 1)]);
+        const T v0 = dadd<T>(dadd<T>(cc, dmul<T>(T(0.25), cb[oc - 1])), cz);
+        const T v1 = dadd<T>(dadd<T>(cc, dmul<T>(T(0.25), cb[oc + 1])), cz);
+        T u0, u1;
+        ld_pair<T>(ut + o0, u0, u1);
+        const T nu0 = dadd<T>(v0, u0), nu1 = dadd<T>(v1, u1);
+        st_pair<T>(uf + (int64_t)F * kSS + o0, nu0, nu1);
+        push_pair<T>(sgb, uf, F, fc, x0, y, nu0, nu1);
+        if (rb) uf[(int64_t)F * kSS + gx + kS * gy] = gv;
+      }
+      if (!slot_and(slot, ok)) {
+        // leave no copy in flight: wait (bounded) for every one issued and not consumed
+        const int issued = min(cn, kBuf + 2 * i);
+        for (int q = 2 * i; q < issued; ++q)
+          mbar_wait(&S.bar[(pk + q) % kBuf], ((pk + q) / kBuf) & 1, A.err, A.timeout_ns);
         return false;
       }
-      const T *ut = S.tile[buf], *cb = S.tile2[buf];
-      const int jr = 2 + 8 * (e.z - 1) + (dx >> 1), jz = 2 + 8 * (e.w - 1) + (dy >> 1);
-      const int oc = jr + kS * jz;
-      T v = dmul<T>(T(0.5), cb[oc]);
-      v = dadd<T>(v, dmul<T>(T(0.25), cb[oc + (2 * ir - 1)]));
-      v = dadd<T>(v, dmul<T>(T(0.25), cb[oc + kS * (2 * iz - 1)]));
-      const T nu = dadd<T>(v, ut[x + kS * y]);
-      uf[(int64_t)F * kSS + x + kS * y] = nu;
-      const int item = A.tr.info[F].z >> 8;
-      push<T>(A, item, uf, F, fc, x, y, nu);
-      if (t < 128) refbnd_ghost<T>(uf, uc, F, fc, t);
-      slot_sync(slot);  // the buffers are refilled kBuf - 1 items later
+      // this iteration's buffers (and records) are free: refill them kBuf blocks later
+      if (t == 0)
+        for (int q = 2 * i + kBuf; q < 2 * i + 2 + kBuf && q < cn; ++q) issue(q);
     }
     pk += cn;
   }
@@ -1533,39 +1579,47 @@ __global__ void __launch_bounds__(NT, 1) k_engine_vcycle(const __grid_constant__
   }
   __shared__ int2 s_halo[32];  // the GS halo cells, packed (halo_pack)
   if (threadIdx.x < 32) s_halo[threadIdx.x] = halo_pack(threadIdx.x);
-  // GS records of the small levels (at most two blocks for this slot), once per launch
-  if (t == 0) S.gs_cached = S.ch_cached = 0u;
+  // the launch-long record cache (single item): level by level from the coarsest, the
+  // slot's GS records, then its restriction and prolongation records, while they fit
+  if (t == 0)
+    for (int l = 0; l < kMaxLev; ++l) {
+      S.off_gs[l] = S.off_res[l] = S.off_pro[l] = -1;
+      S.cstep[l] = 0;
+    }
   slot_sync(slot);
   if (A.nitems == 1) {
-    const int Lc = min(A.lmax, kLevCache);
-    for (int l = 1; l <= Lc; ++l) {
+    int used = 0;
+    for (int l = 1; l <= A.lmax; ++l) {
       const bool loc = l <= A.local_top;
       if (loc && blockIdx.x != 0) continue;
       const int first = loc ? slot : blockIdx.x * nslots + slot, step = loc ? nslots : gridDim.x * nslots;
-      const int n = A.tr.nblk[l - 1];
-      const int nmine = (first < n) ? (n - 1 - first) / step + 1 : 0;
-      if (nmine == 0 || nmine > 2) continue;
-      for (int i = t; i < 5 * nmine; i += 256) {
-        const int q = i / 5, k = i - 5 * q;
-        S.rgs[l - 1][q][k] = A.tr.lvl_rec[l - 1][5 * (first + q * step) + k];
+      if (t == 0) S.cstep[l - 1] = step;
+      int n = A.tr.nblk[l - 1];
+      int nm = (first < n) ? (n - 1 - first) / step + 1 : 0;
+      if (nm > 0 && nm <= kChunk && used + nm <= kRecRows<T>) {
+        for (int i = t; i < 5 * nm; i += 256) {
+          const int q = i / 5, k = i - 5 * q;
+          S.rc[used + q][k] = A.tr.lvl_rec[l - 1][5 * (first + q * step) + k];
+        }
+        if (t == 0) S.off_gs[l - 1] = (signed char)used;
+        used += nm;
       }
-      if (t == 0) S.gs_cached |= 1u << l;
-    }
-    // the child edges of level l (fine at l): restriction and prolongation records
-    for (int l = 2; l <= Lc; ++l) {
-      const bool loc = l <= A.local_top;
-      if (loc && blockIdx.x != 0) continue;
-      const int first = loc ? slot : blockIdx.x * nslots + slot, step = loc ? nslots : gridDim.x * nslots;
-      const int n = A.tr.nch[l - 1];
-      const int nmine = (first < n) ? (n - 1 - first) / step + 1 : 0;
-      if (nmine == 0 || nmine > 2) continue;
-      for (int i = t; i < 6 * nmine; i += 256) {
-        const int q = i / 6, k = i - 6 * q;
-        const int4 e = A.tr.lvl_child[l - 1][first + q * step];
-        S.rres[l - 1][q][k] = k == 0 ? e : k == 1 ? A.tr.info[e.x] : A.tr.faces[4 * e.y + k - 2];
-        if (k < 5) S.rpro[l - 1][q][k] = k == 0 ? e : A.tr.faces[4 * e.x + k - 1];
+      // the child edges of level l (fine at l)
+      n = l >= 2 ? A.tr.nch[l - 1] : 0;
+      nm = (first < n) ? (n - 1 - first) / step + 1 : 0;
+      if (nm > 0 && nm <= kChunk && used + 2 * nm <= kRecRows<T>) {
+        for (int i = t; i < 6 * nm; i += 256) {
+          const int q = i / 6, k = i - 6 * q;
+          const int4 e = A.tr.lvl_child[l - 1][first + q * step];
+          S.rc[used + q][k] = k == 0 ? e : k == 1 ? A.tr.info[e.x] : A.tr.faces[4 * e.y + k - 2];
+          if (k < 5) S.rc[used + nm + q][k] = k == 0 ? e : A.tr.faces[4 * e.x + k - 1];
+        }
+        if (t == 0) {
+          S.off_res[l - 1] = (signed char)used;
+          S.off_pro[l - 1] = (signed char)(used + nm);
+        }
+        used += 2 * nm;
       }
-      if (t == 0) S.ch_cached |= 1u << l;
     }
   }
   __syncthreads();
