@@ -556,15 +556,17 @@ __device__ __forceinline__ void st_pair(T *p, T a, T b) {
 }
 
 // The order-2 stencil of applystencil (src/laplacian.jl:25-49,78-118) on values already
-// loaded: the same products and sums, in the same order, as apply5, here free to be
-// contracted into FMAs (the engine agrees with the per-operation kernels to rounding).
+// loaded: apply5's products and sums, in its order, each rounded on its own (no FMA
+// contraction), so that the engine's updates equal the per-operation kernels' and the
+// halo recompute of a neighbour's red edge cell equals the neighbour's own update bit
+// for bit.
 template <typename T>
 __device__ __forceinline__ T sten5(const W5<T> &w, T centre, T zm, T rm, T c, T rp, T zp) {
-  T v = w.zm * zm;
-  v = v + w.rm * rm;
-  v = v + centre * c;
-  v = v + w.rp * rp;
-  v = v + w.zp * zp;
+  T v = dadd<T>(T(0), dmul<T>(w.zm, zm));
+  v = dadd<T>(v, dmul<T>(w.rm, rm));
+  v = dadd<T>(v, dmul<T>(centre, c));
+  v = dadd<T>(v, dmul<T>(w.rp, rp));
+  v = dadd<T>(v, dmul<T>(w.zp, zp));
   return v;
 }
 
@@ -772,11 +774,8 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
         if (fi.x == FACE_NEIGHBOR) {
           auto at = [&](int a, int c) -> T { return (a == hc_.cx && c == hc_.cy) ? hc : tile[a + kS * c]; };
           const W5<T> wh = wrow_w<T>(A.geom, S.wst[buf], hc_.hx, hc_.hy);
-          T v = wh.zm * at(hc_.hx, hc_.hy - 1);
-          v = v + wh.rm * at(hc_.hx - 1, hc_.hy);
-          v = v + centre * tile[hc_.hx + kS * hc_.hy];
-          v = v + wh.rp * at(hc_.hx + 1, hc_.hy);
-          v = v + wh.zp * at(hc_.hx, hc_.hy + 1);
+          const T v = sten5<T>(wh, centre, at(hc_.hx, hc_.hy - 1), at(hc_.hx - 1, hc_.hy),
+                               tile[hc_.hx + kS * hc_.hy], at(hc_.hx + 1, hc_.hy), at(hc_.hx, hc_.hy + 1));
           const T bn = (fas && ((fi.z >> hc_.nsub) & 1)) ? -(hv + v / s)
                        : A.bghost                          ? S.tile2[buf][hc_.hx + kS * hc_.hy]
                                                            : hv;
