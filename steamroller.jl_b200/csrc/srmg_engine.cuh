@@ -1068,57 +1068,51 @@ __device__ void ph_bghost(const EngArgs<T> &A, int gwarp, int nwarps) {
 
 // ---- mixed-precision outer step (FP64) ---------------------------------------------
 
-// u64 += u (FP32 correction) on every valid cell of every level, with pushes of the new
-// values into the copy and mirror ghosts of u64.  A slot takes kUpd blocks of a level
-// per pass, their records, values and face records loaded before any store, so that
-// the loads of several blocks are in flight together.
+// u64 += u (the correction) on every element of every block's tile, ghosts included.
+// After a V-cycle the correction's copy and mirror ghosts hold exactly the neighbour
+// values and the mirrored values (times 1, -1 or 0) that pushes of the new values would
+// write into u64's ghosts, and u64's ghosts hold the same copies of its own values, so
+// the sums there equal the pushed ones bit for bit; refinement-boundary ghosts are
+// recomputed from the coarse level after the restriction.  A slot takes kUpd blocks per
+// pass (levels numbered across so that the work spreads over every slot), thread t < 200
+// the element pair 2t, 2t + 1 of each, every load issued before the stores.
 constexpr int kUpd = 4;
 template <typename T>
 __device__ void ph_update64(const EngArgs<T> &A, int t, int gslot, int gstep) {
-  const int x = 2 + (t & 15), y = 2 + (t >> 4), o = x + kS * y;
-  const bool ex = x <= 3 || x >= 16, ey = y <= 3 || y >= 16;
-  const int fxi = x <= 3 ? 0 : 1, fyi = y <= 3 ? 2 : 3;
+  if (t >= kSS / 2) return;
+  const int e2 = 2 * t;
   int base = 0;
   for (int l = 1; l <= A.lmax; ++l) {
     const int n = A.tr.nblk[l - 1];
     const int4 *blocks = A.tr.lvl_blocks[l - 1];
-    // items are numbered across levels so that the work spreads over every slot
     for (int i = (gslot - base % gstep + gstep) % gstep; i < n; i += kUpd * gstep) {
-      int X[kUpd];
-      unsigned sg[kUpd];
+      int64_t off[kUpd];
       bool on[kUpd];
 #pragma unroll
       for (int k = 0; k < kUpd; ++k) {
         const int ik = i + k * gstep;
         on[k] = false;
-        X[k] = 0;
-        sg[k] = 0u;
+        off[k] = 0;
         if (ik < n) {
           const int4 bk = blocks[ik];
           on[k] = !is_frozen(A, item_of(bk));
-          X[k] = bk.x;
-          if (ex || ey) sg[k] = (unsigned)A.it_sgbits[item_of(bk)];
+          off[k] = (int64_t)bk.x * kSS + e2;
         }
       }
-      double nv[kUpd];
-      int2 fx[kUpd], fy[kUpd];
+      double a0[kUpd], a1[kUpd];
+      T c0[kUpd], c1[kUpd];
 #pragma unroll
       for (int k = 0; k < kUpd; ++k) {
-        nv[k] = 0.0;
-        fx[k] = fy[k] = make_int2(FACE_NONE, -1);
+        a0[k] = a1[k] = 0.0;
+        c0[k] = c1[k] = T(0);
         if (on[k]) {
-          const int64_t a = (int64_t)X[k] * kSS + o;
-          nv[k] = A.mx.u64[a] + (double)A.u[a];
-          if (ex) fx[k] = face_tw(A.tr.faces + 4 * X[k], fxi);
-          if (ey) fy[k] = face_tw(A.tr.faces + 4 * X[k], fyi);
+          ld_pair<double>(A.mx.u64 + off[k], a0[k], a1[k]);
+          ld_pair<T>(A.u + off[k], c0[k], c1[k]);
         }
       }
 #pragma unroll
       for (int k = 0; k < kUpd; ++k)
-        if (on[k]) {
-          A.mx.u64[(int64_t)X[k] * kSS + o] = nv[k];
-          push_tw<double>(sg[k], A.mx.u64, X[k], fx[k], fy[k], x, y, nv[k]);
-        }
+        if (on[k]) st_pair<double>(A.mx.u64 + off[k], a0[k] + (double)c0[k], a1[k] + (double)c1[k]);
     }
     base += n;
   }
@@ -1245,19 +1239,26 @@ __device__ void ph_refbnd64(const EngArgs<T> &A, int l, int t, int gslot, int gs
 }
 
 // Leaf sums of squares per norm chunk (up to kNormChunk consecutive blocks of one item
-// and level) at bpart[c]: per thread over the chunk's blocks in order, the warp sums,
-// then the 8 warp sums in order.  A leaf cell of level l is weighted by 4^-(l-1); cells
-// under a child are skipped (resnorm!, src/multigrid.jl:391-417).
+// and level) at bpart[c]: the two halves of the slot take the chunk's blocks j = half,
+// half + 2, thread h of a half the cell pair (x0, y), (x0 + 1, y), x0 = 2 + 2 (h % 8),
+// y = 2 + h / 8; per thread over its blocks in order, then the warp sums, then the 8 warp
+// sums in order.  A leaf cell of level l is weighted by 4^-(l-1); cells under a child
+// are skipped (resnorm!, src/multigrid.jl:391-417).
 //   defect = false: r = -(b + L u / s_l) of the current iterate u;
 //   defect = true : the FP64 defect r = -(b64 + L u64 / s_l) of the mixed solve, also
-//                   written as the FP32 right-hand side -r, with the FP32 correction
-//                   zeroed (ghosts included).
-// with_b adds the same sums for b (b64 in mixed mode) in bpart_b.
-template <typename T>
+//                   written as the FP32 right-hand side -r (with its neighbour-copy
+//                   ghosts when b's ghosts are kept), with the FP32 correction zeroed
+//                   (ghosts included).
+// with_b adds the same sums for b (b64 in mixed mode) in bpart_b.  kPer of a half's
+// blocks have their loads in flight together (1 in the register-capped 1024-thread
+// shape, whose spills would cost more than the overlap).
+template <typename T, int kPer>
 __device__ void ph_blocknorm(const EngArgs<T> &A, bool defect, bool with_b, int t, int slot, int gslot, int gstep,
                              double *red) {
-  const int x = 2 + (t & 15), y = 2 + (t >> 4), o = x + kS * y;
-  const int mysub = ((x - 2) >> 3) + 2 * ((y - 2) >> 3);
+  const int half = t >> 7, h = t & 127;
+  const int x0 = 2 + 2 * (h & 7), y = 2 + (h >> 3), o0 = x0 + kS * y;
+  const int mysub = ((x0 - 2) >> 3) + 2 * ((y - 2) >> 3);
+  const bool edge = x0 == 2 || x0 == 16 || y <= 3 || y >= 16;
   const int lane = t & 31, w8 = t >> 5;
   int nb = 0;
   for (int c = gslot; c < A.nchunk; c += gstep) {
@@ -1267,52 +1268,78 @@ __device__ void ph_blocknorm(const EngArgs<T> &A, bool defect, bool with_b, int 
     const int l = ck.x;
     const int4 *blocks = A.tr.lvl_blocks[l - 1] + ck.y;
     const double wl = 1.0 / (double)((int64_t)1 << (2 * (l - 1)));
-    // the chunk's blocks: records first, then every block's residual (loads of all blocks
-    // in flight together: no store in between), then the stores and the sums in order
-    int4 bks[kNormChunk];
-#pragma unroll
-    for (int j = 0; j < kNormChunk; ++j) bks[j] = j < ck.z ? blocks[j] : make_int4(0, 0, 0, 0);
-    double rr[kNormChunk], bvv[kNormChunk];
-#pragma unroll
-    for (int j = 0; j < kNormChunk; ++j) {
-      rr[j] = 0.0;
-      bvv[j] = 0.0;
-      if (j >= ck.z) continue;
-      const int4 bk = bks[j];
-      const int X = bk.x;
-      if (!defect) {
-        const T *par = A.it_par + item * kParStride;
-        const W5<T> w = weights<T>(A.wt, A.geom, bk.y, bk.z, x, y);
-        const T Lu = apply5<T>(A.u + (int64_t)X * kSS, x, y, w, par[32 + l]);
-        const T bb = A.b[(int64_t)X * kSS + o];
-        rr[j] = (double)(-(bb + Lu / par[l]));
-        bvv[j] = (double)bb;
-      } else {
-        const double *par = A.mx.it_par64 + item * kParStride;
-        const W5<double> w = weights<double>(A.mx.wt64, A.geom, bk.y, bk.z, x, y);
-        const double Lu = apply5<double>(A.mx.u64 + (int64_t)X * kSS, x, y, w, par[32 + l]);
-        bvv[j] = A.mx.b64[(int64_t)X * kSS + o];
-        rr[j] = -(bvv[j] + Lu / par[l]);
-      }
-    }
+    constexpr int kMine = (kNormChunk + 1) / 2;
+    static_assert(kMine % kPer == 0, "passes of kPer blocks");
     double v = 0.0, vb = 0.0;
+#pragma unroll 1
+    for (int p0 = 0; p0 < kMine; p0 += kPer) {
+      // kPer of this half's blocks of the chunk: records first, then every block's residual
+      // pair (loads of all blocks in flight together: no store in between), then the
+      // stores and the sums in order
+      int4 bks[kPer];
 #pragma unroll
-    for (int j = 0; j < kNormChunk; ++j) {
-      if (j >= ck.z) continue;
-      const int4 bk = bks[j];
-      const int X = bk.x;
-      const double r = rr[j], bv = bvv[j];
-      if (defect) {
-        A.b[(int64_t)X * kSS + o] = (T)(-r);
-        if (A.bghost && (x <= 3 || x >= 16 || y <= 3 || y >= 16))
-          copy_ghost<T>(A.b, X, A.tr.faces + 4 * X, x, y, (T)(-r));
-        T *eb = A.u + (int64_t)X * kSS;
-        eb[t] = T(0);
-        if (t < kSS - 256) eb[t + 256] = T(0);
+      for (int q = 0; q < kPer; ++q) {
+        const int j = 2 * (p0 + q) + half;
+        bks[q] = j < ck.z ? blocks[j] : make_int4(0, 0, 0, 0);
       }
-      if (!((bk.w >> mysub) & 1)) {  // a leaf cell
-        v = fma(r, r, v);
-        vb = fma(bv, bv, vb);
+      double rr0[kPer], rr1[kPer], bb0[kPer], bb1[kPer];
+#pragma unroll
+      for (int q = 0; q < kPer; ++q) {
+        rr0[q] = rr1[q] = bb0[q] = bb1[q] = 0.0;
+        if (2 * (p0 + q) + half >= ck.z) continue;
+        const int4 bk = bks[q];
+        const int64_t xo = (int64_t)bk.x * kSS + o0;
+        if (!defect) {
+          const T *par = A.it_par + item * kParStride;
+          const T s = par[l], centre = par[32 + l];
+          const W5<T> w0 = weights<T>(A.wt, A.geom, bk.y, bk.z, x0, y);
+          const W5<T> w1 = weights<T>(A.wt, A.geom, bk.y, bk.z, x0 + 1, y);
+          T c0v, c1v, dn0, dn1, up0, up1, b0, b1;
+          ld_pair<T>(A.u + xo, c0v, c1v);
+          ld_pair<T>(A.u + xo - kS, dn0, dn1);
+          ld_pair<T>(A.u + xo + kS, up0, up1);
+          ld_pair<T>(A.b + xo, b0, b1);
+          const T Lu0 = sten5<T>(w0, centre, dn0, A.u[xo - 1], c0v, c1v, up0);
+          const T Lu1 = sten5<T>(w1, centre, dn1, c0v, c1v, A.u[xo + 2], up1);
+          rr0[q] = (double)(-(b0 + Lu0 / s));
+          rr1[q] = (double)(-(b1 + Lu1 / s));
+          bb0[q] = (double)b0;
+          bb1[q] = (double)b1;
+        } else {
+          const double *par = A.mx.it_par64 + item * kParStride;
+          const double s = par[l], centre = par[32 + l];
+          const W5<double> w0 = weights<double>(A.mx.wt64, A.geom, bk.y, bk.z, x0, y);
+          const W5<double> w1 = weights<double>(A.mx.wt64, A.geom, bk.y, bk.z, x0 + 1, y);
+          const double *ub = A.mx.u64;
+          double c0v, c1v, dn0, dn1, up0, up1;
+          ld_pair<double>(ub + xo, c0v, c1v);
+          ld_pair<double>(ub + xo - kS, dn0, dn1);
+          ld_pair<double>(ub + xo + kS, up0, up1);
+          ld_pair<double>(A.mx.b64 + xo, bb0[q], bb1[q]);
+          const double Lu0 = sten5<double>(w0, centre, dn0, ub[xo - 1], c0v, c1v, up0);
+          const double Lu1 = sten5<double>(w1, centre, dn1, c0v, c1v, ub[xo + 2], up1);
+          rr0[q] = -(bb0[q] + Lu0 / s);
+          rr1[q] = -(bb1[q] + Lu1 / s);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kPer; ++q) {
+        if (2 * (p0 + q) + half >= ck.z) continue;
+        const int4 bk = bks[q];
+        const int X = bk.x;
+        if (defect) {
+          const T v0 = (T)(-rr0[q]), v1 = (T)(-rr1[q]);
+          st_pair<T>(A.b + (int64_t)X * kSS + o0, v0, v1);
+          if (A.bghost && edge) push_pair<T, false>(0u, A.b, X, A.tr.faces + 4 * X, x0, y, v0, v1);
+          float4 *eb = reinterpret_cast<float4 *>(A.u + (int64_t)X * kSS);
+          for (int k = h; k < (int)(kSS * sizeof(T) / 16); k += 128) eb[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if (!((bk.w >> mysub) & 1)) {  // leaf cells
+          v = fma(rr0[q], rr0[q], v);
+          v = fma(rr1[q], rr1[q], v);
+          vb = fma(bb0[q], bb0[q], vb);
+          vb = fma(bb1[q], bb1[q], vb);
+        }
       }
     }
     for (int off = 16; off > 0; off >>= 1) {
@@ -1679,7 +1706,8 @@ __global__ void __launch_bounds__(NT, 1) k_engine_vcycle(const __grid_constant__
   // Norm step: per-block partials, barrier, per-item sums and freezing, barrier.
   int steps = 0;  // mixed: defect-correction steps run
   auto norm_step = [&](bool defect, bool first, int ncyc) -> bool {
-    ph_blocknorm<T>(A, defect, first, t, slot, gslot, gstep, reinterpret_cast<double *>(&S.tile[0][0]));
+    ph_blocknorm<T, NT == 1024 ? 1 : 2>(A, defect, first, t, slot, gslot, gstep,
+                                         reinterpret_cast<double *>(&S.tile[0][0]));
     if (!sync(true, false, false)) return false;
     ph_itemnorm<T>(A, first, ncyc, steps, s_direct);
     return sync(true, false, false);
