@@ -229,6 +229,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
 // larger staging area measured slower.
 constexpr int kBuf = 4;
 constexpr int kChunk = 32;
+// The thread of a slot that issues the GS, restriction and prolongation tile copies: its
+// last (warp 3 of the second half), which has neither the GS halo update (warp 1 of
+// each half) nor a share of the restriction's 2 x 2 sums (threads 0-63 of each half), so
+// that no warp carries two of those extra paths between slot barriers (config 2's mixed
+// solve: issuing from thread 0 with the halo on warp 0 cost 4-5%).
+constexpr int kIssuer = 255;
 constexpr int kWRow = 2 * kS;  // a weight row: wm, then wp, at the tile positions 0..19
 // Launch-long record cache: a single-item launch loads, once at its start and level by
 // level from the coarsest, a slot's whole share of a level's GS, restriction and
@@ -509,7 +515,7 @@ __device__ __forceinline__ HaloCell halo_cell(int t) {
   return h;
 }
 
-// Red halo cell m (0..31) of a block, handled by lane m of warp 0 of a half slot (the
+// Red halo cell m (0..31) of a block, handled by lane m of warp 1 of a half slot (the
 // cell 2 (m % 8) + (m / 8 % 2) of ghost face m / 8), packed into two ints once per CTA:
 // {hx | hy << 5 | nx << 10 | ny << 15 | f << 20 | nsub << 22, (cx + 1) | (cy + 1) << 6 |
 // (cnx + 1) << 12 | (cny + 1) << 18}, the corner fields all -1 where there is none.
@@ -653,9 +659,10 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
   const bool yodd = (y & 1) != 0;  // red (colour 0 of RedBlack{0}, updated first) is x0 if y is odd
   const int xr = yodd ? x0 : x0 + 1, xbk = yodd ? x0 + 1 : x0;  // the pair's red and black cells
   const int mysub = ((x0 - 2) >> 3) + 2 * ((y - 2) >> 3);
-  // warp 0 of a half: the 32 red halo cells, lane m taking entry m of the halo table (one
-  // warp issues the halo code instead of a quarter of every warp's lanes)
-  const bool hthr = wv == 0;
+  // warp 1 of a half: the 32 red halo cells, lane m taking entry m of the halo table (one
+  // warp issues the halo code instead of a quarter of every warp's lanes; not warp 0,
+  // whose first half holds thread 0)
+  const bool hthr = wv == 1;
   const int hm = lane;  // this lane's entry of the halo table
   // neighbour values of the halo cell, loaded one iteration ahead
   // (b comes from b's ghost layer when A.bghost, except the FAS right-hand side of a
@@ -709,7 +716,7 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
       slot_sync(slot);
       if (cn == 0) continue;
     }
-    if (t == 0)
+    if (t == kIssuer)
       for (int q = 0; q < kBuf && q < cn; ++q) issue(q);
     if (half < cn) prefetch(half);
     for (int i = 0; 2 * i < cn; ++i) {
@@ -796,7 +803,7 @@ __device__ bool ph_gsi(const EngArgs<T> &A, int l, const T *src, T *dst, const T
         return false;
       }
       // the buffers of the previous iteration are free: refill them kBuf blocks later
-      if (t == 0 && i >= 1)
+      if (t == kIssuer && i >= 1)
         for (int q = 2 * i - 2 + kBuf; q < 2 * i + kBuf && q < cn; ++q) issue(q);
       if (act) {
         T dn0, dn1, up0, up1;
@@ -881,7 +888,7 @@ __device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
       slot_sync(slot);
       if (cn == 0) continue;
     }
-    if (t == 0)
+    if (t == kIssuer)
       for (int q = 0; q < kBuf && q < cn; ++q) issue(q);
     for (int i = 0; 2 * i < cn; ++i) {
       const int j = 2 * i + half;
@@ -917,7 +924,7 @@ __device__ bool ph_restrict(const EngArgs<T> &A, int l, const T *uf, T *uc, int 
         return false;
       }
       // the buffers of the previous iteration are free: refill them kBuf blocks later
-      if (t == 0 && i >= 1)
+      if (t == kIssuer && i >= 1)
         for (int q = 2 * i - 2 + kBuf; q < 2 * i + kBuf && q < cn; ++q) issue(q);
       if (act && h < 64) {
         const int kx = h & 7, ky = h >> 3;
@@ -981,7 +988,7 @@ __device__ bool ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int f
       slot_sync(slot);
       if (cn == 0) continue;
     }
-    if (t == 0)
+    if (t == kIssuer)
       for (int q = 0; q < kBuf && q < cn; ++q) issue(q);
     for (int i = 0; 2 * i < cn; ++i) {
       const int j = 2 * i + half;
@@ -1026,7 +1033,7 @@ __device__ bool ph_prolong(const EngArgs<T> &A, int l, T *uf, const T *uc, int f
         return false;
       }
       // this iteration's buffers (and records) are free: refill them kBuf blocks later
-      if (t == 0)
+      if (t == kIssuer)
         for (int q = 2 * i + kBuf; q < 2 * i + 2 + kBuf && q < cn; ++q) issue(q);
     }
     pk += cn;
