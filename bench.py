@@ -45,12 +45,12 @@ SEED = 2
 TARGET_LEAF = 1_500_000
 METRIC = "field solves/sec at 1e-8 rel residual (mixed-precision multigrid; plain FP64 GPU alongside)"
 # DRAM bytes of one plain FP64 V-cycle launch on the config-2 tree, from an ncu capture
-# (57.03 MB read + 39.74 MB written)
-TRAFFIC_VCYCLE_CONFIG2 = 96.77e6
+# (57.52 MB read + 40.66 MB written)
+TRAFFIC_VCYCLE_CONFIG2 = 98.18e6
 # DRAM bytes of one mixed-solve launch on the config-2 tree (the tuned V(1,1) cycle,
 # 9 V-cycles in 3 defect-correction steps, the direct solve on level 2), from an ncu
-# capture (171.37 MB read + 151.77 MB written)
-TRAFFIC_MIXED_CONFIG2 = 323.15e6
+# capture (170.85 MB read + 137.01 MB written)
+TRAFFIC_MIXED_CONFIG2 = 307.87e6
 
 
 def peaks():
