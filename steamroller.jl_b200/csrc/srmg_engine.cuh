@@ -128,18 +128,24 @@ __device__ __forceinline__ long long gtimer() {
   return t;
 }
 
-// Grid-wide barrier on a monotonic counter.  A wait longer than timeout_ns sets the
-// error word and returns false; every CTA then leaves the kernel at its next check.
-__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err, unsigned &epoch,
-                                             long long timeout_ns) {
-  __shared__ int ok_s;
+// Grid-wide barrier on a monotonic counter, also usable in two halves: grid_arrive
+// counts this CTA in (its earlier memory operations, loads included, ordered before the
+// count by the release) without waiting; grid_wait waits for every CTA of the same
+// epoch.  A wait longer than timeout_ns sets the error word and returns false; every CTA
+// then leaves the kernel at its next check.
+__device__ __forceinline__ void grid_arrive(unsigned *bar, unsigned &epoch) {
   // this phase's generic-proxy stores are ordered before the next phase's bulk copies
   asm volatile("fence.proxy.async.global;" ::: "memory");
   __syncthreads();
   if (threadIdx.x == 0) {
     epoch++;
-    const unsigned target = epoch * gridDim.x;
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
+  }
+}
+__device__ __forceinline__ bool grid_wait(unsigned *bar, int *err, unsigned epoch, long long timeout_ns) {
+  __shared__ int ok_s;
+  if (threadIdx.x == 0) {
+    const unsigned target = epoch * gridDim.x;
     int ok = 1;
     const long long t0 = gtimer();
     // the error word and the clock are read every 32 polls only: each read is another
@@ -163,6 +169,11 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err, unsigned &
   __syncthreads();
   asm volatile("fence.proxy.async.global;" ::: "memory");
   return ok_s != 0;
+}
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err, unsigned &epoch,
+                                             long long timeout_ns) {
+  grid_arrive(bar, epoch);
+  return grid_wait(bar, err, epoch, timeout_ns);
 }
 
 __device__ __forceinline__ void slot_sync(int slot) {
@@ -1568,6 +1579,45 @@ __device__ void ph_direct2_rows(const EngArgs<T> &A, T *u, int lt, bool make_e, 
   }
 }
 
+// ph_direct2_rows around a split barrier, for grids whose CTAs hold at most one row per
+// warp: the CTA counts itself in once its right-hand side reads of level 2 are done,
+// forms its rows' products (the same sums in the same order) while the other CTAs
+// arrive, and writes them after the wait, so that the products overlap the barrier
+// instead of following it.
+template <typename T>
+__device__ bool ph_direct2_rows_split(const EngArgs<T> &A, T *u, int lt, bool make_e, const double *rhs,
+                                      const double *uold, unsigned &epoch) {
+  const int2 rg = A.it_lrange[lt - 1];
+  const int n = 256 * rg.y;
+  const int4 *blocks = A.tr.lvl_blocks[lt - 1] + rg.x;
+  const double *P = A.it_P[0];
+  const int rpc = (n + gridDim.x - 1) / gridDim.x, r0 = blockIdx.x * rpc, r1 = min(n, r0 + rpc);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = r0 + warp;
+  grid_arrive(A.bar, epoch);
+  double acc = 0.0;
+  if (q < r1) {
+    const double *pr = P + (int64_t)q * n;
+    for (int j = lane; j < n; j += 32) acc = fma(pr[j], rhs[j], acc);
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  }
+  if (!grid_wait(A.bar, A.err, epoch, A.timeout_ns)) return false;
+  if (q < r1 && lane == 0) {
+    const int c = q & 255, x = 2 + (c & 15), y = 2 + (c >> 4);
+    const int X = blocks[q >> 8].x;
+    const int4 *fc = A.tr.faces + 4 * X;
+    const T nu = (T)acc;
+    u[(int64_t)X * kSS + x + kS * y] = nu;
+    push<T>(A, 0, u, X, fc, x, y, nu);
+    if (make_e) {
+      const T ev = nu - (T)uold[q - r0];
+      A.e[(int64_t)X * kSS + x + kS * y] = ev;
+      push<T>(A, 0, A.e, X, fc, x, y, ev);
+    }
+  }
+  return true;
+}
+
 // Copy level l's blocks (valid cells and face ghosts) from src to dst.
 template <typename T>
 __device__ void ph_copy_back(const EngArgs<T> &A, int l, const T *src, T *dst, int first, int step, int t) {
@@ -1793,8 +1843,14 @@ __global__ void __launch_bounds__(NT, 1) k_engine_vcycle(const __grid_constant__
     if (A.it_P && lt == 2) {
       // a lone item's direct solve on level 2, grid-wide (never CTA-local: local_top = 0)
       ph_direct2_rhs<T>(A, fld(2), 2, s_rhs, s_direct);
-      if (!sync(true, false, false)) return false;
-      ph_direct2_rows<T>(A, fld(2), 2, L > 2, s_rhs, s_direct);
+      const int n2 = 256 * A.it_lrange[1].y;
+      if ((n2 + (int)gridDim.x - 1) / (int)gridDim.x <= (int)(blockDim.x >> 5)) {
+        if (!ph_direct2_rows_split<T>(A, fld(2), 2, L > 2, s_rhs, s_direct, epoch)) return false;
+        stamp();
+      } else {
+        if (!sync(true, false, false)) return false;
+        ph_direct2_rows<T>(A, fld(2), 2, L > 2, s_rhs, s_direct);
+      }
       if (!sync(true, false, false)) return false;
     } else if (A.it_P) {
       const bool loc = 1 <= K;
