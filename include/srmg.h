@@ -219,6 +219,25 @@ int srmg_solve(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc,
                double s, int op, double k2, int geom, const int8_t bc[9],
                const srmg_solve_opts *opts, srmg_stats *stats);
 
+/* srmg_solve in two calls.  No counterpart in the reference, whose solves are
+ * synchronous calls on host arrays: it exists for callers with several independent
+ * problems, whose host-to-device and device-to-host copies (the bulk of a host-array
+ * solve's time on the PCIe link) can overlap another problem's solve.
+ * srmg_solve_async enqueues on the context's stream the copies of u and b in, the
+ * solve, and the copy of u out, and returns without waiting; srmg_solve_wait(ctx,
+ * stats) waits for them, fills stats (device_ms spans the copies and the solve) and
+ * returns what srmg_solve would have returned.  u and b must stay valid and untouched
+ * until the wait, and should be page-locked (srmg_host_register, or pinned memory) for
+ * the copies to run asynchronously.  Between the two calls the context takes no other
+ * call (SRMG_ERR_BADARG); two contexts holding the same tree give two solves in flight,
+ * whose kernels run one after the other while their copies overlap.  Single 2D trees
+ * on the persistent engine only (SRMG_ERR_UNSUPPORTED otherwise: use srmg_solve), no
+ * learned warm start.  Results equal srmg_solve's bit for bit. */
+int srmg_solve_async(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc,
+                     double s, int op, double k2, int geom, const int8_t bc[9],
+                     const srmg_solve_opts *opts);
+int srmg_solve_wait(srmg_ctx *ctx, srmg_stats *stats);
+
 /* ---- DEVICE pointers (fields already resident in HBM) --------------------------- */
 /* Same semantics as the host entry points; pointers are device addresses of
  * nblk_alloc-block fields; work is ordered on the context's stream and these calls

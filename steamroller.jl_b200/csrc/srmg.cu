@@ -174,6 +174,8 @@ extern "C" const char *srmg_last_error(const srmg_ctx *ctx) {
 
 extern "C" int srmg_set_stream(srmg_ctx *ctx, void *s) {
   if (!ctx) return SRMG_ERR_BADARG;
+  if (ctx->async_pending)
+    return fail(ctx, SRMG_ERR_BADARG, "an asynchronous solve is in flight on this context: call srmg_solve_wait first");
   ctx->stream = s ? (cudaStream_t)s : ctx->own_stream;
   return SRMG_OK;
 }
@@ -582,6 +584,8 @@ extern "C" int srmg_set_tree(srmg_ctx *ctx, int nlev, const int64_t *npairs,
                              const srmg_boundary *const *bd, const int64_t *nrb,
                              const srmg_refbnd *const *rb, const int64_t *nch,
                              const srmg_child *const *ch, uint64_t generation) {
+  if (ctx && ctx->async_pending)
+    return fail(ctx, SRMG_ERR_BADARG, "an asynchronous solve is in flight on this context: call srmg_solve_wait first");
   RC(build_tree(ctx, nlev, npairs, pairs, nnb, nb, nbd, bd, nrb, rb, nch, ch, generation, nullptr, 1));
   // keep the arrays for forests built from this tree
   HostTree &h = ctx->htree;
@@ -617,6 +621,8 @@ int srmg::check_call(srmg_ctx *ctx, int64_t nblk_alloc, int op, int geom, const 
 
 int srmg::check_call_any(srmg_ctx *ctx, int64_t nblk_alloc, int op, int geom, const int8_t *bc) {
   if (!ctx) return SRMG_ERR_BADARG;
+  if (ctx->async_pending)
+    return fail(ctx, SRMG_ERR_BADARG, "an asynchronous solve is in flight on this context: call srmg_solve_wait first");
   if (!ctx->has_tree) return fail(ctx, SRMG_ERR_NOTREE, "no tree: call srmg_set_tree first");
   if (nblk_alloc < ctx->max_blk)
     return fail(ctx, SRMG_ERR_BADARG, "field holds %lld blocks but the tree uses block %lld",
@@ -993,6 +999,8 @@ int srmg::read_small(srmg_ctx *ctx, int n) {
 
 extern "C" int srmg_set_option(srmg_ctx *ctx, const char *key, int64_t value) {
   if (!ctx || !key) return SRMG_ERR_BADARG;
+  if (ctx->async_pending)
+    return fail(ctx, SRMG_ERR_BADARG, "an asynchronous solve is in flight on this context: call srmg_solve_wait first");
   if (!strcmp(key, "engine")) ctx->use_engine = value != 0;
   else if (!strcmp(key, "trace")) ctx->trace_on = value != 0;
   else if (!strcmp(key, "b_copy_back")) ctx->b_copy_back = value != 0;

@@ -614,6 +614,8 @@ extern "C" int srmg_set_tree3(srmg_ctx *ctx, int nlev, const int64_t *npairs, co
                               const int64_t *nnb, const srmg_neighbor3 *const *nb, const int64_t *nbd,
                               const srmg_boundary3 *const *bd, const int64_t *nrb, const srmg_refbnd3 *const *rb,
                               const int64_t *nch, const srmg_child3 *const *ch, uint64_t generation) {
+  if (ctx && ctx->async_pending)
+    return fail(ctx, SRMG_ERR_BADARG, "an asynchronous solve is in flight on this context: call srmg_solve_wait first");
   if (!ctx) return SRMG_ERR_BADARG;
   if (ctx->D != 3) return fail(ctx, SRMG_ERR_BADARG, "srmg_set_tree3 needs a context created with D = 3");
   if (nlev < 1 || nlev > 20 || !npairs || !pairs || !nnb || !nb || !nbd || !bd || !nrb || !rb || !nch || !ch)

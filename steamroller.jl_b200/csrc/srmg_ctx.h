@@ -196,6 +196,7 @@ struct srmg_ctx {
   // are never written, and non-leaf b is unspecified after a V-cycle), and the host
   // ranges page-locked through srmg_host_register {address, bytes}
   bool b_copy_back = false;
+  bool async_pending = false;  // srmg_solve_async enqueued a solve that srmg_solve_wait has not finished
   std::vector<std::pair<void *, size_t>> host_reg;
 
   // coarsest-level direct inverses, by operator and level-1 structure

@@ -461,3 +461,60 @@ extern "C" int srmg_solve(srmg_ctx *ctx, double *u, const double *b, int64_t nbl
   CK(cudaStreamSynchronize(ctx->stream));
   return SRMG_OK;
 }
+
+// ---- asynchronous host-array solve ----------------------------------------------------
+// srmg_solve split at its host synchronisation: the copies of u and b in, the persistent
+// solve, the copy of u out and the read-back of the solve's record are enqueued on the
+// context's stream, and srmg_solve_wait finishes them.  A caller with several
+// independent problems alternates two contexts on the same tree, so that one problem's
+// copies overlap the other's solve.
+extern "C" int srmg_solve_async(srmg_ctx *ctx, double *u, const double *b, int64_t nblk_alloc, double s, int op,
+                                double k2, int geom, const int8_t bc[9], const srmg_solve_opts *opts) {
+  RC(check_call_any(ctx, nblk_alloc, op, geom, bc));
+  if (!u || !b) return fail(ctx, SRMG_ERR_BADARG, "srmg_solve_async: null field");
+  if (ctx->D != 2 || ctx->nitems != 1)
+    return fail(ctx, SRMG_ERR_UNSUPPORTED, "srmg_solve_async: single two-dimensional trees only; use srmg_solve");
+  srmg_solve_opts o;
+  if (opts) o = *opts; else srmg_solve_opts_default(&o);
+  if (!(o.tol > 0) || o.max_cycles < 0 || o.ndown < 0 || o.nup < 0 || o.ntop < 0)
+    return fail(ctx, SRMG_ERR_BADARG, "srmg_solve_async: bad options");
+  if (o.mode != SRMG_MODE_FP64 && o.mode != SRMG_MODE_MIXED && o.mode != SRMG_MODE_FP64_DIRECT)
+    return fail(ctx, SRMG_ERR_BADARG, "unknown solve mode %d", o.mode);
+  if (o.warm_start) return fail(ctx, SRMG_ERR_UNSUPPORTED, "srmg_solve_async: no learned warm start; use srmg_solve");
+  const std::vector<ItemSpec> specs = uniform_items(ctx, s, op, k2, bc);
+  if (o.mode != SRMG_MODE_FP64 && specs[0].op == SRMG_OP_LAPLACIAN4)
+    return fail(ctx, SRMG_ERR_UNSUPPORTED, "mixed and direct modes support order-2 discretisations");
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  double *du, *db;
+  RC(stage_in(ctx, 0, u, nblk_alloc, &du));
+  RC(stage_in(ctx, 1, b, nblk_alloc, &db));
+  RC(solve_reserve(ctx, nblk_alloc, o.mode));
+  if (!engine_ok(ctx, &o, {du, db}))
+    return fail(ctx, SRMG_ERR_UNSUPPORTED, "srmg_solve_async needs the persistent engine; use srmg_solve");
+  ItemTabs tabs;
+  RC(prepare_items(ctx, specs.data(), geom, o.omega, o.mode != SRMG_MODE_FP64, 0, 0.0, &tabs, direct_top(ctx)));
+  RC(solve_enqueue(ctx, du, db, nblk_alloc, tabs, geom, &o));
+  RC(items_host_reserve(ctx));
+  RC(items_d2h(ctx));
+  RC(stage_out(ctx, u, du, nblk_alloc));
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  ctx->async_pending = true;
+  return SRMG_OK;
+}
+
+extern "C" int srmg_solve_wait(srmg_ctx *ctx, srmg_stats *stats) {
+  if (!ctx) return SRMG_ERR_BADARG;
+  if (!ctx->async_pending) return fail(ctx, SRMG_ERR_BADARG, "srmg_solve_wait: no asynchronous solve in flight");
+  ctx->async_pending = false;
+  CK(cudaEventSynchronize(ctx->ev1));
+  RC(engine_check(ctx));
+  srmg_stats st;
+  memset(&st, 0, sizeof st);
+  item_stats(ctx, 0, &st);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  st.device_ms = ms;
+  if (stats) *stats = st;
+  if (st.status) return fail(ctx, st.status, "residual is not finite after %d cycles", st.cycles);
+  return SRMG_OK;
+}

@@ -105,6 +105,8 @@ SIGNATURES = {
     "srmg_resnorm_dev": (_I, [_P, _P, _P, _P, _I64, _D, _I, _D, _I, _P, ctypes.POINTER(_D)]),
     "srmg_solve_dev": (_I, [_P, _P, _P, _I64, _D, _I, _D, _I, _P, ctypes.POINTER(SolveOpts),
                             ctypes.POINTER(Stats)]),
+    "srmg_solve_async": (_I, [_P, _P, _P, _I64, _D, _I, _D, _I, _P, ctypes.POINTER(SolveOpts)]),
+    "srmg_solve_wait": (_I, [_P, ctypes.POINTER(Stats)]),
     "srmg_fill_ghost_dev": (_I, [_P, _P, _I64, _I, _P, _I]),
     "srmg_gs_level_dev": (_I, [_P, _P, _P, _I64, _I, _D, _D, _I, _D, _I, _I]),
     "srmg_gs_iter_dev": (_I, [_P, _P, _P, _I64, _I, _D, _D, _I, _I, _D, _I, _P]),
@@ -432,6 +434,26 @@ def solve(ctx: Context, u, b, s, geometry, bc, lpldisc=None, tol=1e-8, mode=MODE
     rc = f(ctx.handle, _ptr(u), _ptr(b), u.shape[0], s, op, k2, geometry, bca.ctypes.data,
            ctypes.byref(o), ctypes.byref(st))
     ctx.check(rc)
+    return st.as_dict()
+
+
+def solve_async(ctx: Context, u, b, s, geometry, bc, lpldisc=None, tol=1e-8, mode=MODE_FP64,
+                max_cycles=1000, ndown=2, ntop=4, nup=2, omega=1.0, inner_cycles=2):
+    """srmg_solve_async on host arrays (numpy, page-locked for overlap): enqueues the
+    copies in, the solve and the copy out on the context's stream and returns at once.
+    u and b must stay alive and untouched until solve_wait(ctx)."""
+    assert isinstance(u, np.ndarray) and isinstance(b, np.ndarray)
+    op, k2 = _disc(lpldisc)
+    bca = _bc(bc)
+    o = SolveOpts(tol, max_cycles, mode, ndown, ntop, nup, omega, inner_cycles, 0)
+    ctx.check(lib().srmg_solve_async(ctx.handle, _ptr(u), _ptr(b), u.shape[0], s, op, k2, geometry,
+                                     bca.ctypes.data, ctypes.byref(o)))
+
+
+def solve_wait(ctx: Context):
+    """Waits for the context's srmg_solve_async; returns its stats dict."""
+    st = Stats()
+    ctx.check(lib().srmg_solve_wait(ctx.handle, ctypes.byref(st)))
     return st.as_dict()
 
 
