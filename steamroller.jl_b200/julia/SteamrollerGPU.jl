@@ -247,6 +247,44 @@ function solve!(u::GPUField, b::GPUField, s, tree, conn, geometry::GPUGeom,
     (st[2], st[4])
 end
 
+"""
+    solve_async!(u, b, s, tree, conn, geometry, bc, lpldisc; tol=1e-8, mixed=true)
+    solve_wait!() -> (cycles, relative residual)
+
+`solve!` in two calls: `solve_async!` enqueues the copies of `u` and `b`, the solve and
+the copy of `u` back and returns at once, so that Julia code can run meanwhile;
+`solve_wait!` waits for them.  `u` and `b` must stay untouched until the wait, and the
+context takes no other call in between.  Not used by `run_from_input`.
+"""
+function solve_async!(u::GPUField, b::GPUField, s, tree, conn, geometry::GPUGeom,
+                      bc::GeneralHomogeneousBoundaryConditions{2}, lpldisc::GPUDisc;
+                      tol=1e-8, mixed=true, max_cycles=1000, ndown=2, ntop=4, nup=2, ω=1.0)
+    upload!(tree, conn)
+    op, k2 = opcode(lpldisc)
+    a = Ref(bc.a)
+    opts = Ref((Float64(tol), Cint(max_cycles), Cint(mixed ? 1 : 0), Cint(ndown), Cint(ntop), Cint(nup),
+                Float64(ω), Cint(2), Cint(0)))
+    GC.@preserve u b a opts begin
+        check(ccall((:srmg_solve_async, libsrmg), Cint,
+                    (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int64, Float64, Cint, Float64, Cint,
+                     Ptr{Int8}, Ptr{Cvoid}),
+                    context(), pointer(u.u), pointer(b.u), size(u.u, 3), Float64(s), op, k2,
+                    geomcode(geometry), Base.unsafe_convert(Ptr{Int8}, a),
+                    Base.unsafe_convert(Ptr{Cvoid}, opts)))
+    end
+    nothing
+end
+
+function solve_wait!()
+    stats = Ref((Cint(0), Cint(0), Cint(0), 0.0, 0.0, 0.0, 0.0))
+    GC.@preserve stats begin
+        check(ccall((:srmg_solve_wait, libsrmg), Cint, (Ptr{Cvoid}, Ptr{Cvoid}),
+                    context(), Base.unsafe_convert(Ptr{Cvoid}, stats)))
+    end
+    st = stats[]
+    (st[2], st[4])
+end
+
 # ---- three-dimensional trees: a second context created with D = 3 ----------------------
 
 mutable struct State3
