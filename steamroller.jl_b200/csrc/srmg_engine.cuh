@@ -5,15 +5,16 @@
 //   GS iteration     : one full red-black Gauss-Seidel iteration (red sweep, copy and
 //                      mirror ghost fills, black sweep, fills; src/multigrid.jl:250-265)
 //                      in ONE phase.  The iteration reads the level's current buffer and
-//                      writes the other one (ping-pong per level).  Each CTA stages its
+//                      writes the other one (ping-pong per level).  A half slot stages its
 //                      block with ghosts in shared memory, updates the red cells, then
 //                      recomputes the red update of every neighbour edge cell its black
 //                      cells will read (their stencils touch only black cells and stored
-//                      ghosts of the old buffer, so the values are bit-identical to the
-//                      neighbour's own), updates the black cells, and writes the block
-//                      plus the ghost values it feeds: the facing ghosts of its
-//                      neighbours (fill_ghost_copy!), its mirror ghosts (fill_ghost_bnd!)
-//                      and its frozen refinement ghosts.  No two CTAs write one address.
+//                      ghosts of the old buffer, and every product and sum is rounded as
+//                      in the neighbour's own update, so the values are bit-identical),
+//                      updates the black cells, and writes the block plus the ghost
+//                      values it feeds: the facing ghosts of its neighbours
+//                      (fill_ghost_copy!), its mirror ghosts (fill_ghost_bnd!) and its
+//                      frozen refinement ghosts.  No two slots write one address.
 //   restrict         : per fine block: residual (src/multigrid.jl:309-323) and the
 //                      restriction of r and u to the parent's subblock
 //                      (src/restrict.jl:5-25, same summation order), with pushes of the
@@ -28,8 +29,10 @@
 // The coarse correction e = u - u1 of a level (diffto!, src/blockfield.jl:569-576) and
 // its ghosts are produced in that level's last GS iteration.  Levels 1..local_top are
 // processed by CTA 0 alone with CTA barriers.  Block tiles reach shared memory through
-// bulk asynchronous copies (cp.async.bulk, no multicast) into a triple-buffered
-// per-slot pipeline; every wait on an mbarrier or a barrier is bounded in time.
+// bulk asynchronous copies (cp.async.bulk, no multicast) into a four-buffer per-slot
+// pipeline; every wait on an mbarrier or a barrier is bounded in time.  The arithmetic
+// of every phase is the per-operation kernels' (the same products and sums, rounded the
+// same way, in the same order), so an FP64 V-cycle equals the oracle's bit for bit.
 //
 // One launch can carry several independent problems ("items"): the trees of a forest,
 // each with its own operator (Poisson or Helmholtz k^2, scale s, boundary table).  The
