@@ -190,6 +190,63 @@ __device__ __forceinline__ void d3_gs_rb(double *__restrict__ u, const double *_
   }
 }
 
+// d3_gs_rb on a StarStencil{3} tree, also writing the face ghosts that copy or mirror
+// each updated cell -- the neighbour's facing ghost (fill_ghost_copy!) and the block's own
+// mirror ghost with its sign (fill_ghost_bnd!), the operations of d3_fill's passes 1 and 2
+// -- so that no fill launch follows the sweep.  The sweep reads only cells and ghosts of
+// the other colour, and each ghost it writes copies a cell of its own colour or mirrors
+// an unchanged cell of the other colour, so no thread reads a value another one writes.
+__device__ __forceinline__ void d3_gs_rb_push(double *__restrict__ u, const double *__restrict__ b, Level3View L,
+                                              Op3 p, int parity, const Signs27 &sg) {
+  const int64_t total = (int64_t)L.nblk * (kM * kM * kM / 2);
+  const double nwc = -(p.omega / p.diag);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t / 2048), c = (int)(t % 2048);
+    const int z = kG + c / 128, y = kG + (c / 8) % 16, k = c % 8;
+    const int pp = parity ^ ((y + 1) & 1) ^ ((z + 1) & 1);
+    const int x = kG + 2 * k + pp;
+    const int64_t base = (int64_t)L.blocks[bi].x * S3;
+    const int o = o3(x, y, z);
+    const double Lu = lhs3(u + base, o, p.op, p.centre);
+    const double v = fma(p.s, b[base + o], Lu);
+    const double nu = fma(nwc, v, u[base + o]);
+    u[base + o] = nu;
+    const int q[3] = {x, y, z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int f = q[d] < kG + 2 ? -1 : q[d] >= kG + kM - 2 ? 1 : 0;
+      if (!f) continue;
+      const int4 fi = L.faces[27 * bi + 13 + f * (d == 0 ? 1 : d == 1 ? 3 : 9)];
+      int g[3] = {x, y, z};
+      if (fi.x == FACE_NEIGHBOR) {
+        g[d] -= kM * f;  // the neighbour's facing ghost
+        u[(int64_t)fi.y * S3 + o3(g[0], g[1], g[2])] = nu;
+      } else if (fi.x == FACE_BOUNDARY) {
+        const int b1 = unpack(fi.z, 0), b2 = unpack(fi.z, 1), b3 = unpack(fi.z, 2);
+        const int bb[3] = {b1, b2, b3};
+        const double sgn = sg.v[(1 + b1) + 3 * (1 + b2) + 9 * (1 + b3)];
+        auto mirror = [&](int *m) {
+#pragma unroll
+          for (int e = 0; e < 3; ++e)
+            if (bb[e]) m[e] = bb[e] < 0 ? 2 * kG - 1 - m[e] : 2 * (kG + kM) - 1 - m[e];
+        };
+        mirror(g);
+        u[base + o3(g[0], g[1], g[2])] = __dmul_rn(sgn, nu);
+        // one layer in from the face: also the first-layer mirror of the other colour's
+        // edge cell beside this one (unchanged by this sweep), which that cell's own
+        // sweep reads next -- the value the fill after this sweep would give it
+        if (q[d] == (f < 0 ? kG + 1 : kG + kM - 2)) {
+          int m[3] = {x, y, z};
+          m[d] += f;
+          const double w = u[base + o3(m[0], m[1], m[2])];
+          mirror(m);
+          u[base + o3(m[0], m[1], m[2])] = __dmul_rn(sgn, w);
+        }
+      }
+    }
+  }
+}
+
 // FourColors{P1,P2} (src/multigrid.jl:206-232) for D = 3: cells (x + p1, y + p2, z) on
 // the even grid of the first two dimensions, p_a = (P_a + z + 1) mod 2 (1-based z);
 // u -= omega (Lu + s b) / c, unfused.
@@ -287,6 +344,10 @@ __device__ __forceinline__ void d3_copy(double *__restrict__ dst, const double *
 // The per-operation kernels: each one body, launched alone or run by the sequencer.
 __global__ void k3_fill(double *__restrict__ u, Level3View L, Signs27 sg, int phase) { d3_fill(u, L, sg, phase); }
 __global__ void k3_gs_rb(double *__restrict__ u, const double *__restrict__ b, Level3View L, Op3 p, int parity) { d3_gs_rb(u, b, L, p, parity); }
+__global__ void k3_gs_rb_push(double *__restrict__ u, const double *__restrict__ b, Level3View L, Op3 p, int parity,
+                              Signs27 sg) {
+  d3_gs_rb_push(u, b, L, p, parity, sg);
+}
 __global__ void k3_gs4(double *__restrict__ u, const double *__restrict__ b, Level3View L, Op3 p, int P1, int P2) { d3_gs4(u, b, L, p, P1, P2); }
 __global__ void k3_residual(double *__restrict__ r, const double *__restrict__ u, const double *__restrict__ b,
                             Level3View L, Op3 p) { d3_residual(r, u, b, L, p); }
@@ -302,7 +363,7 @@ __global__ void k3_copy(double *__restrict__ dst, const double *__restrict__ a1,
 // barrier (release/acquire on a counter, bounded wait) separates consecutive records,
 // so every operation sees its predecessors' writes as a separate launch would, and the
 // results are those of the launches.
-enum Seq3Kind { S3_FILL = 1, S3_GS_RB, S3_GS4, S3_RESIDUAL, S3_POSTRESTRICT, S3_RESTRICT, S3_INTERP_ADD, S3_COPY };
+enum Seq3Kind { S3_FILL = 1, S3_GS_RB, S3_GS4, S3_RESIDUAL, S3_POSTRESTRICT, S3_RESTRICT, S3_INTERP_ADD, S3_COPY, S3_GS_RB_PUSH };
 struct SeqOp3 {
   int kind, i0, i1, pad;
   double *a;
@@ -324,6 +385,7 @@ __global__ void __launch_bounds__(kSeq3Threads, kSeq3PerSM)
     switch (op.kind) {
       case S3_FILL: d3_fill(op.a, op.lv, op.sg, op.i0); break;
       case S3_GS_RB: d3_gs_rb(op.a, op.b, op.lv, op.p, op.i0); break;
+      case S3_GS_RB_PUSH: d3_gs_rb_push(op.a, op.b, op.lv, op.p, op.i0, op.sg); break;
       case S3_GS4: d3_gs4(op.a, op.b, op.lv, op.p, op.i0, op.i1); break;
       case S3_RESIDUAL: d3_residual(op.a, op.b, op.c, op.lv, op.p); break;
       case S3_POSTRESTRICT: d3_postrestrict(op.a, op.b, op.c, op.lv, op.p); break;
@@ -480,11 +542,20 @@ int gs_colour(srmg_ctx *ctx, double *u, const double *b, int l, const Op3 &p, in
 }
 
 // gauss_seidel_iter! (src/multigrid.jl:250-295): each colour followed by copy and
-// boundary ghosts
+// boundary ghosts -- on StarStencil{3} trees at order 2 written by the sweep itself
+// (d3_gs_rb_push), one launch a colour instead of two
 int gs_iter(srmg_ctx *ctx, double *u, const double *b, int l, const Op3 &p, int n, const Signs27 &sg) {
   const int ncol = p.op == SRMG_OP_LAPLACIAN4 ? 4 : 2;
+  const bool push = !ctx->has_corners && p.op != SRMG_OP_LAPLACIAN4;
+  const int nb = ctx->nblk_host[l - 1];
   for (int i = 0; i < n; ++i)
     for (int c = 0; c < ncol; ++c) {
+      if (push) {
+        if (!nb || seq3_push(ctx, S3_GS_RB_PUSH, c, 0, u, b, nullptr, view(ctx, l), &p, &sg)) continue;
+        k3_gs_rb_push<<<grid3((int64_t)nb * 2048, 256), 256, 0, ctx->stream>>>(u, b, view(ctx, l), p, c, sg);
+        ctx->launches++;
+        continue;
+      }
       RC(gs_colour(ctx, u, b, l, p, c));
       RC(fill(ctx, u, l, sg, 3));
     }
