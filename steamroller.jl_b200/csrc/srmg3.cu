@@ -541,12 +541,15 @@ int gs_colour(srmg_ctx *ctx, double *u, const double *b, int l, const Op3 &p, in
   return SRMG_OK;
 }
 
+// Whether gs_iter's sweeps write their own copy and mirror ghosts (d3_gs_rb_push).
+bool gs_pushes(const srmg_ctx *ctx, const Op3 &p) { return !ctx->has_corners && p.op != SRMG_OP_LAPLACIAN4; }
+
 // gauss_seidel_iter! (src/multigrid.jl:250-295): each colour followed by copy and
 // boundary ghosts -- on StarStencil{3} trees at order 2 written by the sweep itself
 // (d3_gs_rb_push), one launch a colour instead of two
 int gs_iter(srmg_ctx *ctx, double *u, const double *b, int l, const Op3 &p, int n, const Signs27 &sg) {
   const int ncol = p.op == SRMG_OP_LAPLACIAN4 ? 4 : 2;
-  const bool push = !ctx->has_corners && p.op != SRMG_OP_LAPLACIAN4;
+  const bool push = gs_pushes(ctx, p);
   const int nb = ctx->nblk_host[l - 1];
   for (int i = 0; i < n; ++i)
     for (int c = 0; c < ncol; ++c) {
@@ -631,7 +634,10 @@ int vcycle(srmg_ctx *ctx, double *u, double *b, double *r, double *u1, double s,
     RC(interp_add(ctx, u, u1, l));
     RC(fill(ctx, u, l, sg, 7));
     RC(gs_iter(ctx, u, b, l, p, nup, sg));
-    RC(fill(ctx, u, l, sg, 7));
+    // after sweeps that write their own copy and mirror ghosts this fill would change
+    // nothing: those ghosts are current, and the refinement ghosts interpolate level
+    // l - 1, which has not changed since the fill above
+    if (!gs_pushes(ctx, p)) RC(fill(ctx, u, l, sg, 7));
   }
   return SRMG_OK;
 }
