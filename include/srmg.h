@@ -366,7 +366,7 @@ int srmg_selftest_barrier_timeout(srmg_ctx *ctx, int timeout_ms);
  * on the GPU (several streams or contexts at once) race on it.  The first call on each
  * device looks up the array's device address and keeps it for the life of the process
  * (the device's primary context must outlive the calls: no use after a
- * cudaDeviceReset); make that first call before any stream capture begins. */
+ * cudaDeviceReset). */
 int srmg_resnorm_noalloc(srmg_ctx *ctx, const double *b, const double *u, int64_t nblk_alloc,
                          double s, int op, double k2, int geom, double *out);
 
