@@ -320,7 +320,9 @@ def main():
     nleaf = leaf_cells(problem.tree)
     cfg = {"workload": "config2: refined channel tree, Poisson, cylindrical r-z, tol 1e-8",
            "leaf_cells": nleaf, "blocks": problem.tree.nblocks(), "levels": problem.tree.finest_level(),
-           "block": "16x16 + 2 ghosts", "tol": TOL, "vcycle": "(ndown,nup,ntop)=(2,2,4)",
+           "block": "16x16 + 2 ghosts", "tol": TOL,
+           "vcycle": "(ndown,nup,ntop)=(2,2,4), omega 1 for the plain FP64 leg and the reference arm; "
+                     "the mixed and FP64 + direct legs use 'tuned'",
            "parallelism": f"replicas x{world}", "l2": "flushed between timed steps (256 MB write)"}
 
     if args.impl == "reference":
