@@ -574,6 +574,12 @@ int srmg_ssprk3_stage_dev(srmg_ctx *ctx, double *out, const double *n, const dou
  *                      one cooperative launch that walks the recorded operations with
  *                      a grid barrier between consecutive ones (bit-identical results);
  *                      0 (default: graph replay measured faster on 2D and 3D trees);
+ *   "gs_push"          1 (default) = on 2D trees off the persistent engine, every colour
+ *                      sweep of gauss_seidel_iter! after its first writes the copy and
+ *                      boundary ghosts of the cells it updates, instead of a fill launch
+ *                      after it (bit-identical results; tables built once per tree from
+ *                      the fill itself, trees whose fill the tables cannot express keep
+ *                      the fill launches); 0 = a fill launch after every colour;
  *   "direct_level"     the level of the FP64 direct coarsest solve of mixed and
  *                      SRMG_MODE_FP64_DIRECT solves on the persistent kernel: 0 (default)
  *                      = level 2 for a lone tree whose level 2 holds 1..4 blocks and has no

@@ -103,6 +103,10 @@ void srmg::free_tree(srmg_ctx *ctx) {
   ctx->nch_host.clear();
   ctx->has_tree = false;
   ctx->fbc_built = false;
+  if (ctx->push_tab.p) cudaFree(ctx->push_tab.p);
+  ctx->push_tab = DevBuf{};
+  ctx->push_lv.clear();
+  ctx->push_state = 0;
 }
 
 extern "C" void srmg_destroy(srmg_ctx *ctx) {
@@ -751,6 +755,164 @@ int srmg::L_fill_ghost(srmg_ctx *ctx, T *u, int l, const Signs &sg, int mask) {
   return SRMG_OK;
 }
 
+// ------------------------------------------------------------------ Gauss-Seidel ghost pushes
+
+// The push tables come from the fill itself.  The copy-and-boundary fill (mask 3) of
+// every level runs twice on an identity field (each valid cell holds its index in the
+// field + 1, each ghost 0): once with every boundary-table entry 1, once with entry k
+// the k-th prime.  A ghost left 0 by the first run takes no valid cell's value (it
+// mirrors a refinement ghost, or no pass writes it) and is never pushed; any other ghost
+// names its source cell, and the ratio of the two runs names the boundary-table entries
+// of the mirrors between them (at most two: a corner's and a face's).  A table is used
+// only where pushing cannot race the sweep: no cell of the source's colour other than
+// the source itself reads the ghost (the 5-point stencil for the red-black sweep, the
+// 9-point one for the four-colour sweep).  Anything else -- a ghost that is not a signed
+// copy of one valid cell of its own level -- leaves the tree on the fill launches.
+// Identity field for building the push tables: every valid cell holds its own index in
+// the field + 1 (exact in a double), every ghost 0; `copies` consecutive fields.
+static __global__ void k_push_ident(double *__restrict__ a, int64_t n, int copies) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % kSS), x = c % kS, y = c / kS;
+    const bool valid = x >= kG && x < kG + kM && y >= kG && y < kG + kM;
+    for (int k = 0; k < copies; ++k) a[k * n + i] = valid ? (double)(i + 1) : 0.0;
+  }
+}
+
+int srmg::ensure_gs_push(srmg_ctx *ctx) {
+  if (ctx->push_state != 0 || !ctx->use_gs_push || !ctx->has_tree || ctx->D != 2 || ctx->seq_rec) return SRMG_OK;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(ctx->stream, &cap));
+  if (cap != cudaStreamCaptureStatusNone) return SRMG_OK;
+  ctx->push_state = -1;
+  const int64_t nf = ctx->max_blk * kSS;
+  if (nf <= 0 || nf >= ((int64_t)1 << 31)) return SRMG_OK;
+  static const int kPrime[9] = {2, 3, 5, 7, 11, 13, 17, 19, 23};
+  Signs ones, primes;
+  for (int i = 0; i < 9; i++) {
+    ones.v[i] = 1.0;
+    primes.v[i] = kPrime[i];
+  }
+  std::vector<double> h((size_t)(2 * nf));
+  {
+    double *d = nullptr;
+    CK(cudaMalloc(&d, (size_t)(2 * nf) * sizeof(double)));
+    const int64_t l0 = ctx->launches;
+    k_push_ident<<<grid_for(nf, 256, kGridCap), 256, 0, ctx->stream>>>(d, nf, 2);
+    int rc = SRMG_OK;
+    for (int l = 1; l <= ctx->nlev && rc == SRMG_OK; l++) {
+      rc = L_fill_ghost<double>(ctx, d, l, ones, 3);
+      if (rc == SRMG_OK) rc = L_fill_ghost<double>(ctx, d + nf, l, primes, 3);
+    }
+    ctx->launches = l0;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h.data(), d, (size_t)(2 * nf) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d);
+    RC(rc);
+    CK(e);
+  }
+  std::vector<std::vector<int4>> blocks(ctx->nlev);
+  std::vector<int> lvl_of((size_t)ctx->max_blk, 0), bi_of((size_t)ctx->max_blk, -1);
+  for (int l = 1; l <= ctx->nlev; l++) {
+    const DevLevel &L = ctx->lv[l - 1];
+    blocks[l - 1].resize(L.nblk);
+    if (L.nblk) CK(cudaMemcpy(blocks[l - 1].data(), L.blocks, L.nblk * sizeof(int4), cudaMemcpyDeviceToHost));
+    for (int bi = 0; bi < L.nblk; bi++) {
+      const int blk = blocks[l - 1][bi].x;
+      if (blk < 0 || blk >= ctx->max_blk) return SRMG_OK;
+      lvl_of[blk] = l;
+      bi_of[blk] = bi;
+    }
+  }
+  auto valid = [](int x, int y) { return x >= kG && x < kG + kM && y >= kG && y < kG + kM; };
+  bool ok2 = true, ok4 = true;
+  struct Ent { int key, dest, sg; };
+  std::vector<std::vector<Ent>> ents(ctx->nlev);
+  for (int l = 1; l <= ctx->nlev; l++)
+    for (int bi = 0; bi < ctx->lv[l - 1].nblk; bi++) {
+      const int blk = blocks[l - 1][bi].x;
+      for (int g = 0; g < kSS; g++) {
+        const int gx = g % kS, gy = g / kS;
+        if (valid(gx, gy)) continue;
+        const int64_t gi = (int64_t)blk * kSS + g;
+        const double a = h[gi], a2 = h[nf + gi];
+        if (a == 0.0) {
+          if (a2 != 0.0) return SRMG_OK;
+          continue;
+        }
+        if (!(a >= 1.0 && a <= (double)nf && a == std::floor(a))) return SRMG_OK;
+        const int64_t src = (int64_t)a - 1;
+        const int sblk = (int)(src / kSS), sc = (int)(src % kSS), sx = sc % kS, sy = sc / kS;
+        if (!valid(sx, sy) || lvl_of[sblk] != l) return SRMG_OK;
+        int s1 = 15, s2 = 15;
+        bool found = a2 == a;
+        for (int i = 0; i < 9 && !found; i++) {
+          if (a2 == a * kPrime[i]) {
+            s1 = i;
+            found = true;
+          }
+          for (int j = i; j < 9 && !found; j++)
+            if (a2 == a * (kPrime[i] * kPrime[j])) {
+              s1 = i;
+              s2 = j;
+              found = true;
+            }
+        }
+        if (!found) return SRMG_OK;
+        for (int dy = -1; dy <= 1; dy++)
+          for (int dx = -1; dx <= 1; dx++) {
+            const int rx = gx + dx, ry = gy + dy;
+            if (!valid(rx, ry) || (sblk == blk && rx == sx && ry == sy)) continue;
+            if (((rx ^ sx) & 1) == 0 && ((ry ^ sy) & 1) == 0) ok4 = false;
+            if (dx * dx + dy * dy == 1 && ((rx + ry + sx + sy) & 1) == 0) ok2 = false;
+          }
+        ents[l - 1].push_back({bi_of[sblk] * 256 + (sx - kG) + kM * (sy - kG), (int)gi, s1 | (s2 << 4)});
+      }
+    }
+  if (!ok2 && !ok4) return SRMG_OK;
+  // per level: offsets (nblk * 256 + 1 ints), then the entries sorted by source cell
+  std::vector<size_t> at(ctx->nlev);
+  size_t bytes = 0;
+  for (int l = 1; l <= ctx->nlev; l++) {
+    at[l - 1] = bytes;
+    const int nb = ctx->lv[l - 1].nblk;
+    if (!nb) continue;
+    bytes += ((size_t)nb * 256 + 1) * sizeof(int);
+    bytes = (bytes + 15) & ~(size_t)15;
+    bytes += ents[l - 1].size() * sizeof(int2);
+    bytes = (bytes + 15) & ~(size_t)15;
+  }
+  std::vector<char> stage(bytes);
+  for (int l = 1; l <= ctx->nlev; l++) {
+    const int nb = ctx->lv[l - 1].nblk;
+    if (!nb) continue;
+    int *off = reinterpret_cast<int *>(stage.data() + at[l - 1]);
+    const size_t ent_at = (at[l - 1] + ((size_t)nb * 256 + 1) * sizeof(int) + 15) & ~(size_t)15;
+    int2 *ent = reinterpret_cast<int2 *>(stage.data() + ent_at);
+    std::fill(off, off + nb * 256 + 1, 0);
+    for (const Ent &e : ents[l - 1]) off[e.key + 1]++;
+    for (int k = 0; k < nb * 256; k++) off[k + 1] += off[k];
+    std::vector<int> fillp(off, off + nb * 256);
+    for (const Ent &e : ents[l - 1]) ent[fillp[e.key]++] = make_int2(e.dest, e.sg);
+  }
+  RC(ensure(ctx, ctx->push_tab, bytes));
+  CK(cudaMemcpy(ctx->push_tab.p, stage.data(), bytes, cudaMemcpyHostToDevice));
+  ctx->push_lv.assign(ctx->nlev, PushView{nullptr, nullptr});
+  for (int l = 1; l <= ctx->nlev; l++) {
+    const int nb = ctx->lv[l - 1].nblk;
+    if (!nb) continue;
+    char *base = static_cast<char *>(ctx->push_tab.p);
+    const size_t ent_at = (at[l - 1] + ((size_t)nb * 256 + 1) * sizeof(int) + 15) & ~(size_t)15;
+    ctx->push_lv[l - 1] = PushView{reinterpret_cast<const int *>(base + at[l - 1]),
+                                   reinterpret_cast<const int2 *>(base + ent_at)};
+  }
+  ctx->push_ok2 = ok2;
+  ctx->push_ok4 = ok4;
+  ctx->push_state = 1;
+  return SRMG_OK;
+}
+
 template <typename T>
 int srmg::L_gs_colour(srmg_ctx *ctx, T *u, const T *b, int l, const OpParams<T> &p, int parity) {
   const DevLevel &L = ctx->lv[l - 1];
@@ -771,25 +933,50 @@ int srmg::L_gs_colour(srmg_ctx *ctx, T *u, const T *b, int l, const OpParams<T> 
   return SRMG_OK;
 }
 
+// One colour sweep that writes the copy and boundary ghosts of the cells it updates.
+template <typename T>
+static int L_gs_colour_push(srmg_ctx *ctx, T *u, const T *b, int l, const OpParams<T> &p, int parity,
+                            const Signs &sg) {
+  const DevLevel &L = ctx->lv[l - 1];
+  const int threads = 128;
+  unsigned sw = 0;  // entry + 1, two bits an entry (every entry is -1, 0 or 1 here)
+  for (int i = 0; i < 9; i++) sw |= (unsigned)((int)sg.v[i] + 1) << (2 * i);
+  if (p.op == SRMG_OP_LAPLACIAN4)
+    k_gs4_push<T><<<grid_for((int64_t)L.nblk * 64, threads, kGridCap), threads, 0, ctx->stream>>>(
+        u, b, L.view(l), p, parity >> 1, parity & 1, ctx->push_lv[l - 1], sw);
+  else
+    k_gs_colour_push<T><<<grid_for((int64_t)L.nblk * 128, threads, kGridCap), threads, 0, ctx->stream>>>(
+        u, b, L.view(l), p, wtab<T>(ctx), parity, ctx->push_lv[l - 1], sw);
+  ctx->launches++;
+  return SRMG_OK;
+}
+
+// gauss_seidel_iter! (src/multigrid.jl:250-295): red-black (two colours) or, at order 4,
+// four colours {0,0}, {0,1}, {1,0}, {1,1}, each followed by copy and boundary ghosts.
+// With the push tables (ensure_gs_push) the first colour keeps its fill launch -- after
+// it the ghosts are what the fill makes of the current cells, whatever they held before
+// -- and every later colour writes the ghosts of the cells it updates itself, which is
+// all that the fill after it would change: one launch a colour instead of two, the
+// same values.
 template <typename T>
 int srmg::L_gs_iter(srmg_ctx *ctx, T *u, const T *b, int l, const OpParams<T> &p, int n,
                     const Signs &sg) {
-  if (p.op == SRMG_OP_LAPLACIAN4) {
-    // four colours {0,0}, {0,1}, {1,0}, {1,1}, each followed by copy and boundary ghosts
-    // (src/multigrid.jl:268-295)
-    for (int i = 0; i < n; i++)
-      for (int c = 0; c < 4; c++) {
-        RC(L_gs_colour<T>(ctx, u, b, l, p, c));
-        RC(L_fill_ghost<T>(ctx, u, l, sg, 3));
+  const bool four = p.op == SRMG_OP_LAPLACIAN4;
+  if (ctx->push_state == 0) RC(ensure_gs_push(ctx));
+  bool unit = true;
+  for (int i = 0; i < 9; i++) unit = unit && (sg.v[i] == 1.0 || sg.v[i] == -1.0 || sg.v[i] == 0.0);
+  const bool push = ctx->use_gs_push && ctx->push_state == 1 && !ctx->seq_rec && unit &&
+                    (four ? ctx->push_ok4 : ctx->push_ok2) && ctx->lv[l - 1].nblk > 0;
+  const int ncol = four ? 4 : 2;
+  for (int i = 0; i < n; i++)
+    for (int c = 0; c < ncol; c++) {
+      if (push && (i > 0 || c > 0)) {
+        RC(L_gs_colour_push<T>(ctx, u, b, l, p, c, sg));
+        continue;
       }
-    return SRMG_OK;
-  }
-  for (int i = 0; i < n; i++) {
-    RC(L_gs_colour<T>(ctx, u, b, l, p, 0));
-    RC(L_fill_ghost<T>(ctx, u, l, sg, 3));
-    RC(L_gs_colour<T>(ctx, u, b, l, p, 1));
-    RC(L_fill_ghost<T>(ctx, u, l, sg, 3));
-  }
+      RC(L_gs_colour<T>(ctx, u, b, l, p, c));
+      RC(L_fill_ghost<T>(ctx, u, l, sg, 3));
+    }
   return SRMG_OK;
 }
 
@@ -1013,6 +1200,10 @@ extern "C" int srmg_set_option(srmg_ctx *ctx, const char *key, int64_t value) {
     ctx->use_op_seq = value != 0;
     if (!ctx->use_op_seq) drop_op_graphs(ctx);
   }
+  else if (!strcmp(key, "gs_push")) {
+    ctx->use_gs_push = value != 0;
+    drop_op_graphs(ctx);
+  }
   else if (!strcmp(key, "op_graphs")) {
     ctx->use_op_graphs = value != 0;
     if (!ctx->use_op_graphs) drop_op_graphs(ctx);
@@ -1077,6 +1268,7 @@ int srmg::vcycle_ops(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
   const bool seq = ctx->use_op_seq;
   if (!(ctx->use_op_graphs || seq) || ncycles <= 0 || cap != cudaStreamCaptureStatusNone)
     return run_vcycles(ctx, u, b, r, u1, s, op, k2, geom, bc, lmax, ndown, ntop, nup, omega, ncycles);
+  RC(ensure_gs_push(ctx));  // before the key: a graph bakes in whether the sweeps push
   std::vector<char> key;
   for (const void *p : {(const void *)u, (const void *)b, (const void *)r, (const void *)u1, (const void *)ctx->d_tree,
                         (const void *)ctx->stream})
@@ -1084,6 +1276,7 @@ int srmg::vcycle_ops(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
   for (double v : {s, k2, omega}) put(key, v);
   for (int v : {op, geom, lmax, ndown, ntop, nup, ncycles, ctx->D}) put(key, v);
   put(key, ctx->generation);
+  put(key, (int)(ctx->use_gs_push && ctx->push_state == 1));
   const int nbc = ctx->D == 3 ? 27 : 9;
   for (int i = 0; i < nbc; i++) put(key, (int8_t)(bc ? bc[i] : 1));
   if (seq) {

@@ -113,6 +113,14 @@ struct srmg_ctx {
   unsigned refbnd_levels = 0;  // bit l: level l has refinement-boundary faces
   bool has_corners = false;    // the tree came with a BoxStencil connectivity (diagonal edges)
   bool merge_fill = true;      // 3D: copy and boundary fill passes may share a launch
+  // 2D per-operation Gauss-Seidel: colour sweeps that write their own copy and boundary
+  // ghosts (ensure_gs_push).  push_state 0 = tables not built for this tree, 1 = built,
+  // -1 = not used on this tree.
+  bool use_gs_push = true;
+  int push_state = 0;
+  bool push_ok2 = false, push_ok4 = false;  // race-free for red-black / four-colour sweeps
+  srmg::DevBuf push_tab;
+  std::vector<srmg::PushView> push_lv;      // per level, index l-1
   bool trace_on = false;
   srmg::DevBuf trace;        // %globaltimer stamps after every engine phase (CTA 0)
 

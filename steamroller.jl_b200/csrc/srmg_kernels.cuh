@@ -255,9 +255,39 @@ __device__ __forceinline__ void d_fill_ghost(T *__restrict__ u, LevelView lv, Si
 
 // ---- red-black Gauss-Seidel colour sweep (src/multigrid.jl:153-180, 238-243) ------
 // Colour P updates valid cells with (x + y + 1) & 1 == P (0-based local indices).
+// Ghost pushes of a colour sweep (2D trees, per-operation path): for every valid cell
+// whose value a copy-and-boundary fill (fill_ghost! passes 1 and 2) writes into ghost
+// cells, the list of those ghosts, CSR by (level-local block, cell): off[bi*256 + cell]
+// .. off[bi*256 + cell + 1] index ent, ent = {ghost's index in the field, boundary-table
+// entries of the mirrors on the way (low and high 4 bits, 15 = none)}.  The sweep that
+// updates the cell writes them, so no fill launch has to follow it.  Built from the
+// fill itself (srmg.cu, ensure_gs_push).  The boundary table reaches the sweep packed,
+// two bits an entry (entry + 1: the pushes are used only where every entry is -1, 0 or 1).
+struct PushView {
+  const int *off;
+  const int2 *ent;
+};
+
 template <typename T>
-__device__ __forceinline__ void d_gs_colour(T *__restrict__ u, const T *__restrict__ b, LevelView lv,
-                            OpParams<T> p, WTab<T> wt, int parity) {
+__device__ __forceinline__ void push_ghosts(T *__restrict__ u, const PushView &pv, unsigned sg, int bi, int x, int y,
+                                            T v) {
+  const int c = bi * 256 + (x - kG) + kM * (y - kG);
+  const int e1 = pv.off[c + 1];
+  for (int e = pv.off[c]; e < e1; ++e) {
+    const int2 d = pv.ent[e];
+    T w = v;
+    // boundary-table entries are -1, 0 or 1: the products are exact in any order
+    const int k1 = d.y & 15, k2 = d.y >> 4;
+    if (k1 < 9) w = dmul<T>(T((int)((sg >> (2 * k1)) & 3u) - 1), w);
+    if (k2 < 9) w = dmul<T>(T((int)((sg >> (2 * k2)) & 3u) - 1), w);
+    u[d.x] = w;
+  }
+}
+
+template <typename T, bool kPush>
+__device__ __forceinline__ void d_gs_colour_impl(T *__restrict__ u, const T *__restrict__ b, LevelView lv,
+                                                 OpParams<T> p, WTab<T> wt, int parity, PushView pv,
+                                                 unsigned sg) {
   const int64_t total = (int64_t)lv.nblk * 128;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
@@ -270,8 +300,16 @@ __device__ __forceinline__ void d_gs_colour(T *__restrict__ u, const T *__restri
     const T Lu = apply5<T>(ub, x, y, w, p.centre);
     const int o = x + kS * y;
     const T v = fma(p.s, b[(int64_t)bk.x * kSS + o], Lu);
-    ub[o] = fma(p.nwc, v, ub[o]);
+    const T nv = fma(p.nwc, v, ub[o]);
+    ub[o] = nv;
+    if (kPush) push_ghosts<T>(u, pv, sg, bi, x, y, nv);
   }
+}
+
+template <typename T>
+__device__ __forceinline__ void d_gs_colour(T *__restrict__ u, const T *__restrict__ b, LevelView lv,
+                                            OpParams<T> p, WTab<T> wt, int parity) {
+  d_gs_colour_impl<T, false>(u, b, lv, p, wt, parity, PushView{nullptr, nullptr}, 0u);
 }
 
 // ---- residual (src/multigrid.jl:309-323, 349-354): r = -(b + Lu/s) ---------------
@@ -437,8 +475,9 @@ __global__ void __launch_bounds__(NT) k_reduce_sqrt(double *__restrict__ out,
 
 // gauss_seidel!(..., FourColors{P1,P2}) (src/multigrid.jl:206-232): cells
 // (2 + 2a + p1, 2 + 2b + p2), u -= omega (Lu + s b) / c, unfused.
-template <typename T>
-__device__ __forceinline__ void d_gs4(T *__restrict__ u, const T *__restrict__ b, LevelView lv, OpParams<T> p, int p1, int p2) {
+template <typename T, bool kPush>
+__device__ __forceinline__ void d_gs4_impl(T *__restrict__ u, const T *__restrict__ b, LevelView lv, OpParams<T> p,
+                                           int p1, int p2, PushView pv, unsigned sg) {
   const int64_t total = (int64_t)lv.nblk * 64;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
@@ -451,8 +490,15 @@ __device__ __forceinline__ void d_gs4(T *__restrict__ u, const T *__restrict__ b
     const int o = x + kS * y;
     const T cdiag = T(diagelm4(p.geom, ir, iz));
     const T upd = dmul<T>(p.omega, dadd<T>(Lu, dmul<T>(p.s, b[(int64_t)bk.x * kSS + o]))) / cdiag;
-    ub[o] = ub[o] - upd;
+    const T nv = ub[o] - upd;
+    ub[o] = nv;
+    if (kPush) push_ghosts<T>(u, pv, sg, bi, x, y, nv);
   }
+}
+
+template <typename T>
+__device__ __forceinline__ void d_gs4(T *__restrict__ u, const T *__restrict__ b, LevelView lv, OpParams<T> p, int p1, int p2) {
+  d_gs4_impl<T, false>(u, b, lv, p, p1, p2, PushView{nullptr, nullptr}, 0u);
 }
 
 // rhs! over rhs_level! (src/multigrid.jl:363-388): q1 = R q on the valid cells.  Order
@@ -622,6 +668,19 @@ __global__ void k_diff_level(T *__restrict__ dst, const T *__restrict__ a1, cons
 template <typename T>
 __global__ void k_gs4(T *__restrict__ u, const T *__restrict__ b, LevelView lv, OpParams<T> p, int p1, int p2) {
   d_gs4<T>(u, b, lv, p, p1, p2);
+}
+
+// The colour sweeps with their ghost pushes (PushView).
+template <typename T>
+__global__ void k_gs_colour_push(T *__restrict__ u, const T *__restrict__ b, LevelView lv, OpParams<T> p,
+                                 WTab<T> wt, int parity, PushView pv, unsigned sg) {
+  d_gs_colour_impl<T, true>(u, b, lv, p, wt, parity, pv, sg);
+}
+
+template <typename T>
+__global__ void k_gs4_push(T *__restrict__ u, const T *__restrict__ b, LevelView lv, OpParams<T> p, int p1, int p2,
+                           PushView pv, unsigned sg) {
+  d_gs4_impl<T, true>(u, b, lv, p, p1, p2, pv, sg);
 }
 
 }  // namespace srmg
