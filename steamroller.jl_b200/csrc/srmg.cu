@@ -778,7 +778,9 @@ static __global__ void k_push_ident(double *__restrict__ a, int64_t n, int copie
   }
 }
 
-int srmg::ensure_gs_push(srmg_ctx *ctx) {
+int srmg::ensure_gs_push(srmg_ctx *ctx, int op) {
+  if (ctx->D == 3)
+    return ctx->has_tree && (ctx->has_corners || op == SRMG_OP_LAPLACIAN4) ? d3_ensure_push(ctx) : SRMG_OK;
   if (ctx->push_state != 0 || !ctx->use_gs_push || !ctx->has_tree || ctx->D != 2 || ctx->seq_rec) return SRMG_OK;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   CK(cudaStreamIsCapturing(ctx->stream, &cap));
@@ -962,7 +964,7 @@ template <typename T>
 int srmg::L_gs_iter(srmg_ctx *ctx, T *u, const T *b, int l, const OpParams<T> &p, int n,
                     const Signs &sg) {
   const bool four = p.op == SRMG_OP_LAPLACIAN4;
-  if (ctx->push_state == 0) RC(ensure_gs_push(ctx));
+  if (ctx->push_state == 0) RC(ensure_gs_push(ctx, p.op));
   bool unit = true;
   for (int i = 0; i < 9; i++) unit = unit && (sg.v[i] == 1.0 || sg.v[i] == -1.0 || sg.v[i] == 0.0);
   const bool push = ctx->use_gs_push && ctx->push_state == 1 && !ctx->seq_rec && unit &&
@@ -1268,7 +1270,7 @@ int srmg::vcycle_ops(srmg_ctx *ctx, double *u, double *b, double *r, double *u1,
   const bool seq = ctx->use_op_seq;
   if (!(ctx->use_op_graphs || seq) || ncycles <= 0 || cap != cudaStreamCaptureStatusNone)
     return run_vcycles(ctx, u, b, r, u1, s, op, k2, geom, bc, lmax, ndown, ntop, nup, omega, ncycles);
-  RC(ensure_gs_push(ctx));  // before the key: a graph bakes in whether the sweeps push
+  RC(ensure_gs_push(ctx, op));  // before the key: a graph bakes in whether the sweeps push
   std::vector<char> key;
   for (const void *p : {(const void *)u, (const void *)b, (const void *)r, (const void *)u1, (const void *)ctx->d_tree,
                         (const void *)ctx->stream})

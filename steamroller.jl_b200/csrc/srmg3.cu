@@ -358,6 +358,76 @@ __global__ void k3_interp_add(double *__restrict__ u, const double *__restrict__
 __global__ void k3_copy(double *__restrict__ dst, const double *__restrict__ a1, const double *__restrict__ a2,
                         Level3View L) { d3_copy(dst, a1, a2, L); }
 
+// Table-driven ghost pushes of a colour sweep (octrees other than StarStencil{3} at
+// order 2): off[bi*4096 + cell] .. off[bi*4096 + cell + 1] index ent = {the ghost's
+// index in the field, up to three boundary-table entries of the mirrors on the way,
+// 5 bits each, 31 = none}; the boundary table comes packed, two bits an entry (entry
+// + 1: the pushes run only where every entry is -1, 0 or 1, so the products are exact
+// in any order).  Tables built from the fill itself (ensure_push3).
+__device__ __forceinline__ void push3(double *__restrict__ u, const PushView &pv, unsigned long long sg, int bi,
+                                      int x, int y, int z, double v) {
+  const int c = bi * 4096 + (x - kG) + kM * (y - kG) + kM * kM * (z - kG);
+  const int e1 = pv.off[c + 1];
+  for (int e = pv.off[c]; e < e1; ++e) {
+    const int2 d = pv.ent[e];
+    double w = v;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int i = (d.y >> (5 * k)) & 31;
+      if (i < 27) w = __dmul_rn((double)((int)((sg >> (2 * i)) & 3ull) - 1), w);
+    }
+    u[d.x] = w;
+  }
+}
+
+// d3_gs_rb / d3_gs4 with the table pushes after each update.
+__global__ void k3_gs_rb_tpush(double *__restrict__ u, const double *__restrict__ b, Level3View L, Op3 p, int parity,
+                               PushView pv, unsigned long long sg) {
+  const int64_t total = (int64_t)L.nblk * (kM * kM * kM / 2);
+  const double nwc = -(p.omega / p.diag);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t / 2048), c = (int)(t % 2048);
+    const int z = kG + c / 128, y = kG + (c / 8) % 16, k = c % 8;
+    const int pp = parity ^ ((y + 1) & 1) ^ ((z + 1) & 1);
+    const int x = kG + 2 * k + pp;
+    const int64_t base = (int64_t)L.blocks[bi].x * S3;
+    const int o = o3(x, y, z);
+    const double Lu = lhs3(u + base, o, p.op, p.centre);
+    const double v = fma(p.s, b[base + o], Lu);
+    const double nv = fma(nwc, v, u[base + o]);
+    u[base + o] = nv;
+    push3(u, pv, sg, bi, x, y, z, nv);
+  }
+}
+
+__global__ void k3_gs4_push(double *__restrict__ u, const double *__restrict__ b, Level3View L, Op3 p, int P1, int P2,
+                            PushView pv, unsigned long long sg) {
+  const int64_t total = (int64_t)L.nblk * 1024;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int bi = (int)(t / 1024), c = (int)(t % 1024);
+    const int z = kG + c / 64;
+    const int p1 = (P1 + z + 1) & 1, p2 = (P2 + z + 1) & 1;
+    const int x = kG + 2 * (c % 8) + p1, y = kG + 2 * ((c / 8) % 8) + p2;
+    const int64_t base = (int64_t)L.blocks[bi].x * S3;
+    const int o = o3(x, y, z);
+    const double Lu = lhs3(u + base, o, p.op, p.centre);
+    const double upd = __dmul_rn(p.omega, __dadd_rn(Lu, __dmul_rn(p.s, b[base + o]))) / p.diag;
+    const double nv = u[base + o] - upd;
+    u[base + o] = nv;
+    push3(u, pv, sg, bi, x, y, z, nv);
+  }
+}
+
+// Identity field for the push tables: valid cells hold their index in the field + 1,
+// ghosts 0; `copies` consecutive fields.
+__global__ void k3_push_ident(double *__restrict__ a, int64_t n, int copies) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % S3), x = c % S, y = (c / S) % S, z = c / S2;
+    const bool valid = x >= kG && x < kG + kM && y >= kG && y < kG + kM && z >= kG && z < kG + kM;
+    for (int k = 0; k < copies; ++k) a[k * n + i] = valid ? (double)(i + 1) : 0.0;
+  }
+}
+
 // ---- the sequencer (3D): a recorded per-operation V-cycle in one cooperative launch --
 // The records are the launches the per-operation path would make, in order; a grid
 // barrier (release/acquire on a counter, bounded wait) separates consecutive records,
@@ -525,6 +595,150 @@ int fill(srmg_ctx *ctx, double *u, int l, const Signs27 &sg, int mask) {
   return SRMG_OK;
 }
 
+// The push tables of an octree, read off its copy-and-boundary fill (mask 3) run on an
+// identity field: once with every boundary entry 1 (each ghost then holds its source
+// cell's index + 1, or 0 if it takes no valid cell's value) and once with entry k the
+// k-th prime (the ratio names the entries of the mirrors on the way, at most three).
+// The tables are used for a colouring only if no cell of the source's colour other
+// than the source reads a pushed ghost: the 6 face neighbours for red-black, the 18
+// face and edge neighbours of the order-4 stencil for four colours.  Anything the tables
+// cannot express leaves the tree on the fill launches (push_state -1).
+int ensure_push3(srmg_ctx *ctx) {
+  if (ctx->push_state != 0 || !ctx->use_gs_push || !ctx->has_tree || ctx->seq_rec) return SRMG_OK;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(ctx->stream, &cap));
+  if (cap != cudaStreamCaptureStatusNone) return SRMG_OK;
+  ctx->push_state = -1;
+  const int64_t nf = ctx->max_blk * S3;
+  if (nf <= 0 || nf >= ((int64_t)1 << 31)) return SRMG_OK;
+  static const int kPrime[27] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43,
+                                 47, 53, 59, 61, 67, 71, 73, 79, 83, 89, 97, 101, 103};
+  Signs27 ones, primes;
+  for (int i = 0; i < 27; i++) {
+    ones.v[i] = 1.0;
+    primes.v[i] = kPrime[i];
+  }
+  std::vector<double> h((size_t)(2 * nf));
+  {
+    double *d = nullptr;
+    CK(cudaMalloc(&d, (size_t)(2 * nf) * sizeof(double)));
+    const int64_t l0 = ctx->launches;
+    k3_push_ident<<<grid3(nf, 256), 256, 0, ctx->stream>>>(d, nf, 2);
+    int rc = SRMG_OK;
+    for (int l = 1; l <= ctx->nlev && rc == SRMG_OK; l++) {
+      rc = fill(ctx, d, l, ones, 3);
+      if (rc == SRMG_OK) rc = fill(ctx, d + nf, l, primes, 3);
+    }
+    ctx->launches = l0;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h.data(), d, (size_t)(2 * nf) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d);
+    RC(rc);
+    CK(e);
+  }
+  std::vector<std::vector<int4>> blocks(ctx->nlev);
+  std::vector<int> lvl_of((size_t)ctx->max_blk, 0), bi_of((size_t)ctx->max_blk, -1);
+  for (int l = 1; l <= ctx->nlev; l++) {
+    const Dev3Level &L = ctx->lv3[l - 1];
+    blocks[l - 1].resize(L.nblk);
+    if (L.nblk) CK(cudaMemcpy(blocks[l - 1].data(), L.blocks, L.nblk * sizeof(int4), cudaMemcpyDeviceToHost));
+    for (int bi = 0; bi < L.nblk; bi++) {
+      const int blk = blocks[l - 1][bi].x;
+      if (blk < 0 || blk >= ctx->max_blk) return SRMG_OK;
+      lvl_of[blk] = l;
+      bi_of[blk] = bi;
+    }
+  }
+  auto valid = [](int x, int y, int z) {
+    return x >= kG && x < kG + kM && y >= kG && y < kG + kM && z >= kG && z < kG + kM;
+  };
+  bool ok2 = true, ok4 = true;
+  struct Ent { int key, dest, sg; };
+  std::vector<std::vector<Ent>> ents(ctx->nlev);
+  for (int l = 1; l <= ctx->nlev; l++)
+    for (int bi = 0; bi < ctx->lv3[l - 1].nblk; bi++) {
+      const int blk = blocks[l - 1][bi].x;
+      for (int g = 0; g < S3; g++) {
+        const int gx = g % S, gy = (g / S) % S, gz = g / S2;
+        if (valid(gx, gy, gz)) continue;
+        const int64_t gi = (int64_t)blk * S3 + g;
+        const double a = h[gi], a2 = h[nf + gi];
+        if (a == 0.0) {
+          if (a2 != 0.0) return SRMG_OK;
+          continue;
+        }
+        if (!(a >= 1.0 && a <= (double)nf && a == std::floor(a))) return SRMG_OK;
+        const int64_t src = (int64_t)a - 1;
+        const int sblk = (int)(src / S3), sc = (int)(src % S3);
+        const int sx = sc % S, sy = (sc / S) % S, sz = sc / S2;
+        if (!valid(sx, sy, sz) || lvl_of[sblk] != l) return SRMG_OK;
+        // the ratio of the two runs, factored into at most three primes
+        const double q = a2 / a;
+        if (!(q >= 1.0 && q == std::floor(q) && a2 == a * q)) return SRMG_OK;
+        int64_t rest = (int64_t)q;
+        int idx[3] = {31, 31, 31}, nidx = 0;
+        for (int i = 0; i < 27 && rest > 1; i++)
+          while (rest % kPrime[i] == 0 && rest > 1) {
+            if (nidx == 3) return SRMG_OK;
+            idx[nidx++] = i;
+            rest /= kPrime[i];
+          }
+        if (rest != 1) return SRMG_OK;
+        for (int dz = -1; dz <= 1; dz++)
+          for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+              const int nz = (dx != 0) + (dy != 0) + (dz != 0);
+              if (nz == 0 || nz == 3) continue;
+              const int rx = gx + dx, ry = gy + dy, rz = gz + dz;
+              if (!valid(rx, ry, rz) || (sblk == blk && rx == sx && ry == sy && rz == sz)) continue;
+              if (((rx + rz + sx + sz) & 1) == 0 && ((ry + rz + sy + sz) & 1) == 0) ok4 = false;
+              if (nz == 1 && ((rx + ry + rz + sx + sy + sz) & 1) == 0) ok2 = false;
+            }
+        ents[l - 1].push_back({bi_of[sblk] * 4096 + (sx - kG) + kM * (sy - kG) + kM * kM * (sz - kG), (int)gi,
+                               idx[0] | (idx[1] << 5) | (idx[2] << 10)});
+      }
+    }
+  if (!ok2 && !ok4) return SRMG_OK;
+  std::vector<size_t> at(ctx->nlev), ent_at(ctx->nlev);
+  size_t bytes = 0;
+  for (int l = 1; l <= ctx->nlev; l++) {
+    const int nb = ctx->lv3[l - 1].nblk;
+    at[l - 1] = ent_at[l - 1] = bytes;
+    if (!nb) continue;
+    bytes += ((size_t)nb * 4096 + 1) * sizeof(int);
+    bytes = (bytes + 15) & ~(size_t)15;
+    ent_at[l - 1] = bytes;
+    bytes += ents[l - 1].size() * sizeof(int2);
+    bytes = (bytes + 15) & ~(size_t)15;
+  }
+  std::vector<char> stage(bytes);
+  for (int l = 1; l <= ctx->nlev; l++) {
+    const int nb = ctx->lv3[l - 1].nblk;
+    if (!nb) continue;
+    int *off = reinterpret_cast<int *>(stage.data() + at[l - 1]);
+    int2 *ent = reinterpret_cast<int2 *>(stage.data() + ent_at[l - 1]);
+    std::fill(off, off + nb * 4096 + 1, 0);
+    for (const Ent &e : ents[l - 1]) off[e.key + 1]++;
+    for (int k = 0; k < nb * 4096; k++) off[k + 1] += off[k];
+    std::vector<int> fillp(off, off + nb * 4096);
+    for (const Ent &e : ents[l - 1]) ent[fillp[e.key]++] = make_int2(e.dest, e.sg);
+  }
+  RC(ensure(ctx, ctx->push_tab, bytes));
+  CK(cudaMemcpy(ctx->push_tab.p, stage.data(), bytes, cudaMemcpyHostToDevice));
+  ctx->push_lv.assign(ctx->nlev, PushView{nullptr, nullptr});
+  char *base = static_cast<char *>(ctx->push_tab.p);
+  for (int l = 1; l <= ctx->nlev; l++)
+    if (ctx->lv3[l - 1].nblk)
+      ctx->push_lv[l - 1] = PushView{reinterpret_cast<const int *>(base + at[l - 1]),
+                                     reinterpret_cast<const int2 *>(base + ent_at[l - 1])};
+  ctx->push_ok2 = ok2;
+  ctx->push_ok4 = ok4;
+  ctx->push_state = 1;
+  return SRMG_OK;
+}
+
 int gs_colour(srmg_ctx *ctx, double *u, const double *b, int l, const Op3 &p, int colour) {
   const int n = ctx->nblk_host[l - 1];
   if (!n) return SRMG_OK;
@@ -551,11 +765,34 @@ int gs_iter(srmg_ctx *ctx, double *u, const double *b, int l, const Op3 &p, int 
   const int ncol = p.op == SRMG_OP_LAPLACIAN4 ? 4 : 2;
   const bool push = gs_pushes(ctx, p);
   const int nb = ctx->nblk_host[l - 1];
+  // elsewhere the table pushes (ensure_push3): the first colour keeps its fill launch,
+  // which makes the ghosts what the fill makes of the current cells; every later colour
+  // writes the ghosts of the cells it updates, all that the fill after it would change
+  bool tpush = false;
+  unsigned long long sw = 0;
+  if (!push && ctx->use_gs_push && nb > 0) {
+    if (ctx->push_state == 0) RC(ensure_push3(ctx));
+    bool unit = true;
+    for (int i = 0; i < 27; i++) unit = unit && (sg.v[i] == 1.0 || sg.v[i] == -1.0 || sg.v[i] == 0.0);
+    tpush = ctx->push_state == 1 && !ctx->seq_rec && unit &&
+            (p.op == SRMG_OP_LAPLACIAN4 ? ctx->push_ok4 : ctx->push_ok2);
+    for (int i = 0; tpush && i < 27; i++) sw |= (unsigned long long)((int)sg.v[i] + 1) << (2 * i);
+  }
   for (int i = 0; i < n; ++i)
     for (int c = 0; c < ncol; ++c) {
       if (push) {
         if (!nb || seq3_push(ctx, S3_GS_RB_PUSH, c, 0, u, b, nullptr, view(ctx, l), &p, &sg)) continue;
         k3_gs_rb_push<<<grid3((int64_t)nb * 2048, 256), 256, 0, ctx->stream>>>(u, b, view(ctx, l), p, c, sg);
+        ctx->launches++;
+        continue;
+      }
+      if (tpush && (i > 0 || c > 0)) {
+        if (p.op == SRMG_OP_LAPLACIAN4)
+          k3_gs4_push<<<grid3((int64_t)nb * 1024, 256), 256, 0, ctx->stream>>>(u, b, view(ctx, l), p, c >> 1, c & 1,
+                                                                               ctx->push_lv[l - 1], sw);
+        else
+          k3_gs_rb_tpush<<<grid3((int64_t)nb * 2048, 256), 256, 0, ctx->stream>>>(u, b, view(ctx, l), p, c,
+                                                                                  ctx->push_lv[l - 1], sw);
         ctx->launches++;
         continue;
       }
@@ -684,6 +921,9 @@ int pack3(const int64_t v[3], int add) {
 }
 
 }  // namespace
+
+// the D = 3 part of ensure_gs_push: octrees whose sweeps do not push by rule
+int srmg::d3_ensure_push(srmg_ctx *ctx) { return ensure_push3(ctx); }
 
 // ------------------------------------------------------------------ tree upload
 

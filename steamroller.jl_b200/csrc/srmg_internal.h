@@ -17,9 +17,11 @@ int check_call_any(srmg_ctx *ctx, int64_t nblk_alloc, int op, int geom, const in
 // values per block of the context's fields: 20^D
 inline int64_t block_elems(const srmg_ctx *ctx) { return ctx->D == 3 ? (int64_t)kS * kS * kS : (int64_t)kSS; }
 void free_tree(srmg_ctx *ctx);
-// Builds the 2D Gauss-Seidel push tables of the context's tree once (not while the
-// stream is capturing or a sequence is recorded): push_state becomes 1 or -1.
-int ensure_gs_push(srmg_ctx *ctx);
+// Builds the Gauss-Seidel push tables of the context's tree once (not while the stream
+// is capturing or a sequence is recorded): push_state becomes 1 or -1.  On octrees only
+// where the sweeps of operator `op` do not push by rule (BoxStencil{3} or order 4).
+int ensure_gs_push(srmg_ctx *ctx, int op);
+int d3_ensure_push(srmg_ctx *ctx);
 void drop_op_graphs(srmg_ctx *ctx);
 // One cooperative launch of the sequencer over `nops` recorded operations (srmg_seq.cu).
 int seq_launch(srmg_ctx *ctx, const void *d_ops, int nops);

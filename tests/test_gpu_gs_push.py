@@ -109,3 +109,45 @@ def test_gs_iter_push_with_stale_ghosts():
             ctx.close()
         for l, (a, g) in enumerate(zip(res[1], res[0])):
             np.testing.assert_array_equal(_bits(a), _bits(g), err_msg=f"op {lpl_op} level {l + 1}")
+
+
+def cases3():
+    from srmg import gen3
+    from srmg.tree3 import Tree3, populate, connectivity as connectivity3, BOX3
+    t = Tree3((1, 1, 1), 3)
+    populate(t, 3)
+    # (order 4 needs a BoxStencil{3} connectivity)
+    for name, stencil, op, lpl in (("box3_order2", BOX3, 0, None), ("box3_order4", BOX3, 2, "laplacian4")):
+        conn = connectivity3(t, stencil)
+        p = gen3.make_problem3(t, conn, lambda x, y, z: np.cos(3 * x) * y * (1 - z), (1.0 / 16) ** 2, op=op)
+        yield name, t, conn, p, lpl
+
+
+@pytest.mark.parametrize("case", list(cases3()), ids=lambda c: c[0])
+def test_octree_vcycle_and_fmg_push_bit_identical(case):
+    """The octrees whose sweeps do not push by rule (BoxStencil{3}, order 4) push from
+    tables read off their fill; V-cycles and FMG equal the fill path's bit for bit."""
+    import torch
+    _, t, conn, p, lpl = case
+    out, launches = {}, {}
+    for push in (1, 0):
+        ctx = mg.Context(0, D=3).set_tree(t, conn)
+        for k, v in dict(op_graphs=0, op_sequencer=0, gs_push=push).items():
+            ctx.set_option(k, v)
+        b = torch.from_numpy(p.b).cuda()
+        u, r, u1 = torch.zeros_like(b), torch.zeros_like(b), torch.zeros_like(b)
+        torch.cuda.synchronize()
+        l0 = ctx.launches()
+        mg.vcycle_(ctx, u, b, r, u1, p.s, 0, p.bc, lpl, ndown=2, ntop=4, nup=2, ncycles=2)
+        ctx.synchronize()
+        launches[push] = ctx.launches() - l0
+        v = u.cpu().numpy().copy()
+        u.zero_()
+        b.copy_(torch.from_numpy(p.b))
+        mg.fmg_(ctx, u, b, r, u1, p.s, 0, p.bc, lpl, ndown=2, ntop=4, nup=2)
+        ctx.synchronize()
+        out[push] = (v, u.cpu().numpy().copy())
+        ctx.close()
+    for a, g, what in zip(out[1], out[0], ("vcycle", "fmg")):
+        np.testing.assert_array_equal(_bits(a), _bits(g), err_msg=what)
+    assert launches[1] < launches[0]
