@@ -574,7 +574,8 @@ int srmg_ssprk3_stage_dev(srmg_ctx *ctx, double *out, const double *n, const dou
  *                      one cooperative launch that walks the recorded operations with
  *                      a grid barrier between consecutive ones (bit-identical results);
  *                      0 (default: graph replay measured faster on 2D and 3D trees);
- *   "gs_push"          1 (default) = on 2D trees off the persistent engine, every colour
+ *   "gs_push"          1 (default) = on 2D trees off the persistent engine and on
+ *                      BoxStencil{3} or order-4 octrees, every colour
  *                      sweep of gauss_seidel_iter! after its first writes the copy and
  *                      boundary ghosts of the cells it updates, instead of a fill launch
  *                      after it (bit-identical results; tables built once per tree from
